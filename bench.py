@@ -1,0 +1,340 @@
+#!/usr/bin/env python
+"""Benchmark: particle-steps/s of the plain path at N=1,048,576, theta=0.5.
+
+Workload (the precision-study disk at theta 0.5): N = 1,048,576 equal-mass
+bodies (m = 1e-9 Msun) around a 1 Msun star, Keplerian disk in XZ with r in
+[0.3, 30] AU (Sigma ~ r^-1.5), Rayleigh e/i (sigma 0.01 / 0.005 rad),
+softening 5e-4 AU, dt 0.002 T0, no collisions, drag or perturber, FP32 state
+(the reference's ParticleData precision), FP32 forces.  Inputs are seeded
+synthetic disks (seed = rank); there is no dataset.
+
+A step is one pass of src/main.cu:101-139 through the engine (nbody_sim_step):
+fused stream kernel, keys, radix sort, permute, tree, walk.  Each timed step
+is bracketed by CUDA events on the engine's stream with an L2 flush (a 256 MB
+write) before it, outside the events.  ``value`` is whole-job particle-steps/s
+(sum over ranks / max time over ranks).  ``e2e`` is the same metric through
+nbody_sim_step_host with pinned host buffers: copyToGPU of x..az + mass, one
+step, copyToCPU of x..az, every step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU (torchrun): every rank advances its own disk (independent replicas,
+no collective in the data path; "scaling": "weak").
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+METRIC = "particle-steps/s at N=1M theta=0.5"
+UNIT = "particle-steps/s"
+WORKLOAD = dict(n=1 << 20, r_min=0.3, r_max=30.0, m=1e-9, eps=5e-4, theta=0.5, dt=0.002)
+# interactions of the walk, per accepted source-target pair (survey 8d):
+# 3 sub, 3 FMA as 2 each for r^2+eps^2, rsqrt as 1, 3 mul, 3 FMA as 2 each
+FLOP_PER_INTERACTION = 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=WORKLOAD["n"])
+    ap.add_argument("--theta", type=float, default=WORKLOAD["theta"])
+    ap.add_argument("--precision", choices=["f32", "f64"], default="f32")
+    ap.add_argument("--leaf-max", type=int, default=8)
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-flush", action="store_true")
+    return ap.parse_args()
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=timedelta(seconds=300))
+    return ws, rank, local
+
+
+def allreduce_max(v: float, ws: int) -> float:
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def make_ic(nb, n, seed, dtype=np.float32):
+    d = nb.make_disk(n, WORKLOAD["r_min"], WORKLOAD["r_max"], 0.01, 0.005, 1.0, seed)
+    st = {k: v.astype(dtype) for k, v in d.items()}
+    st["m"] = np.full(n, WORKLOAD["m"], np.float32)
+    return st
+
+
+class Clocks:
+    """nvidia-smi samples (200 ms) of the GPU during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.p = None
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-i", str(index), "-lms", "200"], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            out, _ = self.p.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+            out, _ = self.p.communicate()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower() in ("active", "1", "yes"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def fp32_peak(smax_mhz: float | None):
+    """FP32 SIMT peak from the SM count and the max SM clock (no measured
+    FP32 figure exists for this pool): SMs x 128 lanes x 2 FLOP x clock."""
+    import torch
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    mhz = smax_mhz or 1965.0
+    peaks = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks):
+        with open(peaks) as f:
+            mhz = float(json.load(f).get("sm_max_mhz", mhz))
+    return sms * 128 * 2 * mhz * 1e6 / 1e12, f"derived: {sms} SM x 128 FP32 lanes x 2 x {mhz:.0f} MHz"
+
+
+def walk_traffic():
+    """Per-launch DRAM bytes of the walk from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "walk_n1m_traffic.txt")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        for line in f:
+            if line.startswith("bytes_per_launch"):
+                return float(line.split("=")[1])
+    return None
+
+
+def cpu_port_step(st, n, nthreads=0, steps=1):
+    """The CPU restatement of the reference step (oracle/port.c), timed."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    port = oracle.Port()
+    w = WORKLOAD
+    sp = port.step_params(w["dt"], w["theta"], w["eps"], 1.0, r_coll=0.0, collisions=False)
+    s = {k: np.array(st[k][:n], np.float32) for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+    port.run(s, sp, 0, nthreads=nthreads)  # initial forces (untimed)
+    t0 = time.perf_counter()
+    port.run(s, sp, steps, nthreads=nthreads, initial_forces=False)
+    return time.perf_counter() - t0
+
+
+def run_reference(args, ws, rank):
+    """The reference's CPU path (its host build of the force and integrator
+    formulas, oracle/port.c) on all host cores; rank 0 only."""
+    if rank != 0:
+        return
+    import importlib
+    nb = importlib.import_module("nbody-sim_b200")
+    n = args.n
+    st = make_ic(nb, n, 0)
+    cores = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_port_step(st, n, 0, 1)
+    secs = [cpu_port_step(st, n, 0, 1) for _ in range(args.steps)]
+    total = sum(secs)
+    value = n * args.steps / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"Keplerian disk N={n} r=[0.3,30] AU theta={args.theta} "
+                               f"eps=5e-4 dt=0.002, FP32 state", "n": n, "theta": args.theta,
+                   "parallelism": "cpu", "l2": "n/a (host)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} full steps at N={n} (CAS-octree build, "
+                                   "20-pass summarize, DFS sort, walk, KDK), OpenMP"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+    nb = importlib.import_module("nbody-sim_b200")
+    torch.cuda.set_device(local)
+    n = args.n
+    w = WORKLOAD
+    prec = nb.STATE_F64 if args.precision == "f64" else nb.STATE_F32
+    st = make_ic(nb, n, rank, np.float64 if prec == nb.STATE_F64 else np.float32)
+    prm = nb.sim_params(dt=w["dt"], theta=args.theta, softening=w["eps"], star_mass=1.0,
+                        r_coll=0.0, restitution=0.0, gas_drag_rate=0.0, state_precision=prec,
+                        leaf_max=args.leaf_max)
+    stream = torch.cuda.current_stream()
+    sim = nb.Sim(prm, n)
+    sim.set_stream(stream.cuda_stream)
+    sim.set_state(st["x"], st["y"], st["z"], st["vx"], st["vy"], st["vz"], st["m"])
+    for _ in range(args.warmup):
+        sim.step(1)
+    sim.sync()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    sim.set_profiling(True)
+    sim.profile(reset=True)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    clocks = Clocks(torch.cuda.current_device()) if rank == 0 else None
+    barrier(ws)
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        if not args.no_flush:
+            flush.zero_()
+        starts[k].record(stream)
+        sim.step(1)
+        ends[k].record(stream)
+    torch.cuda.synchronize()
+    barrier(ws)
+    ck = clocks.stop() if clocks else None
+    sim.sync()
+    ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    prof = sim.profile(reset=True)
+    stats = sim.stats()
+    ms_max = allreduce_max(ms, ws)
+    value = n * ws * args.steps / (ms_max * 1e-3)
+
+    # e2e: the public host-buffer call, pinned memory, copies in the timed region
+    e2e = None
+    if args.e2e_steps > 0 and prec == nb.STATE_F32:
+        pin = {k: torch.from_numpy(np.ascontiguousarray(st[k], np.float32)).pin_memory()
+               for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+        g = sim.get_state()
+        for k in ("ax", "ay", "az"):
+            pin[k] = torch.from_numpy(g[k]).pin_memory()
+        for k in ("x", "y", "z", "vx", "vy", "vz"):
+            pin[k].copy_(torch.from_numpy(g[k]))
+        host = {k: v.numpy() for k, v in pin.items()}
+        sim.set_profiling(False)
+        sim.step_host(host, host["m"], 1)  # warm-up
+        es = [torch.cuda.Event(enable_timing=True) for _ in range(args.e2e_steps)]
+        ee = [torch.cuda.Event(enable_timing=True) for _ in range(args.e2e_steps)]
+        barrier(ws)
+        for k in range(args.e2e_steps):
+            es[k].record(stream)
+            sim.step_host(host, host["m"], 1)
+            ee[k].record(stream)
+        torch.cuda.synchronize()
+        e_ms = allreduce_max(sum(a.elapsed_time(b) for a, b in zip(es, ee)), ws)
+        e2e = {"value": n * ws * args.e2e_steps / (e_ms * 1e-3), "unit": UNIT,
+               "h2d_bytes_per_step": 4 * n * 10, "d2h_bytes_per_step": 4 * n * 9,
+               "ms_per_step": e_ms / args.e2e_steps}
+
+    walk_ms = prof["walk"] / max(prof["steps"], 1)
+    flops = FLOP_PER_INTERACTION * stats.interactions
+    peak, peak_src = fp32_peak(ck["sm_max_mhz"] if ck else None)
+    achieved = flops / (walk_ms * 1e-3) / 1e12
+    traffic = walk_traffic()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"Keplerian disk N={n} r=[0.3,30] AU theta={args.theta} "
+                               f"eps=5e-4 dt=0.002, {args.precision.upper()} state, "
+                               "no collisions/drag/perturber", "n": n, "theta": args.theta,
+                   "state": args.precision, "leaf_max": args.leaf_max,
+                   "parallelism": f"replicas x{ws}",
+                   "l2": "flushed (256 MB write) before every timed step"},
+        "gpu_launches": int(prof["launches"]),
+        "phase_ms_per_step": {k: prof[k] / max(prof["steps"], 1)
+                              for k in nb.PHASE_NAMES},
+        "interactions_per_particle": stats.interactions / n,
+        "roofline": {"bound": "fp32-simt", "kernel": "k_walk", "achieved": achieved,
+                     "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                     "peak_source": peak_src, "traffic": traffic,
+                     "algorithmic": f"{FLOP_PER_INTERACTION} FLOP x {stats.interactions} "
+                                    "interactions per launch"},
+        "e2e": e2e,
+        "clocks": ck,
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cores = os.cpu_count() or 1
+        secs = cpu_port_step(st, n, 0, 1)
+        line["cpu_baseline"] = {"value": n / secs, "unit": UNIT, "cores": cores, "kind": "port",
+                                "sample": f"1 full step at N={n} of the reference algorithm "
+                                          "(oracle/port.c: CAS octree, summarize, DFS, walk, "
+                                          "KDK), OpenMP"}
+    sim.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, ws, rank)
+        else:
+            run_ours(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,334 @@
+/*
+ * nbody_b200.h -- C ABI of libnbody_b200.so, the B200 (sm_100a) engine for the
+ * per-step path of ualiberik/nbody-sim: octree build, Barnes-Hut force walk,
+ * perturber, two-pass collision impulse, KDK leapfrog + gas drag, FoF
+ * aggregates and the frames.bin / stats.csv writers.
+ *
+ * Plain pointers and sizes only.  Every entry point returns NBODY_OK (0) or an
+ * NBODY_ERR_* code; nbody_last_error() then gives a message (thread-local).
+ * Each function below names the reference interface it replaces
+ * (path:line within the reference project).
+ *
+ * Threading and synchronisation: the phase functions (nbody_tree_*,
+ * nbody_half_kick, ...) mirror the reference launchers, which all return
+ * after cudaDeviceSynchronize (include/Integrator.cuh:6, BHTree.cuh:42); they
+ * run on the legacy default stream and synchronise it before returning.  The
+ * engine functions (nbody_sim_*) are asynchronous on the engine's stream
+ * until nbody_sim_sync().
+ */
+#ifndef NBODY_B200_H
+#define NBODY_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NBODY_OK 0
+#define NBODY_ERR_CUDA 1      /* a CUDA runtime call failed                         */
+#define NBODY_ERR_ARG 2       /* bad argument (size mismatch, null pointer, range)  */
+#define NBODY_ERR_OVERFLOW 3  /* a bounded device loop gave up (stack, union-find)  */
+#define NBODY_ERR_TIMEOUT 4   /* reserved: a bounded wait expired                  */
+#define NBODY_ERR_IO 5        /* file could not be opened / written                 */
+#define NBODY_ERR_CONFIG 6    /* configuration rejected (loadConfig's checks)       */
+#define NBODY_ERR_STATE 7     /* call out of order (e.g. force before build)        */
+
+#define NBODY_ABI_VERSION 1
+
+const char* nbody_last_error(void);
+int nbody_abi_version(void);
+
+/* ---------------------------------------------------------------- data --- */
+
+/* SoA particle arrays; same fields, order and types as ParticleData
+ * (include/ParticleData.h:19-32).  Pointers are device pointers for the phase
+ * API, host or device (as stated) elsewhere. */
+typedef struct nbody_particles {
+  float* x;
+  float* y;
+  float* z;
+  float* vx;
+  float* vy;
+  float* vz;
+  float* ax;
+  float* ay;
+  float* az;
+  float* mass;
+  int* id;
+  int n;
+} nbody_particles;
+
+/* Config (include/Config.h:4-36): same fields and defaults. */
+typedef struct nbody_config {
+  int n_particles;
+  float disk_r_min;
+  float disk_r_max;
+  float disk_h_factor;
+  float particle_mass_msun;
+  float star_mass_msun;
+  float softening_AU;
+  float theta;
+  float collision_radius_factor;
+  float restitution;
+  float gas_drag_rate;
+  float dt;
+  float total_time;
+  int output_every_n_steps;
+  char output_dir[1024];
+  int perturber_enabled;
+  float perturber_mass_mjup;
+  float perturber_radius_AU;
+  float perturber_phase0;
+} nbody_config;
+
+/* Config member initialisers (include/Config.h:5-35). */
+void nbody_config_defaults(nbody_config* cfg);
+/* loadConfig (src/config/Config.cpp:6-55): same keys, defaults, checks and
+ * messages; NBODY_ERR_IO for an unreadable file, NBODY_ERR_CONFIG otherwise. */
+int nbody_config_load(const char* path, nbody_config* cfg);
+/* particlePhysicalRadius (src/disk/DiskInit.cpp:10-16), AU at 3000 kg/m^3. */
+float nbody_particle_radius(float particle_mass_msun);
+
+/* Perturber (include/Perturber.h:28-37). */
+typedef struct nbody_perturber {
+  int enabled;
+  float r;
+  float mass_msun;
+  float phase0;
+  float omega;
+  float x, y, z;
+} nbody_perturber;
+/* makePerturber (include/Perturber.h:39-57). */
+void nbody_perturber_make(const nbody_config* cfg, nbody_perturber* p);
+/* updatePerturber (include/Perturber.h:60-66). */
+void nbody_perturber_update(nbody_perturber* p, float sim_time);
+
+/* ------------------------------------------------- octree phase API --- */
+
+typedef struct nbody_tree nbody_tree;
+
+/* allocateOctree (src/physics/BHTree.cu:358-381). */
+int nbody_tree_create(int n_bodies, nbody_tree** out);
+/* freeOctree (src/physics/BHTree.cu:383-395). */
+void nbody_tree_destroy(nbody_tree* t);
+/* resetOctree (src/physics/BHTree.cu:397-420): nothing to clear here (the
+ * build overwrites every node it uses); resets the device status word. */
+int nbody_tree_reset(nbody_tree* t);
+/* launchBBoxKernel (src/physics/BHTree.cu:422-452): bbox of p->x,y,z padded
+ * x1.001 about its middle, computed and padded on the device. */
+int nbody_tree_bbox(nbody_tree* t, const nbody_particles* p);
+/* launchBuildKernel (src/physics/BHTree.cu:454-499): Morton keys, radix sort,
+ * Karras radix tree.  Runs the bbox itself if nbody_tree_bbox was not called. */
+int nbody_tree_build(nbody_tree* t, const nbody_particles* p);
+/* launchSummarizeKernel (src/physics/BHTree.cu:501-516): FP64 centre of mass
+ * and mass of every node in one bottom-up pass, and the octree layout. */
+int nbody_tree_summarize(nbody_tree* t);
+/* launchSortKernel (src/physics/BHTree.cu:518-525): fills the tree's sort_idx
+ * (nbody_tree_sort_idx) with the body order of the octree (Morton order). */
+int nbody_tree_sort(nbody_tree* t);
+/* tree.sort_idx (include/BHTree.cuh:20): device array of n_bodies ints. */
+int* nbody_tree_sort_idx(nbody_tree* t);
+/* Copies tree.sort_idx into dst (device if dst_on_device, else host), the
+ * cudaMemcpy of tests/test_bhtree.cu:14. */
+int nbody_tree_sort_idx_copy(nbody_tree* t, int* dst, int dst_on_device);
+/* launchForceKernel (src/physics/BHTree.cu:600-609): OVERWRITES p->ax,ay,az
+ * with the softened star pull plus the Barnes-Hut sum (theta = half-size over
+ * distance to the centre of mass, BHTree.cu:577). */
+int nbody_tree_force(nbody_tree* t, nbody_particles* p, float theta, float softening,
+                     float star_mass);
+/* launchCollisionKernel (src/physics/BHTree.cu:688-708): two-pass inelastic
+ * impulse for pairs closer than r_coll; updates p->vx,vy,vz in place. */
+int nbody_tree_collide(nbody_tree* t, nbody_particles* p, float r_coll, float restitution);
+/* Bodies opened directly instead of subdivided further (default 8). */
+int nbody_tree_set_leaf_max(nbody_tree* t, int leaf_max);
+
+typedef struct nbody_tree_stats {
+  int n_bodies;
+  int n_nodes;
+  float bbox_min[3];   /* padded, as tree.bbox_min after launchBBoxKernel */
+  float bbox_max[3];
+  float root_center[3];
+  float root_half;     /* cell_size of the root (BHTree.cu:484-485)      */
+  double root_mass;
+  double root_com[3];
+  unsigned long long interactions; /* accepted interactions of the last force */
+  int status;          /* device status bits of the last calls                */
+} nbody_tree_stats;
+int nbody_tree_stats_get(nbody_tree* t, nbody_tree_stats* out);
+
+/* ---------------------------------------------- integrator / perturber --- */
+
+/* launchHalfKickKernel (include/Integrator.cuh:9, Integrator.cu:80-85). */
+int nbody_half_kick(nbody_particles* p, float dt_half);
+/* launchDriftKernel (include/Integrator.cuh:12, Integrator.cu:87-92). */
+int nbody_drift(nbody_particles* p, float dt);
+/* launchResetAccelerationKernel (include/Integrator.cuh:15). */
+int nbody_reset_acc(nbody_particles* p);
+/* launchGasDragKernel (include/Integrator.cuh:21-22, Integrator.cu:100-109):
+ * no-op when drag_rate <= 0; decay = expf(-drag_rate * dt) on the host. */
+int nbody_gas_drag(nbody_particles* p, float drag_rate, float dt, float star_mass);
+/* launchPerturberForceKernel (include/Perturber.h:73-75): ADDS the pull. */
+int nbody_perturber_force(nbody_particles* p, float px, float py, float pz, float pmass,
+                          float softening);
+
+/* ------------------------------------------------------------- FoF --- */
+
+/* GPU friends-of-friends over device positions x,y,z (n bodies), linking
+ * pairs with ((dx*dx + dy*dy) + dz*dz) < link_length^2 in FP32 exactly as
+ * detectAggregates (src/analysis/Aggregate.cpp:26-52).  Outputs (device):
+ * labels[i] = smallest index in i's group, agg_size[i] = group size clamped
+ * to 65535 or 1 for singletons (src/main.cu:153-161).  *n_groups (host) =
+ * groups with >= 2 members.  Uses t's buffers (t must hold >= n bodies). */
+int nbody_fof(nbody_tree* t, const float* x, const float* y, const float* z, int n,
+              float link_length, int* labels, uint16_t* agg_size, int* n_groups);
+
+/* Aggregate (include/Aggregate.h:4-12) without the member list. */
+typedef struct nbody_aggregate {
+  int id;
+  int n_particles;
+  float mass_msun;
+  float cx, cy, cz;
+  float vx, vy, vz;
+  float dist_center;
+  int first_member;   /* smallest member index (the group's label) */
+} nbody_aggregate;
+
+/* Aggregate records of detectAggregates (Aggregate.cpp:54-74) from host
+ * labels: groups of >= 2 ordered by smallest member, mass = n * particle
+ * mass, mean position / velocity summed in ascending member index.
+ * Writes at most max_aggs records; returns the group count in *n_aggs. */
+int nbody_aggregates(const float* x, const float* y, const float* z, const float* vx,
+                     const float* vy, const float* vz, const int* labels, int n,
+                     float particle_mass, nbody_aggregate* out, int max_aggs, int* n_aggs);
+
+/* --------------------------------------------------------- writers --- */
+
+typedef struct nbody_writer nbody_writer;
+/* OutputWriter::OutputWriter (src/io/OutputWriter.cpp:16-34): creates
+ * dir/frames.bin (32-byte v2 header) and dir/stats.csv (15-column header). */
+int nbody_writer_open(const char* dir, const nbody_config* cfg, nbody_writer** out);
+/* OutputWriter::writeFrame (OutputWriter.cpp:96-115); host arrays. */
+int nbody_writer_frame(nbody_writer* w, const float* x, const float* y, const float* z, int n,
+                       float sim_time, const uint16_t* agg_size);
+/* OutputWriter::writeStats (OutputWriter.cpp:124-148). */
+int nbody_writer_stats(nbody_writer* w, const nbody_aggregate* aggs, int n_aggs, int frame_idx,
+                       float sim_time);
+/* OutputWriter::writePerturberStats (OutputWriter.cpp:161-186). */
+int nbody_writer_perturber(nbody_writer* w, int frame_idx, float sim_time, int n_aggregates,
+                           float px, float py, float pz, float mass_msun, float omega);
+/* OutputWriter::finalize (OutputWriter.cpp:191-197). */
+int nbody_writer_finalize(nbody_writer* w, int total_frames);
+/* OutputWriter::~OutputWriter (OutputWriter.cpp:39-42). */
+void nbody_writer_close(nbody_writer* w);
+
+/* ------------------------------------------------------------ engine --- */
+/* The whole step of src/main.cu:101-139 with the state resident on the GPU
+ * in Morton order: one fused stream kernel (dv + K2 + drag + K1 + drift +
+ * bbox), keys, sort, tree, walk (+ star, + perturber), collision. */
+
+#define NBODY_STATE_F32 0    /* positions/velocities float (reference)     */
+#define NBODY_STATE_F64 1    /* positions/velocities double                */
+
+typedef struct nbody_sim_params {
+  float dt;
+  float theta;
+  float softening;
+  float star_mass;
+  float r_coll;              /* <= 0: no collision pass                    */
+  float restitution;
+  float gas_drag_rate;       /* <= 0: no drag                              */
+  int perturber_enabled;
+  float perturber_mass_mjup;
+  float perturber_radius_au;
+  float perturber_phase0;
+  int state_precision;       /* NBODY_STATE_*                              */
+  int leaf_max;              /* <= 0: default (8)                          */
+} nbody_sim_params;
+
+/* Parameters of src/main.cu:58-73 from a Config (r_coll = factor * radius). */
+void nbody_sim_params_from_config(const nbody_config* cfg, nbody_sim_params* out);
+
+typedef struct nbody_sim nbody_sim;
+int nbody_sim_create(const nbody_sim_params* p, int n, nbody_sim** out);
+void nbody_sim_destroy(nbody_sim* s);
+/* Runs on this CUDA stream (a cudaStream_t); 0 = the legacy default stream. */
+int nbody_sim_set_stream(nbody_sim* s, void* cuda_stream);
+/* State in the caller's particle order (index i = particle id i).  on_device:
+ * pointers are device (1) or host (0).  Mass is float.  Setting the state
+ * resets the step counter and computes the forces at t = 0 (main.cu:85-96). */
+int nbody_sim_set_state(nbody_sim* s, const float* x, const float* y, const float* z,
+                        const float* vx, const float* vy, const float* vz, const float* mass,
+                        int on_device);
+int nbody_sim_set_state_f64(nbody_sim* s, const double* x, const double* y, const double* z,
+                            const double* vx, const double* vy, const double* vz,
+                            const float* mass, int on_device);
+/* Advances nsteps steps (asynchronous). */
+int nbody_sim_step(nbody_sim* s, int nsteps);
+/* Waits for the engine's stream and reports device status bits as errors. */
+int nbody_sim_sync(nbody_sim* s);
+/* State after the last step, in the caller's order (acceleration pointers may
+ * be null).  Synchronises. */
+int nbody_sim_get_state(nbody_sim* s, float* x, float* y, float* z, float* vx, float* vy,
+                        float* vz, float* ax, float* ay, float* az, int on_device);
+int nbody_sim_get_state_f64(nbody_sim* s, double* x, double* y, double* z, double* vx,
+                            double* vy, double* vz, int on_device);
+/* FoF of the current positions (FP32 snapshot), outputs in caller order. */
+int nbody_sim_fof(nbody_sim* s, float link_length, int* labels, uint16_t* agg_size,
+                  int* n_groups, int on_device);
+
+typedef struct nbody_sim_stats {
+  int n;
+  int steps_done;
+  int n_nodes;
+  unsigned long long interactions;  /* accepted interactions of the last walk */
+  int status;
+} nbody_sim_stats;
+int nbody_sim_stats_get(nbody_sim* s, nbody_sim_stats* out);
+
+/* Per-phase device time of the steps run while profiling is on: CUDA events
+ * at the phase boundaries of every step, on the engine's stream.  Phase k of
+ * a step runs from its boundary k to boundary k+1; the stream phase also
+ * holds the closing dv + K2 + drag of the call's last step. */
+#define NBODY_PHASE_STREAM 0   /* dv + K2 + drag + K1 + drift + bbox          */
+#define NBODY_PHASE_SORT 1     /* Morton keys + radix sort                    */
+#define NBODY_PHASE_PERMUTE 2  /* state gathered into key order               */
+#define NBODY_PHASE_TREE 3     /* Karras tree, FP64 moments, octree layout    */
+#define NBODY_PHASE_WALK 4     /* Barnes-Hut walk (+ star, + perturber)       */
+#define NBODY_PHASE_COLLIDE 5  /* collision neighbour search                  */
+#define NBODY_PHASES 6
+typedef struct nbody_sim_profile {
+  double ms[NBODY_PHASES];   /* summed over the profiled steps */
+  int steps;
+  unsigned long long launches;  /* kernels launched by nbody_sim_step */
+} nbody_sim_profile;
+int nbody_sim_set_profiling(nbody_sim* s, int on);
+/* Synchronises, then returns the sums since the last reset. */
+int nbody_sim_profile_get(nbody_sim* s, nbody_sim_profile* out, int reset);
+
+/* Host-buffer round trip, the per-call work of a caller that keeps its
+ * ParticleData on the host (copyToGPU, nsteps of src/main.cu:101-139,
+ * copyToCPU; include/ParticleData.h:90-123): copies x..az and mass in,
+ * advances nsteps with the given accelerations as the current forces, copies
+ * x..az back out.  The step counter (simulation time) continues across calls.
+ * NBODY_STATE_F32 only.  Synchronous. */
+int nbody_sim_step_host(nbody_sim* s, float* x, float* y, float* z, float* vx, float* vy,
+                        float* vz, float* ax, float* ay, float* az, const float* mass,
+                        int nsteps);
+
+/* ------------------------------------------------------ initial disks --- */
+
+/* Synthetic disk of n bodies: star mass at the origin, disk in XZ, +Y pole;
+ * r from Sigma ~ r^-1.5 (inverse CDF as src/disk/DiskInit.cpp:42-44), Rayleigh
+ * eccentricity/inclination (sigma_e, sigma_i), uniform node / periapsis /
+ * mean anomaly, Keplerian state (G = 1), FP64 then rounded.  Counter-based
+ * RNG (splitmix64 of seed, index, draw), so any subset is reproducible.
+ * Host arrays; x..vz double. */
+int nbody_make_disk(int n, double r_min, double r_max, double sigma_e, double sigma_i,
+                    double star_mass, uint64_t seed, double* x, double* y, double* z,
+                    double* vx, double* vy, double* vz);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NBODY_B200_H */

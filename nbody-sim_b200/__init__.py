@@ -1,0 +1,618 @@
+"""nbody-b200: Python binding of libnbody_b200.so (the C ABI in include/nbody_b200.h).
+
+The package directory is named ``nbody-sim_b200``; import it with
+``importlib.import_module("nbody-sim_b200")``.
+
+Everything computational runs in the CUDA library; this module only declares
+the C signatures, moves buffers (torch CUDA tensors for device memory, numpy
+for host memory) and turns NBODY_ERR_* codes into exceptions.  There is no CPU
+fallback: if the shared library is missing or fails to load, importing the
+package raises.
+
+Python-side names mirror the reference API they wrap:
+
+* :class:`ParticleData`, :func:`allocate_particles_gpu`, :func:`copy_to_gpu`,
+  :func:`copy_to_cpu` -- include/ParticleData.h:19-123
+* :class:`Octree` (``reset``, ``bbox``, ``build``, ``summarize``, ``sort``,
+  ``force``, ``collide``) -- include/BHTree.cuh:38-50
+* :func:`half_kick`, :func:`drift`, :func:`reset_acceleration`,
+  :func:`gas_drag`, :func:`perturber_force` -- include/Integrator.cuh:9-22,
+  include/Perturber.h:73-75
+* :func:`make_perturber`, :func:`update_perturber` -- include/Perturber.h:39-66
+* :func:`load_config`, :func:`particle_physical_radius` -- include/Config.h:38,
+  include/DiskInit.h:14
+* :func:`detect_aggregates` -- include/Aggregate.h:17-18
+* :class:`OutputWriter` -- include/OutputWriter.h:15-51
+* :class:`Sim` -- the step loop of src/main.cu:85-139 resident on the GPU
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libnbody_b200.so")
+
+NBODY_OK = 0
+NBODY_ERR_CUDA = 1
+NBODY_ERR_ARG = 2
+NBODY_ERR_OVERFLOW = 3
+NBODY_ERR_TIMEOUT = 4
+NBODY_ERR_IO = 5
+NBODY_ERR_CONFIG = 6
+NBODY_ERR_STATE = 7
+STATE_F32 = 0
+STATE_F64 = 1
+
+
+class NBodyError(RuntimeError):
+    """An NBODY_ERR_* status from the C ABI (``code`` holds the value)."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(msg)
+        self.code = code
+
+
+_F = C.POINTER(C.c_float)
+_D = C.POINTER(C.c_double)
+_I = C.POINTER(C.c_int)
+_U16 = C.POINTER(C.c_uint16)
+_VP = C.c_void_p
+
+
+class nbody_particles(C.Structure):
+    _fields_ = [(k, _F) for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "mass")] + [
+        ("id", _I), ("n", C.c_int)]
+
+
+class nbody_config(C.Structure):
+    _fields_ = [
+        ("n_particles", C.c_int), ("disk_r_min", C.c_float), ("disk_r_max", C.c_float),
+        ("disk_h_factor", C.c_float), ("particle_mass_msun", C.c_float),
+        ("star_mass_msun", C.c_float), ("softening_AU", C.c_float), ("theta", C.c_float),
+        ("collision_radius_factor", C.c_float), ("restitution", C.c_float),
+        ("gas_drag_rate", C.c_float), ("dt", C.c_float), ("total_time", C.c_float),
+        ("output_every_n_steps", C.c_int), ("output_dir", C.c_char * 1024),
+        ("perturber_enabled", C.c_int), ("perturber_mass_mjup", C.c_float),
+        ("perturber_radius_AU", C.c_float), ("perturber_phase0", C.c_float)]
+
+    def to_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["output_dir"] = self.output_dir.decode()
+        d["perturber_enabled"] = bool(self.perturber_enabled)
+        return d
+
+
+class nbody_perturber(C.Structure):
+    _fields_ = [("enabled", C.c_int), ("r", C.c_float), ("mass_msun", C.c_float),
+                ("phase0", C.c_float), ("omega", C.c_float),
+                ("x", C.c_float), ("y", C.c_float), ("z", C.c_float)]
+
+
+class nbody_tree_stats(C.Structure):
+    _fields_ = [("n_bodies", C.c_int), ("n_nodes", C.c_int), ("bbox_min", C.c_float * 3),
+                ("bbox_max", C.c_float * 3), ("root_center", C.c_float * 3),
+                ("root_half", C.c_float), ("root_mass", C.c_double),
+                ("root_com", C.c_double * 3), ("interactions", C.c_ulonglong),
+                ("status", C.c_int)]
+
+
+class nbody_aggregate(C.Structure):
+    _fields_ = [("id", C.c_int), ("n_particles", C.c_int), ("mass_msun", C.c_float),
+                ("cx", C.c_float), ("cy", C.c_float), ("cz", C.c_float),
+                ("vx", C.c_float), ("vy", C.c_float), ("vz", C.c_float),
+                ("dist_center", C.c_float), ("first_member", C.c_int)]
+
+
+class nbody_sim_params(C.Structure):
+    _fields_ = [("dt", C.c_float), ("theta", C.c_float), ("softening", C.c_float),
+                ("star_mass", C.c_float), ("r_coll", C.c_float), ("restitution", C.c_float),
+                ("gas_drag_rate", C.c_float), ("perturber_enabled", C.c_int),
+                ("perturber_mass_mjup", C.c_float), ("perturber_radius_au", C.c_float),
+                ("perturber_phase0", C.c_float), ("state_precision", C.c_int),
+                ("leaf_max", C.c_int)]
+
+
+NBODY_PHASES = 6
+PHASE_NAMES = ("stream", "sort", "permute", "tree", "walk", "collide")
+
+
+class nbody_sim_profile(C.Structure):
+    _fields_ = [("ms", C.c_double * NBODY_PHASES), ("steps", C.c_int),
+                ("launches", C.c_ulonglong)]
+
+
+class nbody_sim_stats(C.Structure):
+    _fields_ = [("n", C.c_int), ("steps_done", C.c_int), ("n_nodes", C.c_int),
+                ("interactions", C.c_ulonglong), ("status", C.c_int)]
+
+
+# (name, restype, argtypes): every symbol include/nbody_b200.h declares
+SIGNATURES = [
+    ("nbody_last_error", C.c_char_p, []),
+    ("nbody_abi_version", C.c_int, []),
+    ("nbody_config_defaults", None, [C.POINTER(nbody_config)]),
+    ("nbody_config_load", C.c_int, [C.c_char_p, C.POINTER(nbody_config)]),
+    ("nbody_particle_radius", C.c_float, [C.c_float]),
+    ("nbody_perturber_make", None, [C.POINTER(nbody_config), C.POINTER(nbody_perturber)]),
+    ("nbody_perturber_update", None, [C.POINTER(nbody_perturber), C.c_float]),
+    ("nbody_tree_create", C.c_int, [C.c_int, C.POINTER(_VP)]),
+    ("nbody_tree_destroy", None, [_VP]),
+    ("nbody_tree_reset", C.c_int, [_VP]),
+    ("nbody_tree_bbox", C.c_int, [_VP, C.POINTER(nbody_particles)]),
+    ("nbody_tree_build", C.c_int, [_VP, C.POINTER(nbody_particles)]),
+    ("nbody_tree_summarize", C.c_int, [_VP]),
+    ("nbody_tree_sort", C.c_int, [_VP]),
+    ("nbody_tree_sort_idx", _I, [_VP]),
+    ("nbody_tree_sort_idx_copy", C.c_int, [_VP, _I, C.c_int]),
+    ("nbody_tree_force", C.c_int, [_VP, C.POINTER(nbody_particles), C.c_float, C.c_float,
+                                   C.c_float]),
+    ("nbody_tree_collide", C.c_int, [_VP, C.POINTER(nbody_particles), C.c_float, C.c_float]),
+    ("nbody_tree_set_leaf_max", C.c_int, [_VP, C.c_int]),
+    ("nbody_tree_stats_get", C.c_int, [_VP, C.POINTER(nbody_tree_stats)]),
+    ("nbody_half_kick", C.c_int, [C.POINTER(nbody_particles), C.c_float]),
+    ("nbody_drift", C.c_int, [C.POINTER(nbody_particles), C.c_float]),
+    ("nbody_reset_acc", C.c_int, [C.POINTER(nbody_particles)]),
+    ("nbody_gas_drag", C.c_int, [C.POINTER(nbody_particles), C.c_float, C.c_float, C.c_float]),
+    ("nbody_perturber_force", C.c_int, [C.POINTER(nbody_particles), C.c_float, C.c_float,
+                                        C.c_float, C.c_float, C.c_float]),
+    ("nbody_fof", C.c_int, [_VP, _VP, _VP, _VP, C.c_int, C.c_float, _VP, _VP, _I]),
+    ("nbody_aggregates", C.c_int, [_F, _F, _F, _F, _F, _F, _I, C.c_int, C.c_float,
+                                   C.POINTER(nbody_aggregate), C.c_int, _I]),
+    ("nbody_writer_open", C.c_int, [C.c_char_p, C.POINTER(nbody_config), C.POINTER(_VP)]),
+    ("nbody_writer_frame", C.c_int, [_VP, _F, _F, _F, C.c_int, C.c_float, _U16]),
+    ("nbody_writer_stats", C.c_int, [_VP, C.POINTER(nbody_aggregate), C.c_int, C.c_int,
+                                     C.c_float]),
+    ("nbody_writer_perturber", C.c_int, [_VP, C.c_int, C.c_float, C.c_int, C.c_float, C.c_float,
+                                         C.c_float, C.c_float, C.c_float]),
+    ("nbody_writer_finalize", C.c_int, [_VP, C.c_int]),
+    ("nbody_writer_close", None, [_VP]),
+    ("nbody_sim_params_from_config", None, [C.POINTER(nbody_config),
+                                            C.POINTER(nbody_sim_params)]),
+    ("nbody_sim_create", C.c_int, [C.POINTER(nbody_sim_params), C.c_int, C.POINTER(_VP)]),
+    ("nbody_sim_destroy", None, [_VP]),
+    ("nbody_sim_set_stream", C.c_int, [_VP, _VP]),
+    ("nbody_sim_set_state", C.c_int, [_VP] + [_VP] * 7 + [C.c_int]),
+    ("nbody_sim_set_state_f64", C.c_int, [_VP] + [_VP] * 7 + [C.c_int]),
+    ("nbody_sim_step", C.c_int, [_VP, C.c_int]),
+    ("nbody_sim_sync", C.c_int, [_VP]),
+    ("nbody_sim_get_state", C.c_int, [_VP] + [_VP] * 9 + [C.c_int]),
+    ("nbody_sim_get_state_f64", C.c_int, [_VP] + [_VP] * 6 + [C.c_int]),
+    ("nbody_sim_fof", C.c_int, [_VP, C.c_float, _VP, _VP, _I, C.c_int]),
+    ("nbody_sim_stats_get", C.c_int, [_VP, C.POINTER(nbody_sim_stats)]),
+    ("nbody_sim_set_profiling", C.c_int, [_VP, C.c_int]),
+    ("nbody_sim_profile_get", C.c_int, [_VP, C.POINTER(nbody_sim_profile), C.c_int]),
+    ("nbody_sim_step_host", C.c_int, [_VP] + [_VP] * 10 + [C.c_int]),
+    ("nbody_make_disk", C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                  C.c_double, C.c_uint64, _D, _D, _D, _D, _D, _D]),
+]
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python nbody-sim_b200/build.py` "
+            "(there is no CPU fallback)")
+    lib = C.CDLL(LIB_PATH)
+    for name, res, args in SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def _check(rc: int):
+    if rc != NBODY_OK:
+        raise NBodyError(rc, lib.nbody_last_error().decode())
+
+
+# ------------------------------------------------------------------ config
+def default_config() -> nbody_config:
+    c = nbody_config()
+    lib.nbody_config_defaults(C.byref(c))
+    return c
+
+
+def load_config(path: str) -> nbody_config:
+    """loadConfig (src/config/Config.cpp:6-55); raises NBodyError."""
+    c = nbody_config()
+    _check(lib.nbody_config_load(os.fsencode(path), C.byref(c)))
+    return c
+
+
+def particle_physical_radius(particle_mass_msun: float) -> float:
+    return float(lib.nbody_particle_radius(particle_mass_msun))
+
+
+def make_perturber(cfg: nbody_config) -> nbody_perturber:
+    p = nbody_perturber()
+    lib.nbody_perturber_make(C.byref(cfg), C.byref(p))
+    return p
+
+
+def update_perturber(p: nbody_perturber, sim_time: float) -> None:
+    lib.nbody_perturber_update(C.byref(p), sim_time)
+
+
+# --------------------------------------------------------------- particles
+FIELDS = ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "mass")
+
+
+@dataclass
+class ParticleData:
+    """SoA particles (include/ParticleData.h:19-32): torch CUDA float tensors
+    (device) or numpy float32 arrays (host), plus int ids."""
+
+    n: int
+    arrays: dict = field(default_factory=dict)
+
+    def __getattr__(self, k):
+        a = self.__dict__.get("arrays", {})
+        if k in a:
+            return a[k]
+        raise AttributeError(k)
+
+    def struct(self) -> nbody_particles:
+        s = nbody_particles()
+        s.n = self.n
+        for k in FIELDS:
+            a = self.arrays.get(k)
+            if a is not None:
+                setattr(s, k, C.cast(_data_ptr(a), _F))
+        if self.arrays.get("id") is not None:
+            s.id = C.cast(_data_ptr(self.arrays["id"]), _I)
+        return s
+
+
+def _data_ptr(a):
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    return a.ctypes.data
+
+
+def allocate_particles_cpu(n: int) -> ParticleData:
+    arr = {k: np.zeros(n, np.float32) for k in FIELDS}
+    arr["id"] = np.zeros(n, np.int32)
+    return ParticleData(n, arr)
+
+
+def allocate_particles_gpu(n: int, device="cuda") -> ParticleData:
+    import torch
+    arr = {k: torch.zeros(n, dtype=torch.float32, device=device) for k in FIELDS}
+    arr["id"] = torch.zeros(n, dtype=torch.int32, device=device)
+    return ParticleData(n, arr)
+
+
+def copy_to_gpu(cpu: ParticleData, gpu: ParticleData) -> None:
+    """copyToGPU (include/ParticleData.h:90-105), same size check."""
+    import torch
+    if cpu.n != gpu.n:
+        raise RuntimeError(f"copyToGPU: CPU n={cpu.n} != GPU n={gpu.n}")
+    for k in FIELDS + ("id",):
+        gpu.arrays[k].copy_(torch.from_numpy(np.ascontiguousarray(cpu.arrays[k])))
+
+
+def copy_to_cpu(gpu: ParticleData, cpu: ParticleData) -> None:
+    """copyToCPU (include/ParticleData.h:108-123)."""
+    if cpu.n != gpu.n:
+        raise RuntimeError(f"copyToCPU: GPU n={gpu.n} != CPU n={cpu.n}")
+    for k in FIELDS + ("id",):
+        cpu.arrays[k][:] = gpu.arrays[k].cpu().numpy()
+
+
+# ------------------------------------------------------------ phase API
+class Octree:
+    """OctreeData + its launchers (include/BHTree.cuh:38-50); each call
+    synchronises before returning, as the reference launchers do."""
+
+    def __init__(self, n_bodies: int, leaf_max: int | None = None):
+        h = _VP()
+        _check(lib.nbody_tree_create(n_bodies, C.byref(h)))
+        self.h = h
+        self.n_bodies = n_bodies
+        if leaf_max is not None:
+            _check(lib.nbody_tree_set_leaf_max(self.h, leaf_max))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.nbody_tree_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def reset(self):
+        _check(lib.nbody_tree_reset(self.h))
+
+    def bbox(self, p: ParticleData):
+        s = p.struct()
+        _check(lib.nbody_tree_bbox(self.h, C.byref(s)))
+
+    def build(self, p: ParticleData):
+        s = p.struct()
+        _check(lib.nbody_tree_build(self.h, C.byref(s)))
+
+    def summarize(self):
+        _check(lib.nbody_tree_summarize(self.h))
+
+    def sort(self):
+        _check(lib.nbody_tree_sort(self.h))
+
+    def sort_idx(self) -> np.ndarray:
+        """tree.sort_idx (include/BHTree.cuh:20) copied to the host."""
+        out = np.zeros(self.n_bodies, np.int32)
+        _check(lib.nbody_tree_sort_idx_copy(self.h, out.ctypes.data_as(_I), 0))
+        return out
+
+    def force(self, p: ParticleData, theta: float, softening: float, star_mass: float):
+        s = p.struct()
+        _check(lib.nbody_tree_force(self.h, C.byref(s), theta, softening, star_mass))
+
+    def collide(self, p: ParticleData, r_coll: float, restitution: float):
+        s = p.struct()
+        _check(lib.nbody_tree_collide(self.h, C.byref(s), r_coll, restitution))
+
+    def stats(self) -> nbody_tree_stats:
+        st = nbody_tree_stats()
+        _check(lib.nbody_tree_stats_get(self.h, C.byref(st)))
+        return st
+
+    def fof(self, x, y, z, link_length: float):
+        """Device FoF over torch CUDA float tensors -> (labels, agg_size, n_groups)."""
+        import torch
+        n = x.numel()
+        labels = torch.empty(n, dtype=torch.int32, device=x.device)
+        agg = torch.empty(n, dtype=torch.int16, device=x.device)
+        ng = C.c_int()
+        _check(lib.nbody_fof(self.h, x.data_ptr(), y.data_ptr(), z.data_ptr(), n, link_length,
+                             labels.data_ptr(), agg.data_ptr(), C.byref(ng)))
+        return labels, agg, ng.value  # agg: int16 tensor holding uint16 sizes
+
+
+def half_kick(p: ParticleData, dt_half: float):
+    s = p.struct(); _check(lib.nbody_half_kick(C.byref(s), dt_half))
+
+
+def drift(p: ParticleData, dt: float):
+    s = p.struct(); _check(lib.nbody_drift(C.byref(s), dt))
+
+
+def reset_acceleration(p: ParticleData):
+    s = p.struct(); _check(lib.nbody_reset_acc(C.byref(s)))
+
+
+def gas_drag(p: ParticleData, drag_rate: float, dt: float, star_mass: float):
+    s = p.struct(); _check(lib.nbody_gas_drag(C.byref(s), drag_rate, dt, star_mass))
+
+
+def perturber_force(p: ParticleData, px, py, pz, pmass, softening):
+    s = p.struct(); _check(lib.nbody_perturber_force(C.byref(s), px, py, pz, pmass, softening))
+
+
+# --------------------------------------------------------------- FoF
+@dataclass
+class Aggregate:
+    """include/Aggregate.h:4-12."""
+    id: int
+    n_particles: int
+    mass_msun: float
+    cx: float
+    cy: float
+    cz: float
+    vx: float
+    vy: float
+    vz: float
+    dist_center: float
+    particle_ids: list
+
+
+def aggregates_from_labels(x, y, z, vx, vy, vz, labels, particle_mass: float):
+    """Aggregate records (Aggregate.cpp:54-74) from host labels, ordered by
+    smallest member index; returns the raw nbody_aggregate array."""
+    arrs = [np.ascontiguousarray(a, np.float32) for a in (x, y, z, vx, vy, vz)]
+    lab = np.ascontiguousarray(labels, np.int32)
+    n = len(lab)
+    cnt = C.c_int()
+    _check(lib.nbody_aggregates(*[a.ctypes.data_as(_F) for a in arrs], lab.ctypes.data_as(_I), n,
+                                particle_mass, None, 0, C.byref(cnt)))
+    out = (nbody_aggregate * max(cnt.value, 1))()
+    _check(lib.nbody_aggregates(*[a.ctypes.data_as(_F) for a in arrs], lab.ctypes.data_as(_I), n,
+                                particle_mass, out, cnt.value, C.byref(cnt)))
+    return out, cnt.value
+
+
+def detect_aggregates(p: ParticleData, link_length: float, cfg: nbody_config, tree=None):
+    """detectAggregates (include/Aggregate.h:17-18) on host particles: the
+    links and union-find run on the GPU, the records on the host."""
+    import torch
+    n = p.n
+    own = tree is None
+    tree = tree or Octree(max(n, 1))
+    try:
+        xs = [torch.from_numpy(np.ascontiguousarray(p.arrays[k], np.float32)).cuda()
+              for k in ("x", "y", "z")]
+        labels, _, _ = tree.fof(*xs, link_length)
+        lab = labels.cpu().numpy()
+    finally:
+        if own:
+            tree.close()
+    recs, g = aggregates_from_labels(p.x, p.y, p.z, p.vx, p.vy, p.vz, lab, cfg.particle_mass_msun)
+    members = {}
+    for i, l in enumerate(lab):
+        members.setdefault(int(l), []).append(i)
+    out = []
+    for k in range(g):
+        r = recs[k]
+        out.append(Aggregate(r.id, r.n_particles, r.mass_msun, r.cx, r.cy, r.cz, r.vx, r.vy,
+                             r.vz, r.dist_center, members[r.first_member]))
+    return out
+
+
+# ------------------------------------------------------------- writer
+class OutputWriter:
+    """frames.bin + stats.csv writer (include/OutputWriter.h:15-51)."""
+
+    def __init__(self, output_dir: str, cfg: nbody_config):
+        h = _VP()
+        _check(lib.nbody_writer_open(os.fsencode(output_dir), C.byref(cfg), C.byref(h)))
+        self.h = h
+
+    def write_frame(self, p: ParticleData, sim_time: float, agg_sizes):
+        agg = np.ascontiguousarray(agg_sizes, np.uint16)
+        if len(agg) != p.n:
+            raise RuntimeError("OutputWriter::writeFrame: agg_sizes_per_particle size mismatch")
+        xs = [np.ascontiguousarray(p.arrays[k], np.float32) for k in ("x", "y", "z")]
+        _check(lib.nbody_writer_frame(self.h, *[a.ctypes.data_as(_F) for a in xs], p.n, sim_time,
+                                      agg.ctypes.data_as(_U16)))
+
+    def write_stats(self, aggs, frame_idx: int, sim_time: float):
+        arr = (nbody_aggregate * max(len(aggs), 1))()
+        for k, a in enumerate(aggs):
+            r = arr[k]
+            r.id, r.n_particles, r.mass_msun = a.id, a.n_particles, a.mass_msun
+            r.cx, r.cy, r.cz, r.vx, r.vy, r.vz = a.cx, a.cy, a.cz, a.vx, a.vy, a.vz
+            r.dist_center = a.dist_center
+        _check(lib.nbody_writer_stats(self.h, arr, len(aggs), frame_idx, sim_time))
+
+    def write_perturber_stats(self, frame_idx, sim_time, n_aggregates, px, py, pz, mass, omega):
+        _check(lib.nbody_writer_perturber(self.h, frame_idx, sim_time, n_aggregates, px, py, pz,
+                                          mass, omega))
+
+    def finalize(self, total_frames: int):
+        _check(lib.nbody_writer_finalize(self.h, total_frames))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.nbody_writer_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------- engine
+def sim_params(cfg: nbody_config | None = None, **kw) -> nbody_sim_params:
+    p = nbody_sim_params()
+    if cfg is not None:
+        lib.nbody_sim_params_from_config(C.byref(cfg), C.byref(p))
+    else:
+        p.dt, p.theta, p.softening, p.star_mass, p.leaf_max = 0.01, 0.5, 0.01, 1.0, 8
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+class Sim:
+    """The GPU-resident step engine (nbody_sim_* in include/nbody_b200.h)."""
+
+    def __init__(self, params: nbody_sim_params, n: int):
+        h = _VP()
+        _check(lib.nbody_sim_create(C.byref(params), n, C.byref(h)))
+        self.h, self.n, self.params = h, n, params
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.nbody_sim_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr: int):
+        _check(lib.nbody_sim_set_stream(self.h, stream_ptr))
+
+    def set_state(self, x, y, z, vx, vy, vz, mass):
+        """Host numpy (float32 or float64) or CUDA torch tensors, caller order."""
+        arrs = [x, y, z, vx, vy, vz]
+        on_dev = hasattr(x, "data_ptr")
+        if on_dev:
+            dbl = str(x.dtype) == "torch.float64"
+            ptrs = [a.data_ptr() for a in arrs]
+            mptr = mass.data_ptr()
+            keep = None
+        else:
+            dbl = np.asarray(x).dtype == np.float64
+            keep = [np.ascontiguousarray(a, np.float64 if dbl else np.float32) for a in arrs]
+            km = np.ascontiguousarray(mass, np.float32)
+            ptrs = [a.ctypes.data for a in keep]
+            mptr = km.ctypes.data
+        fn = lib.nbody_sim_set_state_f64 if dbl else lib.nbody_sim_set_state
+        _check(fn(self.h, *ptrs, mptr, int(on_dev)))
+        del keep
+
+    def step(self, nsteps: int = 1):
+        _check(lib.nbody_sim_step(self.h, nsteps))
+
+    def sync(self):
+        _check(lib.nbody_sim_sync(self.h))
+
+    def get_state(self, double: bool = False, accel: bool = True):
+        """Host numpy state in caller order: dict x..vz (+ ax..az)."""
+        n = self.n
+        dt = np.float64 if double else np.float32
+        out = {k: np.zeros(n, dt) for k in ("x", "y", "z", "vx", "vy", "vz")}
+        if double:
+            _check(lib.nbody_sim_get_state_f64(self.h, *[out[k].ctypes.data for k in out], 0))
+        else:
+            acc = {k: np.zeros(n, np.float32) for k in ("ax", "ay", "az")} if accel else None
+            aptr = [acc[k].ctypes.data for k in ("ax", "ay", "az")] if accel else [None] * 3
+            _check(lib.nbody_sim_get_state(self.h, *[out[k].ctypes.data for k in out], *aptr, 0))
+            if accel:
+                out.update(acc)
+        return out
+
+    def fof(self, link_length: float):
+        labels = np.zeros(self.n, np.int32)
+        agg = np.zeros(self.n, np.uint16)
+        ng = C.c_int()
+        _check(lib.nbody_sim_fof(self.h, link_length, labels.ctypes.data, agg.ctypes.data,
+                                 C.byref(ng), 0))
+        return labels, agg, ng.value
+
+    def stats(self) -> nbody_sim_stats:
+        st = nbody_sim_stats()
+        _check(lib.nbody_sim_stats_get(self.h, C.byref(st)))
+        return st
+
+    def set_profiling(self, on: bool = True):
+        _check(lib.nbody_sim_set_profiling(self.h, int(on)))
+
+    def profile(self, reset: bool = True) -> dict:
+        pr = nbody_sim_profile()
+        _check(lib.nbody_sim_profile_get(self.h, C.byref(pr), int(reset)))
+        d = {name: pr.ms[k] for k, name in enumerate(PHASE_NAMES)}
+        d["steps"] = pr.steps
+        d["launches"] = pr.launches
+        return d
+
+    def step_host(self, st: dict, mass, nsteps: int = 1):
+        """Host round trip (copyToGPU, nsteps, copyToCPU) on float32 arrays in place."""
+        keys = ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")
+        _check(lib.nbody_sim_step_host(self.h, *[st[k].ctypes.data for k in keys],
+                                       mass.ctypes.data, nsteps))
+
+
+# --------------------------------------------------------- initial disks
+def make_disk(n: int, r_min: float, r_max: float, sigma_e=0.01, sigma_i=0.005, star_mass=1.0,
+              seed: int = 0):
+    """Synthetic Keplerian disk (nbody_make_disk): dict of float64 numpy arrays."""
+    out = {k: np.zeros(n, np.float64) for k in ("x", "y", "z", "vx", "vy", "vz")}
+    _check(lib.nbody_make_disk(n, r_min, r_max, sigma_e, sigma_i, star_mass, seed,
+                               *[out[k].ctypes.data_as(_D) for k in ("x", "y", "z", "vx", "vy",
+                                                                       "vz")]))
+    return out

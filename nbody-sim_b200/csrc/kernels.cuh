@@ -1,0 +1,154 @@
+// kernels.cuh -- internal launch interface of the nbody-b200 CUDA library.
+//
+// Data layout in HBM (all SoA, Morton order unless noted):
+//   body4[s]      float4 (x, y, z, m) of the s-th body in key order (16 B)
+//   keys/perm     uint32 Morton key and source index per body
+//   binary tree   Karras radix tree over the sorted keys: left/right/parent,
+//                 [lo,hi] body range, prefix length (bits), FP64 mass moments
+//                 and a float AABB per internal node
+//   octree        compressed octree over the same keys; the children of a
+//                 node are contiguous: com4 (x,y,z,m float, from FP64 sums),
+//                 info int4 (first_child, body_lo, count<<4|nchild,
+//                 bits of half-size), box_lo/box_hi float4 (tight AABB)
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace nb {
+
+// Root cube and key quantisation, computed on the device from the bbox.
+struct TreeGeom {
+  float bmin[3], bmax[3];  // padded bbox: launchBBoxKernel semantics (BHTree.cu:440-446)
+  float rc[3];             // root centre (BHTree.cu:481-483)
+  float rhs;               // root half size (BHTree.cu:484-485)
+  double lo[3];            // lower corner of the root cube
+  double scale;            // 1024 / (2 rhs): cells per unit length at level 10
+};
+
+struct OctNodes {
+  float4* com = nullptr;
+  int4* info = nullptr;
+  float4* box_lo = nullptr;
+  float4* box_hi = nullptr;
+};
+
+// Scratch + outputs of one tree build for up to `cap` bodies.
+struct TreeWork {
+  int cap = 0;
+  // sort
+  uint32_t *keys = nullptr, *perm = nullptr, *keys_alt = nullptr, *perm_alt = nullptr;
+  uint32_t* counts = nullptr;
+  // bodies in key order
+  float4* body4 = nullptr;
+  // binary radix tree (internal nodes 0..n-2, leaves encoded n-1+j)
+  int *bin_left = nullptr, *bin_right = nullptr, *bin_parent = nullptr;
+  int *bin_lo = nullptr, *bin_hi = nullptr;
+  uint8_t* bin_prefix = nullptr;
+  int* bin_visit = nullptr;
+  double4* bin_sum = nullptr;  // (m, m x, m y, m z)
+  float4 *bin_box_lo = nullptr, *bin_box_hi = nullptr;
+  // octree layout
+  uint8_t* oct_nch = nullptr;
+  uint32_t* oct_off = nullptr;
+  int* oct_final = nullptr;
+  uint32_t* scan_tmp = nullptr;
+  OctNodes oct;
+  // device words
+  unsigned long long* bbox_enc = nullptr;  // 6: min xyz, max xyz (ordered bits)
+  TreeGeom* geom = nullptr;
+  int* n_nodes = nullptr;
+  int* status = nullptr;
+};
+
+void tree_alloc(TreeWork& w, int cap);
+void tree_free(TreeWork& w);
+
+// bbox of n positions of type T (float or double) into w.bbox_enc (reset first).
+template <typename T>
+void launch_bbox(TreeWork& w, const T* x, const T* y, const T* z, int n, cudaStream_t s);
+void launch_bbox_reset(TreeWork& w, cudaStream_t s);
+// Morton keys of n positions using w.bbox_enc; writes w.geom, keys, perm = 0..n-1.
+template <typename T>
+void launch_keys(TreeWork& w, const T* x, const T* y, const T* z, int n, cudaStream_t s);
+// body4[s] = (x,y,z,m)[perm[s]] for float inputs in caller order.
+void launch_gather_body4(TreeWork& w, const float* x, const float* y, const float* z,
+                         const float* m, int n, cudaStream_t s);
+// Karras tree + FP64 bottom-up + compressed octree.  xd/yd/zd (optional,
+// key order) give FP64 positions for the moments; otherwise body4 is used.
+void launch_build_topology(TreeWork& w, int n, cudaStream_t s);
+void launch_build_moments(TreeWork& w, int n, const double* xd, const double* yd,
+                          const double* zd, cudaStream_t s);
+
+size_t radix_sort_count_words(int n);
+void radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt,
+                      uint32_t* counts, int n, int bits, cudaStream_t s);
+size_t scan_tmp_words(int n);
+void scan_exclusive_u32(uint32_t* data, int n, uint32_t* tmp, cudaStream_t s);
+
+// ------------------------------------------------------------------ walk
+struct WalkArgs {
+  const float4* com;
+  const int4* info;
+  const float4* body;
+  int n;
+  float theta2;           // theta^2
+  float eps;              // softening
+  float star_mass;
+  int star_in_walk;       // 1: add the softened star pull in FP32 (reference form)
+  int leaf_max;           // nodes with <= leaf_max bodies are opened into bodies
+  const float4* pert;     // (px, py, pz, m) of the perturber, or nullptr
+  float* ax;
+  float* ay;
+  float* az;
+  const uint32_t* scatter;  // output index map (caller order), or nullptr
+  int* spill;
+  int spill_cap;
+  unsigned long long* inter;  // accepted interactions (sources x targets)
+  int* work;
+  int* status;
+  int group;              // targets per warp group: 32 or 64
+};
+int walk_spill_slots(int device);  // warps resident at once (spill area slots)
+void launch_walk(const WalkArgs& a, cudaStream_t s);
+
+// ------------------------------------------------------------ collisions
+struct NeighborArgs {
+  const int4* info;
+  const float4* box_lo;
+  const float4* box_hi;
+  const float4* body;
+  int n;
+  int leaf_max;
+  int* spill;
+  int spill_cap;
+  int* work;
+  int* status;
+};
+// Two-pass impulse (BHTree.cu:620-686): dv[s] for body s in key order.
+// v* are velocities in key order, or in caller order when vmap != nullptr
+// (v[vmap[j]] is body j's velocity).
+void launch_collide(const NeighborArgs& a, const float* vx, const float* vy, const float* vz,
+                    const uint32_t* vmap, float r_coll, float restitution, float* dvx,
+                    float* dvy, float* dvz, cudaStream_t s);
+// FoF links (Aggregate.cpp:36-42 test) -> union-find over original ids.
+void launch_fof_link(const NeighborArgs& a, const uint32_t* ids, float link_length,
+                     int* parent, cudaStream_t s);
+void launch_fof_finish(int* parent, int n, int* labels, int* sizes, uint16_t* agg_size,
+                       int* n_groups, int* status, cudaStream_t s);
+
+// -------------------------------------------------------- streaming (compat)
+void launch_half_kick(float* vx, float* vy, float* vz, const float* ax, const float* ay,
+                      const float* az, float dt_half, int n, cudaStream_t s);
+void launch_drift(float* x, float* y, float* z, const float* vx, const float* vy,
+                  const float* vz, float dt, int n, cudaStream_t s);
+void launch_reset_acc(float* ax, float* ay, float* az, int n, cudaStream_t s);
+void launch_gas_drag(const float* x, const float* y, const float* z, float* vx, float* vy,
+                     float* vz, float decay, float star_mass, int n, cudaStream_t s);
+void launch_perturber_force(float* ax, float* ay, float* az, const float* x, const float* y,
+                            const float* z, float px, float py, float pz, float pmass,
+                            float eps, int n, cudaStream_t s);
+void launch_apply_dv(float* vx, float* vy, float* vz, const float* dvx, const float* dvy,
+                     const float* dvz, const uint32_t* map, int n, cudaStream_t s);
+void launch_copy_perm(int* dst, const uint32_t* perm, int n, cudaStream_t s);
+
+}  // namespace nb

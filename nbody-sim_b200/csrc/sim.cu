@@ -1,0 +1,795 @@
+// sim.cu -- the step engine: src/main.cu:85-139 with the state resident on
+// the GPU, kept in the Morton order of the last tree build.
+//
+// One step (reference launch order K1, D, tree, force, perturber, collision,
+// K2, drag) becomes:
+//   k_stream  : [dv + K2 + drag of the previous step] + K1 + drift + bbox
+//   k_keys    : 30-bit Morton keys of the new positions (bbox from k_stream)
+//   sort      : 4-pass radix sort -> permutation
+//   k_permute : state gathered into the new key order (+ float4 bodies)
+//   Karras tree, bottom-up FP64 moments, octree layout
+//   k_walk    : star + Barnes-Hut + perturber accelerations
+//   k_neighbors (collisions only): dv
+// and the trailing dv + K2 + drag is fused into the next step's k_stream.
+// Both kicks of a step boundary use the same acceleration, so fusing K2(n)
+// with K1(n+1) changes no arithmetic.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "capi_util.h"
+#include "common.cuh"
+#include "kernels.cuh"
+#include "physics.cuh"
+
+namespace nb {
+namespace {
+
+constexpr int kThreads = 256;
+
+int stream_grid(int n) { return std::max(1, std::min(div_up(n, kThreads), 148 * 8)); }
+
+template <typename R>
+struct StateArrays {
+  R* v[6];  // x y z vx vy vz
+  float* m;
+  int* id;
+};
+
+template <typename Tin, typename Tout>
+__global__ void k_convert(const Tin* __restrict__ in, Tout* __restrict__ out, int n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = (Tout)in[i];
+}
+
+__global__ void k_iota(int* __restrict__ id, int n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    id[i] = (int)i;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kThreads)
+k_permute(const uint32_t* __restrict__ perm, StateArrays<R> in, StateArrays<R> out, int n,
+          float4* __restrict__ body4) {
+  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
+       s += (long long)gridDim.x * blockDim.x) {
+    const uint32_t o = perm[s];
+    R q[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      q[k] = in.v[k][o];
+      out.v[k][s] = q[k];
+    }
+    const float m = in.m[o];
+    out.m[s] = m;
+    out.id[s] = in.id[o];
+    body4[s] = make_float4((float)q[0], (float)q[1], (float)q[2], m);
+  }
+}
+
+struct StreamArgs {
+  const float* ax;
+  const float* ay;
+  const float* az;
+  const float* dvx;  // nullptr: no collision pass
+  const float* dvy;
+  const float* dvz;
+  double dt;
+  double dth;
+  double decay;      // drag retention factor; <= 0 disables drag
+  float decay_f;     // expf(-rate dt), the reference's float factor
+  float dt_f;
+  float dth_f;
+  double eps;
+  double star_mass;
+  unsigned long long* bbox;
+};
+
+// Fused step boundary.  kEnd: dv + K2 + drag (main.cu:131-139);
+// kBegin: K1 + drift (main.cu:104-107) + bbox of the new positions.
+template <typename R, bool kEnd, bool kBegin>
+__global__ void __launch_bounds__(kThreads) k_stream(StateArrays<R> st, int n, StreamArgs a) {
+  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
+       s += (long long)gridDim.x * blockDim.x) {
+    R x = st.v[0][s], y = st.v[1][s], z = st.v[2][s];
+    R vx = st.v[3][s], vy = st.v[4][s], vz = st.v[5][s];
+    R ax = (R)a.ax[s], ay = (R)a.ay[s], az = (R)a.az[s];
+    if (sizeof(R) == 8) {  // FP64 state: the stiff star term in FP64
+      double sx, sy, sz;
+      star_accel<double>((double)x, (double)y, (double)z, a.eps, a.star_mass, sx, sy, sz);
+      ax += (R)sx; ay += (R)sy; az += (R)sz;
+    }
+    if (kEnd) {
+      if (a.dvx) {  // bhtree_applyCollisionDeltaKernel (BHTree.cu:683-685)
+        vx += (R)a.dvx[s]; vy += (R)a.dvy[s]; vz += (R)a.dvz[s];
+      }
+      if (sizeof(R) == 4) {  // integrator_halfKickKernel: v += a dt/2 (one FMA)
+        vx = fmaf((float)ax, a.dth_f, (float)vx);
+        vy = fmaf((float)ay, a.dth_f, (float)vy);
+        vz = fmaf((float)az, a.dth_f, (float)vz);
+        if (a.decay > 0.0) {
+          float fvx = (float)vx, fvy = (float)vy, fvz = (float)vz;
+          gas_drag<float>((float)x, (float)z, fvx, fvy, fvz, a.decay_f, (float)a.star_mass);
+          vx = fvx; vy = fvy; vz = fvz;
+        }
+      } else {
+        vx = fma(ax, (R)a.dth, vx); vy = fma(ay, (R)a.dth, vy); vz = fma(az, (R)a.dth, vz);
+        if (a.decay > 0.0) gas_drag<R>(x, z, vx, vy, vz, (R)a.decay, (R)a.star_mass);
+      }
+    }
+    if (kBegin) {
+      if (sizeof(R) == 4) {
+        vx = fmaf((float)ax, a.dth_f, (float)vx);
+        vy = fmaf((float)ay, a.dth_f, (float)vy);
+        vz = fmaf((float)az, a.dth_f, (float)vz);
+        x = fmaf((float)vx, a.dt_f, (float)x);
+        y = fmaf((float)vy, a.dt_f, (float)y);
+        z = fmaf((float)vz, a.dt_f, (float)z);
+      } else {
+        vx = fma(ax, (R)a.dth, vx); vy = fma(ay, (R)a.dth, vy); vz = fma(az, (R)a.dth, vz);
+        x = fma(vx, (R)a.dt, x); y = fma(vy, (R)a.dt, y); z = fma(vz, (R)a.dt, z);
+      }
+      lo[0] = fmin(lo[0], (double)x); hi[0] = fmax(hi[0], (double)x);
+      lo[1] = fmin(lo[1], (double)y); hi[1] = fmax(hi[1], (double)y);
+      lo[2] = fmin(lo[2], (double)z); hi[2] = fmax(hi[2], (double)z);
+      st.v[0][s] = x; st.v[1][s] = y; st.v[2][s] = z;
+    }
+    st.v[3][s] = vx; st.v[4][s] = vy; st.v[5][s] = vz;
+  }
+  if (kBegin) {
+    __shared__ double sb[6][kThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      double p = warp_min(lo[k]), q = warp_max(hi[k]);
+      if (lane == 0) { sb[k][warp] = p; sb[3 + k][warp] = q; }
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+      const int k = threadIdx.x;
+      double v = sb[k][0];
+      for (int w = 1; w < kThreads / 32; ++w) v = (k < 3) ? fmin(v, sb[k][w]) : fmax(v, sb[k][w]);
+      if (v == v && fabs(v) != INFINITY) {
+        if (k < 3) atomicMin(a.bbox + k, ordered_bits(v));
+        else atomicMax(a.bbox + k, ordered_bits(v));
+      }
+    }
+  }
+}
+
+// Writes the state back in caller order (out[id[s]] = state[s]); with
+// accelerations, adds the FP64 star term in FP64 mode.
+template <typename R, typename T>
+__global__ void __launch_bounds__(kThreads)
+k_unsort(StateArrays<R> st, int n, T* __restrict__ o0, T* __restrict__ o1, T* __restrict__ o2,
+         T* __restrict__ o3, T* __restrict__ o4, T* __restrict__ o5, const float* __restrict__ ax,
+         const float* __restrict__ ay, const float* __restrict__ az, float* __restrict__ oax,
+         float* __restrict__ oay, float* __restrict__ oaz, double eps, double star_mass) {
+  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
+       s += (long long)gridDim.x * blockDim.x) {
+    const int o = st.id[s];
+    o0[o] = (T)st.v[0][s]; o1[o] = (T)st.v[1][s]; o2[o] = (T)st.v[2][s];
+    o3[o] = (T)st.v[3][s]; o4[o] = (T)st.v[4][s]; o5[o] = (T)st.v[5][s];
+    if (oax) {
+      double gx = ax[s], gy = ay[s], gz = az[s];
+      if (sizeof(R) == 8) {
+        double sx, sy, sz;
+        star_accel<double>((double)st.v[0][s], (double)st.v[1][s], (double)st.v[2][s], eps,
+                           star_mass, sx, sy, sz);
+        gx += sx; gy += sy; gz += sz;
+      }
+      oax[o] = (float)gx; oay[o] = (float)gy; oaz[o] = (float)gz;
+    }
+  }
+}
+
+__global__ void k_scatter_labels(const int* __restrict__ in_l, const uint16_t* __restrict__ in_s,
+                                 int n, int* __restrict__ out_l, uint16_t* __restrict__ out_s) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    out_l[i] = in_l[i];
+    out_s[i] = in_s[i];
+  }
+}
+
+template <typename T>
+T* dalloc(size_t count, const char* what) {
+  T* p = nullptr;
+  check(cudaMalloc(&p, sizeof(T) * (count ? count : 1)), what);
+  return p;
+}
+
+}  // namespace
+
+struct SimBase {
+  virtual ~SimBase() {}
+  nbody_sim_params p{};
+  int n = 0;
+  cudaStream_t st = 0;
+  int steps_done = 0;
+  bool has_state = false;
+  TreeWork tw;
+  float *ax = nullptr, *ay = nullptr, *az = nullptr;
+  float *dvx = nullptr, *dvy = nullptr, *dvz = nullptr;
+  float4* pert_tab = nullptr;
+  int pert_cap = 0;
+  int* spill = nullptr;
+  int spill_cap = 0;
+  int* work = nullptr;
+  unsigned long long* inter = nullptr;
+  int* parent = nullptr;
+  int* labels = nullptr;
+  int* sizes = nullptr;
+  uint16_t* agg = nullptr;
+  int* ngroups = nullptr;
+  void* staging = nullptr;  // n doubles
+  nbody_perturber pert{};
+  // profiling: events at phase boundaries of every step, read lazily
+  bool profiling = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::vector<cudaEvent_t>> ev_pending;  // per record: NBODY_PHASES + 1 events
+  std::vector<bool> ev_is_step;
+  std::vector<cudaEvent_t>* ev_cur = nullptr;
+  double phase_ms[NBODY_PHASES] = {0};
+  int profiled_steps = 0;
+  unsigned long long launches = 0;
+
+  cudaEvent_t take_event() {
+    if (ev_pool.empty()) {
+      cudaEvent_t e;
+      check(cudaEventCreate(&e), "cudaEventCreate");
+      return e;
+    }
+    cudaEvent_t e = ev_pool.back();
+    ev_pool.pop_back();
+    return e;
+  }
+  void mark(int phase) {  // boundary before `phase` (NBODY_PHASES = end)
+    if (!ev_cur) return;
+    check(cudaEventRecord((*ev_cur)[phase], st), "cudaEventRecord");
+  }
+  void begin_step_profile(bool is_step = true) {
+    if (!profiling) { ev_cur = nullptr; return; }
+    ev_is_step.push_back(is_step);
+    ev_pending.emplace_back();
+    ev_cur = &ev_pending.back();
+    for (int k = 0; k <= NBODY_PHASES; ++k) ev_cur->push_back(take_event());
+    for (int k = 0; k <= NBODY_PHASES; ++k) mark(k);  // phases skipped this step read 0
+  }
+  void collect_profile() {
+    if (ev_pending.empty()) return;
+    check(cudaStreamSynchronize(st), "profile sync");
+    for (size_t r = 0; r < ev_pending.size(); ++r) {
+      auto& evs = ev_pending[r];
+      for (int k = 0; k < NBODY_PHASES; ++k) {
+        float ms = 0.f;
+        check(cudaEventElapsedTime(&ms, evs[k], evs[k + 1]), "cudaEventElapsedTime");
+        phase_ms[k] += ms;
+      }
+      if (ev_is_step[r]) ++profiled_steps;
+      for (cudaEvent_t e : evs) ev_pool.push_back(e);
+    }
+    ev_pending.clear();
+    ev_is_step.clear();
+    ev_cur = nullptr;
+  }
+
+  virtual void set_state(const void* const* v, bool is_double, const float* mass,
+                         bool on_device, bool forces = true) = 0;
+  virtual void get_state(void* const* v, bool as_double, float* const* a, bool on_device) = 0;
+  virtual void step(int nsteps) = 0;
+  virtual const uint32_t* ids() = 0;
+  virtual void load_accel(const float* ax, const float* ay, const float* az) = 0;
+
+  void common_alloc() {
+    tree_alloc(tw, n);
+    ax = dalloc<float>(n, "ax"); ay = dalloc<float>(n, "ay"); az = dalloc<float>(n, "az");
+    dvx = dalloc<float>(n, "dvx"); dvy = dalloc<float>(n, "dvy"); dvz = dalloc<float>(n, "dvz");
+    spill_cap = 4096;
+    spill = dalloc<int>((size_t)walk_spill_slots(0) * spill_cap, "walk spill");
+    work = dalloc<int>(1, "work");
+    inter = dalloc<unsigned long long>(1, "inter");
+    parent = dalloc<int>(n, "fof parent");
+    labels = dalloc<int>(n, "fof labels");
+    sizes = dalloc<int>(n, "fof sizes");
+    agg = dalloc<uint16_t>(n, "fof agg");
+    ngroups = dalloc<int>(1, "fof ngroups");
+    staging = dalloc<double>(n, "staging");
+  }
+
+  void common_free() {
+    for (auto& evs : ev_pending)
+      for (cudaEvent_t e : evs) ev_pool.push_back(e);
+    for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
+    tree_free(tw);
+    void* ptrs[] = {ax, ay, az, dvx, dvy, dvz, pert_tab, spill, work, inter,
+                    parent, labels, sizes, agg, ngroups, staging};
+    for (void* q : ptrs)
+      if (q) cudaFree(q);
+  }
+
+  // Perturber positions for force times (k+1) dt, k in [k0, k0+count), by the
+  // host arithmetic of updatePerturber (Perturber.h:60-66).
+  void upload_perturber(int k0, int count) {
+    if (!p.perturber_enabled || count <= 0) return;
+    if (count > pert_cap) {
+      if (pert_tab) cudaFree(pert_tab);
+      pert_cap = std::max(count, 64);
+      pert_tab = dalloc<float4>(pert_cap, "perturber table");
+    }
+    std::vector<float4> h(count);
+    for (int k = 0; k < count; ++k) {
+      nbody_perturber q = pert;
+      nbody_perturber_update(&q, (float)(k0 + k + 1) * p.dt);
+      h[k] = make_float4(q.x, q.y, q.z, q.mass_msun);
+    }
+    check(cudaMemcpyAsync(pert_tab, h.data(), sizeof(float4) * count, cudaMemcpyHostToDevice, st),
+          "perturber upload");
+  }
+
+  int check_status() {
+    int s = 0;
+    check(cudaStreamSynchronize(st), "engine sync");
+    check(cudaMemcpy(&s, tw.status, sizeof(int), cudaMemcpyDeviceToHost), "status read");
+    return s;
+  }
+
+  void fof(float ll, int* out_labels, uint16_t* out_agg, int* n_groups, bool on_device) {
+    NeighborArgs na{tw.oct.info, tw.oct.box_lo, tw.oct.box_hi, tw.body4, n,
+                    p.leaf_max, spill, spill_cap, work, tw.status};
+    launch_fof_link(na, ids(), ll, parent, st);
+    launch_fof_finish(parent, n, labels, sizes, agg, ngroups, tw.status, st);
+    if (on_device) {
+      k_scatter_labels<<<stream_grid(n), kThreads, 0, st>>>(labels, agg, n, out_labels, out_agg);
+      check(cudaGetLastError(), "fof copy");
+    } else {
+      check(cudaMemcpyAsync(out_labels, labels, sizeof(int) * n, cudaMemcpyDeviceToHost, st),
+            "fof labels D2H");
+      check(cudaMemcpyAsync(out_agg, agg, sizeof(uint16_t) * n, cudaMemcpyDeviceToHost, st),
+            "fof sizes D2H");
+    }
+    check(cudaMemcpyAsync(n_groups, ngroups, sizeof(int), cudaMemcpyDeviceToHost, st),
+          "fof groups D2H");
+    check(cudaStreamSynchronize(st), "fof sync");
+  }
+};
+
+template <typename R>
+struct SimImpl : SimBase {
+  StateArrays<R> s[2]{};
+  int cur = 0;
+  float* vf = nullptr;  // FP64 mode: float velocities for the collision pass
+
+  SimImpl(const nbody_sim_params& prm, int nn) {
+    p = prm;
+    n = nn;
+    if (p.leaf_max <= 0) p.leaf_max = 8;
+    nbody_config c;
+    nbody_config_defaults(&c);
+    c.perturber_enabled = p.perturber_enabled;
+    c.perturber_mass_mjup = p.perturber_mass_mjup;
+    c.perturber_radius_AU = p.perturber_radius_au;
+    c.perturber_phase0 = p.perturber_phase0;
+    c.star_mass_msun = p.star_mass;
+    nbody_perturber_make(&c, &pert);
+    common_alloc();
+    for (int b = 0; b < 2; ++b) {
+      for (int k = 0; k < 6; ++k) s[b].v[k] = dalloc<R>(n, "state");
+      s[b].m = dalloc<float>(n, "mass");
+      s[b].id = dalloc<int>(n, "id");
+    }
+  }
+
+  ~SimImpl() override {
+    for (int b = 0; b < 2; ++b) {
+      for (int k = 0; k < 6; ++k) cudaFree(s[b].v[k]);
+      cudaFree(s[b].m);
+      cudaFree(s[b].id);
+    }
+    if (vf) cudaFree(vf);
+    common_free();
+  }
+
+  const uint32_t* ids() override { return (const uint32_t*)s[cur].id; }
+
+  void set_state(const void* const* v, bool is_double, const float* mass, bool on_device,
+                 bool forces) override {
+    cur = 0;
+    const size_t esz = is_double ? sizeof(double) : sizeof(float);
+    for (int k = 0; k < 6; ++k) {
+      const void* src = v[k];
+      if (!on_device) {
+        check(cudaMemcpyAsync(staging, src, esz * n, cudaMemcpyHostToDevice, st), "state H2D");
+        src = staging;
+      }
+      if (is_double)
+        k_convert<double, R><<<stream_grid(n), kThreads, 0, st>>>((const double*)src, s[0].v[k], n);
+      else
+        k_convert<float, R><<<stream_grid(n), kThreads, 0, st>>>((const float*)src, s[0].v[k], n);
+      check(cudaGetLastError(), "state convert");
+    }
+    check(cudaMemcpyAsync(s[0].m, mass, sizeof(float) * n,
+                          on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st),
+          "mass copy");
+    k_iota<<<stream_grid(n), kThreads, 0, st>>>(s[0].id, n);
+    check(cudaGetLastError(), "iota");
+    steps_done = 0;
+    has_state = true;
+    if (forces) {
+      launch_bbox<R>(tw, s[0].v[0], s[0].v[1], s[0].v[2], n, st);
+      compute_forces(-1);
+    } else {
+      launch_bbox_reset(tw, st);  // the next k_stream accumulates the bbox
+    }
+  }
+
+  void load_accel(const float* hax, const float* hay, const float* haz) override {
+    // caller order == current order right after set_state (id = iota)
+    check(cudaMemcpyAsync(ax, hax, sizeof(float) * n, cudaMemcpyHostToDevice, st), "ax H2D");
+    check(cudaMemcpyAsync(ay, hay, sizeof(float) * n, cudaMemcpyHostToDevice, st), "ay H2D");
+    check(cudaMemcpyAsync(az, haz, sizeof(float) * n, cudaMemcpyHostToDevice, st), "az H2D");
+  }
+
+  // Tree + walk for the current positions; pert_k indexes the perturber table
+  // (-1: time 0, positions from makePerturber).
+  void compute_forces(int pert_k) {
+    StateArrays<R>& a = s[cur];
+    StateArrays<R>& b = s[1 - cur];
+    mark(NBODY_PHASE_SORT);
+    launch_keys<R>(tw, a.v[0], a.v[1], a.v[2], n, st);
+    launch_bbox_reset(tw, st);
+    radix_sort_pairs(tw.keys, tw.perm, tw.keys_alt, tw.perm_alt, tw.counts, n, 30, st);
+    mark(NBODY_PHASE_PERMUTE);
+    k_permute<R><<<stream_grid(n), kThreads, 0, st>>>(tw.perm, a, b, n, tw.body4);
+    check(cudaGetLastError(), "k_permute launch");
+    cur = 1 - cur;
+    mark(NBODY_PHASE_TREE);
+    launch_build_topology(tw, n, st);
+    if (sizeof(R) == 8)
+      launch_build_moments(tw, n, (const double*)s[cur].v[0], (const double*)s[cur].v[1],
+                           (const double*)s[cur].v[2], st);
+    else
+      launch_build_moments(tw, n, nullptr, nullptr, nullptr, st);
+    const float4* pp = nullptr;
+    if (p.perturber_enabled) {
+      if (pert_k < 0) {
+        upload_perturber(-1, 1);  // (float)(0) * dt = 0
+      }
+      pp = pert_tab + std::max(pert_k, 0);
+    }
+    check(cudaMemsetAsync(inter, 0, sizeof(unsigned long long), st), "inter reset");
+    WalkArgs w{};
+    w.com = tw.oct.com; w.info = tw.oct.info; w.body = tw.body4; w.n = n;
+    w.theta2 = p.theta * p.theta; w.eps = p.softening; w.star_mass = p.star_mass;
+    w.star_in_walk = (sizeof(R) == 4) ? 1 : 0;
+    w.leaf_max = p.leaf_max; w.pert = pp;
+    w.ax = ax; w.ay = ay; w.az = az; w.scatter = nullptr;
+    w.spill = spill; w.spill_cap = spill_cap; w.inter = inter; w.work = work;
+    w.status = tw.status; w.group = 32;
+    mark(NBODY_PHASE_WALK);
+    launch_walk(w, st);
+    mark(NBODY_PHASE_COLLIDE);
+    // keys, bbox reset, 12 sort kernels, permute, karras, bottom-up, mark,
+    // 3 scan kernels, assign, write, walk
+    launches += 24;
+  }
+
+  void collide() {
+    NeighborArgs na{tw.oct.info, tw.oct.box_lo, tw.oct.box_hi, tw.body4, n,
+                    p.leaf_max, spill, spill_cap, work, tw.status};
+    if (sizeof(R) == 4) {
+      launch_collide(na, (const float*)s[cur].v[3], (const float*)s[cur].v[4],
+                     (const float*)s[cur].v[5], nullptr, p.r_coll, p.restitution, dvx, dvy, dvz,
+                     st);
+    } else {
+      // float copies of the half-step velocities for the FP32 impulse
+      if (!vf) vf = dalloc<float>(3 * (size_t)n, "velocity scratch");
+      for (int k = 0; k < 3; ++k)
+        k_convert<R, float><<<stream_grid(n), kThreads, 0, st>>>(s[cur].v[3 + k], vf + k * n, n);
+      check(cudaGetLastError(), "velocity convert");
+      launch_collide(na, vf, vf + n, vf + 2 * n, nullptr, p.r_coll, p.restitution, dvx, dvy, dvz,
+                     st);
+    }
+  }
+
+  void stream_kernel(bool end, bool begin) {
+    StreamArgs a{};
+    a.ax = ax; a.ay = ay; a.az = az;
+    const bool coll = p.r_coll > 0.f;
+    a.dvx = coll ? dvx : nullptr; a.dvy = coll ? dvy : nullptr; a.dvz = coll ? dvz : nullptr;
+    a.dt_f = p.dt;
+    a.dth_f = p.dt * 0.5f;
+    a.dt = (double)p.dt;
+    a.dth = (double)p.dt * 0.5;
+    const bool drag = p.gas_drag_rate > 0.f;
+    a.decay_f = drag ? expf(-p.gas_drag_rate * p.dt) : 0.f;
+    a.decay = drag ? std::exp(-(double)p.gas_drag_rate * (double)p.dt) : 0.0;
+    a.eps = p.softening;
+    a.star_mass = p.star_mass;
+    a.bbox = tw.bbox_enc;
+    const int g = stream_grid(n);
+    if (end && begin)
+      k_stream<R, true, true><<<g, kThreads, 0, st>>>(s[cur], n, a);
+    else if (end)
+      k_stream<R, true, false><<<g, kThreads, 0, st>>>(s[cur], n, a);
+    else
+      k_stream<R, false, true><<<g, kThreads, 0, st>>>(s[cur], n, a);
+    check(cudaGetLastError(), "k_stream launch");
+  }
+
+  void step(int nsteps) override {
+    if (nsteps <= 0) return;
+    upload_perturber(steps_done, nsteps);
+    const bool coll = p.r_coll > 0.f;
+    for (int k = 0; k < nsteps; ++k) {
+      begin_step_profile();
+      mark(NBODY_PHASE_STREAM);
+      stream_kernel(k > 0, true);
+      compute_forces(k);
+      if (coll) {
+        collide();
+        launches += (sizeof(R) == 8) ? 4 : 1;
+      }
+      mark(NBODY_PHASES);
+      launches += 1;
+    }
+    // the last step's dv + K2 + drag: a record that adds to the stream phase only
+    begin_step_profile(false);
+    stream_kernel(true, false);
+    for (int k = NBODY_PHASE_STREAM + 1; k <= NBODY_PHASES; ++k) mark(k);
+    launches += 1;
+    ev_cur = nullptr;
+    steps_done += nsteps;
+  }
+
+  void get_state(void* const* v, bool as_double, float* const* acc, bool on_device) override {
+    // unsort into device buffers (caller memory if on device, else staging)
+    const size_t esz = as_double ? sizeof(double) : sizeof(float);
+    std::vector<void*> dst(6);
+    std::vector<void*> tmp;
+    for (int k = 0; k < 6; ++k) {
+      if (on_device) {
+        dst[k] = v[k];
+      } else {
+        void* t = nullptr;
+        check(cudaMallocAsync(&t, esz * n, st), "get_state temp");
+        tmp.push_back(t);
+        dst[k] = t;
+      }
+    }
+    float* da[3] = {nullptr, nullptr, nullptr};
+    if (acc && acc[0]) {
+      for (int k = 0; k < 3; ++k) {
+        if (on_device) {
+          da[k] = acc[k];
+        } else {
+          void* t = nullptr;
+          check(cudaMallocAsync(&t, sizeof(float) * n, st), "get_state temp");
+          tmp.push_back(t);
+          da[k] = (float*)t;
+        }
+      }
+    }
+    if (as_double)
+      k_unsort<R, double><<<stream_grid(n), kThreads, 0, st>>>(
+          s[cur], n, (double*)dst[0], (double*)dst[1], (double*)dst[2], (double*)dst[3],
+          (double*)dst[4], (double*)dst[5], ax, ay, az, da[0], da[1], da[2], p.softening,
+          p.star_mass);
+    else
+      k_unsort<R, float><<<stream_grid(n), kThreads, 0, st>>>(
+          s[cur], n, (float*)dst[0], (float*)dst[1], (float*)dst[2], (float*)dst[3],
+          (float*)dst[4], (float*)dst[5], ax, ay, az, da[0], da[1], da[2], p.softening,
+          p.star_mass);
+    check(cudaGetLastError(), "k_unsort launch");
+    if (!on_device) {
+      for (int k = 0; k < 6; ++k)
+        check(cudaMemcpyAsync(v[k], dst[k], esz * n, cudaMemcpyDeviceToHost, st), "state D2H");
+      if (da[0])
+        for (int k = 0; k < 3; ++k)
+          check(cudaMemcpyAsync(acc[k], da[k], sizeof(float) * n, cudaMemcpyDeviceToHost, st),
+                "accel D2H");
+      for (void* t : tmp) check(cudaFreeAsync(t, st), "get_state free");
+    }
+    check(cudaStreamSynchronize(st), "get_state sync");
+  }
+};
+
+SimBase* make_sim(const nbody_sim_params& p, int n) {
+  if (p.state_precision == NBODY_STATE_F64) return new SimImpl<double>(p, n);
+  return new SimImpl<float>(p, n);
+}
+
+}  // namespace nb
+
+struct nbody_sim {
+  nb::SimBase* impl;
+};
+
+extern "C" {
+
+void nbody_sim_params_from_config(const nbody_config* cfg, nbody_sim_params* out) {
+  std::memset(out, 0, sizeof(*out));
+  out->dt = cfg->dt;
+  out->theta = cfg->theta;
+  out->softening = cfg->softening_AU;
+  out->star_mass = cfg->star_mass_msun;
+  // main.cu:58-59: r_coll = collision_radius_factor * particlePhysicalRadius
+  out->r_coll = cfg->collision_radius_factor * nbody_particle_radius(cfg->particle_mass_msun);
+  out->restitution = cfg->restitution;
+  out->gas_drag_rate = cfg->gas_drag_rate;
+  out->perturber_enabled = cfg->perturber_enabled;
+  out->perturber_mass_mjup = cfg->perturber_mass_mjup;
+  out->perturber_radius_au = cfg->perturber_radius_AU;
+  out->perturber_phase0 = cfg->perturber_phase0;
+  out->state_precision = NBODY_STATE_F32;
+  out->leaf_max = 8;
+}
+
+int nbody_sim_create(const nbody_sim_params* p, int n, nbody_sim** out) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(p && out, "nbody_sim_create: null argument");
+    NBODY_REQUIRE(n > 0 && n < (1 << 27), "nbody_sim_create: n must be in [1, 2^27)");
+    NBODY_REQUIRE(p->dt > 0.f, "nbody_sim_create: dt must be positive");
+    NBODY_REQUIRE(p->state_precision == NBODY_STATE_F32 || p->state_precision == NBODY_STATE_F64,
+                  "nbody_sim_create: unknown state precision");
+    *out = nullptr;
+    nbody_sim* s = new nbody_sim{nb::make_sim(*p, n)};
+    *out = s;
+  })
+}
+
+void nbody_sim_destroy(nbody_sim* s) {
+  if (!s) return;
+  cudaStreamSynchronize(s->impl->st);
+  delete s->impl;
+  delete s;
+}
+
+int nbody_sim_set_stream(nbody_sim* s, void* stream) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(s, "nbody_sim_set_stream: null sim");
+    s->impl->st = (cudaStream_t)stream;
+  })
+}
+
+int nbody_sim_set_state(nbody_sim* s, const float* x, const float* y, const float* z,
+                        const float* vx, const float* vy, const float* vz, const float* mass,
+                        int on_device) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(s && x && y && z && vx && vy && vz && mass, "nbody_sim_set_state: null array");
+    const void* v[6] = {x, y, z, vx, vy, vz};
+    s->impl->set_state(v, false, mass, on_device != 0);
+  })
+}
+
+int nbody_sim_set_state_f64(nbody_sim* s, const double* x, const double* y, const double* z,
+                            const double* vx, const double* vy, const double* vz,
+                            const float* mass, int on_device) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(s && x && y && z && vx && vy && vz && mass,
+                  "nbody_sim_set_state_f64: null array");
+    const void* v[6] = {x, y, z, vx, vy, vz};
+    s->impl->set_state(v, true, mass, on_device != 0);
+  })
+}
+
+int nbody_sim_step(nbody_sim* s, int nsteps) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(s, "nbody_sim_step: null sim");
+    NBODY_REQUIRE(s->impl->has_state, "nbody_sim_step: state not set");
+    NBODY_REQUIRE(nsteps >= 0, "nbody_sim_step: negative step count");
+    s->impl->step(nsteps);
+  })
+}
+
+int nbody_sim_sync(nbody_sim* s) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(s, "nbody_sim_sync: null sim");
+    int st = s->impl->check_status();
+    if (st) {
+      nb::check(cudaMemsetAsync(s->impl->tw.status, 0, sizeof(int), s->impl->st), "status reset");
+      throw nb::ArgError("device status " + std::to_string(st) +
+                             " (1 walk stack, 2 union-find, 4 tree, 8 non-finite position)",
+                         NBODY_ERR_OVERFLOW);
+    }
+  })
+}
+
+int nbody_sim_get_state(nbody_sim* s, float* x, float* y, float* z, float* vx, float* vy,
+                        float* vz, float* ax, float* ay, float* az, int on_device) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(s && x && y && z && vx && vy && vz, "nbody_sim_get_state: null array");
+    NBODY_REQUIRE(s->impl->has_state, "nbody_sim_get_state: state not set");
+    void* v[6] = {x, y, z, vx, vy, vz};
+    float* a[3] = {ax, ay, az};
+    s->impl->get_state(v, false, (ax && ay && az) ? a : nullptr, on_device != 0);
+  })
+}
+
+int nbody_sim_get_state_f64(nbody_sim* s, double* x, double* y, double* z, double* vx,
+                            double* vy, double* vz, int on_device) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(s && x && y && z && vx && vy && vz, "nbody_sim_get_state_f64: null array");
+    NBODY_REQUIRE(s->impl->has_state, "nbody_sim_get_state_f64: state not set");
+    void* v[6] = {x, y, z, vx, vy, vz};
+    s->impl->get_state(v, true, nullptr, on_device != 0);
+  })
+}
+
+int nbody_sim_fof(nbody_sim* s, float link_length, int* labels, uint16_t* agg_size,
+                  int* n_groups, int on_device) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(s && labels && agg_size && n_groups, "nbody_sim_fof: null argument");
+    NBODY_REQUIRE(s->impl->has_state, "nbody_sim_fof: state not set");
+    s->impl->fof(link_length, labels, agg_size, n_groups, on_device != 0);
+  })
+}
+
+int nbody_sim_set_profiling(nbody_sim* s, int on) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(s, "nbody_sim_set_profiling: null sim");
+    s->impl->profiling = on != 0;
+  })
+}
+
+int nbody_sim_profile_get(nbody_sim* s, nbody_sim_profile* out, int reset) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(s && out, "nbody_sim_profile_get: null argument");
+    nb::SimBase* b = s->impl;
+    b->collect_profile();
+    std::memset(out, 0, sizeof(*out));
+    for (int k = 0; k < NBODY_PHASES; ++k) out->ms[k] = b->phase_ms[k];
+    out->steps = b->profiled_steps;
+    out->launches = b->launches;
+    if (reset) {
+      for (int k = 0; k < NBODY_PHASES; ++k) b->phase_ms[k] = 0.0;
+      b->profiled_steps = 0;
+      b->launches = 0;
+    }
+  })
+}
+
+int nbody_sim_stats_get(nbody_sim* s, nbody_sim_stats* out) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(s && out, "nbody_sim_stats_get: null argument");
+    nb::SimBase* b = s->impl;
+    nb::check(cudaStreamSynchronize(b->st), "stats sync");
+    std::memset(out, 0, sizeof(*out));
+    out->n = b->n;
+    out->steps_done = b->steps_done;
+    nb::check(cudaMemcpy(&out->n_nodes, b->tw.n_nodes, sizeof(int), cudaMemcpyDeviceToHost),
+              "n_nodes");
+    nb::check(cudaMemcpy(&out->interactions, b->inter, sizeof(unsigned long long),
+                         cudaMemcpyDeviceToHost), "interactions");
+    nb::check(cudaMemcpy(&out->status, b->tw.status, sizeof(int), cudaMemcpyDeviceToHost),
+              "status");
+  })
+}
+
+int nbody_sim_step_host(nbody_sim* s, float* x, float* y, float* z, float* vx, float* vy,
+                        float* vz, float* ax, float* ay, float* az, const float* mass,
+                        int nsteps) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(s && x && y && z && vx && vy && vz && ax && ay && az && mass,
+                  "nbody_sim_step_host: null array");
+    nb::SimBase* b = s->impl;
+    NBODY_REQUIRE(b->p.state_precision == NBODY_STATE_F32,
+                  "nbody_sim_step_host: needs NBODY_STATE_F32");
+    NBODY_REQUIRE(nsteps >= 0, "nbody_sim_step_host: negative step count");
+    const int steps0 = b->steps_done;
+    const void* v[6] = {x, y, z, vx, vy, vz};
+    b->set_state(v, false, mass, false, false);  // copyToGPU of ParticleData
+    b->load_accel(ax, ay, az);
+    b->steps_done = steps0;                      // the caller's clock continues
+    b->step(nsteps);
+    void* o[6] = {x, y, z, vx, vy, vz};
+    float* a[3] = {ax, ay, az};
+    b->get_state(o, false, a, false);            // copyToCPU
+  })
+}
+
+}  // extern "C"
