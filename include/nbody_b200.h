@@ -154,6 +154,8 @@ typedef struct nbody_tree_stats {
   double root_com[3];
   unsigned long long interactions; /* accepted interactions of the last force */
   int status;          /* device status bits of the last calls                */
+  unsigned long long walk_nodes_visited;  /* node tests of the last force walk */
+  unsigned long long walk_stack_spills;   /* stack spills of the last force walk */
 } nbody_tree_stats;
 int nbody_tree_stats_get(nbody_tree* t, nbody_tree_stats* out);
 
@@ -283,6 +285,9 @@ typedef struct nbody_sim_stats {
   int n_nodes;
   unsigned long long interactions;  /* accepted interactions of the last walk */
   int status;
+  unsigned long long walk_nodes_visited;  /* node tests of the last walk */
+  unsigned long long walk_stack_spills;   /* stack spills of the last walk */
+  unsigned long long walk_groups;         /* warp groups of the last walk */
 } nbody_sim_stats;
 int nbody_sim_stats_get(nbody_sim* s, nbody_sim_stats* out);
 

@@ -97,7 +97,8 @@ class nbody_tree_stats(C.Structure):
                 ("bbox_max", C.c_float * 3), ("root_center", C.c_float * 3),
                 ("root_half", C.c_float), ("root_mass", C.c_double),
                 ("root_com", C.c_double * 3), ("interactions", C.c_ulonglong),
-                ("status", C.c_int)]
+                ("status", C.c_int), ("walk_nodes_visited", C.c_ulonglong),
+                ("walk_stack_spills", C.c_ulonglong)]
 
 
 class nbody_aggregate(C.Structure):
@@ -127,7 +128,9 @@ class nbody_sim_profile(C.Structure):
 
 class nbody_sim_stats(C.Structure):
     _fields_ = [("n", C.c_int), ("steps_done", C.c_int), ("n_nodes", C.c_int),
-                ("interactions", C.c_ulonglong), ("status", C.c_int)]
+                ("interactions", C.c_ulonglong), ("status", C.c_int),
+                ("walk_nodes_visited", C.c_ulonglong), ("walk_stack_spills", C.c_ulonglong),
+                ("walk_groups", C.c_ulonglong)]
 
 
 # (name, restype, argtypes): every symbol include/nbody_b200.h declares

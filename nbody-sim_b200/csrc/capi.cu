@@ -50,6 +50,7 @@ struct nbody_tree {
   int spill_cap = 4096;
   int* work = nullptr;
   unsigned long long* inter = nullptr;
+  unsigned long long* counters = nullptr;
   int* parent = nullptr;
   int* sizes = nullptr;
   int* ngroups = nullptr;
@@ -89,6 +90,7 @@ int nbody_tree_create(int n_bodies, nbody_tree** out) {
       t->spill = nb::dalloc<int>((size_t)nb::walk_spill_slots(0) * t->spill_cap, "spill");
       t->work = nb::dalloc<int>(1, "work");
       t->inter = nb::dalloc<unsigned long long>(1, "inter");
+      t->counters = nb::dalloc<unsigned long long>(3, "walk counters");
       t->parent = nb::dalloc<int>(n_bodies, "fof parent");
       t->sizes = nb::dalloc<int>(n_bodies, "fof sizes");
       t->ngroups = nb::dalloc<int>(1, "fof groups");
@@ -106,7 +108,7 @@ void nbody_tree_destroy(nbody_tree* t) {
   cudaStreamSynchronize(0);
   nb::tree_free(t->tw);
   void* ptrs[] = {t->sort_idx, t->dvx, t->dvy, t->dvz, t->spill, t->work,
-                  t->inter, t->parent, t->sizes, t->ngroups};
+                  t->inter, t->counters, t->parent, t->sizes, t->ngroups};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   delete t;
@@ -149,6 +151,7 @@ int nbody_tree_build(nbody_tree* t, const nbody_particles* p) {
                          t->n, 30, 0);
     nb::launch_gather_body4(t->tw, p->x, p->y, p->z, p->mass, t->n, 0);
     nb::launch_build_topology(t->tw, t->n, 0);
+    nb::launch_build_groups(t->tw, t->n, 32, 0);
     nb::finish("launchBuildKernel");
     t->have_bbox = false;
     t->built = true;
@@ -195,12 +198,15 @@ int nbody_tree_force(nbody_tree* t, nbody_particles* p, float theta, float softe
     nb::check_particles(p, t->n, false, true);
     if (!t->summarized) throw nb::ArgError("nbody_tree_force: tree not summarized", NBODY_ERR_STATE);
     nb::check(cudaMemset(t->inter, 0, sizeof(unsigned long long)), "inter reset");
+    nb::check(cudaMemset(t->counters, 0, 3 * sizeof(unsigned long long)), "counters reset");
     nb::WalkArgs w{};
     w.com = t->tw.oct.com; w.info = t->tw.oct.info; w.body = t->tw.body4; w.n = t->n;
+    w.groups = t->tw.groups; w.n_groups = t->tw.n_groups;
     w.theta2 = theta * theta; w.eps = softening; w.star_mass = star_mass; w.star_in_walk = 1;
     w.leaf_max = t->leaf_max; w.pert = nullptr;
     w.ax = p->ax; w.ay = p->ay; w.az = p->az; w.scatter = t->tw.perm;
     w.spill = t->spill; w.spill_cap = t->spill_cap; w.inter = t->inter; w.work = t->work;
+    w.counters = t->counters;
     w.status = t->tw.status; w.group = 32;
     nb::launch_walk(w, 0);
     nb::finish("launchForceKernel");
@@ -214,7 +220,7 @@ int nbody_tree_collide(nbody_tree* t, nbody_particles* p, float r_coll, float re
     nb::check_particles(p, t->n, true, false);
     if (!t->summarized) throw nb::ArgError("nbody_tree_collide: tree not summarized", NBODY_ERR_STATE);
     nb::NeighborArgs na{t->tw.oct.info, t->tw.oct.box_lo, t->tw.oct.box_hi, t->tw.body4, t->n,
-                        t->leaf_max, t->spill, t->spill_cap, t->work, t->tw.status};
+                        t->tw.groups, t->tw.n_groups, t->leaf_max, t->spill, t->spill_cap, t->work, t->tw.status};
     nb::launch_collide(na, p->vx, p->vy, p->vz, t->tw.perm, r_coll, restitution, t->dvx, t->dvy,
                        t->dvz, 0);
     nb::launch_apply_dv(p->vx, p->vy, p->vz, t->dvx, t->dvy, t->dvz, t->tw.perm, t->n, 0);
@@ -270,6 +276,10 @@ int nbody_tree_stats_get(nbody_tree* t, nbody_tree_stats* out) {
                          cudaMemcpyDeviceToHost), "interactions read");
     nb::check(cudaMemcpy(&out->status, t->tw.status, sizeof(int), cudaMemcpyDeviceToHost),
               "status read");
+    unsigned long long c[3];
+    nb::check(cudaMemcpy(c, t->counters, sizeof(c), cudaMemcpyDeviceToHost), "counters read");
+    out->walk_nodes_visited = c[0];
+    out->walk_stack_spills = c[1];
   })
 }
 
@@ -334,9 +344,10 @@ int nbody_fof(nbody_tree* t, const float* x, const float* y, const float* z, int
     nb::radix_sort_pairs(w.keys, w.perm, w.keys_alt, w.perm_alt, w.counts, n, 30, 0);
     nb::launch_gather_body4(w, x, y, z, nullptr, n, 0);
     nb::launch_build_topology(w, n, 0);
+    nb::launch_build_groups(w, n, 32, 0);
     nb::launch_build_moments(w, n, nullptr, nullptr, nullptr, 0);
     nb::NeighborArgs na{w.oct.info, w.oct.box_lo, w.oct.box_hi, w.body4, n,
-                        t->leaf_max, t->spill, t->spill_cap, t->work, w.status};
+                        w.groups, w.n_groups, t->leaf_max, t->spill, t->spill_cap, t->work, w.status};
     nb::launch_fof_link(na, w.perm, link_length, t->parent, 0);
     nb::launch_fof_finish(t->parent, n, labels, t->sizes, agg_size, t->ngroups, w.status, 0);
     nb::finish("nbody_fof");

@@ -58,6 +58,10 @@ struct TreeWork {
   TreeGeom* geom = nullptr;
   int* n_nodes = nullptr;
   int* status = nullptr;
+  // warp target groups: (first body, count), maximal binary nodes <= 32 bodies
+  int2* groups = nullptr;
+  uint32_t* group_flag = nullptr;
+  int* n_groups = nullptr;
 };
 
 void tree_alloc(TreeWork& w, int cap);
@@ -78,6 +82,8 @@ void launch_gather_body4(TreeWork& w, const float* x, const float* y, const floa
 void launch_build_topology(TreeWork& w, int n, cudaStream_t s);
 void launch_build_moments(TreeWork& w, int n, const double* xd, const double* yd,
                           const double* zd, cudaStream_t s);
+// Target groups (needs the topology): w.groups, w.n_groups (device).
+void launch_build_groups(TreeWork& w, int n, int gmax, cudaStream_t s);
 
 size_t radix_sort_count_words(int n);
 void radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt,
@@ -91,6 +97,8 @@ struct WalkArgs {
   const int4* info;
   const float4* body;
   int n;
+  const int2* groups;     // target groups (first body, count <= 32)
+  const int* n_groups;    // device count of groups
   float theta2;           // theta^2
   float eps;              // softening
   float star_mass;
@@ -104,6 +112,7 @@ struct WalkArgs {
   int* spill;
   int spill_cap;
   unsigned long long* inter;  // accepted interactions (sources x targets)
+  unsigned long long* counters;  // optional: nodes visited, stack spills, groups
   int* work;
   int* status;
   int group;              // targets per warp group: 32 or 64
@@ -118,6 +127,8 @@ struct NeighborArgs {
   const float4* box_hi;
   const float4* body;
   int n;
+  const int2* groups;
+  const int* n_groups;
   int leaf_max;
   int* spill;
   int spill_cap;

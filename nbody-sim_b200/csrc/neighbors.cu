@@ -83,7 +83,7 @@ k_neighbors(const NeighborArgs a, float radius, CollideOut co, FofOut fo) {
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   NbSmem& w = smem[wib];
   int* spill = a.spill + (size_t)(blockIdx.x * kNbWarps + wib) * (size_t)a.spill_cap;
-  const int n_groups = (a.n + 31) >> 5;
+  const int n_groups = *a.n_groups;
   // conservative per-axis reach: a pair that passes the FP32 test is closer
   // than radius (1 + 2^-20) on every axis
   const float reach = radius * 1.00001f + 1e-30f;
@@ -93,9 +93,10 @@ k_neighbors(const NeighborArgs a, float radius, CollideOut co, FofOut fo) {
     if (lane == 0) g = atomicAdd(a.work, 1);
     g = __shfl_sync(kFull, g, 0);
     if (g >= n_groups) break;
-    const int s = g * 32 + lane;
-    const bool valid = s < a.n;
-    const float4 me = a.body[valid ? s : g * 32];
+    const int2 gr = a.groups[g];
+    const int s = gr.x + lane;
+    const bool valid = lane < gr.y;
+    const float4 me = a.body[valid ? s : gr.x];
     const float gx0 = warp_min(me.x) - reach, gx1 = warp_max(me.x) + reach;
     const float gy0 = warp_min(me.y) - reach, gy1 = warp_max(me.y) + reach;
     const float gz0 = warp_min(me.z) - reach, gz1 = warp_max(me.z) + reach;
@@ -279,7 +280,7 @@ template <int kMode>
 void launch_nb(const NeighborArgs& a, float radius, const CollideOut& co, const FofOut& fo,
                cudaStream_t s) {
   if (a.n <= 0) return;
-  const int groups = (a.n + 31) / 32;
+  const int groups = a.n;  // upper bound on the group count
   int grid = sm_count() * nb_blocks_per_sm<kMode>();
   // the spill area is sized for the walk's slot count; never exceed it
   grid = std::min(grid, walk_spill_slots(0) / kNbWarps);

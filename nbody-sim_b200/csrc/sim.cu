@@ -221,6 +221,7 @@ struct SimBase {
   int spill_cap = 0;
   int* work = nullptr;
   unsigned long long* inter = nullptr;
+  unsigned long long* counters = nullptr;  // walk: nodes visited, spills, groups
   int* parent = nullptr;
   int* labels = nullptr;
   int* sizes = nullptr;
@@ -293,6 +294,7 @@ struct SimBase {
     spill = dalloc<int>((size_t)walk_spill_slots(0) * spill_cap, "walk spill");
     work = dalloc<int>(1, "work");
     inter = dalloc<unsigned long long>(1, "inter");
+    counters = dalloc<unsigned long long>(3, "walk counters");
     parent = dalloc<int>(n, "fof parent");
     labels = dalloc<int>(n, "fof labels");
     sizes = dalloc<int>(n, "fof sizes");
@@ -306,7 +308,7 @@ struct SimBase {
       for (cudaEvent_t e : evs) ev_pool.push_back(e);
     for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
     tree_free(tw);
-    void* ptrs[] = {ax, ay, az, dvx, dvy, dvz, pert_tab, spill, work, inter,
+    void* ptrs[] = {ax, ay, az, dvx, dvy, dvz, pert_tab, spill, work, inter, counters,
                     parent, labels, sizes, agg, ngroups, staging};
     for (void* q : ptrs)
       if (q) cudaFree(q);
@@ -340,7 +342,7 @@ struct SimBase {
 
   void fof(float ll, int* out_labels, uint16_t* out_agg, int* n_groups, bool on_device) {
     NeighborArgs na{tw.oct.info, tw.oct.box_lo, tw.oct.box_hi, tw.body4, n,
-                    p.leaf_max, spill, spill_cap, work, tw.status};
+                    tw.groups, tw.n_groups, p.leaf_max, spill, spill_cap, work, tw.status};
     launch_fof_link(na, ids(), ll, parent, st);
     launch_fof_finish(parent, n, labels, sizes, agg, ngroups, tw.status, st);
     if (on_device) {
@@ -449,6 +451,7 @@ struct SimImpl : SimBase {
     cur = 1 - cur;
     mark(NBODY_PHASE_TREE);
     launch_build_topology(tw, n, st);
+    launch_build_groups(tw, n, 32, st);
     if (sizeof(R) == 8)
       launch_build_moments(tw, n, (const double*)s[cur].v[0], (const double*)s[cur].v[1],
                            (const double*)s[cur].v[2], st);
@@ -462,25 +465,28 @@ struct SimImpl : SimBase {
       pp = pert_tab + std::max(pert_k, 0);
     }
     check(cudaMemsetAsync(inter, 0, sizeof(unsigned long long), st), "inter reset");
+    check(cudaMemsetAsync(counters, 0, 3 * sizeof(unsigned long long), st), "counters reset");
     WalkArgs w{};
     w.com = tw.oct.com; w.info = tw.oct.info; w.body = tw.body4; w.n = n;
+    w.groups = tw.groups; w.n_groups = tw.n_groups;
     w.theta2 = p.theta * p.theta; w.eps = p.softening; w.star_mass = p.star_mass;
     w.star_in_walk = (sizeof(R) == 4) ? 1 : 0;
     w.leaf_max = p.leaf_max; w.pert = pp;
     w.ax = ax; w.ay = ay; w.az = az; w.scatter = nullptr;
-    w.spill = spill; w.spill_cap = spill_cap; w.inter = inter; w.work = work;
-    w.status = tw.status; w.group = 32;
+    w.spill = spill; w.spill_cap = spill_cap; w.inter = inter; w.counters = counters;
+    w.work = work; w.status = tw.status; w.group = 32;
     mark(NBODY_PHASE_WALK);
     launch_walk(w, st);
     mark(NBODY_PHASE_COLLIDE);
-    // keys, bbox reset, 12 sort kernels, permute, karras, bottom-up, mark,
-    // 3 scan kernels, assign, write, walk
-    launches += 24;
+    // keys, bbox reset, 20 sort kernels (4 x upsweep, 3 scan, scatter),
+    // permute, karras, 5 group kernels (mark, 3 scan, write), bottom-up,
+    // mark, 3 scan kernels, assign, write, walk
+    launches += 37;
   }
 
   void collide() {
     NeighborArgs na{tw.oct.info, tw.oct.box_lo, tw.oct.box_hi, tw.body4, n,
-                    p.leaf_max, spill, spill_cap, work, tw.status};
+                    tw.groups, tw.n_groups, p.leaf_max, spill, spill_cap, work, tw.status};
     if (sizeof(R) == 4) {
       launch_collide(na, (const float*)s[cur].v[3], (const float*)s[cur].v[4],
                      (const float*)s[cur].v[5], nullptr, p.r_coll, p.restitution, dvx, dvy, dvz,
@@ -767,6 +773,11 @@ int nbody_sim_stats_get(nbody_sim* s, nbody_sim_stats* out) {
                          cudaMemcpyDeviceToHost), "interactions");
     nb::check(cudaMemcpy(&out->status, b->tw.status, sizeof(int), cudaMemcpyDeviceToHost),
               "status");
+    unsigned long long c[3];
+    nb::check(cudaMemcpy(c, b->counters, sizeof(c), cudaMemcpyDeviceToHost), "counters");
+    out->walk_nodes_visited = c[0];
+    out->walk_stack_spills = c[1];
+    out->walk_groups = c[2];
   })
 }
 

@@ -236,18 +236,25 @@ k_scan_down(uint32_t* __restrict__ data, int n, const uint32_t* __restrict__ sum
 
 }  // namespace
 
-size_t radix_sort_count_words(int n) { return (size_t)kBins * (size_t)div_up(n, kTile); }
+size_t scan_tmp_words(int n);
+
+size_t radix_sort_count_words(int n) {
+  const size_t table = (size_t)kBins * (size_t)div_up(n, kTile);
+  return table + scan_tmp_words((int)table);
+}
 
 void radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt,
                       uint32_t* counts, int n, int bits, cudaStream_t s) {
   if (n <= 1) return;
   const int nb = div_up(n, kTile);
   const int passes = (bits + 7) / 8;
+  // the count table is followed by room for the multi-block scan's partials
+  uint32_t* scan_tmp = counts + (size_t)kBins * nb;
   uint32_t *ki = keys, *vi = vals, *ko = keys_alt, *vo = vals_alt;
   for (int p = 0; p < passes; ++p) {
     const int shift = 8 * p;
     k_sort_upsweep<<<nb, kSortThreads, 0, s>>>(ki, counts, n, shift, nb);
-    k_scan_inplace<<<1, 1024, 0, s>>>(counts, kBins * nb);
+    scan_exclusive_u32(counts, kBins * nb, scan_tmp, s);
     k_sort_scatter<<<nb, kSortThreads, 0, s>>>(ki, vi, ko, vo, counts, n, shift, nb);
     uint32_t* t = ki; ki = ko; ko = t;
     t = vi; vi = vo; vo = t;

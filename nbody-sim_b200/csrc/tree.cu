@@ -329,6 +329,51 @@ k_oct_write(int n, const int* __restrict__ lo, const int* __restrict__ hi,
   oct.box_hi[f] = hi4;
 }
 
+// Target groups for the warp walks: the maximal nodes of the binary radix
+// tree holding <= gmax bodies.  They partition the bodies into contiguous
+// key ranges whose bodies share a Morton prefix, so a group never straddles
+// a jump of the space-filling curve (a fixed run of 32 consecutive bodies
+// can: its box then spans most of the domain and its walk degenerates to
+// O(N) work on one warp).
+__global__ void __launch_bounds__(kThreads)
+k_group_mark(int n, int gmax, const int* __restrict__ lo, const int* __restrict__ hi,
+             const int* __restrict__ parent, uint32_t* __restrict__ flag) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nb = 2 * n - 1;
+  if (b >= nb) return;
+  const int cnt = (b >= n - 1) ? 1 : hi[b] - lo[b] + 1;
+  int pc = 0x7fffffff;
+  if (b != 0) {
+    const int p = parent[b];
+    pc = hi[p] - lo[p] + 1;
+  }
+  flag[b] = (cnt <= gmax && pc > gmax) ? 1u : 0u;
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_group_write(int n, int gmax, const int* __restrict__ lo, const int* __restrict__ hi,
+              const int* __restrict__ parent, const uint32_t* __restrict__ off,
+              int2* __restrict__ groups, int* __restrict__ n_groups) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nb = 2 * n - 1;
+  if (b >= nb) return;
+  const bool leaf = b >= n - 1;
+  const int cnt = leaf ? 1 : hi[b] - lo[b] + 1;
+  int pc = 0x7fffffff;
+  if (b != 0) {
+    const int p = parent[b];
+    pc = hi[p] - lo[p] + 1;
+  }
+  const bool is_group = cnt <= gmax && pc > gmax;
+  if (is_group) groups[off[b]] = make_int2(leaf ? b - (n - 1) : lo[b], cnt);
+  if (b == nb - 1) *n_groups = (int)off[b] + (is_group ? 1 : 0);
+}
+
+__global__ void k_group_single(int2* groups, int* n_groups) {
+  groups[0] = make_int2(0, 1);
+  *n_groups = 1;
+}
+
 // N == 1: the root is the single body.
 __global__ void k_oct_single(const float4* __restrict__ body4, const TreeGeom* __restrict__ geom,
                              OctNodes oct, int* __restrict__ n_nodes) {
@@ -383,6 +428,9 @@ void tree_alloc(TreeWork& w, int cap) {
   w.bbox_enc = dalloc<unsigned long long>(6, "bbox");
   w.geom = dalloc<TreeGeom>(1, "geom");
   w.n_nodes = dalloc<int>(1, "n_nodes");
+  w.groups = dalloc<int2>(n, "groups");
+  w.group_flag = dalloc<uint32_t>(nb, "group flags");
+  w.n_groups = dalloc<int>(1, "n_groups");
   w.status = dalloc<int>(1, "status");
   check(cudaMemset(w.status, 0, sizeof(int)), "status init");
   check(cudaMemset(w.n_nodes, 0, sizeof(int)), "n_nodes init");
@@ -393,7 +441,7 @@ void tree_free(TreeWork& w) {
                   w.bin_right, w.bin_parent, w.bin_lo, w.bin_hi, w.bin_prefix, w.bin_visit,
                   w.bin_sum, w.bin_box_lo, w.bin_box_hi, w.oct_nch, w.oct_off, w.oct_final,
                   w.scan_tmp, w.oct.com, w.oct.info, w.oct.box_lo, w.oct.box_hi, w.bbox_enc,
-                  w.geom, w.n_nodes, w.status};
+                  w.geom, w.n_nodes, w.status, w.groups, w.group_flag, w.n_groups};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   w = TreeWork();
@@ -443,6 +491,22 @@ void launch_build_topology(TreeWork& w, int n, cudaStream_t s) {
                                                 w.bin_parent, w.bin_lo, w.bin_hi, w.bin_prefix,
                                                 w.bin_visit);
   check(cudaGetLastError(), "k_karras launch");
+}
+
+void launch_build_groups(TreeWork& w, int n, int gmax, cudaStream_t s) {
+  if (n < 1) return;
+  if (n == 1) {
+    k_group_single<<<1, 1, 0, s>>>(w.groups, w.n_groups);
+    check(cudaGetLastError(), "k_group_single launch");
+    return;
+  }
+  const int nb = 2 * n - 1;
+  k_group_mark<<<grid_for(nb), kThreads, 0, s>>>(n, gmax, w.bin_lo, w.bin_hi, w.bin_parent,
+                                                 w.group_flag);
+  scan_exclusive_u32(w.group_flag, nb, w.scan_tmp, s);
+  k_group_write<<<grid_for(nb), kThreads, 0, s>>>(n, gmax, w.bin_lo, w.bin_hi, w.bin_parent,
+                                                  w.group_flag, w.groups, w.n_groups);
+  check(cudaGetLastError(), "group launch");
 }
 
 void launch_build_moments(TreeWork& w, int n, const double* xd, const double* yd,

@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(const WalkArgs a) {
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   WarpSmem& w = smem[wib];
   int* spill = a.spill + (size_t)(blockIdx.x * kWalkWarps + wib) * (size_t)a.spill_cap;
-  const int n_groups = (a.n + 31) >> 5;
+  const int n_groups = *a.n_groups;
   const float eps2 = a.eps * a.eps;
 
   while (true) {
@@ -82,21 +82,19 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(const WalkArgs a) {
     if (lane == 0) g = atomicAdd(a.work, 1);
     g = __shfl_sync(kFull, g, 0);
     if (g >= n_groups) break;
-    const int s = g * 32 + lane;
-    const bool valid = s < a.n;
-    const float4 me = a.body[valid ? s : g * 32];
+    const int2 gr = a.groups[g];
+    const int s = gr.x + lane;
+    const bool valid = lane < gr.y;
+    const float4 me = a.body[valid ? s : gr.x];
     const float gx0 = warp_min(me.x), gx1 = warp_max(me.x);
     const float gy0 = warp_min(me.y), gy1 = warp_max(me.y);
     const float gz0 = warp_min(me.z), gz1 = warp_max(me.z);
 
+    // The tree sum starts from zero: adding ~10^3 terms into an accumulator
+    // that already holds the star pull (10^3-10^5 times larger) would round
+    // every term at the star's ulp.  Star and perturber are added at the end.
     float ax = 0.f, ay = 0.f, az = 0.f;
-    if (a.star_in_walk) {  // softened star term, BHTree.cu:547-553
-      float dx = -me.x, dy = -me.y, dz = -me.z;
-      float r2 = dx * dx + dy * dy + dz * dz + a.eps * a.eps;
-      float r = sqrtf(r2);
-      float f = a.star_mass / (r2 * r);
-      ax += f * dx; ay += f * dy; az += f * dz;
-    }
+    unsigned long long visited = 0, spills = 0;
 
     int top = 1, spilled = 0, nlist = 0;
     unsigned long long evaluated = 0;
@@ -115,6 +113,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(const WalkArgs a) {
       }
       const int take = min(top, 32);
       top -= take;
+      visited += take;
       const int node = (lane < take) ? w.stk[top + lane] : -1;
       __syncwarp();
 
@@ -166,6 +165,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(const WalkArgs a) {
       if (ptotal > 0) {
         if (top + ptotal > kStk) {
           if (spilled + top > a.spill_cap) { overflow = true; break; }
+          ++spills;
           for (int k = lane; k < top; k += 32) __stcg(spill + spilled + k, w.stk[k]);
           spilled += top;
           top = 0;
@@ -211,6 +211,13 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(const WalkArgs a) {
     evaluated += nlist;
     __syncwarp();
 
+    if (a.star_in_walk) {  // softened star term, BHTree.cu:547-553
+      float dx = -me.x, dy = -me.y, dz = -me.z;
+      float r2 = dx * dx + dy * dy + dz * dz + a.eps * a.eps;
+      float r = sqrtf(r2);
+      float f = a.star_mass / (r2 * r);
+      ax += f * dx; ay += f * dy; az += f * dz;
+    }
     if (a.pert) {  // perturber_forceKernel, Perturber.cu:20-34 (adds)
       const float4 p = *a.pert;
       float dx = p.x - me.x, dy = p.y - me.y, dz = p.z - me.z;
@@ -229,6 +236,11 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(const WalkArgs a) {
     if (lane == 0) {
       if (overflow) atomicOr(a.status, kStatusStackOverflow);
       atomicAdd(a.inter, evaluated * (unsigned long long)nvalid);
+      if (a.counters) {
+        atomicAdd(a.counters + 0, visited);
+        atomicAdd(a.counters + 1, spills);
+        atomicAdd(a.counters + 2, 1ull);
+      }
     }
   }
 }
@@ -268,7 +280,7 @@ int walk_spill_slots(int) {
 void launch_walk(const WalkArgs& a, cudaStream_t s) {
   if (a.n <= 0) return;
   const bool soft = a.eps > 0.f;
-  const int groups = (a.n + 31) / 32;
+  const int groups = a.n;  // upper bound on the group count
   int grid = num_sms() * walk_blocks_per_sm(soft);
   grid = std::min(grid, (groups + kWalkWarps - 1) / kWalkWarps);
   if (grid < 1) grid = 1;

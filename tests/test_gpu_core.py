@@ -96,20 +96,22 @@ def test_force_accuracy_vs_direct_and_reference_walk(nb, cuda, port, n, theta):
     err = np.linalg.norm(a - d, axis=1) / np.linalg.norm(d, axis=1)
     # the headline tolerance: median relative force error <= 1e-3 vs FP64 direct sum
     assert np.median(err) <= 1e-3
-    # self-gravity alone (the star dominates the total by ~1e4)
+    # self-gravity alone (the star dominates the total by ~1e4, so an FP32
+    # total cannot resolve it): both walks again with star_mass = 0
+    p0 = to_gpu(nb, cuda, st)
+    t0 = build(nb, p0)
+    t0.force(p0, theta, eps, 0.0)
+    a0 = np.stack([host(p0, "ax"), host(p0, "ay"), host(p0, "az")], 1).astype(np.float64)
     sx, sy, sz = port.direct_f64(st["x"], st["y"], st["z"], st["m"], tg, eps, 1.0, False)
-    star = -np.stack([st["x"], st["y"], st["z"]], 1).astype(np.float64)
-    r2 = (star ** 2).sum(1) + eps * eps
-    star *= (1.0 / r2 ** 1.5)[:, None]
     s_ref = np.stack([sx, sy, sz], 1)
-    e_self = np.linalg.norm(a - star - s_ref, axis=1) / np.linalg.norm(s_ref, axis=1)
+    e_self = np.linalg.norm(a0 - s_ref, axis=1) / np.linalg.norm(s_ref, axis=1)
     # the reference walk (CPU restatement) on the same input, same theta
-    rx, ry, rz, info = port.forces(st["x"], st["y"], st["z"], st["m"], theta, eps, 1.0)
+    rx, ry, rz, info = port.forces(st["x"], st["y"], st["z"], st["m"], theta, eps, 0.0)
     r = np.stack([rx, ry, rz], 1).astype(np.float64)
-    e_ref_self = np.linalg.norm(r - star - s_ref, axis=1) / np.linalg.norm(s_ref, axis=1)
+    e_ref_self = np.linalg.norm(r - s_ref, axis=1) / np.linalg.norm(s_ref, axis=1)
     # the group walk opens at least what each body's own test would open
-    assert np.median(e_self) <= np.median(e_ref_self) * 1.05 + 1e-7
-    assert np.percentile(e_self, 99) <= np.percentile(e_ref_self, 99) * 1.05 + 1e-7
+    assert np.median(e_self) <= np.median(e_ref_self)
+    assert np.percentile(e_self, 99) <= np.percentile(e_ref_self, 99)
     assert t.stats().status == 0
 
 
@@ -124,7 +126,8 @@ def test_force_overwrites_and_zero_softening(nb, cuda, port):
     dx, dy, dz = port.direct_f64(st["x"], st["y"], st["z"], st["m"], np.arange(2000), 0.0, 1.0)
     d = np.stack([dx, dy, dz], 1)
     err = np.linalg.norm(a - d, axis=1) / np.linalg.norm(d, axis=1)
-    assert err.max() < 1e-5
+    # FP32 sum of 2000 unsoftened terms (close pairs cancel against the star)
+    assert err.max() < 5e-5
 
 
 # ---------------------------------------------------------- perturber kernel
