@@ -142,6 +142,9 @@ int nbody_tree_force(nbody_tree* t, nbody_particles* p, float theta, float softe
 int nbody_tree_collide(nbody_tree* t, nbody_particles* p, float r_coll, float restitution);
 /* Bodies opened directly instead of subdivided further (default 8). */
 int nbody_tree_set_leaf_max(nbody_tree* t, int leaf_max);
+/* Targets per lane of the force walk: 1 (warp groups of <= 32 bodies, the
+ * default) or 2 (<= 64); takes effect at the next summarize. */
+int nbody_tree_set_targets_per_lane(nbody_tree* t, int targets_per_lane);
 
 typedef struct nbody_tree_stats {
   int n_bodies;
@@ -246,6 +249,7 @@ typedef struct nbody_sim_params {
   float perturber_phase0;
   int state_precision;       /* NBODY_STATE_*                              */
   int leaf_max;              /* <= 0: default (8)                          */
+  int targets_per_lane;      /* walk: 1 (groups <= 32) or 2 (<= 64); 0: 1  */
 } nbody_sim_params;
 
 /* Parameters of src/main.cu:58-73 from a Config (r_coll = factor * radius). */

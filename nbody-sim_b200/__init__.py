@@ -114,7 +114,7 @@ class nbody_sim_params(C.Structure):
                 ("gas_drag_rate", C.c_float), ("perturber_enabled", C.c_int),
                 ("perturber_mass_mjup", C.c_float), ("perturber_radius_au", C.c_float),
                 ("perturber_phase0", C.c_float), ("state_precision", C.c_int),
-                ("leaf_max", C.c_int)]
+                ("leaf_max", C.c_int), ("targets_per_lane", C.c_int)]
 
 
 NBODY_PHASES = 6
@@ -155,6 +155,7 @@ SIGNATURES = [
                                    C.c_float]),
     ("nbody_tree_collide", C.c_int, [_VP, C.POINTER(nbody_particles), C.c_float, C.c_float]),
     ("nbody_tree_set_leaf_max", C.c_int, [_VP, C.c_int]),
+    ("nbody_tree_set_targets_per_lane", C.c_int, [_VP, C.c_int]),
     ("nbody_tree_stats_get", C.c_int, [_VP, C.POINTER(nbody_tree_stats)]),
     ("nbody_half_kick", C.c_int, [C.POINTER(nbody_particles), C.c_float]),
     ("nbody_drift", C.c_int, [C.POINTER(nbody_particles), C.c_float]),
@@ -314,13 +315,16 @@ class Octree:
     """OctreeData + its launchers (include/BHTree.cuh:38-50); each call
     synchronises before returning, as the reference launchers do."""
 
-    def __init__(self, n_bodies: int, leaf_max: int | None = None):
+    def __init__(self, n_bodies: int, leaf_max: int | None = None,
+                 targets_per_lane: int | None = None):
         h = _VP()
         _check(lib.nbody_tree_create(n_bodies, C.byref(h)))
         self.h = h
         self.n_bodies = n_bodies
         if leaf_max is not None:
             _check(lib.nbody_tree_set_leaf_max(self.h, leaf_max))
+        if targets_per_lane is not None:
+            _check(lib.nbody_tree_set_targets_per_lane(self.h, targets_per_lane))
 
     def close(self):
         if getattr(self, "h", None):
@@ -512,6 +516,7 @@ def sim_params(cfg: nbody_config | None = None, **kw) -> nbody_sim_params:
         lib.nbody_sim_params_from_config(C.byref(cfg), C.byref(p))
     else:
         p.dt, p.theta, p.softening, p.star_mass, p.leaf_max = 0.01, 0.5, 0.01, 1.0, 8
+        p.targets_per_lane = 1
     for k, v in kw.items():
         setattr(p, k, v)
     return p

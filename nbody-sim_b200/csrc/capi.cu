@@ -82,6 +82,7 @@ int nbody_tree_create(int n_bodies, nbody_tree** out) {
     try {
       t->n = n_bodies;
       nb::tree_alloc(t->tw, n_bodies);
+      t->tw.group_max = 32;
       t->sort_idx = nb::dalloc<int>(n_bodies, "sort_idx");
       nb::check(cudaMemset(t->sort_idx, 0, sizeof(int) * n_bodies), "sort_idx init");
       t->dvx = nb::dalloc<float>(n_bodies, "dvx");
@@ -129,6 +130,13 @@ int nbody_tree_set_leaf_max(nbody_tree* t, int leaf_max) {
   })
 }
 
+int nbody_tree_set_targets_per_lane(nbody_tree* t, int k) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(t && (k == 1 || k == 2), "nbody_tree_set_targets_per_lane: 1 or 2");
+    t->tw.group_max = 32 * k;
+  })
+}
+
 int nbody_tree_bbox(nbody_tree* t, const nbody_particles* p) {
   NBODY_API_BODY({
     NBODY_REQUIRE(t, "nbody_tree_bbox: null tree");
@@ -151,7 +159,6 @@ int nbody_tree_build(nbody_tree* t, const nbody_particles* p) {
                          t->n, 30, 0);
     nb::launch_gather_body4(t->tw, p->x, p->y, p->z, p->mass, t->n, 0);
     nb::launch_build_topology(t->tw, t->n, 0);
-    nb::launch_build_groups(t->tw, t->n, 32, 0);
     nb::finish("launchBuildKernel");
     t->have_bbox = false;
     t->built = true;
@@ -207,7 +214,7 @@ int nbody_tree_force(nbody_tree* t, nbody_particles* p, float theta, float softe
     w.ax = p->ax; w.ay = p->ay; w.az = p->az; w.scatter = t->tw.perm;
     w.spill = t->spill; w.spill_cap = t->spill_cap; w.inter = t->inter; w.work = t->work;
     w.counters = t->counters;
-    w.status = t->tw.status; w.group = 32;
+    w.status = t->tw.status; w.targets_per_lane = t->tw.group_max / 32;
     nb::launch_walk(w, 0);
     nb::finish("launchForceKernel");
     t->throw_status("launchForceKernel");
@@ -260,8 +267,11 @@ int nbody_tree_stats_get(nbody_tree* t, nbody_tree_stats* out) {
     nb::check(cudaMemcpy(&out->n_nodes, t->tw.n_nodes, sizeof(int), cudaMemcpyDeviceToHost),
               "n_nodes read");
     if (t->n >= 2) {
+      // total of the FP64 moment prefix sums (tile prefixes, last entry)
+      const int ntiles = t->n / nb::kMomentTile + 1;
       double4 s;
-      nb::check(cudaMemcpy(&s, t->tw.bin_sum, sizeof(double4), cudaMemcpyDeviceToHost), "root read");
+      nb::check(cudaMemcpy(&s, t->tw.mom_tiles + (ntiles + 1) + ntiles, sizeof(double4),
+                           cudaMemcpyDeviceToHost), "root read");
       out->root_mass = s.x;
       if (s.x > 0) {
         out->root_com[0] = s.y / s.x; out->root_com[1] = s.z / s.x; out->root_com[2] = s.w / s.x;
@@ -344,7 +354,6 @@ int nbody_fof(nbody_tree* t, const float* x, const float* y, const float* z, int
     nb::radix_sort_pairs(w.keys, w.perm, w.keys_alt, w.perm_alt, w.counts, n, 30, 0);
     nb::launch_gather_body4(w, x, y, z, nullptr, n, 0);
     nb::launch_build_topology(w, n, 0);
-    nb::launch_build_groups(w, n, 32, 0);
     nb::launch_build_moments(w, n, nullptr, nullptr, nullptr, 0);
     nb::NeighborArgs na{w.oct.info, w.oct.box_lo, w.oct.box_hi, w.body4, n,
                         w.groups, w.n_groups, t->leaf_max, t->spill, t->spill_cap, t->work, w.status};

@@ -4,17 +4,21 @@
 //   body4[s]      float4 (x, y, z, m) of the s-th body in key order (16 B)
 //   keys/perm     uint32 Morton key and source index per body
 //   binary tree   Karras radix tree over the sorted keys: left/right/parent,
-//                 [lo,hi] body range, prefix length (bits), FP64 mass moments
-//                 and a float AABB per internal node
+//                 [lo,hi] body range, prefix length (bits)
+//   moments       FP64 tile-local prefix sums of (m, m x, m y, m z)
 //   octree        compressed octree over the same keys; the children of a
 //                 node are contiguous: com4 (x,y,z,m float, from FP64 sums),
 //                 info int4 (first_child, body_lo, count<<4|nchild,
-//                 bits of half-size), box_lo/box_hi float4 (tight AABB)
+//                 bits of half-size), box_lo/box_hi float4 (the node's
+//                 cell cube, grown by a float-rounding margin)
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
 
 namespace nb {
+
+// Bodies per tile of the FP64 moment prefix sums.
+constexpr int kMomentTile = 2048;
 
 // Root cube and key quantisation, computed on the device from the bbox.
 struct TreeGeom {
@@ -44,13 +48,12 @@ struct TreeWork {
   int *bin_left = nullptr, *bin_right = nullptr, *bin_parent = nullptr;
   int *bin_lo = nullptr, *bin_hi = nullptr;
   uint8_t* bin_prefix = nullptr;
-  int* bin_visit = nullptr;
-  double4* bin_sum = nullptr;  // (m, m x, m y, m z)
-  float4 *bin_box_lo = nullptr, *bin_box_hi = nullptr;
+  // FP64 moments: tile-local prefix sums of (m, m x, m y, m z), tile prefixes
+  double4* mom_ploc = nullptr;
+  double4* mom_tiles = nullptr;
   // octree layout
   uint8_t* oct_nch = nullptr;
   uint32_t* oct_off = nullptr;
-  int* oct_final = nullptr;
   uint32_t* scan_tmp = nullptr;
   OctNodes oct;
   // device words
@@ -62,6 +65,7 @@ struct TreeWork {
   int2* groups = nullptr;
   uint32_t* group_flag = nullptr;
   int* n_groups = nullptr;
+  int group_max = 32;     // bodies per target group (32 x targets per lane)
 };
 
 void tree_alloc(TreeWork& w, int cap);
@@ -77,13 +81,13 @@ void launch_keys(TreeWork& w, const T* x, const T* y, const T* z, int n, cudaStr
 // body4[s] = (x,y,z,m)[perm[s]] for float inputs in caller order.
 void launch_gather_body4(TreeWork& w, const float* x, const float* y, const float* z,
                          const float* m, int n, cudaStream_t s);
-// Karras tree + FP64 bottom-up + compressed octree.  xd/yd/zd (optional,
-// key order) give FP64 positions for the moments; otherwise body4 is used.
+// Karras radix tree over the sorted keys.
 void launch_build_topology(TreeWork& w, int n, cudaStream_t s);
+// FP64 moments, compressed octree (contiguous children) and the target
+// groups.  xd/yd/zd (optional, key order) give FP64 positions for the
+// moments; otherwise body4 is used.
 void launch_build_moments(TreeWork& w, int n, const double* xd, const double* yd,
                           const double* zd, cudaStream_t s);
-// Target groups (needs the topology): w.groups, w.n_groups (device).
-void launch_build_groups(TreeWork& w, int n, int gmax, cudaStream_t s);
 
 size_t radix_sort_count_words(int n);
 void radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt,
@@ -115,7 +119,7 @@ struct WalkArgs {
   unsigned long long* counters;  // optional: nodes visited, stack spills, groups
   int* work;
   int* status;
-  int group;              // targets per warp group: 32 or 64
+  int targets_per_lane;   // 1 or 2: groups of up to 32 or 64 bodies
 };
 int walk_spill_slots(int device);  // warps resident at once (spill area slots)
 void launch_walk(const WalkArgs& a, cudaStream_t s);

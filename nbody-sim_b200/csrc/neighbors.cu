@@ -93,7 +93,10 @@ k_neighbors(const NeighborArgs a, float radius, CollideOut co, FofOut fo) {
     if (lane == 0) g = atomicAdd(a.work, 1);
     g = __shfl_sync(kFull, g, 0);
     if (g >= n_groups) break;
-    const int2 gr = a.groups[g];
+    const int2 grp = a.groups[g];
+    // groups hold up to 64 bodies; search them 32 (one per lane) at a time
+    for (int c0 = 0; c0 < grp.y; c0 += 32) {
+    const int2 gr = make_int2(grp.x + c0, min(32, grp.y - c0));
     const int s = gr.x + lane;
     const bool valid = lane < gr.y;
     const float4 me = a.body[valid ? s : gr.x];
@@ -220,6 +223,7 @@ k_neighbors(const NeighborArgs a, float radius, CollideOut co, FofOut fo) {
       co.dvz[s] = dvz;
     }
     if (lane == 0 && overflow) atomicOr(a.status, kStatusStackOverflow);
+    }  // chunks of the group
   }
 }
 

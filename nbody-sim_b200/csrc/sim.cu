@@ -370,6 +370,7 @@ struct SimImpl : SimBase {
     p = prm;
     n = nn;
     if (p.leaf_max <= 0) p.leaf_max = 8;
+    if (p.targets_per_lane != 2) p.targets_per_lane = 1;
     nbody_config c;
     nbody_config_defaults(&c);
     c.perturber_enabled = p.perturber_enabled;
@@ -379,6 +380,7 @@ struct SimImpl : SimBase {
     c.star_mass_msun = p.star_mass;
     nbody_perturber_make(&c, &pert);
     common_alloc();
+    tw.group_max = 32 * p.targets_per_lane;
     for (int b = 0; b < 2; ++b) {
       for (int k = 0; k < 6; ++k) s[b].v[k] = dalloc<R>(n, "state");
       s[b].m = dalloc<float>(n, "mass");
@@ -451,7 +453,6 @@ struct SimImpl : SimBase {
     cur = 1 - cur;
     mark(NBODY_PHASE_TREE);
     launch_build_topology(tw, n, st);
-    launch_build_groups(tw, n, 32, st);
     if (sizeof(R) == 8)
       launch_build_moments(tw, n, (const double*)s[cur].v[0], (const double*)s[cur].v[1],
                            (const double*)s[cur].v[2], st);
@@ -474,14 +475,14 @@ struct SimImpl : SimBase {
     w.leaf_max = p.leaf_max; w.pert = pp;
     w.ax = ax; w.ay = ay; w.az = az; w.scatter = nullptr;
     w.spill = spill; w.spill_cap = spill_cap; w.inter = inter; w.counters = counters;
-    w.work = work; w.status = tw.status; w.group = 32;
+    w.work = work; w.status = tw.status; w.targets_per_lane = tw.group_max / 32;
     mark(NBODY_PHASE_WALK);
     launch_walk(w, st);
     mark(NBODY_PHASE_COLLIDE);
     // keys, bbox reset, 20 sort kernels (4 x upsweep, 3 scan, scatter),
-    // permute, karras, 5 group kernels (mark, 3 scan, write), bottom-up,
-    // mark, 3 scan kernels, assign, write, walk
-    launches += 37;
+    // permute, karras, mark, 2 x 3 scan kernels, moment tiles, tile scan,
+    // emit, walk
+    launches += 35;
   }
 
   void collide() {
@@ -633,6 +634,7 @@ void nbody_sim_params_from_config(const nbody_config* cfg, nbody_sim_params* out
   out->perturber_phase0 = cfg->perturber_phase0;
   out->state_precision = NBODY_STATE_F32;
   out->leaf_max = 8;
+  out->targets_per_lane = 1;
 }
 
 int nbody_sim_create(const nbody_sim_params* p, int n, nbody_sim** out) {

@@ -137,7 +137,7 @@ __device__ __forceinline__ int delta(const uint32_t* __restrict__ keys, int n, i
 __global__ void __launch_bounds__(kThreads)
 k_karras(const uint32_t* __restrict__ keys, int n, int* __restrict__ left,
          int* __restrict__ right, int* __restrict__ parent, int* __restrict__ lo_out,
-         int* __restrict__ hi_out, uint8_t* __restrict__ prefix, int* __restrict__ visit) {
+         int* __restrict__ hi_out, uint8_t* __restrict__ prefix) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n - 1) return;
   const int d = (delta(keys, n, i, i + 1) - delta(keys, n, i, i - 1)) > 0 ? 1 : -1;
@@ -165,74 +165,110 @@ k_karras(const uint32_t* __restrict__ keys, int n, int* __restrict__ left,
   lo_out[i] = lo;
   hi_out[i] = hi;
   prefix[i] = (uint8_t)(dnode >= 32 ? 30 : dnode - 2);
-  visit[i] = 0;
   if (i == 0) parent[0] = -1;
 }
 
 // ------------------------------------------------------------- moments
-struct Moments {
-  double m, x, y, z;
-  float lx, ly, lz, hx, hy, hz;
-};
+// FP64 prefix sums of (m, m x, m y, m z) over the bodies in key order, kept
+// tile-local: ploc[k] sums the bodies of k's tile before k, tpre[t] sums the
+// tiles before t.  A node's moments over [lo, end) are then
+//   (ploc[end] - ploc[lo]) + (tpre[tile(end)] - tpre[tile(lo)]),
+// two differences of partial sums no larger than the node's own tiles, so
+// cancellation stays at the level of a tile (~1e-13 relative) rather than of
+// the whole disk.  Fixed tiling: the sums are the same on every run.
+constexpr int kTileM = kMomentTile;  // 256 threads x 8 bodies
+constexpr int kPerThr = kTileM / kThreads;
 
-__device__ __forceinline__ Moments leaf_moments(const float4* __restrict__ body4,
-                                                const double* xd, const double* yd,
-                                                const double* zd, int j) {
-  float4 b = body4[j];
-  Moments r;
-  double px = xd ? xd[j] : (double)b.x, py = yd ? yd[j] : (double)b.y,
-         pz = zd ? zd[j] : (double)b.z;
-  r.m = (double)b.w;
-  r.x = r.m * px; r.y = r.m * py; r.z = r.m * pz;
-  r.lx = r.hx = b.x; r.ly = r.hy = b.y; r.lz = r.hz = b.z;
-  return r;
+__device__ __forceinline__ double4 d4add(double4 a, double4 b) {
+  return make_double4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
+}
+__device__ __forceinline__ double4 d4sub(double4 a, double4 b) {
+  return make_double4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w);
+}
+__device__ __forceinline__ double4 d4shfl_up(double4 v, int o) {
+  return make_double4(__shfl_up_sync(kFull, v.x, o), __shfl_up_sync(kFull, v.y, o),
+                      __shfl_up_sync(kFull, v.z, o), __shfl_up_sync(kFull, v.w, o));
 }
 
-__device__ __forceinline__ Moments node_moments(const double4* sum, const float4* blo,
-                                                const float4* bhi, int i) {
-  const double2* s2 = reinterpret_cast<const double2*>(sum + i);
-  const double2 s0 = __ldcg(s2), s1 = __ldcg(s2 + 1);
-  float4 a = __ldcg(blo + i), b = __ldcg(bhi + i);
-  Moments r;
-  r.m = s0.x; r.x = s0.y; r.y = s1.x; r.z = s1.y;
-  r.lx = a.x; r.ly = a.y; r.lz = a.z; r.hx = b.x; r.hy = b.y; r.hz = b.z;
-  return r;
-}
-
-// One thread per leaf climbs while it is the second child to arrive; the
-// node is then the sum left + right (fixed order, so the FP64 sums do not
-// depend on arrival order).  No thread ever waits on another.
 __global__ void __launch_bounds__(kThreads)
-k_bottom_up(const float4* __restrict__ body4, const double* __restrict__ xd,
-            const double* __restrict__ yd, const double* __restrict__ zd, int n,
-            const int* __restrict__ left, const int* __restrict__ right,
-            const int* __restrict__ parent, int* __restrict__ visit, double4* __restrict__ sum,
-            float4* __restrict__ blo, float4* __restrict__ bhi, int* __restrict__ status) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= n || n < 2) return;
-  int p = parent[(n - 1) + j];
-  for (int guard = 0; p >= 0; ++guard) {
-    if (guard > 4096) { atomicOr(status, kStatusTreeLimit); return; }
-    __threadfence();
-    if (atomicAdd(&visit[p], 1) == 0) return;
-    __threadfence();
-    const int l = left[p], r = right[p];
-    Moments a = (l >= n - 1) ? leaf_moments(body4, xd, yd, zd, l - (n - 1))
-                             : node_moments(sum, blo, bhi, l);
-    Moments b = (r >= n - 1) ? leaf_moments(body4, xd, yd, zd, r - (n - 1))
-                             : node_moments(sum, blo, bhi, r);
-    double2* d2 = reinterpret_cast<double2*>(sum + p);
-    __stcg(d2, make_double2(a.m + b.m, a.x + b.x));
-    __stcg(d2 + 1, make_double2(a.y + b.y, a.z + b.z));
-    __stcg(blo + p, make_float4(fminf(a.lx, b.lx), fminf(a.ly, b.ly), fminf(a.lz, b.lz), 0.f));
-    __stcg(bhi + p, make_float4(fmaxf(a.hx, b.hx), fmaxf(a.hy, b.hy), fmaxf(a.hz, b.hz), 0.f));
-    p = parent[p];
+k_moment_tiles(const float4* __restrict__ body4, const double* __restrict__ xd,
+               const double* __restrict__ yd, const double* __restrict__ zd, int n,
+               double4* __restrict__ ploc, double4* __restrict__ tile_sum) {
+  __shared__ double4 s_w[kThreads / 32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const long long base = (long long)blockIdx.x * kTileM + (long long)tid * kPerThr;
+  double4 v[kPerThr];
+  double4 sum = make_double4(0, 0, 0, 0);
+#pragma unroll
+  for (int k = 0; k < kPerThr; ++k) {
+    const long long i = base + k;
+    v[k] = make_double4(0, 0, 0, 0);
+    if (i < n) {
+      const float4 b = body4[i];
+      const double m = (double)b.w;
+      const double px = xd ? xd[i] : (double)b.x, py = yd ? yd[i] : (double)b.y,
+                   pz = zd ? zd[i] : (double)b.z;
+      v[k] = make_double4(m, m * px, m * py, m * pz);
+    }
+    sum = d4add(sum, v[k]);
   }
+  double4 inc = sum;  // warp inclusive scan of the per-thread sums
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    double4 t = d4shfl_up(inc, o);
+    if (lane >= o) inc = d4add(inc, t);
+  }
+  if (lane == 31) s_w[warp] = inc;
+  __syncthreads();
+  double4 run = d4sub(inc, sum);
+  for (int w = 0; w < warp; ++w) run = d4add(run, s_w[w]);
+#pragma unroll
+  for (int k = 0; k < kPerThr; ++k) {
+    const long long i = base + k;
+    if (i <= n) ploc[i] = run;  // index n gets the tile's local prefix at n
+    run = d4add(run, v[k]);
+  }
+  if (tid == kThreads - 1) tile_sum[blockIdx.x] = run;
+}
+
+// Exclusive scan of the tile sums into tpre[0..ntiles] (one warp).
+__global__ void k_tile_scan(const double4* __restrict__ tile_sum, int ntiles,
+                            double4* __restrict__ tpre) {
+  const int lane = threadIdx.x;
+  const int per = (ntiles + 31) / 32;
+  const int lo = lane * per, hi = min(ntiles, lo + per);
+  double4 sum = make_double4(0, 0, 0, 0);
+  for (int t = lo; t < hi; ++t) sum = d4add(sum, tile_sum[t]);
+  double4 inc = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    double4 t = d4shfl_up(inc, o);
+    if (lane >= o) inc = d4add(inc, t);
+  }
+  double4 run = d4sub(inc, sum);
+  for (int t = lo; t < hi; ++t) {
+    tpre[t] = run;
+    run = d4add(run, tile_sum[t]);
+  }
+  if (lane == 31) tpre[ntiles] = inc;
+}
+
+__device__ __forceinline__ double4 range_moments(const double4* __restrict__ ploc,
+                                                 const double4* __restrict__ tpre, int lo,
+                                                 int end) {
+  double4 r = d4sub(ploc[end], ploc[lo]);
+  const int t0 = lo / kTileM, t1 = end / kTileM;
+  if (t0 != t1) r = d4add(r, d4sub(tpre[t1], tpre[t0]));
+  return r;
 }
 
 // ---------------------------------------------------------- octree layout
 __device__ __forceinline__ int bin_level(const uint8_t* prefix, int n, int b) {
   return (b >= n - 1) ? 10 : (int)prefix[b] / 3;
+}
+
+__device__ __forceinline__ int bin_count(const int* lo, const int* hi, int n, int b) {
+  return (b >= n - 1) ? 1 : hi[b] - lo[b] + 1;
 }
 
 // Visits the octree children of top node b (binary descendants that start a
@@ -258,131 +294,141 @@ __device__ __forceinline__ int for_each_oct_child(const int* __restrict__ left,
   return k;
 }
 
+// Per binary node: its octree child count (tops only) and whether it is a
+// target group -- a maximal node with <= gmax bodies.  Groups partition the
+// bodies into contiguous key ranges whose bodies share a Morton prefix, so a
+// group never straddles a jump of the space-filling curve (a fixed run of 32
+// consecutive bodies can: its box then spans most of the domain and its walk
+// degenerates to O(N) work on one warp).
 __global__ void __launch_bounds__(kThreads)
-k_oct_mark(int n, const int* __restrict__ left, const int* __restrict__ right,
-           const int* __restrict__ parent, const uint8_t* __restrict__ prefix,
-           uint8_t* __restrict__ nch, uint32_t* __restrict__ off, int* __restrict__ fin) {
+k_mark(int n, int gmax, const int* __restrict__ left, const int* __restrict__ right,
+       const int* __restrict__ parent, const int* __restrict__ lo, const int* __restrict__ hi,
+       const uint8_t* __restrict__ prefix, uint8_t* __restrict__ nch, uint32_t* __restrict__ off,
+       uint32_t* __restrict__ gflag) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   const int nb = 2 * n - 1;
   if (b >= nb) return;
   const int lb = bin_level(prefix, n, b);
-  const bool top = (b == 0) || lb > bin_level(prefix, n, parent[b]);
+  const int p = (b == 0) ? -1 : parent[b];
+  const bool top = (b == 0) || lb > bin_level(prefix, n, p);
   int cnt = 0;
   if (top && b < n - 1 && lb < 10)
     cnt = for_each_oct_child(left, right, prefix, n, b, lb, [](int, int) {});
   nch[b] = (uint8_t)cnt;
   off[b] = (uint32_t)cnt;
-  fin[b] = top ? 0 : -1;
+  const int c = bin_count(lo, hi, n, b);
+  const int pc = (p < 0) ? 0x7fffffff : bin_count(lo, hi, n, p);
+  gflag[b] = (c <= gmax && pc > gmax) ? 1u : 0u;
 }
 
-__global__ void __launch_bounds__(kThreads)
-k_oct_assign(int n, const int* __restrict__ left, const int* __restrict__ right,
-             const uint8_t* __restrict__ prefix, const uint8_t* __restrict__ nch,
-             const uint32_t* __restrict__ off, int* __restrict__ fin, int* __restrict__ n_nodes) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  const int nb = 2 * n - 1;
-  if (b >= nb) return;
-  if (b == nb - 1) *n_nodes = 1 + (int)(off[b] + nch[b]);
-  if (nch[b] == 0) return;
-  const int lb = bin_level(prefix, n, b);
-  const int base = 1 + (int)off[b];
-  for_each_oct_child(left, right, prefix, n, b, lb, [&](int c, int k) { fin[c] = base + k; });
+__device__ __forceinline__ uint32_t compact3(uint32_t v) {
+  v &= 0x09249249u;
+  v = (v ^ (v >> 2)) & 0x030c30c3u;
+  v = (v ^ (v >> 4)) & 0x0300f00fu;
+  v = (v ^ (v >> 8)) & 0x030000ffu;
+  v = (v ^ (v >> 16)) & 0x000003ffu;
+  return v;
 }
 
-__global__ void __launch_bounds__(kThreads)
-k_oct_write(int n, const int* __restrict__ lo, const int* __restrict__ hi,
-            const uint8_t* __restrict__ prefix, const uint8_t* __restrict__ nch,
-            const uint32_t* __restrict__ off, const int* __restrict__ fin,
-            const double4* __restrict__ sum, const float4* __restrict__ blo,
-            const float4* __restrict__ bhi, const float4* __restrict__ body4,
-            const TreeGeom* __restrict__ geom, OctNodes oct) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  const int nb = 2 * n - 1;
-  if (b >= nb) return;
-  const int f = (b == 0) ? 0 : fin[b];
-  if (f < 0) return;
-  const float rhs = geom->rhs;
-  if (b >= n - 1) {  // single-body leaf
-    const int j = b - (n - 1);
-    float4 p = body4[j];
-    oct.com[f] = p;
-    oct.info[f] = make_int4(-1, j, (1 << 4), __float_as_int(ldexpf(rhs, -10)));
-    oct.box_lo[f] = make_float4(p.x, p.y, p.z, 0.f);
-    oct.box_hi[f] = make_float4(p.x, p.y, p.z, 0.f);
+struct EmitArgs {
+  int n, gmax;
+  const int *left, *right, *parent, *lo, *hi;
+  const uint8_t* prefix;
+  const uint32_t* keys;
+  const uint8_t* nch;
+  const uint32_t* off;
+  const uint32_t* goff;
+  const float4* body4;
+  const double4* ploc;
+  const double4* tpre;
+  const TreeGeom* geom;
+  OctNodes oct;
+  int2* groups;
+  int* n_nodes;
+  int* n_groups;
+};
+
+// Writes the octree record of binary node c into slot f.
+__device__ void write_node(const EmitArgs& a, int c, int f) {
+  const float rhs = a.geom->rhs;
+  if (c >= a.n - 1) {  // single-body leaf
+    const int j = c - (a.n - 1);
+    const float4 p = a.body4[j];
+    a.oct.com[f] = p;
+    a.oct.info[f] = make_int4(-1, j, (1 << 4), __float_as_int(ldexpf(rhs, -10)));
+    a.oct.box_lo[f] = make_float4(p.x, p.y, p.z, 0.f);
+    a.oct.box_hi[f] = make_float4(p.x, p.y, p.z, 0.f);
     return;
   }
-  const int L = (int)prefix[b] / 3;
-  const double4 s = sum[b];
-  float4 lo4 = blo[b], hi4 = bhi[b];
-  float4 c;
-  if (s.x > 0.0) {
-    c = make_float4((float)(s.y / s.x), (float)(s.z / s.x), (float)(s.w / s.x), (float)s.x);
-  } else {
-    c = make_float4(0.5f * (lo4.x + hi4.x), 0.5f * (lo4.y + hi4.y), 0.5f * (lo4.z + hi4.z), 0.f);
+  const int L = (int)a.prefix[c] / 3;
+  const int lo = a.lo[c], hi = a.hi[c];
+  const double4 s = range_moments(a.ploc, a.tpre, lo, hi + 1);
+  // the node's cube: level L cell of its key prefix
+  const uint32_t kl = a.keys[lo] >> (3 * (10 - L));
+  const uint32_t cc[3] = {compact3(kl), compact3(kl >> 1), compact3(kl >> 2)};
+  const double side = ldexp(2.0 * (double)rhs, -L);
+  float blo[3], bhi[3];
+  double ctr[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const double l0 = a.geom->lo[k] + (double)cc[k] * side, h0 = l0 + side;
+    // float positions may sit an ulp outside their FP64-quantised cell
+    const double margin = 1e-6 * (fabs(l0) + fabs(h0) + side) + 1e-30;
+    blo[k] = __double2float_rd(l0 - margin);
+    bhi[k] = __double2float_ru(h0 + margin);
+    ctr[k] = 0.5 * (l0 + h0);
   }
-  const int k = nch[b];
-  const int count = hi[b] - lo[b] + 1;
-  oct.com[f] = c;
-  oct.info[f] = make_int4(k > 0 ? 1 + (int)off[b] : -1, lo[b], (count << 4) | k,
-                          __float_as_int(ldexpf(rhs, -L)));
-  oct.box_lo[f] = lo4;
-  oct.box_hi[f] = hi4;
+  float4 com;
+  if (s.x > 0.0)
+    com = make_float4((float)(s.y / s.x), (float)(s.z / s.x), (float)(s.w / s.x), (float)s.x);
+  else
+    com = make_float4((float)ctr[0], (float)ctr[1], (float)ctr[2], 0.f);
+  const int k = a.nch[c];
+  a.oct.com[f] = com;
+  a.oct.info[f] = make_int4(k > 0 ? 1 + (int)a.off[c] : -1, lo, ((hi - lo + 1) << 4) | k,
+                            __float_as_int(ldexpf(rhs, -L)));
+  a.oct.box_lo[f] = make_float4(blo[0], blo[1], blo[2], 0.f);
+  a.oct.box_hi[f] = make_float4(bhi[0], bhi[1], bhi[2], 0.f);
 }
 
-// Target groups for the warp walks: the maximal nodes of the binary radix
-// tree holding <= gmax bodies.  They partition the bodies into contiguous
-// key ranges whose bodies share a Morton prefix, so a group never straddles
-// a jump of the space-filling curve (a fixed run of 32 consecutive bodies
-// can: its box then spans most of the domain and its walk degenerates to
-// O(N) work on one warp).
-__global__ void __launch_bounds__(kThreads)
-k_group_mark(int n, int gmax, const int* __restrict__ lo, const int* __restrict__ hi,
-             const int* __restrict__ parent, uint32_t* __restrict__ flag) {
+// Every top node writes the records of its octree children into its block
+// of contiguous slots (1 + off[b] ...); node 0 also writes the root.  Target
+// groups are written at their scanned offsets.
+__global__ void __launch_bounds__(kThreads) k_emit(const EmitArgs a) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  const int nb = 2 * n - 1;
+  const int nb = 2 * a.n - 1;
   if (b >= nb) return;
-  const int cnt = (b >= n - 1) ? 1 : hi[b] - lo[b] + 1;
-  int pc = 0x7fffffff;
-  if (b != 0) {
-    const int p = parent[b];
-    pc = hi[p] - lo[p] + 1;
+  if (b == 0) write_node(a, 0, 0);
+  const int k = a.nch[b];
+  if (k > 0) {
+    const int base = 1 + (int)a.off[b];
+    const int lb = (int)a.prefix[b] / 3;
+    for_each_oct_child(a.left, a.right, a.prefix, a.n, b, lb,
+                       [&](int c, int i) { write_node(a, c, base + i); });
   }
-  flag[b] = (cnt <= gmax && pc > gmax) ? 1u : 0u;
-}
-
-__global__ void __launch_bounds__(kThreads)
-k_group_write(int n, int gmax, const int* __restrict__ lo, const int* __restrict__ hi,
-              const int* __restrict__ parent, const uint32_t* __restrict__ off,
-              int2* __restrict__ groups, int* __restrict__ n_groups) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  const int nb = 2 * n - 1;
-  if (b >= nb) return;
-  const bool leaf = b >= n - 1;
-  const int cnt = leaf ? 1 : hi[b] - lo[b] + 1;
-  int pc = 0x7fffffff;
-  if (b != 0) {
-    const int p = parent[b];
-    pc = hi[p] - lo[p] + 1;
+  const int c = bin_count(a.lo, a.hi, a.n, b);
+  const int p = (b == 0) ? -1 : a.parent[b];
+  const int pc = (p < 0) ? 0x7fffffff : bin_count(a.lo, a.hi, a.n, p);
+  const bool g = c <= a.gmax && pc > a.gmax;
+  if (g) a.groups[a.goff[b]] = make_int2(b >= a.n - 1 ? b - (a.n - 1) : a.lo[b], c);
+  if (b == nb - 1) {
+    *a.n_nodes = 1 + (int)(a.off[b] + (uint32_t)k);
+    *a.n_groups = (int)a.goff[b] + (g ? 1 : 0);
   }
-  const bool is_group = cnt <= gmax && pc > gmax;
-  if (is_group) groups[off[b]] = make_int2(leaf ? b - (n - 1) : lo[b], cnt);
-  if (b == nb - 1) *n_groups = (int)off[b] + (is_group ? 1 : 0);
 }
 
-__global__ void k_group_single(int2* groups, int* n_groups) {
-  groups[0] = make_int2(0, 1);
-  *n_groups = 1;
-}
-
-// N == 1: the root is the single body.
-__global__ void k_oct_single(const float4* __restrict__ body4, const TreeGeom* __restrict__ geom,
-                             OctNodes oct, int* __restrict__ n_nodes) {
+// N == 1: the root is the single body and the only group.
+__global__ void k_single(const float4* __restrict__ body4, const TreeGeom* __restrict__ geom,
+                         OctNodes oct, int* __restrict__ n_nodes, int2* __restrict__ groups,
+                         int* __restrict__ n_groups) {
   float4 p = body4[0];
   oct.com[0] = p;
   oct.info[0] = make_int4(-1, 0, (1 << 4), __float_as_int(geom->rhs));
   oct.box_lo[0] = make_float4(p.x, p.y, p.z, 0.f);
   oct.box_hi[0] = make_float4(p.x, p.y, p.z, 0.f);
   *n_nodes = 1;
+  groups[0] = make_int2(0, 1);
+  *n_groups = 1;
 }
 
 template <typename T>
@@ -413,13 +459,10 @@ void tree_alloc(TreeWork& w, int cap) {
   w.bin_lo = dalloc<int>(n, "bin_lo");
   w.bin_hi = dalloc<int>(n, "bin_hi");
   w.bin_prefix = dalloc<uint8_t>(n, "bin_prefix");
-  w.bin_visit = dalloc<int>(n, "bin_visit");
-  w.bin_sum = dalloc<double4>(n, "bin_sum");
-  w.bin_box_lo = dalloc<float4>(n, "bin_box_lo");
-  w.bin_box_hi = dalloc<float4>(n, "bin_box_hi");
+  w.mom_ploc = dalloc<double4>(n + 1, "moment prefix");
+  w.mom_tiles = dalloc<double4>(2 * ((n + 1) / kTileM + 2), "moment tiles");
   w.oct_nch = dalloc<uint8_t>(nb, "oct_nch");
   w.oct_off = dalloc<uint32_t>(nb, "oct_off");
-  w.oct_final = dalloc<int>(nb, "oct_final");
   w.scan_tmp = dalloc<uint32_t>(scan_tmp_words((int)nb), "scan_tmp");
   w.oct.com = dalloc<float4>(nb, "oct com");
   w.oct.info = dalloc<int4>(nb, "oct info");
@@ -438,9 +481,8 @@ void tree_alloc(TreeWork& w, int cap) {
 
 void tree_free(TreeWork& w) {
   void* ptrs[] = {w.keys, w.perm, w.keys_alt, w.perm_alt, w.counts, w.body4, w.bin_left,
-                  w.bin_right, w.bin_parent, w.bin_lo, w.bin_hi, w.bin_prefix, w.bin_visit,
-                  w.bin_sum, w.bin_box_lo, w.bin_box_hi, w.oct_nch, w.oct_off, w.oct_final,
-                  w.scan_tmp, w.oct.com, w.oct.info, w.oct.box_lo, w.oct.box_hi, w.bbox_enc,
+                  w.bin_right, w.bin_parent, w.bin_lo, w.bin_hi, w.bin_prefix, w.mom_ploc,
+                  w.mom_tiles, w.oct_nch, w.oct_off, w.scan_tmp, w.oct.com, w.oct.info, w.oct.box_lo, w.oct.box_hi, w.bbox_enc,
                   w.geom, w.n_nodes, w.status, w.groups, w.group_flag, w.n_groups};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -488,47 +530,34 @@ void launch_gather_body4(TreeWork& w, const float* x, const float* y, const floa
 void launch_build_topology(TreeWork& w, int n, cudaStream_t s) {
   if (n < 2) return;
   k_karras<<<grid_for(n - 1), kThreads, 0, s>>>(w.keys, n, w.bin_left, w.bin_right,
-                                                w.bin_parent, w.bin_lo, w.bin_hi, w.bin_prefix,
-                                                w.bin_visit);
+                                                w.bin_parent, w.bin_lo, w.bin_hi, w.bin_prefix);
   check(cudaGetLastError(), "k_karras launch");
-}
-
-void launch_build_groups(TreeWork& w, int n, int gmax, cudaStream_t s) {
-  if (n < 1) return;
-  if (n == 1) {
-    k_group_single<<<1, 1, 0, s>>>(w.groups, w.n_groups);
-    check(cudaGetLastError(), "k_group_single launch");
-    return;
-  }
-  const int nb = 2 * n - 1;
-  k_group_mark<<<grid_for(nb), kThreads, 0, s>>>(n, gmax, w.bin_lo, w.bin_hi, w.bin_parent,
-                                                 w.group_flag);
-  scan_exclusive_u32(w.group_flag, nb, w.scan_tmp, s);
-  k_group_write<<<grid_for(nb), kThreads, 0, s>>>(n, gmax, w.bin_lo, w.bin_hi, w.bin_parent,
-                                                  w.group_flag, w.groups, w.n_groups);
-  check(cudaGetLastError(), "group launch");
 }
 
 void launch_build_moments(TreeWork& w, int n, const double* xd, const double* yd,
                           const double* zd, cudaStream_t s) {
   if (n < 1) return;
   if (n == 1) {
-    k_oct_single<<<1, 1, 0, s>>>(w.body4, w.geom, w.oct, w.n_nodes);
-    check(cudaGetLastError(), "k_oct_single launch");
+    k_single<<<1, 1, 0, s>>>(w.body4, w.geom, w.oct, w.n_nodes, w.groups, w.n_groups);
+    check(cudaGetLastError(), "k_single launch");
     return;
   }
   const int nb = 2 * n - 1;
-  k_bottom_up<<<grid_for(n), kThreads, 0, s>>>(w.body4, xd, yd, zd, n, w.bin_left, w.bin_right,
-                                               w.bin_parent, w.bin_visit, w.bin_sum,
-                                               w.bin_box_lo, w.bin_box_hi, w.status);
-  k_oct_mark<<<grid_for(nb), kThreads, 0, s>>>(n, w.bin_left, w.bin_right, w.bin_parent,
-                                               w.bin_prefix, w.oct_nch, w.oct_off, w.oct_final);
+  const int kGroupMax = w.group_max;
+  k_mark<<<grid_for(nb), kThreads, 0, s>>>(n, kGroupMax, w.bin_left, w.bin_right, w.bin_parent,
+                                           w.bin_lo, w.bin_hi, w.bin_prefix, w.oct_nch,
+                                           w.oct_off, w.group_flag);
   scan_exclusive_u32(w.oct_off, nb, w.scan_tmp, s);
-  k_oct_assign<<<grid_for(nb), kThreads, 0, s>>>(n, w.bin_left, w.bin_right, w.bin_prefix,
-                                                 w.oct_nch, w.oct_off, w.oct_final, w.n_nodes);
-  k_oct_write<<<grid_for(nb), kThreads, 0, s>>>(n, w.bin_lo, w.bin_hi, w.bin_prefix, w.oct_nch,
-                                                w.oct_off, w.oct_final, w.bin_sum, w.bin_box_lo,
-                                                w.bin_box_hi, w.body4, w.geom, w.oct);
+  scan_exclusive_u32(w.group_flag, nb, w.scan_tmp, s);
+  const int ntiles = n / kTileM + 1;
+  double4* tile_sum = w.mom_tiles;
+  double4* tpre = w.mom_tiles + (ntiles + 1);
+  k_moment_tiles<<<ntiles, kThreads, 0, s>>>(w.body4, xd, yd, zd, n, w.mom_ploc, tile_sum);
+  k_tile_scan<<<1, 32, 0, s>>>(tile_sum, ntiles, tpre);
+  EmitArgs a{n, kGroupMax, w.bin_left, w.bin_right, w.bin_parent, w.bin_lo, w.bin_hi,
+             w.bin_prefix, w.keys, w.oct_nch, w.oct_off, w.group_flag, w.body4, w.mom_ploc,
+             tpre, w.geom, w.oct, w.groups, w.n_nodes, w.n_groups};
+  k_emit<<<grid_for(nb), kThreads, 0, s>>>(a);
   check(cudaGetLastError(), "octree launch");
 }
 

@@ -39,23 +39,37 @@ struct WarpSmem {
 };
 
 template <bool kSoft>
-__device__ __forceinline__ void interact(const float4 s, float px, float py, float pz,
-                                         float eps2, float& ax, float& ay, float& az) {
-  float dx = s.x - px, dy = s.y - py, dz = s.z - pz;
+__device__ __forceinline__ void interact(const float4 s, const float4 p, float eps2,
+                                         float3& acc) {
+  float dx = s.x - p.x, dy = s.y - p.y, dz = s.z - p.z;
   float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
   float inv = rsqrtf(r2);
   if (!kSoft) inv = (r2 > 0.f) ? inv : 0.f;
   float f = s.w * (inv * inv * inv);
-  ax = fmaf(f, dx, ax);
-  ay = fmaf(f, dy, ay);
-  az = fmaf(f, dz, az);
+  acc.x = fmaf(f, dx, acc.x);
+  acc.y = fmaf(f, dy, acc.y);
+  acc.z = fmaf(f, dz, acc.z);
 }
 
-template <bool kSoft>
-__device__ __forceinline__ void eval32(const float4* lst, float px, float py, float pz,
-                                       float eps2, float& ax, float& ay, float& az) {
+// All lanes evaluate sources lst[0..cnt) for their kT targets; every source
+// is one shared-memory broadcast that feeds kT interaction chains.
+template <bool kSoft, int kT, int kCount>
+__device__ __forceinline__ void eval_list(const float4* lst, int cnt, const float4 (&me)[kT],
+                                          float eps2, float3 (&acc)[kT]) {
+  if (kCount > 0) {
 #pragma unroll
-  for (int j = 0; j < 32; ++j) interact<kSoft>(lst[j], px, py, pz, eps2, ax, ay, az);
+    for (int j = 0; j < kCount; ++j) {
+      const float4 src = lst[j];
+#pragma unroll
+      for (int t = 0; t < kT; ++t) interact<kSoft>(src, me[t], eps2, acc[t]);
+    }
+  } else {
+    for (int j = 0; j < cnt; ++j) {
+      const float4 src = lst[j];
+#pragma unroll
+      for (int t = 0; t < kT; ++t) interact<kSoft>(src, me[t], eps2, acc[t]);
+    }
+  }
 }
 
 // Drops the first 32 entries of the list (caller guarantees nlist >= 32).
@@ -68,7 +82,8 @@ __device__ __forceinline__ void list_shift(float4* lst, int nlist, int lane) {
   __syncwarp();
 }
 
-template <bool kSoft>
+// kT targets per lane: a group of up to 32 kT bodies per warp.
+template <bool kSoft, int kT>
 __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(const WalkArgs a) {
   __shared__ WarpSmem smem[kWalkWarps];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -83,21 +98,30 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(const WalkArgs a) {
     g = __shfl_sync(kFull, g, 0);
     if (g >= n_groups) break;
     const int2 gr = a.groups[g];
-    const int s = gr.x + lane;
-    const bool valid = lane < gr.y;
-    const float4 me = a.body[valid ? s : gr.x];
-    const float gx0 = warp_min(me.x), gx1 = warp_max(me.x);
-    const float gy0 = warp_min(me.y), gy1 = warp_max(me.y);
-    const float gz0 = warp_min(me.z), gz1 = warp_max(me.z);
+    float4 me[kT];
+    bool valid[kT];
+    float gx0 = INFINITY, gx1 = -INFINITY, gy0 = INFINITY, gy1 = -INFINITY, gz0 = INFINITY,
+          gz1 = -INFINITY;
+#pragma unroll
+    for (int t = 0; t < kT; ++t) {
+      valid[t] = lane + 32 * t < gr.y;
+      me[t] = a.body[valid[t] ? gr.x + lane + 32 * t : gr.x];
+      gx0 = fminf(gx0, me[t].x); gx1 = fmaxf(gx1, me[t].x);
+      gy0 = fminf(gy0, me[t].y); gy1 = fmaxf(gy1, me[t].y);
+      gz0 = fminf(gz0, me[t].z); gz1 = fmaxf(gz1, me[t].z);
+    }
+    gx0 = warp_min(gx0); gx1 = warp_max(gx1);
+    gy0 = warp_min(gy0); gy1 = warp_max(gy1);
+    gz0 = warp_min(gz0); gz1 = warp_max(gz1);
 
     // The tree sum starts from zero: adding ~10^3 terms into an accumulator
     // that already holds the star pull (10^3-10^5 times larger) would round
     // every term at the star's ulp.  Star and perturber are added at the end.
-    float ax = 0.f, ay = 0.f, az = 0.f;
-    unsigned long long visited = 0, spills = 0;
-
+    float3 acc[kT];
+#pragma unroll
+    for (int t = 0; t < kT; ++t) acc[t] = make_float3(0.f, 0.f, 0.f);
+    unsigned long long visited = 0, spills = 0, evaluated = 0;
     int top = 1, spilled = 0, nlist = 0;
-    unsigned long long evaluated = 0;
     bool overflow = false;
     if (lane == 0) w.stk[0] = 0;
     __syncwarp();
@@ -152,7 +176,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(const WalkArgs a) {
       nlist += __popc(m1);
       __syncwarp();
       if (nlist >= 32) {
-        eval32<kSoft>(w.lst, me.x, me.y, me.z, eps2, ax, ay, az);
+        eval_list<kSoft, kT, 32>(w.lst, 32, me, eps2, acc);
         evaluated += 32;
         list_shift(w.lst, nlist, lane);
         nlist -= 32;
@@ -198,7 +222,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(const WalkArgs a) {
           nlist += min(32, btotal - base);
           __syncwarp();
           if (nlist >= 32) {
-            eval32<kSoft>(w.lst, me.x, me.y, me.z, eps2, ax, ay, az);
+            eval_list<kSoft, kT, 32>(w.lst, 32, me, eps2, acc);
             evaluated += 32;
             list_shift(w.lst, nlist, lane);
             nlist -= 32;
@@ -207,35 +231,39 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(const WalkArgs a) {
       }
     }
 
-    for (int j = 0; j < nlist; ++j) interact<kSoft>(w.lst[j], me.x, me.y, me.z, eps2, ax, ay, az);
+    eval_list<kSoft, kT, 0>(w.lst, nlist, me, eps2, acc);
     evaluated += nlist;
     __syncwarp();
 
-    if (a.star_in_walk) {  // softened star term, BHTree.cu:547-553
-      float dx = -me.x, dy = -me.y, dz = -me.z;
-      float r2 = dx * dx + dy * dy + dz * dz + a.eps * a.eps;
-      float r = sqrtf(r2);
-      float f = a.star_mass / (r2 * r);
-      ax += f * dx; ay += f * dy; az += f * dz;
+    const float4 p = a.pert ? *a.pert : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int t = 0; t < kT; ++t) {
+      float ax = acc[t].x, ay = acc[t].y, az = acc[t].z;
+      if (a.star_in_walk) {  // softened star term, BHTree.cu:547-553
+        float dx = -me[t].x, dy = -me[t].y, dz = -me[t].z;
+        float r2 = dx * dx + dy * dy + dz * dz + a.eps * a.eps;
+        float r = sqrtf(r2);
+        float f = a.star_mass / (r2 * r);
+        ax += f * dx; ay += f * dy; az += f * dz;
+      }
+      if (a.pert) {  // perturber_forceKernel, Perturber.cu:20-34 (adds)
+        float dx = p.x - me[t].x, dy = p.y - me[t].y, dz = p.z - me[t].z;
+        float r2 = dx * dx + dy * dy + dz * dz + a.eps * a.eps;
+        float r = sqrtf(r2);
+        float f = p.w / (r2 * r);
+        ax += f * dx; ay += f * dy; az += f * dz;
+      }
+      if (valid[t]) {
+        const int s = gr.x + lane + 32 * t;
+        const uint32_t o = a.scatter ? a.scatter[s] : (uint32_t)s;
+        a.ax[o] = ax;
+        a.ay[o] = ay;
+        a.az[o] = az;
+      }
     }
-    if (a.pert) {  // perturber_forceKernel, Perturber.cu:20-34 (adds)
-      const float4 p = *a.pert;
-      float dx = p.x - me.x, dy = p.y - me.y, dz = p.z - me.z;
-      float r2 = dx * dx + dy * dy + dz * dz + a.eps * a.eps;
-      float r = sqrtf(r2);
-      float f = p.w / (r2 * r);
-      ax += f * dx; ay += f * dy; az += f * dz;
-    }
-    if (valid) {
-      const uint32_t o = a.scatter ? a.scatter[s] : (uint32_t)s;
-      a.ax[o] = ax;
-      a.ay[o] = ay;
-      a.az[o] = az;
-    }
-    const int nvalid = __popc(__ballot_sync(kFull, valid));
     if (lane == 0) {
       if (overflow) atomicOr(a.status, kStatusStackOverflow);
-      atomicAdd(a.inter, evaluated * (unsigned long long)nvalid);
+      atomicAdd(a.inter, evaluated * (unsigned long long)gr.y);
       if (a.counters) {
         atomicAdd(a.counters + 0, visited);
         atomicAdd(a.counters + 1, spills);
@@ -245,17 +273,12 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(const WalkArgs a) {
   }
 }
 
-int g_walk_blocks_per_sm[2] = {0, 0};
-
-int walk_blocks_per_sm(bool soft) {
-  int& b = g_walk_blocks_per_sm[soft ? 1 : 0];
+template <bool kSoft, int kT>
+int walk_blocks_per_sm() {
+  static int b = 0;
   if (b == 0) {
-    if (soft)
-      check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<true>, kWalkWarps * 32, 0),
-            "walk occupancy");
-    else
-      check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<false>, kWalkWarps * 32, 0),
-            "walk occupancy");
+    check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<kSoft, kT>, kWalkWarps * 32, 0),
+          "walk occupancy");
     if (b < 1) b = 1;
   }
   return b;
@@ -271,24 +294,33 @@ int num_sms() {
   return sms;
 }
 
+template <bool kSoft, int kT>
+void launch_variant(const WalkArgs& a, cudaStream_t s) {
+  int grid = num_sms() * walk_blocks_per_sm<kSoft, kT>();
+  grid = std::min(grid, (a.n + kWalkWarps - 1) / kWalkWarps);  // groups <= n
+  if (grid < 1) grid = 1;
+  k_walk<kSoft, kT><<<grid, kWalkWarps * 32, 0, s>>>(a);
+}
+
 }  // namespace
 
 int walk_spill_slots(int) {
-  return num_sms() * std::max(walk_blocks_per_sm(true), walk_blocks_per_sm(false)) * kWalkWarps;
+  const int b = std::max(std::max(walk_blocks_per_sm<true, 1>(), walk_blocks_per_sm<false, 1>()),
+                         std::max(walk_blocks_per_sm<true, 2>(), walk_blocks_per_sm<false, 2>()));
+  return num_sms() * b * kWalkWarps;
 }
 
 void launch_walk(const WalkArgs& a, cudaStream_t s) {
   if (a.n <= 0) return;
-  const bool soft = a.eps > 0.f;
-  const int groups = a.n;  // upper bound on the group count
-  int grid = num_sms() * walk_blocks_per_sm(soft);
-  grid = std::min(grid, (groups + kWalkWarps - 1) / kWalkWarps);
-  if (grid < 1) grid = 1;
   check(cudaMemsetAsync(a.work, 0, sizeof(int), s), "walk work reset");
-  if (soft)
-    k_walk<true><<<grid, kWalkWarps * 32, 0, s>>>(a);
-  else
-    k_walk<false><<<grid, kWalkWarps * 32, 0, s>>>(a);
+  const bool soft = a.eps > 0.f;
+  if (a.targets_per_lane == 2) {
+    if (soft) launch_variant<true, 2>(a, s);
+    else launch_variant<false, 2>(a, s);
+  } else {
+    if (soft) launch_variant<true, 1>(a, s);
+    else launch_variant<false, 1>(a, s);
+  }
   check(cudaGetLastError(), "k_walk launch");
 }
 

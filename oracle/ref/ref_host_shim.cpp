@@ -67,6 +67,23 @@ int ref_load_config(const char* path, float* f, int* i, char* out_dir, int dir_l
     }
 }
 
+// initDisk (src/disk/DiskInit.cpp:18-69) into caller arrays (n = cfg size).
+int ref_init_disk(int n, unsigned seed, float* x, float* y, float* z, float* vx, float* vy,
+                  float* vz) {
+  try {
+    Config c;
+    c.n_particles = n;
+    ParticleData p = initDisk(c, seed);
+    size_t b = (size_t)n * sizeof(float);
+    std::memcpy(x, p.x, b); std::memcpy(y, p.y, b); std::memcpy(z, p.z, b);
+    std::memcpy(vx, p.vx, b); std::memcpy(vy, p.vy, b); std::memcpy(vz, p.vz, b);
+    freeParticlesCPU(p);
+    return 0;
+  } catch (...) {
+    return 1;
+  }
+}
+
 float ref_particle_radius(float particle_mass_msun) {
     Config c;
     c.particle_mass_msun = particle_mass_msun;

@@ -33,8 +33,8 @@ def host(p, k):
     return p.arrays[k].cpu().numpy()
 
 
-def build(nb, p, leaf_max=None):
-    t = nb.Octree(p.n, leaf_max)
+def build(nb, p, leaf_max=None, tpl=None):
+    t = nb.Octree(p.n, leaf_max, tpl)
     t.reset()
     t.bbox(p)
     t.build(p)
@@ -82,12 +82,13 @@ def test_star_force_single_body(nb, cuda):
 
 
 # ---------------------------------------------------- forces: oracle and FP64
-@pytest.mark.parametrize("n,theta", [(4096, 0.5), (4096, 0.3), (20000, 0.7)])
-def test_force_accuracy_vs_direct_and_reference_walk(nb, cuda, port, n, theta):
+@pytest.mark.parametrize("n,theta,tpl", [(4096, 0.5, 1), (4096, 0.5, 2), (4096, 0.3, 2),
+                                         (20000, 0.7, 1), (20000, 0.7, 2)])
+def test_force_accuracy_vs_direct_and_reference_walk(nb, cuda, port, n, theta, tpl):
     st = disk(nb, n, 0.5, 5.0, seed=1, m=1e-8)
     eps = 1e-3
     p = to_gpu(nb, cuda, st)
-    t = build(nb, p)
+    t = build(nb, p, tpl=tpl)
     t.force(p, theta, eps, 1.0)
     a = np.stack([host(p, "ax"), host(p, "ay"), host(p, "az")], 1).astype(np.float64)
     tg = np.arange(n)
@@ -99,7 +100,7 @@ def test_force_accuracy_vs_direct_and_reference_walk(nb, cuda, port, n, theta):
     # self-gravity alone (the star dominates the total by ~1e4, so an FP32
     # total cannot resolve it): both walks again with star_mass = 0
     p0 = to_gpu(nb, cuda, st)
-    t0 = build(nb, p0)
+    t0 = build(nb, p0, tpl=tpl)
     t0.force(p0, theta, eps, 0.0)
     a0 = np.stack([host(p0, "ax"), host(p0, "ay"), host(p0, "az")], 1).astype(np.float64)
     sx, sy, sz = port.direct_f64(st["x"], st["y"], st["z"], st["m"], tg, eps, 1.0, False)

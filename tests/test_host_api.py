@@ -1,0 +1,275 @@
+"""Host-side C ABI (CPU suite): the library loads and exports every symbol the
+header declares; Config loading, aggregate records, the frames.bin/stats.csv
+writer and the perturber orbit agree with the reference's own host code
+(golden fixtures from tests/golden/make_golden.py); the disk generator."""
+from __future__ import annotations
+
+import json
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, ROOT, golden
+
+
+def header_symbols():
+    text = open(os.path.join(ROOT, "include", "nbody_b200.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(nbody_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_header_symbol(nb):
+    syms = header_symbols()
+    assert len(syms) > 40
+    out = subprocess.run(["nm", "-D", "--defined-only", nb.LIB_PATH], capture_output=True,
+                         text=True, check=True).stdout
+    exported = set(re.findall(r" T (nbody_[a-z0-9_]+)", out))
+    missing = [s for s in syms if s not in exported]
+    assert not missing, missing
+    declared = {name for name, _, _ in nb.SIGNATURES}
+    assert set(syms) <= declared, sorted(set(syms) - declared)
+
+
+def test_abi_version(nb):
+    assert nb.lib.nbody_abi_version() == 1
+
+
+def test_package_has_no_cpu_fallback(nb):
+    src = open(os.path.join(ROOT, "nbody-sim_b200", "__init__.py")).read()
+    assert "oracle" not in src.replace("oracle/", "")
+
+
+# ------------------------------------------------------------------ config
+CONFIG_FIELDS = ["disk_r_min", "disk_r_max", "disk_h_factor", "particle_mass_msun",
+                 "star_mass_msun", "softening_AU", "theta", "collision_radius_factor",
+                 "restitution", "gas_drag_rate", "dt", "total_time", "perturber_mass_mjup",
+                 "perturber_radius_AU", "perturber_phase0", "n_particles",
+                 "output_every_n_steps", "perturber_enabled", "output_dir"]
+
+
+def _cases():
+    with open(golden("config_cases.json")) as f:
+        return json.load(f)
+
+
+@pytest.mark.parametrize("name", sorted(_cases().keys()))
+def test_config_load_matches_reference(nb, name):
+    case = _cases()[name]
+    path = os.path.join(GOLDEN, "configs", name)
+    if case["ok"]:
+        c = nb.load_config(path).to_dict()
+        for k in CONFIG_FIELDS:
+            want = case["cfg"][k]
+            if isinstance(want, float):
+                assert np.float32(c[k]) == np.float32(want), k
+            else:
+                assert c[k] == want, k
+    else:
+        with pytest.raises(nb.NBodyError) as e:
+            nb.load_config(path)
+        msg, want = str(e.value), case["error"]
+        if want.startswith("JSON parse error in"):
+            assert msg.startswith(f"JSON parse error in '{path}': ")
+            assert e.value.code == nb.NBODY_ERR_CONFIG
+        elif want.startswith("Cannot open config"):
+            assert msg == f"Cannot open config: {path}"
+            assert e.value.code == nb.NBODY_ERR_IO
+        else:
+            assert msg == want
+            assert e.value.code == nb.NBODY_ERR_CONFIG
+
+
+def test_config_defaults_match_reference_struct(nb):
+    c = nb.default_config().to_dict()
+    assert c["n_particles"] == 100000 and c["output_every_n_steps"] == 200
+    assert np.float32(c["particle_mass_msun"]) == np.float32(3.003e-7)
+    assert np.float32(c["collision_radius_factor"]) == np.float32(100.0)
+    assert c["output_dir"] == "data" and not c["perturber_enabled"]
+
+
+def test_reference_configs_load_identically(nb, refhost):
+    cfgdir = "/root/reference/config"
+    if not os.path.isdir(cfgdir):
+        pytest.skip("reference checkout absent")
+    for f in sorted(os.listdir(cfgdir)):
+        want = refhost.load_config(os.path.join(cfgdir, f))
+        got = nb.load_config(os.path.join(cfgdir, f)).to_dict()
+        for k in CONFIG_FIELDS:
+            if isinstance(want[k], float):
+                assert np.float32(got[k]) == np.float32(want[k]), (f, k)
+            else:
+                assert got[k] == want[k], (f, k)
+
+
+def test_reference_config_test_expectation_documented(nb, refhost):
+    """tests/test_config.cpp:5-21 expects output_every_n_steps == 200 and
+    total_time == 2000 from config/simulation.json, which holds 50 / 500: the
+    reference's own test fails there; both loaders return the file's values."""
+    path = "/root/reference/config/simulation.json"
+    if not os.path.exists(path):
+        pytest.skip("reference checkout absent")
+    c = nb.load_config(path).to_dict()
+    assert c["output_every_n_steps"] == 50 and c["total_time"] == 500.0
+    assert c["n_particles"] == 100000 and np.float32(c["theta"]) == np.float32(0.5)
+
+
+def test_particle_radius_matches_reference(nb):
+    with open(golden("radius.json")) as f:
+        for m, r in json.load(f).items():
+            assert np.float32(nb.particle_physical_radius(float(m))) == np.float32(r), m
+    # tests/test_disk_init.cpp:57-77
+    assert abs(nb.particle_physical_radius(3.003e-7) / 2.416e-5 - 1) < 0.01
+
+
+def test_sim_params_from_config(nb):
+    c = nb.load_config(os.path.join(GOLDEN, "configs", "full.json"))
+    p = nb.sim_params(c)
+    r = np.float32(5.0) * np.float32(nb.particle_physical_radius(1e-8))
+    assert np.float32(p.r_coll) == r
+    assert p.perturber_enabled == 1 and np.float32(p.perturber_radius_au) == np.float32(5.2)
+
+
+# ----------------------------------------------------------------- perturber
+def test_perturber_host_orbit_bit_exact_with_oracle(nb, port):
+    c = nb.default_config()
+    c.perturber_enabled, c.perturber_mass_mjup, c.perturber_radius_AU = 1, 3.0, 10.0
+    c.perturber_phase0 = 0.3
+    p = nb.make_perturber(c)
+    q = port.perturber(True, 3.0, 10.0, 0.3, 1.0)
+    for k in ("r", "mass_msun", "phase0", "omega", "x", "y", "z"):
+        assert getattr(p, k) == getattr(q, k), k
+    for t in (0.0, 0.005, 17.5, 1234.5678):
+        nb.update_perturber(p, t)
+        q2 = port.perturber_at(q, t)
+        assert (p.x, p.y, p.z) == (q2.x, q2.y, q2.z)
+    c.perturber_enabled = 0
+    d = nb.make_perturber(c)
+    d.x = d.y = d.z = 42.0
+    nb.update_perturber(d, 1000.0)
+    assert (d.x, d.y, d.z) == (42.0, 42.0, 42.0)  # tests/test_perturber.cu:87-98
+
+
+# ---------------------------------------------------------------- aggregates
+@pytest.mark.parametrize("name", ["fof_a.npz", "fof_b.npz", "fof_c.npz"])
+def test_aggregate_records_match_reference(nb, name):
+    g = np.load(golden(name))
+    recs, ng = nb.aggregates_from_labels(g["x"], g["y"], g["z"], g["vx"], g["vy"], g["vz"],
+                                         g["labels"], float(g["particle_mass"]))
+    assert ng == int(g["n_groups"])
+    for k in range(ng):
+        r = recs[k]
+        assert r.first_member == g["g_label"][k] and r.n_particles == g["g_n"][k]
+        assert np.float32(r.mass_msun) == g["g_mass"][k]
+        assert np.float32(r.cx) == g["g_c"][3 * k] and np.float32(r.cz) == g["g_c"][3 * k + 2]
+        assert np.float32(r.vy) == g["g_v"][3 * k + 1]
+        assert np.float32(r.dist_center) == g["g_dist"][k]
+
+
+def test_aggregates_reject_bad_labels(nb):
+    x = np.zeros(3, np.float32)
+    with pytest.raises(nb.NBodyError):
+        nb.aggregates_from_labels(x, x, x, x, x, x, np.array([0, 5, 1], np.int32), 1.0)
+
+
+# --------------------------------------------------------------------- writer
+def test_writer_bytes_match_reference(nb, tmp_path):
+    d = np.load(os.path.join(GOLDEN, "writer_run", "inputs.npz"))
+    c = nb.default_config()
+    c.n_particles, c.dt, c.output_every_n_steps = int(d["n"]), float(d["dt"]), int(d["output_every"])
+    w = nb.OutputWriter(str(tmp_path), c)
+    p = nb.allocate_particles_cpu(int(d["n"]))
+    p.arrays["x"][:], p.arrays["y"][:], p.arrays["z"][:] = d["x"], d["y"], d["z"]
+    aggs = []
+    for k in range(2):
+        aggs.append(nb.Aggregate(k, int(d["g_n"][k]), d["g_mass"][k], *d["g_c"][3 * k:3 * k + 3],
+                                 *d["g_v"][3 * k:3 * k + 3], d["g_dist"][k], []))
+    pert = d["pert"].reshape(3, 5)
+    for f in range(3):
+        t = float(d["t"][f])
+        w.write_frame(p, t, d["agg"])
+        w.write_stats(aggs, f, t)
+        w.write_perturber_stats(f, t, 2, *[float(v) for v in pert[f]])
+    w.finalize(3)
+    w.close()
+    for fn in ("frames.bin", "stats.csv"):
+        got = open(tmp_path / fn, "rb").read()
+        want = open(os.path.join(GOLDEN, "writer_run", fn), "rb").read()
+        assert got == want, fn
+    # test_frames_validator.cs:39 size formula
+    n = int(d["n"])
+    assert len(open(tmp_path / "frames.bin", "rb").read()) == 32 + 3 * (8 + n * 14)
+
+
+def test_writer_header_and_size_check(nb, tmp_path):
+    # tests/test_output.cpp:15-81
+    c = nb.default_config()
+    c.n_particles, c.dt, c.output_every_n_steps = 4, 0.01, 1
+    w = nb.OutputWriter(str(tmp_path), c)
+    p = nb.allocate_particles_cpu(4)
+    p.arrays["x"][:] = [1, 2, 3, 4]
+    w.write_frame(p, 0.0, np.ones(4, np.uint16))
+    w.write_frame(p, 1.0, np.ones(4, np.uint16))
+    w.finalize(2)
+    with pytest.raises(RuntimeError):
+        w.write_frame(p, 2.0, np.ones(3, np.uint16))
+    w.close()
+    b = open(tmp_path / "frames.bin", "rb").read()
+    assert b[:4] == b"NBOD"
+    assert np.frombuffer(b[4:16], np.uint32).tolist() == [2, 4, 2]
+    assert np.frombuffer(b[16:32], np.float64).tolist() == [np.float32(0.01), np.float32(0.01)]
+    assert np.frombuffer(b[32:40], np.float64)[0] == 0.0
+    assert np.frombuffer(b[40:44], np.float32)[0] == 1.0
+
+
+def test_writer_open_error(nb):
+    c = nb.default_config()
+    with pytest.raises(nb.NBodyError) as e:
+        nb.OutputWriter("/nonexistent_dir_for_test/sub", c)
+    assert e.value.code == nb.NBODY_ERR_IO
+    assert "OutputWriter: cannot open" in str(e.value)
+
+
+# ------------------------------------------------------------- disk generator
+def test_disk_generator_recipe(nb):
+    n = 20000
+    d = nb.make_disk(n, 0.5, 5.0, 0.01, 0.005, 1.0, 3)
+    x, y, z, vx, vy, vz = (d[k] for k in ("x", "y", "z", "vx", "vy", "vz"))
+    r = np.sqrt(x * x + y * y + z * z)
+    assert r.min() > 0.5 * (1 - 0.05) and r.max() < 5.0 * (1 + 0.05)  # a(1 +- e), e << 1
+    # angular momentum along -Y (same sense as initDisk: x = r cos phi, z = r sin phi)
+    ly = z * vx - x * vz
+    assert (ly < 0).mean() > 0.999
+    # Rayleigh inclination: |y|/r ~ sin(i) sin(..); rms tilt ~ sigma_i
+    tilt = np.abs(y) / r
+    assert 0.001 < np.sqrt(np.mean(tilt ** 2)) < 0.01
+    # eccentricity from the orbit, mean of Rayleigh(0.01) = 0.01 sqrt(pi/2)
+    v2 = vx * vx + vy * vy + vz * vz
+    rv = x * vx + y * vy + z * vz
+    ex = (v2 - 1 / r) * x - rv * vx
+    ey = (v2 - 1 / r) * y - rv * vy
+    ez = (v2 - 1 / r) * z - rv * vz
+    e = np.sqrt(ex * ex + ey * ey + ez * ez)
+    assert abs(e.mean() - 0.01 * np.sqrt(np.pi / 2)) < 5e-4
+    # Sigma ~ r^-1.5: the semi-major axis CDF is (sqrt a - sqrt r_min)/(sqrt r_max - sqrt r_min)
+    a = 1 / (2 / r - v2)
+    u = (np.sqrt(a) - np.sqrt(0.5)) / (np.sqrt(5.0) - np.sqrt(0.5))
+    assert abs(np.mean(u) - 0.5) < 0.01
+
+
+def test_disk_generator_deterministic(nb):
+    a = nb.make_disk(1000, 0.3, 30.0, 0.01, 0.005, 1.0, 7)
+    b = nb.make_disk(1000, 0.3, 30.0, 0.01, 0.005, 1.0, 7)
+    c = nb.make_disk(500, 0.3, 30.0, 0.01, 0.005, 1.0, 7)
+    d = nb.make_disk(1000, 0.3, 30.0, 0.01, 0.005, 1.0, 8)
+    for k in a:
+        np.testing.assert_array_equal(a[k], b[k])
+        np.testing.assert_array_equal(a[k][:500], c[k])  # counter-based: prefixes agree
+    assert not np.array_equal(a["x"], d["x"])
+
+
+def test_disk_generator_rejects_bad_args(nb):
+    with pytest.raises(nb.NBodyError):
+        nb.make_disk(10, 5.0, 1.0)
