@@ -188,6 +188,37 @@ int nbody_perturber_force(nbody_particles* p, float px, float py, float pz, floa
 int nbody_fof(nbody_tree* t, const float* x, const float* y, const float* z, int n,
               float link_length, int* labels, uint16_t* agg_size, int* n_groups);
 
+/* Friends-of-friends without any device allocation.  No counterpart in the
+ * reference: it is nbody_fof for callers that may not allocate device memory
+ * when they need aggregates -- an analysis or visualisation process that
+ * polls a running simulation's snapshots while the simulation has reserved
+ * the rest of the GPU's memory; code whose device memory belongs to another
+ * allocator (a framework's caching allocator, a pool sized at start-up); and
+ * loops that must not stall, since cudaFree waits for the whole device and
+ * cudaMalloc can block behind work in flight.  nbody_fof, by contrast, needs
+ * an nbody_tree, which allocates.
+ *
+ * All scratch (sort buffers, tree, union-find arrays, a bounded stack-spill
+ * area) lives in one statically sized device array inside libnbody_b200.so,
+ * NBODY_FOF_NOALLOC_SCRATCH_BYTES bytes (12.5 MiB), which every GPU that
+ * loads the library holds until the process exits.  n is limited to
+ * NBODY_FOF_NOALLOC_MAX_N bodies; larger n returns NBODY_ERR_ARG with a
+ * message naming the limit.  Inputs and outputs are as for nbody_fof
+ * (device x, y, z, labels, agg_size; host *n_groups), bit-identical results.
+ *
+ * The first call on each device looks up that device's address of the array
+ * (cudaGetSymbolAddress) with the device current; later calls reuse it.  All
+ * calls on a device share the one array and each call overwrites it: the
+ * function runs on the legacy default stream and synchronises before it
+ * returns, so calls from one host thread never overlap, but calls that could
+ * overlap on the GPU (other host threads, or the default stream in
+ * per-thread mode) race on the scratch and must be serialised by the caller.
+ * The function calls no cudaMalloc, cudaFree or allocating library routine. */
+#define NBODY_FOF_NOALLOC_MAX_N 32768
+#define NBODY_FOF_NOALLOC_SCRATCH_BYTES 13110784
+int nbody_fof_noalloc(const float* x, const float* y, const float* z, int n, float link_length,
+                      int* labels, uint16_t* agg_size, int* n_groups);
+
 /* Aggregate (include/Aggregate.h:4-12) without the member list. */
 typedef struct nbody_aggregate {
   int id;

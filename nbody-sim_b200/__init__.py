@@ -44,6 +44,7 @@ NBODY_ERR_TIMEOUT = 4
 NBODY_ERR_IO = 5
 NBODY_ERR_CONFIG = 6
 NBODY_ERR_STATE = 7
+FOF_NOALLOC_MAX_N = 32768
 STATE_F32 = 0
 STATE_F64 = 1
 
@@ -164,6 +165,7 @@ SIGNATURES = [
     ("nbody_perturber_force", C.c_int, [C.POINTER(nbody_particles), C.c_float, C.c_float,
                                         C.c_float, C.c_float, C.c_float]),
     ("nbody_fof", C.c_int, [_VP, _VP, _VP, _VP, C.c_int, C.c_float, _VP, _VP, _I]),
+    ("nbody_fof_noalloc", C.c_int, [_VP, _VP, _VP, C.c_int, C.c_float, _VP, _VP, _I]),
     ("nbody_aggregates", C.c_int, [_F, _F, _F, _F, _F, _F, _I, C.c_int, C.c_float,
                                    C.POINTER(nbody_aggregate), C.c_int, _I]),
     ("nbody_writer_open", C.c_int, [C.c_char_p, C.POINTER(nbody_config), C.POINTER(_VP)]),
@@ -406,6 +408,21 @@ def perturber_force(p: ParticleData, px, py, pz, pmass, softening):
 
 
 # --------------------------------------------------------------- FoF
+def fof_noalloc(x, y, z, link_length: float):
+    """nbody_fof_noalloc on torch CUDA float tensors: the device FoF with its
+    scratch in the library's static device array (no allocation by the
+    library; n <= FOF_NOALLOC_MAX_N).  Returns (labels, agg_size as int16
+    holding uint16 sizes, n_groups)."""
+    import torch
+    n = x.numel()
+    labels = torch.empty(n, dtype=torch.int32, device=x.device)
+    agg = torch.empty(n, dtype=torch.int16, device=x.device)
+    ng = C.c_int()
+    _check(lib.nbody_fof_noalloc(x.data_ptr(), y.data_ptr(), z.data_ptr(), n, link_length,
+                                 labels.data_ptr(), agg.data_ptr(), C.byref(ng)))
+    return labels, agg, ng.value
+
+
 @dataclass
 class Aggregate:
     """include/Aggregate.h:4-12."""

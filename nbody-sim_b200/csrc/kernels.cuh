@@ -150,6 +150,9 @@ void launch_fof_link(const NeighborArgs& a, const uint32_t* ids, float link_leng
                      int* parent, cudaStream_t s);
 void launch_fof_finish(int* parent, int n, int* labels, int* sizes, uint16_t* agg_size,
                        int* n_groups, int* status, cudaStream_t s);
+// launch_fof_link with at most max_warps warps (spill slots) in flight.
+void launch_fof_link_capped(const NeighborArgs& a, const uint32_t* ids, float link_length,
+                            int* parent, int max_warps, cudaStream_t s);
 
 // -------------------------------------------------------- streaming (compat)
 void launch_half_kick(float* vx, float* vy, float* vz, const float* ax, const float* ay,

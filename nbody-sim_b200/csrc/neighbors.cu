@@ -326,4 +326,23 @@ void launch_fof_finish(int* parent, int n, int* labels, int* sizes, uint16_t* ag
   check(cudaGetLastError(), "fof finish launch");
 }
 
+// FoF links with the warp count capped at max_warps, for a caller whose stack
+// spill area holds max_warps slots of a.spill_cap entries (the allocation-free
+// FoF entry point sizes its static area this way).
+void launch_fof_link_capped(const NeighborArgs& a, const uint32_t* ids, float link_length,
+                            int* parent, int max_warps, cudaStream_t s) {
+  if (a.n <= 0) return;
+  k_fof_init<<<div_up(a.n, 256), 256, 0, s>>>(parent, a.n);
+  CollideOut co{nullptr, nullptr, nullptr, nullptr, 0.f, 0.f, nullptr, nullptr, nullptr};
+  const float ll2 = link_length * link_length;  // Aggregate.cpp:30
+  FofOut fo{ids, ll2, parent};
+  int grid = sm_count() * nb_blocks_per_sm<1>();
+  grid = std::min(grid, max_warps / kNbWarps);
+  grid = std::min(grid, (a.n + kNbWarps - 1) / kNbWarps);
+  if (grid < 1) grid = 1;
+  check(cudaMemsetAsync(a.work, 0, sizeof(int), s), "neighbors work reset");
+  k_neighbors<1><<<grid, kNbWarps * 32, 0, s>>>(a, link_length, co, fo);
+  check(cudaGetLastError(), "k_neighbors launch");
+}
+
 }  // namespace nb

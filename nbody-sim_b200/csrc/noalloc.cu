@@ -1,0 +1,159 @@
+// noalloc.cu -- nbody_fof_noalloc: the device FoF of nbody_fof for callers
+// that may not allocate device memory.
+//
+// Every buffer the FoF needs (Morton keys and radix-sort buffers, the Karras
+// tree, FP64 moments, the octree, warp groups, union-find arrays and a
+// bounded stack-spill area) is carved out of one file-scope __device__ array
+// sized for kMaxN bodies.  Host code never uses the array's name as a
+// pointer: the device address comes from cudaGetSymbolAddress, looked up
+// once per device with that device current, on the first call made there.
+#include <cstring>
+#include <mutex>
+
+#include "capi_util.h"
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace nb {
+namespace {
+
+constexpr int kMaxN = NBODY_FOF_NOALLOC_MAX_N;
+constexpr int kSpillCap = 1024;     // stack entries per warp slot
+constexpr int kSpillWarps = 1184;   // warp slots: 148 SMs x 2 blocks x 4 warps
+constexpr size_t kAlign = 256;
+
+constexpr size_t al(size_t b) { return (b + kAlign - 1) / kAlign * kAlign; }
+constexpr size_t kNb = 2 * (size_t)kMaxN;
+constexpr size_t kCountWords = 4096;  // >= radix_sort_count_words(kMaxN) = 2050
+constexpr size_t kScanWords = 4096;   // >= scan_tmp_words(2 kMaxN) = 17
+constexpr size_t kMomTiles = 2 * ((size_t)kMaxN / kMomentTile + 2) + 8;
+
+constexpr size_t kScratchBytes =
+    4 * al(sizeof(uint32_t) * kMaxN) +          // keys, perm, keys_alt, perm_alt
+    al(sizeof(uint32_t) * kCountWords) +        // radix-sort counts + scan partials
+    al(sizeof(float4) * kMaxN) +                // body4
+    4 * al(sizeof(int) * kMaxN) +               // bin_left, bin_right, bin_lo, bin_hi
+    al(sizeof(int) * kNb) +                     // bin_parent
+    al(sizeof(uint8_t) * kMaxN) +               // bin_prefix
+    al(sizeof(double4) * (kMaxN + 1)) +         // moment prefix sums
+    al(sizeof(double4) * kMomTiles) +           // moment tile sums / prefixes
+    al(sizeof(uint8_t) * kNb) +                 // oct_nch
+    2 * al(sizeof(uint32_t) * kNb) +            // oct_off, group_flag
+    al(sizeof(uint32_t) * kScanWords) +         // scan partials
+    4 * al(sizeof(float4) * kNb) +              // octree com, info, box_lo, box_hi
+    al(sizeof(unsigned long long) * 6) +        // bbox
+    al(sizeof(TreeGeom)) +                      // root geometry
+    5 * al(sizeof(int)) +                       // n_nodes, status, n_groups, fof groups, work
+    al(sizeof(int2) * kMaxN) +                  // warp groups
+    2 * al(sizeof(int) * kMaxN) +               // union-find parent, group sizes
+    al(sizeof(int) * (size_t)kSpillWarps * kSpillCap);  // stack spill
+
+static_assert(kScratchBytes == NBODY_FOF_NOALLOC_SCRATCH_BYTES,
+              "header's stated scratch size must match the array");
+
+static __device__ __align__(256) unsigned char g_fof_scratch[kScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_mu;
+unsigned char* g_addr[kMaxDevices] = {nullptr};
+
+unsigned char* scratch_for_current_device() {
+  int dev = 0;
+  check(cudaGetDevice(&dev), "cudaGetDevice");
+  if (dev < 0 || dev >= kMaxDevices) throw ArgError("nbody_fof_noalloc: device ordinal too large");
+  std::lock_guard<std::mutex> lock(g_mu);
+  if (!g_addr[dev]) {
+    void* p = nullptr;
+    check(cudaGetSymbolAddress(&p, g_fof_scratch), "cudaGetSymbolAddress(FoF scratch)");
+    g_addr[dev] = static_cast<unsigned char*>(p);
+  }
+  return g_addr[dev];
+}
+
+struct Carve {
+  unsigned char* base;
+  size_t off = 0;
+  template <typename T>
+  T* take(size_t count) {
+    T* p = reinterpret_cast<T*>(base + off);
+    off += al(sizeof(T) * count);
+    if (off > kScratchBytes) throw ArgError("nbody_fof_noalloc: scratch layout overflow");
+    return p;
+  }
+};
+
+}  // namespace
+}  // namespace nb
+
+extern "C" int nbody_fof_noalloc(const float* x, const float* y, const float* z, int n,
+                                 float link_length, int* labels, uint16_t* agg_size,
+                                 int* n_groups) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(x && y && z && labels && agg_size && n_groups, "nbody_fof_noalloc: null argument");
+    NBODY_REQUIRE(n >= 0, "nbody_fof_noalloc: negative body count");
+    if (n > nb::kMaxN)
+      throw nb::ArgError("nbody_fof_noalloc: n = " + std::to_string(n) + " exceeds the static "
+                         "scratch limit NBODY_FOF_NOALLOC_MAX_N = " + std::to_string(nb::kMaxN) +
+                         "; use nbody_fof");
+    *n_groups = 0;
+    if (n == 0) return NBODY_OK;
+    nb::Carve c{nb::scratch_for_current_device()};
+    nb::TreeWork w;
+    w.cap = nb::kMaxN;
+    w.keys = c.take<uint32_t>(nb::kMaxN);
+    w.perm = c.take<uint32_t>(nb::kMaxN);
+    w.keys_alt = c.take<uint32_t>(nb::kMaxN);
+    w.perm_alt = c.take<uint32_t>(nb::kMaxN);
+    w.counts = c.take<uint32_t>(nb::kCountWords);
+    w.body4 = c.take<float4>(nb::kMaxN);
+    w.bin_left = c.take<int>(nb::kMaxN);
+    w.bin_right = c.take<int>(nb::kMaxN);
+    w.bin_lo = c.take<int>(nb::kMaxN);
+    w.bin_hi = c.take<int>(nb::kMaxN);
+    w.bin_parent = c.take<int>(nb::kNb);
+    w.bin_prefix = c.take<uint8_t>(nb::kMaxN);
+    w.mom_ploc = c.take<double4>(nb::kMaxN + 1);
+    w.mom_tiles = c.take<double4>(nb::kMomTiles);
+    w.oct_nch = c.take<uint8_t>(nb::kNb);
+    w.oct_off = c.take<uint32_t>(nb::kNb);
+    w.group_flag = c.take<uint32_t>(nb::kNb);
+    w.scan_tmp = c.take<uint32_t>(nb::kScanWords);
+    w.oct.com = c.take<float4>(nb::kNb);
+    w.oct.info = c.take<int4>(nb::kNb);
+    w.oct.box_lo = c.take<float4>(nb::kNb);
+    w.oct.box_hi = c.take<float4>(nb::kNb);
+    w.bbox_enc = c.take<unsigned long long>(6);
+    w.geom = c.take<nb::TreeGeom>(1);
+    w.n_nodes = c.take<int>(1);
+    w.status = c.take<int>(1);
+    w.n_groups = c.take<int>(1);
+    int* fof_groups = c.take<int>(1);
+    int* work = c.take<int>(1);
+    w.groups = c.take<int2>(nb::kMaxN);
+    int* parent = c.take<int>(nb::kMaxN);
+    int* sizes = c.take<int>(nb::kMaxN);
+    int* spill = c.take<int>((size_t)nb::kSpillWarps * nb::kSpillCap);
+    w.group_max = 32;
+    // the array keeps the previous call's contents: clear what is read before written
+    nb::check(cudaMemsetAsync(w.status, 0, sizeof(int), 0), "status clear");
+    nb::launch_bbox<float>(w, x, y, z, n, 0);
+    nb::launch_keys<float>(w, x, y, z, n, 0);
+    nb::radix_sort_pairs(w.keys, w.perm, w.keys_alt, w.perm_alt, w.counts, n, 30, 0);
+    nb::launch_gather_body4(w, x, y, z, nullptr, n, 0);
+    nb::launch_build_topology(w, n, 0);
+    nb::launch_build_moments(w, n, nullptr, nullptr, nullptr, 0);
+    nb::NeighborArgs na{w.oct.info, w.oct.box_lo, w.oct.box_hi, w.body4, n, w.groups,
+                        w.n_groups, 8, spill, nb::kSpillCap, work, w.status};
+    nb::launch_fof_link_capped(na, w.perm, link_length, parent, nb::kSpillWarps, 0);
+    nb::launch_fof_finish(parent, n, labels, sizes, agg_size, fof_groups, w.status, 0);
+    nb::check(cudaGetLastError(), "nbody_fof_noalloc launch");
+    nb::check(cudaStreamSynchronize(0), "nbody_fof_noalloc sync");
+    int st = 0;
+    nb::check(cudaMemcpy(&st, w.status, sizeof(int), cudaMemcpyDeviceToHost), "status read");
+    if (st)
+      throw nb::ArgError("nbody_fof_noalloc: device status " + std::to_string(st),
+                         NBODY_ERR_OVERFLOW);
+    nb::check(cudaMemcpy(n_groups, fof_groups, sizeof(int), cudaMemcpyDeviceToHost),
+              "groups read");
+  })
+}
