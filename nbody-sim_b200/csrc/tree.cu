@@ -363,26 +363,29 @@ __device__ void write_node(const EmitArgs& a, int c, int f) {
   const int L = (int)a.prefix[c] / 3;
   const int lo = a.lo[c], hi = a.hi[c];
   const double4 s = range_moments(a.ploc, a.tpre, lo, hi + 1);
-  // the node's cube: level L cell of its key prefix
+  // the node's cube: level L cell of its key prefix (side 2 rhs / 2^L, exact
+  // power-of-two scaling), grown by a margin for float positions that sit an
+  // ulp outside their FP64-quantised cell
   const uint32_t kl = a.keys[lo] >> (3 * (10 - L));
   const uint32_t cc[3] = {compact3(kl), compact3(kl >> 1), compact3(kl >> 2)};
-  const double side = ldexp(2.0 * (double)rhs, -L);
-  float blo[3], bhi[3];
-  double ctr[3];
+  const double side = (double)a.geom->rhs * (double)(2.0f / (float)(1u << L));
+  float blo[3], bhi[3], ctr[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
-    const double l0 = a.geom->lo[k] + (double)cc[k] * side, h0 = l0 + side;
-    // float positions may sit an ulp outside their FP64-quantised cell
-    const double margin = 1e-6 * (fabs(l0) + fabs(h0) + side) + 1e-30;
-    blo[k] = __double2float_rd(l0 - margin);
-    bhi[k] = __double2float_ru(h0 + margin);
-    ctr[k] = 0.5 * (l0 + h0);
+    const double l0 = a.geom->lo[k] + (double)cc[k] * side;
+    const float fl = (float)l0, fs = (float)side;
+    const float margin = 1e-6f * (fabsf(fl) + fs) + 1e-30f;
+    blo[k] = fl - margin;
+    bhi[k] = fl + fs + margin;
+    ctr[k] = fl + 0.5f * fs;
   }
   float4 com;
-  if (s.x > 0.0)
-    com = make_float4((float)(s.y / s.x), (float)(s.z / s.x), (float)(s.w / s.x), (float)s.x);
-  else
-    com = make_float4((float)ctr[0], (float)ctr[1], (float)ctr[2], 0.f);
+  if (s.x > 0.0) {
+    const double inv = 1.0 / s.x;
+    com = make_float4((float)(s.y * inv), (float)(s.z * inv), (float)(s.w * inv), (float)s.x);
+  } else {
+    com = make_float4(ctr[0], ctr[1], ctr[2], 0.f);
+  }
   const int k = a.nch[c];
   a.oct.com[f] = com;
   a.oct.info[f] = make_int4(k > 0 ? 1 + (int)a.off[c] : -1, lo, ((hi - lo + 1) << 4) | k,
@@ -391,21 +394,36 @@ __device__ void write_node(const EmitArgs& a, int c, int f) {
   a.oct.box_hi[f] = make_float4(bhi[0], bhi[1], bhi[2], 0.f);
 }
 
-// Every top node writes the records of its octree children into its block
-// of contiguous slots (1 + off[b] ...); node 0 also writes the root.  Target
-// groups are written at their scanned offsets.
+// Every top node owns a block of contiguous slots (1 + off[b] ...) for its
+// octree children; node 0 also owns slot 0, the root.  A warp gathers the
+// (child, slot) pairs of its 32 binary nodes in shared memory and then writes
+// the records one per lane, so the up-to-8 records of one parent do not
+// serialise on a single thread.  Target groups are written at their scanned
+// offsets.
+constexpr int kEmitWarps = kThreads / 32;
+
 __global__ void __launch_bounds__(kThreads) k_emit(const EmitArgs a) {
+  __shared__ int2 s_job[kEmitWarps][32 * 8 + 1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   const int nb = 2 * a.n - 1;
-  if (b >= nb) return;
-  if (b == 0) write_node(a, 0, 0);
-  const int k = a.nch[b];
+  const bool in = b < nb;
+  const int k = in ? a.nch[b] : 0;
+  const int extra = (b == 0) ? 1 : 0;  // the root record
+  const int incl = warp_incl_scan(k + extra, lane);
+  const int total = __shfl_sync(kFull, incl, 31);
+  int pos = incl - k - extra;
+  int2* job = s_job[warp];
+  if (extra) job[pos++] = make_int2(0, 0);
   if (k > 0) {
     const int base = 1 + (int)a.off[b];
     const int lb = (int)a.prefix[b] / 3;
     for_each_oct_child(a.left, a.right, a.prefix, a.n, b, lb,
-                       [&](int c, int i) { write_node(a, c, base + i); });
+                       [&](int c, int i) { job[pos + i] = make_int2(c, base + i); });
   }
+  __syncwarp();
+  for (int j = lane; j < total; j += 32) write_node(a, job[j].x, job[j].y);
+  if (!in) return;
   const int c = bin_count(a.lo, a.hi, a.n, b);
   const int p = (b == 0) ? -1 : a.parent[b];
   const int pc = (p < 0) ? 0x7fffffff : bin_count(a.lo, a.hi, a.n, p);
