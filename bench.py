@@ -56,6 +56,12 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-flush", action="store_true")
+    ap.add_argument("--workload", choices=["disk1m", "ensemble"], default="disk1m",
+                    help="disk1m: the headline single disk; ensemble: 64 disks (C4) against "
+                         "the same disks run one by one")
+    ap.add_argument("--disks", type=int, default=64)
+    ap.add_argument("--solo-steps", type=int, default=10,
+                    help="timed steps per disk of the one-by-one comparison")
     return ap.parse_args()
 
 
@@ -322,12 +328,136 @@ def run_ours(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_ensemble(args, ws, rank, local):
+    """64 disks of uneven size (N log-uniform in [2048, 65536]) with their own
+    perturbers, collisions and drag, FP64 state: the batched ensemble engine
+    against the same disks stepped one by one through nbody_sim.  With several
+    ranks each rank takes a share of the disks balanced by N log N (strong
+    scaling, no collective in the data path)."""
+    import torch
+    nb = importlib.import_module("nbody-sim_b200")
+    wl = importlib.import_module("nbody-sim_b200.workloads")
+    torch.cuda.set_device(local)
+    specs_all = wl.c4_disks(args.disks)
+    mine = wl.partition_disks([d["n"] for d in specs_all], ws)[rank]
+    specs = [specs_all[k] for k in mine]
+    prm = wl.c4_params(nb)
+    st, m = wl.ensemble_state(nb, specs)
+    n = len(m)
+    n_all = sum(d["n"] for d in specs_all)
+    stream = torch.cuda.current_stream()
+    ens = nb.Ensemble(prm, specs)
+    ens.set_stream(stream.cuda_stream)
+    ens.set_state(st["x"], st["y"], st["z"], st["vx"], st["vy"], st["vz"], m)
+    tuned = ens.autotune()
+    for _ in range(args.warmup):
+        ens.step(1)
+    ens.sync()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    s0 = ens.stats()
+    clocks = Clocks(torch.cuda.current_device()) if rank == 0 else None
+    barrier(ws)
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        if not args.no_flush:
+            flush.zero_()
+        starts[k].record(stream)
+        ens.step(1)
+        ends[k].record(stream)
+    torch.cuda.synchronize()
+    barrier(ws)
+    ck = clocks.stop() if clocks else None
+    ens.sync()
+    s1 = ens.stats()
+    ms = sum(a.elapsed_time(b) for a, b in zip(starts, ends))
+    ms_max = allreduce_max(ms, ws)
+    value = n_all * args.steps / (ms_max * 1e-3)
+
+    # e2e: nbody_ensemble_step_host, state and accelerations in from pinned
+    # host buffers and back out, every step
+    g = ens.get_state(double=True, accel=True)
+    host = {k: torch.from_numpy(np.ascontiguousarray(g[k])).pin_memory().numpy()
+            for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")}
+    hm = torch.from_numpy(m).pin_memory().numpy()
+    e_steps = max(args.e2e_steps, 1)
+    ens.step_host(host, hm, 1)  # warm-up
+    es = [torch.cuda.Event(enable_timing=True) for _ in range(e_steps)]
+    ee = [torch.cuda.Event(enable_timing=True) for _ in range(e_steps)]
+    barrier(ws)
+    for k in range(e_steps):
+        es[k].record(stream)
+        ens.step_host(host, hm, 1)
+        ee[k].record(stream)
+    torch.cuda.synchronize()
+    e_ms = allreduce_max(sum(a.elapsed_time(b) for a, b in zip(es, ee)), ws)
+
+    # the same disks one by one through nbody_sim (each its own tree, walk, ...)
+    solo_ms = 0.0
+    for spec in specs:
+        d, md = wl.disk_state(nb, spec)
+        p = wl.c4_params(nb)
+        p.perturber_enabled = spec["perturber_enabled"]
+        p.perturber_mass_mjup = spec["perturber_mass_mjup"]
+        p.perturber_radius_au = spec["perturber_radius_au"]
+        p.perturber_phase0 = spec["perturber_phase0"]
+        sim = nb.Sim(p, spec["n"])
+        sim.set_stream(stream.cuda_stream)
+        sim.set_state(d["x"], d["y"], d["z"], d["vx"], d["vy"], d["vz"], md)
+        for _ in range(2):
+            sim.step(1)
+        sim.sync()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if not args.no_flush:
+            flush.zero_()
+        a.record(stream)
+        for _ in range(args.solo_steps):
+            sim.step(1)
+        b.record(stream)
+        torch.cuda.synchronize()
+        solo_ms += a.elapsed_time(b) / args.solo_steps
+        sim.close()
+    solo_ms = allreduce_max(solo_ms, ws)
+    line = {
+        "metric": f"ensemble particle-steps/s ({args.disks} disks)", "value": value, "unit": UNIT,
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{args.disks} Keplerian disks, N log-uniform [2048,65536] "
+                               f"(total {n_all}), r=[0.5,5] AU, m=1e-8, perturber log-uniform "
+                               "[0.3,10] MJ at U[5,30] AU, collisions (factor 5, e=0), drag "
+                               "1e-3, theta 0.5, dt 0.005, FP64 state",
+                   "n_total": n_all, "disks": args.disks, "parallelism": f"disks over {ws} ranks",
+                   "l2": "flushed (256 MB write) before every timed step",
+                   "autotune": [list(t) for t in tuned],
+                   "targets_per_lane": s1.targets_per_lane, "leaf_max": s1.leaf_max},
+        "gpu_launches": int(s1.launches - s0.launches),
+        "graph_launches": int(s1.graph_launches - s0.graph_launches),
+        "one_by_one": {"ms_per_step": solo_ms,
+                       "value": n_all / (solo_ms * 1e-3),
+                       "speedup": solo_ms / (ms_max / args.steps),
+                       "sample": f"each disk alone through nbody_sim, {args.solo_steps} steps "
+                                 "after 2 warm-up, per-step times summed"},
+        "e2e": {"value": n_all * e_steps / (e_ms * 1e-3), "unit": UNIT,
+                "h2d_bytes_per_step": n * (6 * 8 + 3 * 4 + 4),
+                "d2h_bytes_per_step": n * (6 * 8 + 3 * 4),
+                "ms_per_step": e_ms / e_steps},
+        "clocks": ck,
+    }
+    ens.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     ws, rank, local = dist_setup()
     try:
         if args.impl == "reference":
             run_reference(args, ws, rank)
+        elif args.workload == "ensemble":
+            run_ensemble(args, ws, rank, local)
         else:
             run_ours(args, ws, rank, local)
     finally:

@@ -356,6 +356,77 @@ int nbody_sim_step_host(nbody_sim* s, float* x, float* y, float* z, float* vx, f
                         float* vz, float* ax, float* ay, float* az, const float* mass,
                         int nsteps);
 
+/* ----------------------------------------------------------- ensemble --- */
+
+/* Many independent disks advanced together.  The reference runs one disk per
+ * process (src/main.cu:101-139); an ensemble runs every disk's step order
+ * (main.cu:101-139 per disk) with each phase one launch over all disks, and a
+ * whole step replayed as one CUDA graph.  Disks share dt, theta, softening,
+ * star mass, collision radius, restitution, drag and precision (the
+ * nbody_sim_params); each has its own body count and perturber
+ * (src/physics/Perturber.h:39-58).  A body feels only its own disk, its star
+ * and its perturber: results equal those of separate nbody_sim runs up to the
+ * float summation order of the tree walk. */
+typedef struct nbody_disk_spec {
+  int n;                      /* bodies, >= 2 */
+  int perturber_enabled;
+  float perturber_mass_mjup;
+  float perturber_radius_au;
+  float perturber_phase0;
+} nbody_disk_spec;
+
+typedef struct nbody_ensemble nbody_ensemble;
+
+int nbody_ensemble_create(const nbody_sim_params* p, const nbody_disk_spec* disks, int n_disks,
+                          nbody_ensemble** out);
+int nbody_ensemble_destroy(nbody_ensemble* e);
+int nbody_ensemble_set_stream(nbody_ensemble* e, void* cuda_stream);
+/* State of all disks concatenated in disk order (disk 0's bodies first),
+ * host or device SoA; computes the forces at t = 0. */
+int nbody_ensemble_set_state(nbody_ensemble* e, const float* x, const float* y, const float* z,
+                             const float* vx, const float* vy, const float* vz,
+                             const float* mass, int on_device);
+int nbody_ensemble_set_state_f64(nbody_ensemble* e, const double* x, const double* y,
+                                 const double* z, const double* vx, const double* vy,
+                                 const double* vz, const float* mass, int on_device);
+/* nsteps steps of every disk; asynchronous on the ensemble's stream. */
+int nbody_ensemble_step(nbody_ensemble* e, int nsteps);
+int nbody_ensemble_sync(nbody_ensemble* e);
+int nbody_ensemble_get_state(nbody_ensemble* e, float* x, float* y, float* z, float* vx,
+                             float* vy, float* vz, float* ax, float* ay, float* az,
+                             int on_device);
+int nbody_ensemble_get_state_f64(nbody_ensemble* e, double* x, double* y, double* z,
+                                 double* vx, double* vy, double* vz, float* ax, float* ay,
+                                 float* az, int on_device);
+/* Host round trip, as nbody_sim_step_host: loads x..vz (double) and the
+ * accelerations of that state, advances nsteps without recomputing the
+ * starting forces, writes x..az back.  The step counter continues across
+ * calls.  Synchronous. */
+int nbody_ensemble_step_host(nbody_ensemble* e, double* x, double* y, double* z, double* vx,
+                             double* vy, double* vz, float* ax, float* ay, float* az,
+                             const float* mass, int nsteps);
+/* Force-evaluation autotuner: times one force evaluation of the current state
+ * for each (targets_per_lane, leaf_max) candidate (candidates[2k],
+ * candidates[2k+1]; NULL = the built-in list) and keeps the fastest.  The
+ * forces are recomputed with the kept setting, so the state is unchanged.
+ * Needs set_state first.  ms_out (optional) receives each candidate's time. */
+int nbody_ensemble_autotune(nbody_ensemble* e, const int* candidates, int n_candidates,
+                            float* ms_out);
+/* 0: launch the step's kernels one by one; 1 (default): replay CUDA graphs. */
+int nbody_ensemble_set_graphs(nbody_ensemble* e, int on);
+typedef struct nbody_ensemble_stats {
+  int n_disks;
+  int n_total;
+  int steps_done;
+  int targets_per_lane;
+  int leaf_max;
+  int status;
+  unsigned long long interactions;  /* accepted interactions of the last walk */
+  unsigned long long launches;      /* kernels launched so far (graph nodes included) */
+  unsigned long long graph_launches;
+} nbody_ensemble_stats;
+int nbody_ensemble_stats_get(nbody_ensemble* e, nbody_ensemble_stats* out);
+
 /* ------------------------------------------------------ initial disks --- */
 
 /* Synthetic disk of n bodies: star mass at the origin, disk in XZ, +Y pole;

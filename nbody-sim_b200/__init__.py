@@ -24,6 +24,8 @@ Python-side names mirror the reference API they wrap:
 * :func:`detect_aggregates` -- include/Aggregate.h:17-18
 * :class:`OutputWriter` -- include/OutputWriter.h:15-51
 * :class:`Sim` -- the step loop of src/main.cu:85-139 resident on the GPU
+* :class:`Ensemble` -- many independent disks, each with main.cu's step loop,
+  stepped together (one launch per phase over all disks, CUDA graphs)
 """
 from __future__ import annotations
 
@@ -44,6 +46,8 @@ NBODY_ERR_TIMEOUT = 4
 NBODY_ERR_IO = 5
 NBODY_ERR_CONFIG = 6
 NBODY_ERR_STATE = 7
+NBODY_STATE_F32 = 0
+NBODY_STATE_F64 = 1
 FOF_NOALLOC_MAX_N = 32768
 STATE_F32 = 0
 STATE_F64 = 1
@@ -134,6 +138,19 @@ class nbody_sim_stats(C.Structure):
                 ("walk_groups", C.c_ulonglong)]
 
 
+class nbody_disk_spec(C.Structure):
+    _fields_ = [("n", C.c_int), ("perturber_enabled", C.c_int),
+                ("perturber_mass_mjup", C.c_float), ("perturber_radius_au", C.c_float),
+                ("perturber_phase0", C.c_float)]
+
+
+class nbody_ensemble_stats(C.Structure):
+    _fields_ = [("n_disks", C.c_int), ("n_total", C.c_int), ("steps_done", C.c_int),
+                ("targets_per_lane", C.c_int), ("leaf_max", C.c_int), ("status", C.c_int),
+                ("interactions", C.c_ulonglong), ("launches", C.c_ulonglong),
+                ("graph_launches", C.c_ulonglong)]
+
+
 # (name, restype, argtypes): every symbol include/nbody_b200.h declares
 SIGNATURES = [
     ("nbody_last_error", C.c_char_p, []),
@@ -192,6 +209,20 @@ SIGNATURES = [
     ("nbody_sim_set_profiling", C.c_int, [_VP, C.c_int]),
     ("nbody_sim_profile_get", C.c_int, [_VP, C.POINTER(nbody_sim_profile), C.c_int]),
     ("nbody_sim_step_host", C.c_int, [_VP] + [_VP] * 10 + [C.c_int]),
+    ("nbody_ensemble_create", C.c_int, [C.POINTER(nbody_sim_params), C.POINTER(nbody_disk_spec),
+                                        C.c_int, C.POINTER(_VP)]),
+    ("nbody_ensemble_destroy", C.c_int, [_VP]),
+    ("nbody_ensemble_set_stream", C.c_int, [_VP, _VP]),
+    ("nbody_ensemble_set_state", C.c_int, [_VP] + [_VP] * 7 + [C.c_int]),
+    ("nbody_ensemble_set_state_f64", C.c_int, [_VP] + [_VP] * 7 + [C.c_int]),
+    ("nbody_ensemble_step", C.c_int, [_VP, C.c_int]),
+    ("nbody_ensemble_sync", C.c_int, [_VP]),
+    ("nbody_ensemble_get_state", C.c_int, [_VP] + [_VP] * 9 + [C.c_int]),
+    ("nbody_ensemble_get_state_f64", C.c_int, [_VP] + [_VP] * 9 + [C.c_int]),
+    ("nbody_ensemble_step_host", C.c_int, [_VP] + [_VP] * 10 + [C.c_int]),
+    ("nbody_ensemble_autotune", C.c_int, [_VP, _VP, C.c_int, _VP]),
+    ("nbody_ensemble_set_graphs", C.c_int, [_VP, C.c_int]),
+    ("nbody_ensemble_stats_get", C.c_int, [_VP, C.POINTER(nbody_ensemble_stats)]),
     ("nbody_make_disk", C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                   C.c_double, C.c_uint64, _D, _D, _D, _D, _D, _D]),
 ]
@@ -630,6 +661,108 @@ class Sim:
         keys = ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")
         _check(lib.nbody_sim_step_host(self.h, *[st[k].ctypes.data for k in keys],
                                        mass.ctypes.data, nsteps))
+
+
+class Ensemble:
+    """Many independent disks stepped together (nbody_ensemble_* in include/nbody_b200.h).
+
+    ``disks`` is a list of dicts with keys n, perturber_enabled,
+    perturber_mass_mjup, perturber_radius_au, perturber_phase0.  State arrays
+    hold every disk's bodies concatenated in disk order.
+    """
+
+    def __init__(self, params: nbody_sim_params, disks):
+        specs = (nbody_disk_spec * len(disks))()
+        for k, d in enumerate(disks):
+            specs[k].n = int(d["n"])
+            specs[k].perturber_enabled = int(d.get("perturber_enabled", 0))
+            specs[k].perturber_mass_mjup = float(d.get("perturber_mass_mjup", 1.0))
+            specs[k].perturber_radius_au = float(d.get("perturber_radius_au", 5.2))
+            specs[k].perturber_phase0 = float(d.get("perturber_phase0", 0.0))
+        h = _VP()
+        _check(lib.nbody_ensemble_create(C.byref(params), specs, len(disks), C.byref(h)))
+        self.h, self.params = h, params
+        self.sizes = [int(d["n"]) for d in disks]
+        self.offsets = np.concatenate([[0], np.cumsum(self.sizes)]).astype(np.int64)
+        self.n = int(self.offsets[-1])
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.nbody_ensemble_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr: int):
+        _check(lib.nbody_ensemble_set_stream(self.h, stream_ptr))
+
+    def set_state(self, x, y, z, vx, vy, vz, mass):
+        """Host numpy (float32 or float64) or CUDA torch tensors, disk order."""
+        arrs = [x, y, z, vx, vy, vz]
+        on_dev = hasattr(x, "data_ptr")
+        if on_dev:
+            dbl = str(x.dtype) == "torch.float64"
+            ptrs = [a.data_ptr() for a in arrs]
+            mptr = mass.data_ptr()
+            keep = None
+        else:
+            dbl = np.asarray(x).dtype == np.float64
+            keep = [np.ascontiguousarray(a, np.float64 if dbl else np.float32) for a in arrs]
+            km = np.ascontiguousarray(mass, np.float32)
+            ptrs = [a.ctypes.data for a in keep]
+            mptr = km.ctypes.data
+        fn = lib.nbody_ensemble_set_state_f64 if dbl else lib.nbody_ensemble_set_state
+        _check(fn(self.h, *ptrs, mptr, int(on_dev)))
+        del keep
+
+    def step(self, nsteps: int = 1):
+        _check(lib.nbody_ensemble_step(self.h, nsteps))
+
+    def sync(self):
+        _check(lib.nbody_ensemble_sync(self.h))
+
+    def get_state(self, double: bool = False, accel: bool = True):
+        """Host numpy state in disk order: dict x..vz (+ ax..az)."""
+        n = self.n
+        dt = np.float64 if double else np.float32
+        out = {k: np.zeros(n, dt) for k in ("x", "y", "z", "vx", "vy", "vz")}
+        acc = {k: np.zeros(n, np.float32) for k in ("ax", "ay", "az")} if accel else None
+        aptr = [acc[k].ctypes.data for k in ("ax", "ay", "az")] if accel else [None] * 3
+        fn = lib.nbody_ensemble_get_state_f64 if double else lib.nbody_ensemble_get_state
+        _check(fn(self.h, *[out[k].ctypes.data for k in out], *aptr, 0))
+        if accel:
+            out.update(acc)
+        return out
+
+    def step_host(self, st: dict, mass, nsteps: int = 1):
+        """Host round trip on float64 x..vz and float32 ax..az arrays, in place."""
+        keys = ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")
+        _check(lib.nbody_ensemble_step_host(self.h, *[st[k].ctypes.data for k in keys],
+                                            mass.ctypes.data, nsteps))
+
+    def autotune(self, candidates=None):
+        """Times one force evaluation per (targets_per_lane, leaf_max); keeps the fastest.
+
+        Returns [(tpl, leaf_max, ms), ...]."""
+        if candidates is None:
+            candidates = [(1, 4), (1, 8), (1, 16), (2, 8), (2, 16)]
+        flat = np.ascontiguousarray(np.array(candidates, np.int32).reshape(-1))
+        ms = np.zeros(len(candidates), np.float32)
+        _check(lib.nbody_ensemble_autotune(self.h, flat.ctypes.data, len(candidates),
+                                           ms.ctypes.data))
+        return [(int(a), int(b), float(t)) for (a, b), t in zip(candidates, ms)]
+
+    def set_graphs(self, on: bool = True):
+        _check(lib.nbody_ensemble_set_graphs(self.h, int(on)))
+
+    def stats(self) -> nbody_ensemble_stats:
+        st = nbody_ensemble_stats()
+        _check(lib.nbody_ensemble_stats_get(self.h, C.byref(st)))
+        return st
 
 
 # --------------------------------------------------------- initial disks

@@ -81,7 +81,27 @@ void launch_keys(TreeWork& w, const T* x, const T* y, const T* z, int n, cudaStr
 // body4[s] = (x,y,z,m)[perm[s]] for float inputs in caller order.
 void launch_gather_body4(TreeWork& w, const float* x, const float* y, const float* z,
                          const float* m, int n, cudaStream_t s);
-// Karras radix tree over the sorted keys.
+// Karras radix tree over sorted keys that use their low key_bits bits.
+template <typename K>
+void launch_karras(TreeWork& w, const K* keys, int n, int key_bits, cudaStream_t s);
+// Octree, FP64 moments and target groups over a Karras tree whose keys carry
+// a disk index in the disk_bits above the 30 Morton bits: one root slot per
+// disk (slots 0..n_roots-1), geoms[d] the root cube of disk d, group_disk
+// (optional) receives each group's disk.
+template <typename K>
+void launch_octree(TreeWork& w, const K* keys, int n, int disk_bits, int n_roots,
+                   const TreeGeom* geoms, int* group_disk, const double* xd, const double* yd,
+                   const double* zd, cudaStream_t s);
+// Ensembles: root cube of every disk from its encoded bbox (6 words per
+// disk); bbox accumulators reset for n_disks; composite keys
+// (disk << 30 | Morton) with disk[i] the body's disk.
+void launch_geoms(const unsigned long long* enc, TreeGeom* geoms, int n_disks, cudaStream_t s);
+void launch_bbox_reset_n(unsigned long long* enc, int n_disks, cudaStream_t s);
+template <typename T>
+void launch_keys_multi(const T* x, const T* y, const T* z, const int* disk, int n,
+                       const TreeGeom* geoms, uint64_t* keys, uint32_t* perm, int* status,
+                       cudaStream_t s);
+// Single disk: Karras radix tree over w.keys.
 void launch_build_topology(TreeWork& w, int n, cudaStream_t s);
 // FP64 moments, compressed octree (contiguous children) and the target
 // groups.  xd/yd/zd (optional, key order) give FP64 positions for the
@@ -90,7 +110,11 @@ void launch_build_moments(TreeWork& w, int n, const double* xd, const double* yd
                           const double* zd, cudaStream_t s);
 
 size_t radix_sort_count_words(int n);
-void radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt,
+// Stable LSD sort of (key, value) by the low `bits` bits of the keys; K is
+// uint32_t (single disk, 30-bit Morton keys) or uint64_t (ensemble: disk
+// index above the 30 Morton bits).
+template <typename K>
+void radix_sort_pairs(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt,
                       uint32_t* counts, int n, int bits, cudaStream_t s);
 size_t scan_tmp_words(int n);
 void scan_exclusive_u32(uint32_t* data, int n, uint32_t* tmp, cudaStream_t s);
@@ -120,6 +144,11 @@ struct WalkArgs {
   int* work;
   int* status;
   int targets_per_lane;   // 1 or 2: groups of up to 32 or 64 bodies
+  // ensembles: a group's walk starts at its disk's root slot, and pert holds
+  // n_disks perturbers per force evaluation, the current one at *pert_step
+  const int* group_disk;  // nullptr: one disk
+  int n_disks;
+  const int* pert_step;   // nullptr: pert points at the current entries
 };
 int walk_spill_slots(int device);  // warps resident at once (spill area slots)
 void launch_walk(const WalkArgs& a, cudaStream_t s);
@@ -138,6 +167,7 @@ struct NeighborArgs {
   int spill_cap;
   int* work;
   int* status;
+  const int* group_disk;  // nullptr: one disk (root slot 0)
 };
 // Two-pass impulse (BHTree.cu:620-686): dv[s] for body s in key order.
 // v* are velocities in key order, or in caller order when vmap != nullptr

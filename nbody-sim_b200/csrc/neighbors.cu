@@ -94,6 +94,7 @@ k_neighbors(const NeighborArgs a, float radius, CollideOut co, FofOut fo) {
     g = __shfl_sync(kFull, g, 0);
     if (g >= n_groups) break;
     const int2 grp = a.groups[g];
+    const int disk = a.group_disk ? a.group_disk[g] : 0;
     // groups hold up to 64 bodies; search them 32 (one per lane) at a time
     for (int c0 = 0; c0 < grp.y; c0 += 32) {
     const int2 gr = make_int2(grp.x + c0, min(32, grp.y - c0));
@@ -114,7 +115,7 @@ k_neighbors(const NeighborArgs a, float radius, CollideOut co, FofOut fo) {
 
     int top = 1, spilled = 0;
     bool overflow = false;
-    if (lane == 0) w.stk[0] = 0;
+    if (lane == 0) w.stk[0] = disk;  // root slot of the group's disk
     __syncwarp();
     while (true) {
       if (top == 0) {

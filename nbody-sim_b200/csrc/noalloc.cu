@@ -24,7 +24,7 @@ constexpr size_t kAlign = 256;
 
 constexpr size_t al(size_t b) { return (b + kAlign - 1) / kAlign * kAlign; }
 constexpr size_t kNb = 2 * (size_t)kMaxN;
-constexpr size_t kCountWords = 4096;  // >= radix_sort_count_words(kMaxN) = 2050
+constexpr size_t kCountWords = 4096;  // >= 2050 words the 32-bit-key sort of kMaxN uses
 constexpr size_t kScanWords = 4096;   // >= scan_tmp_words(2 kMaxN) = 17
 constexpr size_t kMomTiles = 2 * ((size_t)kMaxN / kMomentTile + 2) + 8;
 

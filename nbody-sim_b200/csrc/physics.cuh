@@ -27,6 +27,30 @@ __device__ __forceinline__ void gas_drag(R xi, R zi, R& vx, R& vy, R& vz, R deca
   vy = v_y_new;
 }
 
+// FP64 state (the engine's own precision mode, no reference kernel to match):
+// every multiply-add is an explicit fma or a separately rounded product, so
+// each kernel that inlines it rounds the same way whatever the compiler's
+// contraction choices (the fused kick of a step boundary and the split
+// closing/opening kicks of two calls then agree bit for bit).
+template <>
+__device__ __forceinline__ void gas_drag<double>(double xi, double zi, double& vx, double& vy,
+                                                 double& vz, double decay, double star_mass) {
+  const double r_xz2 = fma(xi, xi, __dmul_rn(zi, zi));
+  if (r_xz2 < 1e-12) return;
+  const double inv_r = 1.0 / sqrt(r_xz2);
+  const double vxi = vx, vyi = vy, vzi = vz;
+  const double v_r = __dmul_rn(fma(vxi, xi, __dmul_rn(vzi, zi)), inv_r);
+  const double v_phi = __dmul_rn(fma(vxi, -zi, __dmul_rn(vzi, xi)), inv_r);
+  const double v_kep_mag = sqrt(__dmul_rn(star_mass, inv_r));
+  const double v_kep = (v_phi >= 0.0) ? v_kep_mag : -v_kep_mag;
+  const double v_r_new = __dmul_rn(v_r, decay);
+  const double v_phi_new = fma(v_phi - v_kep, decay, v_kep);
+  const double ux = __dmul_rn(xi, inv_r), uz = __dmul_rn(zi, inv_r);
+  vx = fma(v_r_new, ux, __dmul_rn(v_phi_new, -uz));
+  vz = fma(v_r_new, uz, __dmul_rn(v_phi_new, ux));
+  vy = __dmul_rn(vyi, decay);
+}
+
 // Softened star pull -M x / (|x|^2 + eps^2)^(3/2) (BHTree.cu:547-553 form).
 template <typename R>
 __device__ __forceinline__ void star_accel(R x, R y, R z, R eps, R star_mass, R& ax, R& ay,
@@ -38,6 +62,18 @@ __device__ __forceinline__ void star_accel(R x, R y, R z, R eps, R star_mass, R&
   ax = f * dx;
   ay = f * dy;
   az = f * dz;
+}
+
+template <>
+__device__ __forceinline__ void star_accel<double>(double x, double y, double z, double eps,
+                                                   double star_mass, double& ax, double& ay,
+                                                   double& az) {
+  const double r2 = fma(x, x, fma(y, y, fma(z, z, __dmul_rn(eps, eps))));
+  const double r = sqrt(r2);
+  const double f = star_mass / __dmul_rn(r2, r);
+  ax = __dmul_rn(f, -x);
+  ay = __dmul_rn(f, -y);
+  az = __dmul_rn(f, -z);
 }
 
 }  // namespace nb

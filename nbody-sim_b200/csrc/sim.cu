@@ -35,6 +35,7 @@ struct StateArrays {
   R* v[6];  // x y z vx vy vz
   float* m;
   int* id;
+  int* disk;  // ensembles: the body's disk (nullptr for one disk)
 };
 
 template <typename Tin, typename Tout>
@@ -66,6 +67,7 @@ k_permute(const uint32_t* __restrict__ perm, StateArrays<R> in, StateArrays<R> o
     const float m = in.m[o];
     out.m[s] = m;
     out.id[s] = in.id[o];
+    if (in.disk) out.disk[s] = in.disk[o];
     body4[s] = make_float4((float)q[0], (float)q[1], (float)q[2], m);
   }
 }
@@ -90,7 +92,7 @@ struct StreamArgs {
 
 // Fused step boundary.  kEnd: dv + K2 + drag (main.cu:131-139);
 // kBegin: K1 + drift (main.cu:104-107) + bbox of the new positions.
-template <typename R, bool kEnd, bool kBegin>
+template <typename R, bool kEnd, bool kBegin, bool kMulti = false>
 __global__ void __launch_bounds__(kThreads) k_stream(StateArrays<R> st, int n, StreamArgs a) {
   double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
   for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
@@ -133,14 +135,39 @@ __global__ void __launch_bounds__(kThreads) k_stream(StateArrays<R> st, int n, S
         vx = fma(ax, (R)a.dth, vx); vy = fma(ay, (R)a.dth, vy); vz = fma(az, (R)a.dth, vz);
         x = fma(vx, (R)a.dt, x); y = fma(vy, (R)a.dt, y); z = fma(vz, (R)a.dt, z);
       }
-      lo[0] = fmin(lo[0], (double)x); hi[0] = fmax(hi[0], (double)x);
-      lo[1] = fmin(lo[1], (double)y); hi[1] = fmax(hi[1], (double)y);
-      lo[2] = fmin(lo[2], (double)z); hi[2] = fmax(hi[2], (double)z);
+      if (kMulti) {
+        // per-disk bbox: one warp-wide reduction when the warp's bodies share
+        // a disk (the common case), per-lane atomics at a disk boundary
+        const int d = st.disk[s];
+        const unsigned act = __activemask();
+        const int d0 = __shfl_sync(act, d, __ffs(act) - 1);
+        const bool same = __all_sync(act, d == d0) && act == kFull;
+        unsigned long long* bb = a.bbox + 6 * d;
+        if (same) {
+          double v6[6] = {(double)x, (double)y, (double)z, (double)x, (double)y, (double)z};
+#pragma unroll
+          for (int k = 0; k < 3; ++k) { v6[k] = warp_min(v6[k]); v6[3 + k] = warp_max(v6[3 + k]); }
+          if ((threadIdx.x & 31) == 0) {
+            for (int k = 0; k < 3; ++k) {
+              atomicMin(bb + k, ordered_bits(v6[k]));
+              atomicMax(bb + 3 + k, ordered_bits(v6[3 + k]));
+            }
+          }
+        } else {
+          atomicMin(bb + 0, ordered_bits((double)x)); atomicMax(bb + 3, ordered_bits((double)x));
+          atomicMin(bb + 1, ordered_bits((double)y)); atomicMax(bb + 4, ordered_bits((double)y));
+          atomicMin(bb + 2, ordered_bits((double)z)); atomicMax(bb + 5, ordered_bits((double)z));
+        }
+      } else {
+        lo[0] = fmin(lo[0], (double)x); hi[0] = fmax(hi[0], (double)x);
+        lo[1] = fmin(lo[1], (double)y); hi[1] = fmax(hi[1], (double)y);
+        lo[2] = fmin(lo[2], (double)z); hi[2] = fmax(hi[2], (double)z);
+      }
       st.v[0][s] = x; st.v[1][s] = y; st.v[2][s] = z;
     }
     st.v[3][s] = vx; st.v[4][s] = vy; st.v[5][s] = vz;
   }
-  if (kBegin) {
+  if (kBegin && !kMulti) {
     __shared__ double sb[6][kThreads / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -196,6 +223,39 @@ __global__ void k_scatter_labels(const int* __restrict__ in_l, const uint16_t* _
   }
 }
 
+// Ensemble: each body's disk from the per-disk offsets (binary search).
+__global__ void k_disk_of(const int* __restrict__ offsets, int n_disks, int n,
+                          int* __restrict__ disk) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    int lo = 0, hi = n_disks - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (offsets[mid] <= i) lo = mid;
+      else hi = mid - 1;
+    }
+    disk[i] = lo;
+  }
+}
+
+// Per-disk bbox of the current positions (warp-aggregated atomics).
+template <typename R>
+__global__ void __launch_bounds__(kThreads)
+k_bbox_multi(StateArrays<R> st, int n, unsigned long long* __restrict__ bbox) {
+  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
+       s += (long long)gridDim.x * blockDim.x) {
+    const double p3[3] = {(double)st.v[0][s], (double)st.v[1][s], (double)st.v[2][s]};
+    unsigned long long* bb = bbox + 6 * st.disk[s];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      atomicMin(bb + k, ordered_bits(p3[k]));
+      atomicMax(bb + 3 + k, ordered_bits(p3[k]));
+    }
+  }
+}
+
+__global__ void k_increment(int* c) { *c += 1; }
+
 template <typename T>
 T* dalloc(size_t count, const char* what) {
   T* p = nullptr;
@@ -204,6 +264,60 @@ T* dalloc(size_t count, const char* what) {
 }
 
 }  // namespace
+
+// Writes the state back in the caller's order (by id) as float or double,
+// with the accelerations (plus the star term the FP64 walk leaves out), into
+// device buffers or, through stream-ordered temporaries, host buffers.
+template <typename R>
+void state_out(const StateArrays<R>& a, int n, const float* ax, const float* ay,
+               const float* az, float eps, float star_mass, void* const* v, bool as_double,
+               float* const* acc, bool on_device, cudaStream_t st) {
+  const size_t esz = as_double ? sizeof(double) : sizeof(float);
+  std::vector<void*> dst(6);
+  std::vector<void*> tmp;
+  for (int k = 0; k < 6; ++k) {
+    if (on_device) {
+      dst[k] = v[k];
+    } else {
+      void* t = nullptr;
+      check(cudaMallocAsync(&t, esz * n, st), "get_state temp");
+      tmp.push_back(t);
+      dst[k] = t;
+    }
+  }
+  float* da[3] = {nullptr, nullptr, nullptr};
+  if (acc && acc[0]) {
+    for (int k = 0; k < 3; ++k) {
+      if (on_device) {
+        da[k] = acc[k];
+      } else {
+        void* t = nullptr;
+        check(cudaMallocAsync(&t, sizeof(float) * n, st), "get_state temp");
+        tmp.push_back(t);
+        da[k] = (float*)t;
+      }
+    }
+  }
+  if (as_double)
+    k_unsort<R, double><<<stream_grid(n), kThreads, 0, st>>>(
+        a, n, (double*)dst[0], (double*)dst[1], (double*)dst[2], (double*)dst[3],
+        (double*)dst[4], (double*)dst[5], ax, ay, az, da[0], da[1], da[2], eps, star_mass);
+  else
+    k_unsort<R, float><<<stream_grid(n), kThreads, 0, st>>>(
+        a, n, (float*)dst[0], (float*)dst[1], (float*)dst[2], (float*)dst[3], (float*)dst[4],
+        (float*)dst[5], ax, ay, az, da[0], da[1], da[2], eps, star_mass);
+  check(cudaGetLastError(), "k_unsort launch");
+  if (!on_device) {
+    for (int k = 0; k < 6; ++k)
+      check(cudaMemcpyAsync(v[k], dst[k], esz * n, cudaMemcpyDeviceToHost, st), "state D2H");
+    if (da[0])
+      for (int k = 0; k < 3; ++k)
+        check(cudaMemcpyAsync(acc[k], da[k], sizeof(float) * n, cudaMemcpyDeviceToHost, st),
+              "accel D2H");
+    for (void* t : tmp) check(cudaFreeAsync(t, st), "get_state free");
+  }
+  check(cudaStreamSynchronize(st), "get_state sync");
+}
 
 struct SimBase {
   virtual ~SimBase() {}
@@ -554,54 +668,8 @@ struct SimImpl : SimBase {
   }
 
   void get_state(void* const* v, bool as_double, float* const* acc, bool on_device) override {
-    // unsort into device buffers (caller memory if on device, else staging)
-    const size_t esz = as_double ? sizeof(double) : sizeof(float);
-    std::vector<void*> dst(6);
-    std::vector<void*> tmp;
-    for (int k = 0; k < 6; ++k) {
-      if (on_device) {
-        dst[k] = v[k];
-      } else {
-        void* t = nullptr;
-        check(cudaMallocAsync(&t, esz * n, st), "get_state temp");
-        tmp.push_back(t);
-        dst[k] = t;
-      }
-    }
-    float* da[3] = {nullptr, nullptr, nullptr};
-    if (acc && acc[0]) {
-      for (int k = 0; k < 3; ++k) {
-        if (on_device) {
-          da[k] = acc[k];
-        } else {
-          void* t = nullptr;
-          check(cudaMallocAsync(&t, sizeof(float) * n, st), "get_state temp");
-          tmp.push_back(t);
-          da[k] = (float*)t;
-        }
-      }
-    }
-    if (as_double)
-      k_unsort<R, double><<<stream_grid(n), kThreads, 0, st>>>(
-          s[cur], n, (double*)dst[0], (double*)dst[1], (double*)dst[2], (double*)dst[3],
-          (double*)dst[4], (double*)dst[5], ax, ay, az, da[0], da[1], da[2], p.softening,
-          p.star_mass);
-    else
-      k_unsort<R, float><<<stream_grid(n), kThreads, 0, st>>>(
-          s[cur], n, (float*)dst[0], (float*)dst[1], (float*)dst[2], (float*)dst[3],
-          (float*)dst[4], (float*)dst[5], ax, ay, az, da[0], da[1], da[2], p.softening,
-          p.star_mass);
-    check(cudaGetLastError(), "k_unsort launch");
-    if (!on_device) {
-      for (int k = 0; k < 6; ++k)
-        check(cudaMemcpyAsync(v[k], dst[k], esz * n, cudaMemcpyDeviceToHost, st), "state D2H");
-      if (da[0])
-        for (int k = 0; k < 3; ++k)
-          check(cudaMemcpyAsync(acc[k], da[k], sizeof(float) * n, cudaMemcpyDeviceToHost, st),
-                "accel D2H");
-      for (void* t : tmp) check(cudaFreeAsync(t, st), "get_state free");
-    }
-    check(cudaStreamSynchronize(st), "get_state sync");
+    state_out<R>(s[cur], n, ax, ay, az, p.softening, p.star_mass, v, as_double, acc, on_device,
+                 st);
   }
 };
 
@@ -802,6 +870,604 @@ int nbody_sim_step_host(nbody_sim* s, float* x, float* y, float* z, float* vx, f
     void* o[6] = {x, y, z, vx, vy, vz};
     float* a[3] = {ax, ay, az};
     b->get_state(o, false, a, false);            // copyToCPU
+  })
+}
+
+}  // extern "C"
+
+
+// ======================================================================
+// Ensemble: independent disks of uneven size advanced together, every phase
+// one launch over all disks.  Bodies carry their disk index; the Morton key
+// gets the disk index above its 30 bits, so one radix sort orders all disks
+// and the Karras tree splits by disk first.  Each disk is its own octree
+// (root slot = disk index, own root cube), warp groups never span disks, and
+// every group walks its own disk's tree with its own perturber.  A step is
+// captured once per variant as a CUDA graph and replayed; the perturber
+// table row it reads is a device counter that the step increments.
+namespace nb {
+
+template <typename R>
+struct EnsembleImpl;
+
+struct EnsembleBase {
+  virtual ~EnsembleBase() {}
+  nbody_sim_params p{};
+  int D = 0, n = 0;
+  cudaStream_t st = 0;
+  bool has_state = false;
+  int steps_done = 0;
+  unsigned long long launches = 0, graph_launches = 0;
+  virtual void set_stream(cudaStream_t s) = 0;
+  virtual void set_state(const void* const* v, bool is_double, const float* mass,
+                         bool on_device, bool forces = true) = 0;
+  virtual void load_accel(const float* const* acc) = 0;
+  virtual void step(int nsteps) = 0;
+  virtual void get_state(void* const* v, bool as_double, float* const* a, bool on_device) = 0;
+  virtual void autotune(const int* cand, int nc, float* ms) = 0;
+  virtual void set_graphs(bool on) = 0;
+  virtual void stats(nbody_ensemble_stats* out) = 0;
+  virtual void sync() = 0;
+};
+
+template <typename R>
+struct EnsembleImpl : EnsembleBase {
+  int disk_bits = 0;
+  std::vector<int> off;
+  std::vector<nbody_perturber> pert;
+  bool own_stream = false;
+  TreeWork tw;
+  uint64_t *keys64 = nullptr, *keys64_alt = nullptr;
+  StateArrays<R> s[2]{};
+  int cur = 0;
+  float *ax = nullptr, *ay = nullptr, *az = nullptr, *dvx = nullptr, *dvy = nullptr,
+        *dvz = nullptr, *vf = nullptr;
+  TreeGeom* geoms = nullptr;
+  unsigned long long* bbox = nullptr;
+  int* group_disk = nullptr;
+  int* d_off = nullptr;
+  float4* pert_tab = nullptr;
+  int pert_rows = 0;
+  int* pert_step = nullptr;
+  int* spill = nullptr;
+  int spill_cap = 4096;
+  int* work = nullptr;
+  unsigned long long* inter = nullptr;
+  unsigned long long* counters = nullptr;
+  void* staging = nullptr;
+  bool use_graphs = true;
+  cudaStream_t cap_st = nullptr;
+  // [first step of a call?][state buffer at step start]
+  cudaGraphExec_t gx[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  unsigned long long g_kernels[2][2] = {{0, 0}, {0, 0}};
+
+  EnsembleImpl(const nbody_sim_params& prm, const nbody_disk_spec* disks, int nd) {
+    p = prm;
+    if (p.leaf_max <= 0) p.leaf_max = 8;
+    if (p.targets_per_lane != 2) p.targets_per_lane = 1;
+    D = nd;
+    while ((1 << disk_bits) < D) ++disk_bits;
+    off.assign(D + 1, 0);
+    pert.resize(D);
+    for (int d = 0; d < D; ++d) {
+      off[d + 1] = off[d] + disks[d].n;
+      nbody_config c;
+      nbody_config_defaults(&c);
+      c.perturber_enabled = disks[d].perturber_enabled;
+      c.perturber_mass_mjup = disks[d].perturber_mass_mjup;
+      c.perturber_radius_AU = disks[d].perturber_radius_au;
+      c.perturber_phase0 = disks[d].perturber_phase0;
+      c.star_mass_msun = p.star_mass;
+      nbody_perturber_make(&c, &pert[d]);
+    }
+    n = off[D];
+    check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "ensemble stream");
+    own_stream = true;
+    tree_alloc(tw, n);
+    tw.group_max = 32 * p.targets_per_lane;
+    keys64 = dalloc<uint64_t>(n, "keys64");
+    keys64_alt = dalloc<uint64_t>(n, "keys64_alt");
+    for (int b = 0; b < 2; ++b) {
+      for (int k = 0; k < 6; ++k) s[b].v[k] = dalloc<R>(n, "state");
+      s[b].m = dalloc<float>(n, "mass");
+      s[b].id = dalloc<int>(n, "id");
+      s[b].disk = dalloc<int>(n, "disk");
+    }
+    ax = dalloc<float>(n, "ax"); ay = dalloc<float>(n, "ay"); az = dalloc<float>(n, "az");
+    dvx = dalloc<float>(n, "dvx"); dvy = dalloc<float>(n, "dvy"); dvz = dalloc<float>(n, "dvz");
+    if (sizeof(R) == 8) vf = dalloc<float>(3 * (size_t)n, "velocity scratch");
+    geoms = dalloc<TreeGeom>(D, "geoms");
+    bbox = dalloc<unsigned long long>(6 * (size_t)D, "bboxes");
+    group_disk = dalloc<int>(n, "group disk");
+    d_off = dalloc<int>(D + 1, "offsets");
+    check(cudaMemcpy(d_off, off.data(), sizeof(int) * (D + 1), cudaMemcpyHostToDevice),
+          "offsets");
+    pert_step = dalloc<int>(1, "perturber row");
+    spill = dalloc<int>((size_t)walk_spill_slots(0) * spill_cap, "walk spill");
+    work = dalloc<int>(1, "work");
+    inter = dalloc<unsigned long long>(1, "inter");
+    counters = dalloc<unsigned long long>(3, "counters");
+    staging = dalloc<double>(n, "staging");
+    reserve_perturber_rows(64);
+  }
+
+  ~EnsembleImpl() override {
+    if (st) cudaStreamSynchronize(st);
+    drop_graphs();
+    for (int b = 0; b < 2; ++b) {
+      for (int k = 0; k < 6; ++k) cudaFree(s[b].v[k]);
+      cudaFree(s[b].m); cudaFree(s[b].id); cudaFree(s[b].disk);
+    }
+    void* ptrs[] = {keys64, keys64_alt, ax,       ay,        az,    dvx,      dvy,
+                    dvz,    vf,         geoms,    bbox,      group_disk, d_off, pert_tab,
+                    pert_step, spill,   work,     inter,     counters,   staging};
+    for (void* q : ptrs)
+      if (q) cudaFree(q);
+    tree_free(tw);
+    if (cap_st) cudaStreamDestroy(cap_st);
+    if (own_stream && st) cudaStreamDestroy(st);
+  }
+
+  void drop_graphs() {
+    for (auto& row : gx)
+      for (auto& g : row)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  }
+
+  void set_stream(cudaStream_t stream) override {
+    check(cudaStreamSynchronize(st), "ensemble sync");
+    drop_graphs();
+    if (own_stream) cudaStreamDestroy(st);
+    own_stream = false;
+    st = stream;
+  }
+
+  void set_graphs(bool on) override {
+    if (!on) drop_graphs();
+    use_graphs = on;
+  }
+
+  void reserve_perturber_rows(int rows) {
+    if (rows <= pert_rows) return;
+    check(cudaStreamSynchronize(st), "perturber table sync");
+    if (pert_tab) cudaFree(pert_tab);
+    pert_rows = std::max(rows, 2 * pert_rows);
+    pert_tab = dalloc<float4>((size_t)pert_rows * D, "perturber table");
+    drop_graphs();  // the captured walks hold the old table
+  }
+
+  // Row k: every disk's perturber at t = (k0 + k) dt (updatePerturber,
+  // Perturber.h:60-66, on the host as in the reference), mass 0 when off.
+  void upload_perturbers(int k0, int count) {
+    reserve_perturber_rows(count);
+    std::vector<float4> h((size_t)count * D);
+    for (int k = 0; k < count; ++k)
+      for (int d = 0; d < D; ++d) {
+        nbody_perturber q = pert[d];
+        nbody_perturber_update(&q, (float)(k0 + k) * p.dt);
+        h[(size_t)k * D + d] = make_float4(q.x, q.y, q.z, q.enabled ? q.mass_msun : 0.f);
+      }
+    check(cudaMemcpyAsync(pert_tab, h.data(), sizeof(float4) * h.size(), cudaMemcpyHostToDevice,
+                          st),
+          "perturber upload");
+    check(cudaMemsetAsync(pert_step, 0, sizeof(int), st), "perturber row reset");
+  }
+
+  void set_state(const void* const* v, bool is_double, const float* mass, bool on_device,
+                 bool forces) override {
+    check(cudaStreamSynchronize(st), "ensemble sync");
+    cur = 0;
+    const size_t esz = is_double ? sizeof(double) : sizeof(float);
+    for (int k = 0; k < 6; ++k) {
+      const void* src = v[k];
+      if (!on_device) {
+        check(cudaMemcpyAsync(staging, src, esz * n, cudaMemcpyHostToDevice, st), "state H2D");
+        src = staging;
+      }
+      if (is_double)
+        k_convert<double, R><<<stream_grid(n), kThreads, 0, st>>>((const double*)src, s[0].v[k],
+                                                                   n);
+      else
+        k_convert<float, R><<<stream_grid(n), kThreads, 0, st>>>((const float*)src, s[0].v[k], n);
+    }
+    check(cudaMemcpyAsync(s[0].m, mass, sizeof(float) * n,
+                          on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st),
+          "mass copy");
+    k_iota<<<stream_grid(n), kThreads, 0, st>>>(s[0].id, n);
+    k_disk_of<<<stream_grid(n), kThreads, 0, st>>>(d_off, D, n, s[0].disk);
+    check(cudaGetLastError(), "ensemble state");
+    launches += 8;
+    steps_done = 0;
+    has_state = true;
+    if (forces) {
+      upload_perturbers(0, 1);
+      forces_from_scratch();
+    } else {
+      launch_bbox_reset_n(bbox, D, st);  // the next stream kernel accumulates them
+      launches += 1;
+    }
+  }
+
+  // Accelerations of the state just set (caller order is the current order).
+  void load_accel(const float* const* acc) override {
+    float* dst[3] = {ax, ay, az};
+    for (int k = 0; k < 3; ++k)
+      check(cudaMemcpyAsync(dst[k], acc[k], sizeof(float) * n, cudaMemcpyHostToDevice, st),
+            "accel H2D");
+  }
+
+  // Bounding boxes of the current positions, then forces (no step).
+  void forces_from_scratch() {
+    launch_bbox_reset_n(bbox, D, st);
+    k_bbox_multi<R><<<stream_grid(n), kThreads, 0, st>>>(s[cur], n, bbox);
+    check(cudaGetLastError(), "k_bbox_multi launch");
+    launches += 2;
+    compute_forces();
+  }
+
+  // Keys, sort, permute into key order, tree, walk.  Leaves the bounding
+  // boxes reset for the next stream kernel to accumulate.
+  void compute_forces() {
+    StateArrays<R>& a = s[cur];
+    StateArrays<R>& b = s[1 - cur];
+    const int key_bits = 30 + disk_bits;
+    launch_geoms(bbox, geoms, D, st);
+    launch_keys_multi<R>(a.v[0], a.v[1], a.v[2], a.disk, n, geoms, keys64, tw.perm, tw.status,
+                         st);
+    launch_bbox_reset_n(bbox, D, st);
+    radix_sort_pairs<uint64_t>(keys64, tw.perm, keys64_alt, tw.perm_alt, tw.counts, n, key_bits,
+                               st);
+    k_permute<R><<<stream_grid(n), kThreads, 0, st>>>(tw.perm, a, b, n, tw.body4);
+    check(cudaGetLastError(), "k_permute launch");
+    cur = 1 - cur;
+    launch_karras<uint64_t>(tw, keys64, n, key_bits, st);
+    if (sizeof(R) == 8)
+      launch_octree<uint64_t>(tw, keys64, n, disk_bits, D, geoms, group_disk,
+                              (const double*)s[cur].v[0], (const double*)s[cur].v[1],
+                              (const double*)s[cur].v[2], st);
+    else
+      launch_octree<uint64_t>(tw, keys64, n, disk_bits, D, geoms, group_disk, nullptr, nullptr,
+                              nullptr, st);
+    check(cudaMemsetAsync(inter, 0, sizeof(unsigned long long), st), "inter reset");
+    check(cudaMemsetAsync(counters, 0, 3 * sizeof(unsigned long long), st), "counters reset");
+    WalkArgs w{};
+    w.com = tw.oct.com; w.info = tw.oct.info; w.body = tw.body4; w.n = n;
+    w.groups = tw.groups; w.n_groups = tw.n_groups;
+    w.theta2 = p.theta * p.theta; w.eps = p.softening; w.star_mass = p.star_mass;
+    w.star_in_walk = (sizeof(R) == 4) ? 1 : 0;
+    w.leaf_max = p.leaf_max;
+    w.pert = pert_tab; w.pert_step = pert_step; w.n_disks = D; w.group_disk = group_disk;
+    w.ax = ax; w.ay = ay; w.az = az; w.scatter = nullptr;
+    w.spill = spill; w.spill_cap = spill_cap; w.inter = inter; w.counters = counters;
+    w.work = work; w.status = tw.status; w.targets_per_lane = tw.group_max / 32;
+    launch_walk(w, st);
+    // geoms, keys, bbox reset, 5 per sort pass, permute, karras, mark,
+    // 2 x 3 scan kernels, moment tiles, tile scan, emit, walk
+    launches += 3 + 5 * ((key_bits + 7) / 8) + 3 + 6 + 4;
+  }
+
+  void collide() {
+    NeighborArgs na{tw.oct.info, tw.oct.box_lo, tw.oct.box_hi, tw.body4, n, tw.groups,
+                    tw.n_groups, p.leaf_max, spill, spill_cap, work, tw.status, group_disk};
+    if (sizeof(R) == 4) {
+      launch_collide(na, (const float*)s[cur].v[3], (const float*)s[cur].v[4],
+                     (const float*)s[cur].v[5], nullptr, p.r_coll, p.restitution, dvx, dvy, dvz,
+                     st);
+      launches += 1;
+    } else {
+      // float copies of the half-step velocities for the FP32 impulse
+      for (int k = 0; k < 3; ++k)
+        k_convert<R, float><<<stream_grid(n), kThreads, 0, st>>>(s[cur].v[3 + k], vf + k * n, n);
+      check(cudaGetLastError(), "velocity convert");
+      launch_collide(na, vf, vf + n, vf + 2 * n, nullptr, p.r_coll, p.restitution, dvx, dvy, dvz,
+                     st);
+      launches += 4;
+    }
+  }
+
+  void stream_kernel(bool end, bool begin) {
+    StreamArgs a{};
+    a.ax = ax; a.ay = ay; a.az = az;
+    const bool coll = p.r_coll > 0.f;
+    a.dvx = coll ? dvx : nullptr; a.dvy = coll ? dvy : nullptr; a.dvz = coll ? dvz : nullptr;
+    a.dt_f = p.dt; a.dth_f = p.dt * 0.5f;
+    a.dt = (double)p.dt; a.dth = (double)p.dt * 0.5;
+    const bool drag = p.gas_drag_rate > 0.f;
+    a.decay_f = drag ? expf(-p.gas_drag_rate * p.dt) : 0.f;
+    a.decay = drag ? std::exp(-(double)p.gas_drag_rate * (double)p.dt) : 0.0;
+    a.eps = p.softening; a.star_mass = p.star_mass; a.bbox = bbox;
+    const int g = stream_grid(n);
+    if (end && begin) k_stream<R, true, true, true><<<g, kThreads, 0, st>>>(s[cur], n, a);
+    else if (end) k_stream<R, true, false, true><<<g, kThreads, 0, st>>>(s[cur], n, a);
+    else k_stream<R, false, true, true><<<g, kThreads, 0, st>>>(s[cur], n, a);
+    check(cudaGetLastError(), "k_stream launch");
+    launches += 1;
+  }
+
+  // main.cu:101-139 for every disk: (dv + K2 + drag of the previous step),
+  // K1 + drift + bbox, tree + walk (+ star, + perturber at t_{n+1}),
+  // collisions on v_1/2; then the perturber row advances.
+  void one_step(bool first) {
+    stream_kernel(!first, true);
+    compute_forces();
+    if (p.r_coll > 0.f) collide();
+    k_increment<<<1, 1, 0, st>>>(pert_step);
+    check(cudaGetLastError(), "k_increment launch");
+    launches += 1;
+  }
+
+  // The step's launches have fixed pointers and sizes; only the state buffer
+  // the step starts from (it flips at the permute) and whether the previous
+  // step's closing kick is pending change, so four graphs cover every step.
+  cudaGraphExec_t graph_for(bool first) {
+    const int f = first ? 1 : 0, c = cur;
+    if (gx[f][c]) return gx[f][c];
+    cudaGraph_t graph = nullptr;
+    const unsigned long long l0 = launches;
+    // Captured on a private stream (the caller's may be the legacy default
+    // stream, which cannot capture) and launched on the caller's.
+    if (!cap_st) check(cudaStreamCreateWithFlags(&cap_st, cudaStreamNonBlocking), "capture stream");
+    cudaStream_t user = st;
+    st = cap_st;
+    check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+    one_step(first);
+    const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+    st = user;
+    check(ce, "end capture");
+    cur = c;  // captured, not run
+    g_kernels[f][c] = launches - l0;
+    launches = l0;
+    check(cudaGraphInstantiate(&gx[f][c], graph, 0), "graph instantiate");
+    cudaGraphDestroy(graph);
+    return gx[f][c];
+  }
+
+  void step(int nsteps) override {
+    if (nsteps <= 0) return;
+    upload_perturbers(steps_done + 1, nsteps);
+    for (int k = 0; k < nsteps; ++k) {
+      const bool first = (k == 0);
+      if (use_graphs) {
+        const int f = first ? 1 : 0, c = cur;
+        check(cudaGraphLaunch(graph_for(first), st), "graph launch");
+        launches += g_kernels[f][c];
+        graph_launches += 1;
+        cur = 1 - cur;
+      } else {
+        one_step(first);
+      }
+    }
+    stream_kernel(true, false);
+    steps_done += nsteps;
+  }
+
+  void get_state(void* const* v, bool as_double, float* const* acc, bool on_device) override {
+    state_out<R>(s[cur], n, ax, ay, az, p.softening, p.star_mass, v, as_double, acc, on_device,
+                 st);
+    launches += 1;
+  }
+
+  void autotune(const int* cand, int nc, float* ms_out) override {
+    static const int kDefault[] = {1, 4, 1, 8, 1, 16, 2, 8, 2, 16};
+    if (!cand) {
+      cand = kDefault;
+      nc = 5;
+    }
+    upload_perturbers(steps_done, 1);  // the forces of the current time
+    cudaEvent_t e0, e1;
+    check(cudaEventCreate(&e0), "event");
+    check(cudaEventCreate(&e1), "event");
+    float best = 0.f;
+    int best_k = -1;
+    for (int k = 0; k < nc; ++k) {
+      p.targets_per_lane = cand[2 * k] == 2 ? 2 : 1;
+      p.leaf_max = std::max(1, cand[2 * k + 1]);
+      tw.group_max = 32 * p.targets_per_lane;
+      forces_from_scratch();  // warm-up with this setting
+      check(cudaEventRecord(e0, st), "event");
+      forces_from_scratch();
+      check(cudaEventRecord(e1, st), "event");
+      check(cudaEventSynchronize(e1), "event sync");
+      float ms = 0.f;
+      check(cudaEventElapsedTime(&ms, e0, e1), "event time");
+      if (ms_out) ms_out[k] = ms;
+      if (best_k < 0 || ms < best) {
+        best = ms;
+        best_k = k;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    p.targets_per_lane = cand[2 * best_k] == 2 ? 2 : 1;
+    p.leaf_max = std::max(1, cand[2 * best_k + 1]);
+    tw.group_max = 32 * p.targets_per_lane;
+    drop_graphs();
+    forces_from_scratch();
+  }
+
+  void stats(nbody_ensemble_stats* out) override {
+    check(cudaStreamSynchronize(st), "ensemble sync");
+    out->n_disks = D;
+    out->n_total = n;
+    out->steps_done = steps_done;
+    out->targets_per_lane = p.targets_per_lane;
+    out->leaf_max = p.leaf_max;
+    check(cudaMemcpy(&out->status, tw.status, sizeof(int), cudaMemcpyDeviceToHost), "status");
+    check(cudaMemcpy(&out->interactions, inter, sizeof(unsigned long long),
+                     cudaMemcpyDeviceToHost),
+          "interactions");
+    out->launches = launches;
+    out->graph_launches = graph_launches;
+  }
+
+  void sync() override {
+    int s = 0;
+    check(cudaStreamSynchronize(st), "ensemble sync");
+    check(cudaMemcpy(&s, tw.status, sizeof(int), cudaMemcpyDeviceToHost), "status read");
+    if (s) {
+      check(cudaMemsetAsync(tw.status, 0, sizeof(int), st), "status reset");
+      throw ArgError("device status " + std::to_string(s) +
+                         " (1 walk stack, 2 union-find, 4 tree, 8 non-finite position)",
+                     NBODY_ERR_OVERFLOW);
+    }
+  }
+};
+
+EnsembleBase* make_ensemble(const nbody_sim_params& p, const nbody_disk_spec* d, int nd) {
+  if (p.state_precision == NBODY_STATE_F64) return new EnsembleImpl<double>(p, d, nd);
+  return new EnsembleImpl<float>(p, d, nd);
+}
+
+}  // namespace nb
+
+struct nbody_ensemble {
+  nb::EnsembleBase* impl;
+};
+
+extern "C" {
+
+int nbody_ensemble_create(const nbody_sim_params* p, const nbody_disk_spec* disks, int n_disks,
+                          nbody_ensemble** out) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(p && disks && out, "nbody_ensemble_create: null argument");
+    *out = nullptr;
+    NBODY_REQUIRE(n_disks >= 1 && n_disks <= (1 << 20),
+                  "nbody_ensemble_create: n_disks must be in [1, 2^20]");
+    long long total = 0;
+    for (int d = 0; d < n_disks; ++d) {
+      NBODY_REQUIRE(disks[d].n >= 2, "nbody_ensemble_create: every disk needs >= 2 bodies");
+      total += disks[d].n;
+    }
+    NBODY_REQUIRE(total < (1 << 27), "nbody_ensemble_create: total bodies must be < 2^27");
+    NBODY_REQUIRE(p->dt > 0.f, "nbody_ensemble_create: dt must be positive");
+    NBODY_REQUIRE(p->state_precision == NBODY_STATE_F32 || p->state_precision == NBODY_STATE_F64,
+                  "nbody_ensemble_create: unknown state precision");
+    *out = new nbody_ensemble{nb::make_ensemble(*p, disks, n_disks)};
+  })
+}
+
+int nbody_ensemble_destroy(nbody_ensemble* e) {
+  NBODY_API_BODY({
+    if (e) {
+      delete e->impl;
+      delete e;
+    }
+  })
+}
+
+int nbody_ensemble_set_stream(nbody_ensemble* e, void* stream) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(e, "nbody_ensemble_set_stream: null ensemble");
+    e->impl->set_stream((cudaStream_t)stream);
+  })
+}
+
+int nbody_ensemble_set_state(nbody_ensemble* e, const float* x, const float* y, const float* z,
+                             const float* vx, const float* vy, const float* vz,
+                             const float* mass, int on_device) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(e && x && y && z && vx && vy && vz && mass,
+                  "nbody_ensemble_set_state: null array");
+    const void* v[6] = {x, y, z, vx, vy, vz};
+    e->impl->set_state(v, false, mass, on_device != 0, true);
+  })
+}
+
+int nbody_ensemble_set_state_f64(nbody_ensemble* e, const double* x, const double* y,
+                                 const double* z, const double* vx, const double* vy,
+                                 const double* vz, const float* mass, int on_device) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(e && x && y && z && vx && vy && vz && mass,
+                  "nbody_ensemble_set_state_f64: null array");
+    const void* v[6] = {x, y, z, vx, vy, vz};
+    e->impl->set_state(v, true, mass, on_device != 0, true);
+  })
+}
+
+int nbody_ensemble_step(nbody_ensemble* e, int nsteps) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(e, "nbody_ensemble_step: null ensemble");
+    NBODY_REQUIRE(e->impl->has_state, "nbody_ensemble_step: state not set");
+    NBODY_REQUIRE(nsteps >= 0, "nbody_ensemble_step: negative step count");
+    e->impl->step(nsteps);
+  })
+}
+
+int nbody_ensemble_sync(nbody_ensemble* e) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(e, "nbody_ensemble_sync: null ensemble");
+    e->impl->sync();
+  })
+}
+
+int nbody_ensemble_get_state(nbody_ensemble* e, float* x, float* y, float* z, float* vx,
+                             float* vy, float* vz, float* ax, float* ay, float* az,
+                             int on_device) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(e && x && y && z && vx && vy && vz, "nbody_ensemble_get_state: null array");
+    NBODY_REQUIRE(e->impl->has_state, "nbody_ensemble_get_state: state not set");
+    void* v[6] = {x, y, z, vx, vy, vz};
+    float* a[3] = {ax, ay, az};
+    e->impl->get_state(v, false, (ax && ay && az) ? a : nullptr, on_device != 0);
+  })
+}
+
+int nbody_ensemble_get_state_f64(nbody_ensemble* e, double* x, double* y, double* z,
+                                 double* vx, double* vy, double* vz, float* ax, float* ay,
+                                 float* az, int on_device) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(e && x && y && z && vx && vy && vz,
+                  "nbody_ensemble_get_state_f64: null array");
+    NBODY_REQUIRE(e->impl->has_state, "nbody_ensemble_get_state_f64: state not set");
+    void* v[6] = {x, y, z, vx, vy, vz};
+    float* a[3] = {ax, ay, az};
+    e->impl->get_state(v, true, (ax && ay && az) ? a : nullptr, on_device != 0);
+  })
+}
+
+int nbody_ensemble_step_host(nbody_ensemble* e, double* x, double* y, double* z, double* vx,
+                             double* vy, double* vz, float* ax, float* ay, float* az,
+                             const float* mass, int nsteps) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(e && x && y && z && vx && vy && vz && ax && ay && az && mass,
+                  "nbody_ensemble_step_host: null array");
+    NBODY_REQUIRE(nsteps >= 0, "nbody_ensemble_step_host: negative step count");
+    nb::EnsembleBase* b = e->impl;
+    const int steps0 = b->has_state ? b->steps_done : 0;
+    const void* v[6] = {x, y, z, vx, vy, vz};
+    const float* a[3] = {ax, ay, az};
+    b->set_state(v, true, mass, false, false);
+    b->load_accel(a);
+    b->steps_done = steps0;  // the caller's clock continues
+    b->step(nsteps);
+    void* o[6] = {x, y, z, vx, vy, vz};
+    float* ao[3] = {ax, ay, az};
+    b->get_state(o, true, ao, false);
+  })
+}
+
+int nbody_ensemble_autotune(nbody_ensemble* e, const int* candidates, int n_candidates,
+                            float* ms_out) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(e, "nbody_ensemble_autotune: null ensemble");
+    NBODY_REQUIRE(e->impl->has_state, "nbody_ensemble_autotune: state not set");
+    NBODY_REQUIRE(!candidates || n_candidates >= 1,
+                  "nbody_ensemble_autotune: empty candidate list");
+    e->impl->autotune(candidates, n_candidates, ms_out);
+  })
+}
+
+int nbody_ensemble_set_graphs(nbody_ensemble* e, int on) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(e, "nbody_ensemble_set_graphs: null ensemble");
+    e->impl->set_graphs(on != 0);
+  })
+}
+
+int nbody_ensemble_stats_get(nbody_ensemble* e, nbody_ensemble_stats* out) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(e && out, "nbody_ensemble_stats_get: null argument");
+    e->impl->stats(out);
   })
 }
 

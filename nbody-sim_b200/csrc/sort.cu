@@ -17,23 +17,30 @@ namespace {
 
 constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / kWarp;
-constexpr int kSortItems = 16;
-constexpr int kTile = kSortThreads * kSortItems;  // 4096 keys per block
+// keys per thread: 16 (uint32 keys, 4096-key tiles) or 8 (uint64, 2048) so
+// the staged tile stays within 48 KB of static shared memory
+template <typename K>
+constexpr int sort_items() { return sizeof(K) == 8 ? 8 : 16; }
+template <typename K>
+constexpr int sort_tile() { return kSortThreads * sort_items<K>(); }
+constexpr int kMinTile = kSortThreads * 8;
 constexpr int kBins = 256;
 
+template <typename K>
 __global__ void __launch_bounds__(kSortThreads)
-k_sort_upsweep(const uint32_t* __restrict__ keys, uint32_t* __restrict__ counts, int n,
+k_sort_upsweep(const K* __restrict__ keys, uint32_t* __restrict__ counts, int n,
                int shift, int nblocks) {
   __shared__ uint32_t s_hist[kBins];
   const int tid = threadIdx.x, lane = tid & 31;
   s_hist[tid] = 0;
   __syncthreads();
-  const long long base = (long long)blockIdx.x * kTile;
+  constexpr int kItems = sort_items<K>();
+  const long long base = (long long)blockIdx.x * sort_tile<K>();
 #pragma unroll 4
-  for (int r = 0; r < kSortItems; ++r) {
+  for (int r = 0; r < kItems; ++r) {
     long long idx = base + (long long)r * kSortThreads + tid;
     bool valid = idx < n;
-    uint32_t d = valid ? (__ldg(keys + idx) >> shift) & 0xffu : kBins;
+    uint32_t d = valid ? (uint32_t)(__ldg(keys + idx) >> shift) & 0xffu : kBins;
     unsigned peers = __match_any_sync(kFull, d);
     int leader = __ffs(peers) - 1;
     if (valid && lane == leader) atomicAdd(&s_hist[d], (uint32_t)__popc(peers));
@@ -80,12 +87,15 @@ __global__ void __launch_bounds__(1024) k_scan_inplace(uint32_t* __restrict__ da
   }
 }
 
+template <typename K>
 __global__ void __launch_bounds__(kSortThreads)
-k_sort_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
-               uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out,
+k_sort_scatter(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+               K* __restrict__ keys_out, uint32_t* __restrict__ vals_out,
                const uint32_t* __restrict__ offsets, int n, int shift, int nblocks) {
+  constexpr int kItems = sort_items<K>();
+  constexpr int kTile = sort_tile<K>();
   __shared__ uint32_t s_cnt[kSortWarps][kBins];
-  __shared__ uint32_t s_keys[kTile];
+  __shared__ K s_keys[kTile];
   __shared__ uint32_t s_vals[kTile];
   __shared__ uint32_t s_base[kBins];
   __shared__ uint32_t s_glob[kBins];
@@ -96,15 +106,16 @@ k_sort_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict_
   __syncthreads();
 
   const long long tile0 = (long long)blockIdx.x * kTile;
-  const long long wbase = tile0 + (long long)warp * (kWarp * kSortItems);
-  uint32_t k_reg[kSortItems], v_reg[kSortItems], r_reg[kSortItems];
+  const long long wbase = tile0 + (long long)warp * (kWarp * kItems);
+  K k_reg[kItems];
+  uint32_t v_reg[kItems], r_reg[kItems];
 #pragma unroll
-  for (int r = 0; r < kSortItems; ++r) {
+  for (int r = 0; r < kItems; ++r) {
     long long idx = wbase + r * kWarp + lane;
     bool valid = idx < n;
-    uint32_t key = valid ? __ldg(keys_in + idx) : 0xffffffffu;
+    K key = valid ? __ldg(keys_in + idx) : (K)0;
     uint32_t val = valid ? __ldg(vals_in + idx) : 0u;
-    uint32_t d = valid ? (key >> shift) & 0xffu : kBins;
+    uint32_t d = valid ? (uint32_t)(key >> shift) & 0xffu : kBins;
     unsigned peers = __match_any_sync(kFull, d);
     int leader = __ffs(peers) - 1;
     uint32_t old = 0;
@@ -146,10 +157,10 @@ k_sort_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict_
   __syncthreads();
 
 #pragma unroll
-  for (int r = 0; r < kSortItems; ++r) {
+  for (int r = 0; r < kItems; ++r) {
     long long idx = wbase + r * kWarp + lane;
     if (idx < n) {
-      uint32_t d = (k_reg[r] >> shift) & 0xffu;
+      uint32_t d = (uint32_t)(k_reg[r] >> shift) & 0xffu;
       uint32_t lp = s_base[d] + s_cnt[warp][d] + r_reg[r];
       s_keys[lp] = k_reg[r];
       s_vals[lp] = v_reg[r];
@@ -159,8 +170,8 @@ k_sort_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict_
 
   const int tile_n = (int)min((long long)kTile, (long long)n - tile0);
   for (int i = tid; i < tile_n; i += kSortThreads) {
-    uint32_t key = s_keys[i];
-    uint32_t d = (key >> shift) & 0xffu;
+    K key = s_keys[i];
+    uint32_t d = (uint32_t)(key >> shift) & 0xffu;
     uint32_t g = s_glob[d] + (uint32_t)i - s_base[d];
     keys_out[g] = key;
     vals_out[g] = s_vals[i];
@@ -239,34 +250,41 @@ k_scan_down(uint32_t* __restrict__ data, int n, const uint32_t* __restrict__ sum
 size_t scan_tmp_words(int n);
 
 size_t radix_sort_count_words(int n) {
-  const size_t table = (size_t)kBins * (size_t)div_up(n, kTile);
+  const size_t table = (size_t)kBins * (size_t)div_up(n, kMinTile);
   return table + scan_tmp_words((int)table);
 }
 
-void radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt,
+template <typename K>
+void radix_sort_pairs(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt,
                       uint32_t* counts, int n, int bits, cudaStream_t s) {
   if (n <= 1) return;
-  const int nb = div_up(n, kTile);
+  const int nb = div_up(n, sort_tile<K>());
   const int passes = (bits + 7) / 8;
   // the count table is followed by room for the multi-block scan's partials
   uint32_t* scan_tmp = counts + (size_t)kBins * nb;
-  uint32_t *ki = keys, *vi = vals, *ko = keys_alt, *vo = vals_alt;
+  K *ki = keys, *ko = keys_alt;
+  uint32_t *vi = vals, *vo = vals_alt;
   for (int p = 0; p < passes; ++p) {
     const int shift = 8 * p;
-    k_sort_upsweep<<<nb, kSortThreads, 0, s>>>(ki, counts, n, shift, nb);
+    k_sort_upsweep<K><<<nb, kSortThreads, 0, s>>>(ki, counts, n, shift, nb);
     scan_exclusive_u32(counts, kBins * nb, scan_tmp, s);
-    k_sort_scatter<<<nb, kSortThreads, 0, s>>>(ki, vi, ko, vo, counts, n, shift, nb);
-    uint32_t* t = ki; ki = ko; ko = t;
-    t = vi; vi = vo; vo = t;
+    k_sort_scatter<K><<<nb, kSortThreads, 0, s>>>(ki, vi, ko, vo, counts, n, shift, nb);
+    K* t = ki; ki = ko; ko = t;
+    uint32_t* u = vi; vi = vo; vo = u;
   }
   if (ki != keys) {
-    check(cudaMemcpyAsync(keys, ki, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, s),
+    check(cudaMemcpyAsync(keys, ki, sizeof(K) * n, cudaMemcpyDeviceToDevice, s),
           "radix sort copy-back keys");
     check(cudaMemcpyAsync(vals, vi, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, s),
           "radix sort copy-back vals");
   }
   check(cudaGetLastError(), "radix_sort_pairs launch");
 }
+
+template void radix_sort_pairs<uint32_t>(uint32_t*, uint32_t*, uint32_t*, uint32_t*, uint32_t*,
+                                         int, int, cudaStream_t);
+template void radix_sort_pairs<uint64_t>(uint64_t*, uint32_t*, uint64_t*, uint32_t*, uint32_t*,
+                                         int, int, cudaStream_t);
 
 }  // namespace nb
 

@@ -113,6 +113,46 @@ k_keys(const T* __restrict__ x, const T* __restrict__ y, const T* __restrict__ z
   }
 }
 
+__global__ void k_geoms(const unsigned long long* __restrict__ enc, TreeGeom* __restrict__ geoms,
+                        int n_disks) {
+  const int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= n_disks) return;
+  TreeGeom g;
+  compute_geom(enc + 6 * d, g);
+  geoms[d] = g;
+}
+
+__global__ void k_bbox_reset_n(unsigned long long* enc, int n_disks) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < 6 * n_disks) enc[i] = ((i % 6) < 3) ? ~0ull : 0ull;
+}
+
+// Ensemble keys: (disk << 30) | Morton key in the disk's own root cube.
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_keys_multi(const T* __restrict__ x, const T* __restrict__ y, const T* __restrict__ z,
+             const int* __restrict__ disk, int n, const TreeGeom* __restrict__ geoms,
+             uint64_t* __restrict__ keys, uint32_t* __restrict__ perm, int* __restrict__ status) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int d = disk[i];
+    const TreeGeom& g = geoms[d];
+    double p[3] = {(double)x[i], (double)y[i], (double)z[i]};
+    uint32_t c[3];
+    bool finite = true;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      double q = (p[k] - g.lo[k]) * g.scale;
+      finite &= (q == q);
+      q = fmin(fmax(q, 0.0), 1023.0);
+      c[k] = (q == q) ? (uint32_t)q : 0u;
+    }
+    if (!finite) atomicOr(status, kStatusNonFinite);
+    keys[i] = ((uint64_t)d << 30) | (uint64_t)morton30(c[0], c[1], c[2]);
+    perm[i] = (uint32_t)i;
+  }
+}
+
 __global__ void __launch_bounds__(kThreads)
 k_gather_body4(const uint32_t* __restrict__ perm, const float* __restrict__ x,
                const float* __restrict__ y, const float* __restrict__ z,
@@ -127,15 +167,23 @@ k_gather_body4(const uint32_t* __restrict__ perm, const float* __restrict__ x,
 // ---------------------------------------------------------------- Karras
 // delta(i, j): common prefix of keys i and j, with the index as tie-break so
 // equal keys still form a valid binary radix tree (Karras 2012, sec. 4).
-__device__ __forceinline__ int delta(const uint32_t* __restrict__ keys, int n, int i, int j) {
+__device__ __forceinline__ int clz_key(uint32_t v) { return __clz(v); }
+__device__ __forceinline__ int clz_key(uint64_t v) { return __clzll((long long)v); }
+
+template <typename K>
+__device__ __forceinline__ int delta(const K* __restrict__ keys, int n, int i, int j) {
   if (j < 0 || j >= n) return -1;
-  uint32_t a = keys[i], b = keys[j];
-  if (a != b) return __clz(a ^ b);
-  return 32 + __clz((uint32_t)i ^ (uint32_t)j);
+  K a = keys[i], b = keys[j];
+  if (a != b) return clz_key(a ^ b);
+  return 8 * (int)sizeof(K) + __clz((uint32_t)i ^ (uint32_t)j);
 }
 
+// key_bits: the low bits of K the keys use (30 Morton bits, plus the disk
+// index above them for an ensemble).  prefix[] stores the common prefix in
+// those bits, key_bits for runs of equal keys.
+template <typename K>
 __global__ void __launch_bounds__(kThreads)
-k_karras(const uint32_t* __restrict__ keys, int n, int* __restrict__ left,
+k_karras(const K* __restrict__ keys, int n, int key_bits, int* __restrict__ left,
          int* __restrict__ right, int* __restrict__ parent, int* __restrict__ lo_out,
          int* __restrict__ hi_out, uint8_t* __restrict__ prefix) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -164,7 +212,8 @@ k_karras(const uint32_t* __restrict__ keys, int n, int* __restrict__ left,
   parent[rc] = i;
   lo_out[i] = lo;
   hi_out[i] = hi;
-  prefix[i] = (uint8_t)(dnode >= 32 ? 30 : dnode - 2);
+  constexpr int kW = 8 * (int)sizeof(K);
+  prefix[i] = (uint8_t)(dnode >= kW ? key_bits : dnode - (kW - key_bits));
   if (i == 0) parent[0] = -1;
 }
 
@@ -263,8 +312,12 @@ __device__ __forceinline__ double4 range_moments(const double4* __restrict__ plo
 }
 
 // ---------------------------------------------------------- octree layout
-__device__ __forceinline__ int bin_level(const uint8_t* prefix, int n, int b) {
-  return (b >= n - 1) ? 10 : (int)prefix[b] / 3;
+// Octree level of binary node b: leaves and equal-key runs are level 10;
+// nodes whose prefix does not cover the disk bits span several disks (-1).
+__device__ __forceinline__ int bin_level(const uint8_t* prefix, int n, int b, int disk_bits) {
+  if (b >= n - 1) return 10;
+  const int p = (int)prefix[b];
+  return (p < disk_bits) ? -1 : (p - disk_bits) / 3;
 }
 
 __device__ __forceinline__ int bin_count(const int* lo, const int* hi, int n, int b) {
@@ -277,14 +330,14 @@ template <typename F>
 __device__ __forceinline__ int for_each_oct_child(const int* __restrict__ left,
                                                   const int* __restrict__ right,
                                                   const uint8_t* __restrict__ prefix, int n,
-                                                  int b, int lb, F f) {
+                                                  int disk_bits, int b, int lb, F f) {
   int stack[8];
   int top = 0, k = 0;
   stack[top++] = right[b];
   stack[top++] = left[b];
   while (top > 0) {
     int c = stack[--top];
-    if (c >= n - 1 || bin_level(prefix, n, c) > lb) {
+    if (c >= n - 1 || bin_level(prefix, n, c, disk_bits) > lb) {
       f(c, k++);
     } else if (top + 2 <= 8) {
       stack[top++] = right[c];
@@ -300,25 +353,38 @@ __device__ __forceinline__ int for_each_oct_child(const int* __restrict__ left,
 // group never straddles a jump of the space-filling curve (a fixed run of 32
 // consecutive bodies can: its box then spans most of the domain and its walk
 // degenerates to O(N) work on one warp).
+// A node is an octree node ("top") when it starts a deeper level than its
+// parent; a disk's root is a top whose parent spans several disks (or node 0
+// of a single disk).  Groups never span disks.
+__device__ __forceinline__ void classify(int n, int disk_bits, const int* __restrict__ parent,
+                                         const uint8_t* __restrict__ prefix, int b, int& lb,
+                                         int& lp, bool& top, int& p) {
+  lb = bin_level(prefix, n, b, disk_bits);
+  p = (b == 0) ? -1 : parent[b];
+  lp = (p < 0) ? -1 : bin_level(prefix, n, p, disk_bits);
+  top = lb >= 0 && (p < 0 || lb > lp);
+}
+
 __global__ void __launch_bounds__(kThreads)
-k_mark(int n, int gmax, const int* __restrict__ left, const int* __restrict__ right,
-       const int* __restrict__ parent, const int* __restrict__ lo, const int* __restrict__ hi,
+k_mark(int n, int gmax, int disk_bits, const int* __restrict__ left,
+       const int* __restrict__ right, const int* __restrict__ parent,
+       const int* __restrict__ lo, const int* __restrict__ hi,
        const uint8_t* __restrict__ prefix, uint8_t* __restrict__ nch, uint32_t* __restrict__ off,
        uint32_t* __restrict__ gflag) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   const int nb = 2 * n - 1;
   if (b >= nb) return;
-  const int lb = bin_level(prefix, n, b);
-  const int p = (b == 0) ? -1 : parent[b];
-  const bool top = (b == 0) || lb > bin_level(prefix, n, p);
+  int lb, lp, p;
+  bool top;
+  classify(n, disk_bits, parent, prefix, b, lb, lp, top, p);
   int cnt = 0;
   if (top && b < n - 1 && lb < 10)
-    cnt = for_each_oct_child(left, right, prefix, n, b, lb, [](int, int) {});
+    cnt = for_each_oct_child(left, right, prefix, n, disk_bits, b, lb, [](int, int) {});
   nch[b] = (uint8_t)cnt;
   off[b] = (uint32_t)cnt;
   const int c = bin_count(lo, hi, n, b);
-  const int pc = (p < 0) ? 0x7fffffff : bin_count(lo, hi, n, p);
-  gflag[b] = (c <= gmax && pc > gmax) ? 1u : 0u;
+  const int pc = (p < 0 || lp < 0) ? 0x7fffffff : bin_count(lo, hi, n, p);
+  gflag[b] = (lb >= 0 && c <= gmax && pc > gmax) ? 1u : 0u;
 }
 
 __device__ __forceinline__ uint32_t compact3(uint32_t v) {
@@ -330,11 +396,12 @@ __device__ __forceinline__ uint32_t compact3(uint32_t v) {
   return v;
 }
 
+template <typename K>
 struct EmitArgs {
-  int n, gmax;
+  int n, gmax, disk_bits, n_roots;
   const int *left, *right, *parent, *lo, *hi;
   const uint8_t* prefix;
-  const uint32_t* keys;
+  const K* keys;
   const uint8_t* nch;
   const uint32_t* off;
   const uint32_t* goff;
@@ -344,13 +411,21 @@ struct EmitArgs {
   const TreeGeom* geom;
   OctNodes oct;
   int2* groups;
+  int* group_disk;  // optional: disk of each group
   int* n_nodes;
   int* n_groups;
 };
 
+// Disk index of a key (the bits above the 30 Morton bits).
+template <typename K>
+__device__ __forceinline__ int key_disk(K k) { return (int)(k >> 30); }
+
 // Writes the octree record of binary node c into slot f.
-__device__ void write_node(const EmitArgs& a, int c, int f) {
-  const float rhs = a.geom->rhs;
+template <typename K>
+__device__ void write_node(const EmitArgs<K>& a, int c, int f) {
+  const int first = (c >= a.n - 1) ? c - (a.n - 1) : a.lo[c];
+  const TreeGeom* geom = a.geom + key_disk(a.keys[first]);
+  const float rhs = geom->rhs;
   if (c >= a.n - 1) {  // single-body leaf
     const int j = c - (a.n - 1);
     const float4 p = a.body4[j];
@@ -360,19 +435,19 @@ __device__ void write_node(const EmitArgs& a, int c, int f) {
     a.oct.box_hi[f] = make_float4(p.x, p.y, p.z, 0.f);
     return;
   }
-  const int L = (int)a.prefix[c] / 3;
+  const int L = ((int)a.prefix[c] - a.disk_bits) / 3;
   const int lo = a.lo[c], hi = a.hi[c];
   const double4 s = range_moments(a.ploc, a.tpre, lo, hi + 1);
   // the node's cube: level L cell of its key prefix (side 2 rhs / 2^L, exact
   // power-of-two scaling), grown by a margin for float positions that sit an
   // ulp outside their FP64-quantised cell
-  const uint32_t kl = a.keys[lo] >> (3 * (10 - L));
+  const uint32_t kl = (uint32_t)(a.keys[lo] & (K)0x3fffffffu) >> (3 * (10 - L));
   const uint32_t cc[3] = {compact3(kl), compact3(kl >> 1), compact3(kl >> 2)};
-  const double side = (double)a.geom->rhs * (double)(2.0f / (float)(1u << L));
+  const double side = (double)rhs * (double)(2.0f / (float)(1u << L));
   float blo[3], bhi[3], ctr[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
-    const double l0 = a.geom->lo[k] + (double)cc[k] * side;
+    const double l0 = geom->lo[k] + (double)cc[k] * side;
     const float fl = (float)l0, fs = (float)side;
     const float margin = 1e-6f * (fabsf(fl) + fs) + 1e-30f;
     blo[k] = fl - margin;
@@ -388,49 +463,57 @@ __device__ void write_node(const EmitArgs& a, int c, int f) {
   }
   const int k = a.nch[c];
   a.oct.com[f] = com;
-  a.oct.info[f] = make_int4(k > 0 ? 1 + (int)a.off[c] : -1, lo, ((hi - lo + 1) << 4) | k,
+  a.oct.info[f] = make_int4(k > 0 ? a.n_roots + (int)a.off[c] : -1, lo, ((hi - lo + 1) << 4) | k,
                             __float_as_int(ldexpf(rhs, -L)));
   a.oct.box_lo[f] = make_float4(blo[0], blo[1], blo[2], 0.f);
   a.oct.box_hi[f] = make_float4(bhi[0], bhi[1], bhi[2], 0.f);
 }
 
-// Every top node owns a block of contiguous slots (1 + off[b] ...) for its
-// octree children; node 0 also owns slot 0, the root.  A warp gathers the
+// Every top node owns a block of contiguous slots (n_roots + off[b] ...) for
+// its octree children; slots 0 .. n_roots-1 hold the roots (one per disk,
+// slot = disk index).  A warp gathers the
 // (child, slot) pairs of its 32 binary nodes in shared memory and then writes
 // the records one per lane, so the up-to-8 records of one parent do not
 // serialise on a single thread.  Target groups are written at their scanned
 // offsets.
 constexpr int kEmitWarps = kThreads / 32;
 
-__global__ void __launch_bounds__(kThreads) k_emit(const EmitArgs a) {
+template <typename K>
+__global__ void __launch_bounds__(kThreads) k_emit(const EmitArgs<K> a) {
   __shared__ int2 s_job[kEmitWarps][32 * 8 + 1];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   const int nb = 2 * a.n - 1;
   const bool in = b < nb;
+  int lb = -1, lp = -1, p = -1;
+  bool top = false;
+  if (in) classify(a.n, a.disk_bits, a.parent, a.prefix, b, lb, lp, top, p);
   const int k = in ? a.nch[b] : 0;
-  const int extra = (b == 0) ? 1 : 0;  // the root record
+  const bool disk_root = top && (p < 0 || lp < 0);
+  const int first = (b >= a.n - 1) ? b - (a.n - 1) : (in ? a.lo[b] : 0);
+  const int extra = disk_root ? 1 : 0;
   const int incl = warp_incl_scan(k + extra, lane);
   const int total = __shfl_sync(kFull, incl, 31);
   int pos = incl - k - extra;
   int2* job = s_job[warp];
-  if (extra) job[pos++] = make_int2(0, 0);
+  if (extra) job[pos++] = make_int2(b, key_disk(a.keys[first]));  // slot = disk index
   if (k > 0) {
-    const int base = 1 + (int)a.off[b];
-    const int lb = (int)a.prefix[b] / 3;
-    for_each_oct_child(a.left, a.right, a.prefix, a.n, b, lb,
+    const int base = a.n_roots + (int)a.off[b];
+    for_each_oct_child(a.left, a.right, a.prefix, a.n, a.disk_bits, b, lb,
                        [&](int c, int i) { job[pos + i] = make_int2(c, base + i); });
   }
   __syncwarp();
   for (int j = lane; j < total; j += 32) write_node(a, job[j].x, job[j].y);
   if (!in) return;
   const int c = bin_count(a.lo, a.hi, a.n, b);
-  const int p = (b == 0) ? -1 : a.parent[b];
-  const int pc = (p < 0) ? 0x7fffffff : bin_count(a.lo, a.hi, a.n, p);
-  const bool g = c <= a.gmax && pc > a.gmax;
-  if (g) a.groups[a.goff[b]] = make_int2(b >= a.n - 1 ? b - (a.n - 1) : a.lo[b], c);
+  const int pc = (p < 0 || lp < 0) ? 0x7fffffff : bin_count(a.lo, a.hi, a.n, p);
+  const bool g = lb >= 0 && c <= a.gmax && pc > a.gmax;
+  if (g) {
+    a.groups[a.goff[b]] = make_int2(first, c);
+    if (a.group_disk) a.group_disk[a.goff[b]] = key_disk(a.keys[first]);
+  }
   if (b == nb - 1) {
-    *a.n_nodes = 1 + (int)(a.off[b] + (uint32_t)k);
+    *a.n_nodes = a.n_roots + (int)(a.off[b] + (uint32_t)k);
     *a.n_groups = (int)a.goff[b] + (g ? 1 : 0);
   }
 }
@@ -545,26 +628,57 @@ void launch_gather_body4(TreeWork& w, const float* x, const float* y, const floa
   check(cudaGetLastError(), "k_gather_body4 launch");
 }
 
-void launch_build_topology(TreeWork& w, int n, cudaStream_t s) {
+void launch_geoms(const unsigned long long* enc, TreeGeom* geoms, int n_disks, cudaStream_t s) {
+  k_geoms<<<div_up(n_disks, 64), 64, 0, s>>>(enc, geoms, n_disks);
+  check(cudaGetLastError(), "k_geoms launch");
+}
+
+void launch_bbox_reset_n(unsigned long long* enc, int n_disks, cudaStream_t s) {
+  k_bbox_reset_n<<<div_up(6 * n_disks, 256), 256, 0, s>>>(enc, n_disks);
+  check(cudaGetLastError(), "k_bbox_reset_n launch");
+}
+
+template <typename T>
+void launch_keys_multi(const T* x, const T* y, const T* z, const int* disk, int n,
+                       const TreeGeom* geoms, uint64_t* keys, uint32_t* perm, int* status,
+                       cudaStream_t s) {
+  int g = std::min(grid_for(n), 148 * 16);
+  if (g < 1) g = 1;
+  k_keys_multi<T><<<g, kThreads, 0, s>>>(x, y, z, disk, n, geoms, keys, perm, status);
+  check(cudaGetLastError(), "k_keys_multi launch");
+}
+
+template void launch_keys_multi<float>(const float*, const float*, const float*, const int*, int,
+                                       const TreeGeom*, uint64_t*, uint32_t*, int*, cudaStream_t);
+template void launch_keys_multi<double>(const double*, const double*, const double*, const int*,
+                                        int, const TreeGeom*, uint64_t*, uint32_t*, int*,
+                                        cudaStream_t);
+
+template <typename K>
+void launch_karras(TreeWork& w, const K* keys, int n, int key_bits, cudaStream_t s) {
   if (n < 2) return;
-  k_karras<<<grid_for(n - 1), kThreads, 0, s>>>(w.keys, n, w.bin_left, w.bin_right,
-                                                w.bin_parent, w.bin_lo, w.bin_hi, w.bin_prefix);
+  k_karras<K><<<grid_for(n - 1), kThreads, 0, s>>>(keys, n, key_bits, w.bin_left, w.bin_right,
+                                                   w.bin_parent, w.bin_lo, w.bin_hi,
+                                                   w.bin_prefix);
   check(cudaGetLastError(), "k_karras launch");
 }
 
-void launch_build_moments(TreeWork& w, int n, const double* xd, const double* yd,
-                          const double* zd, cudaStream_t s) {
+template <typename K>
+void launch_octree(TreeWork& w, const K* keys, int n, int disk_bits, int n_roots,
+                   const TreeGeom* geoms, int* group_disk, const double* xd, const double* yd,
+                   const double* zd, cudaStream_t s) {
   if (n < 1) return;
   if (n == 1) {
-    k_single<<<1, 1, 0, s>>>(w.body4, w.geom, w.oct, w.n_nodes, w.groups, w.n_groups);
+    k_single<<<1, 1, 0, s>>>(w.body4, geoms, w.oct, w.n_nodes, w.groups, w.n_groups);
+    if (group_disk) check(cudaMemsetAsync(group_disk, 0, sizeof(int), s), "group disk");
     check(cudaGetLastError(), "k_single launch");
     return;
   }
   const int nb = 2 * n - 1;
-  const int kGroupMax = w.group_max;
-  k_mark<<<grid_for(nb), kThreads, 0, s>>>(n, kGroupMax, w.bin_left, w.bin_right, w.bin_parent,
-                                           w.bin_lo, w.bin_hi, w.bin_prefix, w.oct_nch,
-                                           w.oct_off, w.group_flag);
+  const int gmax = w.group_max;
+  k_mark<<<grid_for(nb), kThreads, 0, s>>>(n, gmax, disk_bits, w.bin_left, w.bin_right,
+                                           w.bin_parent, w.bin_lo, w.bin_hi, w.bin_prefix,
+                                           w.oct_nch, w.oct_off, w.group_flag);
   scan_exclusive_u32(w.oct_off, nb, w.scan_tmp, s);
   scan_exclusive_u32(w.group_flag, nb, w.scan_tmp, s);
   const int ntiles = n / kTileM + 1;
@@ -572,11 +686,25 @@ void launch_build_moments(TreeWork& w, int n, const double* xd, const double* yd
   double4* tpre = w.mom_tiles + (ntiles + 1);
   k_moment_tiles<<<ntiles, kThreads, 0, s>>>(w.body4, xd, yd, zd, n, w.mom_ploc, tile_sum);
   k_tile_scan<<<1, 32, 0, s>>>(tile_sum, ntiles, tpre);
-  EmitArgs a{n, kGroupMax, w.bin_left, w.bin_right, w.bin_parent, w.bin_lo, w.bin_hi,
-             w.bin_prefix, w.keys, w.oct_nch, w.oct_off, w.group_flag, w.body4, w.mom_ploc,
-             tpre, w.geom, w.oct, w.groups, w.n_nodes, w.n_groups};
-  k_emit<<<grid_for(nb), kThreads, 0, s>>>(a);
+  EmitArgs<K> a{n, gmax, disk_bits, n_roots, w.bin_left, w.bin_right, w.bin_parent, w.bin_lo,
+                w.bin_hi, w.bin_prefix, keys, w.oct_nch, w.oct_off, w.group_flag, w.body4,
+                w.mom_ploc, tpre, geoms, w.oct, w.groups, group_disk, w.n_nodes, w.n_groups};
+  k_emit<K><<<grid_for(nb), kThreads, 0, s>>>(a);
   check(cudaGetLastError(), "octree launch");
+}
+
+template void launch_karras<uint64_t>(TreeWork&, const uint64_t*, int, int, cudaStream_t);
+template void launch_octree<uint64_t>(TreeWork&, const uint64_t*, int, int, int,
+                                      const TreeGeom*, int*, const double*, const double*,
+                                      const double*, cudaStream_t);
+
+void launch_build_topology(TreeWork& w, int n, cudaStream_t s) {
+  launch_karras<uint32_t>(w, w.keys, n, 30, s);
+}
+
+void launch_build_moments(TreeWork& w, int n, const double* xd, const double* yd,
+                          const double* zd, cudaStream_t s) {
+  launch_octree<uint32_t>(w, w.keys, n, 0, 1, w.geom, nullptr, xd, yd, zd, s);
 }
 
 }  // namespace nb

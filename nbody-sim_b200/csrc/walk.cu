@@ -98,6 +98,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(const WalkArgs a) {
     g = __shfl_sync(kFull, g, 0);
     if (g >= n_groups) break;
     const int2 gr = a.groups[g];
+    const int disk = a.group_disk ? a.group_disk[g] : 0;
     float4 me[kT];
     bool valid[kT];
     float gx0 = INFINITY, gx1 = -INFINITY, gy0 = INFINITY, gy1 = -INFINITY, gz0 = INFINITY,
@@ -123,7 +124,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(const WalkArgs a) {
     unsigned long long visited = 0, spills = 0, evaluated = 0;
     int top = 1, spilled = 0, nlist = 0;
     bool overflow = false;
-    if (lane == 0) w.stk[0] = 0;
+    if (lane == 0) w.stk[0] = disk;  // root slot of the group's disk
     __syncwarp();
 
     while (true) {
@@ -235,7 +236,8 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(const WalkArgs a) {
     evaluated += nlist;
     __syncwarp();
 
-    const float4 p = a.pert ? *a.pert : make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (a.pert) p = a.pert[(a.pert_step ? *a.pert_step * a.n_disks : 0) + disk];
 #pragma unroll
     for (int t = 0; t < kT; ++t) {
       float ax = acc[t].x, ay = acc[t].y, az = acc[t].z;
