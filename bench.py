@@ -56,9 +56,13 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-flush", action="store_true")
-    ap.add_argument("--workload", choices=["disk1m", "ensemble"], default="disk1m",
+    ap.add_argument("--workload", choices=["disk1m", "ensemble", "precision"], default="disk1m",
                     help="disk1m: the headline single disk; ensemble: 64 disks (C4) against "
-                         "the same disks run one by one")
+                         "the same disks run one by one; precision: force error vs FP64 "
+                         "direct sum over theta, and energy / L_y drift per state precision")
+    ap.add_argument("--targets", type=int, default=16384,
+                    help="precision study: force-error targets (seeded random subset)")
+    ap.add_argument("--drift-steps", type=int, default=200)
     ap.add_argument("--disks", type=int, default=64)
     ap.add_argument("--solo-steps", type=int, default=10,
                     help="timed steps per disk of the one-by-one comparison")
@@ -450,6 +454,61 @@ def run_ensemble(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_precision(args, ws, rank, local):
+    """Precision study on the headline disk (N = 2^20, r in [0.3, 30] AU,
+    m = 1e-9, eps = 5e-4, dt = 0.002, gravity only, so E and L_y are
+    conserved).  (1) Relative error of the walk's total and self-gravity
+    accelerations against the FP64 direct sum on a seeded random subset of
+    targets, theta in {0.3, 0.5, 0.7}.  (2) |dE/E| and |dL_y/L_y| after
+    --drift-steps steps at theta 0.5 for FP32, FP64 and hi/lo float-pair
+    state, with the softened pair energy summed directly in FP64."""
+    import torch
+    if rank != 0:
+        return
+    nb = importlib.import_module("nbody-sim_b200")
+    dg = importlib.import_module("nbody-sim_b200.diagnostics")
+    torch.cuda.set_device(local)
+    n, w = args.n, WORKLOAD
+    ic = make_ic(nb, n, 0, np.float64)
+    targets = np.sort(np.random.default_rng(0).choice(n, min(args.targets, n), replace=False))
+    st32 = {k: ic[k].astype(np.float32) for k in ("x", "y", "z")}
+    st32["m"] = ic["m"]
+    forces = {}
+    for theta in (0.3, 0.5, 0.7):
+        forces[f"{theta}"] = dg.force_errors(st32, theta, w["eps"], 1.0, targets)
+    drift = {}
+    stream = torch.cuda.current_stream()
+    for name, prec in (("f32", nb.STATE_F32), ("f64", nb.STATE_F64),
+                       ("f32x2", nb.STATE_F32X2)):
+        prm = nb.sim_params(dt=w["dt"], theta=0.5, softening=w["eps"], star_mass=1.0,
+                            r_coll=0.0, restitution=0.0, gas_drag_rate=0.0,
+                            state_precision=prec, leaf_max=args.leaf_max)
+        sim = nb.Sim(prm, n)
+        sim.set_stream(stream.cuda_stream)
+        dt_ = np.float32 if prec == nb.STATE_F32 else np.float64
+        sim.set_state(*[ic[k].astype(dt_) for k in ("x", "y", "z", "vx", "vy", "vz")], ic["m"])
+        c0 = dg.conserved(sim.get_state(double=True), ic["m"], w["eps"], 1.0)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        sim.step(args.drift_steps)
+        b.record(stream)
+        sim.sync()
+        ms = a.elapsed_time(b) / args.drift_steps
+        c1 = dg.conserved(sim.get_state(double=True), ic["m"], w["eps"], 1.0)
+        sim.close()
+        drift[name] = {"dE_over_E": abs(c1["E"] - c0["E"]) / abs(c0["E"]),
+                       "dLy_over_Ly": abs(c1["L_y"] - c0["L_y"]) / abs(c0["L_y"]),
+                       "ms_per_step": ms, "E0": c0, "E1": c1}
+    line = {
+        "study": "precision", "n": n, "targets": len(targets), "data": "synthetic",
+        "config": {"workload": f"Keplerian disk N={n} r=[0.3,30] AU m=1e-9 eps=5e-4 dt=0.002, "
+                               "gravity only", "drift_steps": args.drift_steps,
+                   "drift_theta": 0.5, "leaf_max": args.leaf_max},
+        "force_error_vs_fp64_direct": forces, "drift": drift,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     ws, rank, local = dist_setup()
@@ -458,6 +517,8 @@ def main():
             run_reference(args, ws, rank)
         elif args.workload == "ensemble":
             run_ensemble(args, ws, rank, local)
+        elif args.workload == "precision":
+            run_precision(args, ws, rank, local)
         else:
             run_ours(args, ws, rank, local)
     finally:

@@ -265,6 +265,7 @@ void nbody_writer_close(nbody_writer* w);
 
 #define NBODY_STATE_F32 0    /* positions/velocities float (reference)     */
 #define NBODY_STATE_F64 1    /* positions/velocities double                */
+#define NBODY_STATE_F32X2 2  /* hi/lo float pairs (~48 bits), FP64 kicks   */
 
 typedef struct nbody_sim_params {
   float dt;
@@ -426,6 +427,19 @@ typedef struct nbody_ensemble_stats {
   unsigned long long graph_launches;
 } nbody_ensemble_stats;
 int nbody_ensemble_stats_get(nbody_ensemble* e, nbody_ensemble_stats* out);
+
+/* -------------------------------------------------------- diagnostics --- */
+
+/* FP64 direct sum of the softened self-gravity (no star term) for a list of
+ * targets: a_t = sum_{j != i} m_j d / (|d|^2 + eps^2)^{3/2} and
+ * phi_t = -sum_{j != i} m_j / (|d|^2 + eps^2)^{1/2}, i = targets[t] (targets
+ * NULL: every body, n_targets ignored).  The yardstick for the walk's force
+ * error and the pair term of the softened energy.  No reference counterpart
+ * (the reference has no accuracy diagnostics).  Device arrays; any output may
+ * be NULL; synchronous. */
+int nbody_direct_f64(const double* x, const double* y, const double* z, const float* mass, int n,
+                     const int* targets, int n_targets, double eps, double* ax, double* ay,
+                     double* az, double* phi);
 
 /* ------------------------------------------------------ initial disks --- */
 

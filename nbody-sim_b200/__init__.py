@@ -48,9 +48,11 @@ NBODY_ERR_CONFIG = 6
 NBODY_ERR_STATE = 7
 NBODY_STATE_F32 = 0
 NBODY_STATE_F64 = 1
+NBODY_STATE_F32X2 = 2
 FOF_NOALLOC_MAX_N = 32768
 STATE_F32 = 0
 STATE_F64 = 1
+STATE_F32X2 = 2
 
 
 class NBodyError(RuntimeError):
@@ -223,6 +225,7 @@ SIGNATURES = [
     ("nbody_ensemble_autotune", C.c_int, [_VP, _VP, C.c_int, _VP]),
     ("nbody_ensemble_set_graphs", C.c_int, [_VP, C.c_int]),
     ("nbody_ensemble_stats_get", C.c_int, [_VP, C.POINTER(nbody_ensemble_stats)]),
+    ("nbody_direct_f64", C.c_int, [_VP] * 4 + [C.c_int, _VP, C.c_int, C.c_double] + [_VP] * 4),
     ("nbody_make_disk", C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                   C.c_double, C.c_uint64, _D, _D, _D, _D, _D, _D]),
 ]
@@ -763,6 +766,23 @@ class Ensemble:
         st = nbody_ensemble_stats()
         _check(lib.nbody_ensemble_stats_get(self.h, C.byref(st)))
         return st
+
+
+def direct_f64(x, y, z, mass, eps: float, targets=None, want_acc=True, want_phi=False):
+    """FP64 direct-sum self-gravity (nbody_direct_f64) on CUDA tensors.
+
+    x, y, z: float64 CUDA tensors; mass: float32; targets: int32 CUDA tensor
+    or None (every body).  Returns (ax, ay, az, phi) float64 tensors (None
+    where not wanted)."""
+    import torch
+    n = x.numel()
+    nt = n if targets is None else targets.numel()
+    mk = lambda on: torch.empty(nt, dtype=torch.float64, device=x.device) if on else None
+    ax, ay, az, phi = mk(want_acc), mk(want_acc), mk(want_acc), mk(want_phi)
+    p = lambda t: None if t is None else t.data_ptr()
+    _check(lib.nbody_direct_f64(p(x), p(y), p(z), p(mass), n, p(targets), nt, eps,
+                                p(ax), p(ay), p(az), p(phi)))
+    return ax, ay, az, phi
 
 
 # --------------------------------------------------------- initial disks

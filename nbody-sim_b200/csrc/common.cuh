@@ -20,6 +20,31 @@ enum StatusBits : int {
   kStatusNonFinite = 8,       // a non-finite position reached key generation
 };
 
+// Hi/lo float pair state (NBODY_STATE_F32X2): value = hi + lo with
+// |lo| <= ulp(hi)/2, about 48 significant bits in 8 bytes.  Kernels convert
+// to double, compute in FP64 and split back; the tree reads hi.
+struct __align__(8) HiLo {
+  float hi, lo;
+  HiLo() = default;
+  __host__ __device__ explicit HiLo(double v) {
+    hi = (float)v;
+    lo = (float)(v - (double)hi);
+  }
+  __host__ __device__ explicit HiLo(float v) : hi(v), lo(0.f) {}
+  __host__ __device__ explicit operator double() const { return (double)hi + (double)lo; }
+  __host__ __device__ explicit operator float() const { return hi; }
+};
+
+// Arithmetic type of a state storage type.
+template <typename R>
+struct ComputeOf {
+  using type = R;
+};
+template <>
+struct ComputeOf<HiLo> {
+  using type = double;
+};
+
 struct CudaError : std::runtime_error {
   explicit CudaError(const std::string& s) : std::runtime_error(s) {}
 };

@@ -1,0 +1,80 @@
+// direct.cu -- FP64 direct-sum self-gravity: the accuracy yardstick of the
+// tree walk and the pair potential of the softened energy.
+//
+// For each target i (a list, or every body):
+//   a_i   =  sum_{j != i} m_j (x_j - x_i) / (|x_j - x_i|^2 + eps^2)^{3/2}
+//   phi_i = -sum_{j != i} m_j / (|x_j - x_i|^2 + eps^2)^{1/2}
+// in FP64 with a fixed source order (j ascending), so results are
+// deterministic.  One thread per target; sources stream through shared
+// memory in tiles of kTile bodies.  The softened star term of
+// src/physics/BHTree.cu:547-553 is not included: callers add it in FP64.
+#include <algorithm>
+
+#include "capi_util.h"
+#include "common.cuh"
+
+namespace nb {
+namespace {
+
+constexpr int kThreadsD = 256;
+constexpr int kTile = 256;
+
+__global__ void __launch_bounds__(kThreadsD)
+k_direct(const double* __restrict__ x, const double* __restrict__ y,
+         const double* __restrict__ z, const float* __restrict__ m, int n,
+         const int* __restrict__ targets, int nt, double eps2, double* __restrict__ ax,
+         double* __restrict__ ay, double* __restrict__ az, double* __restrict__ phi) {
+  __shared__ double4 src[kTile];
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = t < nt;
+  const int i = live ? (targets ? targets[t] : t) : -1;
+  const double xi = live ? x[i] : 0.0, yi = live ? y[i] : 0.0, zi = live ? z[i] : 0.0;
+  double sx = 0.0, sy = 0.0, sz = 0.0, sp = 0.0;
+  for (int base = 0; base < n; base += kTile) {
+    const int j = base + threadIdx.x;
+    __syncthreads();
+    src[threadIdx.x] = (j < n) ? make_double4(x[j], y[j], z[j], (double)m[j])
+                               : make_double4(0.0, 0.0, 0.0, 0.0);
+    __syncthreads();
+    const int cnt = min(kTile, n - base);
+    if (!live) continue;
+#pragma unroll 4
+    for (int k = 0; k < cnt; ++k) {
+      const double4 s = src[k];
+      const double dx = s.x - xi, dy = s.y - yi, dz = s.z - zi;
+      const double r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
+      const double inv = (base + k == i) ? 0.0 : rsqrt(r2);
+      const double minv = s.w * inv;
+      const double f = minv * inv * inv;
+      sx = fma(f, dx, sx);
+      sy = fma(f, dy, sy);
+      sz = fma(f, dz, sz);
+      sp -= minv;
+    }
+  }
+  if (live) {
+    if (ax) ax[t] = sx;
+    if (ay) ay[t] = sy;
+    if (az) az[t] = sz;
+    if (phi) phi[t] = sp;
+  }
+}
+
+}  // namespace
+}  // namespace nb
+
+extern "C" int nbody_direct_f64(const double* x, const double* y, const double* z,
+                                const float* mass, int n, const int* targets, int n_targets,
+                                double eps, double* ax, double* ay, double* az, double* phi) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(x && y && z && mass, "nbody_direct_f64: null array");
+    NBODY_REQUIRE(n >= 0, "nbody_direct_f64: negative n");
+    const int nt = targets ? n_targets : n;
+    NBODY_REQUIRE(nt >= 0, "nbody_direct_f64: negative target count");
+    if (nt == 0 || n == 0) return NBODY_OK;
+    nb::k_direct<<<nb::div_up(nt, nb::kThreadsD), nb::kThreadsD>>>(
+        x, y, z, mass, n, targets, nt, eps * eps, ax, ay, az, phi);
+    nb::check(cudaGetLastError(), "k_direct launch");
+    nb::check(cudaDeviceSynchronize(), "k_direct");
+  })
+}

@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "capi_util.h"
@@ -27,6 +28,12 @@ namespace nb {
 namespace {
 
 constexpr int kThreads = 256;
+
+// State storage: float (the reference's), double, or hi/lo float pairs.
+template <typename R>
+constexpr bool kIsF32 = std::is_same<R, float>::value;
+template <typename R>
+constexpr bool kIsF64 = std::is_same<R, double>::value;
 
 int stream_grid(int n) { return std::max(1, std::min(div_up(n, kThreads), 148 * 8)); }
 
@@ -94,22 +101,23 @@ struct StreamArgs {
 // kBegin: K1 + drift (main.cu:104-107) + bbox of the new positions.
 template <typename R, bool kEnd, bool kBegin, bool kMulti = false>
 __global__ void __launch_bounds__(kThreads) k_stream(StateArrays<R> st, int n, StreamArgs a) {
+  using C = typename ComputeOf<R>::type;
   double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
   for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
        s += (long long)gridDim.x * blockDim.x) {
-    R x = st.v[0][s], y = st.v[1][s], z = st.v[2][s];
-    R vx = st.v[3][s], vy = st.v[4][s], vz = st.v[5][s];
-    R ax = (R)a.ax[s], ay = (R)a.ay[s], az = (R)a.az[s];
-    if (sizeof(R) == 8) {  // FP64 state: the stiff star term in FP64
+    C x = (C)st.v[0][s], y = (C)st.v[1][s], z = (C)st.v[2][s];
+    C vx = (C)st.v[3][s], vy = (C)st.v[4][s], vz = (C)st.v[5][s];
+    C ax = (C)a.ax[s], ay = (C)a.ay[s], az = (C)a.az[s];
+    if (sizeof(C) == 8) {  // FP64 arithmetic: the stiff star term in FP64
       double sx, sy, sz;
       star_accel<double>((double)x, (double)y, (double)z, a.eps, a.star_mass, sx, sy, sz);
-      ax += (R)sx; ay += (R)sy; az += (R)sz;
+      ax += (C)sx; ay += (C)sy; az += (C)sz;
     }
     if (kEnd) {
       if (a.dvx) {  // bhtree_applyCollisionDeltaKernel (BHTree.cu:683-685)
-        vx += (R)a.dvx[s]; vy += (R)a.dvy[s]; vz += (R)a.dvz[s];
+        vx += (C)a.dvx[s]; vy += (C)a.dvy[s]; vz += (C)a.dvz[s];
       }
-      if (sizeof(R) == 4) {  // integrator_halfKickKernel: v += a dt/2 (one FMA)
+      if (sizeof(C) == 4) {  // integrator_halfKickKernel: v += a dt/2 (one FMA)
         vx = fmaf((float)ax, a.dth_f, (float)vx);
         vy = fmaf((float)ay, a.dth_f, (float)vy);
         vz = fmaf((float)az, a.dth_f, (float)vz);
@@ -119,12 +127,12 @@ __global__ void __launch_bounds__(kThreads) k_stream(StateArrays<R> st, int n, S
           vx = fvx; vy = fvy; vz = fvz;
         }
       } else {
-        vx = fma(ax, (R)a.dth, vx); vy = fma(ay, (R)a.dth, vy); vz = fma(az, (R)a.dth, vz);
-        if (a.decay > 0.0) gas_drag<R>(x, z, vx, vy, vz, (R)a.decay, (R)a.star_mass);
+        vx = fma(ax, (C)a.dth, vx); vy = fma(ay, (C)a.dth, vy); vz = fma(az, (C)a.dth, vz);
+        if (a.decay > 0.0) gas_drag<C>(x, z, vx, vy, vz, (C)a.decay, (C)a.star_mass);
       }
     }
     if (kBegin) {
-      if (sizeof(R) == 4) {
+      if (sizeof(C) == 4) {
         vx = fmaf((float)ax, a.dth_f, (float)vx);
         vy = fmaf((float)ay, a.dth_f, (float)vy);
         vz = fmaf((float)az, a.dth_f, (float)vz);
@@ -132,8 +140,8 @@ __global__ void __launch_bounds__(kThreads) k_stream(StateArrays<R> st, int n, S
         y = fmaf((float)vy, a.dt_f, (float)y);
         z = fmaf((float)vz, a.dt_f, (float)z);
       } else {
-        vx = fma(ax, (R)a.dth, vx); vy = fma(ay, (R)a.dth, vy); vz = fma(az, (R)a.dth, vz);
-        x = fma(vx, (R)a.dt, x); y = fma(vy, (R)a.dt, y); z = fma(vz, (R)a.dt, z);
+        vx = fma(ax, (C)a.dth, vx); vy = fma(ay, (C)a.dth, vy); vz = fma(az, (C)a.dth, vz);
+        x = fma(vx, (C)a.dt, x); y = fma(vy, (C)a.dt, y); z = fma(vz, (C)a.dt, z);
       }
       if (kMulti) {
         // per-disk bbox: one warp-wide reduction when the warp's bodies share
@@ -163,9 +171,9 @@ __global__ void __launch_bounds__(kThreads) k_stream(StateArrays<R> st, int n, S
         lo[1] = fmin(lo[1], (double)y); hi[1] = fmax(hi[1], (double)y);
         lo[2] = fmin(lo[2], (double)z); hi[2] = fmax(hi[2], (double)z);
       }
-      st.v[0][s] = x; st.v[1][s] = y; st.v[2][s] = z;
+      st.v[0][s] = (R)x; st.v[1][s] = (R)y; st.v[2][s] = (R)z;
     }
-    st.v[3][s] = vx; st.v[4][s] = vy; st.v[5][s] = vz;
+    st.v[3][s] = (R)vx; st.v[4][s] = (R)vy; st.v[5][s] = (R)vz;
   }
   if (kBegin && !kMulti) {
     __shared__ double sb[6][kThreads / 32];
@@ -203,7 +211,7 @@ k_unsort(StateArrays<R> st, int n, T* __restrict__ o0, T* __restrict__ o1, T* __
     o3[o] = (T)st.v[3][s]; o4[o] = (T)st.v[4][s]; o5[o] = (T)st.v[5][s];
     if (oax) {
       double gx = ax[s], gy = ay[s], gz = az[s];
-      if (sizeof(R) == 8) {
+      if (sizeof(typename ComputeOf<R>::type) == 8) {  // the walk left the star out
         double sx, sy, sz;
         star_accel<double>((double)st.v[0][s], (double)st.v[1][s], (double)st.v[2][s], eps,
                            star_mass, sx, sy, sz);
@@ -567,7 +575,7 @@ struct SimImpl : SimBase {
     cur = 1 - cur;
     mark(NBODY_PHASE_TREE);
     launch_build_topology(tw, n, st);
-    if (sizeof(R) == 8)
+    if (kIsF64<R>)
       launch_build_moments(tw, n, (const double*)s[cur].v[0], (const double*)s[cur].v[1],
                            (const double*)s[cur].v[2], st);
     else
@@ -585,7 +593,7 @@ struct SimImpl : SimBase {
     w.com = tw.oct.com; w.info = tw.oct.info; w.body = tw.body4; w.n = n;
     w.groups = tw.groups; w.n_groups = tw.n_groups;
     w.theta2 = p.theta * p.theta; w.eps = p.softening; w.star_mass = p.star_mass;
-    w.star_in_walk = (sizeof(R) == 4) ? 1 : 0;
+    w.star_in_walk = kIsF32<R> ? 1 : 0;
     w.leaf_max = p.leaf_max; w.pert = pp;
     w.ax = ax; w.ay = ay; w.az = az; w.scatter = nullptr;
     w.spill = spill; w.spill_cap = spill_cap; w.inter = inter; w.counters = counters;
@@ -602,7 +610,7 @@ struct SimImpl : SimBase {
   void collide() {
     NeighborArgs na{tw.oct.info, tw.oct.box_lo, tw.oct.box_hi, tw.body4, n,
                     tw.groups, tw.n_groups, p.leaf_max, spill, spill_cap, work, tw.status};
-    if (sizeof(R) == 4) {
+    if (kIsF32<R>) {
       launch_collide(na, (const float*)s[cur].v[3], (const float*)s[cur].v[4],
                      (const float*)s[cur].v[5], nullptr, p.r_coll, p.restitution, dvx, dvy, dvz,
                      st);
@@ -653,7 +661,7 @@ struct SimImpl : SimBase {
       compute_forces(k);
       if (coll) {
         collide();
-        launches += (sizeof(R) == 8) ? 4 : 1;
+        launches += kIsF32<R> ? 1 : 4;
       }
       mark(NBODY_PHASES);
       launches += 1;
@@ -675,6 +683,7 @@ struct SimImpl : SimBase {
 
 SimBase* make_sim(const nbody_sim_params& p, int n) {
   if (p.state_precision == NBODY_STATE_F64) return new SimImpl<double>(p, n);
+  if (p.state_precision == NBODY_STATE_F32X2) return new SimImpl<HiLo>(p, n);
   return new SimImpl<float>(p, n);
 }
 
@@ -710,7 +719,7 @@ int nbody_sim_create(const nbody_sim_params* p, int n, nbody_sim** out) {
     NBODY_REQUIRE(p && out, "nbody_sim_create: null argument");
     NBODY_REQUIRE(n > 0 && n < (1 << 27), "nbody_sim_create: n must be in [1, 2^27)");
     NBODY_REQUIRE(p->dt > 0.f, "nbody_sim_create: dt must be positive");
-    NBODY_REQUIRE(p->state_precision == NBODY_STATE_F32 || p->state_precision == NBODY_STATE_F64,
+    NBODY_REQUIRE(p->state_precision >= NBODY_STATE_F32 && p->state_precision <= NBODY_STATE_F32X2,
                   "nbody_sim_create: unknown state precision");
     *out = nullptr;
     nbody_sim* s = new nbody_sim{nb::make_sim(*p, n)};
@@ -975,7 +984,7 @@ struct EnsembleImpl : EnsembleBase {
     }
     ax = dalloc<float>(n, "ax"); ay = dalloc<float>(n, "ay"); az = dalloc<float>(n, "az");
     dvx = dalloc<float>(n, "dvx"); dvy = dalloc<float>(n, "dvy"); dvz = dalloc<float>(n, "dvz");
-    if (sizeof(R) == 8) vf = dalloc<float>(3 * (size_t)n, "velocity scratch");
+    if (!kIsF32<R>) vf = dalloc<float>(3 * (size_t)n, "velocity scratch");
     geoms = dalloc<TreeGeom>(D, "geoms");
     bbox = dalloc<unsigned long long>(6 * (size_t)D, "bboxes");
     group_disk = dalloc<int>(n, "group disk");
@@ -1121,7 +1130,7 @@ struct EnsembleImpl : EnsembleBase {
     check(cudaGetLastError(), "k_permute launch");
     cur = 1 - cur;
     launch_karras<uint64_t>(tw, keys64, n, key_bits, st);
-    if (sizeof(R) == 8)
+    if (kIsF64<R>)
       launch_octree<uint64_t>(tw, keys64, n, disk_bits, D, geoms, group_disk,
                               (const double*)s[cur].v[0], (const double*)s[cur].v[1],
                               (const double*)s[cur].v[2], st);
@@ -1134,7 +1143,7 @@ struct EnsembleImpl : EnsembleBase {
     w.com = tw.oct.com; w.info = tw.oct.info; w.body = tw.body4; w.n = n;
     w.groups = tw.groups; w.n_groups = tw.n_groups;
     w.theta2 = p.theta * p.theta; w.eps = p.softening; w.star_mass = p.star_mass;
-    w.star_in_walk = (sizeof(R) == 4) ? 1 : 0;
+    w.star_in_walk = kIsF32<R> ? 1 : 0;
     w.leaf_max = p.leaf_max;
     w.pert = pert_tab; w.pert_step = pert_step; w.n_disks = D; w.group_disk = group_disk;
     w.ax = ax; w.ay = ay; w.az = az; w.scatter = nullptr;
@@ -1149,7 +1158,7 @@ struct EnsembleImpl : EnsembleBase {
   void collide() {
     NeighborArgs na{tw.oct.info, tw.oct.box_lo, tw.oct.box_hi, tw.body4, n, tw.groups,
                     tw.n_groups, p.leaf_max, spill, spill_cap, work, tw.status, group_disk};
-    if (sizeof(R) == 4) {
+    if (kIsF32<R>) {
       launch_collide(na, (const float*)s[cur].v[3], (const float*)s[cur].v[4],
                      (const float*)s[cur].v[5], nullptr, p.r_coll, p.restitution, dvx, dvy, dvz,
                      st);
@@ -1315,6 +1324,7 @@ struct EnsembleImpl : EnsembleBase {
 
 EnsembleBase* make_ensemble(const nbody_sim_params& p, const nbody_disk_spec* d, int nd) {
   if (p.state_precision == NBODY_STATE_F64) return new EnsembleImpl<double>(p, d, nd);
+  if (p.state_precision == NBODY_STATE_F32X2) return new EnsembleImpl<HiLo>(p, d, nd);
   return new EnsembleImpl<float>(p, d, nd);
 }
 
@@ -1340,7 +1350,7 @@ int nbody_ensemble_create(const nbody_sim_params* p, const nbody_disk_spec* disk
     }
     NBODY_REQUIRE(total < (1 << 27), "nbody_ensemble_create: total bodies must be < 2^27");
     NBODY_REQUIRE(p->dt > 0.f, "nbody_ensemble_create: dt must be positive");
-    NBODY_REQUIRE(p->state_precision == NBODY_STATE_F32 || p->state_precision == NBODY_STATE_F64,
+    NBODY_REQUIRE(p->state_precision >= NBODY_STATE_F32 && p->state_precision <= NBODY_STATE_F32X2,
                   "nbody_ensemble_create: unknown state precision");
     *out = new nbody_ensemble{nb::make_ensemble(*p, disks, n_disks)};
   })

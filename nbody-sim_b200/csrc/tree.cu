@@ -619,6 +619,10 @@ template void launch_keys<float>(TreeWork&, const float*, const float*, const fl
                                  cudaStream_t);
 template void launch_keys<double>(TreeWork&, const double*, const double*, const double*, int,
                                   cudaStream_t);
+template void launch_bbox<HiLo>(TreeWork&, const HiLo*, const HiLo*, const HiLo*, int,
+                                cudaStream_t);
+template void launch_keys<HiLo>(TreeWork&, const HiLo*, const HiLo*, const HiLo*, int,
+                                cudaStream_t);
 
 void launch_gather_body4(TreeWork& w, const float* x, const float* y, const float* z,
                          const float* m, int n, cudaStream_t s) {
@@ -653,6 +657,8 @@ template void launch_keys_multi<float>(const float*, const float*, const float*,
 template void launch_keys_multi<double>(const double*, const double*, const double*, const int*,
                                         int, const TreeGeom*, uint64_t*, uint32_t*, int*,
                                         cudaStream_t);
+template void launch_keys_multi<HiLo>(const HiLo*, const HiLo*, const HiLo*, const int*, int,
+                                      const TreeGeom*, uint64_t*, uint32_t*, int*, cudaStream_t);
 
 template <typename K>
 void launch_karras(TreeWork& w, const K* keys, int n, int key_bits, cudaStream_t s) {
