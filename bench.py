@@ -56,13 +56,16 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-flush", action="store_true")
-    ap.add_argument("--workload", choices=["disk1m", "ensemble", "precision"], default="disk1m",
+    ap.add_argument("--workload", choices=["disk1m", "ensemble", "precision", "adjoint"],
+                    default="disk1m",
                     help="disk1m: the headline single disk; ensemble: 64 disks (C4) against "
                          "the same disks run one by one; precision: force error vs FP64 "
                          "direct sum over theta, and energy / L_y drift per state precision")
     ap.add_argument("--targets", type=int, default=16384,
                     help="precision study: force-error targets (seeded random subset)")
     ap.add_argument("--drift-steps", type=int, default=200)
+    ap.add_argument("--fd-components", type=int, default=1024,
+                    help="adjoint study: velocity components checked by central differences")
     ap.add_argument("--disks", type=int, default=64)
     ap.add_argument("--solo-steps", type=int, default=10,
                     help="timed steps per disk of the one-by-one comparison")
@@ -509,6 +512,137 @@ def run_precision(args, ws, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def run_adjoint(args, ws, rank, local):
+    """Gradient study: N = 65536 disk (r in [0.5, 5] AU, m = 1e-8, eps 1e-3),
+    gas drag 1e-3, perturber 3 M_J at 10 AU, 200 steps of dt 0.005, FP64
+    state.  Loss: mass-weighted mean e^2 of the bodies ending inside 2 AU.
+    Gradients with respect to every initial velocity and the perturber's mass
+    and radius through the adjoint engine; checked against FP64 central
+    differences (h = 1e-6 relative) of the frozen-tree forward on a seeded
+    set of velocity components and both perturber parameters.  Costs: the
+    recording forward and the backward against the plain engine
+    (nbody_sim, FP64 state, same physics) over the same steps."""
+    import torch
+    if rank != 0:
+        return
+    nb = importlib.import_module("nbody-sim_b200")
+    torch.cuda.set_device(local)
+    n, steps, pm, pr = 65536, 200, 3.0, 10.0
+    prm = nb.sim_params(dt=0.005, theta=0.5, softening=1e-3, star_mass=1.0, r_coll=0.0,
+                        restitution=0.0, gas_drag_rate=1e-3, perturber_enabled=1,
+                        perturber_mass_mjup=pm, perturber_radius_au=pr, perturber_phase0=0.0,
+                        state_precision=nb.STATE_F64, leaf_max=args.leaf_max)
+    d = nb.make_disk(n, 0.5, 5.0, 0.01, 0.005, 1.0, 0)
+    x0 = torch.tensor(np.stack([d["x"], d["y"], d["z"]]), dtype=torch.float64, device="cuda")
+    v0 = torch.tensor(np.stack([d["vx"], d["vy"], d["vz"]]), dtype=torch.float64, device="cuda")
+    mass = torch.full((n,), 1e-8, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    # plain forward: the engine, same physics and steps
+    sim = nb.Sim(prm, n)
+    sim.set_stream(stream.cuda_stream)
+    m_np = np.full(n, 1e-8, np.float32)
+    sim.set_state(d["x"], d["y"], d["z"], d["vx"], d["vy"], d["vz"], m_np)
+    sim.step(5)
+    sim.sync()
+    sim.set_state(d["x"], d["y"], d["z"], d["vx"], d["vy"], d["vz"], m_np)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    sim.step(steps)
+    b.record(stream)
+    sim.sync()
+    plain_ms = a.elapsed_time(b)
+    sim.close()
+
+    eng = nb.Adjoint(prm, n, steps)
+    eng.set_stream(stream.cuda_stream)
+    # warm-up (sizes the tape pool), then the measured gradient
+    eng.forward(x0, v0, mass, pm, pr)
+    x0r = x0.clone().requires_grad_(True)
+    v0r = v0.clone().requires_grad_(True)
+    pmt = torch.tensor(pm, dtype=torch.float64, device="cuda", requires_grad=True)
+    prt = torch.tensor(pr, dtype=torch.float64, device="cuda", requires_grad=True)
+    x, v = nb.disk_trajectory(eng, x0r, v0r, pmt, prt, mass)
+    loss = nb.eccentricity_loss(x, v, mass)
+    loss.backward()
+    st = eng.stats()
+
+    def loss_diff(plus, minus):
+        (xp, vp), (xm, vm) = plus, minus
+        rp = torch.sqrt((xp * xp).sum(0))
+        w = mass.to(torch.float64) * (rp < 2.0).to(torch.float64)
+        dd = nb.eccentricity2(xp, vp) - nb.eccentricity2(xm, vm)
+        return float(((w * dd).sum() / w.sum()).item())
+
+    speed = torch.sqrt((v0 * v0).sum(0))
+    rng = np.random.default_rng(0)
+    picks = rng.choice(3 * n, min(args.fd_components, 3 * n), replace=False)
+    def fd_v(c, k, hrel):
+        h = hrel * float(speed[k])
+        vp = v0.clone(); vp[c, k] += h
+        vm = v0.clone(); vm[c, k] -= h
+        return loss_diff(eng.replay(x0, vp, pm, pr, fp64=True),
+                         eng.replay(x0, vm, pm, pr, fp64=True)) / (2 * h)
+
+    rels, rels_best, skipped = [], [], 0
+    gnorm = float(v0r.grad.abs().max())
+    t0 = time.perf_counter()
+    for q in picks:
+        c, k = int(q) // n, int(q) % n
+        g_fd = fd_v(c, k, 1e-6)
+        g_ad = float(v0r.grad[c, k])
+        scale = max(abs(g_ad), abs(g_fd))
+        if scale < 1e-6 * gnorm:  # bodies that barely touch the loss: no signal to check
+            skipped += 1
+            continue
+        r6 = abs(g_ad - g_fd) / scale
+        rels.append(r6)
+        if r6 > 1e-4:  # round-off-limited quotient: the next larger step
+            g5 = fd_v(c, k, 1e-5)
+            r6 = min(r6, abs(g_ad - g5) / max(abs(g_ad), abs(g5)))
+        rels_best.append(r6)
+    fd_secs = time.perf_counter() - t0
+    par = {}
+    for name, g_ad, base in (("perturber_mass_mjup", float(pmt.grad), pm),
+                             ("perturber_radius_au", float(prt.grad), pr)):
+        row = {"adjoint": g_ad}
+        for hrel in (1e-4, 1e-5, 1e-6):
+            dpm = hrel * pm if name.startswith("perturber_mass") else 0.0
+            dpr = hrel * pr if dpm == 0.0 else 0.0
+            g_fd = loss_diff(eng.replay(x0, v0, pm + dpm, pr + dpr, fp64=True),
+                             eng.replay(x0, v0, pm - dpm, pr - dpr, fp64=True)) / (2 * hrel * base)
+            row[f"fd_h{hrel:g}"] = g_fd
+            row[f"rel_h{hrel:g}"] = abs(g_ad - g_fd) / max(abs(g_ad), abs(g_fd), 1e-300)
+        par[name] = row
+    rels = np.array(rels)
+    rels_best = np.array(rels_best)
+    line = {
+        "study": "adjoint", "n": n, "steps": steps, "data": "synthetic",
+        "config": {"workload": "Keplerian disk N=65536 r=[0.5,5] AU m=1e-8 eps=1e-3, drag 1e-3, "
+                               "perturber 3 MJ at 10 AU, dt 0.005, 200 steps, FP64 state, "
+                               "theta 0.5", "loss": "mass-weighted mean e^2, final r < 2 AU",
+                   "tape": "every level kept in HBM (no recomputation)"},
+        "loss": float(loss.item()),
+        "ms": {"plain_forward": plain_ms, "recording_forward": st.ms_forward,
+               "backward": st.ms_backward,
+               "gradient_over_plain_forward": (st.ms_forward + st.ms_backward) / plain_ms,
+               "backward_over_plain_forward": st.ms_backward / plain_ms},
+        "memory_bytes": {"tape": st.tape_bytes, "states": st.state_bytes},
+        "fd_check": {"components": int(len(picks)), "checked": int(len(rels)),
+                     "skipped_no_signal": skipped,
+                     "max_rel": float(rels.max()) if len(rels) else None,
+                     "median_rel": float(np.median(rels)) if len(rels) else None,
+                     "p99_rel": float(np.percentile(rels, 99)) if len(rels) else None,
+                     "within_1e-4": int((rels <= 1e-4).sum()),
+                     "within_1e-4_h1e-6_or_1e-5": int((rels_best <= 1e-4).sum()),
+                     "max_rel_h1e-6_or_1e-5": float(rels_best.max()) if len(rels_best) else None,
+                     "seconds": fd_secs},
+        "perturber": par,
+    }
+    eng.close()
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     ws, rank, local = dist_setup()
@@ -519,6 +653,8 @@ def main():
             run_ensemble(args, ws, rank, local)
         elif args.workload == "precision":
             run_precision(args, ws, rank, local)
+        elif args.workload == "adjoint":
+            run_adjoint(args, ws, rank, local)
         else:
             run_ours(args, ws, rank, local)
     finally:

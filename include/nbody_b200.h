@@ -428,6 +428,58 @@ typedef struct nbody_ensemble_stats {
 } nbody_ensemble_stats;
 int nbody_ensemble_stats_get(nbody_ensemble* e, nbody_ensemble_stats* out);
 
+/* ------------------------------------------------------------ adjoint --- */
+
+/* Reverse-mode derivatives of one disk's trajectory.  The step is the
+ * reference's order (src/main.cu:101-139: K1, drift, tree + force, perturber,
+ * K2, gas drag; collisions are not differentiable and must be off) with FP64
+ * state, FP32 tree-walk self-gravity, and FP64 star, perturber and drag; the
+ * perturber moves on the orbit of updatePerturber (Perturber.h:60-66)
+ * evaluated in FP64.  The forward records a tape in device memory -- every
+ * level's state, sort permutation, warp groups and source lists -- and the
+ * backward is the exact adjoint of that computation with the tree frozen.
+ * nbody_adjoint_replay runs the same frozen-tree forward from other initial
+ * conditions or perturber parameters (the function the backward
+ * differentiates; for finite-difference checks).  No reference counterpart:
+ * the reference has no derivatives.  All arrays are device arrays in caller
+ * order; calls are synchronous. */
+typedef struct nbody_adjoint nbody_adjoint;
+int nbody_adjoint_create(const nbody_sim_params* p, int n, int n_steps, nbody_adjoint** out);
+int nbody_adjoint_destroy(nbody_adjoint* a);
+int nbody_adjoint_set_stream(nbody_adjoint* a, void* cuda_stream);
+/* Records n_steps steps from (x0..vz0, mass) with the perturber at
+ * perturber_radius_au (M_J mass perturber_mass_mjup; params' phase and
+ * enable flag); writes the final state (outputs may be NULL). */
+int nbody_adjoint_forward(nbody_adjoint* a, const double* x0, const double* y0, const double* z0,
+                          const double* vx0, const double* vy0, const double* vz0,
+                          const float* mass, double perturber_mass_mjup,
+                          double perturber_radius_au, double* x, double* y, double* z,
+                          double* vx, double* vy, double* vz);
+/* fp64 = 1: the interactions in FP64 (sources at their FP64 positions and
+ * centres of mass) -- the finite-difference reference, free of the FP32
+ * rounding that a perturbed body's own terms add to a difference quotient. */
+int nbody_adjoint_replay(nbody_adjoint* a, const double* x0, const double* y0, const double* z0,
+                         const double* vx0, const double* vy0, const double* vz0,
+                         double perturber_mass_mjup, double perturber_radius_au, int fp64,
+                         double* x, double* y, double* z, double* vx, double* vy, double* vz);
+/* Adjoint (dL/d final state) -> dL/d initial state and
+ * g_perturber[0] = dL/d mass (per M_J), g_perturber[1] = dL/d radius (per AU). */
+int nbody_adjoint_backward(nbody_adjoint* a, const double* gx, const double* gy, const double* gz,
+                           const double* gvx, const double* gvy, const double* gvz,
+                           double* gx0, double* gy0, double* gz0, double* gvx0, double* gvy0,
+                           double* gvz0, double* g_perturber);
+typedef struct nbody_adjoint_stats {
+  int n;
+  int n_steps;
+  float ms_forward;    /* device time of the last recorded forward  */
+  float ms_backward;   /* device time of the last backward           */
+  float ms_replay;     /* device time of the last replay             */
+  unsigned long long tape_bytes;
+  unsigned long long state_bytes;
+  unsigned long long launches;
+} nbody_adjoint_stats;
+int nbody_adjoint_stats_get(nbody_adjoint* a, nbody_adjoint_stats* out);
+
 /* -------------------------------------------------------- diagnostics --- */
 
 /* FP64 direct sum of the softened self-gravity (no star term) for a list of

@@ -153,6 +153,13 @@ class nbody_ensemble_stats(C.Structure):
                 ("graph_launches", C.c_ulonglong)]
 
 
+class nbody_adjoint_stats(C.Structure):
+    _fields_ = [("n", C.c_int), ("n_steps", C.c_int), ("ms_forward", C.c_float),
+                ("ms_backward", C.c_float), ("ms_replay", C.c_float),
+                ("tape_bytes", C.c_ulonglong), ("state_bytes", C.c_ulonglong),
+                ("launches", C.c_ulonglong)]
+
+
 # (name, restype, argtypes): every symbol include/nbody_b200.h declares
 SIGNATURES = [
     ("nbody_last_error", C.c_char_p, []),
@@ -225,6 +232,15 @@ SIGNATURES = [
     ("nbody_ensemble_autotune", C.c_int, [_VP, _VP, C.c_int, _VP]),
     ("nbody_ensemble_set_graphs", C.c_int, [_VP, C.c_int]),
     ("nbody_ensemble_stats_get", C.c_int, [_VP, C.POINTER(nbody_ensemble_stats)]),
+    ("nbody_adjoint_create", C.c_int, [C.POINTER(nbody_sim_params), C.c_int, C.c_int,
+                                       C.POINTER(_VP)]),
+    ("nbody_adjoint_destroy", C.c_int, [_VP]),
+    ("nbody_adjoint_set_stream", C.c_int, [_VP, _VP]),
+    ("nbody_adjoint_forward", C.c_int, [_VP] + [_VP] * 7 + [C.c_double, C.c_double] + [_VP] * 6),
+    ("nbody_adjoint_replay", C.c_int, [_VP] + [_VP] * 6 + [C.c_double, C.c_double, C.c_int]
+     + [_VP] * 6),
+    ("nbody_adjoint_backward", C.c_int, [_VP] + [_VP] * 13),
+    ("nbody_adjoint_stats_get", C.c_int, [_VP, C.POINTER(nbody_adjoint_stats)]),
     ("nbody_direct_f64", C.c_int, [_VP] * 4 + [C.c_int, _VP, C.c_int, C.c_double] + [_VP] * 4),
     ("nbody_make_disk", C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                   C.c_double, C.c_uint64, _D, _D, _D, _D, _D, _D]),
@@ -766,6 +782,135 @@ class Ensemble:
         st = nbody_ensemble_stats()
         _check(lib.nbody_ensemble_stats_get(self.h, C.byref(st)))
         return st
+
+
+class Adjoint:
+    """Differentiable trajectory of one disk (nbody_adjoint_* in include/nbody_b200.h).
+
+    States are (3, n) float64 CUDA tensors (rows x, y, z) in caller order;
+    ``mass`` a float32 CUDA tensor.  ``forward`` records the tape,
+    ``backward`` returns the adjoints of the initial state and of the
+    perturber's (mass in M_J, radius in AU), ``replay`` reruns the frozen-tree
+    forward with other inputs."""
+
+    def __init__(self, params: nbody_sim_params, n: int, n_steps: int):
+        h = _VP()
+        _check(lib.nbody_adjoint_create(C.byref(params), n, n_steps, C.byref(h)))
+        self.h, self.n, self.n_steps, self.params = h, n, n_steps, params
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.nbody_adjoint_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr: int):
+        _check(lib.nbody_adjoint_set_stream(self.h, stream_ptr))
+
+    @staticmethod
+    def _rows(t):
+        t = t.contiguous()
+        return t, [t[k].data_ptr() for k in range(3)]
+
+    def forward(self, x0, v0, mass, perturber_mass_mjup: float, perturber_radius_au: float):
+        import torch
+        x0, px = self._rows(x0)
+        v0, pv = self._rows(v0)
+        x = torch.empty_like(x0)
+        v = torch.empty_like(v0)
+        _check(lib.nbody_adjoint_forward(self.h, *px, *pv, mass.data_ptr(),
+                                         float(perturber_mass_mjup), float(perturber_radius_au),
+                                         *[x[k].data_ptr() for k in range(3)],
+                                         *[v[k].data_ptr() for k in range(3)]))
+        return x, v
+
+    def replay(self, x0, v0, perturber_mass_mjup: float, perturber_radius_au: float,
+               fp64: bool = False):
+        import torch
+        x0, px = self._rows(x0)
+        v0, pv = self._rows(v0)
+        x = torch.empty_like(x0)
+        v = torch.empty_like(v0)
+        _check(lib.nbody_adjoint_replay(self.h, *px, *pv, float(perturber_mass_mjup),
+                                        float(perturber_radius_au), int(fp64),
+                                        *[x[k].data_ptr() for k in range(3)],
+                                        *[v[k].data_ptr() for k in range(3)]))
+        return x, v
+
+    def backward(self, gx, gv):
+        import torch
+        gx, pgx = self._rows(gx)
+        gv, pgv = self._rows(gv)
+        gx0 = torch.empty_like(gx)
+        gv0 = torch.empty_like(gv)
+        gp = (C.c_double * 2)()
+        _check(lib.nbody_adjoint_backward(self.h, *pgx, *pgv,
+                                          *[gx0[k].data_ptr() for k in range(3)],
+                                          *[gv0[k].data_ptr() for k in range(3)], gp))
+        return gx0, gv0, gp[0], gp[1]
+
+    def stats(self) -> nbody_adjoint_stats:
+        st = nbody_adjoint_stats()
+        _check(lib.nbody_adjoint_stats_get(self.h, C.byref(st)))
+        return st
+
+
+def _trajectory_function():
+    import torch
+
+    class DiskTrajectory(torch.autograd.Function):
+        """(x0, v0, perturber mass M_J, perturber radius AU) -> (x_N, v_N)
+        through an Adjoint engine; backward is the engine's reverse mode."""
+
+        @staticmethod
+        def forward(ctx, x0, v0, pmass, pradius, engine, mass):
+            x, v = engine.forward(x0, v0, mass, float(pmass), float(pradius))
+            ctx.engine = engine
+            return x, v
+
+        @staticmethod
+        def backward(ctx, gx, gv):
+            gx0, gv0, gm, gr = ctx.engine.backward(gx.to(torch.float64), gv.to(torch.float64))
+            dev = gx0.device
+            return (gx0, gv0, torch.tensor(gm, dtype=torch.float64, device=dev),
+                    torch.tensor(gr, dtype=torch.float64, device=dev), None, None)
+
+    return DiskTrajectory
+
+
+def disk_trajectory(engine: "Adjoint", x0, v0, pmass, pradius, mass):
+    """Autograd entry: differentiable final state of ``engine``'s trajectory."""
+    return _trajectory_function().apply(x0, v0, pmass, pradius, engine, mass)
+
+
+def eccentricity2(x, v, star_mass: float = 1.0):
+    """Per-body e^2 (torch, FP64): e = ((|v|^2 - mu/r) x - (x . v) v) / mu."""
+    import torch
+    r = torch.sqrt((x * x).sum(0))
+    v2 = (v * v).sum(0)
+    xv = (x * v).sum(0)
+    mu = float(star_mass)
+    e = ((v2 - mu / r) * x - xv * v) / mu
+    return (e * e).sum(0)
+
+
+def eccentricity_loss(x, v, mass, star_mass: float = 1.0, r_max: float = 2.0):
+    """Mass-weighted mean e^2 over bodies with final r < r_max (torch, FP64):
+    e = ((|v|^2 - mu/r) x - (x . v) v) / mu with mu = star_mass (G = 1)."""
+    import torch
+    r = torch.sqrt((x * x).sum(0))
+    v2 = (v * v).sum(0)
+    xv = (x * v).sum(0)
+    mu = float(star_mass)
+    e = ((v2 - mu / r) * x - xv * v) / mu
+    e2 = (e * e).sum(0)
+    w = mass.to(torch.float64) * (r < r_max).to(torch.float64)
+    return (w * e2).sum() / w.sum()
 
 
 def direct_f64(x, y, z, mass, eps: float, targets=None, want_acc=True, want_phi=False):

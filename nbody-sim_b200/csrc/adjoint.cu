@@ -1,0 +1,1153 @@
+// adjoint.cu -- reverse-mode derivatives of a disk's trajectory through the
+// frozen Barnes-Hut tree.
+//
+// The differentiable step is the reference's step order (src/main.cu:101-139:
+// K1, drift, tree + force, perturber, K2, gas drag; no collisions) with FP64
+// state.  Self-gravity comes from the FP32 tree walk; the star pull
+// (BHTree.cu:547-553 form), the perturber pull (Perturber.cu:20-34 form,
+// position as updatePerturber, Perturber.h:60-66) and the drag
+// (Integrator.cu:47-75) are FP64.
+//
+// Forward: every step records its tape -- the sort permutation, the warp
+// groups and each group's source list as sorted body ranges in evaluation
+// order (a recording variant of the walk) -- and the states of every time
+// level.  All of it stays in HBM.
+//
+// Backward: the exact adjoint of that computation with the tree frozen
+// (same permutations, groups and source lists).  Per level, the tape is
+// replayed with the interaction's vector-Jacobian product: the target side
+// accumulates -g in FP64, the source side adds +g to its centre of mass,
+// whose adjoint reaches each member body j in proportion m_j / M_node (a
+// range add over the sorted body range, resolved by one prefix sum).  The
+// star, perturber and drag Jacobians are applied per body in FP64; the
+// perturber's position and mass adjoints are reduced per level and chained
+// to (mass in M_J, orbit radius) on the host.
+//
+// Replay: the same frozen-tree forward with other initial conditions or
+// perturber parameters -- the function the backward differentiates, used
+// for finite-difference checks.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "capi_util.h"
+#include "common.cuh"
+#include "kernels.cuh"
+#include "moments.cuh"
+#include "physics.cuh"
+#include "walk_math.cuh"
+
+namespace nb {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kRW = 4;  // warps per block of the replay kernels
+constexpr int kTapeChunk = 32;
+
+int grid1(long long n) { return std::max(1, std::min(div_up(n, kThreads), 148 * 8)); }
+
+template <typename T>
+T* dalloc(size_t count, const char* what) {
+  T* p = nullptr;
+  check(cudaMalloc(&p, sizeof(T) * (count ? count : 1)), what);
+  return p;
+}
+
+// Sorted FP64 positions and float bodies of level positions (caller order).
+__global__ void k_gather_sorted(const uint32_t* __restrict__ perm, const double* __restrict__ x,
+                                const double* __restrict__ y, const double* __restrict__ z,
+                                const float* __restrict__ m, int n, double* __restrict__ xs,
+                                double* __restrict__ ys, double* __restrict__ zs,
+                                float4* __restrict__ body4) {
+  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
+       s += (long long)gridDim.x * blockDim.x) {
+    const uint32_t o = perm[s];
+    const double px = x[o], py = y[o], pz = z[o];
+    xs[s] = px; ys[s] = py; zs[s] = pz;
+    body4[s] = make_float4((float)px, (float)py, (float)pz, m[o]);
+  }
+}
+
+__global__ void k_copy_groups(const int2* __restrict__ src, const int* __restrict__ n_groups,
+                              int n, int2* __restrict__ dst, int* __restrict__ n_dst) {
+  const int ng = *n_groups;
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < n;
+       g += (long long)gridDim.x * blockDim.x)
+    if (g < ng) dst[g] = src[g];
+  if (blockIdx.x == 0 && threadIdx.x == 0) *n_dst = ng;
+}
+
+// FP64 acceleration of body o at level positions: float self-gravity plus the
+// softened star and perturber pulls.
+template <typename TA>
+__device__ __forceinline__ void total_accel(double x, double y, double z, TA sx, TA sy, TA sz,
+                                            double eps, double star_mass, double4 p, double& ax,
+                                            double& ay, double& az) {
+  double tx, ty, tz;
+  star_accel<double>(x, y, z, eps, star_mass, tx, ty, tz);
+  ax = (double)sx + tx;
+  ay = (double)sy + ty;
+  az = (double)sz + tz;
+  if (p.w != 0.0) {
+    const double dx = p.x - x, dy = p.y - y, dz = p.z - z;
+    const double r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, __dmul_rn(eps, eps))));
+    const double f = p.w / __dmul_rn(r2, sqrt(r2));
+    ax = fma(f, dx, ax);
+    ay = fma(f, dy, ay);
+    az = fma(f, dz, az);
+  }
+}
+
+template <typename TA>
+struct StepArgsT {
+  const double* x;   // level-L positions (caller order)
+  const double* y;
+  const double* z;
+  double* vx;        // in: v' of step L-1 (kEnd) or v_L; out: v_h of step L
+  double* vy;
+  double* vz;
+  const TA* ax;      // level-L self-gravity (float from the walk, double from
+  const TA* ay;      // the FP64 replay)
+  const TA* az;
+  double* lvx;       // out (optional): v_L
+  double* lvy;
+  double* lvz;
+  double* nx;        // out (kBegin): level L+1 positions
+  double* ny;
+  double* nz;
+  double4 pert;      // perturber (x, y, z, mass in M_sun) at t_L
+  double eps, star_mass, dt, dth, decay;
+  int drag;
+  int n;
+};
+using StepArgs = StepArgsT<float>;
+
+// Boundary of level L: [K2 + drag of step L-1] then [K1 + drift of step L].
+template <bool kEnd, bool kBegin, typename TA>
+__global__ void __launch_bounds__(kThreads) k_dstep(const StepArgsT<TA> a) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double x = a.x[i], y = a.y[i], z = a.z[i];
+    double vx = a.vx[i], vy = a.vy[i], vz = a.vz[i];
+    double ax, ay, az;
+    total_accel(x, y, z, a.ax[i], a.ay[i], a.az[i], a.eps, a.star_mass, a.pert, ax, ay, az);
+    if (kEnd) {
+      vx = fma(ax, a.dth, vx); vy = fma(ay, a.dth, vy); vz = fma(az, a.dth, vz);
+      if (a.drag) gas_drag<double>(x, z, vx, vy, vz, a.decay, a.star_mass);
+    }
+    if (a.lvx) { a.lvx[i] = vx; a.lvy[i] = vy; a.lvz[i] = vz; }
+    if (kBegin) {
+      vx = fma(ax, a.dth, vx); vy = fma(ay, a.dth, vy); vz = fma(az, a.dth, vz);
+      a.nx[i] = fma(vx, a.dt, x); a.ny[i] = fma(vy, a.dt, y); a.nz[i] = fma(vz, a.dt, z);
+    }
+    a.vx[i] = vx; a.vy[i] = vy; a.vz[i] = vz;
+  }
+}
+
+// ------------------------------------------------------------ tape replay
+struct ReplayArgs {
+  const float4* body4;      // level bodies, sorted order
+  const double4* ploc;      // moment prefix (range_moments)
+  const double4* tpre;
+  const uint32_t* perm;     // sorted -> caller
+  const int2* groups;
+  const int* n_groups;
+  const int2* group_tape;
+  const int2* tape;
+  const int* tape_next;
+  float eps2;
+  int* work;
+  int* status;
+  // forward replay: self-gravity out (caller order), float or (FP64 replay)
+  // double
+  float* ax;
+  float* ay;
+  float* az;
+  double* dax;
+  double* day;
+  double* daz;
+  const double* xs;         // FP64 replay: sorted FP64 positions
+  const double* ys;
+  const double* zs;
+  // adjoint replay: lam in (caller order), mu out (sorted), range adds
+  const double* lx;
+  const double* ly;
+  const double* lz;
+  double* mux;
+  double* muy;
+  double* muz;
+  double4* radd;            // n + 1 entries
+};
+
+struct ReplaySmem {
+  double4 dlst[32];  // FP64 replay sources
+  float4 lst[32];
+  int2 ent[32];
+  double mass[32];
+  float4 tme[32];
+  float4 tlam[32];
+  int tid[32];
+};
+
+// Loads up to 32 entries of the tape chain into the warp's list: source
+// float4 (centre of mass from the FP64 prefix sums, or the body itself).
+__device__ __forceinline__ void load_chunk(const ReplayArgs& a, ReplaySmem& w, int chunk, int k,
+                                           int lane) {
+  if (lane < k) {
+    const int2 e = a.tape[(size_t)chunk * kTapeChunk + lane];
+    float4 src;
+    double m;
+    if (e.y == 1) {
+      src = a.body4[e.x];
+      m = (double)src.w;
+    } else {
+      const double4 s = range_moments(a.ploc, a.tpre, e.x, e.x + e.y);
+      src = com_of(s, 0.f, 0.f, 0.f);
+      m = s.x;
+    }
+    w.lst[lane] = src;
+    w.ent[lane] = e;
+    w.mass[lane] = m;
+  }
+  __syncwarp();
+}
+
+// FP64 replay source: the body's FP64 position, or the node's FP64 centre
+// of mass, with its mass.
+__device__ __forceinline__ void load_chunk64(const ReplayArgs& a, ReplaySmem& w, int chunk,
+                                             int k, int lane) {
+  if (lane < k) {
+    const int2 e = a.tape[(size_t)chunk * kTapeChunk + lane];
+    if (e.y == 1) {
+      w.dlst[lane] = make_double4(a.xs[e.x], a.ys[e.x], a.zs[e.x], (double)a.body4[e.x].w);
+    } else {
+      const double4 s = range_moments(a.ploc, a.tpre, e.x, e.x + e.y);
+      const double inv = 1.0 / s.x;
+      w.dlst[lane] = make_double4(s.y * inv, s.z * inv, s.w * inv, s.x);
+    }
+  }
+  __syncwarp();
+}
+
+// The frozen-tree forward with FP64 interactions (the finite-difference
+// reference: free of the FP32 rounding that the perturbed body's own terms
+// would otherwise add to a difference quotient).
+__global__ void __launch_bounds__(kRW * 32) k_replay64(const ReplayArgs a) {
+  __shared__ ReplaySmem smem[kRW];
+  const int lane = threadIdx.x & 31;
+  ReplaySmem& w = smem[threadIdx.x >> 5];
+  const int n_groups = *a.n_groups;
+  const double eps2 = (double)a.eps2;
+  while (true) {
+    int g = 0;
+    if (lane == 0) g = atomicAdd(a.work, 1);
+    g = __shfl_sync(kFull, g, 0);
+    if (g >= n_groups) break;
+    const int2 gr = a.groups[g];
+    const int2 gt = a.group_tape[g];
+    const bool valid = lane < gr.y;
+    const int s = gr.x + (valid ? lane : 0);
+    const double px = a.xs[s], py = a.ys[s], pz = a.zs[s];
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    int chunk = gt.x, done = 0;
+    while (done < gt.y) {
+      const int k = min(kTapeChunk, gt.y - done);
+      load_chunk64(a, w, chunk, k, lane);
+      for (int j = 0; j < k; ++j) {
+        const double4 q = w.dlst[j];
+        const double dx = q.x - px, dy = q.y - py, dz = q.z - pz;
+        const double r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
+        if (r2 <= 0.0) continue;
+        const double inv = 1.0 / sqrt(r2);
+        const double f = q.w * inv * inv * inv;
+        sx = fma(f, dx, sx); sy = fma(f, dy, sy); sz = fma(f, dz, sz);
+      }
+      __syncwarp();
+      done += k;
+      if (done < gt.y) chunk = a.tape_next[chunk];
+      if (chunk < 0 && done < gt.y) {
+        if (lane == 0) atomicOr(a.status, kStatusTapeFull);
+        break;
+      }
+    }
+    if (valid) {
+      const uint32_t o = a.perm[s];
+      a.dax[o] = sx; a.day[o] = sy; a.daz[o] = sz;
+    }
+  }
+}
+
+template <bool kSoft, bool kAdj>
+__global__ void __launch_bounds__(kRW * 32) k_replay(const ReplayArgs a) {
+  __shared__ ReplaySmem smem[kRW];
+  const int lane = threadIdx.x & 31;
+  ReplaySmem& w = smem[threadIdx.x >> 5];
+  const int n_groups = *a.n_groups;
+  while (true) {
+    int g = 0;
+    if (lane == 0) g = atomicAdd(a.work, 1);
+    g = __shfl_sync(kFull, g, 0);
+    if (g >= n_groups) break;
+    const int2 gr = a.groups[g];
+    const int2 gt = a.group_tape[g];
+    if (gt.x < 0 && gt.y > 0) {  // never recorded (tape ran out)
+      if (lane == 0) atomicOr(a.status, kStatusTapeFull);
+      continue;
+    }
+    const bool valid = lane < gr.y;
+    const int s = gr.x + (valid ? lane : 0);
+    const float4 me = a.body4[s];
+    const uint32_t o = a.perm[s];
+    float3 acc = make_float3(0.f, 0.f, 0.f);
+    float3 lam = make_float3(0.f, 0.f, 0.f);
+    double mx = 0.0, my = 0.0, mz = 0.0;
+    if (kAdj) {
+      if (valid) lam = make_float3((float)a.lx[o], (float)a.ly[o], (float)a.lz[o]);
+      w.tme[lane] = me;
+      w.tlam[lane] = make_float4(lam.x, lam.y, lam.z, 0.f);
+      w.tid[lane] = valid ? s : -1;
+      __syncwarp();
+    }
+    int chunk = gt.x, done = 0;
+    while (done < gt.y) {
+      const int k = min(kTapeChunk, gt.y - done);
+      load_chunk(a, w, chunk, k, lane);
+      if (!kAdj) {
+        for (int j = 0; j < k; ++j) interact<kSoft>(w.lst[j], me, a.eps2, acc);
+      } else {
+        // target side: -g for every source except the body itself
+        for (int j = 0; j < k; ++j) {
+          const int2 e = w.ent[j];
+          if (e.y == 1 && e.x == s) continue;
+          const float3 gv = interact_vjp<kSoft>(w.lst[j], me, a.eps2, lam);
+          mx -= (double)gv.x; my -= (double)gv.y; mz -= (double)gv.z;
+        }
+        // source side: lane j sums +g over the group's targets and spreads
+        // it over the source's bodies in proportion to their mass
+        if (lane < k) {
+          const float4 src = w.lst[lane];
+          const int2 e = w.ent[lane];
+          float3 gs = make_float3(0.f, 0.f, 0.f);
+          for (int t = 0; t < gr.y; ++t) {
+            if (e.y == 1 && e.x == w.tid[t]) continue;
+            const float4 tl = w.tlam[t];
+            const float3 gv = interact_vjp<kSoft>(src, w.tme[t], a.eps2,
+                                                  make_float3(tl.x, tl.y, tl.z));
+            gs.x += gv.x; gs.y += gv.y; gs.z += gv.z;
+          }
+          const double inv = 1.0 / w.mass[lane];
+          const double wx = (double)gs.x * inv, wy = (double)gs.y * inv, wz = (double)gs.z * inv;
+          double4* lo = a.radd + e.x;
+          double4* hi = a.radd + e.x + e.y;
+          atomicAdd(&lo->x, wx); atomicAdd(&lo->y, wy); atomicAdd(&lo->z, wz);
+          atomicAdd(&hi->x, -wx); atomicAdd(&hi->y, -wy); atomicAdd(&hi->z, -wz);
+        }
+      }
+      __syncwarp();
+      done += k;
+      if (done < gt.y) chunk = a.tape_next[chunk];
+      if (chunk < 0 && done < gt.y) {  // broken chain: stop, report
+        if (lane == 0) atomicOr(a.status, kStatusTapeFull);
+        break;
+      }
+    }
+    if (valid) {
+      if (!kAdj) {
+        a.ax[o] = acc.x; a.ay[o] = acc.y; a.az[o] = acc.z;
+      } else {
+        a.mux[s] = mx; a.muy[s] = my; a.muz[s] = mz;
+      }
+    }
+  }
+}
+
+// Exclusive tile-local prefix sums of a double4 array in the layout of the
+// moment prefix (index i: sum over [tile start, i)), and the tile totals.
+__global__ void __launch_bounds__(kThreads)
+k_prefix4_tiles(const double4* __restrict__ in, int n, double4* __restrict__ ploc,
+                double4* __restrict__ tile_sum) {
+  constexpr int kPer = kMomentTile / kThreads;
+  __shared__ double4 s_w[kThreads / 32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const long long base = (long long)blockIdx.x * kMomentTile + (long long)tid * kPer;
+  double4 v[kPer];
+  double4 sum = make_double4(0, 0, 0, 0);
+#pragma unroll
+  for (int k = 0; k < kPer; ++k) {
+    const long long i = base + k;
+    v[k] = (i < n) ? in[i] : make_double4(0, 0, 0, 0);
+    sum = d4add(sum, v[k]);
+  }
+  double4 inc = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const double4 t = make_double4(__shfl_up_sync(kFull, inc.x, o), __shfl_up_sync(kFull, inc.y, o),
+                                   __shfl_up_sync(kFull, inc.z, o), __shfl_up_sync(kFull, inc.w, o));
+    if (lane >= o) inc = d4add(inc, t);
+  }
+  if (lane == 31) s_w[warp] = inc;
+  __syncthreads();
+  double4 run = d4sub(inc, sum);
+  for (int q = 0; q < warp; ++q) run = d4add(run, s_w[q]);
+#pragma unroll
+  for (int k = 0; k < kPer; ++k) {
+    const long long i = base + k;
+    if (i <= n) ploc[i] = run;
+    run = d4add(run, v[k]);
+  }
+  if (tid == kThreads - 1) tile_sum[blockIdx.x] = run;
+}
+
+// Exclusive scan of the tile totals (one warp, fixed order).
+__global__ void k_tiles_scan4(const double4* __restrict__ tile_sum, int ntiles,
+                              double4* __restrict__ tpre) {
+  if (threadIdx.x != 0) return;
+  double4 run = make_double4(0, 0, 0, 0);
+  for (int t = 0; t <= ntiles; ++t) {
+    tpre[t] = run;
+    if (t < ntiles) run = d4add(run, tile_sum[t]);
+  }
+}
+
+struct ApplyArgs {
+  const uint32_t* perm;
+  const float4* body4;
+  const double* mux;
+  const double* muy;
+  const double* muz;
+  const double4* rploc;     // prefix of the range adds
+  const double4* rtpre;
+  const double* x;          // level positions (caller order)
+  const double* y;
+  const double* z;
+  const double* lx;         // adjoint of the level's acceleration
+  const double* ly;
+  const double* lz;
+  double* gx;               // position adjoint (in/out)
+  double* gy;
+  double* gz;
+  double* gvx;              // velocity adjoint: v_h of the step that ends here
+  double* gvy;
+  double* gvz;
+  double* plx;              // out: pending acceleration adjoint dt/2 V_h
+  double* ply;
+  double* plz;
+  double4 pert;
+  double eps, star_mass, dt, dth;
+  double* pgrad;            // 4 per level: adjoint of perturber x, y, z, mass
+  int n;
+};
+
+// Per body (sorted index s, caller index o): the walk adjoint (target side
+// plus the mass-weighted share of its ancestors' centre-of-mass adjoints),
+// the FP64 star and perturber Jacobians, then -- unless this is level 0 --
+// the drift and first-kick adjoints of the step that produced the level.
+template <bool kStep>
+__global__ void __launch_bounds__(kThreads) k_adj_apply(const ApplyArgs a) {
+  __shared__ double red[4][kThreads / 32];
+  double pg[4] = {0.0, 0.0, 0.0, 0.0};
+  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < a.n;
+       s += (long long)gridDim.x * blockDim.x) {
+    const uint32_t o = a.perm[s];
+    const double4 P = range_moments(a.rploc, a.rtpre, 0, (int)s + 1);
+    const double m = (double)a.body4[s].w;
+    double gx = a.gx[o] + a.mux[s] + m * P.x;
+    double gy = a.gy[o] + a.muy[s] + m * P.y;
+    double gz = a.gz[o] + a.muz[s] + m * P.z;
+    const double x = a.x[o], y = a.y[o], z = a.z[o];
+    const double lx = a.lx[o], ly = a.ly[o], lz = a.lz[o];
+    {  // star: a = -M x / r^3, da/dx = -M (I/r^3 - 3 x x^T / r^5)
+      const double r2 = fma(x, x, fma(y, y, fma(z, z, a.eps * a.eps)));
+      const double inv = 1.0 / sqrt(r2);
+      const double inv3 = inv * inv * inv, inv5 = inv3 * inv * inv;
+      const double xl = x * lx + y * ly + z * lz;
+      gx -= a.star_mass * (lx * inv3 - 3.0 * x * xl * inv5);
+      gy -= a.star_mass * (ly * inv3 - 3.0 * y * xl * inv5);
+      gz -= a.star_mass * (lz * inv3 - 3.0 * z * xl * inv5);
+    }
+    if (a.pert.w != 0.0) {  // a = m_p d / r^3 with d = p - x
+      const double dx = a.pert.x - x, dy = a.pert.y - y, dz = a.pert.z - z;
+      const double r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, a.eps * a.eps)));
+      const double inv = 1.0 / sqrt(r2);
+      const double inv3 = inv * inv * inv, inv5 = inv3 * inv * inv;
+      const double dl = dx * lx + dy * ly + dz * lz;
+      const double jx = a.pert.w * (lx * inv3 - 3.0 * dx * dl * inv5);
+      const double jy = a.pert.w * (ly * inv3 - 3.0 * dy * dl * inv5);
+      const double jz = a.pert.w * (lz * inv3 - 3.0 * dz * dl * inv5);
+      gx -= jx; gy -= jy; gz -= jz;
+      pg[0] += jx; pg[1] += jy; pg[2] += jz;
+      pg[3] += dl * inv3;
+    }
+    a.gx[o] = gx; a.gy[o] = gy; a.gz[o] = gz;
+    if (kStep) {
+      const double vx = fma(a.dt, gx, a.gvx[o]);
+      const double vy = fma(a.dt, gy, a.gvy[o]);
+      const double vz = fma(a.dt, gz, a.gvz[o]);
+      a.gvx[o] = vx; a.gvy[o] = vy; a.gvz[o] = vz;
+      a.plx[o] = a.dth * vx; a.ply[o] = a.dth * vy; a.plz[o] = a.dth * vz;
+    }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    double v = pg[k];
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(kFull, v, off);
+    if (lane == 0) red[k][warp] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    double v = 0.0;
+    for (int q = 0; q < kThreads / 32; ++q) v += red[threadIdx.x][q];
+    if (v != 0.0) atomicAdd(a.pgrad + threadIdx.x, v);
+  }
+}
+
+struct DragAdjArgs {
+  // level L (start of the step) and L+1 (end), caller order
+  const double* x0;
+  const double* y0;
+  const double* z0;
+  const double* v0x;
+  const double* v0y;
+  const double* v0z;
+  const float* a0x;
+  const float* a0y;
+  const float* a0z;
+  const double* x1;
+  const double* y1;
+  const double* z1;
+  const float* a1x;
+  const float* a1y;
+  const float* a1z;
+  double4 p0, p1;
+  double eps, star_mass, dth, decay;
+  int drag;
+  // adjoints
+  double* gx;   // of x_{L+1} (in/out)
+  double* gy;
+  double* gz;
+  double* gvx;  // in: of v_{L+1}; out: of v' (= of v_h)
+  double* gvy;
+  double* gvz;
+  double* plx;  // in: pending (dt/2 V_h of step L+1, or 0); out: lam_{L+1}
+  double* ply;
+  double* plz;
+  int n;
+};
+
+// Second kick + drag of step L in reverse: v' = v_h + dt/2 A_{L+1} is
+// recomputed as the forward did (its v_phi sign selects the drag branch);
+// drag(x, v') = decay v' + (1 - decay) s sqrt(M) (-z, 0, x) r_xz^{-3/2}.
+__global__ void __launch_bounds__(kThreads) k_adj_drag(const DragAdjArgs a) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n;
+       i += (long long)gridDim.x * blockDim.x) {
+    double gvx = a.gvx[i], gvy = a.gvy[i], gvz = a.gvz[i];
+    if (a.drag) {
+      const double x = a.x1[i], z = a.z1[i];
+      const double rxz2 = fma(x, x, __dmul_rn(z, z));
+      if (!(rxz2 < 1e-12)) {
+        double ax0, ay0, az0, ax1, ay1, az1;
+        total_accel(a.x0[i], a.y0[i], a.z0[i], a.a0x[i], a.a0y[i], a.a0z[i], a.eps, a.star_mass,
+                    a.p0, ax0, ay0, az0);
+        total_accel(x, a.y1[i], z, a.a1x[i], a.a1y[i], a.a1z[i], a.eps, a.star_mass, a.p1, ax1,
+                    ay1, az1);
+        double vx = fma(ax0, a.dth, a.v0x[i]), vz = fma(az0, a.dth, a.v0z[i]);
+        vx = fma(ax1, a.dth, vx);
+        vz = fma(az1, a.dth, vz);
+        const double inv_r = 1.0 / sqrt(rxz2);
+        const double v_phi = __dmul_rn(fma(vx, -z, __dmul_rn(vz, x)), inv_r);
+        const double sgn = (v_phi >= 0.0) ? 1.0 : -1.0;
+        // u = (-z, 0, x) r^-3/2, r = r_xz; c = (1 - decay) s sqrt(M)
+        const double c = (1.0 - a.decay) * sgn * sqrt(a.star_mass);
+        const double r = sqrt(rxz2);
+        const double rm32 = 1.0 / (r * sqrt(r));          // r^-3/2
+        const double rm72 = rm32 / (rxz2);                // r^-7/2
+        const double dux_dx = 1.5 * x * z * rm72;
+        const double dux_dz = -rm32 + 1.5 * z * z * rm72;
+        const double duz_dx = rm32 - 1.5 * x * x * rm72;
+        const double duz_dz = -1.5 * x * z * rm72;
+        a.gx[i] += c * (dux_dx * gvx + duz_dx * gvz);
+        a.gz[i] += c * (dux_dz * gvx + duz_dz * gvz);
+        gvx *= a.decay; gvy *= a.decay; gvz *= a.decay;
+      }
+    }
+    a.gvx[i] = gvx; a.gvy[i] = gvy; a.gvz[i] = gvz;
+    a.plx[i] = fma(a.dth, gvx, a.plx[i]);
+    a.ply[i] = fma(a.dth, gvy, a.ply[i]);
+    a.plz[i] = fma(a.dth, gvz, a.plz[i]);
+  }
+}
+
+}  // namespace
+
+// ================================================================== host
+struct AdjointImpl {
+  nbody_sim_params p{};
+  int n = 0, steps = 0;
+  cudaStream_t st = 0;
+  bool own_stream = false;
+  TreeWork tw;
+  // per level L = 0..steps (caller order): positions, velocities, self-gravity
+  std::vector<double*> X, V;
+  std::vector<float*> A;
+  // per level tape: sort permutation, groups, group tape; the chunk pool is shared
+  std::vector<uint32_t*> perm;
+  std::vector<int2*> groups, gtape;
+  int* ngroups = nullptr;  // per level, device
+  int2* pool = nullptr;
+  int* pool_next = nullptr;
+  int* pool_used = nullptr;
+  int pool_cap = 0;
+  // scratch
+  double *xs = nullptr, *ys = nullptr, *zs = nullptr;
+  double *vw = nullptr, *xw = nullptr;      // work velocity (3n) and positions (2 x 3n)
+  float* aw = nullptr;                       // work self-gravity (3n)
+  double* aw64 = nullptr;                    // FP64 replay self-gravity (3n)
+  double *gx = nullptr, *gv = nullptr, *lam = nullptr, *mu = nullptr;  // 3n each
+  double4 *radd = nullptr, *rploc = nullptr, *rtiles = nullptr;
+  double* pgrad = nullptr;                   // 4 per level
+  float* mass = nullptr;
+  int* spill = nullptr;
+  int spill_cap = 4096;
+  int* work = nullptr;
+  unsigned long long* inter = nullptr;
+  double mjup = 0.0;
+  double pm = 0.0, pr = 1.0;  // perturber mass (M_J) and radius (AU) of the recorded forward
+  bool recorded = false;
+  float ms_forward = 0.f, ms_backward = 0.f, ms_replay = 0.f;
+  unsigned long long launches = 0;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+
+  AdjointImpl(const nbody_sim_params& prm, int nn, int nsteps) {
+    p = prm;
+    n = nn;
+    steps = nsteps;
+    if (p.leaf_max <= 0) p.leaf_max = 8;
+    check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "adjoint stream");
+    own_stream = true;
+    tree_alloc(tw, n);
+    tw.group_max = 32;
+    const size_t n3 = 3 * (size_t)n;
+    for (int L = 0; L <= steps; ++L) {
+      X.push_back(dalloc<double>(n3, "level positions"));
+      V.push_back(dalloc<double>(n3, "level velocities"));
+      A.push_back(dalloc<float>(n3, "level self-gravity"));
+      perm.push_back(dalloc<uint32_t>(n, "level permutation"));
+      groups.push_back(dalloc<int2>(n, "level groups"));
+      gtape.push_back(dalloc<int2>(n, "level group tape"));
+    }
+    ngroups = dalloc<int>(steps + 1, "level group counts");
+    xs = dalloc<double>(n, "sorted x"); ys = dalloc<double>(n, "sorted y");
+    zs = dalloc<double>(n, "sorted z");
+    vw = dalloc<double>(n3, "work velocity");
+    xw = dalloc<double>(2 * n3, "work positions");
+    aw = dalloc<float>(n3, "work self-gravity");
+    gx = dalloc<double>(n3, "position adjoint");
+    gv = dalloc<double>(n3, "velocity adjoint");
+    lam = dalloc<double>(n3, "acceleration adjoint");
+    mu = dalloc<double>(n3, "walk target adjoint");
+    radd = dalloc<double4>(n + 1, "range adds");
+    rploc = dalloc<double4>(n + 2, "range prefix");
+    rtiles = dalloc<double4>(2 * ((n + 1) / kMomentTile + 3), "range tiles");
+    pgrad = dalloc<double>(4 * (size_t)(steps + 1), "perturber adjoints");
+    mass = dalloc<float>(n, "mass");
+    spill = dalloc<int>((size_t)walk_spill_slots(0) * spill_cap, "walk spill");
+    work = dalloc<int>(1, "work");
+    inter = dalloc<unsigned long long>(1, "interactions");
+    pool_used = dalloc<int>(1, "tape chunks used");
+    nbody_config c;
+    nbody_config_defaults(&c);
+    c.perturber_enabled = 1;
+    c.perturber_mass_mjup = 1.f;
+    c.perturber_radius_AU = 1.f;
+    nbody_perturber q;
+    nbody_perturber_make(&c, &q);
+    mjup = (double)q.mass_msun;
+    check(cudaEventCreate(&e0), "event");
+    check(cudaEventCreate(&e1), "event");
+  }
+
+  ~AdjointImpl() {
+    if (st) cudaStreamSynchronize(st);
+    for (auto* q : X) cudaFree(q);
+    for (auto* q : V) cudaFree(q);
+    for (auto* q : A) cudaFree(q);
+    for (auto* q : perm) cudaFree(q);
+    for (auto* q : groups) cudaFree(q);
+    for (auto* q : gtape) cudaFree(q);
+    void* ptrs[] = {ngroups, pool, pool_next, pool_used, xs, ys, zs, vw, xw, aw, aw64, gx, gv, lam,
+                    mu, radd, rploc, rtiles, pgrad, mass, spill, work, inter};
+    for (void* q : ptrs)
+      if (q) cudaFree(q);
+    tree_free(tw);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (own_stream && st) cudaStreamDestroy(st);
+  }
+
+  void set_stream(cudaStream_t s) {
+    check(cudaStreamSynchronize(st), "adjoint sync");
+    if (own_stream) cudaStreamDestroy(st);
+    own_stream = false;
+    st = s;
+  }
+
+  // Perturber (x, y, z, mass in M_sun) at t_L = L dt in FP64: the orbit of
+  // makePerturber/updatePerturber (Perturber.h:39-66) evaluated in double.
+  double4 pert_at(int L, double mass_mj, double radius) const {
+    if (!p.perturber_enabled) return make_double4(0, 0, 0, 0);
+    const double om = std::sqrt((double)p.star_mass / (radius * radius * radius));
+    const double phi = (double)p.perturber_phase0 + om * ((double)L * (double)p.dt);
+    return make_double4(radius * std::cos(phi), 0.0, radius * std::sin(phi), mass_mj * mjup);
+  }
+
+  template <typename TA = float>
+  StepArgsT<TA> step_args(const double* x, double* v, const TA* a, double* lv, double* nx,
+                          double4 pert) const {
+    StepArgsT<TA> s{};
+    s.x = x; s.y = x + n; s.z = x + 2 * (size_t)n;
+    s.vx = v; s.vy = v + n; s.vz = v + 2 * (size_t)n;
+    s.ax = a; s.ay = a + n; s.az = a + 2 * (size_t)n;
+    s.lvx = lv; s.lvy = lv ? lv + n : nullptr; s.lvz = lv ? lv + 2 * (size_t)n : nullptr;
+    s.nx = nx; s.ny = nx ? nx + n : nullptr; s.nz = nx ? nx + 2 * (size_t)n : nullptr;
+    s.pert = pert;
+    s.eps = p.softening; s.star_mass = p.star_mass;
+    s.dt = (double)p.dt; s.dth = (double)p.dt * 0.5;
+    s.drag = p.gas_drag_rate > 0.f;
+    s.decay = s.drag ? std::exp(-(double)p.gas_drag_rate * (double)p.dt) : 1.0;
+    s.n = n;
+    return s;
+  }
+
+  template <typename TA>
+  void launch_step(bool end, bool begin, const StepArgsT<TA>& s) {
+    if (end && begin) k_dstep<true, true, TA><<<grid1(n), kThreads, 0, st>>>(s);
+    else if (end) k_dstep<true, false, TA><<<grid1(n), kThreads, 0, st>>>(s);
+    else k_dstep<false, true, TA><<<grid1(n), kThreads, 0, st>>>(s);
+    check(cudaGetLastError(), "k_dstep launch");
+    launches += 1;
+  }
+
+  // Tree + recording walk at level L's positions X[L] -> A[L] and the tape.
+  void record_level(int L) {
+    const double* x = X[L];
+    const size_t n1 = n, n2 = 2 * (size_t)n;
+    launch_bbox<double>(tw, x, x + n1, x + n2, n, st);
+    launch_keys<double>(tw, x, x + n1, x + n2, n, st);
+    radix_sort_pairs(tw.keys, tw.perm, tw.keys_alt, tw.perm_alt, tw.counts, n, 30, st);
+    k_gather_sorted<<<grid1(n), kThreads, 0, st>>>(tw.perm, x, x + n1, x + n2, mass, n, xs, ys,
+                                                   zs, tw.body4);
+    launch_build_topology(tw, n, st);
+    launch_build_moments(tw, n, xs, ys, zs, st);
+    check(cudaMemcpyAsync(perm[L], tw.perm, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st),
+          "tape permutation");
+    k_copy_groups<<<grid1(n), kThreads, 0, st>>>(tw.groups, tw.n_groups, n, groups[L],
+                                                 ngroups + L);
+    WalkArgs w{};
+    w.com = tw.oct.com; w.info = tw.oct.info; w.body = tw.body4; w.n = n;
+    w.groups = tw.groups; w.n_groups = tw.n_groups;
+    w.theta2 = p.theta * p.theta; w.eps = p.softening; w.star_mass = 0.f;
+    w.star_in_walk = 0; w.leaf_max = p.leaf_max; w.pert = nullptr;
+    float* a = A[L];
+    w.ax = a; w.ay = a + n1; w.az = a + n2; w.scatter = tw.perm;
+    w.spill = spill; w.spill_cap = spill_cap; w.inter = inter; w.counters = nullptr;
+    w.work = work; w.status = tw.status; w.targets_per_lane = 1;
+    w.tape = pool; w.tape_next = pool_next; w.tape_used = pool_used; w.tape_cap = pool_cap;
+    w.group_tape = gtape[L];
+    launch_walk(w, st);
+    // bbox, keys, 20 sort, gather, copy groups, karras, mark, 6 scans,
+    // moment tiles, tile scan, emit, walk
+    launches += 36;
+  }
+
+  void ensure_pool(int chunks) {
+    if (chunks <= pool_cap) return;
+    check(cudaStreamSynchronize(st), "tape pool sync");
+    if (pool) cudaFree(pool);
+    if (pool_next) cudaFree(pool_next);
+    pool_cap = chunks;
+    pool = dalloc<int2>((size_t)pool_cap * kTapeChunk, "tape pool");
+    pool_next = dalloc<int>(pool_cap, "tape links");
+  }
+
+  int read_status() {
+    int s = 0;
+    check(cudaStreamSynchronize(st), "adjoint sync");
+    check(cudaMemcpy(&s, tw.status, sizeof(int), cudaMemcpyDeviceToHost), "status");
+    return s;
+  }
+
+  // Forward with recording: initial state (device, caller order SoA) and the
+  // perturber's mass (M_J) and orbit radius (AU).
+  void forward(const double* const* x0, const float* m, double mass_mj, double radius) {
+    pm = mass_mj;
+    pr = radius;
+    check(cudaMemcpyAsync(mass, m, sizeof(float) * n, cudaMemcpyDeviceToDevice, st), "mass");
+    for (int k = 0; k < 3; ++k)
+      check(cudaMemcpyAsync(X[0] + (size_t)k * n, x0[k], sizeof(double) * n,
+                            cudaMemcpyDeviceToDevice, st),
+            "initial positions");
+    // size the tape pool from level 0, then record the whole run (again if
+    // the estimate fell short)
+    if (pool_cap == 0) ensure_pool(std::max(1024, n / 32 * 24));
+    for (int attempt = 0; attempt < 4; ++attempt) {
+      check(cudaMemsetAsync(tw.status, 0, sizeof(int), st), "status reset");
+      check(cudaMemsetAsync(pool_used, 0, sizeof(int), st), "tape reset");
+      record_level(0);
+      int used = 0;
+      check(cudaStreamSynchronize(st), "adjoint sync");
+      check(cudaMemcpy(&used, pool_used, sizeof(int), cudaMemcpyDeviceToHost), "tape used");
+      const long long need = (long long)used * (steps + 1) * 5 / 4 + 1024;
+      if (need > pool_cap) {
+        ensure_pool((int)std::min<long long>(need, 0x7fffffffLL / kTapeChunk));
+        continue;
+      }
+      break;
+    }
+    for (int attempt = 0; attempt < 3; ++attempt) {
+      check(cudaMemsetAsync(tw.status, 0, sizeof(int), st), "status reset");
+      check(cudaMemsetAsync(pool_used, 0, sizeof(int), st), "tape reset");
+      check(cudaEventRecord(e0, st), "event");
+      record_level(0);
+      for (int k = 0; k < 3; ++k)
+        check(cudaMemcpyAsync(vw + (size_t)k * n, x0[3 + k], sizeof(double) * n,
+                              cudaMemcpyDeviceToDevice, st),
+              "initial velocities");
+      for (int L = 0; L <= steps; ++L) {
+        const bool end = L > 0, begin = L < steps;
+        launch_step(end, begin, step_args<float>(X[L], vw, A[L], V[L],
+                                                 begin ? X[L + 1] : nullptr, pert_at(L, pm, pr)));
+        if (begin) record_level(L + 1);
+      }
+      check(cudaEventRecord(e1, st), "event");
+      const int s = read_status();
+      if (s & kStatusTapeFull) {
+        int used = 0;
+        check(cudaMemcpy(&used, pool_used, sizeof(int), cudaMemcpyDeviceToHost), "tape used");
+        ensure_pool((int)std::min<long long>((long long)used * 3 / 2 + 1024,
+                                             0x7fffffffLL / kTapeChunk));
+        continue;
+      }
+      if (s) throw ArgError("adjoint forward: device status " + std::to_string(s),
+                            NBODY_ERR_OVERFLOW);
+      check(cudaEventElapsedTime(&ms_forward, e0, e1), "event time");
+      recorded = true;
+      return;
+    }
+    throw ArgError("adjoint forward: tape pool could not be sized", NBODY_ERR_OVERFLOW);
+  }
+
+  // Level L's bodies in its recorded order and their moment prefix.
+  void level_bodies(int L, const double* x) {
+    const size_t n1 = n, n2 = 2 * (size_t)n;
+    k_gather_sorted<<<grid1(n), kThreads, 0, st>>>(perm[L], x, x + n1, x + n2, mass, n, xs, ys,
+                                                   zs, tw.body4);
+    launch_moment_prefix(tw, n, xs, ys, zs, st);
+    launches += 3;
+  }
+
+  ReplayArgs replay_args(int L) {
+    ReplayArgs r{};
+    r.body4 = tw.body4;
+    r.ploc = tw.mom_ploc;
+    r.tpre = moment_tile_prefix(tw, n);
+    r.perm = perm[L];
+    r.groups = groups[L];
+    r.n_groups = ngroups + L;
+    r.group_tape = gtape[L];
+    r.tape = pool;
+    r.tape_next = pool_next;
+    r.eps2 = p.softening * p.softening;
+    r.work = work;
+    r.status = tw.status;
+    return r;
+  }
+
+  void launch_replay(const ReplayArgs& r, bool adj, bool fp64 = false) {
+    check(cudaMemsetAsync(work, 0, sizeof(int), st), "replay work reset");
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = std::max(1, std::min(sms * 8, div_up(n, kRW)));
+    const bool soft = p.softening > 0.f;
+    if (fp64) {
+      k_replay64<<<grid, kRW * 32, 0, st>>>(r);
+    } else if (adj) {
+      if (soft) k_replay<true, true><<<grid, kRW * 32, 0, st>>>(r);
+      else k_replay<false, true><<<grid, kRW * 32, 0, st>>>(r);
+    } else {
+      if (soft) k_replay<true, false><<<grid, kRW * 32, 0, st>>>(r);
+      else k_replay<false, false><<<grid, kRW * 32, 0, st>>>(r);
+    }
+    check(cudaGetLastError(), "k_replay launch");
+    launches += 1;
+  }
+
+  // Frozen-tape forward from new initial conditions and perturber
+  // parameters; final state into out (device).  fp64: FP64 interactions.
+  void replay(const double* const* x0, double mass_mj, double radius, double* const* out,
+              bool fp64) {
+    if (!recorded) throw ArgError("adjoint replay: no recorded forward", NBODY_ERR_STATE);
+    const size_t n3 = 3 * (size_t)n;
+    double* xa = xw;
+    double* xb = xw + n3;
+    for (int k = 0; k < 3; ++k) {
+      check(cudaMemcpyAsync(xa + (size_t)k * n, x0[k], sizeof(double) * n,
+                            cudaMemcpyDeviceToDevice, st), "replay positions");
+      check(cudaMemcpyAsync(vw + (size_t)k * n, x0[3 + k], sizeof(double) * n,
+                            cudaMemcpyDeviceToDevice, st), "replay velocities");
+    }
+    check(cudaMemsetAsync(tw.status, 0, sizeof(int), st), "status reset");
+    check(cudaEventRecord(e0, st), "event");
+    for (int L = 0; L <= steps; ++L) {
+      level_bodies(L, xa);
+      ReplayArgs r = replay_args(L);
+      const bool end = L > 0, begin = L < steps;
+      if (fp64) {
+        if (!aw64) aw64 = dalloc<double>(3 * (size_t)n, "FP64 replay self-gravity");
+        r.dax = aw64; r.day = aw64 + n; r.daz = aw64 + 2 * (size_t)n;
+        r.xs = xs; r.ys = ys; r.zs = zs;
+        launch_replay(r, false, true);
+        launch_step(end, begin, step_args<double>(xa, vw, aw64, nullptr, begin ? xb : nullptr,
+                                                  pert_at(L, mass_mj, radius)));
+      } else {
+        r.ax = aw; r.ay = aw + n; r.az = aw + 2 * (size_t)n;
+        launch_replay(r, false);
+        launch_step(end, begin, step_args<float>(xa, vw, aw, nullptr, begin ? xb : nullptr,
+                                                 pert_at(L, mass_mj, radius)));
+      }
+      if (begin) std::swap(xa, xb);
+    }
+    check(cudaEventRecord(e1, st), "event");
+    for (int k = 0; k < 3; ++k) {
+      check(cudaMemcpyAsync(out[k], xa + (size_t)k * n, sizeof(double) * n,
+                            cudaMemcpyDeviceToDevice, st), "replay out");
+      check(cudaMemcpyAsync(out[3 + k], vw + (size_t)k * n, sizeof(double) * n,
+                            cudaMemcpyDeviceToDevice, st), "replay out");
+    }
+    const int s = read_status();
+    if (s) throw ArgError("adjoint replay: device status " + std::to_string(s), NBODY_ERR_OVERFLOW);
+    check(cudaEventElapsedTime(&ms_replay, e0, e1), "event time");
+  }
+
+  // Force adjoint at level L: lam (caller order) -> added to gx; then, for
+  // L > 0, the drift and first-kick adjoints of step L-1.
+  void force_adjoint(int L, bool step) {
+    level_bodies(L, X[L]);
+    check(cudaMemsetAsync(radd, 0, sizeof(double4) * (n + 1), st), "range add reset");
+    ReplayArgs r = replay_args(L);
+    r.lx = lam; r.ly = lam + n; r.lz = lam + 2 * (size_t)n;
+    r.mux = mu; r.muy = mu + n; r.muz = mu + 2 * (size_t)n;
+    r.radd = radd;
+    launch_replay(r, true);
+    const int ntiles = (n + 1) / kMomentTile + 1;
+    double4* tpre = rtiles + (ntiles + 1);
+    k_prefix4_tiles<<<ntiles, kThreads, 0, st>>>(radd, n + 1, rploc, rtiles);
+    k_tiles_scan4<<<1, 32, 0, st>>>(rtiles, ntiles, tpre);
+    ApplyArgs a{};
+    a.perm = perm[L]; a.body4 = tw.body4;
+    a.mux = mu; a.muy = mu + n; a.muz = mu + 2 * (size_t)n;
+    a.rploc = rploc; a.rtpre = tpre;
+    a.x = X[L]; a.y = X[L] + n; a.z = X[L] + 2 * (size_t)n;
+    a.lx = lam; a.ly = lam + n; a.lz = lam + 2 * (size_t)n;
+    a.gx = gx; a.gy = gx + n; a.gz = gx + 2 * (size_t)n;
+    a.gvx = gv; a.gvy = gv + n; a.gvz = gv + 2 * (size_t)n;
+    a.plx = lam; a.ply = lam + n; a.plz = lam + 2 * (size_t)n;  // lam is consumed per body
+    a.pert = pert_at(L, pm, pr);
+    a.eps = p.softening; a.star_mass = p.star_mass;
+    a.dt = (double)p.dt; a.dth = (double)p.dt * 0.5;
+    a.pgrad = pgrad + 4 * (size_t)L;
+    a.n = n;
+    if (step) k_adj_apply<true><<<grid1(n), kThreads, 0, st>>>(a);
+    else k_adj_apply<false><<<grid1(n), kThreads, 0, st>>>(a);
+    check(cudaGetLastError(), "adjoint apply launch");
+    launches += 4;
+  }
+
+  // Adjoint of the final state (device, caller order) -> adjoint of the
+  // initial state and of (perturber mass in M_J, perturber radius in AU).
+  void backward(const double* const* g_final, double* const* g_init, double* g_par) {
+    if (!recorded) throw ArgError("adjoint backward: no recorded forward", NBODY_ERR_STATE);
+    const size_t n3 = 3 * (size_t)n;
+    for (int k = 0; k < 3; ++k) {
+      check(cudaMemcpyAsync(gx + (size_t)k * n, g_final[k], sizeof(double) * n,
+                            cudaMemcpyDeviceToDevice, st), "final adjoint");
+      check(cudaMemcpyAsync(gv + (size_t)k * n, g_final[3 + k], sizeof(double) * n,
+                            cudaMemcpyDeviceToDevice, st), "final adjoint");
+    }
+    check(cudaMemsetAsync(lam, 0, sizeof(double) * n3, st), "pending reset");
+    check(cudaMemsetAsync(pgrad, 0, sizeof(double) * 4 * (steps + 1), st), "perturber reset");
+    check(cudaMemsetAsync(tw.status, 0, sizeof(int), st), "status reset");
+    check(cudaEventRecord(e0, st), "event");
+    const double dth = (double)p.dt * 0.5;
+    const bool drag = p.gas_drag_rate > 0.f;
+    const double decay = drag ? std::exp(-(double)p.gas_drag_rate * (double)p.dt) : 1.0;
+    for (int L = steps - 1; L >= 0; --L) {
+      DragAdjArgs d{};
+      d.x0 = X[L]; d.y0 = X[L] + n; d.z0 = X[L] + 2 * (size_t)n;
+      d.v0x = V[L]; d.v0y = V[L] + n; d.v0z = V[L] + 2 * (size_t)n;
+      d.a0x = A[L]; d.a0y = A[L] + n; d.a0z = A[L] + 2 * (size_t)n;
+      d.x1 = X[L + 1]; d.y1 = X[L + 1] + n; d.z1 = X[L + 1] + 2 * (size_t)n;
+      d.a1x = A[L + 1]; d.a1y = A[L + 1] + n; d.a1z = A[L + 1] + 2 * (size_t)n;
+      d.p0 = pert_at(L, pm, pr);
+      d.p1 = pert_at(L + 1, pm, pr);
+      d.eps = p.softening; d.star_mass = p.star_mass; d.dth = dth; d.decay = decay;
+      d.drag = drag;
+      d.gx = gx; d.gy = gx + n; d.gz = gx + 2 * (size_t)n;
+      d.gvx = gv; d.gvy = gv + n; d.gvz = gv + 2 * (size_t)n;
+      d.plx = lam; d.ply = lam + n; d.plz = lam + 2 * (size_t)n;
+      d.n = n;
+      k_adj_drag<<<grid1(n), kThreads, 0, st>>>(d);
+      check(cudaGetLastError(), "k_adj_drag launch");
+      launches += 1;
+      force_adjoint(L + 1, true);
+    }
+    force_adjoint(0, false);
+    check(cudaEventRecord(e1, st), "event");
+    for (int k = 0; k < 3; ++k) {
+      check(cudaMemcpyAsync(g_init[k], gx + (size_t)k * n, sizeof(double) * n,
+                            cudaMemcpyDeviceToDevice, st), "initial adjoint");
+      check(cudaMemcpyAsync(g_init[3 + k], gv + (size_t)k * n, sizeof(double) * n,
+                            cudaMemcpyDeviceToDevice, st), "initial adjoint");
+    }
+    std::vector<double> pg(4 * (size_t)(steps + 1));
+    check(cudaMemcpyAsync(pg.data(), pgrad, sizeof(double) * pg.size(), cudaMemcpyDeviceToHost,
+                          st), "perturber adjoints");
+    const int s = read_status();
+    if (s) throw ArgError("adjoint backward: device status " + std::to_string(s),
+                          NBODY_ERR_OVERFLOW);
+    check(cudaEventElapsedTime(&ms_backward, e0, e1), "event time");
+    // chain: p(t) = r (cos phi, 0, sin phi), phi = phi0 + sqrt(M / r^3) t;
+    // mass in M_sun = mass_mj * mjup
+    double gm = 0.0, gr = 0.0;
+    if (p.perturber_enabled) {
+      const double r = pr;
+      const double om = std::sqrt((double)p.star_mass / (r * r * r));
+      for (int L = 0; L <= steps; ++L) {
+        const double t = (double)L * (double)p.dt;
+        const double phi = (double)p.perturber_phase0 + om * t;
+        const double c = std::cos(phi), sn = std::sin(phi);
+        const double k = -1.5 * om * t;  // r dphi/dr
+        const double dpx = c - k * sn, dpz = sn + k * c;
+        gr += pg[4 * L + 0] * dpx + pg[4 * L + 2] * dpz;
+        gm += pg[4 * L + 3] * mjup;
+      }
+    }
+    g_par[0] = gm;
+    g_par[1] = gr;
+  }
+
+  size_t tape_bytes() const {
+    return (size_t)pool_cap * (kTapeChunk * sizeof(int2) + sizeof(int)) +
+           (size_t)(steps + 1) * n * (sizeof(uint32_t) + 2 * sizeof(int2));
+  }
+  size_t state_bytes() const {
+    return (size_t)(steps + 1) * n * (6 * sizeof(double) + 3 * sizeof(float));
+  }
+};
+
+}  // namespace nb
+
+struct nbody_adjoint {
+  nb::AdjointImpl* impl;
+};
+
+extern "C" {
+
+int nbody_adjoint_create(const nbody_sim_params* p, int n, int n_steps, nbody_adjoint** out) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(p && out, "nbody_adjoint_create: null argument");
+    *out = nullptr;
+    NBODY_REQUIRE(n >= 2 && n < (1 << 26), "nbody_adjoint_create: n must be in [2, 2^26)");
+    NBODY_REQUIRE(n_steps >= 1, "nbody_adjoint_create: n_steps must be >= 1");
+    NBODY_REQUIRE(p->dt > 0.f, "nbody_adjoint_create: dt must be positive");
+    NBODY_REQUIRE(p->r_coll <= 0.f,
+                  "nbody_adjoint_create: collisions are not differentiable (r_coll must be 0)");
+    *out = new nbody_adjoint{new nb::AdjointImpl(*p, n, n_steps)};
+  })
+}
+
+int nbody_adjoint_destroy(nbody_adjoint* a) {
+  NBODY_API_BODY({
+    if (a) {
+      delete a->impl;
+      delete a;
+    }
+  })
+}
+
+int nbody_adjoint_set_stream(nbody_adjoint* a, void* stream) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(a, "nbody_adjoint_set_stream: null handle");
+    a->impl->set_stream((cudaStream_t)stream);
+  })
+}
+
+int nbody_adjoint_forward(nbody_adjoint* a, const double* x0, const double* y0, const double* z0,
+                          const double* vx0, const double* vy0, const double* vz0,
+                          const float* mass, double perturber_mass_mjup,
+                          double perturber_radius_au, double* x, double* y, double* z,
+                          double* vx, double* vy, double* vz) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(a && x0 && y0 && z0 && vx0 && vy0 && vz0 && mass,
+                  "nbody_adjoint_forward: null input");
+    NBODY_REQUIRE(perturber_radius_au > 0.0, "nbody_adjoint_forward: radius must be positive");
+    const double* in[6] = {x0, y0, z0, vx0, vy0, vz0};
+    nb::AdjointImpl* m = a->impl;
+    m->forward(in, mass, perturber_mass_mjup, perturber_radius_au);
+    double* out[6] = {x, y, z, vx, vy, vz};
+    const size_t n = m->n;
+    for (int k = 0; k < 6; ++k)
+      if (out[k]) {
+        const double* src = (k < 3 ? m->X[m->steps] : m->V[m->steps]) + (k % 3) * n;
+        nb::check(cudaMemcpyAsync(out[k], src, sizeof(double) * n, cudaMemcpyDeviceToDevice,
+                                  m->st), "forward out");
+      }
+    nb::check(cudaStreamSynchronize(m->st), "forward sync");
+  })
+}
+
+int nbody_adjoint_replay(nbody_adjoint* a, const double* x0, const double* y0, const double* z0,
+                         const double* vx0, const double* vy0, const double* vz0,
+                         double perturber_mass_mjup, double perturber_radius_au, int fp64,
+                         double* x, double* y, double* z, double* vx, double* vy, double* vz) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(a && x0 && y0 && z0 && vx0 && vy0 && vz0 && x && y && z && vx && vy && vz,
+                  "nbody_adjoint_replay: null array");
+    NBODY_REQUIRE(perturber_radius_au > 0.0, "nbody_adjoint_replay: radius must be positive");
+    const double* in[6] = {x0, y0, z0, vx0, vy0, vz0};
+    double* out[6] = {x, y, z, vx, vy, vz};
+    a->impl->replay(in, perturber_mass_mjup, perturber_radius_au, out, fp64 != 0);
+  })
+}
+
+int nbody_adjoint_backward(nbody_adjoint* a, const double* gx, const double* gy, const double* gz,
+                           const double* gvx, const double* gvy, const double* gvz,
+                           double* gx0, double* gy0, double* gz0, double* gvx0, double* gvy0,
+                           double* gvz0, double* g_perturber) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(a && gx && gy && gz && gvx && gvy && gvz && gx0 && gy0 && gz0 && gvx0 &&
+                      gvy0 && gvz0 && g_perturber,
+                  "nbody_adjoint_backward: null array");
+    const double* gin[6] = {gx, gy, gz, gvx, gvy, gvz};
+    double* gout[6] = {gx0, gy0, gz0, gvx0, gvy0, gvz0};
+    a->impl->backward(gin, gout, g_perturber);
+  })
+}
+
+int nbody_adjoint_stats_get(nbody_adjoint* a, nbody_adjoint_stats* out) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(a && out, "nbody_adjoint_stats_get: null argument");
+    nb::AdjointImpl* m = a->impl;
+    out->n = m->n;
+    out->n_steps = m->steps;
+    out->ms_forward = m->ms_forward;
+    out->ms_backward = m->ms_backward;
+    out->ms_replay = m->ms_replay;
+    out->tape_bytes = m->tape_bytes();
+    out->state_bytes = m->state_bytes();
+    out->launches = m->launches;
+  })
+}
+
+}  // extern "C"

@@ -18,6 +18,7 @@ enum StatusBits : int {
   kStatusUnionFindLimit = 2,  // FoF union loop hit its iteration cap
   kStatusTreeLimit = 4,       // tree bottom-up climb exceeded its bound
   kStatusNonFinite = 8,       // a non-finite position reached key generation
+  kStatusTapeFull = 16,       // a recording walk ran out of tape chunks
 };
 
 // Hi/lo float pair state (NBODY_STATE_F32X2): value = hi + lo with

@@ -109,6 +109,13 @@ void launch_build_topology(TreeWork& w, int n, cudaStream_t s);
 void launch_build_moments(TreeWork& w, int n, const double* xd, const double* yd,
                           const double* zd, cudaStream_t s);
 
+// FP64 moment prefix sums only (k_moment_tiles + tile scan) over w.body4 and
+// the optional key-order FP64 positions; moment_tile_prefix is where the
+// tile prefixes land (the tpre argument of range_moments).
+void launch_moment_prefix(TreeWork& w, int n, const double* xd, const double* yd,
+                          const double* zd, cudaStream_t s);
+double4* moment_tile_prefix(TreeWork& w, int n);
+
 size_t radix_sort_count_words(int n);
 // Stable LSD sort of (key, value) by the low `bits` bits of the keys; K is
 // uint32_t (single disk, 30-bit Morton keys) or uint64_t (ensemble: disk
@@ -149,6 +156,15 @@ struct WalkArgs {
   const int* group_disk;  // nullptr: one disk
   int n_disks;
   const int* pert_step;   // nullptr: pert points at the current entries
+  // recording walks (tape != nullptr; targets_per_lane must be 1): every
+  // group's source list as (first body, count) entries in evaluation order,
+  // in chains of 32-entry chunks: tape[c*32 ..], tape_next[c] the next chunk
+  // (-1 ends), group_tape[g] = (first chunk, entries) or (-1, 0)
+  int2* tape;
+  int* tape_next;
+  int* tape_used;         // chunks taken (reset to 0 before the walk)
+  int tape_cap;           // chunks in the pool
+  int2* group_tape;
 };
 int walk_spill_slots(int device);  // warps resident at once (spill area slots)
 void launch_walk(const WalkArgs& a, cudaStream_t s);

@@ -13,6 +13,7 @@
 // `cell_size` of the reference's opening test (BHTree.cu:577).
 #include "common.cuh"
 #include "kernels.cuh"
+#include "moments.cuh"
 
 namespace nb {
 namespace {
@@ -228,12 +229,6 @@ k_karras(const K* __restrict__ keys, int n, int key_bits, int* __restrict__ left
 constexpr int kTileM = kMomentTile;  // 256 threads x 8 bodies
 constexpr int kPerThr = kTileM / kThreads;
 
-__device__ __forceinline__ double4 d4add(double4 a, double4 b) {
-  return make_double4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
-}
-__device__ __forceinline__ double4 d4sub(double4 a, double4 b) {
-  return make_double4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w);
-}
 __device__ __forceinline__ double4 d4shfl_up(double4 v, int o) {
   return make_double4(__shfl_up_sync(kFull, v.x, o), __shfl_up_sync(kFull, v.y, o),
                       __shfl_up_sync(kFull, v.z, o), __shfl_up_sync(kFull, v.w, o));
@@ -302,14 +297,6 @@ __global__ void k_tile_scan(const double4* __restrict__ tile_sum, int ntiles,
   if (lane == 31) tpre[ntiles] = inc;
 }
 
-__device__ __forceinline__ double4 range_moments(const double4* __restrict__ ploc,
-                                                 const double4* __restrict__ tpre, int lo,
-                                                 int end) {
-  double4 r = d4sub(ploc[end], ploc[lo]);
-  const int t0 = lo / kTileM, t1 = end / kTileM;
-  if (t0 != t1) r = d4add(r, d4sub(tpre[t1], tpre[t0]));
-  return r;
-}
 
 // ---------------------------------------------------------- octree layout
 // Octree level of binary node b: leaves and equal-key runs are level 10;
@@ -454,13 +441,7 @@ __device__ void write_node(const EmitArgs<K>& a, int c, int f) {
     bhi[k] = fl + fs + margin;
     ctr[k] = fl + 0.5f * fs;
   }
-  float4 com;
-  if (s.x > 0.0) {
-    const double inv = 1.0 / s.x;
-    com = make_float4((float)(s.y * inv), (float)(s.z * inv), (float)(s.w * inv), (float)s.x);
-  } else {
-    com = make_float4(ctr[0], ctr[1], ctr[2], 0.f);
-  }
+  const float4 com = com_of(s, ctr[0], ctr[1], ctr[2]);
   const int k = a.nch[c];
   a.oct.com[f] = com;
   a.oct.info[f] = make_int4(k > 0 ? a.n_roots + (int)a.off[c] : -1, lo, ((hi - lo + 1) << 4) | k,
@@ -703,6 +684,17 @@ template void launch_karras<uint64_t>(TreeWork&, const uint64_t*, int, int, cuda
 template void launch_octree<uint64_t>(TreeWork&, const uint64_t*, int, int, int,
                                       const TreeGeom*, int*, const double*, const double*,
                                       const double*, cudaStream_t);
+
+void launch_moment_prefix(TreeWork& w, int n, const double* xd, const double* yd,
+                          const double* zd, cudaStream_t s) {
+  if (n < 1) return;
+  const int ntiles = n / kTileM + 1;
+  k_moment_tiles<<<ntiles, kThreads, 0, s>>>(w.body4, xd, yd, zd, n, w.mom_ploc, w.mom_tiles);
+  k_tile_scan<<<1, 32, 0, s>>>(w.mom_tiles, ntiles, moment_tile_prefix(w, n));
+  check(cudaGetLastError(), "moment prefix launch");
+}
+
+double4* moment_tile_prefix(TreeWork& w, int n) { return w.mom_tiles + (n / kTileM + 2); }
 
 void launch_build_topology(TreeWork& w, int n, cudaStream_t s) {
   launch_karras<uint32_t>(w, w.keys, n, 30, s);

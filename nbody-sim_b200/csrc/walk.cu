@@ -23,6 +23,7 @@
 // spill area that runs out raises kStatusStackOverflow instead of hanging.
 #include "common.cuh"
 #include "kernels.cuh"
+#include "walk_math.cuh"
 
 namespace nb {
 namespace {
@@ -36,20 +37,8 @@ struct WarpSmem {
   int stk[kStk];
   int sc[32];
   int slo[32];
+  int sc_body[32];  // recording walks: body index of each leaf-body entry
 };
-
-template <bool kSoft>
-__device__ __forceinline__ void interact(const float4 s, const float4 p, float eps2,
-                                         float3& acc) {
-  float dx = s.x - p.x, dy = s.y - p.y, dz = s.z - p.z;
-  float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-  float inv = rsqrtf(r2);
-  if (!kSoft) inv = (r2 > 0.f) ? inv : 0.f;
-  float f = s.w * (inv * inv * inv);
-  acc.x = fmaf(f, dx, acc.x);
-  acc.y = fmaf(f, dy, acc.y);
-  acc.z = fmaf(f, dz, acc.z);
-}
 
 // All lanes evaluate sources lst[0..cnt) for their kT targets; every source
 // is one shared-memory broadcast that feeds kT interaction chains.
@@ -82,8 +71,64 @@ __device__ __forceinline__ void list_shift(float4* lst, int nlist, int lane) {
   __syncwarp();
 }
 
-// kT targets per lane: a group of up to 32 kT bodies per warp.
-template <bool kSoft, int kT>
+// Tape of a group's source list (recording walks): the entries, in the
+// order the walk evaluates them, go to a chain of 32-entry chunks taken from
+// a pool.  An entry is the sorted body range (first, count) of the source: a
+// node's centre of mass is recomputed from that range on replay, a count of
+// 1 is the body itself.  A pool that runs dry raises kStatusTapeFull and the
+// rest of the group is not recorded (forces are still computed).
+struct TapeCursor {
+  int head = -1, cur = -1, taped = 0;
+  bool ok = true;
+};
+
+__device__ __forceinline__ int tape_alloc(const WalkArgs& a) {
+  const int c = atomicAdd(a.tape_used, 1);
+  if (c >= a.tape_cap) {
+    atomicOr(a.status, kStatusTapeFull);
+    return -1;
+  }
+  return c;
+}
+
+// Appends k <= 32 entries; lane l with `on` writes its entry at offset o.
+__device__ __forceinline__ void tape_append(const WalkArgs& a, TapeCursor& t, bool on, int o,
+                                            int k, int2 e, int lane) {
+  if (k <= 0 || !t.ok) return;
+  const int used = t.taped & 31;
+  int c1 = t.cur, c2 = -1;
+  if (lane == 0) {
+    if (used == 0) {
+      c1 = tape_alloc(a);
+      if (c1 >= 0) {
+        if (t.cur >= 0) a.tape_next[t.cur] = c1;
+        else t.head = c1;
+      }
+    }
+    if (c1 >= 0 && used + k > 32) {
+      c2 = tape_alloc(a);
+      if (c2 >= 0) a.tape_next[c1] = c2;
+    }
+  }
+  c1 = __shfl_sync(kFull, c1, 0);
+  c2 = __shfl_sync(kFull, c2, 0);
+  t.head = __shfl_sync(kFull, t.head, 0);
+  if (c1 < 0 || (used + k > 32 && c2 < 0)) {
+    t.ok = false;
+    return;
+  }
+  if (on) {
+    const int q = used + o;
+    const int c = (q < 32) ? c1 : c2;
+    a.tape[(size_t)c * 32 + (q & 31)] = e;
+  }
+  t.taped += k;
+  t.cur = (used + k > 32) ? c2 : c1;
+}
+
+// kT targets per lane: a group of up to 32 kT bodies per warp.  kRec: also
+// record the group's source list on the tape.
+template <bool kSoft, int kT, bool kRec>
 __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(const WalkArgs a) {
   __shared__ WarpSmem smem[kWalkWarps];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -124,6 +169,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(const WalkArgs a) {
     unsigned long long visited = 0, spills = 0, evaluated = 0;
     int top = 1, spilled = 0, nlist = 0;
     bool overflow = false;
+    TapeCursor tc;
     if (lane == 0) w.stk[0] = disk;  // root slot of the group's disk
     __syncwarp();
 
@@ -174,6 +220,11 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(const WalkArgs a) {
       // accepted sources -> list
       const unsigned m1 = __ballot_sync(kFull, act == 1);
       if (act == 1) w.lst[nlist + __popc(m1 & lanemask_lt())] = c;
+      if (kRec) {
+        const int4 inf = (node >= 0) ? __ldg(a.info + node) : make_int4(0, 0, 0, 0);
+        tape_append(a, tc, act == 1, __popc(m1 & lanemask_lt()), __popc(m1),
+                    make_int2(inf.y, inf.z >> 4), lane);
+      }
       nlist += __popc(m1);
       __syncwarp();
       if (nlist >= 32) {
@@ -219,6 +270,12 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(const WalkArgs a) {
               if (w.sc[o + step - 1] <= gi) o += step;
             const int prev = (o > 0) ? w.sc[o - 1] : 0;
             w.lst[nlist + lane] = __ldg(a.body + w.slo[o] + (gi - prev));
+            if (kRec) w.sc_body[lane] = w.slo[o] + (gi - prev);
+          }
+          if (kRec) {
+            __syncwarp();
+            tape_append(a, tc, gi < btotal, lane, min(32, btotal - base),
+                        make_int2(gi < btotal ? w.sc_body[lane] : 0, 1), lane);
           }
           nlist += min(32, btotal - base);
           __syncwarp();
@@ -263,6 +320,10 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(const WalkArgs a) {
         a.az[o] = az;
       }
     }
+    if (kRec && lane == 0) {
+      if (tc.cur >= 0) a.tape_next[tc.cur] = -1;
+      a.group_tape[g] = make_int2(tc.ok ? tc.head : -1, tc.ok ? tc.taped : 0);
+    }
     if (lane == 0) {
       if (overflow) atomicOr(a.status, kStatusStackOverflow);
       atomicAdd(a.inter, evaluated * (unsigned long long)gr.y);
@@ -275,11 +336,12 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(const WalkArgs a) {
   }
 }
 
-template <bool kSoft, int kT>
+template <bool kSoft, int kT, bool kRec = false>
 int walk_blocks_per_sm() {
   static int b = 0;
   if (b == 0) {
-    check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<kSoft, kT>, kWalkWarps * 32, 0),
+    check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<kSoft, kT, kRec>,
+                                                        kWalkWarps * 32, 0),
           "walk occupancy");
     if (b < 1) b = 1;
   }
@@ -296,19 +358,21 @@ int num_sms() {
   return sms;
 }
 
-template <bool kSoft, int kT>
+template <bool kSoft, int kT, bool kRec = false>
 void launch_variant(const WalkArgs& a, cudaStream_t s) {
-  int grid = num_sms() * walk_blocks_per_sm<kSoft, kT>();
+  int grid = num_sms() * walk_blocks_per_sm<kSoft, kT, kRec>();
   grid = std::min(grid, (a.n + kWalkWarps - 1) / kWalkWarps);  // groups <= n
   if (grid < 1) grid = 1;
-  k_walk<kSoft, kT><<<grid, kWalkWarps * 32, 0, s>>>(a);
+  k_walk<kSoft, kT, kRec><<<grid, kWalkWarps * 32, 0, s>>>(a);
 }
 
 }  // namespace
 
 int walk_spill_slots(int) {
-  const int b = std::max(std::max(walk_blocks_per_sm<true, 1>(), walk_blocks_per_sm<false, 1>()),
-                         std::max(walk_blocks_per_sm<true, 2>(), walk_blocks_per_sm<false, 2>()));
+  const int b = std::max(
+      std::max(std::max(walk_blocks_per_sm<true, 1>(), walk_blocks_per_sm<false, 1>()),
+               std::max(walk_blocks_per_sm<true, 2>(), walk_blocks_per_sm<false, 2>())),
+      std::max(walk_blocks_per_sm<true, 1, true>(), walk_blocks_per_sm<false, 1, true>()));
   return num_sms() * b * kWalkWarps;
 }
 
@@ -316,7 +380,10 @@ void launch_walk(const WalkArgs& a, cudaStream_t s) {
   if (a.n <= 0) return;
   check(cudaMemsetAsync(a.work, 0, sizeof(int), s), "walk work reset");
   const bool soft = a.eps > 0.f;
-  if (a.targets_per_lane == 2) {
+  if (a.tape) {  // recording: groups of <= 32 targets
+    if (soft) launch_variant<true, 1, true>(a, s);
+    else launch_variant<false, 1, true>(a, s);
+  } else if (a.targets_per_lane == 2) {
     if (soft) launch_variant<true, 2>(a, s);
     else launch_variant<false, 2>(a, s);
   } else {
