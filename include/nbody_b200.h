@@ -357,6 +357,31 @@ int nbody_sim_step_host(nbody_sim* s, float* x, float* y, float* z, float* vx, f
                         float* vz, float* ax, float* ay, float* az, const float* mass,
                         int nsteps);
 
+/* Output step of src/main.cu:143-181 on the GPU, overlapped with the steps
+ * that follow.  nbody_sim_output_begin enqueues, behind the steps issued so
+ * far: a snapshot of the state (caller order), FoF of the snapshot with the
+ * Aggregate.cpp:36-42 pair test, agg_size (main.cu:153-161), the aggregate
+ * records of detectAggregates (Aggregate.cpp:54-74, bit for bit, ordered by
+ * smallest member), and their copy into pinned host memory.  It returns at
+ * once; the engine may keep stepping.  nbody_sim_output_wait blocks for the
+ * oldest frame in flight and points *out at the engine's pinned buffers.
+ * Two frames can be in flight; a frame's buffers stay valid until the second
+ * output_begin after its wait (the slot it used comes round again). */
+typedef struct nbody_frame {
+  int n;
+  int frame_index;
+  float sim_time;
+  const float* x;                     /* host, caller order */
+  const float* y;
+  const float* z;
+  const uint16_t* agg_size;           /* main.cu:153-161 */
+  const nbody_aggregate* aggregates;  /* ordered by smallest member */
+  int n_aggregates;
+} nbody_frame;
+int nbody_sim_output_begin(nbody_sim* s, float link_length, float particle_mass,
+                           float sim_time, int frame_index);
+int nbody_sim_output_wait(nbody_sim* s, nbody_frame* out);
+
 /* ----------------------------------------------------------- ensemble --- */
 
 /* Many independent disks advanced together.  The reference runs one disk per

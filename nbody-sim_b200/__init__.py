@@ -140,6 +140,12 @@ class nbody_sim_stats(C.Structure):
                 ("walk_groups", C.c_ulonglong)]
 
 
+class nbody_frame(C.Structure):
+    _fields_ = [("n", C.c_int), ("frame_index", C.c_int), ("sim_time", C.c_float),
+                ("x", _F), ("y", _F), ("z", _F), ("agg_size", _U16),
+                ("aggregates", C.POINTER(nbody_aggregate)), ("n_aggregates", C.c_int)]
+
+
 class nbody_disk_spec(C.Structure):
     _fields_ = [("n", C.c_int), ("perturber_enabled", C.c_int),
                 ("perturber_mass_mjup", C.c_float), ("perturber_radius_au", C.c_float),
@@ -218,6 +224,8 @@ SIGNATURES = [
     ("nbody_sim_set_profiling", C.c_int, [_VP, C.c_int]),
     ("nbody_sim_profile_get", C.c_int, [_VP, C.POINTER(nbody_sim_profile), C.c_int]),
     ("nbody_sim_step_host", C.c_int, [_VP] + [_VP] * 10 + [C.c_int]),
+    ("nbody_sim_output_begin", C.c_int, [_VP, C.c_float, C.c_float, C.c_float, C.c_int]),
+    ("nbody_sim_output_wait", C.c_int, [_VP, C.POINTER(nbody_frame)]),
     ("nbody_ensemble_create", C.c_int, [C.POINTER(nbody_sim_params), C.POINTER(nbody_disk_spec),
                                         C.c_int, C.POINTER(_VP)]),
     ("nbody_ensemble_destroy", C.c_int, [_VP]),
@@ -674,6 +682,29 @@ class Sim:
         d["steps"] = pr.steps
         d["launches"] = pr.launches
         return d
+
+    def output_begin(self, link_length: float, particle_mass: float, sim_time: float,
+                     frame_index: int):
+        """Enqueue one output step (snapshot, FoF, agg_size, aggregates) on the GPU."""
+        _check(lib.nbody_sim_output_begin(self.h, link_length, particle_mass, sim_time,
+                                          frame_index))
+
+    def output_wait(self, copy: bool = True) -> dict:
+        """Oldest frame in flight: x, y, z, agg_size (numpy) and the aggregate records."""
+        f = nbody_frame()
+        _check(lib.nbody_sim_output_wait(self.h, C.byref(f)))
+        n = f.n
+        grab = (lambda a: np.array(a)) if copy else (lambda a: a)
+        out = {"frame_index": f.frame_index, "sim_time": f.sim_time,
+               "x": grab(np.ctypeslib.as_array(f.x, (n,))),
+               "y": grab(np.ctypeslib.as_array(f.y, (n,))),
+               "z": grab(np.ctypeslib.as_array(f.z, (n,))),
+               "agg_size": grab(np.ctypeslib.as_array(f.agg_size, (n,))),
+               "n_aggregates": f.n_aggregates}
+        out["aggregates"] = [nbody_aggregate.from_buffer_copy(f.aggregates[i])
+                             for i in range(f.n_aggregates)]
+        out["_frame"] = f
+        return out
 
     def step_host(self, st: dict, mass, nsteps: int = 1):
         """Host round trip (copyToGPU, nsteps, copyToCPU) on float32 arrays in place."""

@@ -22,6 +22,7 @@
 #include "capi_util.h"
 #include "common.cuh"
 #include "kernels.cuh"
+#include "output.h"
 #include "physics.cuh"
 
 namespace nb {
@@ -406,6 +407,9 @@ struct SimBase {
   virtual void get_state(void* const* v, bool as_double, float* const* a, bool on_device) = 0;
   virtual void step(int nsteps) = 0;
   virtual const uint32_t* ids() = 0;
+  // Positions and velocities in caller order as float, on the engine stream.
+  virtual void snapshot(float* const* dst) = 0;
+  OutputPipe* pipe = nullptr;
   virtual void load_accel(const float* ax, const float* ay, const float* az) = 0;
 
   void common_alloc() {
@@ -426,6 +430,10 @@ struct SimBase {
   }
 
   void common_free() {
+    if (pipe) {
+      delete pipe;
+      pipe = nullptr;
+    }
     for (auto& evs : ev_pending)
       for (cudaEvent_t e : evs) ev_pool.push_back(e);
     for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
@@ -521,6 +529,14 @@ struct SimImpl : SimBase {
   }
 
   const uint32_t* ids() override { return (const uint32_t*)s[cur].id; }
+
+  void snapshot(float* const* d) override {
+    k_unsort<R, float><<<stream_grid(n), kThreads, 0, st>>>(
+        s[cur], n, d[0], d[1], d[2], d[3], d[4], d[5], ax, ay, az, nullptr, nullptr, nullptr,
+        p.softening, p.star_mass);
+    check(cudaGetLastError(), "snapshot launch");
+    launches += 1;
+  }
 
   void set_state(const void* const* v, bool is_double, const float* mass, bool on_device,
                  bool forces) override {
@@ -857,6 +873,28 @@ int nbody_sim_stats_get(nbody_sim* s, nbody_sim_stats* out) {
     out->walk_nodes_visited = c[0];
     out->walk_stack_spills = c[1];
     out->walk_groups = c[2];
+  })
+}
+
+int nbody_sim_output_begin(nbody_sim* s, float link_length, float particle_mass,
+                           float sim_time, int frame_index) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(s, "nbody_sim_output_begin: null sim");
+    nb::SimBase* b = s->impl;
+    NBODY_REQUIRE(b->has_state, "nbody_sim_output_begin: state not set");
+    NBODY_REQUIRE(link_length >= 0.f, "nbody_sim_output_begin: negative link length");
+    if (!b->pipe) b->pipe = new nb::OutputPipe(b->n, b->p.leaf_max);
+    const int k = b->pipe->begin_slot();
+    b->snapshot(b->pipe->slot[k].snap);
+    b->pipe->launch(k, b->st, link_length, particle_mass, sim_time, frame_index);
+  })
+}
+
+int nbody_sim_output_wait(nbody_sim* s, nbody_frame* out) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(s && out, "nbody_sim_output_wait: null argument");
+    NBODY_REQUIRE(s->impl->pipe, "nbody_sim_output_wait: no frame in flight");
+    s->impl->pipe->wait(out);
   })
 }
 
