@@ -530,6 +530,17 @@ int nbody_make_disk(int n, double r_min, double r_max, double sigma_e, double si
                     double star_mass, uint64_t seed, double* x, double* y, double* z,
                     double* vx, double* vy, double* vz);
 
+/* The same disks generated on the GPU, many at once (an ensemble's initial
+ * conditions): disk d has counts[d] bodies and seed seeds[d] (host arrays);
+ * outputs are device arrays with the disks concatenated in order.  Body for
+ * body the arithmetic of nbody_make_disk; the two differ only in the last-ulp
+ * rounding of the device and host math libraries.  Synchronous on stream
+ * (NULL: the legacy stream). */
+int nbody_make_disks_device(const int* counts, const uint64_t* seeds, int n_disks,
+                            double r_min, double r_max, double sigma_e, double sigma_i,
+                            double star_mass, double* x, double* y, double* z, double* vx,
+                            double* vy, double* vz, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

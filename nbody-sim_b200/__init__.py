@@ -249,6 +249,7 @@ SIGNATURES = [
      + [_VP] * 6),
     ("nbody_adjoint_backward", C.c_int, [_VP] + [_VP] * 13),
     ("nbody_adjoint_stats_get", C.c_int, [_VP, C.POINTER(nbody_adjoint_stats)]),
+    ("nbody_make_disks_device", C.c_int, [_VP, _VP, C.c_int] + [C.c_double] * 5 + [_VP] * 7),
     ("nbody_direct_f64", C.c_int, [_VP] * 4 + [C.c_int, _VP, C.c_int, C.c_double] + [_VP] * 4),
     ("nbody_make_disk", C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                   C.c_double, C.c_uint64, _D, _D, _D, _D, _D, _D]),
@@ -970,3 +971,20 @@ def make_disk(n: int, r_min: float, r_max: float, sigma_e=0.01, sigma_i=0.005, s
                                *[out[k].ctypes.data_as(_D) for k in ("x", "y", "z", "vx", "vy",
                                                                        "vz")]))
     return out
+
+
+def make_disks_device(counts, seeds, r_min: float, r_max: float, sigma_e=0.01, sigma_i=0.005,
+                      star_mass=1.0, stream_ptr: int = 0):
+    """Disks generated on the GPU (nbody_make_disks_device): (x, v) as (3, N)
+    float64 CUDA tensors, the disks concatenated in order."""
+    import torch
+    cnt = np.ascontiguousarray(counts, np.int32)
+    sd = np.ascontiguousarray(seeds, np.uint64)
+    total = int(cnt.sum())
+    x = torch.empty((3, total), dtype=torch.float64, device="cuda")
+    v = torch.empty((3, total), dtype=torch.float64, device="cuda")
+    _check(lib.nbody_make_disks_device(cnt.ctypes.data, sd.ctypes.data, len(cnt), r_min, r_max,
+                                       sigma_e, sigma_i, star_mass,
+                                       *[x[k].data_ptr() for k in range(3)],
+                                       *[v[k].data_ptr() for k in range(3)], stream_ptr))
+    return x, v

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "../../include/nbody_b200.h"
+#include "diskgen.h"
 
 namespace nb {
 void set_error(const std::string& msg);
@@ -244,18 +245,6 @@ constexpr float kMsunToMearth = 332946.0f;
 template <typename T>
 void write_raw(std::ofstream& f, const T& v) {
   f.write(reinterpret_cast<const char*>(&v), sizeof(T));
-}
-
-// splitmix64 (Vigna), the disk generator's counter-based source of bits.
-inline uint64_t splitmix64(uint64_t x) {
-  x += 0x9E3779B97F4A7C15ull;
-  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
-  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
-  return x ^ (x >> 31);
-}
-inline double unit(uint64_t seed, uint64_t i, uint64_t k) {
-  uint64_t h = splitmix64(splitmix64(seed) ^ (i * 16u + k));
-  return (double)(h >> 11) * (1.0 / 9007199254740992.0);  // [0, 1)
 }
 
 }  // namespace
@@ -553,46 +542,11 @@ int nbody_make_disk(int n, double r_min, double r_max, double sigma_e, double si
     nb::set_error("nbody_make_disk: bad argument");
     return NBODY_ERR_ARG;
   }
-  const double two_pi = 6.283185307179586476925287;
-  const double sa = std::sqrt(r_min), sb = std::sqrt(r_max);
   for (int i = 0; i < n; ++i) {
-    // semi-major axis from Sigma ~ r^-1.5 (inverse CDF, DiskInit.cpp:42-44)
-    double u = unit(seed, (uint64_t)i, 0);
-    double sr = u * (sb - sa) + sa;
-    double a = sr * sr;
-    // Rayleigh e and i
-    double e = sigma_e * std::sqrt(-2.0 * std::log1p(-unit(seed, (uint64_t)i, 1)));
-    double inc = sigma_i * std::sqrt(-2.0 * std::log1p(-unit(seed, (uint64_t)i, 2)));
-    if (e > 0.9) e = 0.9;
-    double Om = two_pi * unit(seed, (uint64_t)i, 3);
-    double om = two_pi * unit(seed, (uint64_t)i, 4);
-    double M = two_pi * unit(seed, (uint64_t)i, 5);
-    // Kepler's equation E - e sin E = M (Newton)
-    double E = (e < 0.8) ? M : 3.141592653589793;
-    for (int it = 0; it < 60; ++it) {
-      double f = E - e * std::sin(E) - M;
-      double d = f / (1.0 - e * std::cos(E));
-      E -= d;
-      if (std::fabs(d) < 1e-15) break;
-    }
-    const double cE = std::cos(E), sE = std::sin(E);
-    const double q = std::sqrt(1.0 - e * e);
-    const double nmot = std::sqrt(mu / (a * a * a));
-    const double den = 1.0 - e * cE;
-    const double xp = a * (cE - e), yp = a * q * sE;
-    const double vxp = -a * nmot * sE / den, vyp = a * nmot * q * cE / den;
-    // perifocal -> reference frame with the pole +Z
-    const double cO = std::cos(Om), sO = std::sin(Om), co = std::cos(om), so = std::sin(om);
-    const double ci = std::cos(inc), si = std::sin(inc);
-    const double r11 = cO * co - sO * so * ci, r12 = -cO * so - sO * co * ci;
-    const double r21 = sO * co + cO * so * ci, r22 = -sO * so + cO * co * ci;
-    const double r31 = so * si, r32 = co * si;
-    const double X = r11 * xp + r12 * yp, Y = r21 * xp + r22 * yp, Z = r31 * xp + r32 * yp;
-    const double VX = r11 * vxp + r12 * vyp, VY = r21 * vxp + r22 * vyp, VZ = r31 * vxp + r32 * vyp;
-    // disk plane XZ with Y vertical, same sense of rotation as initDisk
-    // (x = r cos phi, z = r sin phi, DiskInit.cpp:47-49): (X, Y, Z) -> (X, -Z, Y)
-    x[i] = X; y[i] = -Z; z[i] = Y;
-    vx[i] = VX; vy[i] = -VZ; vz[i] = VY;
+    double st[6];
+    nb::disk_body(seed, (uint64_t)i, r_min, r_max, sigma_e, sigma_i, mu, st);
+    x[i] = st[0]; y[i] = st[1]; z[i] = st[2];
+    vx[i] = st[3]; vy[i] = st[4]; vz[i] = st[5];
   }
   return NBODY_OK;
 }

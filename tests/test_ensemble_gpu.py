@@ -157,3 +157,21 @@ def test_ensemble_rejects_bad_input(nb, cuda):
         ens.step(1)
     assert e.value.code == nb.NBODY_ERR_ARG
     ens.close()
+
+
+def test_device_disk_generator_matches_host(nb, cuda):
+    """nbody_make_disks_device against nbody_make_disk disk by disk: the same
+    arithmetic, differing only in the math libraries' last-ulp rounding."""
+    counts = [2048, 5003, 1, 0, 9000]
+    seeds = [0, 1, 2, 3, 2 ** 40 + 5]
+    x, v = nb.make_disks_device(counts, seeds, 0.5, 5.0)
+    x, v = x.cpu().numpy(), v.cpu().numpy()
+    off = 0
+    for n, s in zip(counts, seeds):
+        d = nb.make_disk(n, 0.5, 5.0, 0.01, 0.005, 1.0, s)
+        for k, key in enumerate(("x", "y", "z")):
+            assert np.allclose(x[k, off:off + n], d[key], rtol=1e-12, atol=1e-13), (s, key)
+        for k, key in enumerate(("vx", "vy", "vz")):
+            assert np.allclose(v[k, off:off + n], d[key], rtol=1e-12, atol=1e-13), (s, key)
+        off += n
+    assert off == x.shape[1]
