@@ -56,7 +56,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-flush", action="store_true")
-    ap.add_argument("--workload", choices=["disk1m", "ensemble", "precision", "adjoint"],
+    ap.add_argument("--workload", choices=["disk1m", "ensemble", "precision", "adjoint", "c2run"],
                     default="disk1m",
                     help="disk1m: the headline single disk; ensemble: 64 disks (C4) against "
                          "the same disks run one by one; precision: force error vs FP64 "
@@ -643,6 +643,104 @@ def run_adjoint(args, ws, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def run_c2(args, ws, rank, local):
+    """The full-physics run end to end through the reference's loop
+    (src/main.cu:85-190): N = 131072, r in [0.5, 5] AU, m = 1e-8, eps 1e-3,
+    collisions (factor 5, e = 0), drag 1e-3, perturber 1 M_J at 5.2 AU,
+    dt 0.005, 2000 steps, frame + aggregates every 50 steps (40 outputs)
+    written to frames.bin / stats.csv, FP64 state.  Wall-clock particle-steps/s
+    with the GPU output pipeline and with the reference's stop-copy-detect-write
+    order (GPU FoF), and without outputs; the reference's own detectAggregates
+    (one host thread, the O(N^2) loop) timed on one snapshot as the CPU
+    baseline of the output step."""
+    import shutil
+    import tempfile
+    import torch
+    if rank != 0:
+        return
+    nb = importlib.import_module("nbody-sim_b200")
+    run = importlib.import_module("nbody-sim_b200.run")
+    torch.cuda.set_device(local)
+    cfg = nb.default_config()
+    cfg.n_particles = 131072
+    cfg.disk_r_min, cfg.disk_r_max = 0.5, 5.0
+    cfg.particle_mass_msun = 1e-8
+    cfg.softening_AU = 1e-3
+    cfg.theta = 0.5
+    cfg.collision_radius_factor = 5.0
+    cfg.restitution = 0.0
+    cfg.gas_drag_rate = 1e-3
+    cfg.dt = 0.005
+    cfg.total_time = 10.0
+    cfg.output_every_n_steps = 50
+    cfg.perturber_enabled = 1
+    cfg.perturber_mass_mjup = 1.0
+    cfg.perturber_radius_AU = 5.2
+    cfg.perturber_phase0 = 0.0
+    n = cfg.n_particles
+    total = int(np.float32(cfg.total_time) / np.float32(cfg.dt))
+    res = {}
+    tmp = tempfile.mkdtemp(prefix="nbody_c2_")
+    try:
+        # warm-up (library init, allocations)
+        run.run_simulation(cfg, os.path.join(tmp, "warm"), precision=nb.STATE_F64,
+                           total_steps=100)
+        for name, pipelined in (("pipelined", True), ("synchronous", False)):
+            d = os.path.join(tmp, name)
+            r = run.run_simulation(cfg, d, precision=nb.STATE_F64, pipelined=pipelined)
+            r["frames_bytes"] = os.path.getsize(os.path.join(d, "frames.bin"))
+            res[name] = r
+        same = all(open(os.path.join(tmp, "pipelined", f), "rb").read() ==
+                   open(os.path.join(tmp, "synchronous", f), "rb").read()
+                   for f in ("frames.bin", "stats.csv"))
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    # stepping alone
+    prm = nb.sim_params(cfg)
+    prm.state_precision = nb.STATE_F64
+    dsk = nb.make_disk(n, 0.5, 5.0, 0.01, 0.005, 1.0, 0)
+    sim = nb.Sim(prm, n)
+    m = np.full(n, cfg.particle_mass_msun, np.float32)
+    sim.set_state(dsk["x"], dsk["y"], dsk["z"], dsk["vx"], dsk["vy"], dsk["vz"], m)
+    sim.step(10)
+    sim.sync()
+    t0 = time.perf_counter()
+    sim.step(total)
+    sim.sync()
+    step_secs = time.perf_counter() - t0
+    sim.close()
+    line = {
+        "study": "c2run", "data": "synthetic",
+        "config": {"workload": "Keplerian disk N=131072 r=[0.5,5] AU m=1e-8 eps=1e-3, "
+                               "collisions (factor 5), drag 1e-3, perturber 1 MJ at 5.2 AU, "
+                               "dt 0.005, 2000 steps, output every 50, FP64 state"},
+        "steps": total, "outputs": res["pipelined"]["frames"],
+        "particle_steps_per_s": {k: v["particle_steps_per_s"] for k, v in res.items()},
+        "seconds": {k: v["seconds"] for k, v in res.items()},
+        "host_seconds": {k: v["host_seconds"] for k, v in res.items()},
+        "stepping_only_seconds": step_secs,
+        "output_overhead_seconds": {k: v["seconds"] - step_secs for k, v in res.items()},
+        "frames_bytes": res["pipelined"]["frames_bytes"],
+        "pipelined_equals_synchronous_bytes": same,
+    }
+    if not args.no_cpu_baseline:
+        ref = os.path.join(ROOT, "oracle", "_ref", "libref_host.so")
+        if os.path.exists(ref):
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import oracle
+            rh = oracle.RefHost(ref)
+            xs = [dsk[k].astype(np.float32) for k in ("x", "y", "z")]
+            t0 = time.perf_counter()
+            rh.detect_aggregates_count(*xs, float(prm.r_coll))
+            secs = time.perf_counter() - t0
+            line["cpu_baseline"] = {
+                "value": secs, "unit": "s per output (detectAggregates)", "cores": 1,
+                "kind": "reference",
+                "sample": "the reference's Aggregate.cpp detectAggregates on one N=131072 "
+                          "snapshot (its O(N^2) pair loop), x40 outputs in a C2 run"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     ws, rank, local = dist_setup()
@@ -655,6 +753,8 @@ def main():
             run_precision(args, ws, rank, local)
         elif args.workload == "adjoint":
             run_adjoint(args, ws, rank, local)
+        elif args.workload == "c2run":
+            run_c2(args, ws, rank, local)
         else:
             run_ours(args, ws, rank, local)
     finally:

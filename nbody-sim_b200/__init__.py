@@ -557,7 +557,13 @@ class OutputWriter:
         _check(lib.nbody_writer_frame(self.h, *[a.ctypes.data_as(_F) for a in xs], p.n, sim_time,
                                       agg.ctypes.data_as(_U16)))
 
-    def write_stats(self, aggs, frame_idx: int, sim_time: float):
+    def write_stats(self, aggs, frame_idx: int, sim_time: float, count: int | None = None):
+        """aggs: Aggregate-like objects, or (with count) a ctypes array / pointer
+        of nbody_aggregate records passed to the writer as they are."""
+        if count is not None:
+            _check(lib.nbody_writer_stats(self.h, C.cast(aggs, C.POINTER(nbody_aggregate)),
+                                          count, frame_idx, sim_time))
+            return
         arr = (nbody_aggregate * max(len(aggs), 1))()
         for k, a in enumerate(aggs):
             r = arr[k]
@@ -691,7 +697,10 @@ class Sim:
                                           frame_index))
 
     def output_wait(self, copy: bool = True) -> dict:
-        """Oldest frame in flight: x, y, z, agg_size (numpy) and the aggregate records."""
+        """Oldest frame in flight: x, y, z, agg_size (numpy) and the aggregate
+        records.  copy=False returns views of the engine's pinned buffers
+        (valid until the slot is reused) and the records as a raw pointer
+        ("aggregates_ptr"), without per-record Python objects."""
         f = nbody_frame()
         _check(lib.nbody_sim_output_wait(self.h, C.byref(f)))
         n = f.n
@@ -701,10 +710,10 @@ class Sim:
                "y": grab(np.ctypeslib.as_array(f.y, (n,))),
                "z": grab(np.ctypeslib.as_array(f.z, (n,))),
                "agg_size": grab(np.ctypeslib.as_array(f.agg_size, (n,))),
-               "n_aggregates": f.n_aggregates}
-        out["aggregates"] = [nbody_aggregate.from_buffer_copy(f.aggregates[i])
-                             for i in range(f.n_aggregates)]
-        out["_frame"] = f
+               "n_aggregates": f.n_aggregates, "aggregates_ptr": f.aggregates}
+        if copy:
+            out["aggregates"] = [nbody_aggregate.from_buffer_copy(f.aggregates[i])
+                                 for i in range(f.n_aggregates)]
         return out
 
     def step_host(self, st: dict, mass, nsteps: int = 1):

@@ -17,6 +17,7 @@ Two output schedules:
 from __future__ import annotations
 
 import importlib
+import os
 import time
 
 import numpy as np
@@ -62,48 +63,60 @@ def run_simulation(cfg, out_dir: str, state=None, precision=None, pipelined: boo
     ty = np.float64 if dbl else np.float32
     sim.set_state(*[np.asarray(state[k], ty) for k in ("x", "y", "z", "vx", "vy", "vz")],
                   state["m"])
+    os.makedirs(out_dir, exist_ok=True)  # main.cu creates the run directory (:30-41)
     writer = nb.OutputWriter(out_dir, cfg)
     frames = 0
     n_out = total // every
 
-    def write(fr_x, fr_y, fr_z, agg, aggs, t, idx):
+    host = {"wait": 0.0, "write": 0.0, "enqueue": 0.0}
+
+    def write(fr_x, fr_y, fr_z, agg, aggs, n_aggs, t, idx):
+        t_w = time.perf_counter()
         writer.write_frame(_Host(n, fr_x, fr_y, fr_z), t, agg)
-        writer.write_stats(aggs, idx, t)
+        writer.write_stats(aggs, idx, t, count=n_aggs)
         if pert.enabled:
             q = nb.nbody_perturber.from_buffer_copy(pert)
             nb.update_perturber(q, t)
-            writer.write_perturber_stats(idx, t, len(aggs), q.x, q.y, q.z, q.mass_msun,
-                                         q.omega)
+            writer.write_perturber_stats(idx, t, n_aggs, q.x, q.y, q.z, q.mass_msun, q.omega)
+        host["write"] += time.perf_counter() - t_w
 
     t0 = time.perf_counter()
     if pipelined:
         pending = 0
         for k in range(n_out):
+            t_e = time.perf_counter()
             sim.step(every)
             t = np.float32((k + 1) * every) * dt
             sim.output_begin(r_coll, pm, float(t), k)
+            host["enqueue"] += time.perf_counter() - t_e
             pending += 1
             if pending == 2:  # the older frame is ready or nearly so: write it
+                t_q = time.perf_counter()
                 fr = sim.output_wait(copy=False)
-                write(fr["x"], fr["y"], fr["z"], fr["agg_size"], fr["aggregates"],
-                      fr["sim_time"], fr["frame_index"])
+                host["wait"] += time.perf_counter() - t_q
+                write(fr["x"], fr["y"], fr["z"], fr["agg_size"], fr["aggregates_ptr"],
+                      fr["n_aggregates"], fr["sim_time"], fr["frame_index"])
                 frames += 1
                 pending -= 1
         while pending:
             fr = sim.output_wait(copy=False)
-            write(fr["x"], fr["y"], fr["z"], fr["agg_size"], fr["aggregates"], fr["sim_time"],
-                  fr["frame_index"])
+            write(fr["x"], fr["y"], fr["z"], fr["agg_size"], fr["aggregates_ptr"],
+                  fr["n_aggregates"], fr["sim_time"], fr["frame_index"])
             frames += 1
             pending -= 1
     else:
         for k in range(n_out):
+            t_e = time.perf_counter()
             sim.step(every)
+            host["enqueue"] += time.perf_counter() - t_e
             t = float(np.float32((k + 1) * every) * dt)
+            t_q = time.perf_counter()
             s = sim.get_state(accel=False)
             labels, agg, _ = sim.fof(r_coll)
+            host["wait"] += time.perf_counter() - t_q
             aggs, cnt = nb.aggregates_from_labels(s["x"], s["y"], s["z"], s["vx"], s["vy"],
                                                   s["vz"], labels, pm)
-            write(s["x"], s["y"], s["z"], agg, list(aggs)[:cnt], t, k)
+            write(s["x"], s["y"], s["z"], agg, aggs, cnt, t, k)
             frames += 1
     rest = total - n_out * every
     if rest:
@@ -114,4 +127,4 @@ def run_simulation(cfg, out_dir: str, state=None, precision=None, pipelined: boo
     writer.close()
     sim.close()
     return {"steps": total, "frames": frames, "seconds": secs,
-            "particle_steps_per_s": n * total / secs}
+            "particle_steps_per_s": n * total / secs, "host_seconds": host}
