@@ -324,8 +324,14 @@ typedef struct nbody_sim_stats {
   unsigned long long walk_nodes_visited;  /* node tests of the last walk */
   unsigned long long walk_stack_spills;   /* stack spills of the last walk */
   unsigned long long walk_groups;         /* warp groups of the last walk */
+  unsigned long long launches;            /* kernels launched so far (graph nodes included) */
+  unsigned long long graph_launches;      /* steps replayed as one CUDA graph */
 } nbody_sim_stats;
 int nbody_sim_stats_get(nbody_sim* s, nbody_sim_stats* out);
+/* 1 (default): each step is replayed as one CUDA graph (captured on first
+ * use, four variants); 0: its kernels are launched one by one.  Steps run
+ * while profiling is on are always launched one by one. */
+int nbody_sim_set_graphs(nbody_sim* s, int on);
 
 /* Per-phase device time of the steps run while profiling is on: CUDA events
  * at the phase boundaries of every step, on the engine's stream.  Phase k of

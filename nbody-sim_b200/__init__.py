@@ -137,7 +137,8 @@ class nbody_sim_stats(C.Structure):
     _fields_ = [("n", C.c_int), ("steps_done", C.c_int), ("n_nodes", C.c_int),
                 ("interactions", C.c_ulonglong), ("status", C.c_int),
                 ("walk_nodes_visited", C.c_ulonglong), ("walk_stack_spills", C.c_ulonglong),
-                ("walk_groups", C.c_ulonglong)]
+                ("walk_groups", C.c_ulonglong), ("launches", C.c_ulonglong),
+                ("graph_launches", C.c_ulonglong)]
 
 
 class nbody_frame(C.Structure):
@@ -224,6 +225,7 @@ SIGNATURES = [
     ("nbody_sim_set_profiling", C.c_int, [_VP, C.c_int]),
     ("nbody_sim_profile_get", C.c_int, [_VP, C.POINTER(nbody_sim_profile), C.c_int]),
     ("nbody_sim_step_host", C.c_int, [_VP] + [_VP] * 10 + [C.c_int]),
+    ("nbody_sim_set_graphs", C.c_int, [_VP, C.c_int]),
     ("nbody_sim_output_begin", C.c_int, [_VP, C.c_float, C.c_float, C.c_float, C.c_int]),
     ("nbody_sim_output_wait", C.c_int, [_VP, C.POINTER(nbody_frame)]),
     ("nbody_ensemble_create", C.c_int, [C.POINTER(nbody_sim_params), C.POINTER(nbody_disk_spec),
@@ -681,6 +683,9 @@ class Sim:
 
     def set_profiling(self, on: bool = True):
         _check(lib.nbody_sim_set_profiling(self.h, int(on)))
+
+    def set_graphs(self, on: bool = True):
+        _check(lib.nbody_sim_set_graphs(self.h, int(on)))
 
     def profile(self, reset: bool = True) -> dict:
         pr = nbody_sim_profile()

@@ -276,37 +276,20 @@ T* dalloc(size_t count, const char* what) {
 
 // Writes the state back in the caller's order (by id) as float or double,
 // with the accelerations (plus the star term the FP64 walk leaves out), into
-// device buffers or, through stream-ordered temporaries, host buffers.
+// device buffers or, through the persistent device scratch `stage` (6 doubles
+// + 3 floats per body), host buffers.
 template <typename R>
 void state_out(const StateArrays<R>& a, int n, const float* ax, const float* ay,
                const float* az, float eps, float star_mass, void* const* v, bool as_double,
-               float* const* acc, bool on_device, cudaStream_t st) {
+               float* const* acc, bool on_device, void* stage, cudaStream_t st) {
   const size_t esz = as_double ? sizeof(double) : sizeof(float);
+  char* scratch = (char*)stage;
   std::vector<void*> dst(6);
-  std::vector<void*> tmp;
-  for (int k = 0; k < 6; ++k) {
-    if (on_device) {
-      dst[k] = v[k];
-    } else {
-      void* t = nullptr;
-      check(cudaMallocAsync(&t, esz * n, st), "get_state temp");
-      tmp.push_back(t);
-      dst[k] = t;
-    }
-  }
+  for (int k = 0; k < 6; ++k) dst[k] = on_device ? v[k] : (void*)(scratch + k * esz * n);
   float* da[3] = {nullptr, nullptr, nullptr};
-  if (acc && acc[0]) {
-    for (int k = 0; k < 3; ++k) {
-      if (on_device) {
-        da[k] = acc[k];
-      } else {
-        void* t = nullptr;
-        check(cudaMallocAsync(&t, sizeof(float) * n, st), "get_state temp");
-        tmp.push_back(t);
-        da[k] = (float*)t;
-      }
-    }
-  }
+  if (acc && acc[0])
+    for (int k = 0; k < 3; ++k)
+      da[k] = on_device ? acc[k] : (float*)(scratch + 6 * sizeof(double) * n) + (size_t)k * n;
   if (as_double)
     k_unsort<R, double><<<stream_grid(n), kThreads, 0, st>>>(
         a, n, (double*)dst[0], (double*)dst[1], (double*)dst[2], (double*)dst[3],
@@ -323,10 +306,12 @@ void state_out(const StateArrays<R>& a, int n, const float* ax, const float* ay,
       for (int k = 0; k < 3; ++k)
         check(cudaMemcpyAsync(acc[k], da[k], sizeof(float) * n, cudaMemcpyDeviceToHost, st),
               "accel D2H");
-    for (void* t : tmp) check(cudaFreeAsync(t, st), "get_state free");
   }
   check(cudaStreamSynchronize(st), "get_state sync");
 }
+
+// Bytes of the state_out scratch for n bodies.
+inline size_t out_stage_bytes(int n) { return (size_t)n * (6 * sizeof(double) + 3 * sizeof(float)); }
 
 struct SimBase {
   virtual ~SimBase() {}
@@ -340,6 +325,7 @@ struct SimBase {
   float *dvx = nullptr, *dvy = nullptr, *dvz = nullptr;
   float4* pert_tab = nullptr;
   int pert_cap = 0;
+  int* pert_step = nullptr;  // row of pert_tab the next walk reads (device)
   int* spill = nullptr;
   int spill_cap = 0;
   int* work = nullptr;
@@ -351,6 +337,7 @@ struct SimBase {
   uint16_t* agg = nullptr;
   int* ngroups = nullptr;
   void* staging = nullptr;  // n doubles
+  void* out_stage = nullptr;  // get_state to host: out_stage_bytes(n), on first use
   nbody_perturber pert{};
   // profiling: events at phase boundaries of every step, read lazily
   bool profiling = false;
@@ -427,9 +414,26 @@ struct SimBase {
     agg = dalloc<uint16_t>(n, "fof agg");
     ngroups = dalloc<int>(1, "fof ngroups");
     staging = dalloc<double>(n, "staging");
+    pert_step = dalloc<int>(1, "perturber row");
+    check(cudaMemset(pert_step, 0, sizeof(int)), "perturber row init");
+  }
+
+  // CUDA graphs of one step: [first step of a call?][state buffer at step
+  // start]; captured on a private stream, replayed on the engine's.
+  bool use_graphs = true;
+  cudaStream_t cap_st = nullptr;
+  cudaGraphExec_t gx[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  unsigned long long g_kernels[2][2] = {{0, 0}, {0, 0}};
+  unsigned long long graph_launches = 0;
+  void drop_graphs() {
+    for (auto& row : gx)
+      for (auto& g : row)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
   }
 
   void common_free() {
+    drop_graphs();
+    if (cap_st) cudaStreamDestroy(cap_st);
     if (pipe) {
       delete pipe;
       pipe = nullptr;
@@ -438,20 +442,24 @@ struct SimBase {
       for (cudaEvent_t e : evs) ev_pool.push_back(e);
     for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
     tree_free(tw);
-    void* ptrs[] = {ax, ay, az, dvx, dvy, dvz, pert_tab, spill, work, inter, counters,
-                    parent, labels, sizes, agg, ngroups, staging};
+    void* ptrs[] = {ax, ay, az, dvx, dvy, dvz, pert_tab, pert_step, spill, work, inter,
+                    counters, parent, labels, sizes, agg, ngroups, staging, out_stage};
     for (void* q : ptrs)
       if (q) cudaFree(q);
   }
 
   // Perturber positions for force times (k+1) dt, k in [k0, k0+count), by the
-  // host arithmetic of updatePerturber (Perturber.h:60-66).
+  // host arithmetic of updatePerturber (Perturber.h:60-66); the walk reads row
+  // *pert_step, which every step advances (so a captured step needs no host
+  // update).
   void upload_perturber(int k0, int count) {
     if (!p.perturber_enabled || count <= 0) return;
     if (count > pert_cap) {
+      check(cudaStreamSynchronize(st), "perturber table sync");
       if (pert_tab) cudaFree(pert_tab);
-      pert_cap = std::max(count, 64);
+      pert_cap = std::max(count, std::max(64, 2 * pert_cap));
       pert_tab = dalloc<float4>(pert_cap, "perturber table");
+      drop_graphs();  // the captured walks hold the old table
     }
     std::vector<float4> h(count);
     for (int k = 0; k < count; ++k) {
@@ -461,6 +469,7 @@ struct SimBase {
     }
     check(cudaMemcpyAsync(pert_tab, h.data(), sizeof(float4) * count, cudaMemcpyHostToDevice, st),
           "perturber upload");
+    check(cudaMemsetAsync(pert_step, 0, sizeof(int), st), "perturber row reset");
   }
 
   int check_status() {
@@ -516,6 +525,7 @@ struct SimImpl : SimBase {
       s[b].m = dalloc<float>(n, "mass");
       s[b].id = dalloc<int>(n, "id");
     }
+    if (!kIsF32<R>) vf = dalloc<float>(3 * (size_t)n, "velocity scratch");
   }
 
   ~SimImpl() override {
@@ -542,8 +552,15 @@ struct SimImpl : SimBase {
                  bool forces) override {
     cur = 0;
     const size_t esz = is_double ? sizeof(double) : sizeof(float);
+    const bool same = (is_double && kIsF64<R>) || (!is_double && kIsF32<R>);
     for (int k = 0; k < 6; ++k) {
       const void* src = v[k];
+      if (same) {  // the caller's type is the state's: one copy, no conversion pass
+        check(cudaMemcpyAsync(s[0].v[k], src, esz * n,
+                              on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st),
+              "state copy");
+        continue;
+      }
       if (!on_device) {
         check(cudaMemcpyAsync(staging, src, esz * n, cudaMemcpyHostToDevice, st), "state H2D");
         src = staging;
@@ -563,7 +580,7 @@ struct SimImpl : SimBase {
     has_state = true;
     if (forces) {
       launch_bbox<R>(tw, s[0].v[0], s[0].v[1], s[0].v[2], n, st);
-      compute_forces(-1);
+      compute_forces(true);
     } else {
       launch_bbox_reset(tw, st);  // the next k_stream accumulates the bbox
     }
@@ -576,9 +593,9 @@ struct SimImpl : SimBase {
     check(cudaMemcpyAsync(az, haz, sizeof(float) * n, cudaMemcpyHostToDevice, st), "az H2D");
   }
 
-  // Tree + walk for the current positions; pert_k indexes the perturber table
-  // (-1: time 0, positions from makePerturber).
-  void compute_forces(int pert_k) {
+  // Tree + walk for the current positions; initial: the forces of t = 0 (the
+  // perturber where makePerturber puts it), else of the step's row.
+  void compute_forces(bool initial) {
     StateArrays<R>& a = s[cur];
     StateArrays<R>& b = s[1 - cur];
     mark(NBODY_PHASE_SORT);
@@ -596,13 +613,7 @@ struct SimImpl : SimBase {
                            (const double*)s[cur].v[2], st);
     else
       launch_build_moments(tw, n, nullptr, nullptr, nullptr, st);
-    const float4* pp = nullptr;
-    if (p.perturber_enabled) {
-      if (pert_k < 0) {
-        upload_perturber(-1, 1);  // (float)(0) * dt = 0
-      }
-      pp = pert_tab + std::max(pert_k, 0);
-    }
+    if (p.perturber_enabled && initial) upload_perturber(-1, 1);  // (float)(0) * dt = 0
     check(cudaMemsetAsync(inter, 0, sizeof(unsigned long long), st), "inter reset");
     check(cudaMemsetAsync(counters, 0, 3 * sizeof(unsigned long long), st), "counters reset");
     WalkArgs w{};
@@ -610,7 +621,10 @@ struct SimImpl : SimBase {
     w.groups = tw.groups; w.n_groups = tw.n_groups;
     w.theta2 = p.theta * p.theta; w.eps = p.softening; w.star_mass = p.star_mass;
     w.star_in_walk = kIsF32<R> ? 1 : 0;
-    w.leaf_max = p.leaf_max; w.pert = pp;
+    w.leaf_max = p.leaf_max;
+    w.pert = p.perturber_enabled ? pert_tab : nullptr;
+    w.pert_step = p.perturber_enabled ? pert_step : nullptr;
+    w.n_disks = 1;
     w.ax = ax; w.ay = ay; w.az = az; w.scatter = nullptr;
     w.spill = spill; w.spill_cap = spill_cap; w.inter = inter; w.counters = counters;
     w.work = work; w.status = tw.status; w.targets_per_lane = tw.group_max / 32;
@@ -632,7 +646,6 @@ struct SimImpl : SimBase {
                      st);
     } else {
       // float copies of the half-step velocities for the FP32 impulse
-      if (!vf) vf = dalloc<float>(3 * (size_t)n, "velocity scratch");
       for (int k = 0; k < 3; ++k)
         k_convert<R, float><<<stream_grid(n), kThreads, 0, st>>>(s[cur].v[3 + k], vf + k * n, n);
       check(cudaGetLastError(), "velocity convert");
@@ -666,21 +679,61 @@ struct SimImpl : SimBase {
     check(cudaGetLastError(), "k_stream launch");
   }
 
+  // One step (main.cu:101-139): [dv + K2 + drag of the previous step] + K1 +
+  // drift, tree + walk (+ star, + perturber row), collisions; the perturber
+  // row advances.
+  void one_step(bool first) {
+    mark(NBODY_PHASE_STREAM);
+    stream_kernel(!first, true);
+    compute_forces(false);
+    if (p.r_coll > 0.f) {
+      collide();
+      launches += kIsF32<R> ? 1 : 4;
+    }
+    if (p.perturber_enabled) {
+      k_increment<<<1, 1, 0, st>>>(pert_step);
+      check(cudaGetLastError(), "k_increment launch");
+      launches += 1;
+    }
+    mark(NBODY_PHASES);
+    launches += 1;
+  }
+
+  cudaGraphExec_t graph_for(bool first) {
+    const int f = first ? 1 : 0, c = cur;
+    if (gx[f][c]) return gx[f][c];
+    if (!cap_st) check(cudaStreamCreateWithFlags(&cap_st, cudaStreamNonBlocking), "capture stream");
+    cudaGraph_t graph = nullptr;
+    const unsigned long long l0 = launches;
+    cudaStream_t user = st;
+    st = cap_st;
+    check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+    one_step(first);
+    const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+    st = user;
+    check(ce, "end capture");
+    cur = c;  // captured, not run
+    g_kernels[f][c] = launches - l0;
+    launches = l0;
+    check(cudaGraphInstantiate(&gx[f][c], graph, 0), "graph instantiate");
+    cudaGraphDestroy(graph);
+    return gx[f][c];
+  }
+
   void step(int nsteps) override {
     if (nsteps <= 0) return;
     upload_perturber(steps_done, nsteps);
-    const bool coll = p.r_coll > 0.f;
     for (int k = 0; k < nsteps; ++k) {
-      begin_step_profile();
-      mark(NBODY_PHASE_STREAM);
-      stream_kernel(k > 0, true);
-      compute_forces(k);
-      if (coll) {
-        collide();
-        launches += kIsF32<R> ? 1 : 4;
+      if (use_graphs && !profiling) {
+        const int f = (k == 0) ? 1 : 0, c = cur;
+        check(cudaGraphLaunch(graph_for(k == 0), st), "graph launch");
+        launches += g_kernels[f][c];
+        graph_launches += 1;
+        cur = 1 - cur;
+      } else {
+        begin_step_profile();
+        one_step(k == 0);
       }
-      mark(NBODY_PHASES);
-      launches += 1;
     }
     // the last step's dv + K2 + drag: a record that adds to the stream phase only
     begin_step_profile(false);
@@ -692,8 +745,9 @@ struct SimImpl : SimBase {
   }
 
   void get_state(void* const* v, bool as_double, float* const* acc, bool on_device) override {
+    if (!on_device && !out_stage) out_stage = dalloc<char>(out_stage_bytes(n), "output staging");
     state_out<R>(s[cur], n, ax, ay, az, p.softening, p.star_mass, v, as_double, acc, on_device,
-                 st);
+                 out_stage, st);
   }
 };
 
@@ -873,6 +927,16 @@ int nbody_sim_stats_get(nbody_sim* s, nbody_sim_stats* out) {
     out->walk_nodes_visited = c[0];
     out->walk_stack_spills = c[1];
     out->walk_groups = c[2];
+    out->launches = b->launches;
+    out->graph_launches = b->graph_launches;
+  })
+}
+
+int nbody_sim_set_graphs(nbody_sim* s, int on) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(s, "nbody_sim_set_graphs: null sim");
+    if (!on) s->impl->drop_graphs();
+    s->impl->use_graphs = on != 0;
   })
 }
 
@@ -982,6 +1046,7 @@ struct EnsembleImpl : EnsembleBase {
   unsigned long long* inter = nullptr;
   unsigned long long* counters = nullptr;
   void* staging = nullptr;
+  void* out_stage = nullptr;
   bool use_graphs = true;
   cudaStream_t cap_st = nullptr;
   // [first step of a call?][state buffer at step start]
@@ -1045,9 +1110,9 @@ struct EnsembleImpl : EnsembleBase {
       for (int k = 0; k < 6; ++k) cudaFree(s[b].v[k]);
       cudaFree(s[b].m); cudaFree(s[b].id); cudaFree(s[b].disk);
     }
-    void* ptrs[] = {keys64, keys64_alt, ax,       ay,        az,    dvx,      dvy,
-                    dvz,    vf,         geoms,    bbox,      group_disk, d_off, pert_tab,
-                    pert_step, spill,   work,     inter,     counters,   staging};
+    void* ptrs[] = {keys64, keys64_alt, ax,    ay,    az,         dvx,   dvy,
+                    dvz,    vf,         geoms, bbox,  group_disk, d_off, pert_tab,
+                    pert_step, spill,   work,  inter, counters,   staging, out_stage};
     for (void* q : ptrs)
       if (q) cudaFree(q);
     tree_free(tw);
@@ -1289,8 +1354,9 @@ struct EnsembleImpl : EnsembleBase {
   }
 
   void get_state(void* const* v, bool as_double, float* const* acc, bool on_device) override {
+    if (!on_device && !out_stage) out_stage = dalloc<char>(out_stage_bytes(n), "output staging");
     state_out<R>(s[cur], n, ax, ay, az, p.softening, p.star_mass, v, as_double, acc, on_device,
-                 st);
+                 out_stage, st);
     launches += 1;
   }
 
