@@ -29,6 +29,10 @@ namespace nb {
 namespace {
 
 constexpr int kWalkWarps = 4;
+// Five resident blocks (20 warps) per SM: lets the compiler keep the walk in
+// up to 96 registers; at N = 2^20 that is 22% faster than the 64-register
+// build the default heuristic picks (measured 0.93 vs 1.19 ms per walk).
+constexpr int kWalkMinBlocks = 5;
 constexpr int kStk = 384;
 constexpr int kList = 64;
 
@@ -129,7 +133,7 @@ __device__ __forceinline__ void tape_append(const WalkArgs& a, TapeCursor& t, bo
 // kT targets per lane: a group of up to 32 kT bodies per warp.  kRec: also
 // record the group's source list on the tape.
 template <bool kSoft, int kT, bool kRec>
-__global__ void __launch_bounds__(kWalkWarps * 32) k_walk(const WalkArgs a) {
+__global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_walk(const WalkArgs a) {
   __shared__ WarpSmem smem[kWalkWarps];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   WarpSmem& w = smem[wib];
