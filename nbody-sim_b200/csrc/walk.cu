@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_walk(const 
       int act = 0;  // 1: source, 2: bodies of a leaf, 3: open children
       float4 c = make_float4(0.f, 0.f, 0.f, 0.f);
       int first = 0, cnt = 0;
-      float h2 = 0.f, d2 = 0.f;
+      float h2 = 0.f, d2 = 0.f, far2 = 0.f;
       if (node >= 0) {
         c = __ldg(a.com + node);
         const int4 inf = __ldg(a.info + node);
@@ -211,6 +211,11 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_walk(const 
           const float dy = fmaxf(fmaxf(gy0 - c.y, c.y - gy1), 0.f);
           const float dz = fmaxf(fmaxf(gz0 - c.z, c.z - gz1), 0.f);
           d2 = dx * dx + dy * dy + dz * dz;
+          // farthest point of the box: no target is farther than this
+          const float fx = fmaxf(fabsf(c.x - gx0), fabsf(c.x - gx1));
+          const float fy = fmaxf(fabsf(c.y - gy0), fabsf(c.y - gy1));
+          const float fz = fmaxf(fabsf(c.z - gz0), fabsf(c.z - gz1));
+          far2 = fx * fx + fy * fy + fz * fz;
           if (half * half < a.theta2 * d2) {
             act = 1;
           } else if (nch == 0 || cnt <= a.leaf_max) {
@@ -232,7 +237,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_walk(const 
       // opens 11% fewer interactions and makes the walk 25% faster, at
       // unchanged force error.
       {
-        unsigned cand = __ballot_sync(kFull, act >= 2 && d2 > 0.f);
+        unsigned cand = __ballot_sync(kFull, act >= 2 && d2 > 0.f && h2 < a.theta2 * far2);
         while (cand) {
           const int j = __ffs(cand) - 1;
           cand &= cand - 1;
