@@ -734,7 +734,8 @@ struct AdjointImpl {
     const size_t n1 = n, n2 = 2 * (size_t)n;
     launch_bbox<double>(tw, x, x + n1, x + n2, n, st);
     launch_keys<double>(tw, x, x + n1, x + n2, n, st);
-    radix_sort_pairs(tw.keys, tw.perm, tw.keys_alt, tw.perm_alt, tw.counts, n, 30, st);
+    radix_sort_pairs(tw.keys, tw.perm, tw.keys_alt, tw.perm_alt, tw.counts, n, 30, st,
+                     tw.status);
     k_gather_sorted<<<grid1(n), kThreads, 0, st>>>(tw.perm, x, x + n1, x + n2, mass, n, xs, ys,
                                                    zs, tw.body4);
     launch_build_topology(tw, n, st);

@@ -156,7 +156,7 @@ int nbody_tree_build(nbody_tree* t, const nbody_particles* p) {
     if (!t->have_bbox) nb::launch_bbox<float>(t->tw, p->x, p->y, p->z, t->n, 0);
     nb::launch_keys<float>(t->tw, p->x, p->y, p->z, t->n, 0);
     nb::radix_sort_pairs(t->tw.keys, t->tw.perm, t->tw.keys_alt, t->tw.perm_alt, t->tw.counts,
-                         t->n, 30, 0);
+                         t->n, 30, 0, t->tw.status);
     nb::launch_gather_body4(t->tw, p->x, p->y, p->z, p->mass, t->n, 0);
     nb::launch_build_topology(t->tw, t->n, 0);
     nb::finish("launchBuildKernel");
@@ -351,7 +351,7 @@ int nbody_fof(nbody_tree* t, const float* x, const float* y, const float* z, int
     nb::TreeWork& w = t->tw;
     nb::launch_bbox<float>(w, x, y, z, n, 0);
     nb::launch_keys<float>(w, x, y, z, n, 0);
-    nb::radix_sort_pairs(w.keys, w.perm, w.keys_alt, w.perm_alt, w.counts, n, 30, 0);
+    nb::radix_sort_pairs(w.keys, w.perm, w.keys_alt, w.perm_alt, w.counts, n, 30, 0, w.status);
     nb::launch_gather_body4(w, x, y, z, nullptr, n, 0);
     nb::launch_build_topology(w, n, 0);
     nb::launch_build_moments(w, n, nullptr, nullptr, nullptr, 0);

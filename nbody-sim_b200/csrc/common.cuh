@@ -19,6 +19,7 @@ enum StatusBits : int {
   kStatusTreeLimit = 4,       // tree bottom-up climb exceeded its bound
   kStatusNonFinite = 8,       // a non-finite position reached key generation
   kStatusTapeFull = 16,       // a recording walk ran out of tape chunks
+  kStatusSortWait = 32,       // a radix-sort look-back wait gave up
 };
 
 // Hi/lo float pair state (NBODY_STATE_F32X2): value = hi + lo with

@@ -120,9 +120,11 @@ size_t radix_sort_count_words(int n);
 // Stable LSD sort of (key, value) by the low `bits` bits of the keys; K is
 // uint32_t (single disk, 30-bit Morton keys) or uint64_t (ensemble: disk
 // index above the 30 Morton bits).
+// counts: radix_sort_count_words(n) words of scratch; status (optional)
+// receives kStatusSortWait if a look-back wait gave up.
 template <typename K>
 void radix_sort_pairs(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt,
-                      uint32_t* counts, int n, int bits, cudaStream_t s);
+                      uint32_t* counts, int n, int bits, cudaStream_t s, int* status = nullptr);
 size_t scan_tmp_words(int n);
 void scan_exclusive_u32(uint32_t* data, int n, uint32_t* tmp, cudaStream_t s);
 

@@ -24,7 +24,7 @@ constexpr size_t kAlign = 256;
 
 constexpr size_t al(size_t b) { return (b + kAlign - 1) / kAlign * kAlign; }
 constexpr size_t kNb = 2 * (size_t)kMaxN;
-constexpr size_t kCountWords = 4096;  // >= 2050 words the 32-bit-key sort of kMaxN uses
+constexpr size_t kCountWords = 4096;  // >= 3077 words the 32-bit-key sort of kMaxN uses
 constexpr size_t kScanWords = 4096;   // >= scan_tmp_words(2 kMaxN) = 17
 constexpr size_t kMomTiles = 2 * ((size_t)kMaxN / kMomentTile + 2) + 8;
 
@@ -138,7 +138,8 @@ extern "C" int nbody_fof_noalloc(const float* x, const float* y, const float* z,
     nb::check(cudaMemsetAsync(w.status, 0, sizeof(int), 0), "status clear");
     nb::launch_bbox<float>(w, x, y, z, n, 0);
     nb::launch_keys<float>(w, x, y, z, n, 0);
-    nb::radix_sort_pairs(w.keys, w.perm, w.keys_alt, w.perm_alt, w.counts, n, 30, 0);
+    nb::radix_sort_pairs(w.keys, w.perm, w.keys_alt, w.perm_alt, w.counts, n, 30, 0,
+                         w.status);
     nb::launch_gather_body4(w, x, y, z, nullptr, n, 0);
     nb::launch_build_topology(w, n, 0);
     nb::launch_build_moments(w, n, nullptr, nullptr, nullptr, 0);

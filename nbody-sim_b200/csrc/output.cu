@@ -168,7 +168,8 @@ void OutputPipe::enqueue(Slot& sl, float link_length, float particle_mass) {
   // octree of the snapshot
   launch_bbox<float>(tw, x, y, z, n, os);
   launch_keys<float>(tw, x, y, z, n, os);
-  radix_sort_pairs(tw.keys, tw.perm, tw.keys_alt, tw.perm_alt, tw.counts, n, 30, os);
+  radix_sort_pairs(tw.keys, tw.perm, tw.keys_alt, tw.perm_alt, tw.counts, n, 30, os,
+                   tw.status);
   launch_gather_body4(tw, x, y, z, nullptr, n, os);
   launch_build_topology(tw, n, os);
   launch_build_moments(tw, n, nullptr, nullptr, nullptr, os);
@@ -179,7 +180,7 @@ void OutputPipe::enqueue(Slot& sl, float link_length, float particle_mass) {
   launch_fof_finish(parent, n, labels, sizes, agg, ngroups, tw.status, os);
   // aggregate records
   k_label_pairs<<<grid1(n), kThreads, 0, os>>>(labels, n, keys, vals);
-  radix_sort_pairs(keys, vals, keys_alt, vals_alt, tw.counts, n, bits_for(n), os);
+  radix_sort_pairs(keys, vals, keys_alt, vals_alt, tw.counts, n, bits_for(n), os, tw.status);
   k_group_heads<<<grid1(n), kThreads, 0, os>>>(keys, sizes, n, flag);
   check(cudaMemcpyAsync(slotix, flag, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, os),
         "aggregate slots");

@@ -601,7 +601,8 @@ struct SimImpl : SimBase {
     mark(NBODY_PHASE_SORT);
     launch_keys<R>(tw, a.v[0], a.v[1], a.v[2], n, st);
     launch_bbox_reset(tw, st);
-    radix_sort_pairs(tw.keys, tw.perm, tw.keys_alt, tw.perm_alt, tw.counts, n, 30, st);
+    radix_sort_pairs(tw.keys, tw.perm, tw.keys_alt, tw.perm_alt, tw.counts, n, 30, st,
+                     tw.status);
     mark(NBODY_PHASE_PERMUTE);
     k_permute<R><<<stream_grid(n), kThreads, 0, st>>>(tw.perm, a, b, n, tw.body4);
     check(cudaGetLastError(), "k_permute launch");
@@ -848,7 +849,7 @@ int nbody_sim_sync(nbody_sim* s) {
     if (st) {
       nb::check(cudaMemsetAsync(s->impl->tw.status, 0, sizeof(int), s->impl->st), "status reset");
       throw nb::ArgError("device status " + std::to_string(st) +
-                             " (1 walk stack, 2 union-find, 4 tree, 8 non-finite position)",
+                             " (1 walk stack, 2 union-find, 4 tree, 8 non-finite position, 16 tape, 32 sort wait)",
                          NBODY_ERR_OVERFLOW);
     }
   })
@@ -1228,7 +1229,7 @@ struct EnsembleImpl : EnsembleBase {
                          st);
     launch_bbox_reset_n(bbox, D, st);
     radix_sort_pairs<uint64_t>(keys64, tw.perm, keys64_alt, tw.perm_alt, tw.counts, n, key_bits,
-                               st);
+                               st, tw.status);
     k_permute<R><<<stream_grid(n), kThreads, 0, st>>>(tw.perm, a, b, n, tw.body4);
     check(cudaGetLastError(), "k_permute launch");
     cur = 1 - cur;
@@ -1420,7 +1421,7 @@ struct EnsembleImpl : EnsembleBase {
     if (s) {
       check(cudaMemsetAsync(tw.status, 0, sizeof(int), st), "status reset");
       throw ArgError("device status " + std::to_string(s) +
-                         " (1 walk stack, 2 union-find, 4 tree, 8 non-finite position)",
+                         " (1 walk stack, 2 union-find, 4 tree, 8 non-finite position, 16 tape, 32 sort wait)",
                      NBODY_ERR_OVERFLOW);
     }
   }

@@ -1,14 +1,23 @@
-// sort.cu -- stable LSD radix sort of (uint32 key, uint32 value) pairs.
+// sort.cu -- stable LSD radix sort of (uint32 / uint64 key, uint32 value)
+// pairs, one-sweep form.
 //
 // Replaces the reference's serial DFS ordering (bhtree_sortKernel,
 // BHTree.cu:322-352, a <<<1,1>>> launch) by a Morton-order sort: the body
-// order of the octree IS the sorted key order.  Per 8-bit digit: an upsweep
-// (per-block digit counts, warp-aggregated shared atomics so runs of equal
-// digits in nearly sorted input do not serialise), one scan of the
-// digit-major count table, and a stable scatter that ranks keys with
-// __match_any_sync and stages the tile in shared memory so global writes are
-// runs of consecutive addresses.  HBM traffic per pass: 4 B (upsweep) +
-// 8 B read + 8 B write (scatter) per pair.
+// order of the octree IS the sorted key order.  Digits are 8 bits.
+//   * one histogram kernel counts the digits of every pass in a single read
+//     of the keys (a digit's count does not depend on the key order), and a
+//     tiny kernel turns them into each pass's global digit offsets;
+//   * one kernel per pass: a block takes the next tile (atomic ticket, so
+//     tiles start in order), ranks its keys with __match_any_sync, publishes
+//     its per-digit counts, and finds the counts of all earlier tiles by
+//     decoupled look-back over their published words (aggregate or inclusive
+//     prefix, a 2-bit flag over a 30-bit count); then it stages the tile in
+//     shared memory by digit and writes runs of consecutive addresses.
+// HBM traffic per pass: 8 B read + 8 B write per pair (+ 4 B once for the
+// histograms).  Every look-back wait is bounded: a wait that gives up raises
+// kStatusSortWait instead of hanging (the result is then unusable).
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -25,29 +34,6 @@ template <typename K>
 constexpr int sort_tile() { return kSortThreads * sort_items<K>(); }
 constexpr int kMinTile = kSortThreads * 8;
 constexpr int kBins = 256;
-
-template <typename K>
-__global__ void __launch_bounds__(kSortThreads)
-k_sort_upsweep(const K* __restrict__ keys, uint32_t* __restrict__ counts, int n,
-               int shift, int nblocks) {
-  __shared__ uint32_t s_hist[kBins];
-  const int tid = threadIdx.x, lane = tid & 31;
-  s_hist[tid] = 0;
-  __syncthreads();
-  constexpr int kItems = sort_items<K>();
-  const long long base = (long long)blockIdx.x * sort_tile<K>();
-#pragma unroll 4
-  for (int r = 0; r < kItems; ++r) {
-    long long idx = base + (long long)r * kSortThreads + tid;
-    bool valid = idx < n;
-    uint32_t d = valid ? (uint32_t)(__ldg(keys + idx) >> shift) & 0xffu : kBins;
-    unsigned peers = __match_any_sync(kFull, d);
-    int leader = __ffs(peers) - 1;
-    if (valid && lane == leader) atomicAdd(&s_hist[d], (uint32_t)__popc(peers));
-  }
-  __syncthreads();
-  counts[(long long)tid * nblocks + blockIdx.x] = s_hist[tid];
-}
 
 // Exclusive scan of `total` uint32 in place, one block of 1024 threads.
 __global__ void __launch_bounds__(1024) k_scan_inplace(uint32_t* __restrict__ data, int total) {
@@ -87,11 +73,67 @@ __global__ void __launch_bounds__(1024) k_scan_inplace(uint32_t* __restrict__ da
   }
 }
 
+// ------------------------------------------------------------- one sweep
+constexpr uint32_t kFlagA = 1u << 30;  // tile aggregate published
+constexpr uint32_t kFlagP = 2u << 30;  // inclusive prefix published
+constexpr uint32_t kValMask = (1u << 30) - 1u;
+constexpr uint32_t kFlagMask = ~kValMask;
+constexpr int kSpinLimit = 1 << 20;
+constexpr int kMaxPasses = 8;
+
+// Digit counts of every pass in one read: hist[p * 256 + d] (zeroed first).
 template <typename K>
 __global__ void __launch_bounds__(kSortThreads)
-k_sort_scatter(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
-               K* __restrict__ keys_out, uint32_t* __restrict__ vals_out,
-               const uint32_t* __restrict__ offsets, int n, int shift, int nblocks) {
+k_digit_hist(const K* __restrict__ keys, int n, int passes, uint32_t* __restrict__ hist) {
+  __shared__ uint32_t s_h[kMaxPasses][kBins];
+  const int tid = threadIdx.x, lane = tid & 31;
+  for (int i = tid; i < kMaxPasses * kBins; i += kSortThreads) (&s_h[0][0])[i] = 0;
+  __syncthreads();
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long end = (n + 31) / 32 * 32;  // whole warps take part in match_any
+  for (long long i = (long long)blockIdx.x * blockDim.x + tid; i < end; i += stride) {
+    const bool valid = i < n;
+    const K key = valid ? __ldg(keys + i) : (K)0;
+    for (int p = 0; p < passes; ++p) {
+      const uint32_t d = valid ? (uint32_t)(key >> (8 * p)) & 0xffu : kBins;
+      const unsigned peers = __match_any_sync(kFull, d);
+      if (valid && lane == __ffs(peers) - 1) atomicAdd(&s_h[p][d], (uint32_t)__popc(peers));
+    }
+  }
+  __syncthreads();
+  for (int i = tid; i < passes * kBins; i += kSortThreads) {
+    const uint32_t c = (&s_h[0][0])[i];
+    if (c) atomicAdd(hist + i, c);
+  }
+}
+
+// Exclusive scan of each pass's 256 digit counts (one block per pass).
+__global__ void __launch_bounds__(kBins) k_digit_offsets(uint32_t* __restrict__ hist) {
+  __shared__ uint32_t s_w[kBins / 32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  uint32_t* h = hist + (size_t)blockIdx.x * kBins;
+  const uint32_t c = h[tid];
+  uint32_t v = c;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(kFull, v, o);
+    if (lane >= o) v += t;
+  }
+  if (lane == 31) s_w[warp] = v;
+  __syncthreads();
+  uint32_t add = 0;
+  for (int w = 0; w < warp; ++w) add += s_w[w];
+  h[tid] = v - c + add;
+}
+
+// One pass: rank a tile, publish, look back, scatter.  ticket and status
+// (ntiles x 256 words) start at zero.
+template <typename K>
+__global__ void __launch_bounds__(kSortThreads)
+k_onesweep(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+           K* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int n, int shift,
+           const uint32_t* __restrict__ digit_base, int* __restrict__ ticket,
+           uint32_t* __restrict__ status, int* __restrict__ err) {
   constexpr int kItems = sort_items<K>();
   constexpr int kTile = sort_tile<K>();
   __shared__ uint32_t s_cnt[kSortWarps][kBins];
@@ -100,24 +142,27 @@ k_sort_scatter(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_
   __shared__ uint32_t s_base[kBins];
   __shared__ uint32_t s_glob[kBins];
   __shared__ uint32_t s_wsum[kSortWarps];
+  __shared__ int s_tile;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int i = tid; i < kSortWarps * kBins; i += kSortThreads) (&s_cnt[0][0])[i] = 0;
+  if (tid == 0) s_tile = atomicAdd(ticket, 1);
   __syncthreads();
+  const int t = s_tile;
 
-  const long long tile0 = (long long)blockIdx.x * kTile;
+  const long long tile0 = (long long)t * kTile;
   const long long wbase = tile0 + (long long)warp * (kWarp * kItems);
   K k_reg[kItems];
   uint32_t v_reg[kItems], r_reg[kItems];
 #pragma unroll
   for (int r = 0; r < kItems; ++r) {
-    long long idx = wbase + r * kWarp + lane;
-    bool valid = idx < n;
-    K key = valid ? __ldg(keys_in + idx) : (K)0;
-    uint32_t val = valid ? __ldg(vals_in + idx) : 0u;
-    uint32_t d = valid ? (uint32_t)(key >> shift) & 0xffu : kBins;
-    unsigned peers = __match_any_sync(kFull, d);
-    int leader = __ffs(peers) - 1;
+    const long long idx = wbase + r * kWarp + lane;
+    const bool valid = idx < n;
+    const K key = valid ? __ldg(keys_in + idx) : (K)0;
+    const uint32_t val = valid ? __ldg(vals_in + idx) : 0u;
+    const uint32_t d = valid ? (uint32_t)(key >> shift) & 0xffu : kBins;
+    const unsigned peers = __match_any_sync(kFull, d);
+    const int leader = __ffs(peers) - 1;
     uint32_t old = 0;
     if (valid && lane == leader) {
       old = s_cnt[warp][d];
@@ -131,37 +176,59 @@ k_sort_scatter(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_
   }
   __syncthreads();
 
-  // per digit: exclusive prefix over warps; tile-local digit bases
   {
     const int d = tid;  // kSortThreads == kBins
     uint32_t run = 0;
 #pragma unroll
     for (int w = 0; w < kSortWarps; ++w) {
-      uint32_t c = s_cnt[w][d];
+      const uint32_t c = s_cnt[w][d];
       s_cnt[w][d] = run;
       run += c;
     }
+    // run = this tile's count of digit d: publish it, then look back
+    uint32_t* mine = status + (size_t)t * kBins + d;
+    atomicExch(mine, (t == 0 ? kFlagP : kFlagA) | run);
+    uint32_t excl = 0;
+    if (t > 0) {
+      int j = t - 1, spins = 0;
+      while (j >= 0) {
+        const uint32_t w = __ldcv(status + (size_t)j * kBins + d);
+        const uint32_t f = w & kFlagMask;
+        if (f == 0u) {
+          if (++spins > kSpinLimit) {
+            atomicOr(err, kStatusSortWait);
+            break;
+          }
+          continue;
+        }
+        excl += w & kValMask;
+        if (f == kFlagP) break;
+        --j;
+      }
+      atomicExch(mine, kFlagP | ((excl + run) & kValMask));
+    }
+    s_glob[d] = digit_base[d] + excl;
+    // tile-local base of digit d: exclusive prefix over digits
     uint32_t v = run;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      uint32_t t = __shfl_up_sync(kFull, v, o);
-      if (lane >= o) v += t;
+      const uint32_t q = __shfl_up_sync(kFull, v, o);
+      if (lane >= o) v += q;
     }
     if (lane == 31) s_wsum[warp] = v;
     __syncthreads();
     uint32_t add = 0;
     for (int w = 0; w < warp; ++w) add += s_wsum[w];
     s_base[d] = v - run + add;
-    s_glob[d] = offsets[(long long)d * nblocks + blockIdx.x];
   }
   __syncthreads();
 
 #pragma unroll
   for (int r = 0; r < kItems; ++r) {
-    long long idx = wbase + r * kWarp + lane;
+    const long long idx = wbase + r * kWarp + lane;
     if (idx < n) {
-      uint32_t d = (uint32_t)(k_reg[r] >> shift) & 0xffu;
-      uint32_t lp = s_base[d] + s_cnt[warp][d] + r_reg[r];
+      const uint32_t d = (uint32_t)(k_reg[r] >> shift) & 0xffu;
+      const uint32_t lp = s_base[d] + s_cnt[warp][d] + r_reg[r];
       s_keys[lp] = k_reg[r];
       s_vals[lp] = v_reg[r];
     }
@@ -170,14 +237,13 @@ k_sort_scatter(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_
 
   const int tile_n = (int)min((long long)kTile, (long long)n - tile0);
   for (int i = tid; i < tile_n; i += kSortThreads) {
-    K key = s_keys[i];
-    uint32_t d = (uint32_t)(key >> shift) & 0xffu;
-    uint32_t g = s_glob[d] + (uint32_t)i - s_base[d];
+    const K key = s_keys[i];
+    const uint32_t d = (uint32_t)(key >> shift) & 0xffu;
+    const uint32_t g = s_glob[d] + (uint32_t)i - s_base[d];
     keys_out[g] = key;
     vals_out[g] = s_vals[i];
   }
 }
-
 
 // ---------------------------------------------------------------- scan
 constexpr int kScanThreads = 256;
@@ -249,26 +315,37 @@ k_scan_down(uint32_t* __restrict__ data, int n, const uint32_t* __restrict__ sum
 
 size_t scan_tmp_words(int n);
 
+// Scratch of the sort: per-pass digit offsets (passes x 256), per-pass tile
+// tickets (passes), one word for give-up reports when the caller passes no
+// status word, then the tile status words of one pass (ntiles x 256, cleared
+// before every pass).  Sized for the smaller 64-bit-key tiles.
 size_t radix_sort_count_words(int n) {
-  const size_t table = (size_t)kBins * (size_t)div_up(n, kMinTile);
-  return table + scan_tmp_words((int)table);
+  return (size_t)kMaxPasses * kBins + kMaxPasses + 1 + (size_t)kBins * div_up(n, kMinTile);
 }
 
 template <typename K>
 void radix_sort_pairs(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt,
-                      uint32_t* counts, int n, int bits, cudaStream_t s) {
+                      uint32_t* counts, int n, int bits, cudaStream_t s, int* status) {
   if (n <= 1) return;
-  const int nb = div_up(n, sort_tile<K>());
+  const int ntiles = div_up(n, sort_tile<K>());
   const int passes = (bits + 7) / 8;
-  // the count table is followed by room for the multi-block scan's partials
-  uint32_t* scan_tmp = counts + (size_t)kBins * nb;
+  if (passes > kMaxPasses) throw CudaError("radix_sort_pairs: too many key bits");
+  uint32_t* hist = counts;                      // passes x 256
+  int* tickets = (int*)(counts + (size_t)passes * kBins);
+  int* err = status ? status : tickets + passes;
+  uint32_t* st = counts + (size_t)passes * kBins + passes + 1;
+  check(cudaMemsetAsync(counts, 0, sizeof(uint32_t) * ((size_t)passes * kBins + passes + 1), s),
+        "radix sort histogram reset");
+  const int hgrid = std::max(1, std::min(div_up(n, kSortThreads * 8), 148 * 4));
+  k_digit_hist<K><<<hgrid, kSortThreads, 0, s>>>(keys, n, passes, hist);
+  k_digit_offsets<<<passes, kBins, 0, s>>>(hist);
   K *ki = keys, *ko = keys_alt;
   uint32_t *vi = vals, *vo = vals_alt;
   for (int p = 0; p < passes; ++p) {
-    const int shift = 8 * p;
-    k_sort_upsweep<K><<<nb, kSortThreads, 0, s>>>(ki, counts, n, shift, nb);
-    scan_exclusive_u32(counts, kBins * nb, scan_tmp, s);
-    k_sort_scatter<K><<<nb, kSortThreads, 0, s>>>(ki, vi, ko, vo, counts, n, shift, nb);
+    check(cudaMemsetAsync(st, 0, sizeof(uint32_t) * (size_t)ntiles * kBins, s),
+          "radix sort status reset");
+    k_onesweep<K><<<ntiles, kSortThreads, 0, s>>>(ki, vi, ko, vo, n, 8 * p,
+                                                  hist + (size_t)p * kBins, tickets + p, st, err);
     K* t = ki; ki = ko; ko = t;
     uint32_t* u = vi; vi = vo; vo = u;
   }
@@ -282,9 +359,9 @@ void radix_sort_pairs(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt,
 }
 
 template void radix_sort_pairs<uint32_t>(uint32_t*, uint32_t*, uint32_t*, uint32_t*, uint32_t*,
-                                         int, int, cudaStream_t);
+                                         int, int, cudaStream_t, int*);
 template void radix_sort_pairs<uint64_t>(uint64_t*, uint32_t*, uint64_t*, uint32_t*, uint32_t*,
-                                         int, int, cudaStream_t);
+                                         int, int, cudaStream_t, int*);
 
 }  // namespace nb
 

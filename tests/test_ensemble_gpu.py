@@ -144,7 +144,10 @@ def test_ensemble_autotune_keeps_state(nb, cuda):
     assert (stats.targets_per_lane, stats.leaf_max) == best[:2]
     for k in ("x", "y", "z", "vx", "vy", "vz"):
         assert np.array_equal(before[k], after[k]), k
-    assert np.max(rel_acc_err(before, after)) < 1e-5
+    # the kept setting may group targets and open leaves differently: its
+    # forces differ by the walk's approximation error, a few 1e-5 of the total
+    # acceleration here (self-gravity is ~1e-3 of the star's pull)
+    assert np.max(rel_acc_err(before, after)) < 1e-4
 
 
 def test_ensemble_rejects_bad_input(nb, cuda):
