@@ -154,12 +154,18 @@ k_onesweep(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
   const long long wbase = tile0 + (long long)warp * (kWarp * kItems);
   K k_reg[kItems];
   uint32_t v_reg[kItems], r_reg[kItems];
+  // all loads in flight before the ranking starts
+#pragma unroll
+  for (int r = 0; r < kItems; ++r) {
+    const long long idx = wbase + r * kWarp + lane;
+    k_reg[r] = (idx < n) ? __ldg(keys_in + idx) : (K)0;
+    v_reg[r] = (idx < n) ? __ldg(vals_in + idx) : 0u;
+  }
 #pragma unroll
   for (int r = 0; r < kItems; ++r) {
     const long long idx = wbase + r * kWarp + lane;
     const bool valid = idx < n;
-    const K key = valid ? __ldg(keys_in + idx) : (K)0;
-    const uint32_t val = valid ? __ldg(vals_in + idx) : 0u;
+    const K key = k_reg[r];
     const uint32_t d = valid ? (uint32_t)(key >> shift) & 0xffu : kBins;
     const unsigned peers = __match_any_sync(kFull, d);
     const int leader = __ffs(peers) - 1;
@@ -170,8 +176,6 @@ k_onesweep(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
     }
     old = __shfl_sync(kFull, old, leader);
     __syncwarp();
-    k_reg[r] = key;
-    v_reg[r] = val;
     r_reg[r] = old + __popc(peers & lanemask_lt());
   }
   __syncthreads();
