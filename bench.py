@@ -456,7 +456,8 @@ def run_ensemble(args, ws, rank, local):
                    "n_total": n_all, "disks": args.disks, "parallelism": f"disks over {ws} ranks",
                    "l2": "flushed (256 MB write) before every timed step",
                    "autotune": [list(t) for t in tuned],
-                   "targets_per_lane": s1.targets_per_lane, "leaf_max": s1.leaf_max},
+                   "targets_per_lane": s1.targets_per_lane, "leaf_max": s1.leaf_max,
+                   "walk_mode": s1.walk_mode},
         "gpu_launches": int(s1.launches - s0.launches),
         "graph_launches": int(s1.graph_launches - s0.graph_launches),
         "one_by_one": {"ms_per_step": solo_ms,

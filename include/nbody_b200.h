@@ -282,6 +282,12 @@ typedef struct nbody_sim_params {
   int state_precision;       /* NBODY_STATE_*                              */
   int leaf_max;              /* <= 0: default (8)                          */
   int targets_per_lane;      /* walk: 1 (groups <= 32) or 2 (<= 64); 0: 1  */
+  int walk_mode;             /* walk kernel variant (1 target per lane):
+                                0 (default) acceptance vote, 96 registers;
+                                1 vote, 64 registers; 2 no vote, 64
+                                registers.  Same forces to the walk's
+                                approximation level; speed depends on the
+                                disk (2 suits many small compact disks). */
 } nbody_sim_params;
 
 /* Parameters of src/main.cu:58-73 from a Config (r_coll = factor * radius). */
@@ -437,9 +443,10 @@ int nbody_ensemble_get_state_f64(nbody_ensemble* e, double* x, double* y, double
 int nbody_ensemble_step_host(nbody_ensemble* e, double* x, double* y, double* z, double* vx,
                              double* vy, double* vz, float* ax, float* ay, float* az,
                              const float* mass, int nsteps);
-/* Force-evaluation autotuner: times one force evaluation of the current state
- * for each (targets_per_lane, leaf_max) candidate (candidates[2k],
- * candidates[2k+1]; NULL = the built-in list) and keeps the fastest.  The
+/* Force-evaluation autotuner: times force evaluations of the current state
+ * for each (targets_per_lane, leaf_max, walk_mode) candidate
+ * (candidates[3k .. 3k+2]; NULL = the built-in list of 6) and keeps the
+ * fastest (best of two timings each).  The
  * forces are recomputed with the kept setting, so the state is unchanged.
  * Needs set_state first.  ms_out (optional) receives each candidate's time. */
 int nbody_ensemble_autotune(nbody_ensemble* e, const int* candidates, int n_candidates,
@@ -456,6 +463,7 @@ typedef struct nbody_ensemble_stats {
   unsigned long long interactions;  /* accepted interactions of the last walk */
   unsigned long long launches;      /* kernels launched so far (graph nodes included) */
   unsigned long long graph_launches;
+  int walk_mode;
 } nbody_ensemble_stats;
 int nbody_ensemble_stats_get(nbody_ensemble* e, nbody_ensemble_stats* out);
 

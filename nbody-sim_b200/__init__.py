@@ -121,7 +121,7 @@ class nbody_sim_params(C.Structure):
                 ("gas_drag_rate", C.c_float), ("perturber_enabled", C.c_int),
                 ("perturber_mass_mjup", C.c_float), ("perturber_radius_au", C.c_float),
                 ("perturber_phase0", C.c_float), ("state_precision", C.c_int),
-                ("leaf_max", C.c_int), ("targets_per_lane", C.c_int)]
+                ("leaf_max", C.c_int), ("targets_per_lane", C.c_int), ("walk_mode", C.c_int)]
 
 
 NBODY_PHASES = 6
@@ -157,7 +157,7 @@ class nbody_ensemble_stats(C.Structure):
     _fields_ = [("n_disks", C.c_int), ("n_total", C.c_int), ("steps_done", C.c_int),
                 ("targets_per_lane", C.c_int), ("leaf_max", C.c_int), ("status", C.c_int),
                 ("interactions", C.c_ulonglong), ("launches", C.c_ulonglong),
-                ("graph_launches", C.c_ulonglong)]
+                ("graph_launches", C.c_ulonglong), ("walk_mode", C.c_int)]
 
 
 class nbody_adjoint_stats(C.Structure):
@@ -810,16 +810,15 @@ class Ensemble:
                                             mass.ctypes.data, nsteps))
 
     def autotune(self, candidates=None):
-        """Times one force evaluation per (targets_per_lane, leaf_max); keeps the fastest.
-
-        Returns [(tpl, leaf_max, ms), ...]."""
+        """Times force evaluations per (targets_per_lane, leaf_max, walk_mode);
+        keeps the fastest.  Returns [(tpl, leaf_max, walk_mode, ms), ...]."""
         if candidates is None:
-            candidates = [(1, 4), (1, 8), (1, 16), (2, 8), (2, 16)]
+            candidates = [(1, 8, 0), (1, 8, 1), (1, 8, 2), (1, 4, 2), (1, 16, 2), (2, 8, 0)]
         flat = np.ascontiguousarray(np.array(candidates, np.int32).reshape(-1))
         ms = np.zeros(len(candidates), np.float32)
         _check(lib.nbody_ensemble_autotune(self.h, flat.ctypes.data, len(candidates),
                                            ms.ctypes.data))
-        return [(int(a), int(b), float(t)) for (a, b), t in zip(candidates, ms)]
+        return [(int(a), int(b), int(c), float(t)) for (a, b, c), t in zip(candidates, ms)]
 
     def set_graphs(self, on: bool = True):
         _check(lib.nbody_ensemble_set_graphs(self.h, int(on)))

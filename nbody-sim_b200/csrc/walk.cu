@@ -30,10 +30,17 @@ namespace nb {
 namespace {
 
 constexpr int kWalkWarps = 4;
-// Five resident blocks (20 warps) per SM: lets the compiler keep the walk in
-// up to 96 registers; at N = 2^20 that is 22% faster than the 64-register
-// build the default heuristic picks (measured 0.93 vs 1.19 ms per walk).
-constexpr int kWalkMinBlocks = 5;
+// Walk modes (WalkArgs::walk_mode), a trade-off that depends on the disk:
+//   0: acceptance vote, 5 resident blocks per SM (up to 96 registers) -- at
+//      N = 2^20 over r in [0.3, 30] AU the fastest: 1.19 -> 0.62 ms per walk
+//      against mode 2;
+//   1: acceptance vote, 8 blocks per SM (64 registers);
+//   2: no vote, 8 blocks per SM -- the fastest on small compact disks (the
+//      64-disk ensemble), where the vote rarely pays and occupancy matters.
+template <int kMode>
+constexpr int walk_min_blocks() { return kMode == 0 ? 5 : 8; }
+template <int kMode>
+constexpr bool walk_vote() { return kMode != 2; }
 constexpr int kStk = 384;
 constexpr int kList = 64;
 
@@ -133,8 +140,9 @@ __device__ __forceinline__ void tape_append(const WalkArgs& a, TapeCursor& t, bo
 
 // kT targets per lane: a group of up to 32 kT bodies per warp.  kRec: also
 // record the group's source list on the tape.
-template <bool kSoft, int kT, bool kRec>
-__global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_walk(const WalkArgs a) {
+template <bool kSoft, int kT, bool kRec, int kMode>
+__global__ void __launch_bounds__(kWalkWarps * 32, walk_min_blocks<kMode>())
+    k_walk(const WalkArgs a) {
   __shared__ WarpSmem smem[kWalkWarps];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   WarpSmem& w = smem[wib];
@@ -236,7 +244,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_walk(const 
       // candidate, all lanes testing their own targets.  At N = 2^20 this
       // opens 11% fewer interactions and makes the walk 25% faster, at
       // unchanged force error.
-      {
+      if (walk_vote<kMode>()) {
         unsigned cand = __ballot_sync(kFull, act >= 2 && d2 > 0.f && h2 < a.theta2 * far2);
         while (cand) {
           const int j = __ffs(cand) - 1;
@@ -371,11 +379,11 @@ __global__ void __launch_bounds__(kWalkWarps * 32, kWalkMinBlocks) k_walk(const 
   }
 }
 
-template <bool kSoft, int kT, bool kRec = false>
+template <bool kSoft, int kT, bool kRec = false, int kMode = 0>
 int walk_blocks_per_sm() {
   static int b = 0;
   if (b == 0) {
-    check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<kSoft, kT, kRec>,
+    check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<kSoft, kT, kRec, kMode>,
                                                         kWalkWarps * 32, 0),
           "walk occupancy");
     if (b < 1) b = 1;
@@ -393,12 +401,19 @@ int num_sms() {
   return sms;
 }
 
-template <bool kSoft, int kT, bool kRec = false>
+template <bool kSoft, int kT, bool kRec = false, int kMode = 0>
 void launch_variant(const WalkArgs& a, cudaStream_t s) {
-  int grid = num_sms() * walk_blocks_per_sm<kSoft, kT, kRec>();
+  int grid = num_sms() * walk_blocks_per_sm<kSoft, kT, kRec, kMode>();
   grid = std::min(grid, (a.n + kWalkWarps - 1) / kWalkWarps);  // groups <= n
   if (grid < 1) grid = 1;
-  k_walk<kSoft, kT, kRec><<<grid, kWalkWarps * 32, 0, s>>>(a);
+  k_walk<kSoft, kT, kRec, kMode><<<grid, kWalkWarps * 32, 0, s>>>(a);
+}
+
+template <bool kSoft>
+void launch_mode(const WalkArgs& a, cudaStream_t s) {
+  if (a.walk_mode == 1) launch_variant<kSoft, 1, false, 1>(a, s);
+  else if (a.walk_mode == 2) launch_variant<kSoft, 1, false, 2>(a, s);
+  else launch_variant<kSoft, 1, false, 0>(a, s);
 }
 
 }  // namespace
@@ -407,7 +422,11 @@ int walk_spill_slots(int) {
   const int b = std::max(
       std::max(std::max(walk_blocks_per_sm<true, 1>(), walk_blocks_per_sm<false, 1>()),
                std::max(walk_blocks_per_sm<true, 2>(), walk_blocks_per_sm<false, 2>())),
-      std::max(walk_blocks_per_sm<true, 1, true>(), walk_blocks_per_sm<false, 1, true>()));
+      std::max(std::max(walk_blocks_per_sm<true, 1, true>(), walk_blocks_per_sm<false, 1, true>()),
+               std::max(std::max(walk_blocks_per_sm<true, 1, false, 1>(),
+                                 walk_blocks_per_sm<false, 1, false, 1>()),
+                        std::max(walk_blocks_per_sm<true, 1, false, 2>(),
+                                 walk_blocks_per_sm<false, 1, false, 2>()))));
   return num_sms() * b * kWalkWarps;
 }
 
@@ -422,8 +441,8 @@ void launch_walk(const WalkArgs& a, cudaStream_t s) {
     if (soft) launch_variant<true, 2>(a, s);
     else launch_variant<false, 2>(a, s);
   } else {
-    if (soft) launch_variant<true, 1>(a, s);
-    else launch_variant<false, 1>(a, s);
+    if (soft) launch_mode<true>(a, s);
+    else launch_mode<false>(a, s);
   }
   check(cudaGetLastError(), "k_walk launch");
 }

@@ -37,3 +37,26 @@ def test_graph_steps_equal_plain_launches(nb, cuda, precision):
     assert sg.launches == sp.launches
     for k in g:
         assert np.array_equal(g[k], p[k]), k
+
+
+def test_walk_modes_agree(nb, cuda):
+    """The three walk variants: modes 0 and 1 differ only in register budget
+    (bit-identical forces); mode 2 skips the acceptance vote, so it opens more
+    nodes and agrees to the walk's approximation level."""
+    n = 20000
+    st = disk(nb, n, 0.3, 30.0, seed=3, m=1e-9)
+    acc = {}
+    for mode in (0, 1, 2):
+        prm = nb.sim_params(dt=0.002, theta=0.5, softening=5e-4, star_mass=0.0, r_coll=0.0,
+                            gas_drag_rate=0.0, walk_mode=mode)
+        sim = nb.Sim(prm, n)
+        sim.set_state(st["x"], st["y"], st["z"], st["vx"], st["vy"], st["vz"], st["m"])
+        g = sim.get_state(accel=True)
+        acc[mode] = np.stack([g["ax"], g["ay"], g["az"]], 1).astype(np.float64)
+        inter = sim.stats().interactions
+        acc[f"i{mode}"] = inter
+        sim.close()
+    assert np.array_equal(acc[0], acc[1])
+    assert acc["i0"] == acc["i1"] and acc["i2"] > acc["i0"]
+    rel = np.linalg.norm(acc[0] - acc[2], axis=1) / np.linalg.norm(acc[2], axis=1)
+    assert np.median(rel) < 5e-2

@@ -139,9 +139,9 @@ def test_ensemble_autotune_keeps_state(nb, cuda):
     after = e.get_state(double=True, accel=True)
     stats = e.stats()
     e.close()
-    assert len(tuned) == 5 and all(t[2] > 0 for t in tuned)
-    best = min(tuned, key=lambda t: t[2])
-    assert (stats.targets_per_lane, stats.leaf_max) == best[:2]
+    assert len(tuned) == 6 and all(t[3] > 0 for t in tuned)
+    best = min(tuned, key=lambda t: t[3])
+    assert (stats.targets_per_lane, stats.leaf_max, stats.walk_mode) == best[:3]
     for k in ("x", "y", "z", "vx", "vy", "vz"):
         assert np.array_equal(before[k], after[k]), k
     # the kept setting may group targets and open leaves differently: its
