@@ -219,11 +219,13 @@ __global__ void __launch_bounds__(kWalkWarps * 32, walk_min_blocks<kMode>())
           const float dy = fmaxf(fmaxf(gy0 - c.y, c.y - gy1), 0.f);
           const float dz = fmaxf(fmaxf(gz0 - c.z, c.z - gz1), 0.f);
           d2 = dx * dx + dy * dy + dz * dz;
-          // farthest point of the box: no target is farther than this
-          const float fx = fmaxf(fabsf(c.x - gx0), fabsf(c.x - gx1));
-          const float fy = fmaxf(fabsf(c.y - gy0), fabsf(c.y - gy1));
-          const float fz = fmaxf(fabsf(c.z - gz0), fabsf(c.z - gz1));
-          far2 = fx * fx + fy * fy + fz * fz;
+          if (walk_vote<kMode>()) {
+            // farthest point of the box: no target is farther than this
+            const float fx = fmaxf(fabsf(c.x - gx0), fabsf(c.x - gx1));
+            const float fy = fmaxf(fabsf(c.y - gy0), fabsf(c.y - gy1));
+            const float fz = fmaxf(fabsf(c.z - gz0), fabsf(c.z - gz1));
+            far2 = fx * fx + fy * fy + fz * fz;
+          }
           if (half * half < a.theta2 * d2) {
             act = 1;
           } else if (nch == 0 || cnt <= a.leaf_max) {
