@@ -575,8 +575,10 @@ def run_adjoint(args, ws, rank, local):
 
     eng = nb.Adjoint(prm, n, steps)
     eng.set_stream(stream.cuda_stream)
-    # warm-up (sizes the tape pool), then the measured gradient
+    # warm-up (sizes the tape pool, captures the forward and backward graphs),
+    # then the measured gradient
     eng.forward(x0, v0, mass, pm, pr)
+    eng.backward(torch.zeros_like(x0), torch.zeros_like(v0))
     x0r = x0.clone().requires_grad_(True)
     v0r = v0.clone().requires_grad_(True)
     pmt = torch.tensor(pm, dtype=torch.float64, device="cuda", requires_grad=True)

@@ -115,7 +115,8 @@ struct StepArgsT {
   double* nx;        // out (kBegin): level L+1 positions
   double* ny;
   double* nz;
-  double4 pert;      // perturber (x, y, z, mass in M_sun) at t_L
+  const double4* pert_tab;  // perturber (x, y, z, mass in M_sun) per level
+  int level;
   double eps, star_mass, dt, dth, decay;
   int drag;
   int n;
@@ -130,7 +131,8 @@ __global__ void __launch_bounds__(kThreads) k_dstep(const StepArgsT<TA> a) {
     const double x = a.x[i], y = a.y[i], z = a.z[i];
     double vx = a.vx[i], vy = a.vy[i], vz = a.vz[i];
     double ax, ay, az;
-    total_accel(x, y, z, a.ax[i], a.ay[i], a.az[i], a.eps, a.star_mass, a.pert, ax, ay, az);
+    total_accel(x, y, z, a.ax[i], a.ay[i], a.az[i], a.eps, a.star_mass, a.pert_tab[a.level], ax,
+                ay, az);
     if (kEnd) {
       vx = fma(ax, a.dth, vx); vy = fma(ay, a.dth, vy); vz = fma(az, a.dth, vz);
       if (a.drag) gas_drag<double>(x, z, vx, vy, vz, a.decay, a.star_mass);
@@ -432,7 +434,8 @@ struct ApplyArgs {
   double* plx;              // out: pending acceleration adjoint dt/2 V_h
   double* ply;
   double* plz;
-  double4 pert;
+  const double4* pert_tab;
+  int level;
   double eps, star_mass, dt, dth;
   double* pgrad;            // 4 per level: adjoint of perturber x, y, z, mass
   int n;
@@ -465,15 +468,16 @@ __global__ void __launch_bounds__(kThreads) k_adj_apply(const ApplyArgs a) {
       gy -= a.star_mass * (ly * inv3 - 3.0 * y * xl * inv5);
       gz -= a.star_mass * (lz * inv3 - 3.0 * z * xl * inv5);
     }
-    if (a.pert.w != 0.0) {  // a = m_p d / r^3 with d = p - x
-      const double dx = a.pert.x - x, dy = a.pert.y - y, dz = a.pert.z - z;
+    const double4 pt = a.pert_tab[a.level];
+    if (pt.w != 0.0) {  // a = m_p d / r^3 with d = p - x
+      const double dx = pt.x - x, dy = pt.y - y, dz = pt.z - z;
       const double r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, a.eps * a.eps)));
       const double inv = 1.0 / sqrt(r2);
       const double inv3 = inv * inv * inv, inv5 = inv3 * inv * inv;
       const double dl = dx * lx + dy * ly + dz * lz;
-      const double jx = a.pert.w * (lx * inv3 - 3.0 * dx * dl * inv5);
-      const double jy = a.pert.w * (ly * inv3 - 3.0 * dy * dl * inv5);
-      const double jz = a.pert.w * (lz * inv3 - 3.0 * dz * dl * inv5);
+      const double jx = pt.w * (lx * inv3 - 3.0 * dx * dl * inv5);
+      const double jy = pt.w * (ly * inv3 - 3.0 * dy * dl * inv5);
+      const double jz = pt.w * (lz * inv3 - 3.0 * dz * dl * inv5);
       gx -= jx; gy -= jy; gz -= jz;
       pg[0] += jx; pg[1] += jy; pg[2] += jz;
       pg[3] += dl * inv3;
@@ -519,7 +523,8 @@ struct DragAdjArgs {
   const float* a1x;
   const float* a1y;
   const float* a1z;
-  double4 p0, p1;
+  const double4* pert_tab;  // levels L and L+1
+  int level;
   double eps, star_mass, dth, decay;
   int drag;
   // adjoints
@@ -548,8 +553,9 @@ __global__ void __launch_bounds__(kThreads) k_adj_drag(const DragAdjArgs a) {
       if (!(rxz2 < 1e-12)) {
         double ax0, ay0, az0, ax1, ay1, az1;
         total_accel(a.x0[i], a.y0[i], a.z0[i], a.a0x[i], a.a0y[i], a.a0z[i], a.eps, a.star_mass,
-                    a.p0, ax0, ay0, az0);
-        total_accel(x, a.y1[i], z, a.a1x[i], a.a1y[i], a.a1z[i], a.eps, a.star_mass, a.p1, ax1,
+                    a.pert_tab[a.level], ax0, ay0, az0);
+        total_accel(x, a.y1[i], z, a.a1x[i], a.a1y[i], a.a1z[i], a.eps, a.star_mass,
+                    a.pert_tab[a.level + 1], ax1,
                     ay1, az1);
         double vx = fma(ax0, a.dth, a.v0x[i]), vz = fma(az0, a.dth, a.v0z[i]);
         vx = fma(ax1, a.dth, vx);
@@ -617,6 +623,21 @@ struct AdjointImpl {
   float ms_forward = 0.f, ms_backward = 0.f, ms_replay = 0.f;
   unsigned long long launches = 0;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
+  // perturber (x, y, z, mass in M_sun) per level: recorded run, replays
+  double4* pert_fwd = nullptr;
+  double4* pert_rep = nullptr;
+  // The recording forward, the backward and the two replays are each captured
+  // once as a CUDA graph (every buffer they touch is fixed for the engine's
+  // life; inputs and outputs are copied in and out around the launch) and
+  // replayed: at small n a level is a few tens of microseconds of GPU work,
+  // less than launching its kernels one by one.
+  struct Captured {
+    cudaGraphExec_t g = nullptr;
+    unsigned long long kernels = 0;
+  };
+  Captured g_fwd, g_bwd, g_rep[2];
+  double* rep_final[2] = {nullptr, nullptr};  // buffer holding a replay's final positions
+  cudaStream_t cap_st = nullptr;
 
   AdjointImpl(const nbody_sim_params& prm, int nn, int nsteps) {
     p = prm;
@@ -655,6 +676,9 @@ struct AdjointImpl {
     work = dalloc<int>(1, "work");
     inter = dalloc<unsigned long long>(1, "interactions");
     pool_used = dalloc<int>(1, "tape chunks used");
+    aw64 = dalloc<double>(n3, "FP64 replay self-gravity");
+    pert_fwd = dalloc<double4>(steps + 1, "perturber per level");
+    pert_rep = dalloc<double4>(steps + 1, "replay perturber per level");
     nbody_config c;
     nbody_config_defaults(&c);
     c.perturber_enabled = 1;
@@ -669,6 +693,8 @@ struct AdjointImpl {
 
   ~AdjointImpl() {
     if (st) cudaStreamSynchronize(st);
+    drop_graphs();
+    if (cap_st) cudaStreamDestroy(cap_st);
     for (auto* q : X) cudaFree(q);
     for (auto* q : V) cudaFree(q);
     for (auto* q : A) cudaFree(q);
@@ -676,7 +702,8 @@ struct AdjointImpl {
     for (auto* q : groups) cudaFree(q);
     for (auto* q : gtape) cudaFree(q);
     void* ptrs[] = {ngroups, pool, pool_next, pool_used, xs, ys, zs, vw, xw, aw, aw64, gx, gv, lam,
-                    mu, radd, rploc, rtiles, pgrad, mass, spill, work, inter};
+                    mu, radd, rploc, rtiles, pgrad, mass, spill, work, inter, pert_fwd,
+                    pert_rep};
     for (void* q : ptrs)
       if (q) cudaFree(q);
     tree_free(tw);
@@ -703,14 +730,15 @@ struct AdjointImpl {
 
   template <typename TA = float>
   StepArgsT<TA> step_args(const double* x, double* v, const TA* a, double* lv, double* nx,
-                          double4 pert) const {
+                          const double4* tab, int level) const {
     StepArgsT<TA> s{};
     s.x = x; s.y = x + n; s.z = x + 2 * (size_t)n;
     s.vx = v; s.vy = v + n; s.vz = v + 2 * (size_t)n;
     s.ax = a; s.ay = a + n; s.az = a + 2 * (size_t)n;
     s.lvx = lv; s.lvy = lv ? lv + n : nullptr; s.lvz = lv ? lv + 2 * (size_t)n : nullptr;
     s.nx = nx; s.ny = nx ? nx + n : nullptr; s.nz = nx ? nx + 2 * (size_t)n : nullptr;
-    s.pert = pert;
+    s.pert_tab = tab;
+    s.level = level;
     s.eps = p.softening; s.star_mass = p.star_mass;
     s.dt = (double)p.dt; s.dth = (double)p.dt * 0.5;
     s.drag = p.gas_drag_rate > 0.f;
@@ -761,9 +789,59 @@ struct AdjointImpl {
     launches += 36;
   }
 
+  void drop_graphs() {
+    for (Captured* c : {&g_fwd, &g_bwd, &g_rep[0], &g_rep[1]})
+      if (c->g) {
+        cudaGraphExecDestroy(c->g);
+        c->g = nullptr;
+      }
+  }
+
+  // Runs body's launches as one graph (captured on first use, on a private
+  // stream; the caller's stream may be the legacy one), on the engine stream.
+  template <typename F>
+  void run_graph(Captured& c, F&& body) {
+    if (!c.g) {
+      if (!cap_st)
+        check(cudaStreamCreateWithFlags(&cap_st, cudaStreamNonBlocking), "capture stream");
+      cudaStream_t user = st;
+      const unsigned long long l0 = launches;
+      cudaGraph_t graph = nullptr;
+      st = cap_st;
+      check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+      try {
+        body();
+      } catch (...) {
+        cudaStreamEndCapture(st, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        st = user;
+        launches = l0;
+        throw;
+      }
+      const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+      st = user;
+      check(ce, "end capture");
+      c.kernels = launches - l0;
+      launches = l0;
+      const cudaError_t ie = cudaGraphInstantiate(&c.g, graph, 0);
+      cudaGraphDestroy(graph);
+      check(ie, "graph instantiate");
+    }
+    check(cudaGraphLaunch(c.g, st), "graph launch");
+    launches += c.kernels;
+  }
+
+  void upload_pert(double4* tab, double mass_mj, double radius) {
+    std::vector<double4> h(steps + 1);
+    for (int L = 0; L <= steps; ++L) h[L] = pert_at(L, mass_mj, radius);
+    check(cudaMemcpyAsync(tab, h.data(), sizeof(double4) * h.size(), cudaMemcpyHostToDevice, st),
+          "perturber table");
+  }
+
   void ensure_pool(int chunks) {
     if (chunks <= pool_cap) return;
     check(cudaStreamSynchronize(st), "tape pool sync");
+    drop_graphs();  // the captured runs hold the old pool
     if (pool) cudaFree(pool);
     if (pool_next) cudaFree(pool_next);
     pool_cap = chunks;
@@ -805,21 +883,24 @@ struct AdjointImpl {
       }
       break;
     }
+    upload_pert(pert_fwd, pm, pr);
     for (int attempt = 0; attempt < 3; ++attempt) {
-      check(cudaMemsetAsync(tw.status, 0, sizeof(int), st), "status reset");
-      check(cudaMemsetAsync(pool_used, 0, sizeof(int), st), "tape reset");
-      check(cudaEventRecord(e0, st), "event");
-      record_level(0);
       for (int k = 0; k < 3; ++k)
         check(cudaMemcpyAsync(vw + (size_t)k * n, x0[3 + k], sizeof(double) * n,
                               cudaMemcpyDeviceToDevice, st),
               "initial velocities");
-      for (int L = 0; L <= steps; ++L) {
-        const bool end = L > 0, begin = L < steps;
-        launch_step(end, begin, step_args<float>(X[L], vw, A[L], V[L],
-                                                 begin ? X[L + 1] : nullptr, pert_at(L, pm, pr)));
-        if (begin) record_level(L + 1);
-      }
+      check(cudaEventRecord(e0, st), "event");
+      run_graph(g_fwd, [&] {
+        check(cudaMemsetAsync(tw.status, 0, sizeof(int), st), "status reset");
+        check(cudaMemsetAsync(pool_used, 0, sizeof(int), st), "tape reset");
+        record_level(0);
+        for (int L = 0; L <= steps; ++L) {
+          const bool end = L > 0, begin = L < steps;
+          launch_step(end, begin, step_args<float>(X[L], vw, A[L], V[L],
+                                                   begin ? X[L + 1] : nullptr, pert_fwd, L));
+          if (begin) record_level(L + 1);
+        }
+      });
       check(cudaEventRecord(e1, st), "event");
       const int s = read_status();
       if (s & kStatusTapeFull) {
@@ -890,38 +971,42 @@ struct AdjointImpl {
               bool fp64) {
     if (!recorded) throw ArgError("adjoint replay: no recorded forward", NBODY_ERR_STATE);
     const size_t n3 = 3 * (size_t)n;
-    double* xa = xw;
-    double* xb = xw + n3;
+    upload_pert(pert_rep, mass_mj, radius);
     for (int k = 0; k < 3; ++k) {
-      check(cudaMemcpyAsync(xa + (size_t)k * n, x0[k], sizeof(double) * n,
+      check(cudaMemcpyAsync(xw + (size_t)k * n, x0[k], sizeof(double) * n,
                             cudaMemcpyDeviceToDevice, st), "replay positions");
       check(cudaMemcpyAsync(vw + (size_t)k * n, x0[3 + k], sizeof(double) * n,
                             cudaMemcpyDeviceToDevice, st), "replay velocities");
     }
-    check(cudaMemsetAsync(tw.status, 0, sizeof(int), st), "status reset");
+    const int f = fp64 ? 1 : 0;
     check(cudaEventRecord(e0, st), "event");
-    for (int L = 0; L <= steps; ++L) {
-      level_bodies(L, xa);
-      ReplayArgs r = replay_args(L);
-      const bool end = L > 0, begin = L < steps;
-      if (fp64) {
-        if (!aw64) aw64 = dalloc<double>(3 * (size_t)n, "FP64 replay self-gravity");
-        r.dax = aw64; r.day = aw64 + n; r.daz = aw64 + 2 * (size_t)n;
-        r.xs = xs; r.ys = ys; r.zs = zs;
-        launch_replay(r, false, true);
-        launch_step(end, begin, step_args<double>(xa, vw, aw64, nullptr, begin ? xb : nullptr,
-                                                  pert_at(L, mass_mj, radius)));
-      } else {
-        r.ax = aw; r.ay = aw + n; r.az = aw + 2 * (size_t)n;
-        launch_replay(r, false);
-        launch_step(end, begin, step_args<float>(xa, vw, aw, nullptr, begin ? xb : nullptr,
-                                                 pert_at(L, mass_mj, radius)));
+    run_graph(g_rep[f], [&] {
+      check(cudaMemsetAsync(tw.status, 0, sizeof(int), st), "status reset");
+      double* xa = xw;
+      double* xb = xw + n3;
+      for (int L = 0; L <= steps; ++L) {
+        level_bodies(L, xa);
+        ReplayArgs r = replay_args(L);
+        const bool end = L > 0, begin = L < steps;
+        if (fp64) {
+          r.dax = aw64; r.day = aw64 + n; r.daz = aw64 + 2 * (size_t)n;
+          r.xs = xs; r.ys = ys; r.zs = zs;
+          launch_replay(r, false, true);
+          launch_step(end, begin, step_args<double>(xa, vw, aw64, nullptr, begin ? xb : nullptr,
+                                                    pert_rep, L));
+        } else {
+          r.ax = aw; r.ay = aw + n; r.az = aw + 2 * (size_t)n;
+          launch_replay(r, false);
+          launch_step(end, begin, step_args<float>(xa, vw, aw, nullptr, begin ? xb : nullptr,
+                                                   pert_rep, L));
+        }
+        if (begin) std::swap(xa, xb);
       }
-      if (begin) std::swap(xa, xb);
-    }
+      rep_final[f] = xa;
+    });
     check(cudaEventRecord(e1, st), "event");
     for (int k = 0; k < 3; ++k) {
-      check(cudaMemcpyAsync(out[k], xa + (size_t)k * n, sizeof(double) * n,
+      check(cudaMemcpyAsync(out[k], rep_final[f] + (size_t)k * n, sizeof(double) * n,
                             cudaMemcpyDeviceToDevice, st), "replay out");
       check(cudaMemcpyAsync(out[3 + k], vw + (size_t)k * n, sizeof(double) * n,
                             cudaMemcpyDeviceToDevice, st), "replay out");
@@ -954,7 +1039,8 @@ struct AdjointImpl {
     a.gx = gx; a.gy = gx + n; a.gz = gx + 2 * (size_t)n;
     a.gvx = gv; a.gvy = gv + n; a.gvz = gv + 2 * (size_t)n;
     a.plx = lam; a.ply = lam + n; a.plz = lam + 2 * (size_t)n;  // lam is consumed per body
-    a.pert = pert_at(L, pm, pr);
+    a.pert_tab = pert_fwd;
+    a.level = L;
     a.eps = p.softening; a.star_mass = p.star_mass;
     a.dt = (double)p.dt; a.dth = (double)p.dt * 0.5;
     a.pgrad = pgrad + 4 * (size_t)L;
@@ -969,17 +1055,24 @@ struct AdjointImpl {
   // initial state and of (perturber mass in M_J, perturber radius in AU).
   void backward(const double* const* g_final, double* const* g_init, double* g_par) {
     if (!recorded) throw ArgError("adjoint backward: no recorded forward", NBODY_ERR_STATE);
-    const size_t n3 = 3 * (size_t)n;
     for (int k = 0; k < 3; ++k) {
       check(cudaMemcpyAsync(gx + (size_t)k * n, g_final[k], sizeof(double) * n,
                             cudaMemcpyDeviceToDevice, st), "final adjoint");
       check(cudaMemcpyAsync(gv + (size_t)k * n, g_final[3 + k], sizeof(double) * n,
                             cudaMemcpyDeviceToDevice, st), "final adjoint");
     }
+    check(cudaEventRecord(e0, st), "event");
+    run_graph(g_bwd, [&] { backward_levels(); });
+    check(cudaEventRecord(e1, st), "event");
+    finish_backward(g_init, g_par);
+  }
+
+  // Every level of the backward (captured as one graph).
+  void backward_levels() {
+    const size_t n3 = 3 * (size_t)n;
     check(cudaMemsetAsync(lam, 0, sizeof(double) * n3, st), "pending reset");
     check(cudaMemsetAsync(pgrad, 0, sizeof(double) * 4 * (steps + 1), st), "perturber reset");
     check(cudaMemsetAsync(tw.status, 0, sizeof(int), st), "status reset");
-    check(cudaEventRecord(e0, st), "event");
     const double dth = (double)p.dt * 0.5;
     const bool drag = p.gas_drag_rate > 0.f;
     const double decay = drag ? std::exp(-(double)p.gas_drag_rate * (double)p.dt) : 1.0;
@@ -990,8 +1083,8 @@ struct AdjointImpl {
       d.a0x = A[L]; d.a0y = A[L] + n; d.a0z = A[L] + 2 * (size_t)n;
       d.x1 = X[L + 1]; d.y1 = X[L + 1] + n; d.z1 = X[L + 1] + 2 * (size_t)n;
       d.a1x = A[L + 1]; d.a1y = A[L + 1] + n; d.a1z = A[L + 1] + 2 * (size_t)n;
-      d.p0 = pert_at(L, pm, pr);
-      d.p1 = pert_at(L + 1, pm, pr);
+      d.pert_tab = pert_fwd;
+      d.level = L;
       d.eps = p.softening; d.star_mass = p.star_mass; d.dth = dth; d.decay = decay;
       d.drag = drag;
       d.gx = gx; d.gy = gx + n; d.gz = gx + 2 * (size_t)n;
@@ -1004,7 +1097,9 @@ struct AdjointImpl {
       force_adjoint(L + 1, true);
     }
     force_adjoint(0, false);
-    check(cudaEventRecord(e1, st), "event");
+  }
+
+  void finish_backward(double* const* g_init, double* g_par) {
     for (int k = 0; k < 3; ++k) {
       check(cudaMemcpyAsync(g_init[k], gx + (size_t)k * n, sizeof(double) * n,
                             cudaMemcpyDeviceToDevice, st), "initial adjoint");
