@@ -16,7 +16,7 @@
 // Backward: the exact adjoint of that computation with the tree frozen
 // (same permutations, groups and source lists).  Per level, the tape is
 // replayed with the interaction's vector-Jacobian product: the target side
-// accumulates -g in FP64, the source side adds +g to its centre of mass,
+// accumulates -g (FP32 within a 32-source chunk, FP64 across chunks), the source side adds +g to its centre of mass,
 // whose adjoint reaches each member body j in proportion m_j / M_node (a
 // range add over the sorted body range, resolved by one prefix sum).  The
 // star, perturber and drag Jacobians are applied per body in FP64; the
@@ -317,13 +317,16 @@ __global__ void __launch_bounds__(kRW * 32) k_replay(const ReplayArgs a) {
       if (!kAdj) {
         for (int j = 0; j < k; ++j) interact<kSoft>(w.lst[j], me, a.eps2, acc);
       } else {
-        // target side: -g for every source except the body itself
+        // target side: -g for every source except the body itself, summed
+        // over the chunk (<= 32 terms) in FP32, the chunk sums in FP64
+        float3 part = make_float3(0.f, 0.f, 0.f);
         for (int j = 0; j < k; ++j) {
           const int2 e = w.ent[j];
           if (e.y == 1 && e.x == s) continue;
           const float3 gv = interact_vjp<kSoft>(w.lst[j], me, a.eps2, lam);
-          mx -= (double)gv.x; my -= (double)gv.y; mz -= (double)gv.z;
+          part.x += gv.x; part.y += gv.y; part.z += gv.z;
         }
+        mx -= (double)part.x; my -= (double)part.y; mz -= (double)part.z;
         // source side: lane j sums +g over the group's targets and spreads
         // it over the source's bodies in proportion to their mass
         if (lane < k) {
