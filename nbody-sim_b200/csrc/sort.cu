@@ -274,22 +274,26 @@ k_scan_reduce(const uint32_t* __restrict__ data, int n, uint32_t* __restrict__ s
   }
 }
 
+// Shared-memory index with one pad word per 32: thread t's run of
+// kScanItems consecutive words then spreads over all 32 banks.
+__device__ __forceinline__ int pad32(int i) { return i + (i >> 5); }
+
 __global__ void __launch_bounds__(kScanThreads)
 k_scan_down(uint32_t* __restrict__ data, int n, const uint32_t* __restrict__ sums) {
-  __shared__ uint32_t s_tile[kScanTile];
+  __shared__ uint32_t s_tile[kScanTile + kScanTile / 32];
   __shared__ uint32_t s_w[kScanThreads / 32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const long long base = (long long)blockIdx.x * kScanTile;
   for (int r = 0; r < kScanItems; ++r) {
     long long i = base + (long long)r * kScanThreads + tid;
-    s_tile[r * kScanThreads + tid] = (i < n) ? data[i] : 0u;
+    s_tile[pad32(r * kScanThreads + tid)] = (i < n) ? data[i] : 0u;
   }
   __syncthreads();
   uint32_t loc[kScanItems];
   uint32_t sum = 0;
 #pragma unroll
   for (int k = 0; k < kScanItems; ++k) {
-    loc[k] = s_tile[tid * kScanItems + k];
+    loc[k] = s_tile[pad32(tid * kScanItems + k)];
     sum += loc[k];
   }
   uint32_t v = sum;
@@ -305,13 +309,13 @@ k_scan_down(uint32_t* __restrict__ data, int n, const uint32_t* __restrict__ sum
   uint32_t run = add + v - sum;
 #pragma unroll
   for (int k = 0; k < kScanItems; ++k) {
-    s_tile[tid * kScanItems + k] = run;
+    s_tile[pad32(tid * kScanItems + k)] = run;
     run += loc[k];
   }
   __syncthreads();
   for (int r = 0; r < kScanItems; ++r) {
     long long i = base + (long long)r * kScanThreads + tid;
-    if (i < n) data[i] = s_tile[r * kScanThreads + tid];
+    if (i < n) data[i] = s_tile[pad32(r * kScanThreads + tid)];
   }
 }
 
