@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--theta", type=float, default=WORKLOAD["theta"])
     ap.add_argument("--precision", choices=["f32", "f64"], default="f32")
     ap.add_argument("--leaf-max", type=int, default=8)
+    ap.add_argument("--walk-mode", type=int, default=None, choices=[0, 1, 2],
+                    help="force-walk variant (nbody_sim_params.walk_mode); default: the engine's")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-flush", action="store_true")
@@ -239,6 +241,8 @@ def run_ours(args, ws, rank, local):
     prm = nb.sim_params(dt=w["dt"], theta=args.theta, softening=w["eps"], star_mass=1.0,
                         r_coll=0.0, restitution=0.0, gas_drag_rate=0.0, state_precision=prec,
                         leaf_max=args.leaf_max)
+    if args.walk_mode is not None:
+        prm.walk_mode = args.walk_mode
     stream = torch.cuda.current_stream()
     sim = nb.Sim(prm, n)
     sim.set_stream(stream.cuda_stream)

@@ -283,9 +283,9 @@ typedef struct nbody_sim_params {
   int leaf_max;              /* <= 0: default (8)                          */
   int targets_per_lane;      /* walk: 1 (groups <= 32) or 2 (<= 64); 0: 1  */
   int walk_mode;             /* walk kernel variant (1 target per lane):
-                                0 (default) acceptance vote, 96 registers;
-                                1 vote, 64 registers; 2 no vote, 64
-                                registers.  Same forces to the walk's
+                                0 acceptance vote, 96 registers; 1
+                                (default) vote, 64 registers; 2 no vote,
+                                64 registers.  Same forces to the walk's
                                 approximation level; speed depends on the
                                 disk (2 suits many small compact disks). */
 } nbody_sim_params;

@@ -594,6 +594,10 @@ class OutputWriter:
 
 
 # ------------------------------------------------------------- engine
+# the engine's default walk variant (nbody_sim_params.walk_mode; vote, 64 registers)
+WALK_MODE_DEFAULT = 1
+
+
 def sim_params(cfg: nbody_config | None = None, **kw) -> nbody_sim_params:
     p = nbody_sim_params()
     if cfg is not None:
@@ -601,6 +605,7 @@ def sim_params(cfg: nbody_config | None = None, **kw) -> nbody_sim_params:
     else:
         p.dt, p.theta, p.softening, p.star_mass, p.leaf_max = 0.01, 0.5, 0.01, 1.0, 8
         p.targets_per_lane = 1
+        p.walk_mode = WALK_MODE_DEFAULT
     for k, v in kw.items():
         setattr(p, k, v)
     return p

@@ -769,6 +769,7 @@ struct AdjointImpl {
                      tw.status);
     k_gather_sorted<<<grid1(n), kThreads, 0, st>>>(tw.perm, x, x + n1, x + n2, mass, n, xs, ys,
                                                    zs, tw.body4);
+    tw.prune_max = p.leaf_max;
     launch_build_topology(tw, n, st);
     launch_build_moments(tw, n, xs, ys, zs, st);
     check(cudaMemcpyAsync(perm[L], tw.perm, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st),

@@ -215,6 +215,7 @@ int nbody_tree_force(nbody_tree* t, nbody_particles* p, float theta, float softe
     w.spill = t->spill; w.spill_cap = t->spill_cap; w.inter = t->inter; w.work = t->work;
     w.counters = t->counters;
     w.status = t->tw.status; w.targets_per_lane = t->tw.group_max / 32;
+    w.walk_mode = nb::kDefaultWalkMode;
     nb::launch_walk(w, 0);
     nb::finish("launchForceKernel");
     t->throw_status("launchForceKernel");

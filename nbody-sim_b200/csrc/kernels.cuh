@@ -66,6 +66,11 @@ struct TreeWork {
   uint32_t* group_flag = nullptr;
   int* n_groups = nullptr;
   int group_max = 32;     // bodies per target group (32 x targets per lane)
+  // Octree nodes with <= prune_max bodies get no child records (0: every
+  // node down to single bodies).  The walk and the neighbour search open a
+  // node of <= leaf_max bodies straight into its bodies, so a tree built with
+  // prune_max = leaf_max gives them the same results with fewer records.
+  int prune_max = 0;
 };
 
 void tree_alloc(TreeWork& w, int cap);
@@ -129,6 +134,9 @@ size_t scan_tmp_words(int n);
 void scan_exclusive_u32(uint32_t* data, int n, uint32_t* tmp, cudaStream_t s);
 
 // ------------------------------------------------------------------ walk
+// Walk variant used unless a caller picks one (walk.cu lists the variants).
+constexpr int kDefaultWalkMode = 1;
+
 struct WalkArgs {
   const float4* com;
   const int4* info;

@@ -110,6 +110,7 @@ OutputPipe::OutputPipe(int nn, int leaf_max_) : n(nn), leaf_max(leaf_max_) {
   check(cudaStreamCreateWithFlags(&os, cudaStreamNonBlocking), "output stream");
   tree_alloc(tw, n);
   tw.group_max = 32;
+  tw.prune_max = leaf_max;
   parent = dalloc<int>(n, "output parent");
   labels = dalloc<int>(n, "output labels");
   sizes = dalloc<int>(n, "output sizes");

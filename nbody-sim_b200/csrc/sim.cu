@@ -510,7 +510,7 @@ struct SimImpl : SimBase {
     n = nn;
     if (p.leaf_max <= 0) p.leaf_max = 8;
     if (p.targets_per_lane != 2) p.targets_per_lane = 1;
-    if (p.walk_mode < 0 || p.walk_mode > 2) p.walk_mode = 0;
+    if (p.walk_mode < 0 || p.walk_mode > 2) p.walk_mode = kDefaultWalkMode;
     nbody_config c;
     nbody_config_defaults(&c);
     c.perturber_enabled = p.perturber_enabled;
@@ -609,6 +609,7 @@ struct SimImpl : SimBase {
     check(cudaGetLastError(), "k_permute launch");
     cur = 1 - cur;
     mark(NBODY_PHASE_TREE);
+    tw.prune_max = p.leaf_max;
     launch_build_topology(tw, n, st);
     if (kIsF64<R>)
       launch_build_moments(tw, n, (const double*)s[cur].v[0], (const double*)s[cur].v[1],
@@ -785,7 +786,7 @@ void nbody_sim_params_from_config(const nbody_config* cfg, nbody_sim_params* out
   out->state_precision = NBODY_STATE_F32;
   out->leaf_max = 8;
   out->targets_per_lane = 1;
-  out->walk_mode = 0;
+  out->walk_mode = nb::kDefaultWalkMode;
 }
 
 int nbody_sim_create(const nbody_sim_params* p, int n, nbody_sim** out) {
@@ -1061,7 +1062,7 @@ struct EnsembleImpl : EnsembleBase {
     p = prm;
     if (p.leaf_max <= 0) p.leaf_max = 8;
     if (p.targets_per_lane != 2) p.targets_per_lane = 1;
-    if (p.walk_mode < 0 || p.walk_mode > 2) p.walk_mode = 0;
+    if (p.walk_mode < 0 || p.walk_mode > 2) p.walk_mode = kDefaultWalkMode;
     D = nd;
     while ((1 << disk_bits) < D) ++disk_bits;
     off.assign(D + 1, 0);
@@ -1237,6 +1238,7 @@ struct EnsembleImpl : EnsembleBase {
     k_permute<R><<<stream_grid(n), kThreads, 0, st>>>(tw.perm, a, b, n, tw.body4);
     check(cudaGetLastError(), "k_permute launch");
     cur = 1 - cur;
+    tw.prune_max = p.leaf_max;
     launch_karras<uint64_t>(tw, keys64, n, key_bits, st);
     if (kIsF64<R>)
       launch_octree<uint64_t>(tw, keys64, n, disk_bits, D, geoms, group_disk,
@@ -1376,7 +1378,8 @@ struct EnsembleImpl : EnsembleBase {
     auto apply = [&](int k) {
       p.targets_per_lane = cand[3 * k] == 2 ? 2 : 1;
       p.leaf_max = std::max(1, cand[3 * k + 1]);
-      p.walk_mode = (cand[3 * k + 2] >= 0 && cand[3 * k + 2] <= 2) ? cand[3 * k + 2] : 0;
+      p.walk_mode = (cand[3 * k + 2] >= 0 && cand[3 * k + 2] <= 2) ? cand[3 * k + 2]
+                                                                : kDefaultWalkMode;
       tw.group_max = 32 * p.targets_per_lane;
     };
     upload_perturbers(steps_done, 1);  // the forces of the current time

@@ -353,7 +353,7 @@ __device__ __forceinline__ void classify(int n, int disk_bits, const int* __rest
 }
 
 __global__ void __launch_bounds__(kThreads)
-k_mark(int n, int gmax, int disk_bits, const int* __restrict__ left,
+k_mark(int n, int gmax, int prune, int disk_bits, const int* __restrict__ left,
        const int* __restrict__ right, const int* __restrict__ parent,
        const int* __restrict__ lo, const int* __restrict__ hi,
        const uint8_t* __restrict__ prefix, uint8_t* __restrict__ nch, uint32_t* __restrict__ off,
@@ -364,12 +364,12 @@ k_mark(int n, int gmax, int disk_bits, const int* __restrict__ left,
   int lb, lp, p;
   bool top;
   classify(n, disk_bits, parent, prefix, b, lb, lp, top, p);
+  const int c = bin_count(lo, hi, n, b);
   int cnt = 0;
-  if (top && b < n - 1 && lb < 10)
+  if (top && b < n - 1 && lb < 10 && c > prune)
     cnt = for_each_oct_child(left, right, prefix, n, disk_bits, b, lb, [](int, int) {});
   nch[b] = (uint8_t)cnt;
   off[b] = (uint32_t)cnt;
-  const int c = bin_count(lo, hi, n, b);
   const int pc = (p < 0 || lp < 0) ? 0x7fffffff : bin_count(lo, hi, n, p);
   gflag[b] = (lb >= 0 && c <= gmax && pc > gmax) ? 1u : 0u;
 }
@@ -663,9 +663,9 @@ void launch_octree(TreeWork& w, const K* keys, int n, int disk_bits, int n_roots
   }
   const int nb = 2 * n - 1;
   const int gmax = w.group_max;
-  k_mark<<<grid_for(nb), kThreads, 0, s>>>(n, gmax, disk_bits, w.bin_left, w.bin_right,
-                                           w.bin_parent, w.bin_lo, w.bin_hi, w.bin_prefix,
-                                           w.oct_nch, w.oct_off, w.group_flag);
+  k_mark<<<grid_for(nb), kThreads, 0, s>>>(n, gmax, w.prune_max, disk_bits, w.bin_left,
+                                           w.bin_right, w.bin_parent, w.bin_lo, w.bin_hi,
+                                           w.bin_prefix, w.oct_nch, w.oct_off, w.group_flag);
   scan_exclusive_u32(w.oct_off, nb, w.scan_tmp, s);
   scan_exclusive_u32(w.group_flag, nb, w.scan_tmp, s);
   const int ntiles = n / kTileM + 1;
