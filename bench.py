@@ -55,6 +55,9 @@ def parse():
     ap.add_argument("--leaf-max", type=int, default=8)
     ap.add_argument("--walk-mode", type=int, default=None, choices=[0, 1, 2],
                     help="force-walk variant (nbody_sim_params.walk_mode); default: the engine's")
+    ap.add_argument("--group-span", type=int, default=None,
+                    help="target groups from maximal nodes of <= span x 32 bodies "
+                         "(nbody_sim_params.group_span)")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-flush", action="store_true")
@@ -243,6 +246,8 @@ def run_ours(args, ws, rank, local):
                         leaf_max=args.leaf_max)
     if args.walk_mode is not None:
         prm.walk_mode = args.walk_mode
+    if args.group_span is not None:
+        prm.group_span = args.group_span
     stream = torch.cuda.current_stream()
     sim = nb.Sim(prm, n)
     sim.set_stream(stream.cuda_stream)
@@ -371,6 +376,8 @@ def run_ensemble(args, ws, rank, local):
     mine = wl.partition_disks([d["n"] for d in specs_all], ws)[rank]
     specs = [specs_all[k] for k in mine]
     prm = wl.c4_params(nb)
+    if args.group_span is not None:
+        prm.group_span = args.group_span
     st, m = wl.ensemble_state(nb, specs)
     n = len(m)
     n_all = sum(d["n"] for d in specs_all)

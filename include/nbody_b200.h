@@ -288,6 +288,14 @@ typedef struct nbody_sim_params {
                                 64 registers.  Same forces to the walk's
                                 approximation level; speed depends on the
                                 disk (2 suits many small compact disks). */
+  int group_span;            /* walk target groups: maximal tree nodes of
+                                <= group_span x 32 x targets_per_lane
+                                bodies cut into equal runs of <= 32 x
+                                targets_per_lane; 1 .. 64.  Larger spans
+                                fill the warps better and give each group
+                                a larger box.  <= 0: automatic (8 for a
+                                simulation of >= 2^19 bodies, else 1; 1
+                                for an ensemble).                          */
 } nbody_sim_params;
 
 /* Parameters of src/main.cu:58-73 from a Config (r_coll = factor * radius). */

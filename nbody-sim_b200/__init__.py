@@ -121,7 +121,8 @@ class nbody_sim_params(C.Structure):
                 ("gas_drag_rate", C.c_float), ("perturber_enabled", C.c_int),
                 ("perturber_mass_mjup", C.c_float), ("perturber_radius_au", C.c_float),
                 ("perturber_phase0", C.c_float), ("state_precision", C.c_int),
-                ("leaf_max", C.c_int), ("targets_per_lane", C.c_int), ("walk_mode", C.c_int)]
+                ("leaf_max", C.c_int), ("targets_per_lane", C.c_int), ("walk_mode", C.c_int),
+                ("group_span", C.c_int)]
 
 
 NBODY_PHASES = 6
@@ -596,6 +597,8 @@ class OutputWriter:
 # ------------------------------------------------------------- engine
 # the engine's default walk variant (nbody_sim_params.walk_mode; vote, 64 registers)
 WALK_MODE_DEFAULT = 1
+# walk target groups (nbody_sim_params.group_span): 0 lets the engine choose
+GROUP_SPAN_DEFAULT = 0
 
 
 def sim_params(cfg: nbody_config | None = None, **kw) -> nbody_sim_params:
@@ -606,6 +609,7 @@ def sim_params(cfg: nbody_config | None = None, **kw) -> nbody_sim_params:
         p.dt, p.theta, p.softening, p.star_mass, p.leaf_max = 0.01, 0.5, 0.01, 1.0, 8
         p.targets_per_lane = 1
         p.walk_mode = WALK_MODE_DEFAULT
+        p.group_span = GROUP_SPAN_DEFAULT
     for k, v in kw.items():
         setattr(p, k, v)
     return p

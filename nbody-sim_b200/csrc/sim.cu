@@ -511,6 +511,8 @@ struct SimImpl : SimBase {
     if (p.leaf_max <= 0) p.leaf_max = 8;
     if (p.targets_per_lane != 2) p.targets_per_lane = 1;
     if (p.walk_mode < 0 || p.walk_mode > 2) p.walk_mode = kDefaultWalkMode;
+    if (p.group_span <= 0) p.group_span = (n >= kGroupSpanMinBodies) ? kDefaultGroupSpan : 1;
+    if (p.group_span > 64) p.group_span = 64;
     nbody_config c;
     nbody_config_defaults(&c);
     c.perturber_enabled = p.perturber_enabled;
@@ -521,6 +523,7 @@ struct SimImpl : SimBase {
     nbody_perturber_make(&c, &pert);
     common_alloc();
     tw.group_max = 32 * p.targets_per_lane;
+    tw.group_span = p.group_span;
     for (int b = 0; b < 2; ++b) {
       for (int k = 0; k < 6; ++k) s[b].v[k] = dalloc<R>(n, "state");
       s[b].m = dalloc<float>(n, "mass");
@@ -787,6 +790,7 @@ void nbody_sim_params_from_config(const nbody_config* cfg, nbody_sim_params* out
   out->leaf_max = 8;
   out->targets_per_lane = 1;
   out->walk_mode = nb::kDefaultWalkMode;
+  out->group_span = 0;
 }
 
 int nbody_sim_create(const nbody_sim_params* p, int n, nbody_sim** out) {
@@ -1063,6 +1067,8 @@ struct EnsembleImpl : EnsembleBase {
     if (p.leaf_max <= 0) p.leaf_max = 8;
     if (p.targets_per_lane != 2) p.targets_per_lane = 1;
     if (p.walk_mode < 0 || p.walk_mode > 2) p.walk_mode = kDefaultWalkMode;
+    if (p.group_span <= 0) p.group_span = 1;  // small compact disks: keep every group
+    if (p.group_span > 64) p.group_span = 64;
     D = nd;
     while ((1 << disk_bits) < D) ++disk_bits;
     off.assign(D + 1, 0);
@@ -1083,6 +1089,7 @@ struct EnsembleImpl : EnsembleBase {
     own_stream = true;
     tree_alloc(tw, n);
     tw.group_max = 32 * p.targets_per_lane;
+    tw.group_span = p.group_span;
     keys64 = dalloc<uint64_t>(n, "keys64");
     keys64_alt = dalloc<uint64_t>(n, "keys64_alt");
     for (int b = 0; b < 2; ++b) {

@@ -334,12 +334,15 @@ __device__ __forceinline__ int for_each_oct_child(const int* __restrict__ left,
   return k;
 }
 
-// Per binary node: its octree child count (tops only) and whether it is a
-// target group -- a maximal node with <= gmax bodies.  Groups partition the
-// bodies into contiguous key ranges whose bodies share a Morton prefix, so a
-// group never straddles a jump of the space-filling curve (a fixed run of 32
-// consecutive bodies can: its box then spans most of the domain and its walk
-// degenerates to O(N) work on one warp).
+// Per binary node: its octree child count (tops only) and how many target
+// groups it holds -- a maximal node with <= gspan bodies is cut into the
+// fewest equal runs of <= gmax.  Groups partition the bodies into contiguous
+// key ranges inside one node's cell, so a group never straddles a jump of
+// the space-filling curve (a fixed run of 32 consecutive bodies can: its box
+// then spans most of the domain and its walk degenerates to O(N) work on one
+// warp).  gspan = gmax gives the maximal nodes of <= gmax bodies themselves;
+// gspan = 2 gmax fills the warps better (a node of 40 bodies is two runs of
+// 20, not a binary split such as 5 + 30 + 5) at the price of larger boxes.
 // A node is an octree node ("top") when it starts a deeper level than its
 // parent; a disk's root is a top whose parent spans several disks (or node 0
 // of a single disk).  Groups never span disks.
@@ -353,7 +356,7 @@ __device__ __forceinline__ void classify(int n, int disk_bits, const int* __rest
 }
 
 __global__ void __launch_bounds__(kThreads)
-k_mark(int n, int gmax, int prune, int disk_bits, const int* __restrict__ left,
+k_mark(int n, int gmax, int gspan, int prune, int disk_bits, const int* __restrict__ left,
        const int* __restrict__ right, const int* __restrict__ parent,
        const int* __restrict__ lo, const int* __restrict__ hi,
        const uint8_t* __restrict__ prefix, uint8_t* __restrict__ nch, uint32_t* __restrict__ off,
@@ -371,7 +374,7 @@ k_mark(int n, int gmax, int prune, int disk_bits, const int* __restrict__ left,
   nch[b] = (uint8_t)cnt;
   off[b] = (uint32_t)cnt;
   const int pc = (p < 0 || lp < 0) ? 0x7fffffff : bin_count(lo, hi, n, p);
-  gflag[b] = (lb >= 0 && c <= gmax && pc > gmax) ? 1u : 0u;
+  gflag[b] = (lb >= 0 && c <= gspan && pc > gspan) ? (uint32_t)((c + gmax - 1) / gmax) : 0u;
 }
 
 __device__ __forceinline__ uint32_t compact3(uint32_t v) {
@@ -385,7 +388,7 @@ __device__ __forceinline__ uint32_t compact3(uint32_t v) {
 
 template <typename K>
 struct EmitArgs {
-  int n, gmax, disk_bits, n_roots;
+  int n, gmax, gspan, disk_bits, n_roots;
   const int *left, *right, *parent, *lo, *hi;
   const uint8_t* prefix;
   const K* keys;
@@ -488,14 +491,21 @@ __global__ void __launch_bounds__(kThreads) k_emit(const EmitArgs<K> a) {
   if (!in) return;
   const int c = bin_count(a.lo, a.hi, a.n, b);
   const int pc = (p < 0 || lp < 0) ? 0x7fffffff : bin_count(a.lo, a.hi, a.n, p);
-  const bool g = lb >= 0 && c <= a.gmax && pc > a.gmax;
-  if (g) {
-    a.groups[a.goff[b]] = make_int2(first, c);
-    if (a.group_disk) a.group_disk[a.goff[b]] = key_disk(a.keys[first]);
+  const bool g = lb >= 0 && c <= a.gspan && pc > a.gspan;
+  const int ng = g ? (c + a.gmax - 1) / a.gmax : 0;
+  if (g) {  // ng runs of c / ng or c / ng + 1 consecutive bodies
+    const int q = c / ng, r = c % ng;
+    const int disk = a.group_disk ? key_disk(a.keys[first]) : 0;
+    for (int j = 0, s = first; j < ng; ++j) {
+      const int sz = q + (j < r ? 1 : 0);
+      a.groups[a.goff[b] + j] = make_int2(s, sz);
+      if (a.group_disk) a.group_disk[a.goff[b] + j] = disk;
+      s += sz;
+    }
   }
   if (b == nb - 1) {
     *a.n_nodes = a.n_roots + (int)(a.off[b] + (uint32_t)k);
-    *a.n_groups = (int)a.goff[b] + (g ? 1 : 0);
+    *a.n_groups = (int)a.goff[b] + ng;
   }
 }
 
@@ -663,7 +673,8 @@ void launch_octree(TreeWork& w, const K* keys, int n, int disk_bits, int n_roots
   }
   const int nb = 2 * n - 1;
   const int gmax = w.group_max;
-  k_mark<<<grid_for(nb), kThreads, 0, s>>>(n, gmax, w.prune_max, disk_bits, w.bin_left,
+  const int gspan = gmax * std::max(1, w.group_span);
+  k_mark<<<grid_for(nb), kThreads, 0, s>>>(n, gmax, gspan, w.prune_max, disk_bits, w.bin_left,
                                            w.bin_right, w.bin_parent, w.bin_lo, w.bin_hi,
                                            w.bin_prefix, w.oct_nch, w.oct_off, w.group_flag);
   scan_exclusive_u32(w.oct_off, nb, w.scan_tmp, s);
@@ -673,7 +684,7 @@ void launch_octree(TreeWork& w, const K* keys, int n, int disk_bits, int n_roots
   double4* tpre = w.mom_tiles + (ntiles + 1);
   k_moment_tiles<<<ntiles, kThreads, 0, s>>>(w.body4, xd, yd, zd, n, w.mom_ploc, tile_sum);
   k_tile_scan<<<1, 32, 0, s>>>(tile_sum, ntiles, tpre);
-  EmitArgs<K> a{n, gmax, disk_bits, n_roots, w.bin_left, w.bin_right, w.bin_parent, w.bin_lo,
+  EmitArgs<K> a{n, gmax, gspan, disk_bits, n_roots, w.bin_left, w.bin_right, w.bin_parent, w.bin_lo,
                 w.bin_hi, w.bin_prefix, keys, w.oct_nch, w.oct_off, w.group_flag, w.body4,
                 w.mom_ploc, tpre, geoms, w.oct, w.groups, group_disk, w.n_nodes, w.n_groups};
   k_emit<K><<<grid_for(nb), kThreads, 0, s>>>(a);

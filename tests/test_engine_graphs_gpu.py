@@ -60,3 +60,35 @@ def test_walk_modes_agree(nb, cuda):
     assert acc["i0"] == acc["i1"] and acc["i2"] > acc["i0"]
     rel = np.linalg.norm(acc[0] - acc[2], axis=1) / np.linalg.norm(acc[2], axis=1)
     assert np.median(rel) < 5e-2
+
+
+def test_group_span_keeps_the_error_and_fills_the_warps(nb, cuda):
+    """Target groups cut from larger nodes (group_span 8) against the maximal
+    nodes of <= 32 bodies (group_span 1): fewer, fuller groups; the walk's
+    self-gravity error against the FP64 direct sum stays at the same level
+    (a larger group box only makes the acceptance test stricter)."""
+    import torch
+    n = 30000
+    st = disk(nb, n, 0.3, 30.0, seed=4, m=1e-9)
+    tg = np.sort(np.random.default_rng(1).choice(n, 512, replace=False))
+    x64 = [torch.from_numpy(st[k].astype(np.float32).astype(np.float64)).cuda()
+           for k in ("x", "y", "z")]
+    m32 = torch.from_numpy(np.asarray(st["m"], np.float32)).cuda()
+    dx, dy, dz, _ = nb.direct_f64(*x64, m32, 5e-4, targets=torch.from_numpy(tg.astype(np.int32)).cuda())
+    ref = np.stack([dx.cpu().numpy(), dy.cpu().numpy(), dz.cpu().numpy()], 1)
+    res = {}
+    for span in (1, 8):
+        prm = nb.sim_params(dt=0.002, theta=0.5, softening=5e-4, star_mass=0.0, r_coll=0.0,
+                            gas_drag_rate=0.0, group_span=span)
+        sim = nb.Sim(prm, n)
+        sim.set_state(st["x"], st["y"], st["z"], st["vx"], st["vy"], st["vz"], st["m"])
+        g = sim.get_state(accel=True)
+        a = np.stack([g["ax"][tg], g["ay"][tg], g["az"][tg]], 1).astype(np.float64)
+        s = sim.stats()
+        sim.close()
+        assert s.status == 0
+        err = np.linalg.norm(a - ref, axis=1) / np.linalg.norm(ref, axis=1)
+        res[span] = (np.median(err), s.walk_groups)
+    assert res[8][1] < 0.9 * res[1][1], res
+    assert n / res[8][1] <= 32
+    assert res[8][0] < 1.05 * res[1][0], res
