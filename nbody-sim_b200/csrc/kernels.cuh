@@ -142,7 +142,7 @@ void scan_exclusive_u32(uint32_t* data, int n, uint32_t* tmp, cudaStream_t s);
 constexpr int kDefaultWalkMode = 1;
 // Target groups cut from maximal nodes of <= 8 x 32 bodies (TreeWork::
 // group_span): at N = 2^20 warps hold 29 targets on average instead of 22
-// and the walk takes 0.545 ms instead of 0.595 ms.  Below ~2^19 bodies the
+// and the walk takes 0.49 ms instead of 0.55 ms.  Below ~2^19 bodies the
 // fewer groups no longer fill the GPU's warp slots (N = 65536: walk 0.074 ->
 // 0.093 ms, collisions 0.033 -> 0.060 ms), so the automatic choice keeps
 // span 1 there.

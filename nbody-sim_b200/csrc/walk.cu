@@ -33,8 +33,8 @@ constexpr int kWalkWarps = 4;
 // Walk modes (WalkArgs::walk_mode), a trade-off that depends on the disk:
 //   0: acceptance vote, 5 resident blocks per SM (up to 96 registers);
 //   1: acceptance vote, 8 blocks per SM (64 registers) -- the default: at
-//      N = 2^20 over r in [0.3, 30] AU 0.60 ms per walk, against 0.62 ms for
-//      mode 0 and 1.14 ms for mode 2;
+//      N = 2^20 over r in [0.3, 30] AU (groups of span 8) 0.49 ms per walk,
+//      against 0.53 ms for mode 0; 6, 7 or 10 blocks per SM gain nothing;
 //   2: no vote, 8 blocks per SM -- the fastest on small compact disks (the
 //      64-disk ensemble), where the vote rarely pays and occupancy matters.
 template <int kMode>
