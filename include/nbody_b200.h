@@ -200,7 +200,7 @@ int nbody_fof(nbody_tree* t, const float* x, const float* y, const float* z, int
  *
  * All scratch (sort buffers, tree, union-find arrays, a bounded stack-spill
  * area) lives in one statically sized device array inside libnbody_b200.so,
- * NBODY_FOF_NOALLOC_SCRATCH_BYTES bytes (12.5 MiB), which every GPU that
+ * NBODY_FOF_NOALLOC_SCRATCH_BYTES bytes (12.6 MiB), which every GPU that
  * loads the library holds until the process exits.  n is limited to
  * NBODY_FOF_NOALLOC_MAX_N bodies; larger n returns NBODY_ERR_ARG with a
  * message naming the limit.  Inputs and outputs are as for nbody_fof
@@ -215,7 +215,7 @@ int nbody_fof(nbody_tree* t, const float* x, const float* y, const float* z, int
  * per-thread mode) race on the scratch and must be serialised by the caller.
  * The function calls no cudaMalloc, cudaFree or allocating library routine. */
 #define NBODY_FOF_NOALLOC_MAX_N 32768
-#define NBODY_FOF_NOALLOC_SCRATCH_BYTES 13110784
+#define NBODY_FOF_NOALLOC_SCRATCH_BYTES 13176320
 int nbody_fof_noalloc(const float* x, const float* y, const float* z, int n, float link_length,
                       int* labels, uint16_t* agg_size, int* n_groups);
 

@@ -53,6 +53,7 @@ struct TreeWork {
   double4* mom_tiles = nullptr;
   // octree layout
   uint8_t* oct_nch = nullptr;
+  uint8_t* oct_cidx = nullptr;  // a child record's index among its siblings
   uint32_t* oct_off = nullptr;
   uint32_t* scan_tmp = nullptr;
   OctNodes oct;
@@ -136,6 +137,9 @@ void radix_sort_pairs(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt,
                       uint32_t* counts, int n, int bits, cudaStream_t s, int* status = nullptr);
 size_t scan_tmp_words(int n);
 void scan_exclusive_u32(uint32_t* data, int n, uint32_t* tmp, cudaStream_t s);
+// Words of TreeWork::scan_tmp the octree build uses for nb binary nodes
+// (one 64-bit count sum per tile of 256 nodes).
+size_t octree_scan_words(int nb);
 
 // ------------------------------------------------------------------ walk
 // Walk variant used unless a caller picks one (walk.cu lists the variants).

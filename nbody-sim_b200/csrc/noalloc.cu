@@ -25,7 +25,7 @@ constexpr size_t kAlign = 256;
 constexpr size_t al(size_t b) { return (b + kAlign - 1) / kAlign * kAlign; }
 constexpr size_t kNb = 2 * (size_t)kMaxN;
 constexpr size_t kCountWords = 4096;  // >= 3077 words the 32-bit-key sort of kMaxN uses
-constexpr size_t kScanWords = 4096;   // >= scan_tmp_words(2 kMaxN) = 17
+constexpr size_t kScanWords = 4096;   // >= octree_scan_words(2 kMaxN - 1) = 512
 constexpr size_t kMomTiles = 2 * ((size_t)kMaxN / kMomentTile + 2) + 8;
 
 constexpr size_t kScratchBytes =
@@ -37,9 +37,9 @@ constexpr size_t kScratchBytes =
     al(sizeof(uint8_t) * kMaxN) +               // bin_prefix
     al(sizeof(double4) * (kMaxN + 1)) +         // moment prefix sums
     al(sizeof(double4) * kMomTiles) +           // moment tile sums / prefixes
-    al(sizeof(uint8_t) * kNb) +                 // oct_nch
+    2 * al(sizeof(uint8_t) * kNb) +             // oct_nch, oct_cidx
     2 * al(sizeof(uint32_t) * kNb) +            // oct_off, group_flag
-    al(sizeof(uint32_t) * kScanWords) +         // scan partials
+    al(sizeof(uint32_t) * kScanWords) +         // octree tile sums
     4 * al(sizeof(float4) * kNb) +              // octree com, info, box_lo, box_hi
     al(sizeof(unsigned long long) * 6) +        // bbox
     al(sizeof(TreeGeom)) +                      // root geometry
@@ -97,6 +97,8 @@ extern "C" int nbody_fof_noalloc(const float* x, const float* y, const float* z,
                          "; use nbody_fof");
     *n_groups = 0;
     if (n == 0) return NBODY_OK;
+    if (nb::octree_scan_words(2 * n - 1) > nb::kScanWords)
+      throw nb::CudaError("nbody_fof_noalloc: octree tile-sum scratch too small");
     nb::Carve c{nb::scratch_for_current_device()};
     nb::TreeWork w;
     w.cap = nb::kMaxN;
@@ -115,6 +117,7 @@ extern "C" int nbody_fof_noalloc(const float* x, const float* y, const float* z,
     w.mom_ploc = c.take<double4>(nb::kMaxN + 1);
     w.mom_tiles = c.take<double4>(nb::kMomTiles);
     w.oct_nch = c.take<uint8_t>(nb::kNb);
+    w.oct_cidx = c.take<uint8_t>(nb::kNb);
     w.oct_off = c.take<uint32_t>(nb::kNb);
     w.group_flag = c.take<uint32_t>(nb::kNb);
     w.scan_tmp = c.take<uint32_t>(nb::kScanWords);

@@ -181,7 +181,9 @@ __device__ __forceinline__ int delta(const K* __restrict__ keys, int n, int i, i
 
 // key_bits: the low bits of K the keys use (30 Morton bits, plus the disk
 // index above them for an ensemble).  prefix[] stores the common prefix in
-// those bits, key_bits for runs of equal keys.
+// those bits, key_bits for runs of equal keys.  (Staging the block's keys
+// and a halo in shared memory made this kernel slower at N = 2^20: 35 -> 39
+// us; the searches are not what bounds it.)
 template <typename K>
 __global__ void __launch_bounds__(kThreads)
 k_karras(const K* __restrict__ keys, int n, int key_bits, int* __restrict__ left,
@@ -226,19 +228,32 @@ k_karras(const K* __restrict__ keys, int n, int key_bits, int* __restrict__ left
 // two differences of partial sums no larger than the node's own tiles, so
 // cancellation stays at the level of a tile (~1e-13 relative) rather than of
 // the whole disk.  Fixed tiling: the sums are the same on every run.
-constexpr int kTileM = kMomentTile;  // 256 threads x 8 bodies
-constexpr int kPerThr = kTileM / kThreads;
+constexpr int kMomThreads = 1024;
+constexpr int kTileM = kMomentTile;  // 1024 threads x 2 bodies
+constexpr int kPerThr = kTileM / kMomThreads;
 
 __device__ __forceinline__ double4 d4shfl_up(double4 v, int o) {
   return make_double4(__shfl_up_sync(kFull, v.x, o), __shfl_up_sync(kFull, v.y, o),
                       __shfl_up_sync(kFull, v.z, o), __shfl_up_sync(kFull, v.w, o));
 }
 
-__global__ void __launch_bounds__(kThreads)
+__device__ __forceinline__ double4 d4warp_incl_scan(double4 v, int lane) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const double4 t = d4shfl_up(v, o);
+    if (lane >= o) v = d4add(v, t);
+  }
+  return v;
+}
+
+// Large blocks with two bodies per thread keep the registers low and the
+// loads and stores nearly contiguous (8 bodies per thread needed 93
+// registers and ran 513 blocks of 256 threads at 21% warp occupancy).
+__global__ void __launch_bounds__(kMomThreads)
 k_moment_tiles(const float4* __restrict__ body4, const double* __restrict__ xd,
                const double* __restrict__ yd, const double* __restrict__ zd, int n,
                double4* __restrict__ ploc, double4* __restrict__ tile_sum) {
-  __shared__ double4 s_w[kThreads / 32];
+  __shared__ double4 s_w[kMomThreads / 32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const long long base = (long long)blockIdx.x * kTileM + (long long)tid * kPerThr;
   double4 v[kPerThr];
@@ -256,47 +271,59 @@ k_moment_tiles(const float4* __restrict__ body4, const double* __restrict__ xd,
     }
     sum = d4add(sum, v[k]);
   }
-  double4 inc = sum;  // warp inclusive scan of the per-thread sums
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    double4 t = d4shfl_up(inc, o);
-    if (lane >= o) inc = d4add(inc, t);
-  }
+  const double4 inc = d4warp_incl_scan(sum, lane);
   if (lane == 31) s_w[warp] = inc;
   __syncthreads();
-  double4 run = d4sub(inc, sum);
-  for (int w = 0; w < warp; ++w) run = d4add(run, s_w[w]);
+  if (warp == 0) {  // exclusive prefix of the warp sums
+    const double4 x = s_w[lane];
+    const double4 y = d4warp_incl_scan(x, lane);
+    __syncwarp();
+    s_w[lane] = d4sub(y, x);
+  }
+  __syncthreads();
+  double4 run = d4add(s_w[warp], d4sub(inc, sum));
 #pragma unroll
   for (int k = 0; k < kPerThr; ++k) {
     const long long i = base + k;
     if (i <= n) ploc[i] = run;  // index n gets the tile's local prefix at n
     run = d4add(run, v[k]);
   }
-  if (tid == kThreads - 1) tile_sum[blockIdx.x] = run;
+  if (tid == kMomThreads - 1) tile_sum[blockIdx.x] = run;
 }
 
-// Exclusive scan of the tile sums into tpre[0..ntiles] (one warp).
-__global__ void k_tile_scan(const double4* __restrict__ tile_sum, int ntiles,
-                            double4* __restrict__ tpre) {
-  const int lane = threadIdx.x;
-  const int per = (ntiles + 31) / 32;
-  const int lo = lane * per, hi = min(ntiles, lo + per);
-  double4 sum = make_double4(0, 0, 0, 0);
-  for (int t = lo; t < hi; ++t) sum = d4add(sum, tile_sum[t]);
-  double4 inc = sum;
+// Exclusive scan of the tile sums into tpre[0..ntiles] (one block of 1024
+// threads, chunks of 1024 tiles, a fixed order of additions).
+__global__ void __launch_bounds__(1024) k_tile_scan(const double4* __restrict__ tile_sum,
+                                                    int ntiles, double4* __restrict__ tpre) {
+  __shared__ double4 s_w[32];
+  __shared__ double4 s_carry;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) s_carry = make_double4(0, 0, 0, 0);
+  for (int c0 = 0; c0 < ntiles; c0 += 1024) {
+    const int t = c0 + tid;
+    const double4 x = (t < ntiles) ? tile_sum[t] : make_double4(0, 0, 0, 0);
+    double4 inc = x;
 #pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    double4 t = d4shfl_up(inc, o);
-    if (lane >= o) inc = d4add(inc, t);
+    for (int o = 1; o < 32; o <<= 1) {
+      const double4 q = d4shfl_up(inc, o);
+      if (lane >= o) inc = d4add(inc, q);
+    }
+    if (lane == 31) s_w[warp] = inc;
+    __syncthreads();
+    double4 run = s_carry;
+    for (int w = 0; w < warp; ++w) run = d4add(run, s_w[w]);
+    run = d4add(run, d4sub(inc, x));
+    if (t < ntiles) tpre[t] = run;
+    if (t == ntiles - 1) tpre[ntiles] = d4add(run, x);
+    __syncthreads();
+    if (tid == 0) {
+      double4 c = s_carry;
+      for (int w = 0; w < 32; ++w) c = d4add(c, s_w[w]);
+      s_carry = c;
+    }
+    __syncthreads();
   }
-  double4 run = d4sub(inc, sum);
-  for (int t = lo; t < hi; ++t) {
-    tpre[t] = run;
-    run = d4add(run, tile_sum[t]);
-  }
-  if (lane == 31) tpre[ntiles] = inc;
 }
-
 
 // ---------------------------------------------------------- octree layout
 // Octree level of binary node b: leaves and equal-key runs are level 10;
@@ -355,26 +382,177 @@ __device__ __forceinline__ void classify(int n, int disk_bits, const int* __rest
   top = lb >= 0 && (p < 0 || lb > lp);
 }
 
-__global__ void __launch_bounds__(kThreads)
-k_mark(int n, int gmax, int gspan, int prune, int disk_bits, const int* __restrict__ left,
-       const int* __restrict__ right, const int* __restrict__ parent,
-       const int* __restrict__ lo, const int* __restrict__ hi,
-       const uint8_t* __restrict__ prefix, uint8_t* __restrict__ nch, uint32_t* __restrict__ off,
-       uint32_t* __restrict__ gflag) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  const int nb = 2 * n - 1;
+// ------------------------------------------------- octree slots + groups
+// Three passes over the binary nodes, none of which waits on another block:
+//   k_mark   counts each octree node's children (tops with more than `prune`
+//            bodies) and each group node's runs, tells every child its
+//            octree parent and its index among the siblings, and reduces
+//            both counts per tile;
+//   k_tiles  scans the tile sums (one block);
+//   k_apply  scans the counts within each tile, adds the tile prefix, stores
+//            each node's first child slot and writes the group runs.
+// k_emit then writes every record from the node's own data at its slot:
+// n_roots + off[parent] + index, or the disk index for a disk's root.
+// The two counts travel packed in one 64-bit word: children << 31 | runs.
+constexpr int kMarkTile = kThreads;
+constexpr uint8_t kNchTop = 0x80;   // nch[b]: b is an octree node
+constexpr uint8_t kNchRoot = 0x40;  // nch[b]: b is a disk's root
+constexpr uint8_t kNchCount = 0x0f; // nch[b]: its child records (<= 8)
+
+__device__ __forceinline__ unsigned long long pack_counts(uint32_t children, uint32_t runs) {
+  return ((unsigned long long)children << 31) | runs;
+}
+
+template <typename K>
+struct MarkArgs {
+  int n, gmax, gspan, prune, disk_bits;
+  const int *left, *right, *parent, *lo, *hi;
+  const uint8_t* prefix;
+  uint8_t* nch;                // child count | kNchTop | kNchRoot
+  uint32_t* off;               // k_mark: children | runs << 4; k_apply: first child slot - n_roots
+  int* opar;                   // octree parent of each child record (-1 on entry)
+  uint8_t* cidx;               // index of a child record among its siblings
+  unsigned long long* tile_sum;
+};
+
+__device__ __forceinline__ unsigned long long block_sum_u64(unsigned long long v,
+                                                            unsigned long long* s_w) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  if (lane == 0) s_w[warp] = v;
+  __syncthreads();
+  unsigned long long t = 0;
+#pragma unroll
+  for (int w = 0; w < kThreads / 32; ++w) t += s_w[w];
+  return t;
+}
+
+template <typename K>
+__global__ void __launch_bounds__(kThreads) k_mark(const MarkArgs<K> a) {
+  __shared__ unsigned long long s_w[kThreads / 32];
+  const int n = a.n, nb = 2 * n - 1;
+  const int b = blockIdx.x * kMarkTile + threadIdx.x;
+  uint32_t nchild = 0, runs = 0;
+  if (b < nb) {
+    int lb, lp, p;
+    bool top;
+    classify(n, a.disk_bits, a.parent, a.prefix, b, lb, lp, top, p);
+    const int c = bin_count(a.lo, a.hi, n, b);
+    if (top && b < n - 1 && lb < 10 && c > a.prune)
+      nchild = (uint32_t)for_each_oct_child(a.left, a.right, a.prefix, n, a.disk_bits, b, lb,
+                                            [&](int ch, int i) {
+                                              a.opar[ch] = b;
+                                              a.cidx[ch] = (uint8_t)i;
+                                            });
+    const int pc = (p < 0 || lp < 0) ? 0x7fffffff : bin_count(a.lo, a.hi, n, p);
+    if (lb >= 0 && c <= a.gspan && pc > a.gspan) runs = (uint32_t)((c + a.gmax - 1) / a.gmax);
+    const bool root = top && (p < 0 || lp < 0);
+    a.nch[b] = (uint8_t)nchild | (top ? kNchTop : 0) | (root ? kNchRoot : 0);
+    a.off[b] = nchild | (runs << 4);
+  }
+  const unsigned long long t = block_sum_u64(pack_counts(nchild, runs), s_w);
+  if (threadIdx.x == 0) a.tile_sum[blockIdx.x] = t;
+}
+
+// Exclusive scan of the tile sums in place (one block; integer sums; each
+// thread loads 8 sums at once).
+__global__ void __launch_bounds__(1024) k_tiles(unsigned long long* __restrict__ v, int m) {
+  constexpr int kPer = 8;
+  __shared__ unsigned long long s_w[32];
+  __shared__ unsigned long long s_carry;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) s_carry = 0;
+  for (int c0 = 0; c0 < m; c0 += 1024 * kPer) {
+    unsigned long long x[kPer], sum = 0;
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+      const int i = c0 + tid * kPer + k;
+      x[k] = (i < m) ? v[i] : 0ull;
+      sum += x[k];
+    }
+    unsigned long long inc = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long q = __shfl_up_sync(kFull, inc, o);
+      if (lane >= o) inc += q;
+    }
+    if (lane == 31) s_w[warp] = inc;
+    __syncthreads();
+    unsigned long long run = s_carry + inc - sum;
+    for (int w = 0; w < warp; ++w) run += s_w[w];
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+      const int i = c0 + tid * kPer + k;
+      if (i < m) v[i] = run;
+      run += x[k];
+    }
+    __syncthreads();
+    if (tid == 0) {
+      unsigned long long c = s_carry;
+      for (int w = 0; w < 32; ++w) c += s_w[w];
+      s_carry = c;
+    }
+    __syncthreads();
+  }
+}
+
+// Disk index of a key (the bits above the 30 Morton bits).
+template <typename K>
+__device__ __forceinline__ int key_disk(K k) { return (int)(k >> 30); }
+
+template <typename K>
+struct ApplyArgs {
+  int n, n_roots;
+  const int *lo, *hi;
+  const K* keys;
+  uint32_t* off;
+  const unsigned long long* tile_pre;
+  int2* groups;
+  int* group_disk;  // optional: disk of each group
+  int* n_nodes;
+  int* n_groups;
+};
+
+template <typename K>
+__global__ void __launch_bounds__(kThreads) k_apply(const ApplyArgs<K> a) {
+  __shared__ unsigned long long s_w[kThreads / 32];
+  const int n = a.n, nb = 2 * n - 1;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int b = blockIdx.x * kMarkTile + tid;
+  const uint32_t v = (b < nb) ? a.off[b] : 0u;
+  const uint32_t nchild = v & 15u, runs = v >> 4;
+  const unsigned long long mine = pack_counts(nchild, runs);
+  unsigned long long inc = mine;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned long long q = __shfl_up_sync(kFull, inc, o);
+    if (lane >= o) inc += q;
+  }
+  if (lane == 31) s_w[warp] = inc;
+  __syncthreads();
+  unsigned long long ex = a.tile_pre[blockIdx.x] + inc - mine;
+  for (int w = 0; w < warp; ++w) ex += s_w[w];
   if (b >= nb) return;
-  int lb, lp, p;
-  bool top;
-  classify(n, disk_bits, parent, prefix, b, lb, lp, top, p);
-  const int c = bin_count(lo, hi, n, b);
-  int cnt = 0;
-  if (top && b < n - 1 && lb < 10 && c > prune)
-    cnt = for_each_oct_child(left, right, prefix, n, disk_bits, b, lb, [](int, int) {});
-  nch[b] = (uint8_t)cnt;
-  off[b] = (uint32_t)cnt;
-  const int pc = (p < 0 || lp < 0) ? 0x7fffffff : bin_count(lo, hi, n, p);
-  gflag[b] = (lb >= 0 && c <= gspan && pc > gspan) ? (uint32_t)((c + gmax - 1) / gmax) : 0u;
+  const uint32_t first = (uint32_t)(ex >> 31);
+  const uint32_t goff = (uint32_t)(ex & 0x7fffffffull);
+  a.off[b] = first;
+  if (runs > 0) {  // runs of c / runs or c / runs + 1 consecutive bodies
+    const int lo = (b >= n - 1) ? b - (n - 1) : a.lo[b];
+    const int c = (b >= n - 1) ? 1 : a.hi[b] - lo + 1;
+    const int ng = (int)runs, q = c / ng, r = c % ng;
+    const int disk = a.group_disk ? key_disk(a.keys[lo]) : 0;
+    for (int j = 0, s = lo; j < ng; ++j) {
+      const int sz = q + (j < r ? 1 : 0);
+      a.groups[goff + j] = make_int2(s, sz);
+      if (a.group_disk) a.group_disk[goff + j] = disk;
+      s += sz;
+    }
+  }
+  if (b == nb - 1) {
+    *a.n_nodes = a.n_roots + (int)(first + nchild);
+    *a.n_groups = (int)(goff + runs);
+  }
 }
 
 __device__ __forceinline__ uint32_t compact3(uint32_t v) {
@@ -388,27 +566,20 @@ __device__ __forceinline__ uint32_t compact3(uint32_t v) {
 
 template <typename K>
 struct EmitArgs {
-  int n, gmax, gspan, disk_bits, n_roots;
-  const int *left, *right, *parent, *lo, *hi;
+  int n, disk_bits, n_roots;
+  const int *lo, *hi;
   const uint8_t* prefix;
   const K* keys;
   const uint8_t* nch;
   const uint32_t* off;
-  const uint32_t* goff;
+  const int* opar;
+  const uint8_t* cidx;
   const float4* body4;
   const double4* ploc;
   const double4* tpre;
   const TreeGeom* geom;
   OctNodes oct;
-  int2* groups;
-  int* group_disk;  // optional: disk of each group
-  int* n_nodes;
-  int* n_groups;
 };
-
-// Disk index of a key (the bits above the 30 Morton bits).
-template <typename K>
-__device__ __forceinline__ int key_disk(K k) { return (int)(k >> 30); }
 
 // Writes the octree record of binary node c into slot f.
 template <typename K>
@@ -445,7 +616,7 @@ __device__ void write_node(const EmitArgs<K>& a, int c, int f) {
     ctr[k] = fl + 0.5f * fs;
   }
   const float4 com = com_of(s, ctr[0], ctr[1], ctr[2]);
-  const int k = a.nch[c];
+  const int k = a.nch[c] & kNchCount;
   a.oct.com[f] = com;
   a.oct.info[f] = make_int4(k > 0 ? a.n_roots + (int)a.off[c] : -1, lo, ((hi - lo + 1) << 4) | k,
                             __float_as_int(ldexpf(rhs, -L)));
@@ -453,60 +624,24 @@ __device__ void write_node(const EmitArgs<K>& a, int c, int f) {
   a.oct.box_hi[f] = make_float4(bhi[0], bhi[1], bhi[2], 0.f);
 }
 
-// Every top node owns a block of contiguous slots (n_roots + off[b] ...) for
-// its octree children; slots 0 .. n_roots-1 hold the roots (one per disk,
-// slot = disk index).  A warp gathers the
-// (child, slot) pairs of its 32 binary nodes in shared memory and then writes
-// the records one per lane, so the up-to-8 records of one parent do not
-// serialise on a single thread.  Target groups are written at their scanned
-// offsets.
-constexpr int kEmitWarps = kThreads / 32;
-
+// Every octree node with a record writes it: a disk's root at slot = disk
+// index, a child at n_roots + off[parent] + its sibling index.
 template <typename K>
 __global__ void __launch_bounds__(kThreads) k_emit(const EmitArgs<K> a) {
-  __shared__ int2 s_job[kEmitWarps][32 * 8 + 1];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
   const int nb = 2 * a.n - 1;
-  const bool in = b < nb;
-  int lb = -1, lp = -1, p = -1;
-  bool top = false;
-  if (in) classify(a.n, a.disk_bits, a.parent, a.prefix, b, lb, lp, top, p);
-  const int k = in ? a.nch[b] : 0;
-  const bool disk_root = top && (p < 0 || lp < 0);
-  const int first = (b >= a.n - 1) ? b - (a.n - 1) : (in ? a.lo[b] : 0);
-  const int extra = disk_root ? 1 : 0;
-  const int incl = warp_incl_scan(k + extra, lane);
-  const int total = __shfl_sync(kFull, incl, 31);
-  int pos = incl - k - extra;
-  int2* job = s_job[warp];
-  if (extra) job[pos++] = make_int2(b, key_disk(a.keys[first]));  // slot = disk index
-  if (k > 0) {
-    const int base = a.n_roots + (int)a.off[b];
-    for_each_oct_child(a.left, a.right, a.prefix, a.n, a.disk_bits, b, lb,
-                       [&](int c, int i) { job[pos + i] = make_int2(c, base + i); });
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  const uint8_t h = a.nch[b];
+  if (!(h & kNchTop)) return;
+  int f;
+  if (h & kNchRoot) {
+    f = key_disk(a.keys[(b >= a.n - 1) ? b - (a.n - 1) : a.lo[b]]);
+  } else {
+    const int P = a.opar[b];
+    if (P < 0) return;  // under a node the walk opens as bodies: no record
+    f = a.n_roots + (int)a.off[P] + a.cidx[b];
   }
-  __syncwarp();
-  for (int j = lane; j < total; j += 32) write_node(a, job[j].x, job[j].y);
-  if (!in) return;
-  const int c = bin_count(a.lo, a.hi, a.n, b);
-  const int pc = (p < 0 || lp < 0) ? 0x7fffffff : bin_count(a.lo, a.hi, a.n, p);
-  const bool g = lb >= 0 && c <= a.gspan && pc > a.gspan;
-  const int ng = g ? (c + a.gmax - 1) / a.gmax : 0;
-  if (g) {  // ng runs of c / ng or c / ng + 1 consecutive bodies
-    const int q = c / ng, r = c % ng;
-    const int disk = a.group_disk ? key_disk(a.keys[first]) : 0;
-    for (int j = 0, s = first; j < ng; ++j) {
-      const int sz = q + (j < r ? 1 : 0);
-      a.groups[a.goff[b] + j] = make_int2(s, sz);
-      if (a.group_disk) a.group_disk[a.goff[b] + j] = disk;
-      s += sz;
-    }
-  }
-  if (b == nb - 1) {
-    *a.n_nodes = a.n_roots + (int)(a.off[b] + (uint32_t)k);
-    *a.n_groups = (int)a.goff[b] + ng;
-  }
+  write_node(a, b, f);
 }
 
 // N == 1: the root is the single body and the only group.
@@ -554,8 +689,9 @@ void tree_alloc(TreeWork& w, int cap) {
   w.mom_ploc = dalloc<double4>(n + 1, "moment prefix");
   w.mom_tiles = dalloc<double4>(2 * ((n + 1) / kTileM + 2), "moment tiles");
   w.oct_nch = dalloc<uint8_t>(nb, "oct_nch");
+  w.oct_cidx = dalloc<uint8_t>(nb, "oct_cidx");
   w.oct_off = dalloc<uint32_t>(nb, "oct_off");
-  w.scan_tmp = dalloc<uint32_t>(scan_tmp_words((int)nb), "scan_tmp");
+  w.scan_tmp = dalloc<uint32_t>(octree_scan_words((int)nb), "octree tile sums");
   w.oct.com = dalloc<float4>(nb, "oct com");
   w.oct.info = dalloc<int4>(nb, "oct info");
   w.oct.box_lo = dalloc<float4>(nb, "oct box_lo");
@@ -574,7 +710,7 @@ void tree_alloc(TreeWork& w, int cap) {
 void tree_free(TreeWork& w) {
   void* ptrs[] = {w.keys, w.perm, w.keys_alt, w.perm_alt, w.counts, w.body4, w.bin_left,
                   w.bin_right, w.bin_parent, w.bin_lo, w.bin_hi, w.bin_prefix, w.mom_ploc,
-                  w.mom_tiles, w.oct_nch, w.oct_off, w.scan_tmp, w.oct.com, w.oct.info, w.oct.box_lo, w.oct.box_hi, w.bbox_enc,
+                  w.mom_tiles, w.oct_nch, w.oct_cidx, w.oct_off, w.scan_tmp, w.oct.com, w.oct.info, w.oct.box_lo, w.oct.box_hi, w.bbox_enc,
                   w.geom, w.n_nodes, w.status, w.groups, w.group_flag, w.n_groups};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -674,19 +810,24 @@ void launch_octree(TreeWork& w, const K* keys, int n, int disk_bits, int n_roots
   const int nb = 2 * n - 1;
   const int gmax = w.group_max;
   const int gspan = gmax * std::max(1, w.group_span);
-  k_mark<<<grid_for(nb), kThreads, 0, s>>>(n, gmax, gspan, w.prune_max, disk_bits, w.bin_left,
-                                           w.bin_right, w.bin_parent, w.bin_lo, w.bin_hi,
-                                           w.bin_prefix, w.oct_nch, w.oct_off, w.group_flag);
-  scan_exclusive_u32(w.oct_off, nb, w.scan_tmp, s);
-  scan_exclusive_u32(w.group_flag, nb, w.scan_tmp, s);
   const int ntiles = n / kTileM + 1;
   double4* tile_sum = w.mom_tiles;
   double4* tpre = w.mom_tiles + (ntiles + 1);
-  k_moment_tiles<<<ntiles, kThreads, 0, s>>>(w.body4, xd, yd, zd, n, w.mom_ploc, tile_sum);
-  k_tile_scan<<<1, 32, 0, s>>>(tile_sum, ntiles, tpre);
-  EmitArgs<K> a{n, gmax, gspan, disk_bits, n_roots, w.bin_left, w.bin_right, w.bin_parent, w.bin_lo,
-                w.bin_hi, w.bin_prefix, keys, w.oct_nch, w.oct_off, w.group_flag, w.body4,
-                w.mom_ploc, tpre, geoms, w.oct, w.groups, group_disk, w.n_nodes, w.n_groups};
+  k_moment_tiles<<<ntiles, kMomThreads, 0, s>>>(w.body4, xd, yd, zd, n, w.mom_ploc, tile_sum);
+  k_tile_scan<<<1, 1024, 0, s>>>(tile_sum, ntiles, tpre);
+  int* opar = (int*)w.group_flag;
+  unsigned long long* tsum = (unsigned long long*)w.scan_tmp;
+  const int mtiles = div_up(nb, kMarkTile);
+  check(cudaMemsetAsync(opar, 0xff, sizeof(int) * (size_t)nb, s), "octree parent reset");
+  MarkArgs<K> m{n, gmax, gspan, w.prune_max, disk_bits, w.bin_left, w.bin_right, w.bin_parent,
+                w.bin_lo, w.bin_hi, w.bin_prefix, w.oct_nch, w.oct_off, opar, w.oct_cidx, tsum};
+  k_mark<K><<<mtiles, kMarkTile, 0, s>>>(m);
+  k_tiles<<<1, 1024, 0, s>>>(tsum, mtiles);
+  ApplyArgs<K> ap{n, n_roots, w.bin_lo, w.bin_hi, keys, w.oct_off, tsum, w.groups, group_disk,
+                  w.n_nodes, w.n_groups};
+  k_apply<K><<<mtiles, kMarkTile, 0, s>>>(ap);
+  EmitArgs<K> a{n, disk_bits, n_roots, w.bin_lo, w.bin_hi, w.bin_prefix, keys, w.oct_nch,
+                w.oct_off, opar, w.oct_cidx, w.body4, w.mom_ploc, tpre, geoms, w.oct};
   k_emit<K><<<grid_for(nb), kThreads, 0, s>>>(a);
   check(cudaGetLastError(), "octree launch");
 }
@@ -700,10 +841,12 @@ void launch_moment_prefix(TreeWork& w, int n, const double* xd, const double* yd
                           const double* zd, cudaStream_t s) {
   if (n < 1) return;
   const int ntiles = n / kTileM + 1;
-  k_moment_tiles<<<ntiles, kThreads, 0, s>>>(w.body4, xd, yd, zd, n, w.mom_ploc, w.mom_tiles);
-  k_tile_scan<<<1, 32, 0, s>>>(w.mom_tiles, ntiles, moment_tile_prefix(w, n));
+  k_moment_tiles<<<ntiles, kMomThreads, 0, s>>>(w.body4, xd, yd, zd, n, w.mom_ploc, w.mom_tiles);
+  k_tile_scan<<<1, 1024, 0, s>>>(w.mom_tiles, ntiles, moment_tile_prefix(w, n));
   check(cudaGetLastError(), "moment prefix launch");
 }
+
+size_t octree_scan_words(int nb) { return 2 * (size_t)div_up(nb, kMarkTile); }
 
 double4* moment_tile_prefix(TreeWork& w, int n) { return w.mom_tiles + (n / kTileM + 2); }
 
