@@ -46,11 +46,18 @@ constexpr int kList = 64;
 
 struct WarpSmem {
   float4 lst[kList];
+  float4 ext[6];  // the group's targets of least / greatest x, y, z (vote prefilter)
   int stk[kStk];
   int sc[32];
   int slo[32];
   int sc_body[32];  // recording walks: body index of each leaf-body entry
 };
+
+// Squared distance in one fixed rounding, so that the vote and its
+// prefilter test a target identically.
+__device__ __forceinline__ float dist2(float dx, float dy, float dz) {
+  return fmaf(dx, dx, fmaf(dy, dy, __fmul_rn(dz, dz)));
+}
 
 // All lanes evaluate sources lst[0..cnt) for their kT targets; every source
 // is one shared-memory broadcast that feeds kT interaction chains.
@@ -172,6 +179,26 @@ __global__ void __launch_bounds__(kWalkWarps * 32, walk_min_blocks<kMode>())
     gx0 = warp_min(gx0); gx1 = warp_max(gx1);
     gy0 = warp_min(gy0); gy1 = warp_max(gy1);
     gz0 = warp_min(gz0); gz1 = warp_max(gz1);
+    if (walk_vote<kMode>()) {
+      // a target that attains each extreme (invalid lanes hold target 0)
+      const float ev[6] = {gx0, gx1, gy0, gy1, gz0, gz1};
+#pragma unroll
+      for (int e = 0; e < 6; ++e) {
+        int ts = -1;
+#pragma unroll
+        for (int t = kT - 1; t >= 0; --t) {
+          const float cv = (e < 2) ? me[t].x : (e < 4) ? me[t].y : me[t].z;
+          if (cv == ev[e]) ts = t;
+        }
+        const unsigned m = __ballot_sync(kFull, ts >= 0);
+        if (m == 0u) {  // non-finite positions: a point that rejects nothing
+          if (lane == 0) w.ext[e] = make_float4(INFINITY, INFINITY, INFINITY, 0.f);
+        } else if (lane == __ffs(m) - 1) {
+          w.ext[e] = (ts <= 0) ? me[0] : me[kT - 1];
+        }
+      }
+      __syncwarp();
+    }
 
     // The tree sum starts from zero: adding ~10^3 terms into an accumulator
     // that already holds the star pull (10^3-10^5 times larger) would round
@@ -247,7 +274,22 @@ __global__ void __launch_bounds__(kWalkWarps * 32, walk_min_blocks<kMode>())
       // opens 11% fewer interactions and makes the walk 25% faster, at
       // unchanged force error.
       if (walk_vote<kMode>()) {
-        unsigned cand = __ballot_sync(kFull, act >= 2 && d2 > 0.f && h2 < a.theta2 * far2);
+        // Necessary conditions first: the far corner, then the extreme
+        // target on the node's side along each axis must accept it.
+        bool cnd = act >= 2 && d2 > 0.f && h2 < a.theta2 * far2;
+        if (cnd) {
+          const float4 ex = w.ext[c.x > 0.5f * (gx0 + gx1) ? 1 : 0];
+          cnd = h2 < a.theta2 * dist2(c.x - ex.x, c.y - ex.y, c.z - ex.z);
+        }
+        if (cnd) {
+          const float4 ey = w.ext[c.y > 0.5f * (gy0 + gy1) ? 3 : 2];
+          cnd = h2 < a.theta2 * dist2(c.x - ey.x, c.y - ey.y, c.z - ey.z);
+        }
+        if (cnd) {
+          const float4 ez = w.ext[c.z > 0.5f * (gz0 + gz1) ? 5 : 4];
+          cnd = h2 < a.theta2 * dist2(c.x - ez.x, c.y - ez.y, c.z - ez.z);
+        }
+        unsigned cand = __ballot_sync(kFull, cnd);
         while (cand) {
           const int j = __ffs(cand) - 1;
           cand &= cand - 1;
@@ -256,8 +298,8 @@ __global__ void __launch_bounds__(kWalkWarps * 32, walk_min_blocks<kMode>())
           bool ok = true;
 #pragma unroll
           for (int t = 0; t < kT; ++t) {
-            const float ex = cx - me[t].x, ey = cy - me[t].y, ez = cz - me[t].z;
-            ok = ok && (!valid[t] || hh < a.theta2 * (ex * ex + ey * ey + ez * ez));
+            ok = ok && (!valid[t] || hh < a.theta2 * dist2(cx - me[t].x, cy - me[t].y,
+                                                           cz - me[t].z));
           }
           if (__all_sync(kFull, ok) && lane == j) act = 1;
         }
