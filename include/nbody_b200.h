@@ -215,7 +215,7 @@ int nbody_fof(nbody_tree* t, const float* x, const float* y, const float* z, int
  * per-thread mode) race on the scratch and must be serialised by the caller.
  * The function calls no cudaMalloc, cudaFree or allocating library routine. */
 #define NBODY_FOF_NOALLOC_MAX_N 32768
-#define NBODY_FOF_NOALLOC_SCRATCH_BYTES 13176320
+#define NBODY_FOF_NOALLOC_SCRATCH_BYTES 13241856
 int nbody_fof_noalloc(const float* x, const float* y, const float* z, int n, float link_length,
                       int* labels, uint16_t* agg_size, int* n_groups);
 
@@ -539,6 +539,15 @@ int nbody_adjoint_stats_get(nbody_adjoint* a, nbody_adjoint_stats* out);
 int nbody_direct_f64(const double* x, const double* y, const double* z, const float* mass, int n,
                      const int* targets, int n_targets, double eps, double* ax, double* ay,
                      double* az, double* phi);
+
+/* Stable LSD radix sort of (key, value) pairs in place on device arrays, by
+ * the low `bits` key bits (1..32 for 32-bit keys, 1..64 for 64-bit): the sort
+ * behind the body order of every octree (launchSortKernel's sort_idx,
+ * src/physics/BHTree.cu:518-525, comes out of it).  Scratch is allocated and
+ * freed per call; synchronous on the legacy stream.  Returns NBODY_ERR_CUDA
+ * if a tile's look-back wait gave up. */
+int nbody_radix_sort_u32(uint32_t* keys, uint32_t* values, int n, int bits);
+int nbody_radix_sort_u64(uint64_t* keys, uint32_t* values, int n, int bits);
 
 /* ------------------------------------------------------ initial disks --- */
 

@@ -254,6 +254,8 @@ SIGNATURES = [
     ("nbody_adjoint_stats_get", C.c_int, [_VP, C.POINTER(nbody_adjoint_stats)]),
     ("nbody_make_disks_device", C.c_int, [_VP, _VP, C.c_int] + [C.c_double] * 5 + [_VP] * 7),
     ("nbody_direct_f64", C.c_int, [_VP] * 4 + [C.c_int, _VP, C.c_int, C.c_double] + [_VP] * 4),
+    ("nbody_radix_sort_u32", C.c_int, [_VP, _VP, C.c_int, C.c_int]),
+    ("nbody_radix_sort_u64", C.c_int, [_VP, _VP, C.c_int, C.c_int]),
     ("nbody_make_disk", C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                   C.c_double, C.c_uint64, _D, _D, _D, _D, _D, _D]),
 ]
@@ -982,6 +984,20 @@ def direct_f64(x, y, z, mass, eps: float, targets=None, want_acc=True, want_phi=
     _check(lib.nbody_direct_f64(p(x), p(y), p(z), p(mass), n, p(targets), nt, eps,
                                 p(ax), p(ay), p(az), p(phi)))
     return ax, ay, az, phi
+
+
+def radix_sort(keys, values, bits: int):
+    """Stable radix sort of (key, value) pairs in place (nbody_radix_sort_u32 /
+    _u64) on CUDA tensors: keys int32 or int64 (read as unsigned), values
+    int32."""
+    import torch
+    n = keys.numel()
+    if values.numel() != n or values.dtype != torch.int32:
+        raise ValueError("radix_sort: values must be int32 and as long as keys")
+    fn = {torch.int32: lib.nbody_radix_sort_u32, torch.int64: lib.nbody_radix_sort_u64}.get(keys.dtype)
+    if fn is None:
+        raise ValueError("radix_sort: keys must be int32 or int64")
+    _check(fn(keys.data_ptr(), values.data_ptr(), n, bits))
 
 
 # --------------------------------------------------------- initial disks

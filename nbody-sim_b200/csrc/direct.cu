@@ -12,6 +12,7 @@
 
 #include "capi_util.h"
 #include "common.cuh"
+#include "kernels.cuh"
 
 namespace nb {
 namespace {
@@ -77,4 +78,49 @@ extern "C" int nbody_direct_f64(const double* x, const double* y, const double* 
     nb::check(cudaGetLastError(), "k_direct launch");
     nb::check(cudaDeviceSynchronize(), "k_direct");
   })
+}
+
+namespace {
+template <typename K>
+int radix_sort_api(K* keys, uint32_t* values, int n, int bits, const char* what) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(n >= 0, std::string(what) + ": negative n");
+    NBODY_REQUIRE(bits >= 1 && bits <= 8 * (int)sizeof(K), std::string(what) + ": bad bit count");
+    if (n <= 1) return NBODY_OK;
+    NBODY_REQUIRE(keys && values, std::string(what) + ": null array");
+    K* ka = nullptr;
+    uint32_t *va = nullptr, *counts = nullptr;
+    int* status = nullptr;
+    auto release = [&]() {
+      cudaFree(ka);
+      cudaFree(va);
+      cudaFree(counts);
+      cudaFree(status);
+    };
+    try {
+      nb::check(cudaMalloc(&ka, sizeof(K) * (size_t)n), "sort scratch");
+      nb::check(cudaMalloc(&va, sizeof(uint32_t) * (size_t)n), "sort scratch");
+      nb::check(cudaMalloc(&counts, sizeof(uint32_t) * nb::radix_sort_count_words(n)),
+                "sort scratch");
+      nb::check(cudaMalloc(&status, sizeof(int)), "sort status");
+      nb::check(cudaMemset(status, 0, sizeof(int)), "sort status");
+      nb::radix_sort_pairs<K>(keys, values, ka, va, counts, n, bits, 0, status);
+      int st = 0;
+      nb::check(cudaMemcpy(&st, status, sizeof(int), cudaMemcpyDeviceToHost), "sort status");
+      if (st) throw nb::CudaError(std::string(what) + ": a look-back wait gave up");
+    } catch (...) {
+      release();
+      throw;
+    }
+    release();
+  })
+}
+}  // namespace
+
+extern "C" int nbody_radix_sort_u32(uint32_t* keys, uint32_t* values, int n, int bits) {
+  return radix_sort_api<uint32_t>(keys, values, n, bits, "nbody_radix_sort_u32");
+}
+
+extern "C" int nbody_radix_sort_u64(uint64_t* keys, uint32_t* values, int n, int bits) {
+  return radix_sort_api<uint64_t>(keys, values, n, bits, "nbody_radix_sort_u64");
 }

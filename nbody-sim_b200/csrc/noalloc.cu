@@ -24,7 +24,7 @@ constexpr size_t kAlign = 256;
 
 constexpr size_t al(size_t b) { return (b + kAlign - 1) / kAlign * kAlign; }
 constexpr size_t kNb = 2 * (size_t)kMaxN;
-constexpr size_t kCountWords = 4096;  // >= 3077 words the 32-bit-key sort of kMaxN uses
+constexpr size_t kCountWords = 20480;  // >= 18441 words the 32-bit-key sort of kMaxN uses
 constexpr size_t kScanWords = 4096;   // >= octree_scan_words(2 kMaxN - 1) = 512
 constexpr size_t kMomTiles = 2 * ((size_t)kMaxN / kMomentTile + 2) + 8;
 
@@ -97,6 +97,8 @@ extern "C" int nbody_fof_noalloc(const float* x, const float* y, const float* z,
                          "; use nbody_fof");
     *n_groups = 0;
     if (n == 0) return NBODY_OK;
+    if (nb::radix_sort_count_words(n) > nb::kCountWords)
+      throw nb::CudaError("nbody_fof_noalloc: sort scratch too small");
     if (nb::octree_scan_words(2 * n - 1) > nb::kScanWords)
       throw nb::CudaError("nbody_fof_noalloc: octree tile-sum scratch too small");
     nb::Carve c{nb::scratch_for_current_device()};

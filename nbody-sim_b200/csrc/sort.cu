@@ -26,13 +26,15 @@ namespace {
 
 constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / kWarp;
-// keys per thread: 16 (uint32 keys, 4096-key tiles) or 8 (uint64, 2048) so
-// the staged tile stays within 48 KB of static shared memory
+// keys per thread: at most 16 (uint32 keys, 4096-key tiles) or 8 (uint64,
+// 2048) so the staged tile stays within 48 KB of static shared memory; fewer
+// (down to 2) when there would be fewer tiles than half the SMs.  Measured
+// step times (CUDA graphs): N = 2^20 is fastest with 16 (0.745 ms; 8: 0.748,
+// 4: 0.761, 2: 0.797), N = 131072 with 8 or 4 (0.221 ms; 16: 0.225).
 template <typename K>
 constexpr int sort_items() { return sizeof(K) == 8 ? 8 : 16; }
-template <typename K>
-constexpr int sort_tile() { return kSortThreads * sort_items<K>(); }
-constexpr int kMinTile = kSortThreads * 8;
+constexpr int kMinItems = 2;
+constexpr int kMinTile = kSortThreads * kMinItems;
 constexpr int kBins = 256;
 
 // Exclusive scan of `total` uint32 in place, one block of 1024 threads.
@@ -128,14 +130,13 @@ __global__ void __launch_bounds__(kBins) k_digit_offsets(uint32_t* __restrict__ 
 
 // One pass: rank a tile, publish, look back, scatter.  ticket and status
 // (ntiles x 256 words) start at zero.
-template <typename K>
+template <typename K, int kItems>
 __global__ void __launch_bounds__(kSortThreads)
 k_onesweep(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
            K* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int n, int shift,
            const uint32_t* __restrict__ digit_base, int* __restrict__ ticket,
            uint32_t* __restrict__ status, int* __restrict__ err) {
-  constexpr int kItems = sort_items<K>();
-  constexpr int kTile = sort_tile<K>();
+  constexpr int kTile = kSortThreads * kItems;
   __shared__ uint32_t s_cnt[kSortWarps][kBins];
   __shared__ K s_keys[kTile];
   __shared__ uint32_t s_vals[kTile];
@@ -319,6 +320,46 @@ k_scan_down(uint32_t* __restrict__ data, int n, const uint32_t* __restrict__ sum
   }
 }
 
+int sort_sm_count() {
+  static int sms = 0;
+  if (sms == 0) {
+    int dev = 0;
+    check(cudaGetDevice(&dev), "cudaGetDevice");
+    check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+  }
+  return sms;
+}
+
+// Keys per thread for n keys: the largest that still gives half as many
+// tiles as SMs.
+template <typename K>
+int pick_items(int n) {
+  const int target = sort_sm_count() / 2;
+  int it = sort_items<K>();
+  while (it > kMinItems && div_up(n, kSortThreads * it) < target) it >>= 1;
+  return it;
+}
+
+template <typename K, int kItems>
+void launch_onesweep(int ntiles, const K* ki, const uint32_t* vi, K* ko, uint32_t* vo, int n,
+                     int shift, const uint32_t* base, int* ticket, uint32_t* st, int* err,
+                     cudaStream_t s) {
+  k_onesweep<K, kItems><<<ntiles, kSortThreads, 0, s>>>(ki, vi, ko, vo, n, shift, base, ticket,
+                                                        st, err);
+}
+
+template <typename K>
+void launch_onesweep_items(int items, int ntiles, const K* ki, const uint32_t* vi, K* ko,
+                           uint32_t* vo, int n, int shift, const uint32_t* base, int* ticket,
+                           uint32_t* st, int* err, cudaStream_t s) {
+  if constexpr (sizeof(K) == 4) {
+    if (items == 16) return launch_onesweep<K, 16>(ntiles, ki, vi, ko, vo, n, shift, base, ticket, st, err, s);
+  }
+  if (items == 8) return launch_onesweep<K, 8>(ntiles, ki, vi, ko, vo, n, shift, base, ticket, st, err, s);
+  if (items == 4) return launch_onesweep<K, 4>(ntiles, ki, vi, ko, vo, n, shift, base, ticket, st, err, s);
+  launch_onesweep<K, 2>(ntiles, ki, vi, ko, vo, n, shift, base, ticket, st, err, s);
+}
+
 }  // namespace
 
 size_t scan_tmp_words(int n);
@@ -326,7 +367,7 @@ size_t scan_tmp_words(int n);
 // Scratch of the sort: per-pass digit offsets (passes x 256), per-pass tile
 // tickets (passes), one word for give-up reports when the caller passes no
 // status word, then the tile status words of one pass (ntiles x 256, cleared
-// before every pass).  Sized for the smaller 64-bit-key tiles.
+// before every pass).  Sized for the smallest tiles.
 size_t radix_sort_count_words(int n) {
   return (size_t)kMaxPasses * kBins + kMaxPasses + 1 + (size_t)kBins * div_up(n, kMinTile);
 }
@@ -335,7 +376,8 @@ template <typename K>
 void radix_sort_pairs(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt,
                       uint32_t* counts, int n, int bits, cudaStream_t s, int* status) {
   if (n <= 1) return;
-  const int ntiles = div_up(n, sort_tile<K>());
+  const int items = pick_items<K>(n);
+  const int ntiles = div_up(n, kSortThreads * items);
   const int passes = (bits + 7) / 8;
   if (passes > kMaxPasses) throw CudaError("radix_sort_pairs: too many key bits");
   uint32_t* hist = counts;                      // passes x 256
@@ -352,8 +394,8 @@ void radix_sort_pairs(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt,
   for (int p = 0; p < passes; ++p) {
     check(cudaMemsetAsync(st, 0, sizeof(uint32_t) * (size_t)ntiles * kBins, s),
           "radix sort status reset");
-    k_onesweep<K><<<ntiles, kSortThreads, 0, s>>>(ki, vi, ko, vo, n, 8 * p,
-                                                  hist + (size_t)p * kBins, tickets + p, st, err);
+    launch_onesweep_items<K>(items, ntiles, ki, vi, ko, vo, n, 8 * p, hist + (size_t)p * kBins,
+                             tickets + p, st, err, s);
     K* t = ki; ki = ko; ko = t;
     uint32_t* u = vi; vi = vo; vo = u;
   }

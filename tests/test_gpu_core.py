@@ -277,3 +277,38 @@ def test_engine_steps_track_the_reference_loop(nb, cuda, port, precision):
         assert d.max() < 2e-3 and np.median(d) < 2e-5, (k, d.max(), np.median(d))
     assert sim.stats().status == 0
     sim.close()
+
+
+# ------------------------------------------------------------ radix sort
+@pytest.mark.parametrize("n", [0, 1, 2, 1000, 131072, 200_000, 900_000, 1_400_000])
+def test_radix_sort_u32_is_a_stable_argsort(nb, cuda, n):
+    """Every tile size the sort picks by n on a 148-SM B200 (2 keys per
+    thread at 1000, 4 at 131072, 8 at 200000, 16 above) against numpy's
+    stable argsort; 30-bit keys with many duplicates."""
+    import torch
+    rng = np.random.default_rng(n)
+    keys = rng.integers(0, 1 << 30, n, dtype=np.uint32)
+    if n > 10:
+        keys[rng.integers(0, n, n // 3)] = keys[0]  # long runs of one key
+    vals = np.arange(n, dtype=np.int32)
+    k = torch.from_numpy(keys.view(np.int32)).cuda()
+    v = torch.from_numpy(vals).cuda()
+    nb.radix_sort(k, v, 30)
+    order = np.argsort(keys, kind="stable")
+    assert np.array_equal(v.cpu().numpy(), order)
+    assert np.array_equal(k.cpu().numpy().view(np.uint32), keys[order])
+
+
+@pytest.mark.parametrize("n", [5000, 700_000])
+def test_radix_sort_u64_ensemble_keys(nb, cuda, n):
+    """Composite ensemble keys (disk index above 30 Morton bits), 36 bits."""
+    import torch
+    rng = np.random.default_rng(7)
+    keys = (rng.integers(0, 64, n, dtype=np.uint64) << np.uint64(30)) | \
+        rng.integers(0, 1 << 30, n, dtype=np.uint64)
+    vals = np.arange(n, dtype=np.int32)
+    k = torch.from_numpy(keys.view(np.int64)).cuda()
+    v = torch.from_numpy(vals).cuda()
+    nb.radix_sort(k, v, 36)
+    order = np.argsort(keys, kind="stable")
+    assert np.array_equal(v.cpu().numpy(), order)
