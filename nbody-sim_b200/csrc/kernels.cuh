@@ -76,10 +76,18 @@ struct TreeWork {
   // bodies, each cut into the fewest equal runs of <= group_max (1: the
   // maximal nodes of <= group_max bodies themselves).
   int group_span = 1;
+  // Optional overlap (launch_tree): the FP64 moment prefix runs on `side`
+  // while the Karras tree and the slot passes run on the caller's stream,
+  // forked and joined by the two events (graph capture turns them into
+  // parallel branches).  Created by tree_enable_overlap; null: one stream.
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
 
 void tree_alloc(TreeWork& w, int cap);
 void tree_free(TreeWork& w);
+// Creates w.side and its events (freed by tree_free).
+void tree_enable_overlap(TreeWork& w);
 
 // bbox of n positions of type T (float or double) into w.bbox_enc (reset first).
 template <typename T>
@@ -98,10 +106,17 @@ void launch_karras(TreeWork& w, const K* keys, int n, int key_bits, cudaStream_t
 // a disk index in the disk_bits above the 30 Morton bits: one root slot per
 // disk (slots 0..n_roots-1), geoms[d] the root cube of disk d, group_disk
 // (optional) receives each group's disk.
+// moments_ready: the moment prefix is already launched (launch_tree on the
+// side stream, joined through w.ev_join before the records are written).
 template <typename K>
 void launch_octree(TreeWork& w, const K* keys, int n, int disk_bits, int n_roots,
                    const TreeGeom* geoms, int* group_disk, const double* xd, const double* yd,
-                   const double* zd, cudaStream_t s);
+                   const double* zd, cudaStream_t s, bool moments_ready = false);
+// launch_karras + launch_octree, with the moment prefix on w.side when set.
+template <typename K>
+void launch_tree(TreeWork& w, const K* keys, int n, int key_bits, int disk_bits, int n_roots,
+                 const TreeGeom* geoms, int* group_disk, const double* xd, const double* yd,
+                 const double* zd, cudaStream_t s);
 // Ensembles: root cube of every disk from its encoded bbox (6 words per
 // disk); bbox accumulators reset for n_disks; composite keys
 // (disk << 30 | Morton) with disk[i] the body's disk.

@@ -522,6 +522,7 @@ struct SimImpl : SimBase {
     c.star_mass_msun = p.star_mass;
     nbody_perturber_make(&c, &pert);
     common_alloc();
+    tree_enable_overlap(tw);
     tw.group_max = 32 * p.targets_per_lane;
     tw.group_span = p.group_span;
     for (int b = 0; b < 2; ++b) {
@@ -608,17 +609,18 @@ struct SimImpl : SimBase {
     radix_sort_pairs(tw.keys, tw.perm, tw.keys_alt, tw.perm_alt, tw.counts, n, 30, st,
                      tw.status);
     mark(NBODY_PHASE_PERMUTE);
-    k_permute<R><<<stream_grid(n), kThreads, 0, st>>>(tw.perm, a, b, n, tw.body4);
+    k_permute<R><<<div_up(n, kThreads), kThreads, 0, st>>>(tw.perm, a, b, n, tw.body4);
     check(cudaGetLastError(), "k_permute launch");
     cur = 1 - cur;
     mark(NBODY_PHASE_TREE);
     tw.prune_max = p.leaf_max;
-    launch_build_topology(tw, n, st);
     if (kIsF64<R>)
-      launch_build_moments(tw, n, (const double*)s[cur].v[0], (const double*)s[cur].v[1],
-                           (const double*)s[cur].v[2], st);
+      launch_tree<uint32_t>(tw, tw.keys, n, 30, 0, 1, tw.geom, nullptr,
+                            (const double*)s[cur].v[0], (const double*)s[cur].v[1],
+                            (const double*)s[cur].v[2], st);
     else
-      launch_build_moments(tw, n, nullptr, nullptr, nullptr, st);
+      launch_tree<uint32_t>(tw, tw.keys, n, 30, 0, 1, tw.geom, nullptr, nullptr, nullptr, nullptr,
+                            st);
     if (p.perturber_enabled && initial) upload_perturber(-1, 1);  // (float)(0) * dt = 0
     check(cudaMemsetAsync(inter, 0, sizeof(unsigned long long), st), "inter reset");
     check(cudaMemsetAsync(counters, 0, 3 * sizeof(unsigned long long), st), "counters reset");
@@ -1088,6 +1090,7 @@ struct EnsembleImpl : EnsembleBase {
     check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "ensemble stream");
     own_stream = true;
     tree_alloc(tw, n);
+    tree_enable_overlap(tw);
     tw.group_max = 32 * p.targets_per_lane;
     tw.group_span = p.group_span;
     keys64 = dalloc<uint64_t>(n, "keys64");
@@ -1242,18 +1245,17 @@ struct EnsembleImpl : EnsembleBase {
     launch_bbox_reset_n(bbox, D, st);
     radix_sort_pairs<uint64_t>(keys64, tw.perm, keys64_alt, tw.perm_alt, tw.counts, n, key_bits,
                                st, tw.status);
-    k_permute<R><<<stream_grid(n), kThreads, 0, st>>>(tw.perm, a, b, n, tw.body4);
+    k_permute<R><<<div_up(n, kThreads), kThreads, 0, st>>>(tw.perm, a, b, n, tw.body4);
     check(cudaGetLastError(), "k_permute launch");
     cur = 1 - cur;
     tw.prune_max = p.leaf_max;
-    launch_karras<uint64_t>(tw, keys64, n, key_bits, st);
     if (kIsF64<R>)
-      launch_octree<uint64_t>(tw, keys64, n, disk_bits, D, geoms, group_disk,
-                              (const double*)s[cur].v[0], (const double*)s[cur].v[1],
-                              (const double*)s[cur].v[2], st);
+      launch_tree<uint64_t>(tw, keys64, n, key_bits, disk_bits, D, geoms, group_disk,
+                            (const double*)s[cur].v[0], (const double*)s[cur].v[1],
+                            (const double*)s[cur].v[2], st);
     else
-      launch_octree<uint64_t>(tw, keys64, n, disk_bits, D, geoms, group_disk, nullptr, nullptr,
-                              nullptr, st);
+      launch_tree<uint64_t>(tw, keys64, n, key_bits, disk_bits, D, geoms, group_disk, nullptr,
+                            nullptr, nullptr, st);
     check(cudaMemsetAsync(inter, 0, sizeof(unsigned long long), st), "inter reset");
     check(cudaMemsetAsync(counters, 0, 3 * sizeof(unsigned long long), st), "counters reset");
     WalkArgs w{};

@@ -714,7 +714,17 @@ void tree_free(TreeWork& w) {
                   w.geom, w.n_nodes, w.status, w.groups, w.group_flag, w.n_groups};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  if (w.side) cudaStreamDestroy(w.side);
+  if (w.ev_fork) cudaEventDestroy(w.ev_fork);
+  if (w.ev_join) cudaEventDestroy(w.ev_join);
   w = TreeWork();
+}
+
+void tree_enable_overlap(TreeWork& w) {
+  if (w.side) return;
+  check(cudaStreamCreateWithFlags(&w.side, cudaStreamNonBlocking), "tree side stream");
+  check(cudaEventCreateWithFlags(&w.ev_fork, cudaEventDisableTiming), "tree fork event");
+  check(cudaEventCreateWithFlags(&w.ev_join, cudaEventDisableTiming), "tree join event");
 }
 
 void launch_bbox_reset(TreeWork& w, cudaStream_t s) {
@@ -799,7 +809,7 @@ void launch_karras(TreeWork& w, const K* keys, int n, int key_bits, cudaStream_t
 template <typename K>
 void launch_octree(TreeWork& w, const K* keys, int n, int disk_bits, int n_roots,
                    const TreeGeom* geoms, int* group_disk, const double* xd, const double* yd,
-                   const double* zd, cudaStream_t s) {
+                   const double* zd, cudaStream_t s, bool moments_ready) {
   if (n < 1) return;
   if (n == 1) {
     k_single<<<1, 1, 0, s>>>(w.body4, geoms, w.oct, w.n_nodes, w.groups, w.n_groups);
@@ -813,8 +823,10 @@ void launch_octree(TreeWork& w, const K* keys, int n, int disk_bits, int n_roots
   const int ntiles = n / kTileM + 1;
   double4* tile_sum = w.mom_tiles;
   double4* tpre = w.mom_tiles + (ntiles + 1);
-  k_moment_tiles<<<ntiles, kMomThreads, 0, s>>>(w.body4, xd, yd, zd, n, w.mom_ploc, tile_sum);
-  k_tile_scan<<<1, 1024, 0, s>>>(tile_sum, ntiles, tpre);
+  if (!moments_ready) {
+    k_moment_tiles<<<ntiles, kMomThreads, 0, s>>>(w.body4, xd, yd, zd, n, w.mom_ploc, tile_sum);
+    k_tile_scan<<<1, 1024, 0, s>>>(tile_sum, ntiles, tpre);
+  }
   int* opar = (int*)w.group_flag;
   unsigned long long* tsum = (unsigned long long*)w.scan_tmp;
   const int mtiles = div_up(nb, kMarkTile);
@@ -828,14 +840,36 @@ void launch_octree(TreeWork& w, const K* keys, int n, int disk_bits, int n_roots
   k_apply<K><<<mtiles, kMarkTile, 0, s>>>(ap);
   EmitArgs<K> a{n, disk_bits, n_roots, w.bin_lo, w.bin_hi, w.bin_prefix, keys, w.oct_nch,
                 w.oct_off, opar, w.oct_cidx, w.body4, w.mom_ploc, tpre, geoms, w.oct};
+  if (moments_ready) check(cudaStreamWaitEvent(s, w.ev_join, 0), "moment join");
   k_emit<K><<<grid_for(nb), kThreads, 0, s>>>(a);
   check(cudaGetLastError(), "octree launch");
+}
+
+template <typename K>
+void launch_tree(TreeWork& w, const K* keys, int n, int key_bits, int disk_bits, int n_roots,
+                 const TreeGeom* geoms, int* group_disk, const double* xd, const double* yd,
+                 const double* zd, cudaStream_t s) {
+  const bool fork = w.side && n >= 2;
+  if (fork) {
+    check(cudaEventRecord(w.ev_fork, s), "tree fork");
+    check(cudaStreamWaitEvent(w.side, w.ev_fork, 0), "tree fork");
+    launch_moment_prefix(w, n, xd, yd, zd, w.side);
+    check(cudaEventRecord(w.ev_join, w.side), "tree join");
+  }
+  launch_karras<K>(w, keys, n, key_bits, s);
+  launch_octree<K>(w, keys, n, disk_bits, n_roots, geoms, group_disk, xd, yd, zd, s, fork);
 }
 
 template void launch_karras<uint64_t>(TreeWork&, const uint64_t*, int, int, cudaStream_t);
 template void launch_octree<uint64_t>(TreeWork&, const uint64_t*, int, int, int,
                                       const TreeGeom*, int*, const double*, const double*,
-                                      const double*, cudaStream_t);
+                                      const double*, cudaStream_t, bool);
+template void launch_tree<uint32_t>(TreeWork&, const uint32_t*, int, int, int, int,
+                                    const TreeGeom*, int*, const double*, const double*,
+                                    const double*, cudaStream_t);
+template void launch_tree<uint64_t>(TreeWork&, const uint64_t*, int, int, int, int,
+                                    const TreeGeom*, int*, const double*, const double*,
+                                    const double*, cudaStream_t);
 
 void launch_moment_prefix(TreeWork& w, int n, const double* xd, const double* yd,
                           const double* zd, cudaStream_t s) {
