@@ -223,6 +223,34 @@ k_unsort(StateArrays<R> st, int n, T* __restrict__ o0, T* __restrict__ o1, T* __
   }
 }
 
+// The caller-order read-back of nbody_sim_step_host in two halves: the
+// positions (final once the last step's permute has run) and the velocities
+// and accelerations (final at the end of the call).
+template <typename R>
+__global__ void __launch_bounds__(kThreads)
+k_unsort_pos(StateArrays<R> st, int n, float* __restrict__ ox, float* __restrict__ oy,
+             float* __restrict__ oz) {
+  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
+       s += (long long)gridDim.x * blockDim.x) {
+    const int o = st.id[s];
+    ox[o] = (float)st.v[0][s]; oy[o] = (float)st.v[1][s]; oz[o] = (float)st.v[2][s];
+  }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kThreads)
+k_unsort_vel_acc(StateArrays<R> st, int n, float* __restrict__ ovx, float* __restrict__ ovy,
+                 float* __restrict__ ovz, const float* __restrict__ ax,
+                 const float* __restrict__ ay, const float* __restrict__ az,
+                 float* __restrict__ oax, float* __restrict__ oay, float* __restrict__ oaz) {
+  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
+       s += (long long)gridDim.x * blockDim.x) {
+    const int o = st.id[s];
+    ovx[o] = (float)st.v[3][s]; ovy[o] = (float)st.v[4][s]; ovz[o] = (float)st.v[5][s];
+    oax[o] = ax[s]; oay[o] = ay[s]; oaz[o] = az[s];
+  }
+}
+
 __global__ void k_scatter_labels(const int* __restrict__ in_l, const uint16_t* __restrict__ in_s,
                                  int n, int* __restrict__ out_l, uint16_t* __restrict__ out_s) {
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -398,6 +426,13 @@ struct SimBase {
   virtual void snapshot(float* const* dst) = 0;
   OutputPipe* pipe = nullptr;
   virtual void load_accel(const float* ax, const float* ay, const float* az) = 0;
+  // Host round trip of nbody_sim_step_host (float state and float arrays).
+  virtual void step_host(float* const* v, float* const* a, const float* mass, int nsteps) = 0;
+  // Recorded after every permute (an external event node inside the step
+  // graphs): from there on the step leaves the positions alone.
+  cudaEvent_t ev_pos = nullptr;
+  cudaStream_t rb_st = nullptr;  // read-back stream of step_host
+  bool capturing = false;
 
   void common_alloc() {
     tree_alloc(tw, n);
@@ -434,6 +469,8 @@ struct SimBase {
   void common_free() {
     drop_graphs();
     if (cap_st) cudaStreamDestroy(cap_st);
+    if (rb_st) cudaStreamDestroy(rb_st);
+    if (ev_pos) cudaEventDestroy(ev_pos);
     if (pipe) {
       delete pipe;
       pipe = nullptr;
@@ -523,6 +560,8 @@ struct SimImpl : SimBase {
     nbody_perturber_make(&c, &pert);
     common_alloc();
     tree_enable_overlap(tw);
+    check(cudaEventCreateWithFlags(&ev_pos, cudaEventDisableTiming), "position event");
+    check(cudaStreamCreateWithFlags(&rb_st, cudaStreamNonBlocking), "read-back stream");
     tw.group_max = 32 * p.targets_per_lane;
     tw.group_span = p.group_span;
     for (int b = 0; b < 2; ++b) {
@@ -611,6 +650,9 @@ struct SimImpl : SimBase {
     mark(NBODY_PHASE_PERMUTE);
     k_permute<R><<<div_up(n, kThreads), kThreads, 0, st>>>(tw.perm, a, b, n, tw.body4);
     check(cudaGetLastError(), "k_permute launch");
+    check(cudaEventRecordWithFlags(ev_pos, st, capturing ? cudaEventRecordExternal
+                                                         : cudaEventRecordDefault),
+          "position event");
     cur = 1 - cur;
     mark(NBODY_PHASE_TREE);
     tw.prune_max = p.leaf_max;
@@ -717,7 +759,9 @@ struct SimImpl : SimBase {
     cudaStream_t user = st;
     st = cap_st;
     check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+    capturing = true;
     one_step(first);
+    capturing = false;
     const cudaError_t ce = cudaStreamEndCapture(st, &graph);
     st = user;
     check(ce, "end capture");
@@ -757,6 +801,48 @@ struct SimImpl : SimBase {
     if (!on_device && !out_stage) out_stage = dalloc<char>(out_stage_bytes(n), "output staging");
     state_out<R>(s[cur], n, ax, ay, az, p.softening, p.star_mass, v, as_double, acc, on_device,
                  out_stage, st);
+  }
+
+  // copyToGPU, nsteps, copyToCPU.  The positions are final once the last
+  // step's permute has run, so their caller-order gather and copy to the host
+  // go out on the read-back stream while the tree, the walk and the closing
+  // kick still run; the velocities and accelerations follow at the end.
+  void step_host(float* const* v, float* const* acc, const float* mass, int nsteps) override {
+    const int steps0 = steps_done;
+    const void* vin[6] = {v[0], v[1], v[2], v[3], v[4], v[5]};
+    set_state(vin, false, mass, false, false);
+    load_accel(acc[0], acc[1], acc[2]);
+    steps_done = steps0;  // the caller's clock continues
+    void* vout[6] = {v[0], v[1], v[2], v[3], v[4], v[5]};
+    if (nsteps <= 0 || !kIsF32<R>) {
+      step(nsteps);
+      get_state(vout, false, acc, false);
+      return;
+    }
+    step(nsteps);
+    if (!out_stage) out_stage = dalloc<char>(out_stage_bytes(n), "output staging");
+    float* stg = (float*)out_stage;  // 9 n floats of the 60 n bytes
+    const size_t nb = sizeof(float) * (size_t)n;
+    check(cudaStreamWaitEvent(rb_st, ev_pos, 0), "read-back wait");
+    k_unsort_pos<R><<<stream_grid(n), kThreads, 0, rb_st>>>(s[cur], n, stg, stg + n,
+                                                            stg + 2 * (size_t)n);
+    check(cudaGetLastError(), "k_unsort_pos launch");
+    for (int k = 0; k < 3; ++k)
+      check(cudaMemcpyAsync(v[k], stg + k * (size_t)n, nb, cudaMemcpyDeviceToHost, rb_st),
+            "position D2H");
+    float* sv = stg + 3 * (size_t)n;
+    k_unsort_vel_acc<R><<<stream_grid(n), kThreads, 0, st>>>(
+        s[cur], n, sv, sv + n, sv + 2 * (size_t)n, ax, ay, az, sv + 3 * (size_t)n,
+        sv + 4 * (size_t)n, sv + 5 * (size_t)n);
+    check(cudaGetLastError(), "k_unsort_vel_acc launch");
+    for (int k = 0; k < 3; ++k)
+      check(cudaMemcpyAsync(v[3 + k], sv + k * (size_t)n, nb, cudaMemcpyDeviceToHost, st),
+            "velocity D2H");
+    for (int k = 0; k < 3; ++k)
+      check(cudaMemcpyAsync(acc[k], sv + (3 + k) * (size_t)n, nb, cudaMemcpyDeviceToHost, st),
+            "accel D2H");
+    check(cudaStreamSynchronize(rb_st), "read-back sync");
+    check(cudaStreamSynchronize(st), "step_host sync");
   }
 };
 
@@ -983,15 +1069,9 @@ int nbody_sim_step_host(nbody_sim* s, float* x, float* y, float* z, float* vx, f
     NBODY_REQUIRE(b->p.state_precision == NBODY_STATE_F32,
                   "nbody_sim_step_host: needs NBODY_STATE_F32");
     NBODY_REQUIRE(nsteps >= 0, "nbody_sim_step_host: negative step count");
-    const int steps0 = b->steps_done;
-    const void* v[6] = {x, y, z, vx, vy, vz};
-    b->set_state(v, false, mass, false, false);  // copyToGPU of ParticleData
-    b->load_accel(ax, ay, az);
-    b->steps_done = steps0;                      // the caller's clock continues
-    b->step(nsteps);
-    void* o[6] = {x, y, z, vx, vy, vz};
+    float* v[6] = {x, y, z, vx, vy, vz};
     float* a[3] = {ax, ay, az};
-    b->get_state(o, false, a, false);            // copyToCPU
+    b->step_host(v, a, mass, nsteps);  // copyToGPU, nsteps, copyToCPU
   })
 }
 

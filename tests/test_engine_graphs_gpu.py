@@ -92,3 +92,35 @@ def test_group_span_keeps_the_error_and_fills_the_warps(nb, cuda):
     assert res[8][1] < 0.9 * res[1][1], res
     assert n / res[8][1] <= 32
     assert res[8][0] < 1.05 * res[1][0], res
+
+
+@pytest.mark.parametrize("graphs", [True, False], ids=["graphs", "plain"])
+def test_step_host_read_back_equals_get_state(nb, cuda, graphs):
+    """nbody_sim_step_host reads the positions back on a second stream while
+    the step finishes; what it returns must be the engine's final state, as
+    get_state reads it afterwards, bit for bit, over two calls in a row (a
+    read-back that did not wait for the step would return old positions)."""
+    n = 7000
+    st = disk(nb, n, 0.5, 5.0, seed=11, m=1e-8)
+    prm = nb.sim_params(dt=0.005, theta=0.5, softening=1e-3, star_mass=1.0,
+                        r_coll=5.0 * nb.particle_physical_radius(1e-8), restitution=0.0,
+                        gas_drag_rate=1e-3, perturber_enabled=1, perturber_mass_mjup=1.0,
+                        perturber_radius_au=5.2)
+    keys = ("x", "y", "z", "vx", "vy", "vz")
+    host = {k: np.ascontiguousarray(st[k], np.float32) for k in keys}
+    m = np.ascontiguousarray(st["m"], np.float32)
+    sim = nb.Sim(prm, n)
+    sim.set_graphs(graphs)
+    sim.set_state(*[host[k] for k in keys], m)
+    g = sim.get_state(accel=True)
+    for k in ("ax", "ay", "az"):
+        host[k] = g[k].copy()
+    for nsteps in (1, 3):
+        before = {k: v.copy() for k, v in host.items()}
+        sim.step_host(host, m, nsteps)
+        got = sim.get_state(accel=True)
+        for k in got:
+            assert np.array_equal(host[k], got[k]), (nsteps, k)
+        assert not np.array_equal(host["x"], before["x"])
+    assert sim.stats().status == 0
+    sim.close()
