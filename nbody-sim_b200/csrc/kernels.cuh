@@ -95,7 +95,8 @@ void launch_bbox(TreeWork& w, const T* x, const T* y, const T* z, int n, cudaStr
 void launch_bbox_reset(TreeWork& w, cudaStream_t s);
 // Morton keys of n positions using w.bbox_enc; writes w.geom, keys, perm = 0..n-1.
 template <typename T>
-void launch_keys(TreeWork& w, const T* x, const T* y, const T* z, int n, cudaStream_t s);
+void launch_keys(TreeWork& w, const T* x, const T* y, const T* z, int n, cudaStream_t s,
+                 uint32_t* hist = nullptr);
 // body4[s] = (x,y,z,m)[perm[s]] for float inputs in caller order.
 void launch_gather_body4(TreeWork& w, const float* x, const float* y, const float* z,
                          const float* m, int n, cudaStream_t s);
@@ -146,10 +147,16 @@ size_t radix_sort_count_words(int n);
 // uint32_t (single disk, 30-bit Morton keys) or uint64_t (ensemble: disk
 // index above the 30 Morton bits).
 // counts: radix_sort_count_words(n) words of scratch; status (optional)
-// receives kStatusSortWait if a look-back wait gave up.
+// receives kStatusSortWait if a look-back wait gave up.  hist_ready: the
+// digit histograms at the start of counts were cleared by radix_sort_prepare
+// and filled by the kernel that wrote the keys (launch_keys with hist).
 template <typename K>
 void radix_sort_pairs(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt,
-                      uint32_t* counts, int n, int bits, cudaStream_t s, int* status = nullptr);
+                      uint32_t* counts, int n, int bits, cudaStream_t s, int* status = nullptr,
+                      bool hist_ready = false);
+// Clears the histograms and tickets at the start of counts; returns the
+// histograms (passes x 256 words) for a key kernel to fill.
+uint32_t* radix_sort_prepare(uint32_t* counts, int bits, cudaStream_t s);
 size_t scan_tmp_words(int n);
 void scan_exclusive_u32(uint32_t* data, int n, uint32_t* tmp, cudaStream_t s);
 // Words of TreeWork::scan_tmp the octree build uses for nb binary nodes
@@ -233,6 +240,11 @@ struct NeighborArgs {
 void launch_collide(const NeighborArgs& a, const float* vx, const float* vy, const float* vz,
                     const uint32_t* vmap, float r_coll, float restitution, float* dvx,
                     float* dvy, float* dvz, cudaStream_t s);
+// The same with velocities in the state's storage type: vtype 0 float,
+// 1 double, 2 hi/lo float pairs (converted to float as they are read).
+void launch_collide_v(const NeighborArgs& a, const void* vx, const void* vy, const void* vz,
+                      int vtype, const uint32_t* vmap, float r_coll, float restitution,
+                      float* dvx, float* dvy, float* dvz, cudaStream_t s);
 // FoF links (Aggregate.cpp:36-42 test) -> union-find over original ids.
 void launch_fof_link(const NeighborArgs& a, const uint32_t* ids, float link_length,
                      int* parent, cudaStream_t s);

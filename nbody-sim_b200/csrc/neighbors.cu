@@ -59,9 +59,10 @@ __device__ void uf_union(int* parent, int a, int b, int* status) {
 }
 
 struct CollideOut {
-  const float* vx;
-  const float* vy;
-  const float* vz;
+  const void* vx;   // velocities in the state's storage type (vtype)
+  const void* vy;
+  const void* vz;
+  int vtype;        // 0 float, 1 double, 2 hi/lo float pairs
   const uint32_t* vmap;
   float rc2;
   float e;
@@ -69,6 +70,15 @@ struct CollideOut {
   float* dvy;
   float* dvz;
 };
+
+// A velocity component as the FP32 impulse uses it: the float value, the
+// double rounded to float, or the hi word of a hi/lo pair (the conversions
+// of the state's float read-out).
+__device__ __forceinline__ float vel(const void* p, int vtype, uint32_t i) {
+  if (vtype == 1) return (float)__ldg((const double*)p + i);
+  if (vtype == 2) return __ldg((const float2*)p + i).x;
+  return __ldg((const float*)p + i);
+}
 
 struct FofOut {
   const uint32_t* ids;
@@ -108,7 +118,9 @@ k_neighbors(const NeighborArgs a, float radius, CollideOut co, FofOut fo) {
     float vix = 0.f, viy = 0.f, viz = 0.f;
     if (kMode == 0 && valid) {
       const uint32_t vi = co.vmap ? co.vmap[s] : (uint32_t)s;
-      vix = co.vx[vi]; viy = co.vy[vi]; viz = co.vz[vi];
+      vix = vel(co.vx, co.vtype, vi);
+      viy = vel(co.vy, co.vtype, vi);
+      viz = vel(co.vz, co.vtype, vi);
     }
     float dvx = 0.f, dvy = 0.f, dvz = 0.f;
     const int my_id = (kMode == 1 && valid) ? (int)fo.ids[s] : 0;
@@ -198,8 +210,9 @@ k_neighbors(const NeighborArgs a, float radius, CollideOut co, FofOut fo) {
                 const uint32_t vj = co.vmap ? co.vmap[j] : (uint32_t)j;
                 float dist = sqrtf(dist2) + 1e-10f;
                 float nx = dx / dist, ny = dy / dist, nz = dz / dist;
-                float dvn = (co.vx[vj] - vix) * nx + (co.vy[vj] - viy) * ny +
-                            (co.vz[vj] - viz) * nz;
+                float dvn = (vel(co.vx, co.vtype, vj) - vix) * nx +
+                            (vel(co.vy, co.vtype, vj) - viy) * ny +
+                            (vel(co.vz, co.vtype, vj) - viz) * nz;
                 if (dvn < 0.f) {
                   float J = -(1.f + co.e) * dvn * 0.5f;
                   dvx += -J * nx; dvy += -J * ny; dvz += -J * nz;
@@ -298,19 +311,25 @@ void launch_nb(const NeighborArgs& a, float radius, const CollideOut& co, const 
 
 }  // namespace
 
+void launch_collide_v(const NeighborArgs& a, const void* vx, const void* vy, const void* vz,
+                      int vtype, const uint32_t* vmap, float r_coll, float restitution,
+                      float* dvx, float* dvy, float* dvz, cudaStream_t s) {
+  CollideOut co{vx, vy, vz, vtype, vmap, r_coll * r_coll, restitution, dvx, dvy, dvz};
+  FofOut fo{nullptr, 0.f, nullptr};
+  launch_nb<0>(a, r_coll, co, fo, s);
+}
+
 void launch_collide(const NeighborArgs& a, const float* vx, const float* vy, const float* vz,
                     const uint32_t* vmap, float r_coll, float restitution, float* dvx,
                     float* dvy, float* dvz, cudaStream_t s) {
-  CollideOut co{vx, vy, vz, vmap, r_coll * r_coll, restitution, dvx, dvy, dvz};
-  FofOut fo{nullptr, 0.f, nullptr};
-  launch_nb<0>(a, r_coll, co, fo, s);
+  launch_collide_v(a, vx, vy, vz, 0, vmap, r_coll, restitution, dvx, dvy, dvz, s);
 }
 
 void launch_fof_link(const NeighborArgs& a, const uint32_t* ids, float link_length, int* parent,
                      cudaStream_t s) {
   if (a.n <= 0) return;
   k_fof_init<<<div_up(a.n, 256), 256, 0, s>>>(parent, a.n);
-  CollideOut co{nullptr, nullptr, nullptr, nullptr, 0.f, 0.f, nullptr, nullptr, nullptr};
+  CollideOut co{nullptr, nullptr, nullptr, 0, nullptr, 0.f, 0.f, nullptr, nullptr, nullptr};
   const float ll2 = link_length * link_length;  // Aggregate.cpp:30
   FofOut fo{ids, ll2, parent};
   launch_nb<1>(a, link_length, co, fo, s);
@@ -334,7 +353,7 @@ void launch_fof_link_capped(const NeighborArgs& a, const uint32_t* ids, float li
                             int* parent, int max_warps, cudaStream_t s) {
   if (a.n <= 0) return;
   k_fof_init<<<div_up(a.n, 256), 256, 0, s>>>(parent, a.n);
-  CollideOut co{nullptr, nullptr, nullptr, nullptr, 0.f, 0.f, nullptr, nullptr, nullptr};
+  CollideOut co{nullptr, nullptr, nullptr, 0, nullptr, 0.f, 0.f, nullptr, nullptr, nullptr};
   const float ll2 = link_length * link_length;  // Aggregate.cpp:30
   FofOut fo{ids, ll2, parent};
   int grid = sm_count() * nb_blocks_per_sm<1>();

@@ -540,7 +540,6 @@ template <typename R>
 struct SimImpl : SimBase {
   StateArrays<R> s[2]{};
   int cur = 0;
-  float* vf = nullptr;  // FP64 mode: float velocities for the collision pass
 
   SimImpl(const nbody_sim_params& prm, int nn) {
     p = prm;
@@ -569,7 +568,6 @@ struct SimImpl : SimBase {
       s[b].m = dalloc<float>(n, "mass");
       s[b].id = dalloc<int>(n, "id");
     }
-    if (!kIsF32<R>) vf = dalloc<float>(3 * (size_t)n, "velocity scratch");
   }
 
   ~SimImpl() override {
@@ -578,7 +576,6 @@ struct SimImpl : SimBase {
       cudaFree(s[b].m);
       cudaFree(s[b].id);
     }
-    if (vf) cudaFree(vf);
     common_free();
   }
 
@@ -643,10 +640,12 @@ struct SimImpl : SimBase {
     StateArrays<R>& a = s[cur];
     StateArrays<R>& b = s[1 - cur];
     mark(NBODY_PHASE_SORT);
-    launch_keys<R>(tw, a.v[0], a.v[1], a.v[2], n, st);
+    // the key kernel also counts the digits of the sort's four passes
+    uint32_t* hist = radix_sort_prepare(tw.counts, 30, st);
+    launch_keys<R>(tw, a.v[0], a.v[1], a.v[2], n, st, hist);
     launch_bbox_reset(tw, st);
     radix_sort_pairs(tw.keys, tw.perm, tw.keys_alt, tw.perm_alt, tw.counts, n, 30, st,
-                     tw.status);
+                     tw.status, true);
     mark(NBODY_PHASE_PERMUTE);
     k_permute<R><<<div_up(n, kThreads), kThreads, 0, st>>>(tw.perm, a, b, n, tw.body4);
     check(cudaGetLastError(), "k_permute launch");
@@ -682,10 +681,10 @@ struct SimImpl : SimBase {
     mark(NBODY_PHASE_WALK);
     launch_walk(w, st);
     mark(NBODY_PHASE_COLLIDE);
-    // keys, bbox reset, 20 sort kernels (4 x upsweep, 3 scan, scatter),
-    // permute, karras, mark, 2 x 3 scan kernels, moment tiles, tile scan,
-    // emit, walk
-    launches += 35;
+    // keys (+ digit histograms), bbox reset, digit offsets, 4 one-sweep
+    // passes, permute, karras, mark, tile scan, apply, moment tiles, moment
+    // tile scan, emit, walk
+    launches += 16;
   }
 
   void collide() {
@@ -695,13 +694,9 @@ struct SimImpl : SimBase {
       launch_collide(na, (const float*)s[cur].v[3], (const float*)s[cur].v[4],
                      (const float*)s[cur].v[5], nullptr, p.r_coll, p.restitution, dvx, dvy, dvz,
                      st);
-    } else {
-      // float copies of the half-step velocities for the FP32 impulse
-      for (int k = 0; k < 3; ++k)
-        k_convert<R, float><<<stream_grid(n), kThreads, 0, st>>>(s[cur].v[3 + k], vf + k * n, n);
-      check(cudaGetLastError(), "velocity convert");
-      launch_collide(na, vf, vf + n, vf + 2 * n, nullptr, p.r_coll, p.restitution, dvx, dvy, dvz,
-                     st);
+    } else {  // the half-step velocities read in their storage type, rounded to float
+      launch_collide_v(na, s[cur].v[3], s[cur].v[4], s[cur].v[5], kIsF64<R> ? 1 : 2, nullptr,
+                       p.r_coll, p.restitution, dvx, dvy, dvz, st);
     }
   }
 
@@ -739,7 +734,7 @@ struct SimImpl : SimBase {
     compute_forces(false);
     if (p.r_coll > 0.f) {
       collide();
-      launches += kIsF32<R> ? 1 : 4;
+      launches += 1;
     }
     if (p.perturber_enabled) {
       k_increment<<<1, 1, 0, st>>>(pert_step);
@@ -1123,7 +1118,7 @@ struct EnsembleImpl : EnsembleBase {
   StateArrays<R> s[2]{};
   int cur = 0;
   float *ax = nullptr, *ay = nullptr, *az = nullptr, *dvx = nullptr, *dvy = nullptr,
-        *dvz = nullptr, *vf = nullptr;
+        *dvz = nullptr;
   TreeGeom* geoms = nullptr;
   unsigned long long* bbox = nullptr;
   int* group_disk = nullptr;
@@ -1183,7 +1178,6 @@ struct EnsembleImpl : EnsembleBase {
     }
     ax = dalloc<float>(n, "ax"); ay = dalloc<float>(n, "ay"); az = dalloc<float>(n, "az");
     dvx = dalloc<float>(n, "dvx"); dvy = dalloc<float>(n, "dvy"); dvz = dalloc<float>(n, "dvz");
-    if (!kIsF32<R>) vf = dalloc<float>(3 * (size_t)n, "velocity scratch");
     geoms = dalloc<TreeGeom>(D, "geoms");
     bbox = dalloc<unsigned long long>(6 * (size_t)D, "bboxes");
     group_disk = dalloc<int>(n, "group disk");
@@ -1207,7 +1201,7 @@ struct EnsembleImpl : EnsembleBase {
       cudaFree(s[b].m); cudaFree(s[b].id); cudaFree(s[b].disk);
     }
     void* ptrs[] = {keys64, keys64_alt, ax,    ay,    az,         dvx,   dvy,
-                    dvz,    vf,         geoms, bbox,  group_disk, d_off, pert_tab,
+                    dvz,    geoms, bbox,  group_disk, d_off, pert_tab,
                     pert_step, spill,   work,  inter, counters,   staging, out_stage};
     for (void* q : ptrs)
       if (q) cudaFree(q);
@@ -1350,9 +1344,10 @@ struct EnsembleImpl : EnsembleBase {
     w.work = work; w.status = tw.status; w.targets_per_lane = tw.group_max / 32;
     w.walk_mode = p.walk_mode;
     launch_walk(w, st);
-    // geoms, keys, bbox reset, 5 per sort pass, permute, karras, mark,
-    // 2 x 3 scan kernels, moment tiles, tile scan, emit, walk
-    launches += 3 + 5 * ((key_bits + 7) / 8) + 3 + 6 + 4;
+    // geoms, keys, bbox reset, digit histogram and offsets, one one-sweep
+    // kernel per pass, permute, karras, mark, tile scan, apply, moment tiles,
+    // moment tile scan, emit, walk
+    launches += 3 + 2 + (key_bits + 7) / 8 + 9;
   }
 
   void collide() {
@@ -1363,14 +1358,10 @@ struct EnsembleImpl : EnsembleBase {
                      (const float*)s[cur].v[5], nullptr, p.r_coll, p.restitution, dvx, dvy, dvz,
                      st);
       launches += 1;
-    } else {
-      // float copies of the half-step velocities for the FP32 impulse
-      for (int k = 0; k < 3; ++k)
-        k_convert<R, float><<<stream_grid(n), kThreads, 0, st>>>(s[cur].v[3 + k], vf + k * n, n);
-      check(cudaGetLastError(), "velocity convert");
-      launch_collide(na, vf, vf + n, vf + 2 * n, nullptr, p.r_coll, p.restitution, dvx, dvy, dvz,
-                     st);
-      launches += 4;
+    } else {  // the half-step velocities read in their storage type, rounded to float
+      launch_collide_v(na, s[cur].v[3], s[cur].v[4], s[cur].v[5], kIsF64<R> ? 1 : 2, nullptr,
+                       p.r_coll, p.restitution, dvx, dvy, dvz, st);
+      launches += 1;
     }
   }
 

@@ -19,6 +19,7 @@
 #include <algorithm>
 
 #include "common.cuh"
+#include "digit_hist.cuh"
 #include "kernels.cuh"
 
 namespace nb {
@@ -35,7 +36,7 @@ template <typename K>
 constexpr int sort_items() { return sizeof(K) == 8 ? 8 : 16; }
 constexpr int kMinItems = 2;
 constexpr int kMinTile = kSortThreads * kMinItems;
-constexpr int kBins = 256;
+constexpr int kBins = kHistBins;
 
 // Exclusive scan of `total` uint32 in place, one block of 1024 threads.
 __global__ void __launch_bounds__(1024) k_scan_inplace(uint32_t* __restrict__ data, int total) {
@@ -81,32 +82,24 @@ constexpr uint32_t kFlagP = 2u << 30;  // inclusive prefix published
 constexpr uint32_t kValMask = (1u << 30) - 1u;
 constexpr uint32_t kFlagMask = ~kValMask;
 constexpr int kSpinLimit = 1 << 20;
-constexpr int kMaxPasses = 8;
+constexpr int kMaxPasses = kHistMaxPasses;
 
 // Digit counts of every pass in one read: hist[p * 256 + d] (zeroed first).
 template <typename K>
 __global__ void __launch_bounds__(kSortThreads)
 k_digit_hist(const K* __restrict__ keys, int n, int passes, uint32_t* __restrict__ hist) {
   __shared__ uint32_t s_h[kMaxPasses][kBins];
-  const int tid = threadIdx.x, lane = tid & 31;
+  const int tid = threadIdx.x;
   for (int i = tid; i < kMaxPasses * kBins; i += kSortThreads) (&s_h[0][0])[i] = 0;
   __syncthreads();
   const long long stride = (long long)gridDim.x * blockDim.x;
   const long long end = (n + 31) / 32 * 32;  // whole warps take part in match_any
   for (long long i = (long long)blockIdx.x * blockDim.x + tid; i < end; i += stride) {
     const bool valid = i < n;
-    const K key = valid ? __ldg(keys + i) : (K)0;
-    for (int p = 0; p < passes; ++p) {
-      const uint32_t d = valid ? (uint32_t)(key >> (8 * p)) & 0xffu : kBins;
-      const unsigned peers = __match_any_sync(kFull, d);
-      if (valid && lane == __ffs(peers) - 1) atomicAdd(&s_h[p][d], (uint32_t)__popc(peers));
-    }
+    hist_add(s_h, valid ? __ldg(keys + i) : (K)0, valid, passes);
   }
   __syncthreads();
-  for (int i = tid; i < passes * kBins; i += kSortThreads) {
-    const uint32_t c = (&s_h[0][0])[i];
-    if (c) atomicAdd(hist + i, c);
-  }
+  hist_flush(s_h, passes, hist);
 }
 
 // Exclusive scan of each pass's 256 digit counts (one block per pass).
@@ -372,9 +365,17 @@ size_t radix_sort_count_words(int n) {
   return (size_t)kMaxPasses * kBins + kMaxPasses + 1 + (size_t)kBins * div_up(n, kMinTile);
 }
 
+uint32_t* radix_sort_prepare(uint32_t* counts, int bits, cudaStream_t s) {
+  const int passes = (bits + 7) / 8;
+  check(cudaMemsetAsync(counts, 0, sizeof(uint32_t) * ((size_t)passes * kBins + passes + 1), s),
+        "radix sort histogram reset");
+  return counts;
+}
+
 template <typename K>
 void radix_sort_pairs(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt,
-                      uint32_t* counts, int n, int bits, cudaStream_t s, int* status) {
+                      uint32_t* counts, int n, int bits, cudaStream_t s, int* status,
+                      bool hist_ready) {
   if (n <= 1) return;
   const int items = pick_items<K>(n);
   const int ntiles = div_up(n, kSortThreads * items);
@@ -384,10 +385,11 @@ void radix_sort_pairs(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt,
   int* tickets = (int*)(counts + (size_t)passes * kBins);
   int* err = status ? status : tickets + passes;
   uint32_t* st = counts + (size_t)passes * kBins + passes + 1;
-  check(cudaMemsetAsync(counts, 0, sizeof(uint32_t) * ((size_t)passes * kBins + passes + 1), s),
-        "radix sort histogram reset");
-  const int hgrid = std::max(1, std::min(div_up(n, kSortThreads * 8), 148 * 4));
-  k_digit_hist<K><<<hgrid, kSortThreads, 0, s>>>(keys, n, passes, hist);
+  if (!hist_ready) {
+    radix_sort_prepare(counts, bits, s);
+    const int hgrid = std::max(1, std::min(div_up(n, kSortThreads * 8), 148 * 4));
+    k_digit_hist<K><<<hgrid, kSortThreads, 0, s>>>(keys, n, passes, hist);
+  }
   k_digit_offsets<<<passes, kBins, 0, s>>>(hist);
   K *ki = keys, *ko = keys_alt;
   uint32_t *vi = vals, *vo = vals_alt;
@@ -409,9 +411,9 @@ void radix_sort_pairs(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt,
 }
 
 template void radix_sort_pairs<uint32_t>(uint32_t*, uint32_t*, uint32_t*, uint32_t*, uint32_t*,
-                                         int, int, cudaStream_t, int*);
+                                         int, int, cudaStream_t, int*, bool);
 template void radix_sort_pairs<uint64_t>(uint64_t*, uint32_t*, uint64_t*, uint32_t*, uint32_t*,
-                                         int, int, cudaStream_t, int*);
+                                         int, int, cudaStream_t, int*, bool);
 
 }  // namespace nb
 

@@ -12,6 +12,7 @@
 // 2*rhs/2^L that the first 3L key bits select; its half-size rhs/2^L is the
 // `cell_size` of the reference's opening test (BHTree.cu:577).
 #include "common.cuh"
+#include "digit_hist.cuh"
 #include "kernels.cuh"
 #include "moments.cuh"
 
@@ -85,32 +86,49 @@ __device__ void compute_geom(const unsigned long long* enc, TreeGeom& g) {
   g.scale = (rhs > 0.0) ? 512.0 / rhs : 0.0;
 }
 
+// Keys of n positions; hist (optional, 4 x 256 words, cleared) receives the
+// digit counts of the four 8-bit passes of the radix sort that follows.
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
 k_keys(const T* __restrict__ x, const T* __restrict__ y, const T* __restrict__ z, int n,
        const unsigned long long* __restrict__ enc, TreeGeom* __restrict__ geom_out,
-       uint32_t* __restrict__ keys, uint32_t* __restrict__ perm, int* __restrict__ status) {
+       uint32_t* __restrict__ keys, uint32_t* __restrict__ perm, int* __restrict__ status,
+       uint32_t* __restrict__ hist) {
   __shared__ TreeGeom g;
+  __shared__ uint32_t s_h[4][kHistBins];
   if (threadIdx.x == 0) {
     compute_geom(enc, g);
     if (blockIdx.x == 0) *geom_out = g;
   }
+  if (hist)
+    for (int i = threadIdx.x; i < 4 * kHistBins; i += blockDim.x) (&s_h[0][0])[i] = 0;
   __syncthreads();
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+  const long long end = hist ? (n + 31) / 32 * 32 : n;  // whole warps take part in match_any
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < end;
        i += (long long)gridDim.x * blockDim.x) {
-    double p[3] = {(double)x[i], (double)y[i], (double)z[i]};
-    uint32_t c[3];
-    bool finite = true;
+    const bool valid = i < n;
+    uint32_t key = 0;
+    if (valid) {
+      double p[3] = {(double)x[i], (double)y[i], (double)z[i]};
+      uint32_t c[3];
+      bool finite = true;
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      double q = (p[k] - g.lo[k]) * g.scale;
-      finite &= (q == q);
-      q = fmin(fmax(q, 0.0), 1023.0);
-      c[k] = (q == q) ? (uint32_t)q : 0u;
+      for (int k = 0; k < 3; ++k) {
+        double q = (p[k] - g.lo[k]) * g.scale;
+        finite &= (q == q);
+        q = fmin(fmax(q, 0.0), 1023.0);
+        c[k] = (q == q) ? (uint32_t)q : 0u;
+      }
+      if (!finite) atomicOr(status, kStatusNonFinite);
+      key = morton30(c[0], c[1], c[2]);
+      keys[i] = key;
+      perm[i] = (uint32_t)i;
     }
-    if (!finite) atomicOr(status, kStatusNonFinite);
-    keys[i] = morton30(c[0], c[1], c[2]);
-    perm[i] = (uint32_t)i;
+    if (hist) hist_add(s_h, key, valid, 4);
+  }
+  if (hist) {
+    __syncthreads();
+    hist_flush(s_h, 4, hist);
   }
 }
 
@@ -741,10 +759,13 @@ void launch_bbox(TreeWork& w, const T* x, const T* y, const T* z, int n, cudaStr
 }
 
 template <typename T>
-void launch_keys(TreeWork& w, const T* x, const T* y, const T* z, int n, cudaStream_t s) {
-  int g = std::min(grid_for(n), 148 * 16);
+void launch_keys(TreeWork& w, const T* x, const T* y, const T* z, int n, cudaStream_t s,
+                 uint32_t* hist) {
+  // with histograms: fewer blocks, so fewer block histograms to add up
+  int g = hist ? std::min(div_up(n, kThreads * 8), 148 * 4) : std::min(grid_for(n), 148 * 16);
   if (g < 1) g = 1;
-  k_keys<T><<<g, kThreads, 0, s>>>(x, y, z, n, w.bbox_enc, w.geom, w.keys, w.perm, w.status);
+  k_keys<T><<<g, kThreads, 0, s>>>(x, y, z, n, w.bbox_enc, w.geom, w.keys, w.perm, w.status,
+                                   hist);
   check(cudaGetLastError(), "k_keys launch");
 }
 
@@ -753,13 +774,13 @@ template void launch_bbox<float>(TreeWork&, const float*, const float*, const fl
 template void launch_bbox<double>(TreeWork&, const double*, const double*, const double*, int,
                                   cudaStream_t);
 template void launch_keys<float>(TreeWork&, const float*, const float*, const float*, int,
-                                 cudaStream_t);
+                                 cudaStream_t, uint32_t*);
 template void launch_keys<double>(TreeWork&, const double*, const double*, const double*, int,
-                                  cudaStream_t);
+                                  cudaStream_t, uint32_t*);
 template void launch_bbox<HiLo>(TreeWork&, const HiLo*, const HiLo*, const HiLo*, int,
                                 cudaStream_t);
 template void launch_keys<HiLo>(TreeWork&, const HiLo*, const HiLo*, const HiLo*, int,
-                                cudaStream_t);
+                                cudaStream_t, uint32_t*);
 
 void launch_gather_body4(TreeWork& w, const float* x, const float* y, const float* z,
                          const float* m, int n, cudaStream_t s) {
