@@ -650,6 +650,7 @@ struct AdjointImpl {
     check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "adjoint stream");
     own_stream = true;
     tree_alloc(tw, n);
+    tree_enable_overlap(tw);
     tw.group_max = 32;
     const size_t n3 = 3 * (size_t)n;
     for (int L = 0; L <= steps; ++L) {
@@ -764,14 +765,14 @@ struct AdjointImpl {
     const double* x = X[L];
     const size_t n1 = n, n2 = 2 * (size_t)n;
     launch_bbox<double>(tw, x, x + n1, x + n2, n, st);
-    launch_keys<double>(tw, x, x + n1, x + n2, n, st);
+    uint32_t* hist = radix_sort_prepare(tw.counts, 30, st);  // counted by the key kernel
+    launch_keys<double>(tw, x, x + n1, x + n2, n, st, hist);
     radix_sort_pairs(tw.keys, tw.perm, tw.keys_alt, tw.perm_alt, tw.counts, n, 30, st,
-                     tw.status);
+                     tw.status, true);
     k_gather_sorted<<<grid1(n), kThreads, 0, st>>>(tw.perm, x, x + n1, x + n2, mass, n, xs, ys,
                                                    zs, tw.body4);
     tw.prune_max = p.leaf_max;
-    launch_build_topology(tw, n, st);
-    launch_build_moments(tw, n, xs, ys, zs, st);
+    launch_tree<uint32_t>(tw, tw.keys, n, 30, 0, 1, tw.geom, nullptr, xs, ys, zs, st);
     check(cudaMemcpyAsync(perm[L], tw.perm, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st),
           "tape permutation");
     k_copy_groups<<<grid1(n), kThreads, 0, st>>>(tw.groups, tw.n_groups, n, groups[L],

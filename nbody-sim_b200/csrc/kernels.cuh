@@ -124,9 +124,11 @@ void launch_tree(TreeWork& w, const K* keys, int n, int key_bits, int disk_bits,
 void launch_geoms(const unsigned long long* enc, TreeGeom* geoms, int n_disks, cudaStream_t s);
 void launch_bbox_reset_n(unsigned long long* enc, int n_disks, cudaStream_t s);
 template <typename T>
+// hist (optional, from radix_sort_prepare): the digit counts of the sort of
+// the key_bits-bit keys that follows.
 void launch_keys_multi(const T* x, const T* y, const T* z, const int* disk, int n,
                        const TreeGeom* geoms, uint64_t* keys, uint32_t* perm, int* status,
-                       cudaStream_t s);
+                       cudaStream_t s, uint32_t* hist = nullptr, int key_bits = 0);
 // Single disk: Karras radix tree over w.keys.
 void launch_build_topology(TreeWork& w, int n, cudaStream_t s);
 // FP64 moments, compressed octree (contiguous children) and the target

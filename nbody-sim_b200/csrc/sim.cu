@@ -1314,11 +1314,12 @@ struct EnsembleImpl : EnsembleBase {
     StateArrays<R>& b = s[1 - cur];
     const int key_bits = 30 + disk_bits;
     launch_geoms(bbox, geoms, D, st);
+    uint32_t* hist = radix_sort_prepare(tw.counts, key_bits, st);  // counted by the key kernel
     launch_keys_multi<R>(a.v[0], a.v[1], a.v[2], a.disk, n, geoms, keys64, tw.perm, tw.status,
-                         st);
+                         st, hist, key_bits);
     launch_bbox_reset_n(bbox, D, st);
     radix_sort_pairs<uint64_t>(keys64, tw.perm, keys64_alt, tw.perm_alt, tw.counts, n, key_bits,
-                               st, tw.status);
+                               st, tw.status, true);
     k_permute<R><<<div_up(n, kThreads), kThreads, 0, st>>>(tw.perm, a, b, n, tw.body4);
     check(cudaGetLastError(), "k_permute launch");
     cur = 1 - cur;
@@ -1344,10 +1345,10 @@ struct EnsembleImpl : EnsembleBase {
     w.work = work; w.status = tw.status; w.targets_per_lane = tw.group_max / 32;
     w.walk_mode = p.walk_mode;
     launch_walk(w, st);
-    // geoms, keys, bbox reset, digit histogram and offsets, one one-sweep
-    // kernel per pass, permute, karras, mark, tile scan, apply, moment tiles,
-    // moment tile scan, emit, walk
-    launches += 3 + 2 + (key_bits + 7) / 8 + 9;
+    // geoms, keys (+ digit histograms), bbox reset, digit offsets, one
+    // one-sweep kernel per pass, permute, karras, mark, tile scan, apply,
+    // moment tiles, moment tile scan, emit, walk
+    launches += 3 + 1 + (key_bits + 7) / 8 + 9;
   }
 
   void collide() {

@@ -151,24 +151,41 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads)
 k_keys_multi(const T* __restrict__ x, const T* __restrict__ y, const T* __restrict__ z,
              const int* __restrict__ disk, int n, const TreeGeom* __restrict__ geoms,
-             uint64_t* __restrict__ keys, uint32_t* __restrict__ perm, int* __restrict__ status) {
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+             uint64_t* __restrict__ keys, uint32_t* __restrict__ perm, int* __restrict__ status,
+             uint32_t* __restrict__ hist, int passes) {
+  __shared__ uint32_t s_h[kHistMaxPasses][kHistBins];
+  if (hist) {
+    for (int i = threadIdx.x; i < passes * kHistBins; i += blockDim.x) (&s_h[0][0])[i] = 0;
+    __syncthreads();
+  }
+  const long long end = hist ? (n + 31) / 32 * 32 : n;  // whole warps take part in match_any
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < end;
        i += (long long)gridDim.x * blockDim.x) {
-    const int d = disk[i];
-    const TreeGeom& g = geoms[d];
-    double p[3] = {(double)x[i], (double)y[i], (double)z[i]};
-    uint32_t c[3];
-    bool finite = true;
+    const bool valid = i < n;
+    uint64_t key = 0;
+    if (valid) {
+      const int d = disk[i];
+      const TreeGeom& g = geoms[d];
+      double p[3] = {(double)x[i], (double)y[i], (double)z[i]};
+      uint32_t c[3];
+      bool finite = true;
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      double q = (p[k] - g.lo[k]) * g.scale;
-      finite &= (q == q);
-      q = fmin(fmax(q, 0.0), 1023.0);
-      c[k] = (q == q) ? (uint32_t)q : 0u;
+      for (int k = 0; k < 3; ++k) {
+        double q = (p[k] - g.lo[k]) * g.scale;
+        finite &= (q == q);
+        q = fmin(fmax(q, 0.0), 1023.0);
+        c[k] = (q == q) ? (uint32_t)q : 0u;
+      }
+      if (!finite) atomicOr(status, kStatusNonFinite);
+      key = ((uint64_t)d << 30) | (uint64_t)morton30(c[0], c[1], c[2]);
+      keys[i] = key;
+      perm[i] = (uint32_t)i;
     }
-    if (!finite) atomicOr(status, kStatusNonFinite);
-    keys[i] = ((uint64_t)d << 30) | (uint64_t)morton30(c[0], c[1], c[2]);
-    perm[i] = (uint32_t)i;
+    if (hist) hist_add(s_h, key, valid, passes);
+  }
+  if (hist) {
+    __syncthreads();
+    hist_flush(s_h, passes, hist);
   }
 }
 
@@ -803,20 +820,23 @@ void launch_bbox_reset_n(unsigned long long* enc, int n_disks, cudaStream_t s) {
 template <typename T>
 void launch_keys_multi(const T* x, const T* y, const T* z, const int* disk, int n,
                        const TreeGeom* geoms, uint64_t* keys, uint32_t* perm, int* status,
-                       cudaStream_t s) {
-  int g = std::min(grid_for(n), 148 * 16);
+                       cudaStream_t s, uint32_t* hist, int key_bits) {
+  int g = hist ? std::min(div_up(n, kThreads * 8), 148 * 4) : std::min(grid_for(n), 148 * 16);
   if (g < 1) g = 1;
-  k_keys_multi<T><<<g, kThreads, 0, s>>>(x, y, z, disk, n, geoms, keys, perm, status);
+  k_keys_multi<T><<<g, kThreads, 0, s>>>(x, y, z, disk, n, geoms, keys, perm, status, hist,
+                                         (key_bits + 7) / 8);
   check(cudaGetLastError(), "k_keys_multi launch");
 }
 
 template void launch_keys_multi<float>(const float*, const float*, const float*, const int*, int,
-                                       const TreeGeom*, uint64_t*, uint32_t*, int*, cudaStream_t);
+                                       const TreeGeom*, uint64_t*, uint32_t*, int*, cudaStream_t,
+                                       uint32_t*, int);
 template void launch_keys_multi<double>(const double*, const double*, const double*, const int*,
                                         int, const TreeGeom*, uint64_t*, uint32_t*, int*,
-                                        cudaStream_t);
+                                        cudaStream_t, uint32_t*, int);
 template void launch_keys_multi<HiLo>(const HiLo*, const HiLo*, const HiLo*, const int*, int,
-                                      const TreeGeom*, uint64_t*, uint32_t*, int*, cudaStream_t);
+                                      const TreeGeom*, uint64_t*, uint32_t*, int*, cudaStream_t,
+                                      uint32_t*, int);
 
 template <typename K>
 void launch_karras(TreeWork& w, const K* keys, int n, int key_bits, cudaStream_t s) {
