@@ -296,6 +296,14 @@ typedef struct nbody_sim_params {
                                 a larger box.  <= 0: automatic (8 for a
                                 simulation of >= 2^19 bodies, else 1; 1
                                 for an ensemble).                          */
+  int fuse_collisions;       /* 0 (default): the collision impulse comes from
+                                a neighbour search over the step's tree
+                                (launchCollisionKernel's pairs), run on a
+                                second stream beside the force walk; 1: it
+                                is found inside the force walk, among each
+                                group's own sources (no second tree walk).
+                                Same pairs; a body's impulses are summed in
+                                another order.                            */
 } nbody_sim_params;
 
 /* Parameters of src/main.cu:58-73 from a Config (r_coll = factor * radius). */

@@ -122,7 +122,7 @@ class nbody_sim_params(C.Structure):
                 ("perturber_mass_mjup", C.c_float), ("perturber_radius_au", C.c_float),
                 ("perturber_phase0", C.c_float), ("state_precision", C.c_int),
                 ("leaf_max", C.c_int), ("targets_per_lane", C.c_int), ("walk_mode", C.c_int),
-                ("group_span", C.c_int)]
+                ("group_span", C.c_int), ("fuse_collisions", C.c_int)]
 
 
 NBODY_PHASES = 6

@@ -216,6 +216,17 @@ struct WalkArgs {
   int* tape_used;         // chunks taken (reset to 0 before the walk)
   int tape_cap;           // chunks in the pool
   int2* group_tape;
+  // fused collisions (coll_dv[0] != nullptr; targets_per_lane 1, no tape):
+  // every target also gets the two-pass collision impulse of the bodies
+  // closer than coll_r, found in its own source list (walk.cu).  dv is in
+  // the bodies' (key) order; velocities in the state's storage type.
+  const void* coll_v[3];
+  int coll_vtype;         // 0 float, 1 double, 2 hi/lo float pairs
+  float coll_r;
+  float coll_e;
+  float* coll_dv[3];
+  const float4* box_lo;   // node boxes (the octree's), for the reach test
+  const float4* box_hi;
 };
 int walk_spill_slots(int device);  // warps resident at once (spill area slots)
 void launch_walk(const WalkArgs& a, cudaStream_t s);

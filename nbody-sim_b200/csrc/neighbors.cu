@@ -16,6 +16,7 @@
 // bit-identical to the host O(N^2) loop.  Union-find always hooks the larger
 // root under the smaller one, so every root is its component's smallest
 // original index; every loop is bounded and reports kStatusUnionFindLimit.
+#include "collide_math.cuh"
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -71,15 +72,6 @@ struct CollideOut {
   float* dvz;
 };
 
-// A velocity component as the FP32 impulse uses it: the float value, the
-// double rounded to float, or the hi word of a hi/lo pair (the conversions
-// of the state's float read-out).
-__device__ __forceinline__ float vel(const void* p, int vtype, uint32_t i) {
-  if (vtype == 1) return (float)__ldg((const double*)p + i);
-  if (vtype == 2) return __ldg((const float2*)p + i).x;
-  return __ldg((const float*)p + i);
-}
-
 struct FofOut {
   const uint32_t* ids;
   float ll2;
@@ -118,9 +110,9 @@ k_neighbors(const NeighborArgs a, float radius, CollideOut co, FofOut fo) {
     float vix = 0.f, viy = 0.f, viz = 0.f;
     if (kMode == 0 && valid) {
       const uint32_t vi = co.vmap ? co.vmap[s] : (uint32_t)s;
-      vix = vel(co.vx, co.vtype, vi);
-      viy = vel(co.vy, co.vtype, vi);
-      viz = vel(co.vz, co.vtype, vi);
+      vix = coll_vel(co.vx, co.vtype, vi);
+      viy = coll_vel(co.vy, co.vtype, vi);
+      viz = coll_vel(co.vz, co.vtype, vi);
     }
     float dvx = 0.f, dvy = 0.f, dvz = 0.f;
     const int my_id = (kMode == 1 && valid) ? (int)fo.ids[s] : 0;
@@ -204,19 +196,13 @@ k_neighbors(const NeighborArgs a, float radius, CollideOut co, FofOut fo) {
             const int j = w.idx[k];
             if (kMode == 0) {
               // BHTree.cu:642-660 (leaf branch), j != i
-              float dx = q.x - me.x, dy = q.y - me.y, dz = q.z - me.z;
-              float dist2 = dx * dx + dy * dy + dz * dz;
+              const float dx = q.x - me.x, dy = q.y - me.y, dz = q.z - me.z;
+              const float dist2 = coll_dist2(dx, dy, dz);
               if (j != s && dist2 < co.rc2) {
                 const uint32_t vj = co.vmap ? co.vmap[j] : (uint32_t)j;
-                float dist = sqrtf(dist2) + 1e-10f;
-                float nx = dx / dist, ny = dy / dist, nz = dz / dist;
-                float dvn = (vel(co.vx, co.vtype, vj) - vix) * nx +
-                            (vel(co.vy, co.vtype, vj) - viy) * ny +
-                            (vel(co.vz, co.vtype, vj) - viz) * nz;
-                if (dvn < 0.f) {
-                  float J = -(1.f + co.e) * dvn * 0.5f;
-                  dvx += -J * nx; dvy += -J * ny; dvz += -J * nz;
-                }
+                coll_impulse(dx, dy, dz, dist2, coll_vel(co.vx, co.vtype, vj) - vix,
+                             coll_vel(co.vy, co.vtype, vj) - viy,
+                             coll_vel(co.vz, co.vtype, vj) - viz, co.e, dvx, dvy, dvz);
               }
             } else if (j > s) {
               // Aggregate.cpp:38-40, no FMA contraction

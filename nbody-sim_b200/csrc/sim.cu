@@ -338,6 +338,28 @@ void state_out(const StateArrays<R>& a, int n, const float* ax, const float* ay,
   check(cudaStreamSynchronize(st), "get_state sync");
 }
 
+// The collision pass runs beside the force walk on the tree's second stream
+// (it needs the tree and the half-step velocities, not the accelerations):
+// its own group counter and stack-spill area, and the fork / join events.
+struct CollSide {
+  int* work = nullptr;
+  int* spill = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+  void alloc(size_t spill_words) {
+    check(cudaMalloc(&work, sizeof(int)), "collision work");
+    check(cudaMalloc(&spill, sizeof(int) * spill_words), "collision spill");
+    check(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), "collision fork");
+    check(cudaEventCreateWithFlags(&join, cudaEventDisableTiming), "collision join");
+  }
+  void release() {
+    if (work) cudaFree(work);
+    if (spill) cudaFree(spill);
+    if (fork) cudaEventDestroy(fork);
+    if (join) cudaEventDestroy(join);
+    *this = CollSide();
+  }
+};
+
 // Bytes of the state_out scratch for n bodies.
 inline size_t out_stage_bytes(int n) { return (size_t)n * (6 * sizeof(double) + 3 * sizeof(float)); }
 
@@ -432,6 +454,7 @@ struct SimBase {
   // graphs): from there on the step leaves the positions alone.
   cudaEvent_t ev_pos = nullptr;
   cudaStream_t rb_st = nullptr;  // read-back stream of step_host
+  CollSide cs;                   // collisions beside the walk (r_coll > 0)
   bool capturing = false;
 
   void common_alloc() {
@@ -471,6 +494,7 @@ struct SimBase {
     if (cap_st) cudaStreamDestroy(cap_st);
     if (rb_st) cudaStreamDestroy(rb_st);
     if (ev_pos) cudaEventDestroy(ev_pos);
+    cs.release();
     if (pipe) {
       delete pipe;
       pipe = nullptr;
@@ -561,6 +585,7 @@ struct SimImpl : SimBase {
     tree_enable_overlap(tw);
     check(cudaEventCreateWithFlags(&ev_pos, cudaEventDisableTiming), "position event");
     check(cudaStreamCreateWithFlags(&rb_st, cudaStreamNonBlocking), "read-back stream");
+    if (p.r_coll > 0.f) cs.alloc((size_t)walk_spill_slots(0) * spill_cap);
     tw.group_max = 32 * p.targets_per_lane;
     tw.group_span = p.group_span;
     for (int b = 0; b < 2; ++b) {
@@ -678,8 +703,18 @@ struct SimImpl : SimBase {
     w.spill = spill; w.spill_cap = spill_cap; w.inter = inter; w.counters = counters;
     w.work = work; w.status = tw.status; w.targets_per_lane = tw.group_max / 32;
     w.walk_mode = p.walk_mode;
+    if (!initial && coll_fused()) set_coll_args(w);
+    const bool side_coll = !initial && p.r_coll > 0.f && !coll_fused();
+    if (side_coll) {  // the collision pass on the second stream, beside the walk
+      check(cudaEventRecord(cs.fork, st), "collision fork");
+      check(cudaStreamWaitEvent(tw.side, cs.fork, 0), "collision fork");
+      collide(tw.side, cs.work, cs.spill);
+      check(cudaEventRecord(cs.join, tw.side), "collision join");
+      launches += 1;
+    }
     mark(NBODY_PHASE_WALK);
     launch_walk(w, st);
+    if (side_coll) check(cudaStreamWaitEvent(st, cs.join, 0), "collision join");
     mark(NBODY_PHASE_COLLIDE);
     // keys (+ digit histograms), bbox reset, digit offsets, 4 one-sweep
     // passes, permute, karras, mark, tile scan, apply, moment tiles, moment
@@ -687,17 +722,26 @@ struct SimImpl : SimBase {
     launches += 16;
   }
 
-  void collide() {
+  // Collisions inside the walk (one warp per group of <= 32 targets).
+  bool coll_fused() const {
+    return p.r_coll > 0.f && p.fuse_collisions && tw.group_max == 32;
+  }
+  void set_coll_args(WalkArgs& w) {
+    for (int k = 0; k < 3; ++k) w.coll_v[k] = s[cur].v[3 + k];
+    w.coll_vtype = kIsF32<R> ? 0 : (kIsF64<R> ? 1 : 2);
+    w.coll_r = p.r_coll;
+    w.coll_e = p.restitution;
+    w.coll_dv[0] = dvx; w.coll_dv[1] = dvy; w.coll_dv[2] = dvz;
+    w.box_lo = tw.oct.box_lo; w.box_hi = tw.oct.box_hi;
+  }
+
+  void collide(cudaStream_t on, int* wk, int* sp) {
     NeighborArgs na{tw.oct.info, tw.oct.box_lo, tw.oct.box_hi, tw.body4, n,
-                    tw.groups, tw.n_groups, p.leaf_max, spill, spill_cap, work, tw.status};
-    if (kIsF32<R>) {
-      launch_collide(na, (const float*)s[cur].v[3], (const float*)s[cur].v[4],
-                     (const float*)s[cur].v[5], nullptr, p.r_coll, p.restitution, dvx, dvy, dvz,
-                     st);
-    } else {  // the half-step velocities read in their storage type, rounded to float
-      launch_collide_v(na, s[cur].v[3], s[cur].v[4], s[cur].v[5], kIsF64<R> ? 1 : 2, nullptr,
-                       p.r_coll, p.restitution, dvx, dvy, dvz, st);
-    }
+                    tw.groups, tw.n_groups, p.leaf_max, sp, spill_cap, wk, tw.status};
+    // the half-step velocities read in their storage type, rounded to float
+    launch_collide_v(na, s[cur].v[3], s[cur].v[4], s[cur].v[5],
+                     kIsF32<R> ? 0 : (kIsF64<R> ? 1 : 2), nullptr, p.r_coll, p.restitution,
+                     dvx, dvy, dvz, on);
   }
 
   void stream_kernel(bool end, bool begin) {
@@ -731,11 +775,7 @@ struct SimImpl : SimBase {
   void one_step(bool first) {
     mark(NBODY_PHASE_STREAM);
     stream_kernel(!first, true);
-    compute_forces(false);
-    if (p.r_coll > 0.f) {
-      collide();
-      launches += 1;
-    }
+    compute_forces(false);  // with the collision pass when r_coll > 0
     if (p.perturber_enabled) {
       k_increment<<<1, 1, 0, st>>>(pert_step);
       check(cudaGetLastError(), "k_increment launch");
@@ -1188,6 +1228,7 @@ struct EnsembleImpl : EnsembleBase {
     spill = dalloc<int>((size_t)walk_spill_slots(0) * spill_cap, "walk spill");
     work = dalloc<int>(1, "work");
     inter = dalloc<unsigned long long>(1, "inter");
+    if (p.r_coll > 0.f) cs.alloc((size_t)walk_spill_slots(0) * spill_cap);
     counters = dalloc<unsigned long long>(3, "counters");
     staging = dalloc<double>(n, "staging");
     reserve_perturber_rows(64);
@@ -1206,6 +1247,7 @@ struct EnsembleImpl : EnsembleBase {
     for (void* q : ptrs)
       if (q) cudaFree(q);
     tree_free(tw);
+    cs.release();
     if (cap_st) cudaStreamDestroy(cap_st);
     if (own_stream && st) cudaStreamDestroy(st);
   }
@@ -1309,7 +1351,8 @@ struct EnsembleImpl : EnsembleBase {
 
   // Keys, sort, permute into key order, tree, walk.  Leaves the bounding
   // boxes reset for the next stream kernel to accumulate.
-  void compute_forces() {
+  // with_coll: the step's forces, which may carry the fused collisions.
+  void compute_forces(bool with_coll = false) {
     StateArrays<R>& a = s[cur];
     StateArrays<R>& b = s[1 - cur];
     const int key_bits = 30 + disk_bits;
@@ -1344,26 +1387,37 @@ struct EnsembleImpl : EnsembleBase {
     w.spill = spill; w.spill_cap = spill_cap; w.inter = inter; w.counters = counters;
     w.work = work; w.status = tw.status; w.targets_per_lane = tw.group_max / 32;
     w.walk_mode = p.walk_mode;
+    if (with_coll && coll_fused()) {
+      for (int k = 0; k < 3; ++k) w.coll_v[k] = s[cur].v[3 + k];
+      w.coll_vtype = kIsF32<R> ? 0 : (kIsF64<R> ? 1 : 2);
+      w.coll_r = p.r_coll;
+      w.coll_e = p.restitution;
+      w.coll_dv[0] = dvx; w.coll_dv[1] = dvy; w.coll_dv[2] = dvz;
+      w.box_lo = tw.oct.box_lo; w.box_hi = tw.oct.box_hi;
+    }
+    const bool side_coll = with_coll && p.r_coll > 0.f && !coll_fused();
+    if (side_coll) {  // the collision pass on the second stream, beside the walk
+      check(cudaEventRecord(cs.fork, st), "collision fork");
+      check(cudaStreamWaitEvent(tw.side, cs.fork, 0), "collision fork");
+      collide(tw.side, cs.work, cs.spill);
+      check(cudaEventRecord(cs.join, tw.side), "collision join");
+    }
     launch_walk(w, st);
+    if (side_coll) check(cudaStreamWaitEvent(st, cs.join, 0), "collision join");
     // geoms, keys (+ digit histograms), bbox reset, digit offsets, one
     // one-sweep kernel per pass, permute, karras, mark, tile scan, apply,
     // moment tiles, moment tile scan, emit, walk
     launches += 3 + 1 + (key_bits + 7) / 8 + 9;
   }
 
-  void collide() {
+  void collide(cudaStream_t on, int* wk, int* sp) {
     NeighborArgs na{tw.oct.info, tw.oct.box_lo, tw.oct.box_hi, tw.body4, n, tw.groups,
-                    tw.n_groups, p.leaf_max, spill, spill_cap, work, tw.status, group_disk};
-    if (kIsF32<R>) {
-      launch_collide(na, (const float*)s[cur].v[3], (const float*)s[cur].v[4],
-                     (const float*)s[cur].v[5], nullptr, p.r_coll, p.restitution, dvx, dvy, dvz,
-                     st);
-      launches += 1;
-    } else {  // the half-step velocities read in their storage type, rounded to float
-      launch_collide_v(na, s[cur].v[3], s[cur].v[4], s[cur].v[5], kIsF64<R> ? 1 : 2, nullptr,
-                       p.r_coll, p.restitution, dvx, dvy, dvz, st);
-      launches += 1;
-    }
+                    tw.n_groups, p.leaf_max, sp, spill_cap, wk, tw.status, group_disk};
+    // the half-step velocities read in their storage type, rounded to float
+    launch_collide_v(na, s[cur].v[3], s[cur].v[4], s[cur].v[5],
+                     kIsF32<R> ? 0 : (kIsF64<R> ? 1 : 2), nullptr, p.r_coll, p.restitution,
+                     dvx, dvy, dvz, on);
+    launches += 1;
   }
 
   void stream_kernel(bool end, bool begin) {
@@ -1388,10 +1442,16 @@ struct EnsembleImpl : EnsembleBase {
   // main.cu:101-139 for every disk: (dv + K2 + drag of the previous step),
   // K1 + drift + bbox, tree + walk (+ star, + perturber at t_{n+1}),
   // collisions on v_1/2; then the perturber row advances.
+  CollSide cs;  // collisions beside the walk (r_coll > 0)
+
+  bool coll_fused() const {
+    return p.r_coll > 0.f && p.fuse_collisions && tw.group_max == 32;
+  }
+
   void one_step(bool first) {
     stream_kernel(!first, true);
-    compute_forces();
-    if (p.r_coll > 0.f) collide();
+    compute_forces(true);
+    // (the collision pass, when r_coll > 0, runs inside compute_forces)
     k_increment<<<1, 1, 0, st>>>(pert_step);
     check(cudaGetLastError(), "k_increment launch");
     launches += 1;

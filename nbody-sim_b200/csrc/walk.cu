@@ -22,6 +22,7 @@
 //
 // The stack spills to a per-warp global area when it would overflow; a
 // spill area that runs out raises kStatusStackOverflow instead of hanging.
+#include "collide_math.cuh"
 #include "common.cuh"
 #include "kernels.cuh"
 #include "walk_math.cuh"
@@ -46,6 +47,7 @@ constexpr int kList = 64;
 
 struct WarpSmem {
   float4 lst[kList];
+  int lidx[kList];  // fused collisions: body index of each single-body source, else -1
   float4 ext[6];  // the group's targets of least / greatest x, y, z (vote prefilter)
   int stk[kStk];
   int sc[32];
@@ -87,6 +89,74 @@ __device__ __forceinline__ void list_shift(float4* lst, int nlist, int lane) {
   if (lane < rem) t = lst[32 + lane];
   __syncwarp();
   if (lane < rem) lst[lane] = t;
+  __syncwarp();
+}
+
+// Fused collisions: a lane's target (index, half-step velocity) and its
+// accumulated impulse.
+struct CollLane {
+  int self;
+  float vx, vy, vz;
+  float dvx, dvy, dvz;
+};
+
+// Collision sweep of a batch lst[0..cnt): every single-body source closer
+// than r_coll to the lane's target adds its impulse (coll_dist2 and
+// coll_impulse, as the stand-alone neighbour search).
+__device__ __forceinline__ void coll_batch(const WalkArgs& a, const float4* lst, const int* lidx,
+                                           int cnt, const float4 me, bool valid, float rc2,
+                                           CollLane& cl) {
+  for (int j = 0; j < cnt; ++j) {
+    const int b = lidx[j];
+    if (b < 0) continue;
+    const float4 s = lst[j];
+    const float dx = s.x - me.x, dy = s.y - me.y, dz = s.z - me.z;
+    const float d2 = coll_dist2(dx, dy, dz);
+    if (valid && b != cl.self && d2 < rc2)
+      coll_impulse(dx, dy, dz, d2, coll_vel(a.coll_v[0], a.coll_vtype, b) - cl.vx,
+                   coll_vel(a.coll_v[1], a.coll_vtype, b) - cl.vy,
+                   coll_vel(a.coll_v[2], a.coll_vtype, b) - cl.vz, a.coll_e, cl.dvx, cl.dvy,
+                   cl.dvz);
+  }
+}
+
+// Gravity of a batch as eval_list, plus the least softened squared distance
+// seen (a batch whose least distance is beyond r_coll has no collision).
+template <bool kSoft>
+__device__ __forceinline__ void interact_rmin(const float4 src, const float4 me, float eps2,
+                                              float3& acc, float& rmin) {
+  const float dx = src.x - me.x, dy = src.y - me.y, dz = src.z - me.z;
+  rmin = fminf(rmin, fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2))));
+  interact<kSoft>(src, me, eps2, acc);
+}
+
+template <bool kSoft, int kCount>
+__device__ __forceinline__ float eval_list_rmin(const float4* lst, int cnt, const float4 me,
+                                                float eps2, float3& acc) {
+  float rmin = INFINITY;
+  if (kCount > 0) {
+#pragma unroll
+    for (int j = 0; j < kCount; ++j) interact_rmin<kSoft>(lst[j], me, eps2, acc, rmin);
+  } else {
+    for (int j = 0; j < cnt; ++j) interact_rmin<kSoft>(lst[j], me, eps2, acc, rmin);
+  }
+  return rmin;
+}
+
+// Drops the first 32 entries of the list and of its body indices.
+__device__ __forceinline__ void list_shift_idx(float4* lst, int* lidx, int nlist, int lane) {
+  const int rem = nlist - 32;
+  float4 t;
+  int b = -1;
+  if (lane < rem) {
+    t = lst[32 + lane];
+    b = lidx[32 + lane];
+  }
+  __syncwarp();
+  if (lane < rem) {
+    lst[lane] = t;
+    lidx[lane] = b;
+  }
   __syncwarp();
 }
 
@@ -146,8 +216,15 @@ __device__ __forceinline__ void tape_append(const WalkArgs& a, TapeCursor& t, bo
 }
 
 // kT targets per lane: a group of up to 32 kT bodies per warp.  kRec: also
-// record the group's source list on the tape.
-template <bool kSoft, int kT, bool kRec, int kMode>
+// record the group's source list on the tape.  kColl (kT == 1): fused
+// collisions.  A multi-body node whose box comes within r_coll of the group
+// box is opened even when the opening test would accept it, so every body
+// that can touch a target reaches the source list as a single body; each
+// evaluated batch whose least distance is inside r_coll is then swept for
+// collision pairs.  The pairs are those of the stand-alone search: the same
+// squared distance and impulse arithmetic (collide_math.cuh); only the order
+// in which a target's impulses are summed differs.
+template <bool kSoft, int kT, bool kRec, int kMode, bool kColl = false>
 __global__ void __launch_bounds__(kWalkWarps * 32, walk_min_blocks<kMode>())
     k_walk(const WalkArgs a) {
   __shared__ WarpSmem smem[kWalkWarps];
@@ -199,6 +276,20 @@ __global__ void __launch_bounds__(kWalkWarps * 32, walk_min_blocks<kMode>())
       }
       __syncwarp();
     }
+    CollLane cl{-1, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    float rc2 = 0.f, reach = 0.f, rthr = 0.f;
+    if (kColl) {
+      const int s0 = valid[0] ? gr.x + lane : gr.x;
+      cl.self = valid[0] ? s0 : -1;
+      cl.vx = coll_vel(a.coll_v[0], a.coll_vtype, s0);
+      cl.vy = coll_vel(a.coll_v[1], a.coll_vtype, s0);
+      cl.vz = coll_vel(a.coll_v[2], a.coll_vtype, s0);
+      rc2 = a.coll_r * a.coll_r;
+      reach = a.coll_r * 1.00001f + 1e-30f;  // a pair inside r_coll is inside this on each axis
+      // softened squared distances carry eps^2 and a few roundings: a batch
+      // whose least one is above this holds no pair inside r_coll
+      rthr = (rc2 + eps2) * 1.00002f + 1e-37f;
+    }
 
     // The tree sum starts from zero: adding ~10^3 terms into an accumulator
     // that already holds the star pull (10^3-10^5 times larger) would round
@@ -232,9 +323,11 @@ __global__ void __launch_bounds__(kWalkWarps * 32, walk_min_blocks<kMode>())
       float4 c = make_float4(0.f, 0.f, 0.f, 0.f);
       int first = 0, cnt = 0;
       float h2 = 0.f, d2 = 0.f, far2 = 0.f;
+      int4 ninf = make_int4(0, 0, 0, 0);
       if (node >= 0) {
         c = __ldg(a.com + node);
         const int4 inf = __ldg(a.info + node);
+        ninf = inf;
         cnt = inf.z >> 4;
         const int nch = inf.z & 15;
         const float half = __int_as_float(inf.w);
@@ -304,9 +397,32 @@ __global__ void __launch_bounds__(kWalkWarps * 32, walk_min_blocks<kMode>())
           if (__all_sync(kFull, ok) && lane == j) act = 1;
         }
       }
+      if (kColl) {  // an accepted node within reach of the group stays open
+        const int cntb = ninf.z >> 4;
+        if (act == 1 && cntb > 1) {
+          const float4 lo = __ldg(a.box_lo + node), hi = __ldg(a.box_hi + node);
+          if (lo.x <= gx1 + reach && hi.x >= gx0 - reach && lo.y <= gy1 + reach &&
+              hi.y >= gy0 - reach && lo.z <= gz1 + reach && hi.z >= gz0 - reach) {
+            const int nch = ninf.z & 15;
+            if (nch == 0 || cntb <= a.leaf_max) {
+              act = 2;
+              first = ninf.y;
+              cnt = cntb;
+            } else {
+              act = 3;
+              first = ninf.x;
+              cnt = nch;
+            }
+          }
+        }
+      }
       // accepted sources -> list
       const unsigned m1 = __ballot_sync(kFull, act == 1);
-      if (act == 1) w.lst[nlist + __popc(m1 & lanemask_lt())] = c;
+      if (act == 1) {
+        const int pos = nlist + __popc(m1 & lanemask_lt());
+        w.lst[pos] = c;
+        if (kColl) w.lidx[pos] = ((ninf.z >> 4) == 1) ? ninf.y : -1;
+      }
       if (kRec) {
         const int4 inf = (node >= 0) ? __ldg(a.info + node) : make_int4(0, 0, 0, 0);
         tape_append(a, tc, act == 1, __popc(m1 & lanemask_lt()), __popc(m1),
@@ -315,9 +431,16 @@ __global__ void __launch_bounds__(kWalkWarps * 32, walk_min_blocks<kMode>())
       nlist += __popc(m1);
       __syncwarp();
       if (nlist >= 32) {
-        eval_list<kSoft, kT, 32>(w.lst, 32, me, eps2, acc);
+        if (kColl) {
+          const float rmin = eval_list_rmin<kSoft, 32>(w.lst, 32, me[0], eps2, acc[0]);
+          if (__any_sync(kFull, rmin < rthr))
+            coll_batch(a, w.lst, w.lidx, 32, me[0], valid[0], rc2, cl);
+          list_shift_idx(w.lst, w.lidx, nlist, lane);
+        } else {
+          eval_list<kSoft, kT, 32>(w.lst, 32, me, eps2, acc);
+          list_shift(w.lst, nlist, lane);
+        }
         evaluated += 32;
-        list_shift(w.lst, nlist, lane);
         nlist -= 32;
       }
 
@@ -358,6 +481,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, walk_min_blocks<kMode>())
             const int prev = (o > 0) ? w.sc[o - 1] : 0;
             w.lst[nlist + lane] = __ldg(a.body + w.slo[o] + (gi - prev));
             if (kRec) w.sc_body[lane] = w.slo[o] + (gi - prev);
+            if (kColl) w.lidx[nlist + lane] = w.slo[o] + (gi - prev);
           }
           if (kRec) {
             __syncwarp();
@@ -367,16 +491,35 @@ __global__ void __launch_bounds__(kWalkWarps * 32, walk_min_blocks<kMode>())
           nlist += min(32, btotal - base);
           __syncwarp();
           if (nlist >= 32) {
-            eval_list<kSoft, kT, 32>(w.lst, 32, me, eps2, acc);
+            if (kColl) {
+              const float rmin = eval_list_rmin<kSoft, 32>(w.lst, 32, me[0], eps2, acc[0]);
+              if (__any_sync(kFull, rmin < rthr))
+                coll_batch(a, w.lst, w.lidx, 32, me[0], valid[0], rc2, cl);
+              list_shift_idx(w.lst, w.lidx, nlist, lane);
+            } else {
+              eval_list<kSoft, kT, 32>(w.lst, 32, me, eps2, acc);
+              list_shift(w.lst, nlist, lane);
+            }
             evaluated += 32;
-            list_shift(w.lst, nlist, lane);
             nlist -= 32;
           }
         }
       }
     }
 
-    eval_list<kSoft, kT, 0>(w.lst, nlist, me, eps2, acc);
+    if (kColl) {
+      const float rmin = eval_list_rmin<kSoft, 0>(w.lst, nlist, me[0], eps2, acc[0]);
+      if (__any_sync(kFull, rmin < rthr))
+        coll_batch(a, w.lst, w.lidx, nlist, me[0], valid[0], rc2, cl);
+      if (valid[0]) {
+        const int s = gr.x + lane;
+        a.coll_dv[0][s] = cl.dvx;
+        a.coll_dv[1][s] = cl.dvy;
+        a.coll_dv[2][s] = cl.dvz;
+      }
+    } else {
+      eval_list<kSoft, kT, 0>(w.lst, nlist, me, eps2, acc);
+    }
     evaluated += nlist;
     __syncwarp();
 
@@ -423,11 +566,11 @@ __global__ void __launch_bounds__(kWalkWarps * 32, walk_min_blocks<kMode>())
   }
 }
 
-template <bool kSoft, int kT, bool kRec = false, int kMode = 0>
+template <bool kSoft, int kT, bool kRec = false, int kMode = 0, bool kColl = false>
 int walk_blocks_per_sm() {
   static int b = 0;
   if (b == 0) {
-    check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<kSoft, kT, kRec, kMode>,
+    check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<kSoft, kT, kRec, kMode, kColl>,
                                                         kWalkWarps * 32, 0),
           "walk occupancy");
     if (b < 1) b = 1;
@@ -445,19 +588,26 @@ int num_sms() {
   return sms;
 }
 
-template <bool kSoft, int kT, bool kRec = false, int kMode = 0>
+template <bool kSoft, int kT, bool kRec = false, int kMode = 0, bool kColl = false>
 void launch_variant(const WalkArgs& a, cudaStream_t s) {
-  int grid = num_sms() * walk_blocks_per_sm<kSoft, kT, kRec, kMode>();
+  int grid = num_sms() * walk_blocks_per_sm<kSoft, kT, kRec, kMode, kColl>();
   grid = std::min(grid, (a.n + kWalkWarps - 1) / kWalkWarps);  // groups <= n
   if (grid < 1) grid = 1;
-  k_walk<kSoft, kT, kRec, kMode><<<grid, kWalkWarps * 32, 0, s>>>(a);
+  k_walk<kSoft, kT, kRec, kMode, kColl><<<grid, kWalkWarps * 32, 0, s>>>(a);
+}
+
+template <bool kSoft, bool kColl>
+void launch_mode(const WalkArgs& a, cudaStream_t s) {
+  if (a.walk_mode == 1) launch_variant<kSoft, 1, false, 1, kColl>(a, s);
+  else if (a.walk_mode == 2) launch_variant<kSoft, 1, false, 2, kColl>(a, s);
+  else launch_variant<kSoft, 1, false, 0, kColl>(a, s);
 }
 
 template <bool kSoft>
-void launch_mode(const WalkArgs& a, cudaStream_t s) {
-  if (a.walk_mode == 1) launch_variant<kSoft, 1, false, 1>(a, s);
-  else if (a.walk_mode == 2) launch_variant<kSoft, 1, false, 2>(a, s);
-  else launch_variant<kSoft, 1, false, 0>(a, s);
+int coll_blocks_per_sm() {
+  return std::max(std::max(walk_blocks_per_sm<kSoft, 1, false, 0, true>(),
+                           walk_blocks_per_sm<kSoft, 1, false, 1, true>()),
+                  walk_blocks_per_sm<kSoft, 1, false, 2, true>());
 }
 
 }  // namespace
@@ -471,7 +621,8 @@ int walk_spill_slots(int) {
                                  walk_blocks_per_sm<false, 1, false, 1>()),
                         std::max(walk_blocks_per_sm<true, 1, false, 2>(),
                                  walk_blocks_per_sm<false, 1, false, 2>()))));
-  return num_sms() * b * kWalkWarps;
+  const int bc = std::max(coll_blocks_per_sm<true>(), coll_blocks_per_sm<false>());
+  return num_sms() * std::max(b, bc) * kWalkWarps;
 }
 
 void launch_walk(const WalkArgs& a, cudaStream_t s) {
@@ -484,9 +635,12 @@ void launch_walk(const WalkArgs& a, cudaStream_t s) {
   } else if (a.targets_per_lane == 2) {
     if (soft) launch_variant<true, 2>(a, s);
     else launch_variant<false, 2>(a, s);
+  } else if (a.coll_dv[0]) {  // fused collisions
+    if (soft) launch_mode<true, true>(a, s);
+    else launch_mode<false, true>(a, s);
   } else {
-    if (soft) launch_mode<true>(a, s);
-    else launch_mode<false>(a, s);
+    if (soft) launch_mode<true, false>(a, s);
+    else launch_mode<false, false>(a, s);
   }
   check(cudaGetLastError(), "k_walk launch");
 }
