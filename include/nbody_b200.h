@@ -140,6 +140,16 @@ int nbody_tree_force(nbody_tree* t, nbody_particles* p, float theta, float softe
 /* launchCollisionKernel (src/physics/BHTree.cu:688-708): two-pass inelastic
  * impulse for pairs closer than r_coll; updates p->vx,vy,vz in place. */
 int nbody_tree_collide(nbody_tree* t, nbody_particles* p, float r_coll, float restitution);
+/* Collision miss report for the summarized tree (its own copy of the
+ * positions): *pairs = ordered pairs (i, j != i) closer than r_coll, all of
+ * which nbody_tree_collide applies; *missed = how many of them the
+ * reference's traversal would skip, because its cell prune
+ * |x_i - com| - 1.732 half >= r_coll (src/physics/BHTree.cu:663-665) drops a
+ * cell whose centre of mass lies away from the body.  Cells below the tenth
+ * octree level (inside buckets of equal 30-bit keys) are not modelled.
+ * Synchronous. */
+int nbody_tree_collision_report(nbody_tree* t, float r_coll, unsigned long long* pairs,
+                                unsigned long long* missed);
 /* Bodies opened directly instead of subdivided further (default 8). */
 int nbody_tree_set_leaf_max(nbody_tree* t, int leaf_max);
 /* Targets per lane of the force walk: 1 (warp groups of <= 32 bodies, the

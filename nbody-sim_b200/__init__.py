@@ -190,6 +190,7 @@ SIGNATURES = [
                                    C.c_float]),
     ("nbody_tree_collide", C.c_int, [_VP, C.POINTER(nbody_particles), C.c_float, C.c_float]),
     ("nbody_tree_set_leaf_max", C.c_int, [_VP, C.c_int]),
+    ("nbody_tree_collision_report", C.c_int, [_VP, C.c_float, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong)]),
     ("nbody_tree_set_targets_per_lane", C.c_int, [_VP, C.c_int]),
     ("nbody_tree_stats_get", C.c_int, [_VP, C.POINTER(nbody_tree_stats)]),
     ("nbody_half_kick", C.c_int, [C.POINTER(nbody_particles), C.c_float]),
@@ -416,6 +417,14 @@ class Octree:
 
     def summarize(self):
         _check(lib.nbody_tree_summarize(self.h))
+
+    def collision_report(self, r_coll: float):
+        """(pairs, missed): ordered pairs closer than r_coll, and how many of
+        them the reference's collision cell prune would skip
+        (nbody_tree_collision_report)."""
+        pairs, missed = C.c_ulonglong(), C.c_ulonglong()
+        _check(lib.nbody_tree_collision_report(self.h, r_coll, C.byref(pairs), C.byref(missed)))
+        return pairs.value, missed.value
 
     def sort(self):
         _check(lib.nbody_tree_sort(self.h))

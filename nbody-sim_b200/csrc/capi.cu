@@ -237,6 +237,36 @@ int nbody_tree_collide(nbody_tree* t, nbody_particles* p, float r_coll, float re
   })
 }
 
+int nbody_tree_collision_report(nbody_tree* t, float r_coll, unsigned long long* pairs,
+                                unsigned long long* missed) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(t && pairs && missed, "nbody_tree_collision_report: null argument");
+    NBODY_REQUIRE(r_coll >= 0.f, "nbody_tree_collision_report: negative radius");
+    if (!t->summarized)
+      throw nb::ArgError("nbody_tree_collision_report: tree not summarized", NBODY_ERR_STATE);
+    *pairs = 0;
+    *missed = 0;
+    if (t->n < 2 || r_coll == 0.f) return NBODY_OK;
+    unsigned long long* rep = nullptr;
+    nb::check(cudaMalloc(&rep, 2 * sizeof(unsigned long long)), "report counters");
+    unsigned long long h[2] = {0, 0};
+    try {
+      nb::NeighborArgs na{t->tw.oct.info, t->tw.oct.box_lo, t->tw.oct.box_hi, t->tw.body4, t->n,
+                          t->tw.groups, t->tw.n_groups, t->leaf_max, t->spill, t->spill_cap,
+                          t->work, t->tw.status};
+      nb::launch_collision_report(na, t->tw.oct.com, r_coll, rep, 0);
+      nb::check(cudaMemcpy(h, rep, sizeof(h), cudaMemcpyDeviceToHost), "report read");
+    } catch (...) {
+      cudaFree(rep);
+      throw;
+    }
+    cudaFree(rep);
+    t->throw_status("nbody_tree_collision_report");
+    *pairs = h[0];
+    *missed = h[1];
+  })
+}
+
 int nbody_tree_stats_get(nbody_tree* t, nbody_tree_stats* out) {
   NBODY_API_BODY({
     NBODY_REQUIRE(t && out, "nbody_tree_stats_get: null argument");

@@ -253,6 +253,11 @@ struct NeighborArgs {
 void launch_collide(const NeighborArgs& a, const float* vx, const float* vy, const float* vz,
                     const uint32_t* vmap, float r_coll, float restitution, float* dvx,
                     float* dvy, float* dvz, cudaStream_t s);
+// Collision pairs of the octree's bodies (report[0], ordered pairs i, j != i
+// closer than r_coll) and how many of them the reference's cell prune would
+// skip (report[1]); the tree must hold every node (prune_max 0).
+void launch_collision_report(const NeighborArgs& a, const float4* com, float r_coll,
+                             unsigned long long* report, cudaStream_t s);
 // The same with velocities in the state's storage type: vtype 0 float,
 // 1 double, 2 hi/lo float pairs (converted to float as they are read).
 void launch_collide_v(const NeighborArgs& a, const void* vx, const void* vy, const void* vz,

@@ -70,7 +70,44 @@ struct CollideOut {
   float* dvx;
   float* dvy;
   float* dvz;
+  // report mode: the octree's centres of mass, r_coll and the two counters
+  // (pairs, pairs the reference's cell prune would skip)
+  const float4* com;
+  unsigned long long* report;
 };
+
+// Whether bhtree_collisionKernel would skip the pair (target at xi, sorted
+// body j): descending the octree cells that contain j, the first whose
+// |com - x_i| - 1.732 half is not below r_coll is pruned (BHTree.cu:663-665;
+// the same float operations, without contraction).  A chain of single-child
+// cells shares one centre of mass, so testing its smallest cell, the one the
+// compressed octree keeps, decides the whole chain.  Cells below the tenth
+// level (inside a bucket of equal keys) are not modelled.
+__device__ bool ref_prunes(const float4* __restrict__ com, const int4* __restrict__ info,
+                           float4 xi, int j, float r) {
+  int node = 0;
+  for (int depth = 0; depth < 64; ++depth) {
+    const int4 inf = __ldg(info + node);
+    const int nch = inf.z & 15;
+    if (nch == 0) return false;  // a leaf: the reference tests the bodies themselves
+    const float4 c = __ldg(com + node);
+    const float dx = c.x - xi.x, dy = c.y - xi.y, dz = c.z - xi.z;
+    const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+    const float half = __int_as_float(inf.w);
+    if (!(__fsub_rn(sqrtf(d2), __fmul_rn(half, 1.732f)) < r)) return true;
+    int next = -1;
+    for (int k = 0; k < nch; ++k) {
+      const int4 ci = __ldg(info + inf.x + k);
+      if (j >= ci.y && j < ci.y + (ci.z >> 4)) {
+        next = inf.x + k;
+        break;
+      }
+    }
+    if (next < 0) return false;
+    node = next;
+  }
+  return false;
+}
 
 struct FofOut {
   const uint32_t* ids;
@@ -78,7 +115,7 @@ struct FofOut {
   int* parent;
 };
 
-template <int kMode>  // 0: collision impulse, 1: FoF links
+template <int kMode>  // 0: collision impulse, 1: FoF links, 2: collision pair report
 __global__ void __launch_bounds__(kNbWarps * 32)
 k_neighbors(const NeighborArgs a, float radius, CollideOut co, FofOut fo) {
   __shared__ NbSmem smem[kNbWarps];
@@ -115,6 +152,7 @@ k_neighbors(const NeighborArgs a, float radius, CollideOut co, FofOut fo) {
       viz = coll_vel(co.vz, co.vtype, vi);
     }
     float dvx = 0.f, dvy = 0.f, dvz = 0.f;
+    unsigned long long npairs = 0, nmissed = 0;
     const int my_id = (kMode == 1 && valid) ? (int)fo.ids[s] : 0;
 
     int top = 1, spilled = 0;
@@ -204,6 +242,12 @@ k_neighbors(const NeighborArgs a, float radius, CollideOut co, FofOut fo) {
                              coll_vel(co.vy, co.vtype, vj) - viy,
                              coll_vel(co.vz, co.vtype, vj) - viz, co.e, dvx, dvy, dvz);
               }
+            } else if (kMode == 2) {
+              const float dx = q.x - me.x, dy = q.y - me.y, dz = q.z - me.z;
+              if (j != s && coll_dist2(dx, dy, dz) < co.rc2) {
+                ++npairs;
+                if (ref_prunes(co.com, a.info, me, j, radius)) ++nmissed;
+              }
             } else if (j > s) {
               // Aggregate.cpp:38-40, no FMA contraction
               float dx = __fsub_rn(me.x, q.x), dy = __fsub_rn(me.y, q.y),
@@ -221,6 +265,15 @@ k_neighbors(const NeighborArgs a, float radius, CollideOut co, FofOut fo) {
       co.dvx[s] = dvx;
       co.dvy[s] = dvy;
       co.dvz[s] = dvz;
+    }
+    if (kMode == 2) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        npairs += __shfl_xor_sync(kFull, npairs, o);
+        nmissed += __shfl_xor_sync(kFull, nmissed, o);
+      }
+      if (lane == 0 && npairs) atomicAdd(co.report, npairs);
+      if (lane == 0 && nmissed) atomicAdd(co.report + 1, nmissed);
     }
     if (lane == 0 && overflow) atomicOr(a.status, kStatusStackOverflow);
     }  // chunks of the group
@@ -257,7 +310,7 @@ __global__ void k_fof_sizes(const int* labels, const int* sizes, int n, uint16_t
   if ((threadIdx.x & 31) == 0 && local) atomicAdd(n_groups, local);
 }
 
-int g_nb_blocks_per_sm[2] = {0, 0};
+int g_nb_blocks_per_sm[3] = {0, 0, 0};
 
 template <int kMode>
 int nb_blocks_per_sm() {
@@ -300,7 +353,8 @@ void launch_nb(const NeighborArgs& a, float radius, const CollideOut& co, const 
 void launch_collide_v(const NeighborArgs& a, const void* vx, const void* vy, const void* vz,
                       int vtype, const uint32_t* vmap, float r_coll, float restitution,
                       float* dvx, float* dvy, float* dvz, cudaStream_t s) {
-  CollideOut co{vx, vy, vz, vtype, vmap, r_coll * r_coll, restitution, dvx, dvy, dvz};
+  CollideOut co{vx, vy, vz, vtype, vmap, r_coll * r_coll, restitution, dvx, dvy, dvz, nullptr,
+                nullptr};
   FofOut fo{nullptr, 0.f, nullptr};
   launch_nb<0>(a, r_coll, co, fo, s);
 }
@@ -311,11 +365,20 @@ void launch_collide(const NeighborArgs& a, const float* vx, const float* vy, con
   launch_collide_v(a, vx, vy, vz, 0, vmap, r_coll, restitution, dvx, dvy, dvz, s);
 }
 
+void launch_collision_report(const NeighborArgs& a, const float4* com, float r_coll,
+                             unsigned long long* report, cudaStream_t s) {
+  check(cudaMemsetAsync(report, 0, 2 * sizeof(unsigned long long), s), "report reset");
+  CollideOut co{nullptr, nullptr, nullptr, 0, nullptr, r_coll * r_coll, 0.f,
+                nullptr, nullptr, nullptr, com, report};
+  FofOut fo{nullptr, 0.f, nullptr};
+  launch_nb<2>(a, r_coll, co, fo, s);
+}
+
 void launch_fof_link(const NeighborArgs& a, const uint32_t* ids, float link_length, int* parent,
                      cudaStream_t s) {
   if (a.n <= 0) return;
   k_fof_init<<<div_up(a.n, 256), 256, 0, s>>>(parent, a.n);
-  CollideOut co{nullptr, nullptr, nullptr, 0, nullptr, 0.f, 0.f, nullptr, nullptr, nullptr};
+  CollideOut co{nullptr, nullptr, nullptr, 0, nullptr, 0.f, 0.f, nullptr, nullptr, nullptr, nullptr, nullptr};
   const float ll2 = link_length * link_length;  // Aggregate.cpp:30
   FofOut fo{ids, ll2, parent};
   launch_nb<1>(a, link_length, co, fo, s);
@@ -339,7 +402,7 @@ void launch_fof_link_capped(const NeighborArgs& a, const uint32_t* ids, float li
                             int* parent, int max_warps, cudaStream_t s) {
   if (a.n <= 0) return;
   k_fof_init<<<div_up(a.n, 256), 256, 0, s>>>(parent, a.n);
-  CollideOut co{nullptr, nullptr, nullptr, 0, nullptr, 0.f, 0.f, nullptr, nullptr, nullptr};
+  CollideOut co{nullptr, nullptr, nullptr, 0, nullptr, 0.f, 0.f, nullptr, nullptr, nullptr, nullptr, nullptr};
   const float ll2 = link_length * link_length;  // Aggregate.cpp:30
   FofOut fo{ids, ll2, parent};
   int grid = sm_count() * nb_blocks_per_sm<1>();

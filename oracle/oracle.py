@@ -96,6 +96,8 @@ class Port:
         L.orc_force_count.restype = C.c_longlong
         L.orc_collision.argtypes = [C.POINTER(_Tree), _F, _F, _F, _F, _F, _F, C.c_float,
                                     C.c_float, C.c_int]
+        L.orc_collision_pairs.argtypes = [C.POINTER(_Tree), _F, _F, _F, C.c_float, C.c_int]
+        L.orc_collision_pairs.restype = C.c_longlong
         for name in ("orc_half_kick", "orc_drift"):
             getattr(L, name).argtypes = [_F, _F, _F, _F, _F, _F, C.c_float, C.c_int]
         L.orc_gas_drag.argtypes = [_F, _F, _F, _F, _F, _F, C.c_float, C.c_float, C.c_float,
@@ -188,6 +190,17 @@ class Port:
             self.lib.orc_collision(C.byref(t), *[_ptr(a, _F) for a in xs],
                                    *[_ptr(a, _F) for a in vs], r_coll, restitution, nthreads)
             return vs
+        finally:
+            self.free_tree(t)
+
+    def collision_pairs(self, x, y, z, m, r_coll, nthreads=0):
+        """Ordered pairs closer than r_coll that the reference's collision
+        traversal reaches (port.c orc_collision_pairs)."""
+        t = self.build_tree(x, y, z, m)
+        try:
+            xs = [np.ascontiguousarray(a, np.float32) for a in (x, y, z)]
+            return int(self.lib.orc_collision_pairs(C.byref(t), *[_ptr(a, _F) for a in xs],
+                                                    r_coll, nthreads))
         finally:
             self.free_tree(t)
 

@@ -332,6 +332,44 @@ void orc_collision(const orc_tree* t, const float* px, const float* py, const fl
     free(dv);
 }
 
+/* The ordered pairs (i, j != i) closer than r_coll that the traversal of
+ * bhtree_collisionKernel (BHTree.cu:620-673) reaches: its cell prune
+ * |x_i - com| - 1.732 half >= r_coll can skip some (BHTree.cu:663-665). */
+long long orc_collision_pairs(const orc_tree* t, const float* px, const float* py,
+                              const float* pz, float r_coll, int nthreads) {
+    const int n = t->n_bodies;
+    long long total = 0;
+    set_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : total)
+    for (int idx = 0; idx < n; ++idx) {
+        int i = t->sort_idx[idx];
+        if (i < 0) continue;
+        float ix = px[i], iy = py[i], iz = pz[i];
+        int stack[256];
+        int top = 0;
+        stack[top++] = t->n_total - 1;
+        while (top > 0) {
+            int node = stack[--top];
+            if (node < 0) continue;
+            float dx = t->pos_x[node] - ix, dy = t->pos_y[node] - iy, dz = t->pos_z[node] - iz;
+            float dist2 = dx * dx + dy * dy + dz * dz;
+            if (node < n) {
+                if (node != i && dist2 < r_coll * r_coll) ++total;
+            } else {
+                float cell_half = t->cell_size[node];
+                float cell_dist = sqrtf(dist2) - cell_half * 1.732f;
+                if (cell_dist < r_coll) {
+                    for (int k = 0; k < 8; ++k) {
+                        int c = t->child[(long)node * 8 + k];
+                        if (c >= 0 && top < 255) stack[top++] = c;
+                    }
+                }
+            }
+        }
+    }
+    return total;
+}
+
 /* ------------------------------------------------------------ integrator */
 
 /* integrator_halfKickKernel, Integrator.cu:7-15 */

@@ -55,6 +55,8 @@ long long orc_force_count(const orc_tree* t, const float* x, const float* y,
 void orc_collision(const orc_tree* t, const float* x, const float* y, const float* z,
                    float* vx, float* vy, float* vz, float r_coll, float restitution,
                    int nthreads);
+long long orc_collision_pairs(const orc_tree* t, const float* x, const float* y, const float* z,
+                              float r_coll, int nthreads);
 
 /* Integrator.cu:7-76 and the launchers' host-side arithmetic (:80-109). */
 void orc_half_kick(float* vx, float* vy, float* vz, const float* ax, const float* ay,

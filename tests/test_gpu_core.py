@@ -312,3 +312,36 @@ def test_radix_sort_u64_ensemble_keys(nb, cuda, n):
     nb.radix_sort(k, v, 36)
     order = np.argsort(keys, kind="stable")
     assert np.array_equal(v.cpu().numpy(), order)
+
+
+def test_collision_miss_report_matches_the_reference_traversal(nb, cuda, port):
+    """nbody_tree_collision_report on a clustered case: every pair closer
+    than r_coll (brute force, float32), and the pairs that the reference's
+    cell prune (BHTree.cu:663-665) skips, counted by the CPU restatement of
+    its traversal on its own tree.  The report's tree rounds its centres of
+    mass differently, so the missed counts agree to a few pairs."""
+    rng = np.random.default_rng(9)
+    n, r = 4000, np.float32(0.002)
+    centers = rng.random((40, 3)) * 0.05
+    pos = (centers[rng.integers(0, 40, n)] + rng.standard_normal((n, 3)) * 0.002).astype(np.float32)
+    st = {"x": pos[:, 0], "y": pos[:, 1], "z": pos[:, 2], "m": np.full(n, 1e-9, np.float32)}
+    st.update({k: np.zeros(n, np.float32) for k in ("vx", "vy", "vz")})
+    p = to_gpu(nb, cuda, st)
+    t = build(nb, p)
+    pairs, missed = t.collision_report(float(r))
+    x, y, z = [np.ascontiguousarray(pos[:, k]) for k in range(3)]
+    brute = 0
+    for i0 in range(0, n, 500):
+        i1 = min(n, i0 + 500)
+        dx = x[None, :] - x[i0:i1, None]
+        dy = y[None, :] - y[i0:i1, None]
+        dz = z[None, :] - z[i0:i1, None]
+        close = (dx * dx + dy * dy + dz * dz) < r * r
+        close[np.arange(i1 - i0), np.arange(i0, i1)] = False
+        brute += int(close.sum())
+    ref_missed = brute - port.collision_pairs(x, y, z, st["m"], r)
+    assert abs(pairs - brute) <= 2, (pairs, brute)
+    assert ref_missed > 10  # the case exercises the prune
+    assert abs(int(missed) - ref_missed) <= max(3, ref_missed // 10), (missed, ref_missed)
+    # with a radius of zero nothing is close
+    assert t.collision_report(0.0) == (0, 0)
