@@ -358,11 +358,27 @@ typedef struct nbody_sim_stats {
   unsigned long long walk_groups;         /* warp groups of the last walk */
   unsigned long long launches;            /* kernels launched so far (graph nodes included) */
   unsigned long long graph_launches;      /* steps replayed as one CUDA graph */
+  int targets_per_lane;                   /* the walk settings in use (after */
+  int leaf_max;                           /* nbody_sim_autotune, the kept    */
+  int walk_mode;                          /* candidate)                      */
+  int group_span;
 } nbody_sim_stats;
 int nbody_sim_stats_get(nbody_sim* s, nbody_sim_stats* out);
 /* 1 (default): each step is replayed as one CUDA graph (captured on first
  * use, four variants); 0: its kernels are launched one by one.  Steps run
  * while profiling is on are always launched one by one. */
+/* Walk autotuner (as nbody_ensemble_autotune; no reference counterpart):
+ * times two force evaluations of the current state for each candidate
+ * (targets_per_lane, leaf_max, walk_mode, group_span) in candidates[4k ..
+ * 4k+3] (NULL: a built-in list of 6; group_span <= 0: automatic) and keeps
+ * the fastest.  The best variant depends on the disk, and the choice holds
+ * for the state it was timed on: on the C2 disk (N = 131072, collisions)
+ * mode 2 is the faster at t = 0 but 20% slower over a 2000-step run, as
+ * the disk evolves; re-tune along a run.  The forces of the current time are
+ * recomputed with the kept setting (state unchanged; the next step's
+ * collision pass is not affected).  Synchronous; ms_out (optional) receives
+ * each candidate's time. */
+int nbody_sim_autotune(nbody_sim* s, const int* candidates, int n_candidates, float* ms_out);
 int nbody_sim_set_graphs(nbody_sim* s, int on);
 
 /* Per-phase device time of the steps run while profiling is on: CUDA events

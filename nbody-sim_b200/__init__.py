@@ -139,7 +139,8 @@ class nbody_sim_stats(C.Structure):
                 ("interactions", C.c_ulonglong), ("status", C.c_int),
                 ("walk_nodes_visited", C.c_ulonglong), ("walk_stack_spills", C.c_ulonglong),
                 ("walk_groups", C.c_ulonglong), ("launches", C.c_ulonglong),
-                ("graph_launches", C.c_ulonglong)]
+                ("graph_launches", C.c_ulonglong), ("targets_per_lane", C.c_int),
+                ("leaf_max", C.c_int), ("walk_mode", C.c_int), ("group_span", C.c_int)]
 
 
 class nbody_frame(C.Structure):
@@ -227,6 +228,7 @@ SIGNATURES = [
     ("nbody_sim_set_profiling", C.c_int, [_VP, C.c_int]),
     ("nbody_sim_profile_get", C.c_int, [_VP, C.POINTER(nbody_sim_profile), C.c_int]),
     ("nbody_sim_step_host", C.c_int, [_VP] + [_VP] * 10 + [C.c_int]),
+    ("nbody_sim_autotune", C.c_int, [_VP, _VP, C.c_int, _VP]),
     ("nbody_sim_set_graphs", C.c_int, [_VP, C.c_int]),
     ("nbody_sim_output_begin", C.c_int, [_VP, C.c_float, C.c_float, C.c_float, C.c_int]),
     ("nbody_sim_output_wait", C.c_int, [_VP, C.POINTER(nbody_frame)]),
@@ -703,6 +705,18 @@ class Sim:
 
     def set_profiling(self, on: bool = True):
         _check(lib.nbody_sim_set_profiling(self.h, int(on)))
+
+    def autotune(self, candidates=None):
+        """Times force evaluations per (targets_per_lane, leaf_max, walk_mode,
+        group_span) and keeps the fastest (nbody_sim_autotune).  Returns
+        [(tpl, leaf_max, walk_mode, group_span, ms), ...]."""
+        if candidates is None:
+            candidates = [(1, 8, 1, 0), (1, 8, 0, 0), (1, 8, 2, 0), (1, 16, 1, 0), (1, 16, 2, 0),
+                          (1, 4, 2, 0)]
+        flat = np.ascontiguousarray(np.array(candidates, np.int32).reshape(-1))
+        ms = np.zeros(len(candidates), np.float32)
+        _check(lib.nbody_sim_autotune(self.h, flat.ctypes.data, len(candidates), ms.ctypes.data))
+        return [(*map(int, c), float(t)) for c, t in zip(candidates, ms)]
 
     def set_graphs(self, on: bool = True):
         _check(lib.nbody_sim_set_graphs(self.h, int(on)))

@@ -448,6 +448,7 @@ struct SimBase {
   virtual void snapshot(float* const* dst) = 0;
   OutputPipe* pipe = nullptr;
   virtual void load_accel(const float* ax, const float* ay, const float* az) = 0;
+  virtual void autotune(const int* cand, int nc, float* ms_out) = 0;
   // Host round trip of nbody_sim_step_host (float state and float arrays).
   virtual void step_host(float* const* v, float* const* a, const float* mass, int nsteps) = 0;
   // Recorded after every permute (an external event node inside the step
@@ -645,6 +646,7 @@ struct SimImpl : SimBase {
     steps_done = 0;
     has_state = true;
     if (forces) {
+      upload_perturber(-1, 1);  // (float)(0) * dt = 0
       launch_bbox<R>(tw, s[0].v[0], s[0].v[1], s[0].v[2], n, st);
       compute_forces(true);
     } else {
@@ -687,7 +689,6 @@ struct SimImpl : SimBase {
     else
       launch_tree<uint32_t>(tw, tw.keys, n, 30, 0, 1, tw.geom, nullptr, nullptr, nullptr, nullptr,
                             st);
-    if (p.perturber_enabled && initial) upload_perturber(-1, 1);  // (float)(0) * dt = 0
     check(cudaMemsetAsync(inter, 0, sizeof(unsigned long long), st), "inter reset");
     check(cudaMemsetAsync(counters, 0, 3 * sizeof(unsigned long long), st), "counters reset");
     WalkArgs w{};
@@ -879,6 +880,64 @@ struct SimImpl : SimBase {
     check(cudaStreamSynchronize(rb_st), "read-back sync");
     check(cudaStreamSynchronize(st), "step_host sync");
   }
+
+  // Times force evaluations of the current state for each candidate
+  // (targets_per_lane, leaf_max, walk_mode, group_span) and keeps the
+  // fastest; the forces are recomputed with it, the state is unchanged.
+  void autotune(const int* cand, int nc, float* ms_out) override {
+    static const int kDefault[] = {1, 8, 1, 0, 1, 8, 0, 0, 1, 8, 2, 0,
+                                   1, 16, 1, 0, 1, 16, 2, 0, 1, 4, 2, 0};
+    if (!cand) {
+      cand = kDefault;
+      nc = 6;
+    }
+    auto apply = [&](int k) {
+      p.targets_per_lane = cand[4 * k] == 2 ? 2 : 1;
+      p.leaf_max = std::max(1, cand[4 * k + 1]);
+      p.walk_mode = (cand[4 * k + 2] >= 0 && cand[4 * k + 2] <= 2) ? cand[4 * k + 2]
+                                                                : kDefaultWalkMode;
+      const int span = cand[4 * k + 3];
+      p.group_span = span > 0 ? std::min(span, 64) : (n >= kGroupSpanMinBodies ? kDefaultGroupSpan : 1);
+      tw.group_max = 32 * p.targets_per_lane;
+      tw.group_span = p.group_span;
+    };
+    auto forces = [&]() {  // the forces of the current time, no collisions
+      upload_perturber(steps_done - 1, 1);
+      launch_bbox_reset(tw, st);
+      launch_bbox<R>(tw, s[cur].v[0], s[cur].v[1], s[cur].v[2], n, st);
+      compute_forces(true);
+    };
+    cudaEvent_t e0, e1;
+    check(cudaEventCreate(&e0), "event");
+    check(cudaEventCreate(&e1), "event");
+    float best = 0.f;
+    int best_k = -1;
+    for (int k = 0; k < nc; ++k) {
+      apply(k);
+      forces();  // warm-up with this setting
+      float ms = 0.f;
+      for (int rep = 0; rep < 2; ++rep) {  // best of two timed evaluations
+        check(cudaEventRecord(e0, st), "event");
+        forces();
+        check(cudaEventRecord(e1, st), "event");
+        check(cudaEventSynchronize(e1), "event sync");
+        float t = 0.f;
+        check(cudaEventElapsedTime(&t, e0, e1), "event time");
+        ms = (rep == 0) ? t : std::min(ms, t);
+      }
+      if (ms_out) ms_out[k] = ms;
+      if (best_k < 0 || ms < best) {
+        best = ms;
+        best_k = k;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    apply(best_k);
+    drop_graphs();
+    forces();
+    check(cudaStreamSynchronize(st), "autotune sync");
+  }
 };
 
 SimBase* make_sim(const nbody_sim_params& p, int n) {
@@ -1061,6 +1120,19 @@ int nbody_sim_stats_get(nbody_sim* s, nbody_sim_stats* out) {
     out->walk_groups = c[2];
     out->launches = b->launches;
     out->graph_launches = b->graph_launches;
+    out->targets_per_lane = b->p.targets_per_lane;
+    out->leaf_max = b->p.leaf_max;
+    out->walk_mode = b->p.walk_mode;
+    out->group_span = b->p.group_span;
+  })
+}
+
+int nbody_sim_autotune(nbody_sim* s, const int* candidates, int n_candidates, float* ms_out) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(s, "nbody_sim_autotune: null simulation");
+    NBODY_REQUIRE(s->impl->has_state, "nbody_sim_autotune: no state set");
+    NBODY_REQUIRE(!candidates || n_candidates >= 1, "nbody_sim_autotune: no candidates");
+    s->impl->autotune(candidates, n_candidates, ms_out);
   })
 }
 

@@ -36,11 +36,13 @@ class _Host:
 
 
 def run_simulation(cfg, out_dir: str, state=None, precision=None, pipelined: bool = True,
-                   total_steps: int | None = None, seed: int = 0):
+                   total_steps: int | None = None, seed: int = 0, params=None):
     """Runs cfg (an nbody_config) and writes out_dir/frames.bin and stats.csv.
 
     ``state``: dict x..vz (float32 or float64 host arrays) and m; default a
-    Keplerian disk from make_disk(seed).  Returns timings and counts."""
+    Keplerian disk from make_disk(seed).  ``params``: optional overrides of
+    nbody_sim_params fields (e.g. the walk settings an autotune kept).
+    Returns timings and counts."""
     nb = _nb()
     n = cfg.n_particles
     if state is None:
@@ -50,6 +52,8 @@ def run_simulation(cfg, out_dir: str, state=None, precision=None, pipelined: boo
     prm = nb.sim_params(cfg)
     if precision is not None:
         prm.state_precision = precision
+    for k, v in (params or {}).items():
+        setattr(prm, k, v)
     r_coll = prm.r_coll
     pm = cfg.particle_mass_msun
     every = cfg.output_every_n_steps

@@ -162,3 +162,37 @@ def test_fused_collisions_match_the_separate_pass(nb, cuda, precision):
     free = sim.get_state(double=True, accel=False)
     sim.close()
     assert np.abs(free["vx"] - out[1]["vx"]).max() > 1e-3
+
+
+def test_sim_autotune_keeps_the_state_and_the_fastest_setting(nb, cuda):
+    """nbody_sim_autotune mid-run: positions and velocities untouched, the
+    kept setting is the fastest candidate, the recomputed forces agree with
+    the step's own to the walk's approximation level, and stepping goes on."""
+    n = 20000
+    st = disk(nb, n, 0.5, 5.0, seed=5, m=1e-8)
+    prm = nb.sim_params(dt=0.005, theta=0.5, softening=1e-3, star_mass=1.0,
+                        r_coll=5.0 * nb.particle_physical_radius(1e-8), gas_drag_rate=1e-3,
+                        perturber_enabled=1, perturber_mass_mjup=1.0, perturber_radius_au=5.2,
+                        state_precision=1)
+    sim = nb.Sim(prm, n)
+    sim.set_state(st["x"], st["y"], st["z"], st["vx"], st["vy"], st["vz"], st["m"])
+    sim.step(3)
+    before = sim.get_state(double=True, accel=False)
+    acc0 = sim.get_state(double=False, accel=True)
+    tuned = sim.autotune()
+    after = sim.get_state(double=True, accel=False)
+    acc1 = sim.get_state(double=False, accel=True)
+    s = sim.stats()
+    assert len(tuned) == 6 and all(t[4] > 0 for t in tuned)
+    best = min(tuned, key=lambda t: t[4])
+    assert (s.targets_per_lane, s.leaf_max, s.walk_mode) == best[:3]
+    for k in ("x", "y", "z", "vx", "vy", "vz"):
+        assert np.array_equal(before[k], after[k]), k
+    a0 = np.stack([acc0[k] for k in ("ax", "ay", "az")], 1).astype(np.float64)
+    a1 = np.stack([acc1[k] for k in ("ax", "ay", "az")], 1).astype(np.float64)
+    rel = np.linalg.norm(a0 - a1, axis=1) / np.linalg.norm(a0, axis=1)
+    assert rel.max() < 1e-4, rel.max()
+    sim.step(2)
+    sim.sync()
+    assert sim.stats().status == 0 and sim.stats().steps_done == 5
+    sim.close()
