@@ -178,3 +178,28 @@ def test_device_disk_generator_matches_host(nb, cuda):
             assert np.allclose(v[k, off:off + n], d[key], rtol=1e-12, atol=1e-13), (s, key)
         off += n
     assert off == x.shape[1]
+
+
+def test_ensemble_fused_collisions_match_the_separate_pass(nb, cuda):
+    """The ensemble's collisions found inside its force walk (fuse_collisions)
+    against its neighbour pass beside the walk: the same pairs per disk, so
+    the states after a few steps agree to the rounding of the impulse sums."""
+    specs = [dict(s) for s in SPECS]
+    out = []
+    for fuse in (0, 1):
+        prm = params(nb, 1)
+        prm.fuse_collisions = fuse
+        prm.r_coll = 1e-2  # many touching pairs in these disks
+        prm.walk_mode = 1  # the vote walk (the autotuner is not run)
+        st, m = wl.ensemble_state(nb, specs)
+        e = nb.Ensemble(prm, specs)
+        e.set_state(st["x"], st["y"], st["z"], st["vx"], st["vy"], st["vz"], m)
+        e.step(3)
+        e.sync()
+        out.append(e.get_state(double=True, accel=False))
+        assert e.stats().status == 0
+        e.close()
+    for k in ("vx", "vy", "vz"):
+        assert np.abs(out[0][k] - out[1][k]).max() < 1e-5, k
+    for k in ("x", "y", "z"):
+        assert np.abs(out[0][k] - out[1][k]).max() < 1e-7, k
