@@ -206,11 +206,12 @@ k_gather_body4(const uint32_t* __restrict__ perm, const float* __restrict__ x,
 __device__ __forceinline__ int clz_key(uint32_t v) { return __clz(v); }
 __device__ __forceinline__ int clz_key(uint64_t v) { return __clzll((long long)v); }
 
+// ki = keys[i], loaded once by the caller.
 template <typename K>
-__device__ __forceinline__ int delta(const K* __restrict__ keys, int n, int i, int j) {
+__device__ __forceinline__ int delta(const K* __restrict__ keys, int n, K ki, int i, int j) {
   if (j < 0 || j >= n) return -1;
-  K a = keys[i], b = keys[j];
-  if (a != b) return clz_key(a ^ b);
+  const K kj = __ldg(keys + j);
+  if (ki != kj) return clz_key(ki ^ kj);
   return 8 * (int)sizeof(K) + __clz((uint32_t)i ^ (uint32_t)j);
 }
 
@@ -226,19 +227,20 @@ k_karras(const K* __restrict__ keys, int n, int key_bits, int* __restrict__ left
          int* __restrict__ hi_out, uint8_t* __restrict__ prefix) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n - 1) return;
-  const int d = (delta(keys, n, i, i + 1) - delta(keys, n, i, i - 1)) > 0 ? 1 : -1;
-  const int dmin = delta(keys, n, i, i - d);
+  const K ki = __ldg(keys + i);
+  const int d = (delta(keys, n, ki, i, i + 1) - delta(keys, n, ki, i, i - 1)) > 0 ? 1 : -1;
+  const int dmin = delta(keys, n, ki, i, i - d);
   int lmax = 2;
-  while (delta(keys, n, i, i + lmax * d) > dmin) lmax <<= 1;
+  while (delta(keys, n, ki, i, i + lmax * d) > dmin) lmax <<= 1;
   int l = 0;
   for (int t = lmax >> 1; t >= 1; t >>= 1)
-    if (delta(keys, n, i, i + (l + t) * d) > dmin) l += t;
+    if (delta(keys, n, ki, i, i + (l + t) * d) > dmin) l += t;
   const int j = i + l * d;
-  const int dnode = delta(keys, n, i, j);
+  const int dnode = delta(keys, n, ki, i, j);
   int s = 0, t = l;
   do {
     t = (t + 1) >> 1;
-    if (delta(keys, n, i, i + (s + t) * d) > dnode) s += t;
+    if (delta(keys, n, ki, i, i + (s + t) * d) > dnode) s += t;
   } while (t > 1);
   const int gamma = i + s * d + min(d, 0);
   const int lo = min(i, j), hi = max(i, j);
@@ -380,17 +382,30 @@ __device__ __forceinline__ int for_each_oct_child(const int* __restrict__ left,
                                                   const int* __restrict__ right,
                                                   const uint8_t* __restrict__ prefix, int n,
                                                   int disk_bits, int b, int lb, F f) {
-  int stack[8];
-  int top = 0, k = 0;
-  stack[top++] = right[b];
-  stack[top++] = left[b];
-  while (top > 0) {
-    int c = stack[--top];
-    if (c >= n - 1 || bin_level(prefix, n, c, disk_bits) > lb) {
-      f(c, k++);
-    } else if (top + 2 <= 8) {
-      stack[top++] = right[c];
-      stack[top++] = left[c];
+  // Binary nodes of b's own octree level have common prefixes 3 lb .. 3 lb + 2
+  // bits (above the disk bits) and every binary child adds at least one, so
+  // the octree children lie within three binary levels of b: a depth-first
+  // search unrolled to that depth, left first (no stack in local memory).
+  auto is_child = [&](int c) { return c >= n - 1 || bin_level(prefix, n, c, disk_bits) > lb; };
+  int k = 0;
+  const int c1[2] = {left[b], right[b]};
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const int a = c1[i];
+    if (is_child(a)) {
+      f(a, k++);
+      continue;
+    }
+    const int c2[2] = {left[a], right[a]};
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const int e = c2[j];
+      if (is_child(e)) {
+        f(e, k++);
+        continue;
+      }
+      f(left[e], k++);  // three levels down: a deeper octree level
+      f(right[e], k++);
     }
   }
   return k;
