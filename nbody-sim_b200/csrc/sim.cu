@@ -65,17 +65,20 @@ k_permute(const uint32_t* __restrict__ perm, StateArrays<R> in, StateArrays<R> o
           float4* __restrict__ body4) {
   for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
        s += (long long)gridDim.x * blockDim.x) {
+    // every gather first, then every store: the arrays carry no restrict, so
+    // interleaving them would make each load wait for the store before it
     const uint32_t o = perm[s];
     R q[6];
 #pragma unroll
-    for (int k = 0; k < 6; ++k) {
-      q[k] = in.v[k][o];
-      out.v[k][s] = q[k];
-    }
+    for (int k = 0; k < 6; ++k) q[k] = in.v[k][o];
     const float m = in.m[o];
+    const int id = in.id[o];
+    const int dk = in.disk ? in.disk[o] : 0;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) out.v[k][s] = q[k];
     out.m[s] = m;
-    out.id[s] = in.id[o];
-    if (in.disk) out.disk[s] = in.disk[o];
+    out.id[s] = id;
+    if (in.disk) out.disk[s] = dk;
     body4[s] = make_float4((float)q[0], (float)q[1], (float)q[2], m);
   }
 }
@@ -208,8 +211,10 @@ k_unsort(StateArrays<R> st, int n, T* __restrict__ o0, T* __restrict__ o1, T* __
   for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
        s += (long long)gridDim.x * blockDim.x) {
     const int o = st.id[s];
-    o0[o] = (T)st.v[0][s]; o1[o] = (T)st.v[1][s]; o2[o] = (T)st.v[2][s];
-    o3[o] = (T)st.v[3][s]; o4[o] = (T)st.v[4][s]; o5[o] = (T)st.v[5][s];
+    const T q0 = (T)st.v[0][s], q1 = (T)st.v[1][s], q2 = (T)st.v[2][s];
+    const T q3 = (T)st.v[3][s], q4 = (T)st.v[4][s], q5 = (T)st.v[5][s];
+    o0[o] = q0; o1[o] = q1; o2[o] = q2;
+    o3[o] = q3; o4[o] = q4; o5[o] = q5;
     if (oax) {
       double gx = ax[s], gy = ay[s], gz = az[s];
       if (sizeof(typename ComputeOf<R>::type) == 8) {  // the walk left the star out
@@ -233,7 +238,8 @@ k_unsort_pos(StateArrays<R> st, int n, float* __restrict__ ox, float* __restrict
   for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
        s += (long long)gridDim.x * blockDim.x) {
     const int o = st.id[s];
-    ox[o] = (float)st.v[0][s]; oy[o] = (float)st.v[1][s]; oz[o] = (float)st.v[2][s];
+    const float px = (float)st.v[0][s], py = (float)st.v[1][s], pz = (float)st.v[2][s];
+    ox[o] = px; oy[o] = py; oz[o] = pz;
   }
 }
 
@@ -246,8 +252,10 @@ k_unsort_vel_acc(StateArrays<R> st, int n, float* __restrict__ ovx, float* __res
   for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
        s += (long long)gridDim.x * blockDim.x) {
     const int o = st.id[s];
-    ovx[o] = (float)st.v[3][s]; ovy[o] = (float)st.v[4][s]; ovz[o] = (float)st.v[5][s];
-    oax[o] = ax[s]; oay[o] = ay[s]; oaz[o] = az[s];
+    const float vx = (float)st.v[3][s], vy = (float)st.v[4][s], vz = (float)st.v[5][s];
+    const float gx = ax[s], gy = ay[s], gz = az[s];
+    ovx[o] = vx; ovy[o] = vy; ovz[o] = vz;
+    oax[o] = gx; oay[o] = gy; oaz[o] = gz;
   }
 }
 

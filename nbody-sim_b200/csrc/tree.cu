@@ -677,7 +677,7 @@ __device__ void write_node(const EmitArgs<K>& a, int c, int f) {
 // Every octree node with a record writes it: a disk's root at slot = disk
 // index, a child at n_roots + off[parent] + its sibling index.
 template <typename K>
-__global__ void __launch_bounds__(kThreads) k_emit(const EmitArgs<K> a) {
+__global__ void __launch_bounds__(kThreads, 6) k_emit(const EmitArgs<K> a) {
   const int nb = 2 * a.n - 1;
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= nb) return;
