@@ -82,6 +82,7 @@ constexpr uint32_t kFlagP = 2u << 30;  // inclusive prefix published
 constexpr uint32_t kValMask = (1u << 30) - 1u;
 constexpr uint32_t kFlagMask = ~kValMask;
 constexpr int kSpinLimit = 1 << 20;
+constexpr int kLookAhead = 4;  // look-back words read per round
 constexpr int kMaxPasses = kHistMaxPasses;
 
 // Digit counts of every pass in one read: hist[p * 256 + d] (zeroed first).
@@ -188,20 +189,35 @@ k_onesweep(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
     atomicExch(mine, (t == 0 ? kFlagP : kFlagA) | run);
     uint32_t excl = 0;
     if (t > 0) {
+      // Four predecessors per round, loaded together (tiles below 0 read
+      // as an inclusive prefix of 0): a walk back over aggregates takes a
+      // quarter of the dependent L2 round trips.
       int j = t - 1, spins = 0;
       while (j >= 0) {
-        const uint32_t w = __ldcv(status + (size_t)j * kBins + d);
-        const uint32_t f = w & kFlagMask;
-        if (f == 0u) {
+        uint32_t w[kLookAhead];
+#pragma unroll
+        for (int q = 0; q < kLookAhead; ++q)
+          w[q] = (j - q >= 0) ? __ldcv(status + (size_t)(j - q) * kBins + d) : kFlagP;
+        int used = 0;
+        bool done = false;
+#pragma unroll
+        for (int q = 0; q < kLookAhead; ++q) {
+          if (done || used < q) break;  // stop at the first unpublished word
+          const uint32_t f = w[q] & kFlagMask;
+          if (f == 0u) break;
+          excl += w[q] & kValMask;
+          used = q + 1;
+          if (f == kFlagP) done = true;
+        }
+        if (done) break;
+        if (used == 0) {
           if (++spins > kSpinLimit) {
             atomicOr(err, kStatusSortWait);
             break;
           }
           continue;
         }
-        excl += w & kValMask;
-        if (f == kFlagP) break;
-        --j;
+        j -= used;
       }
       atomicExch(mine, kFlagP | ((excl + run) & kValMask));
     }
