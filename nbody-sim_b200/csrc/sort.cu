@@ -82,7 +82,7 @@ constexpr uint32_t kFlagP = 2u << 30;  // inclusive prefix published
 constexpr uint32_t kValMask = (1u << 30) - 1u;
 constexpr uint32_t kFlagMask = ~kValMask;
 constexpr int kSpinLimit = 1 << 20;
-constexpr int kLookAhead = 4;  // look-back words read per round
+constexpr int kLookAhead = 8;  // look-back words read per round
 constexpr int kMaxPasses = kHistMaxPasses;
 
 // Digit counts of every pass in one read: hist[p * 256 + d] (zeroed first).
@@ -189,9 +189,9 @@ k_onesweep(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
     atomicExch(mine, (t == 0 ? kFlagP : kFlagA) | run);
     uint32_t excl = 0;
     if (t > 0) {
-      // Four predecessors per round, loaded together (tiles below 0 read
-      // as an inclusive prefix of 0): a walk back over aggregates takes a
-      // quarter of the dependent L2 round trips.
+      // kLookAhead predecessors per round, loaded together (tiles below 0
+      // read as an inclusive prefix of 0): a walk back over aggregates takes
+      // that many times fewer dependent L2 round trips.
       int j = t - 1, spins = 0;
       while (j >= 0) {
         uint32_t w[kLookAhead];

@@ -648,6 +648,9 @@ __device__ void write_node(const EmitArgs<K>& a, int c, int f) {
   }
   const int L = ((int)a.prefix[c] - a.disk_bits) / 3;
   const int lo = a.lo[c], hi = a.hi[c];
+  // loaded before the record's stores (the arrays carry no restrict)
+  const int k = a.nch[c] & kNchCount;
+  const int first_child = k > 0 ? a.n_roots + (int)a.off[c] : -1;
   const double4 s = range_moments(a.ploc, a.tpre, lo, hi + 1);
   // the node's cube: level L cell of its key prefix (side 2 rhs / 2^L, exact
   // power-of-two scaling), grown by a margin for float positions that sit an
@@ -666,9 +669,8 @@ __device__ void write_node(const EmitArgs<K>& a, int c, int f) {
     ctr[k] = fl + 0.5f * fs;
   }
   const float4 com = com_of(s, ctr[0], ctr[1], ctr[2]);
-  const int k = a.nch[c] & kNchCount;
   a.oct.com[f] = com;
-  a.oct.info[f] = make_int4(k > 0 ? a.n_roots + (int)a.off[c] : -1, lo, ((hi - lo + 1) << 4) | k,
+  a.oct.info[f] = make_int4(first_child, lo, ((hi - lo + 1) << 4) | k,
                             __float_as_int(ldexpf(rhs, -L)));
   a.oct.box_lo[f] = make_float4(blo[0], blo[1], blo[2], 0.f);
   a.oct.box_hi[f] = make_float4(bhi[0], bhi[1], bhi[2], 0.f);
