@@ -231,32 +231,72 @@ k_unsort(StateArrays<R> st, int n, T* __restrict__ o0, T* __restrict__ o1, T* __
 // The caller-order read-back of nbody_sim_step_host in two halves: the
 // positions (final once the last step's permute has run) and the velocities
 // and accelerations (final at the end of the call).
-template <typename R>
+template <typename R, typename T>
 __global__ void __launch_bounds__(kThreads)
-k_unsort_pos(StateArrays<R> st, int n, float* __restrict__ ox, float* __restrict__ oy,
-             float* __restrict__ oz) {
+k_unsort_pos(StateArrays<R> st, int n, T* __restrict__ ox, T* __restrict__ oy,
+             T* __restrict__ oz) {
   for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
        s += (long long)gridDim.x * blockDim.x) {
     const int o = st.id[s];
-    const float px = (float)st.v[0][s], py = (float)st.v[1][s], pz = (float)st.v[2][s];
+    const T px = (T)st.v[0][s], py = (T)st.v[1][s], pz = (T)st.v[2][s];
     ox[o] = px; oy[o] = py; oz[o] = pz;
   }
 }
 
-template <typename R>
+// Velocities and accelerations, as k_unsort writes them (with the star term
+// an FP64 walk leaves out).
+template <typename R, typename T>
 __global__ void __launch_bounds__(kThreads)
-k_unsort_vel_acc(StateArrays<R> st, int n, float* __restrict__ ovx, float* __restrict__ ovy,
-                 float* __restrict__ ovz, const float* __restrict__ ax,
+k_unsort_vel_acc(StateArrays<R> st, int n, T* __restrict__ ovx, T* __restrict__ ovy,
+                 T* __restrict__ ovz, const float* __restrict__ ax,
                  const float* __restrict__ ay, const float* __restrict__ az,
-                 float* __restrict__ oax, float* __restrict__ oay, float* __restrict__ oaz) {
+                 float* __restrict__ oax, float* __restrict__ oay, float* __restrict__ oaz,
+                 double eps, double star_mass) {
   for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
        s += (long long)gridDim.x * blockDim.x) {
     const int o = st.id[s];
-    const float vx = (float)st.v[3][s], vy = (float)st.v[4][s], vz = (float)st.v[5][s];
-    const float gx = ax[s], gy = ay[s], gz = az[s];
+    const T vx = (T)st.v[3][s], vy = (T)st.v[4][s], vz = (T)st.v[5][s];
+    double gx = ax[s], gy = ay[s], gz = az[s];
+    if (sizeof(typename ComputeOf<R>::type) == 8) {  // the walk left the star out
+      double sx, sy, sz;
+      star_accel<double>((double)st.v[0][s], (double)st.v[1][s], (double)st.v[2][s], eps,
+                         star_mass, sx, sy, sz);
+      gx += sx; gy += sy; gz += sz;
+    }
     ovx[o] = vx; ovy[o] = vy; ovz[o] = vz;
-    oax[o] = gx; oay[o] = gy; oaz[o] = gz;
+    oax[o] = (float)gx; oay[o] = (float)gy; oaz[o] = (float)gz;
   }
+}
+
+// The positions-first read-back of a host round trip: positions on rb (once
+// ev_pos, recorded after the last permute, has fired), then velocities and
+// accelerations on st; T is the caller's type.  stage holds 6 T + 3 floats
+// per body.
+template <typename R, typename T>
+void read_back_split(const StateArrays<R>& a, int n, const float* ax, const float* ay,
+                     const float* az, double eps, double star_mass, T* const* v,
+                     float* const* acc, void* stage, cudaEvent_t ev_pos, cudaStream_t rb,
+                     cudaStream_t st) {
+  T* stg = (T*)stage;
+  const size_t nn = (size_t)n, bytes = sizeof(T) * nn, fb = sizeof(float) * nn;
+  check(cudaStreamWaitEvent(rb, ev_pos, 0), "read-back wait");
+  k_unsort_pos<R, T><<<stream_grid(n), kThreads, 0, rb>>>(a, n, stg, stg + nn, stg + 2 * nn);
+  check(cudaGetLastError(), "k_unsort_pos launch");
+  for (int k = 0; k < 3; ++k)
+    check(cudaMemcpyAsync(v[k], stg + k * nn, bytes, cudaMemcpyDeviceToHost, rb),
+          "position D2H");
+  T* sv = stg + 3 * nn;
+  float* sa = (float*)(stg + 6 * nn);
+  k_unsort_vel_acc<R, T><<<stream_grid(n), kThreads, 0, st>>>(
+      a, n, sv, sv + nn, sv + 2 * nn, ax, ay, az, sa, sa + nn, sa + 2 * nn, eps, star_mass);
+  check(cudaGetLastError(), "k_unsort_vel_acc launch");
+  for (int k = 0; k < 3; ++k)
+    check(cudaMemcpyAsync(v[3 + k], sv + k * nn, bytes, cudaMemcpyDeviceToHost, st),
+          "velocity D2H");
+  for (int k = 0; k < 3; ++k)
+    check(cudaMemcpyAsync(acc[k], sa + k * nn, fb, cudaMemcpyDeviceToHost, st), "accel D2H");
+  check(cudaStreamSynchronize(rb), "read-back sync");
+  check(cudaStreamSynchronize(st), "step_host sync");
 }
 
 __global__ void k_scatter_labels(const int* __restrict__ in_l, const uint16_t* __restrict__ in_s,
@@ -865,28 +905,8 @@ struct SimImpl : SimBase {
     }
     step(nsteps);
     if (!out_stage) out_stage = dalloc<char>(out_stage_bytes(n), "output staging");
-    float* stg = (float*)out_stage;  // 9 n floats of the 60 n bytes
-    const size_t nb = sizeof(float) * (size_t)n;
-    check(cudaStreamWaitEvent(rb_st, ev_pos, 0), "read-back wait");
-    k_unsort_pos<R><<<stream_grid(n), kThreads, 0, rb_st>>>(s[cur], n, stg, stg + n,
-                                                            stg + 2 * (size_t)n);
-    check(cudaGetLastError(), "k_unsort_pos launch");
-    for (int k = 0; k < 3; ++k)
-      check(cudaMemcpyAsync(v[k], stg + k * (size_t)n, nb, cudaMemcpyDeviceToHost, rb_st),
-            "position D2H");
-    float* sv = stg + 3 * (size_t)n;
-    k_unsort_vel_acc<R><<<stream_grid(n), kThreads, 0, st>>>(
-        s[cur], n, sv, sv + n, sv + 2 * (size_t)n, ax, ay, az, sv + 3 * (size_t)n,
-        sv + 4 * (size_t)n, sv + 5 * (size_t)n);
-    check(cudaGetLastError(), "k_unsort_vel_acc launch");
-    for (int k = 0; k < 3; ++k)
-      check(cudaMemcpyAsync(v[3 + k], sv + k * (size_t)n, nb, cudaMemcpyDeviceToHost, st),
-            "velocity D2H");
-    for (int k = 0; k < 3; ++k)
-      check(cudaMemcpyAsync(acc[k], sv + (3 + k) * (size_t)n, nb, cudaMemcpyDeviceToHost, st),
-            "accel D2H");
-    check(cudaStreamSynchronize(rb_st), "read-back sync");
-    check(cudaStreamSynchronize(st), "step_host sync");
+    read_back_split<R, float>(s[cur], n, ax, ay, az, p.softening, p.star_mass, v, acc, out_stage,
+                              ev_pos, rb_st, st);
   }
 
   // Times force evaluations of the current state for each candidate
@@ -1219,6 +1239,8 @@ struct EnsembleBase {
   virtual void set_state(const void* const* v, bool is_double, const float* mass,
                          bool on_device, bool forces = true) = 0;
   virtual void load_accel(const float* const* acc) = 0;
+  // Host round trip of nbody_ensemble_step_host (double state arrays).
+  virtual void step_host(double* const* v, float* const* a, const float* mass, int nsteps) = 0;
   virtual void step(int nsteps) = 0;
   virtual void get_state(void* const* v, bool as_double, float* const* a, bool on_device) = 0;
   virtual void autotune(const int* cand, int nc, float* ms) = 0;
@@ -1309,6 +1331,8 @@ struct EnsembleImpl : EnsembleBase {
     work = dalloc<int>(1, "work");
     inter = dalloc<unsigned long long>(1, "inter");
     if (p.r_coll > 0.f) cs.alloc((size_t)walk_spill_slots(0) * spill_cap);
+    check(cudaEventCreateWithFlags(&ev_pos, cudaEventDisableTiming), "position event");
+    check(cudaStreamCreateWithFlags(&rb_st, cudaStreamNonBlocking), "read-back stream");
     counters = dalloc<unsigned long long>(3, "counters");
     staging = dalloc<double>(n, "staging");
     reserve_perturber_rows(64);
@@ -1328,6 +1352,8 @@ struct EnsembleImpl : EnsembleBase {
       if (q) cudaFree(q);
     tree_free(tw);
     cs.release();
+    if (rb_st) cudaStreamDestroy(rb_st);
+    if (ev_pos) cudaEventDestroy(ev_pos);
     if (cap_st) cudaStreamDestroy(cap_st);
     if (own_stream && st) cudaStreamDestroy(st);
   }
@@ -1445,6 +1471,9 @@ struct EnsembleImpl : EnsembleBase {
                                st, tw.status, true);
     k_permute<R><<<div_up(n, kThreads), kThreads, 0, st>>>(tw.perm, a, b, n, tw.body4);
     check(cudaGetLastError(), "k_permute launch");
+    check(cudaEventRecordWithFlags(ev_pos, st, capturing ? cudaEventRecordExternal
+                                                         : cudaEventRecordDefault),
+          "position event");
     cur = 1 - cur;
     tw.prune_max = p.leaf_max;
     if (kIsF64<R>)
@@ -1523,6 +1552,11 @@ struct EnsembleImpl : EnsembleBase {
   // K1 + drift + bbox, tree + walk (+ star, + perturber at t_{n+1}),
   // collisions on v_1/2; then the perturber row advances.
   CollSide cs;  // collisions beside the walk (r_coll > 0)
+  // Recorded after every permute (an external event node in the step
+  // graphs); the read-back stream of step_host waits on it.
+  cudaEvent_t ev_pos = nullptr;
+  cudaStream_t rb_st = nullptr;
+  bool capturing = false;
 
   bool coll_fused() const {
     return p.r_coll > 0.f && p.fuse_collisions && tw.group_max == 32;
@@ -1551,7 +1585,9 @@ struct EnsembleImpl : EnsembleBase {
     cudaStream_t user = st;
     st = cap_st;
     check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+    capturing = true;
     one_step(first);
+    capturing = false;
     const cudaError_t ce = cudaStreamEndCapture(st, &graph);
     st = user;
     check(ce, "end capture");
@@ -1587,6 +1623,27 @@ struct EnsembleImpl : EnsembleBase {
     state_out<R>(s[cur], n, ax, ay, az, p.softening, p.star_mass, v, as_double, acc, on_device,
                  out_stage, st);
     launches += 1;
+  }
+
+  // copyToGPU, nsteps, copyToCPU; the positions go back on the read-back
+  // stream as soon as the last permute has run.
+  void step_host(double* const* v, float* const* acc, const float* mass, int nsteps) override {
+    const int steps0 = has_state ? steps_done : 0;
+    const void* vin[6] = {v[0], v[1], v[2], v[3], v[4], v[5]};
+    const float* ain[3] = {acc[0], acc[1], acc[2]};
+    set_state(vin, true, mass, false, false);
+    load_accel(ain);
+    steps_done = steps0;  // the caller's clock continues
+    if (nsteps <= 0) {
+      void* vout[6] = {v[0], v[1], v[2], v[3], v[4], v[5]};
+      get_state(vout, true, acc, false);
+      return;
+    }
+    step(nsteps);
+    if (!out_stage) out_stage = dalloc<char>(out_stage_bytes(n), "output staging");
+    read_back_split<R, double>(s[cur], n, ax, ay, az, p.softening, p.star_mass, v, acc,
+                               out_stage, ev_pos, rb_st, st);
+    launches += 2;
   }
 
   // Candidates are (targets per lane, leaf size, walk mode) triples.
@@ -1784,17 +1841,9 @@ int nbody_ensemble_step_host(nbody_ensemble* e, double* x, double* y, double* z,
     NBODY_REQUIRE(e && x && y && z && vx && vy && vz && ax && ay && az && mass,
                   "nbody_ensemble_step_host: null array");
     NBODY_REQUIRE(nsteps >= 0, "nbody_ensemble_step_host: negative step count");
-    nb::EnsembleBase* b = e->impl;
-    const int steps0 = b->has_state ? b->steps_done : 0;
-    const void* v[6] = {x, y, z, vx, vy, vz};
-    const float* a[3] = {ax, ay, az};
-    b->set_state(v, true, mass, false, false);
-    b->load_accel(a);
-    b->steps_done = steps0;  // the caller's clock continues
-    b->step(nsteps);
-    void* o[6] = {x, y, z, vx, vy, vz};
-    float* ao[3] = {ax, ay, az};
-    b->get_state(o, true, ao, false);
+    double* v[6] = {x, y, z, vx, vy, vz};
+    float* a[3] = {ax, ay, az};
+    e->impl->step_host(v, a, mass, nsteps);  // copyToGPU, nsteps, copyToCPU
   })
 }
 

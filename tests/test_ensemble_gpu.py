@@ -203,3 +203,29 @@ def test_ensemble_fused_collisions_match_the_separate_pass(nb, cuda):
         assert np.abs(out[0][k] - out[1][k]).max() < 1e-5, k
     for k in ("x", "y", "z"):
         assert np.abs(out[0][k] - out[1][k]).max() < 1e-7, k
+
+
+def test_ensemble_step_host_read_back_equals_get_state(nb, cuda):
+    """nbody_ensemble_step_host reads the positions back on a second stream
+    while the steps finish; what it returns must be the final state, as
+    get_state reads it afterwards, bit for bit, over two calls in a row."""
+    prm = params(nb, 1)
+    st, m = wl.ensemble_state(nb, SPECS)
+    e = nb.Ensemble(prm, SPECS)
+    e.set_state(st["x"], st["y"], st["z"], st["vx"], st["vy"], st["vz"], m)
+    g = e.get_state(double=False, accel=True)
+    host = {k: np.ascontiguousarray(st[k], np.float64) for k in ("x", "y", "z", "vx", "vy", "vz")}
+    for k in ("ax", "ay", "az"):
+        host[k] = np.ascontiguousarray(g[k], np.float32)
+    for nsteps in (1, 3):
+        before = host["x"].copy()
+        e.step_host(host, m, nsteps)
+        got = e.get_state(double=True, accel=False)
+        acc = e.get_state(double=False, accel=True)
+        for k in ("x", "y", "z", "vx", "vy", "vz"):
+            assert np.array_equal(host[k], got[k]), (nsteps, k)
+        for k in ("ax", "ay", "az"):
+            assert np.array_equal(host[k], acc[k]), (nsteps, k)
+        assert not np.array_equal(host["x"], before)
+    assert e.stats().status == 0
+    e.close()
