@@ -737,8 +737,6 @@ struct SimImpl : SimBase {
     else
       launch_tree<uint32_t>(tw, tw.keys, n, 30, 0, 1, tw.geom, nullptr, nullptr, nullptr, nullptr,
                             st);
-    check(cudaMemsetAsync(inter, 0, sizeof(unsigned long long), st), "inter reset");
-    check(cudaMemsetAsync(counters, 0, 3 * sizeof(unsigned long long), st), "counters reset");
     WalkArgs w{};
     w.com = tw.oct.com; w.info = tw.oct.info; w.body = tw.body4; w.n = n;
     w.groups = tw.groups; w.n_groups = tw.n_groups;
@@ -767,8 +765,8 @@ struct SimImpl : SimBase {
     mark(NBODY_PHASE_COLLIDE);
     // keys (+ digit histograms), bbox reset, digit offsets, 4 one-sweep
     // passes, permute, karras, mark, tile scan, apply, moment tiles, moment
-    // tile scan, emit, walk
-    launches += 16;
+    // tile scan, emit, walk reset, walk
+    launches += 17;
   }
 
   // Collisions inside the walk (one warp per group of <= 32 targets).
@@ -1483,8 +1481,6 @@ struct EnsembleImpl : EnsembleBase {
     else
       launch_tree<uint64_t>(tw, keys64, n, key_bits, disk_bits, D, geoms, group_disk, nullptr,
                             nullptr, nullptr, st);
-    check(cudaMemsetAsync(inter, 0, sizeof(unsigned long long), st), "inter reset");
-    check(cudaMemsetAsync(counters, 0, 3 * sizeof(unsigned long long), st), "counters reset");
     WalkArgs w{};
     w.com = tw.oct.com; w.info = tw.oct.info; w.body = tw.body4; w.n = n;
     w.groups = tw.groups; w.n_groups = tw.n_groups;
@@ -1515,8 +1511,8 @@ struct EnsembleImpl : EnsembleBase {
     if (side_coll) check(cudaStreamWaitEvent(st, cs.join, 0), "collision join");
     // geoms, keys (+ digit histograms), bbox reset, digit offsets, one
     // one-sweep kernel per pass, permute, karras, mark, tile scan, apply,
-    // moment tiles, moment tile scan, emit, walk
-    launches += 3 + 1 + (key_bits + 7) / 8 + 9;
+    // moment tiles, moment tile scan, emit, walk reset, walk
+    launches += 3 + 1 + (key_bits + 7) / 8 + 10;
   }
 
   void collide(cudaStream_t on, int* wk, int* sp) {

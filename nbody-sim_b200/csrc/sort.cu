@@ -129,7 +129,8 @@ __global__ void __launch_bounds__(kSortThreads)
 k_onesweep(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
            K* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int n, int shift,
            const uint32_t* __restrict__ digit_base, int* __restrict__ ticket,
-           uint32_t* __restrict__ status, int* __restrict__ err) {
+           uint32_t* __restrict__ status, int* __restrict__ err,
+           uint32_t* __restrict__ clear_next) {
   constexpr int kTile = kSortThreads * kItems;
   __shared__ uint32_t s_cnt[kSortWarps][kBins];
   __shared__ K s_keys[kTile];
@@ -144,6 +145,9 @@ k_onesweep(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
   if (tid == 0) s_tile = atomicAdd(ticket, 1);
   __syncthreads();
   const int t = s_tile;
+  // the next pass's status words of this tile (the pass before last used
+  // them, and it has finished)
+  if (clear_next) clear_next[(size_t)t * kBins + tid] = 0u;
 
   const long long tile0 = (long long)t * kTile;
   const long long wbase = tile0 + (long long)warp * (kWarp * kItems);
@@ -352,21 +356,27 @@ int pick_items(int n) {
 template <typename K, int kItems>
 void launch_onesweep(int ntiles, const K* ki, const uint32_t* vi, K* ko, uint32_t* vo, int n,
                      int shift, const uint32_t* base, int* ticket, uint32_t* st, int* err,
-                     cudaStream_t s) {
+                     uint32_t* clear_next, cudaStream_t s) {
   k_onesweep<K, kItems><<<ntiles, kSortThreads, 0, s>>>(ki, vi, ko, vo, n, shift, base, ticket,
-                                                        st, err);
+                                                        st, err, clear_next);
 }
 
 template <typename K>
 void launch_onesweep_items(int items, int ntiles, const K* ki, const uint32_t* vi, K* ko,
                            uint32_t* vo, int n, int shift, const uint32_t* base, int* ticket,
-                           uint32_t* st, int* err, cudaStream_t s) {
+                           uint32_t* st, int* err, uint32_t* clear_next, cudaStream_t s) {
   if constexpr (sizeof(K) == 4) {
-    if (items == 16) return launch_onesweep<K, 16>(ntiles, ki, vi, ko, vo, n, shift, base, ticket, st, err, s);
+    if (items == 16)
+      return launch_onesweep<K, 16>(ntiles, ki, vi, ko, vo, n, shift, base, ticket, st, err,
+                                    clear_next, s);
   }
-  if (items == 8) return launch_onesweep<K, 8>(ntiles, ki, vi, ko, vo, n, shift, base, ticket, st, err, s);
-  if (items == 4) return launch_onesweep<K, 4>(ntiles, ki, vi, ko, vo, n, shift, base, ticket, st, err, s);
-  launch_onesweep<K, 2>(ntiles, ki, vi, ko, vo, n, shift, base, ticket, st, err, s);
+  if (items == 8)
+    return launch_onesweep<K, 8>(ntiles, ki, vi, ko, vo, n, shift, base, ticket, st, err,
+                                 clear_next, s);
+  if (items == 4)
+    return launch_onesweep<K, 4>(ntiles, ki, vi, ko, vo, n, shift, base, ticket, st, err,
+                                 clear_next, s);
+  launch_onesweep<K, 2>(ntiles, ki, vi, ko, vo, n, shift, base, ticket, st, err, clear_next, s);
 }
 
 }  // namespace
@@ -409,11 +419,18 @@ void radix_sort_pairs(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt,
   k_digit_offsets<<<passes, kBins, 0, s>>>(hist);
   K *ki = keys, *ko = keys_alt;
   uint32_t *vi = vals, *vo = vals_alt;
+  // Two status buffers when the scratch holds them (it is sized for the
+  // smallest tiles): each pass clears the other buffer's words of its own
+  // tiles for the pass after it, so only the first needs a memset.
+  const size_t tile_words = (size_t)ntiles * kBins;
+  const bool two = 2 * (size_t)ntiles <= (size_t)div_up(n, kMinTile);
   for (int p = 0; p < passes; ++p) {
-    check(cudaMemsetAsync(st, 0, sizeof(uint32_t) * (size_t)ntiles * kBins, s),
-          "radix sort status reset");
+    uint32_t* cur = (two && (p & 1)) ? st + tile_words : st;
+    uint32_t* next = (two && p + 1 < passes) ? ((p & 1) ? st : st + tile_words) : nullptr;
+    if (p == 0 || !two)
+      check(cudaMemsetAsync(cur, 0, sizeof(uint32_t) * tile_words, s), "radix sort status reset");
     launch_onesweep_items<K>(items, ntiles, ki, vi, ko, vo, n, 8 * p, hist + (size_t)p * kBins,
-                             tickets + p, st, err, s);
+                             tickets + p, cur, err, next, s);
     K* t = ki; ki = ko; ko = t;
     uint32_t* u = vi; vi = vo; vo = u;
   }

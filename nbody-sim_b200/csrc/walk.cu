@@ -625,9 +625,19 @@ int walk_spill_slots(int) {
   return num_sms() * std::max(b, bc) * kWalkWarps;
 }
 
+// The walk's group counter and statistics, zeroed by one launch (three
+// memset nodes in a step graph cost more than this).
+__global__ void k_walk_reset(int* work, unsigned long long* inter, unsigned long long* counters) {
+  const int t = threadIdx.x;
+  if (t == 0) *work = 0;
+  if (t == 1 && inter) *inter = 0ull;
+  if (t >= 2 && t < 5 && counters) counters[t - 2] = 0ull;
+}
+
 void launch_walk(const WalkArgs& a, cudaStream_t s) {
   if (a.n <= 0) return;
-  check(cudaMemsetAsync(a.work, 0, sizeof(int), s), "walk work reset");
+  k_walk_reset<<<1, 32, 0, s>>>(a.work, a.inter, a.counters);
+  check(cudaGetLastError(), "walk reset launch");
   const bool soft = a.eps > 0.f;
   if (a.tape) {  // recording: groups of <= 32 targets
     if (soft) launch_variant<true, 1, true>(a, s);
