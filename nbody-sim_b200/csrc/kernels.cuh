@@ -82,6 +82,9 @@ struct TreeWork {
   // parallel branches).  Created by tree_enable_overlap; null: one stream.
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // The Karras pass also sets the octree-parent words to -1 (host-side flag:
+  // the next octree build over that tree needs no reset of its own).
+  bool opar_fresh = false;
 };
 
 void tree_alloc(TreeWork& w, int cap);

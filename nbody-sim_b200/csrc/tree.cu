@@ -224,9 +224,13 @@ template <typename K>
 __global__ void __launch_bounds__(kThreads)
 k_karras(const K* __restrict__ keys, int n, int key_bits, int* __restrict__ left,
          int* __restrict__ right, int* __restrict__ parent, int* __restrict__ lo_out,
-         int* __restrict__ hi_out, uint8_t* __restrict__ prefix) {
+         int* __restrict__ hi_out, uint8_t* __restrict__ prefix, int* __restrict__ opar) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n - 1) return;
+  // octree parents of the records the build will write: none yet
+  opar[i] = -1;
+  opar[n - 1 + i] = -1;
+  if (i == 0) opar[2 * n - 2] = -1;
   const K ki = __ldg(keys + i);
   const int d = (delta(keys, n, ki, i, i + 1) - delta(keys, n, ki, i, i - 1)) > 0 ? 1 : -1;
   const int dmin = delta(keys, n, ki, i, i - d);
@@ -860,8 +864,9 @@ void launch_karras(TreeWork& w, const K* keys, int n, int key_bits, cudaStream_t
   if (n < 2) return;
   k_karras<K><<<grid_for(n - 1), kThreads, 0, s>>>(keys, n, key_bits, w.bin_left, w.bin_right,
                                                    w.bin_parent, w.bin_lo, w.bin_hi,
-                                                   w.bin_prefix);
+                                                   w.bin_prefix, (int*)w.group_flag);
   check(cudaGetLastError(), "k_karras launch");
+  w.opar_fresh = true;
 }
 
 template <typename K>
@@ -888,7 +893,9 @@ void launch_octree(TreeWork& w, const K* keys, int n, int disk_bits, int n_roots
   int* opar = (int*)w.group_flag;
   unsigned long long* tsum = (unsigned long long*)w.scan_tmp;
   const int mtiles = div_up(nb, kMarkTile);
-  check(cudaMemsetAsync(opar, 0xff, sizeof(int) * (size_t)nb, s), "octree parent reset");
+  if (!w.opar_fresh)  // set by the Karras pass before the first octree build over it
+    check(cudaMemsetAsync(opar, 0xff, sizeof(int) * (size_t)nb, s), "octree parent reset");
+  w.opar_fresh = false;
   MarkArgs<K> m{n, gmax, gspan, w.prune_max, disk_bits, w.bin_left, w.bin_right, w.bin_parent,
                 w.bin_lo, w.bin_hi, w.bin_prefix, w.oct_nch, w.oct_off, opar, w.oct_cidx, tsum};
   k_mark<K><<<mtiles, kMarkTile, 0, s>>>(m);
