@@ -763,10 +763,10 @@ struct SimImpl : SimBase {
     launch_walk(w, st);
     if (side_coll) check(cudaStreamWaitEvent(st, cs.join, 0), "collision join");
     mark(NBODY_PHASE_COLLIDE);
-    // keys (+ digit histograms), bbox reset, digit offsets, 4 one-sweep
-    // passes, permute, karras, mark, tile scan, apply, moment tiles, moment
-    // tile scan, emit, walk reset, walk
-    launches += 17;
+    // keys (+ digit histograms), bbox reset, 4 one-sweep passes, permute,
+    // karras, mark, tile scan, apply, moment tiles, moment tile scan, emit,
+    // walk reset, walk
+    launches += 16;
   }
 
   // Collisions inside the walk (one warp per group of <= 32 targets).
@@ -1509,10 +1509,10 @@ struct EnsembleImpl : EnsembleBase {
     }
     launch_walk(w, st);
     if (side_coll) check(cudaStreamWaitEvent(st, cs.join, 0), "collision join");
-    // geoms, keys (+ digit histograms), bbox reset, digit offsets, one
-    // one-sweep kernel per pass, permute, karras, mark, tile scan, apply,
-    // moment tiles, moment tile scan, emit, walk reset, walk
-    launches += 3 + 1 + (key_bits + 7) / 8 + 10;
+    // geoms, keys (+ digit histograms), bbox reset, one one-sweep kernel per
+    // pass, permute, karras, mark, tile scan, apply, moment tiles, moment
+    // tile scan, emit, walk reset, walk
+    launches += 3 + (key_bits + 7) / 8 + 10;
   }
 
   void collide(cudaStream_t on, int* wk, int* sp) {

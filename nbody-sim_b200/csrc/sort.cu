@@ -4,9 +4,10 @@
 // Replaces the reference's serial DFS ordering (bhtree_sortKernel,
 // BHTree.cu:322-352, a <<<1,1>>> launch) by a Morton-order sort: the body
 // order of the octree IS the sorted key order.  Digits are 8 bits.
-//   * one histogram kernel counts the digits of every pass in a single read
-//     of the keys (a digit's count does not depend on the key order), and a
-//     tiny kernel turns them into each pass's global digit offsets;
+//   * the digits of every pass are counted in a single read of the keys (a
+//     digit's count does not depend on the key order), by a histogram kernel
+//     or by the kernel that wrote the keys; every tile of a pass scans its
+//     pass's 256 counts into the global digit offsets;
 //   * one kernel per pass: a block takes the next tile (atomic ticket, so
 //     tiles start in order), ranks its keys with __match_any_sync, publishes
 //     its per-digit counts, and finds the counts of all earlier tiles by
@@ -103,24 +104,6 @@ k_digit_hist(const K* __restrict__ keys, int n, int passes, uint32_t* __restrict
   hist_flush(s_h, passes, hist);
 }
 
-// Exclusive scan of each pass's 256 digit counts (one block per pass).
-__global__ void __launch_bounds__(kBins) k_digit_offsets(uint32_t* __restrict__ hist) {
-  __shared__ uint32_t s_w[kBins / 32];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  uint32_t* h = hist + (size_t)blockIdx.x * kBins;
-  const uint32_t c = h[tid];
-  uint32_t v = c;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t t = __shfl_up_sync(kFull, v, o);
-    if (lane >= o) v += t;
-  }
-  if (lane == 31) s_w[warp] = v;
-  __syncthreads();
-  uint32_t add = 0;
-  for (int w = 0; w < warp; ++w) add += s_w[w];
-  h[tid] = v - c + add;
-}
 
 // One pass: rank a tile, publish, look back, scatter.  ticket and status
 // (ntiles x 256 words) start at zero.
@@ -128,7 +111,7 @@ template <typename K, int kItems>
 __global__ void __launch_bounds__(kSortThreads)
 k_onesweep(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
            K* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int n, int shift,
-           const uint32_t* __restrict__ digit_base, int* __restrict__ ticket,
+           const uint32_t* __restrict__ digit_count, int* __restrict__ ticket,
            uint32_t* __restrict__ status, int* __restrict__ err,
            uint32_t* __restrict__ clear_next) {
   constexpr int kTile = kSortThreads * kItems;
@@ -138,6 +121,7 @@ k_onesweep(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
   __shared__ uint32_t s_base[kBins];
   __shared__ uint32_t s_glob[kBins];
   __shared__ uint32_t s_wsum[kSortWarps];
+  __shared__ uint32_t s_hsum[kSortWarps];
   __shared__ int s_tile;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -148,6 +132,16 @@ k_onesweep(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
   // the next pass's status words of this tile (the pass before last used
   // them, and it has finished)
   if (clear_next) clear_next[(size_t)t * kBins + tid] = 0u;
+  // the pass's global digit offsets: an exclusive scan of its digit counts,
+  // redone by every tile (256 words) instead of a kernel of its own
+  const uint32_t hcount = __ldg(digit_count + tid);
+  uint32_t hincl = hcount;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t q = __shfl_up_sync(kFull, hincl, o);
+    if (lane >= o) hincl += q;
+  }
+  if (lane == 31) s_hsum[warp] = hincl;  // read after the ranking's barrier
 
   const long long tile0 = (long long)t * kTile;
   const long long wbase = tile0 + (long long)warp * (kWarp * kItems);
@@ -225,7 +219,9 @@ k_onesweep(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
       }
       atomicExch(mine, kFlagP | ((excl + run) & kValMask));
     }
-    s_glob[d] = digit_base[d] + excl;
+    uint32_t gbase = hincl - hcount;
+    for (int w = 0; w < warp; ++w) gbase += s_hsum[w];
+    s_glob[d] = gbase + excl;
     // tile-local base of digit d: exclusive prefix over digits
     uint32_t v = run;
 #pragma unroll
@@ -383,7 +379,7 @@ void launch_onesweep_items(int items, int ntiles, const K* ki, const uint32_t* v
 
 size_t scan_tmp_words(int n);
 
-// Scratch of the sort: per-pass digit offsets (passes x 256), per-pass tile
+// Scratch of the sort: per-pass digit counts (passes x 256), per-pass tile
 // tickets (passes), one word for give-up reports when the caller passes no
 // status word, then the tile status words of one pass (ntiles x 256, cleared
 // before every pass).  Sized for the smallest tiles.
@@ -416,7 +412,6 @@ void radix_sort_pairs(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt,
     const int hgrid = std::max(1, std::min(div_up(n, kSortThreads * 8), 148 * 4));
     k_digit_hist<K><<<hgrid, kSortThreads, 0, s>>>(keys, n, passes, hist);
   }
-  k_digit_offsets<<<passes, kBins, 0, s>>>(hist);
   K *ki = keys, *ko = keys_alt;
   uint32_t *vi = vals, *vo = vals_alt;
   // Two status buffers when the scratch holds them (it is sized for the
