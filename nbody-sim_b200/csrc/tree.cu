@@ -217,9 +217,10 @@ __device__ __forceinline__ int delta(const K* __restrict__ keys, int n, K ki, in
 
 // key_bits: the low bits of K the keys use (30 Morton bits, plus the disk
 // index above them for an ensemble).  prefix[] stores the common prefix in
-// those bits, key_bits for runs of equal keys.  (Staging the block's keys
-// and a halo in shared memory made this kernel slower at N = 2^20: 35 -> 39
-// us; the searches are not what bounds it.)
+// those bits, key_bits for runs of equal keys.  Tried and slower at N = 2^20:
+// staging the block's keys and a halo in shared memory (35 -> 39 us), and a
+// bottom-up agglomerative build (Apetrei 2014; 130 us: the last climbers'
+// chains of atomics and fences run the depth of the tree).
 template <typename K>
 __global__ void __launch_bounds__(kThreads)
 k_karras(const K* __restrict__ keys, int n, int key_bits, int* __restrict__ left,
