@@ -172,3 +172,39 @@ def test_oracle_direct_sum_symmetry(port):
     ax, ay, az = port.direct_f64(p[:, 0], p[:, 1], p[:, 2], m, np.arange(n), 1e-3, 1.0, False)
     tot = np.array([np.dot(m, ax), np.dot(m, ay), np.dot(m, az)])
     assert np.abs(tot).max() < 1e-12 * np.abs(m).sum() ** 2 / 1e-6 + 1e-18
+
+
+def test_oracle_collision_pairs_against_brute_force(port):
+    """orc_collision_pairs (the reference's collision traversal, counted): it
+    never reports more pairs than exist, finds them all on a uniform cloud,
+    and skips some on clustered data, where a cell's centre of mass can lie
+    away from a body that touches one of its members (BHTree.cu:663-665)."""
+    def brute(x, y, z, r):
+        n = len(x)
+        total = 0
+        for i0 in range(0, n, 500):
+            i1 = min(n, i0 + 500)
+            dx = x[None, :] - x[i0:i1, None]
+            dy = y[None, :] - y[i0:i1, None]
+            dz = z[None, :] - z[i0:i1, None]
+            close = (dx * dx + dy * dy + dz * dz) < r * r
+            close[np.arange(i1 - i0), np.arange(i0, i1)] = False
+            total += int(close.sum())
+        return total
+
+    rng = np.random.default_rng(3)
+    n, r = 2000, np.float32(0.01)
+    pos = rng.random((n, 3)).astype(np.float32) * np.float32(0.2)
+    x, y, z = [np.ascontiguousarray(pos[:, k]) for k in range(3)]
+    m = np.full(n, 1e-9, np.float32)
+    b = brute(x, y, z, r)
+    assert b > 100
+    assert port.collision_pairs(x, y, z, m, r) == b
+    centers = rng.random((40, 3)) * 0.05
+    pos = (centers[rng.integers(0, 40, 4000)] + rng.standard_normal((4000, 3)) * 0.002)
+    pos = pos.astype(np.float32)
+    x, y, z = [np.ascontiguousarray(pos[:, k]) for k in range(3)]
+    m = np.full(4000, 1e-9, np.float32)
+    b = brute(x, y, z, np.float32(0.002))
+    found = port.collision_pairs(x, y, z, m, np.float32(0.002))
+    assert 0 < b - found < b // 100
