@@ -15,9 +15,9 @@
 // Accepted nodes (and single bodies) are appended to a shared-memory source list; nodes that must be
 // opened either push their contiguous children or, when they hold at most
 // leaf_max bodies, append those bodies.  Each full batch of 32 sources is
-// evaluated by all 32 lanes for their own target, reading the source from
-// shared memory as a broadcast: 12 FP32 instructions + 1 MUFU.RSQ per
-// interaction.  The softened self term is exactly zero (d = 0), so no
+// evaluated by all 32 lanes for their own target, reading four sources at a
+// time from shared memory as broadcasts and computing in packed FP32
+// (f32x2): 6 packed instructions + 1 MUFU.RSQ per interaction.  The softened self term is exactly zero (d = 0), so no
 // self-skip test is needed when softening > 0.
 //
 // The stack spills to a per-warp global area when it would overflow; a
@@ -46,7 +46,9 @@ constexpr int kStk = 384;
 constexpr int kList = 64;
 
 struct WarpSmem {
-  float4 lst[kList];
+  // source list, one row per component (x, y, z, mass): four consecutive
+  // sources of a row are one 16-byte broadcast holding two register pairs
+  float lsrc[4][kList];
   int lidx[kList];  // fused collisions: body index of each single-body source, else -1
   float4 ext[6];  // the group's targets of least / greatest x, y, z (vote prefilter)
   int stk[kStk];
@@ -55,40 +57,105 @@ struct WarpSmem {
   int sc_body[32];  // recording walks: body index of each leaf-body entry
 };
 
+__device__ __forceinline__ void lst_put(WarpSmem& w, int j, const float4 s) {
+  w.lsrc[0][j] = s.x;
+  w.lsrc[1][j] = s.y;
+  w.lsrc[2][j] = s.z;
+  w.lsrc[3][j] = s.w;
+}
+
+__device__ __forceinline__ float4 lst_get(const WarpSmem& w, int j) {
+  return make_float4(w.lsrc[0][j], w.lsrc[1][j], w.lsrc[2][j], w.lsrc[3][j]);
+}
+
+__device__ __forceinline__ float4 lst_row4(const WarpSmem& w, int c, int j) {
+  return *reinterpret_cast<const float4*>(&w.lsrc[c][j]);
+}
+
 // Squared distance in one fixed rounding, so that the vote and its
 // prefilter test a target identically.
 __device__ __forceinline__ float dist2(float dx, float dy, float dz) {
   return fmaf(dx, dx, fmaf(dy, dy, __fmul_rn(dz, dz)));
 }
 
-// All lanes evaluate sources lst[0..cnt) for their kT targets; every source
-// is one shared-memory broadcast that feeds kT interaction chains.
-template <bool kSoft, int kT, int kCount>
-__device__ __forceinline__ void eval_list(const float4* lst, int cnt, const float4 (&me)[kT],
-                                          float eps2, float3 (&acc)[kT]) {
-  if (kCount > 0) {
+// Sources j .. j+3 (j a multiple of 4) against the lane's kT targets: two
+// packed interactions per target, sources j, j+2 in the .x halves of the
+// accumulators and j+1, j+3 in the .y halves.  kRmin: also the least
+// softened r^2 seen.
+template <bool kSoft, int kT, bool kRmin>
+__device__ __forceinline__ void eval_quad(const WarpSmem& w, int j, const PairTgt (&pt)[kT],
+                                          const float2 e2, PairAcc (&acc)[kT], float& rmin) {
+  const float4 qx = lst_row4(w, 0, j), qy = lst_row4(w, 1, j);
+  const float4 qz = lst_row4(w, 2, j), qm = lst_row4(w, 3, j);
 #pragma unroll
-    for (int j = 0; j < kCount; ++j) {
-      const float4 src = lst[j];
-#pragma unroll
-      for (int t = 0; t < kT; ++t) interact<kSoft>(src, me[t], eps2, acc[t]);
-    }
-  } else {
-    for (int j = 0; j < cnt; ++j) {
-      const float4 src = lst[j];
-#pragma unroll
-      for (int t = 0; t < kT; ++t) interact<kSoft>(src, me[t], eps2, acc[t]);
-    }
+  for (int t = 0; t < kT; ++t) {
+    const float2 r0 = interact2<kSoft>(make_float2(qx.x, qx.y), make_float2(qy.x, qy.y),
+                                       make_float2(qz.x, qz.y), make_float2(qm.x, qm.y), pt[t],
+                                       e2, acc[t]);
+    const float2 r1 = interact2<kSoft>(make_float2(qx.z, qx.w), make_float2(qy.z, qy.w),
+                                       make_float2(qz.z, qz.w), make_float2(qm.z, qm.w), pt[t],
+                                       e2, acc[t]);
+    if (kRmin) rmin = fminf(rmin, fminf(fminf(r0.x, r0.y), fminf(r1.x, r1.y)));
   }
 }
 
-// Drops the first 32 entries of the list (caller guarantees nlist >= 32).
-__device__ __forceinline__ void list_shift(float4* lst, int nlist, int lane) {
-  const int rem = nlist - 32;
-  float4 t;
-  if (lane < rem) t = lst[32 + lane];
+// One source in scalar FP32 into the .x halves.
+template <bool kSoft, int kT, bool kRmin>
+__device__ __forceinline__ void eval_one(const WarpSmem& w, int j, const float4 (&me)[kT],
+                                         float eps2, PairAcc (&acc)[kT], float& rmin) {
+  const float4 s = lst_get(w, j);
+#pragma unroll
+  for (int t = 0; t < kT; ++t) {
+    if (kRmin) {
+      const float dx = s.x - me[t].x, dy = s.y - me[t].y, dz = s.z - me[t].z;
+      rmin = fminf(rmin, fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2))));
+    }
+    float3 a3 = make_float3(acc[t].x.x, acc[t].y.x, acc[t].z.x);
+    interact<kSoft>(s, me[t], eps2, a3);
+    acc[t].x.x = a3.x;
+    acc[t].y.x = a3.y;
+    acc[t].z.x = a3.z;
+  }
+}
+
+// All lanes evaluate sources 0 .. cnt of the list for their kT targets
+// (kCount > 0: exactly kCount, a multiple of 4): each quad of sources is four
+// shared-memory broadcasts feeding 2 kT packed interaction chains; a tail of
+// fewer than four goes through eval_one.  kSeq (recording walks): every
+// source through eval_one, in list order, as the tape replay sums them.
+// Returns the least softened r^2 when kRmin.
+template <bool kSoft, int kT, int kCount, bool kRmin = false, bool kSeq = false>
+__device__ __forceinline__ float eval_list(const WarpSmem& w, int cnt, const float4 (&me)[kT],
+                                           const PairTgt (&pt)[kT], float eps2, const float2 e2,
+                                           PairAcc (&acc)[kT]) {
+  static_assert(kCount % 4 == 0, "full batches are whole quads");
+  float rmin = INFINITY;
+  if (kSeq) {
+    const int c = (kCount > 0) ? kCount : cnt;
+    for (int j = 0; j < c; ++j) eval_one<kSoft, kT, kRmin>(w, j, me, eps2, acc, rmin);
+  } else if (kCount > 0) {
+#pragma unroll
+    for (int j = 0; j < kCount; j += 4) eval_quad<kSoft, kT, kRmin>(w, j, pt, e2, acc, rmin);
+  } else {
+    int j = 0;
+    for (; j + 4 <= cnt; j += 4) eval_quad<kSoft, kT, kRmin>(w, j, pt, e2, acc, rmin);
+    for (; j < cnt; ++j) eval_one<kSoft, kT, kRmin>(w, j, me, eps2, acc, rmin);
+  }
+  return rmin;
+}
+
+// Drops the first 32 entries of the list (and, with fused collisions, of
+// their body indices): each lane moves one 16-byte piece of one row; the
+// entries past the list's end that move with them are never read.
+template <bool kColl>
+__device__ __forceinline__ void list_shift(WarpSmem& w, int lane) {
+  const int row = lane >> 3, q = (lane & 7) * 4;
+  const float4 t = lst_row4(w, row, 32 + q);
+  int b = -1;
+  if (kColl) b = w.lidx[32 + lane];
   __syncwarp();
-  if (lane < rem) lst[lane] = t;
+  *reinterpret_cast<float4*>(&w.lsrc[row][q]) = t;
+  if (kColl) w.lidx[lane] = b;
   __syncwarp();
 }
 
@@ -100,16 +167,16 @@ struct CollLane {
   float dvx, dvy, dvz;
 };
 
-// Collision sweep of a batch lst[0..cnt): every single-body source closer
-// than r_coll to the lane's target adds its impulse (coll_dist2 and
+// Collision sweep of a batch 0 .. cnt of the list: every single-body source
+// closer than r_coll to the lane's target adds its impulse (coll_dist2 and
 // coll_impulse, as the stand-alone neighbour search).
-__device__ __forceinline__ void coll_batch(const WalkArgs& a, const float4* lst, const int* lidx,
-                                           int cnt, const float4 me, bool valid, float rc2,
+__device__ __forceinline__ void coll_batch(const WalkArgs& a, const WarpSmem& w, int cnt,
+                                           const float4 me, bool valid, float rc2,
                                            CollLane& cl) {
   for (int j = 0; j < cnt; ++j) {
-    const int b = lidx[j];
+    const int b = w.lidx[j];
     if (b < 0) continue;
-    const float4 s = lst[j];
+    const float4 s = lst_get(w, j);
     const float dx = s.x - me.x, dy = s.y - me.y, dz = s.z - me.z;
     const float d2 = coll_dist2(dx, dy, dz);
     if (valid && b != cl.self && d2 < rc2)
@@ -118,46 +185,6 @@ __device__ __forceinline__ void coll_batch(const WalkArgs& a, const float4* lst,
                    coll_vel(a.coll_v[2], a.coll_vtype, b) - cl.vz, a.coll_e, cl.dvx, cl.dvy,
                    cl.dvz);
   }
-}
-
-// Gravity of a batch as eval_list, plus the least softened squared distance
-// seen (a batch whose least distance is beyond r_coll has no collision).
-template <bool kSoft>
-__device__ __forceinline__ void interact_rmin(const float4 src, const float4 me, float eps2,
-                                              float3& acc, float& rmin) {
-  const float dx = src.x - me.x, dy = src.y - me.y, dz = src.z - me.z;
-  rmin = fminf(rmin, fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2))));
-  interact<kSoft>(src, me, eps2, acc);
-}
-
-template <bool kSoft, int kCount>
-__device__ __forceinline__ float eval_list_rmin(const float4* lst, int cnt, const float4 me,
-                                                float eps2, float3& acc) {
-  float rmin = INFINITY;
-  if (kCount > 0) {
-#pragma unroll
-    for (int j = 0; j < kCount; ++j) interact_rmin<kSoft>(lst[j], me, eps2, acc, rmin);
-  } else {
-    for (int j = 0; j < cnt; ++j) interact_rmin<kSoft>(lst[j], me, eps2, acc, rmin);
-  }
-  return rmin;
-}
-
-// Drops the first 32 entries of the list and of its body indices.
-__device__ __forceinline__ void list_shift_idx(float4* lst, int* lidx, int nlist, int lane) {
-  const int rem = nlist - 32;
-  float4 t;
-  int b = -1;
-  if (lane < rem) {
-    t = lst[32 + lane];
-    b = lidx[32 + lane];
-  }
-  __syncwarp();
-  if (lane < rem) {
-    lst[lane] = t;
-    lidx[lane] = b;
-  }
-  __syncwarp();
 }
 
 // Tape of a group's source list (recording walks): the entries, in the
@@ -294,9 +321,16 @@ __global__ void __launch_bounds__(kWalkWarps * 32, walk_min_blocks<kMode>())
     // The tree sum starts from zero: adding ~10^3 terms into an accumulator
     // that already holds the star pull (10^3-10^5 times larger) would round
     // every term at the star's ulp.  Star and perturber are added at the end.
-    float3 acc[kT];
+    PairAcc acc[kT];
+    PairTgt pt[kT];
 #pragma unroll
-    for (int t = 0; t < kT; ++t) acc[t] = make_float3(0.f, 0.f, 0.f);
+    for (int t = 0; t < kT; ++t) {
+      acc[t].x = acc[t].y = acc[t].z = make_float2(0.f, 0.f);
+      pt[t].x = make_float2(-me[t].x, -me[t].x);
+      pt[t].y = make_float2(-me[t].y, -me[t].y);
+      pt[t].z = make_float2(-me[t].z, -me[t].z);
+    }
+    const float2 e2 = make_float2(eps2, eps2);
     unsigned long long visited = 0, spills = 0, evaluated = 0;
     int top = 1, spilled = 0, nlist = 0;
     bool overflow = false;
@@ -420,7 +454,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, walk_min_blocks<kMode>())
       const unsigned m1 = __ballot_sync(kFull, act == 1);
       if (act == 1) {
         const int pos = nlist + __popc(m1 & lanemask_lt());
-        w.lst[pos] = c;
+        lst_put(w, pos, c);
         if (kColl) w.lidx[pos] = ((ninf.z >> 4) == 1) ? ninf.y : -1;
       }
       if (kRec) {
@@ -431,15 +465,10 @@ __global__ void __launch_bounds__(kWalkWarps * 32, walk_min_blocks<kMode>())
       nlist += __popc(m1);
       __syncwarp();
       if (nlist >= 32) {
-        if (kColl) {
-          const float rmin = eval_list_rmin<kSoft, 32>(w.lst, 32, me[0], eps2, acc[0]);
-          if (__any_sync(kFull, rmin < rthr))
-            coll_batch(a, w.lst, w.lidx, 32, me[0], valid[0], rc2, cl);
-          list_shift_idx(w.lst, w.lidx, nlist, lane);
-        } else {
-          eval_list<kSoft, kT, 32>(w.lst, 32, me, eps2, acc);
-          list_shift(w.lst, nlist, lane);
-        }
+        const float rmin = eval_list<kSoft, kT, 32, kColl, kRec>(w, 32, me, pt, eps2, e2, acc);
+        if (kColl && __any_sync(kFull, rmin < rthr))
+          coll_batch(a, w, 32, me[0], valid[0], rc2, cl);
+        list_shift<kColl>(w, lane);
         evaluated += 32;
         nlist -= 32;
       }
@@ -479,7 +508,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, walk_min_blocks<kMode>())
             for (int step = 16; step > 0; step >>= 1)
               if (w.sc[o + step - 1] <= gi) o += step;
             const int prev = (o > 0) ? w.sc[o - 1] : 0;
-            w.lst[nlist + lane] = __ldg(a.body + w.slo[o] + (gi - prev));
+            lst_put(w, nlist + lane, __ldg(a.body + w.slo[o] + (gi - prev)));
             if (kRec) w.sc_body[lane] = w.slo[o] + (gi - prev);
             if (kColl) w.lidx[nlist + lane] = w.slo[o] + (gi - prev);
           }
@@ -491,15 +520,11 @@ __global__ void __launch_bounds__(kWalkWarps * 32, walk_min_blocks<kMode>())
           nlist += min(32, btotal - base);
           __syncwarp();
           if (nlist >= 32) {
-            if (kColl) {
-              const float rmin = eval_list_rmin<kSoft, 32>(w.lst, 32, me[0], eps2, acc[0]);
-              if (__any_sync(kFull, rmin < rthr))
-                coll_batch(a, w.lst, w.lidx, 32, me[0], valid[0], rc2, cl);
-              list_shift_idx(w.lst, w.lidx, nlist, lane);
-            } else {
-              eval_list<kSoft, kT, 32>(w.lst, 32, me, eps2, acc);
-              list_shift(w.lst, nlist, lane);
-            }
+            const float rmin =
+                eval_list<kSoft, kT, 32, kColl, kRec>(w, 32, me, pt, eps2, e2, acc);
+            if (kColl && __any_sync(kFull, rmin < rthr))
+              coll_batch(a, w, 32, me[0], valid[0], rc2, cl);
+            list_shift<kColl>(w, lane);
             evaluated += 32;
             nlist -= 32;
           }
@@ -507,18 +532,15 @@ __global__ void __launch_bounds__(kWalkWarps * 32, walk_min_blocks<kMode>())
       }
     }
 
+    const float rmin = eval_list<kSoft, kT, 0, kColl, kRec>(w, nlist, me, pt, eps2, e2, acc);
     if (kColl) {
-      const float rmin = eval_list_rmin<kSoft, 0>(w.lst, nlist, me[0], eps2, acc[0]);
-      if (__any_sync(kFull, rmin < rthr))
-        coll_batch(a, w.lst, w.lidx, nlist, me[0], valid[0], rc2, cl);
+      if (__any_sync(kFull, rmin < rthr)) coll_batch(a, w, nlist, me[0], valid[0], rc2, cl);
       if (valid[0]) {
         const int s = gr.x + lane;
         a.coll_dv[0][s] = cl.dvx;
         a.coll_dv[1][s] = cl.dvy;
         a.coll_dv[2][s] = cl.dvz;
       }
-    } else {
-      eval_list<kSoft, kT, 0>(w.lst, nlist, me, eps2, acc);
     }
     evaluated += nlist;
     __syncwarp();
@@ -527,7 +549,10 @@ __global__ void __launch_bounds__(kWalkWarps * 32, walk_min_blocks<kMode>())
     if (a.pert) p = a.pert[(a.pert_step ? *a.pert_step * a.n_disks : 0) + disk];
 #pragma unroll
     for (int t = 0; t < kT; ++t) {
-      float ax = acc[t].x, ay = acc[t].y, az = acc[t].z;
+      // recording walks sum in the .x halves alone, in list order
+      float ax = kRec ? acc[t].x.x : acc[t].x.x + acc[t].x.y;
+      float ay = kRec ? acc[t].y.x : acc[t].y.x + acc[t].y.y;
+      float az = kRec ? acc[t].z.x : acc[t].z.x + acc[t].z.y;
       if (a.star_in_walk) {  // softened star term, BHTree.cu:547-553
         float dx = -me[t].x, dy = -me[t].y, dz = -me[t].z;
         float r2 = dx * dx + dy * dy + dz * dz + a.eps * a.eps;

@@ -30,6 +30,39 @@ __device__ __forceinline__ void interact(const float4 s, const float4 p, float e
   acc.z = fmaf(f, dz, acc.z);
 }
 
+// A target's accelerations as pairs: .x sums the even-indexed sources of a
+// list, .y the odd-indexed ones, added together once the walk is done.
+struct PairAcc {
+  float2 x, y, z;
+};
+
+// A target's negated coordinates, each in both halves of a pair.
+struct PairTgt {
+  float2 x, y, z;
+};
+
+// interact() on two sources at once in packed FP32 (f32x2, sm_100): the same
+// operations in the same order on each half, so each interaction rounds as
+// interact() rounds it (s + (-p) is s - p exactly).  sx .. sm hold the two
+// sources' coordinates and masses.  Returns the two softened r^2.
+template <bool kSoft>
+__device__ __forceinline__ float2 interact2(const float2 sx, const float2 sy, const float2 sz,
+                                            const float2 sm, const PairTgt& p, const float2 e2,
+                                            PairAcc& acc) {
+  const float2 dx = __fadd2_rn(sx, p.x), dy = __fadd2_rn(sy, p.y), dz = __fadd2_rn(sz, p.z);
+  const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, e2)));
+  float2 inv = make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
+  if (!kSoft) {
+    inv.x = (r2.x > 0.f) ? inv.x : 0.f;
+    inv.y = (r2.y > 0.f) ? inv.y : 0.f;
+  }
+  const float2 f = __fmul2_rn(sm, __fmul2_rn(__fmul2_rn(inv, inv), inv));
+  acc.x = __ffma2_rn(f, dx, acc.x);
+  acc.y = __ffma2_rn(f, dy, acc.y);
+  acc.z = __ffma2_rn(f, dz, acc.z);
+  return r2;
+}
+
 // Vector-Jacobian product of one interaction: with d = s - p and
 // K(d) = d / (|d|^2 + eps^2)^{3/2}, returns g = m_s (dK/dd) lam
 //   = m_s (lam r^-3 - 3 d (d . lam) r^-5),   r^2 = |d|^2 + eps^2.
