@@ -12,17 +12,25 @@ constexpr int kHistBins = 256;       // 8-bit digits
 constexpr int kHistMaxPasses = 8;    // up to 64-bit keys
 
 // Adds the digits of one key per lane to the block's histograms s_h[pass][d].
-// Every lane of the warp calls it (valid = false for lanes without a key):
-// lanes with equal digits are merged by __match_any_sync into one atomic,
-// which matters for nearly sorted keys, whose high digits mostly agree.
+// Every lane of the warp calls it (valid = false for lanes without a key).
+// Lanes whose digit equals the previous lane's join that lane's run, and the
+// first lane of each run adds the run's length in one atomic: the keys come
+// nearly sorted, so their high digits form a few long runs.  Equal digits in
+// separate runs each add their own run (one count per key either way).
 template <typename K>
 __device__ __forceinline__ void hist_add(uint32_t (*s_h)[kHistBins], K key, bool valid,
                                          int passes) {
   const int lane = threadIdx.x & 31;
+  const unsigned above = ~((2u << lane) - 1u);  // lanes after this one (none for lane 31)
   for (int p = 0; p < passes; ++p) {
     const uint32_t d = valid ? (uint32_t)(key >> (8 * p)) & 0xffu : (uint32_t)kHistBins;
-    const unsigned peers = __match_any_sync(kFull, d);
-    if (valid && lane == __ffs(peers) - 1) atomicAdd(&s_h[p][d], (uint32_t)__popc(peers));
+    const uint32_t prev = __shfl_up_sync(kFull, d, 1);
+    const unsigned heads = __ballot_sync(kFull, lane == 0 || d != prev);
+    if (valid && ((heads >> lane) & 1u)) {
+      const unsigned later = heads & above;
+      const int next = later ? __ffs(later) - 1 : 32;
+      atomicAdd(&s_h[p][d], (uint32_t)(next - lane));
+    }
   }
 }
 

@@ -95,7 +95,7 @@ k_digit_hist(const K* __restrict__ keys, int n, int passes, uint32_t* __restrict
   for (int i = tid; i < kMaxPasses * kBins; i += kSortThreads) (&s_h[0][0])[i] = 0;
   __syncthreads();
   const long long stride = (long long)gridDim.x * blockDim.x;
-  const long long end = (n + 31) / 32 * 32;  // whole warps take part in match_any
+  const long long end = (n + 31) / 32 * 32;  // whole warps count digits (hist_add)
   for (long long i = (long long)blockIdx.x * blockDim.x + tid; i < end; i += stride) {
     const bool valid = i < n;
     hist_add(s_h, valid ? __ldg(keys + i) : (K)0, valid, passes);

@@ -103,7 +103,7 @@ k_keys(const T* __restrict__ x, const T* __restrict__ y, const T* __restrict__ z
   if (hist)
     for (int i = threadIdx.x; i < 4 * kHistBins; i += blockDim.x) (&s_h[0][0])[i] = 0;
   __syncthreads();
-  const long long end = hist ? (n + 31) / 32 * 32 : n;  // whole warps take part in match_any
+  const long long end = hist ? (n + 31) / 32 * 32 : n;  // whole warps count digits (hist_add)
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < end;
        i += (long long)gridDim.x * blockDim.x) {
     const bool valid = i < n;
@@ -158,7 +158,7 @@ k_keys_multi(const T* __restrict__ x, const T* __restrict__ y, const T* __restri
     for (int i = threadIdx.x; i < passes * kHistBins; i += blockDim.x) (&s_h[0][0])[i] = 0;
     __syncthreads();
   }
-  const long long end = hist ? (n + 31) / 32 * 32 : n;  // whole warps take part in match_any
+  const long long end = hist ? (n + 31) / 32 * 32 : n;  // whole warps count digits (hist_add)
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < end;
        i += (long long)gridDim.x * blockDim.x) {
     const bool valid = i < n;

@@ -17,8 +17,9 @@
 // leaf_max bodies, append those bodies.  Each full batch of 32 sources is
 // evaluated by all 32 lanes for their own target, reading four sources at a
 // time from shared memory as broadcasts and computing in packed FP32
-// (f32x2): 6 packed instructions + 1 MUFU.RSQ per interaction.  The softened self term is exactly zero (d = 0), so no
-// self-skip test is needed when softening > 0.
+// (f32x2): 6 packed instructions + 1 MUFU.RSQ per interaction.  The softened
+// self term is exactly zero (d = 0), so no self-skip test is needed when
+// softening > 0.
 //
 // The stack spills to a per-warp global area when it would overflow; a
 // spill area that runs out raises kStatusStackOverflow instead of hanging.
@@ -34,8 +35,9 @@ constexpr int kWalkWarps = 4;
 // Walk modes (WalkArgs::walk_mode), a trade-off that depends on the disk:
 //   0: acceptance vote, 5 resident blocks per SM (up to 96 registers);
 //   1: acceptance vote, 8 blocks per SM (64 registers) -- the default: at
-//      N = 2^20 over r in [0.3, 30] AU (groups of span 8) 0.49 ms per walk,
-//      against 0.53 ms for mode 0; 6, 7 or 10 blocks per SM gain nothing;
+//      N = 2^20 over r in [0.3, 30] AU (groups of span 8) the step takes
+//      0.641 ms, against 0.667 ms with mode 0 and 0.645 / 0.652 ms with 7 / 6
+//      blocks per SM;
 //   2: no vote, 8 blocks per SM -- the fastest on small compact disks (the
 //      64-disk ensemble), where the vote rarely pays and occupancy matters.
 template <int kMode>
@@ -101,9 +103,8 @@ __device__ __forceinline__ void eval_quad(const WarpSmem& w, int j, const PairTg
 
 // One source in scalar FP32 into the .x halves.
 template <bool kSoft, int kT, bool kRmin>
-__device__ __forceinline__ void eval_one(const WarpSmem& w, int j, const float4 (&me)[kT],
-                                         float eps2, PairAcc (&acc)[kT], float& rmin) {
-  const float4 s = lst_get(w, j);
+__device__ __forceinline__ void eval_one(const float4 s, const float4 (&me)[kT], float eps2,
+                                         PairAcc (&acc)[kT], float& rmin) {
 #pragma unroll
   for (int t = 0; t < kT; ++t) {
     if (kRmin) {
@@ -132,14 +133,23 @@ __device__ __forceinline__ float eval_list(const WarpSmem& w, int cnt, const flo
   float rmin = INFINITY;
   if (kSeq) {
     const int c = (kCount > 0) ? kCount : cnt;
-    for (int j = 0; j < c; ++j) eval_one<kSoft, kT, kRmin>(w, j, me, eps2, acc, rmin);
+    int j = 0;
+    for (; j + 4 <= c; j += 4) {
+      const float4 qx = lst_row4(w, 0, j), qy = lst_row4(w, 1, j);
+      const float4 qz = lst_row4(w, 2, j), qm = lst_row4(w, 3, j);
+      eval_one<kSoft, kT, kRmin>(make_float4(qx.x, qy.x, qz.x, qm.x), me, eps2, acc, rmin);
+      eval_one<kSoft, kT, kRmin>(make_float4(qx.y, qy.y, qz.y, qm.y), me, eps2, acc, rmin);
+      eval_one<kSoft, kT, kRmin>(make_float4(qx.z, qy.z, qz.z, qm.z), me, eps2, acc, rmin);
+      eval_one<kSoft, kT, kRmin>(make_float4(qx.w, qy.w, qz.w, qm.w), me, eps2, acc, rmin);
+    }
+    for (; j < c; ++j) eval_one<kSoft, kT, kRmin>(lst_get(w, j), me, eps2, acc, rmin);
   } else if (kCount > 0) {
 #pragma unroll
     for (int j = 0; j < kCount; j += 4) eval_quad<kSoft, kT, kRmin>(w, j, pt, e2, acc, rmin);
   } else {
     int j = 0;
     for (; j + 4 <= cnt; j += 4) eval_quad<kSoft, kT, kRmin>(w, j, pt, e2, acc, rmin);
-    for (; j < cnt; ++j) eval_one<kSoft, kT, kRmin>(w, j, me, eps2, acc, rmin);
+    for (; j < cnt; ++j) eval_one<kSoft, kT, kRmin>(lst_get(w, j), me, eps2, acc, rmin);
   }
   return rmin;
 }
