@@ -41,7 +41,6 @@ constexpr int kBins = kHistBins;
 
 // Exclusive scan of `total` uint32 in place, one block of 1024 threads.
 __global__ void __launch_bounds__(1024) k_scan_inplace(uint32_t* __restrict__ data, int total) {
-  __shared__ uint32_t s_part[1024];
   __shared__ uint32_t s_warp[32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int per = (total + 1023) / 1024;
@@ -69,7 +68,6 @@ __global__ void __launch_bounds__(1024) k_scan_inplace(uint32_t* __restrict__ da
   }
   __syncthreads();
   uint32_t run = v - sum + (warp > 0 ? s_warp[warp - 1] : 0u);
-  s_part[tid] = run;
   for (long long i = lo; i < hi; ++i) {
     uint32_t c = data[i];
     data[i] = run;
