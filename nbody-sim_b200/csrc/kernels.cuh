@@ -205,6 +205,7 @@ struct WalkArgs {
   int* status;
   int targets_per_lane;   // 1 or 2: groups of up to 32 or 64 bodies
   int walk_mode;          // 0, 1, 2: see walk.cu (targets_per_lane 1 only)
+  bool counters_zeroed;   // work, inter and counters already zero (no reset launch)
   // ensembles: a group's walk starts at its disk's root slot, and pert holds
   // n_disks perturbers per force evaluation, the current one at *pert_step
   const int* group_disk;  // nullptr: one disk

@@ -59,10 +59,29 @@ __global__ void k_iota(int* __restrict__ id, int n) {
     id[i] = (int)i;
 }
 
+// What the permute kernel also zeroes, in its first block: the encoded
+// bounding boxes (6 words per disk, after the key kernel has read them) that
+// the next stream kernel accumulates, and the walk's group counter and
+// statistics (the walk is then launched with counters_zeroed).
+struct StepReset {
+  unsigned long long* enc = nullptr;
+  int enc_words = 0;
+  int* work = nullptr;
+  unsigned long long* inter = nullptr;
+  unsigned long long* counters = nullptr;
+};
+
 template <typename R>
 __global__ void __launch_bounds__(kThreads)
 k_permute(const uint32_t* __restrict__ perm, StateArrays<R> in, StateArrays<R> out, int n,
-          float4* __restrict__ body4) {
+          float4* __restrict__ body4, const StepReset r) {
+  if (blockIdx.x == 0) {  // counters the step uses next (each has a sole writer)
+    for (int i = threadIdx.x; i < r.enc_words; i += blockDim.x)
+      r.enc[i] = ((i % 6) < 3) ? ~0ull : 0ull;
+    if (threadIdx.x == 0 && r.work) *r.work = 0;
+    if (threadIdx.x == 1 && r.inter) *r.inter = 0ull;
+    if (threadIdx.x >= 2 && threadIdx.x < 5 && r.counters) r.counters[threadIdx.x - 2] = 0ull;
+  }
   for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
        s += (long long)gridDim.x * blockDim.x) {
     // every gather first, then every store: the arrays carry no restrict, so
@@ -718,11 +737,14 @@ struct SimImpl : SimBase {
     // the key kernel also counts the digits of the sort's four passes
     uint32_t* hist = radix_sort_prepare(tw.counts, 30, st);
     launch_keys<R>(tw, a.v[0], a.v[1], a.v[2], n, st, hist);
-    launch_bbox_reset(tw, st);
     radix_sort_pairs(tw.keys, tw.perm, tw.keys_alt, tw.perm_alt, tw.counts, n, 30, st,
                      tw.status, true);
     mark(NBODY_PHASE_PERMUTE);
-    k_permute<R><<<div_up(n, kThreads), kThreads, 0, st>>>(tw.perm, a, b, n, tw.body4);
+    StepReset rs;
+    rs.enc = tw.bbox_enc; rs.enc_words = 6;
+    rs.work = work; rs.inter = inter; rs.counters = counters;
+    k_permute<R><<<std::max(1, div_up(n, kThreads)), kThreads, 0, st>>>(tw.perm, a, b, n,
+                                                                        tw.body4, rs);
     check(cudaGetLastError(), "k_permute launch");
     check(cudaEventRecordWithFlags(ev_pos, st, capturing ? cudaEventRecordExternal
                                                          : cudaEventRecordDefault),
@@ -750,6 +772,7 @@ struct SimImpl : SimBase {
     w.spill = spill; w.spill_cap = spill_cap; w.inter = inter; w.counters = counters;
     w.work = work; w.status = tw.status; w.targets_per_lane = tw.group_max / 32;
     w.walk_mode = p.walk_mode;
+    w.counters_zeroed = true;
     if (!initial && coll_fused()) set_coll_args(w);
     const bool side_coll = !initial && p.r_coll > 0.f && !coll_fused();
     if (side_coll) {  // the collision pass on the second stream, beside the walk
@@ -763,10 +786,10 @@ struct SimImpl : SimBase {
     launch_walk(w, st);
     if (side_coll) check(cudaStreamWaitEvent(st, cs.join, 0), "collision join");
     mark(NBODY_PHASE_COLLIDE);
-    // keys (+ digit histograms), bbox reset, 4 one-sweep passes, permute,
-    // karras, mark, tile scan, apply, moment tiles, moment tile scan, emit,
-    // walk reset, walk
-    launches += 16;
+    // keys (+ digit histograms), 4 one-sweep passes, permute (+ bbox and
+    // walk counter resets), karras, mark, tile scan, apply, moment tiles,
+    // moment tile scan, emit, walk
+    launches += 14;
   }
 
   // Collisions inside the walk (one warp per group of <= 32 targets).
@@ -1464,10 +1487,13 @@ struct EnsembleImpl : EnsembleBase {
     uint32_t* hist = radix_sort_prepare(tw.counts, key_bits, st);  // counted by the key kernel
     launch_keys_multi<R>(a.v[0], a.v[1], a.v[2], a.disk, n, geoms, keys64, tw.perm, tw.status,
                          st, hist, key_bits);
-    launch_bbox_reset_n(bbox, D, st);
     radix_sort_pairs<uint64_t>(keys64, tw.perm, keys64_alt, tw.perm_alt, tw.counts, n, key_bits,
                                st, tw.status, true);
-    k_permute<R><<<div_up(n, kThreads), kThreads, 0, st>>>(tw.perm, a, b, n, tw.body4);
+    StepReset rs;
+    rs.enc = bbox; rs.enc_words = 6 * D;
+    rs.work = work; rs.inter = inter; rs.counters = counters;
+    k_permute<R><<<std::max(1, div_up(n, kThreads)), kThreads, 0, st>>>(tw.perm, a, b, n,
+                                                                        tw.body4, rs);
     check(cudaGetLastError(), "k_permute launch");
     check(cudaEventRecordWithFlags(ev_pos, st, capturing ? cudaEventRecordExternal
                                                          : cudaEventRecordDefault),
@@ -1492,6 +1518,7 @@ struct EnsembleImpl : EnsembleBase {
     w.spill = spill; w.spill_cap = spill_cap; w.inter = inter; w.counters = counters;
     w.work = work; w.status = tw.status; w.targets_per_lane = tw.group_max / 32;
     w.walk_mode = p.walk_mode;
+    w.counters_zeroed = true;
     if (with_coll && coll_fused()) {
       for (int k = 0; k < 3; ++k) w.coll_v[k] = s[cur].v[3 + k];
       w.coll_vtype = kIsF32<R> ? 0 : (kIsF64<R> ? 1 : 2);
@@ -1509,10 +1536,10 @@ struct EnsembleImpl : EnsembleBase {
     }
     launch_walk(w, st);
     if (side_coll) check(cudaStreamWaitEvent(st, cs.join, 0), "collision join");
-    // geoms, keys (+ digit histograms), bbox reset, one one-sweep kernel per
-    // pass, permute, karras, mark, tile scan, apply, moment tiles, moment
-    // tile scan, emit, walk reset, walk
-    launches += 3 + (key_bits + 7) / 8 + 10;
+    // geoms, keys (+ digit histograms), one one-sweep kernel per pass,
+    // permute (+ bbox and walk counter resets), karras, mark, tile scan,
+    // apply, moment tiles, moment tile scan, emit, walk
+    launches += 2 + (key_bits + 7) / 8 + 9;
   }
 
   void collide(cudaStream_t on, int* wk, int* sp) {

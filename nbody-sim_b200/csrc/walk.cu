@@ -671,8 +671,10 @@ __global__ void k_walk_reset(int* work, unsigned long long* inter, unsigned long
 
 void launch_walk(const WalkArgs& a, cudaStream_t s) {
   if (a.n <= 0) return;
-  k_walk_reset<<<1, 32, 0, s>>>(a.work, a.inter, a.counters);
-  check(cudaGetLastError(), "walk reset launch");
+  if (!a.counters_zeroed) {
+    k_walk_reset<<<1, 32, 0, s>>>(a.work, a.inter, a.counters);
+    check(cudaGetLastError(), "walk reset launch");
+  }
   const bool soft = a.eps > 0.f;
   if (a.tape) {  // recording: groups of <= 32 targets
     if (soft) launch_variant<true, 1, true>(a, s);
