@@ -183,13 +183,24 @@ struct ReplayArgs {
 
 struct ReplaySmem {
   double4 dlst[32];  // FP64 replay sources
-  float4 lst[32];
+  // FP32 sources, one row per component (x, y, z, mass): two entries of a
+  // row from an even index are one 8-byte load into a register pair
+  float src[4][32];
   int2 ent[32];
   double mass[32];
-  float4 tme[32];
-  float4 tlam[32];
+  // the group's targets, one row per component: negated x, y, z, then the
+  // adjoint's x, y, z
+  float tgt[6][32];
   int tid[32];
 };
+
+__device__ __forceinline__ float2 row2(const float* r, int j) {
+  return *reinterpret_cast<const float2*>(r + j);
+}
+
+__device__ __forceinline__ float4 src_at(const ReplaySmem& w, int j) {
+  return make_float4(w.src[0][j], w.src[1][j], w.src[2][j], w.src[3][j]);
+}
 
 // Loads up to 32 entries of the tape chain into the warp's list: source
 // float4 (centre of mass from the FP64 prefix sums, or the body itself).
@@ -207,7 +218,10 @@ __device__ __forceinline__ void load_chunk(const ReplayArgs& a, ReplaySmem& w, i
       src = com_of(s, 0.f, 0.f, 0.f);
       m = s.x;
     }
-    w.lst[lane] = src;
+    w.src[0][lane] = src.x;
+    w.src[1][lane] = src.y;
+    w.src[2][lane] = src.z;
+    w.src[3][lane] = src.w;
     w.ent[lane] = e;
     w.mass[lane] = m;
   }
@@ -305,8 +319,12 @@ __global__ void __launch_bounds__(kRW * 32) k_replay(const ReplayArgs a) {
     double mx = 0.0, my = 0.0, mz = 0.0;
     if (kAdj) {
       if (valid) lam = make_float3((float)a.lx[o], (float)a.ly[o], (float)a.lz[o]);
-      w.tme[lane] = me;
-      w.tlam[lane] = make_float4(lam.x, lam.y, lam.z, 0.f);
+      w.tgt[0][lane] = -me.x;
+      w.tgt[1][lane] = -me.y;
+      w.tgt[2][lane] = -me.z;
+      w.tgt[3][lane] = lam.x;
+      w.tgt[4][lane] = lam.y;
+      w.tgt[5][lane] = lam.z;
       w.tid[lane] = valid ? s : -1;
       __syncwarp();
     }
@@ -315,29 +333,68 @@ __global__ void __launch_bounds__(kRW * 32) k_replay(const ReplayArgs a) {
       const int k = min(kTapeChunk, gt.y - done);
       load_chunk(a, w, chunk, k, lane);
       if (!kAdj) {
-        for (int j = 0; j < k; ++j) interact<kSoft>(w.lst[j], me, a.eps2, acc);
+        for (int j = 0; j < k; ++j) interact<kSoft>(src_at(w, j), me, a.eps2, acc);
       } else {
-        // target side: -g for every source except the body itself, summed
-        // over the chunk (<= 32 terms) in FP32, the chunk sums in FP64
-        float3 part = make_float3(0.f, 0.f, 0.f);
-        for (int j = 0; j < k; ++j) {
+        const float2 e2 = make_float2(a.eps2, a.eps2);
+        // target side: -g for every source except the body itself (a mass of
+        // 0), sources in pairs through the packed product, summed over the
+        // chunk (<= 32 terms) in FP32, the chunk sums in FP64
+        PairTgt me2;
+        me2.x = make_float2(-me.x, -me.x);
+        me2.y = make_float2(-me.y, -me.y);
+        me2.z = make_float2(-me.z, -me.z);
+        const float2 l2x = make_float2(lam.x, lam.x), l2y = make_float2(lam.y, lam.y);
+        const float2 l2z = make_float2(lam.z, lam.z);
+        PairAcc p2;
+        p2.x = p2.y = p2.z = make_float2(0.f, 0.f);
+        int j = 0;
+        for (; j + 2 <= k; j += 2) {
+          const int4 ee = *reinterpret_cast<const int4*>(&w.ent[j]);
+          float2 m2 = row2(w.src[3], j);
+          if (ee.y == 1 && ee.x == s) m2.x = 0.f;
+          if (ee.w == 1 && ee.z == s) m2.y = 0.f;
+          interact_vjp2<kSoft>(row2(w.src[0], j), row2(w.src[1], j), row2(w.src[2], j), m2, me2,
+                               e2, l2x, l2y, l2z, p2);
+        }
+        float3 part = make_float3(p2.x.x + p2.x.y, p2.y.x + p2.y.y, p2.z.x + p2.z.y);
+        for (; j < k; ++j) {
           const int2 e = w.ent[j];
           if (e.y == 1 && e.x == s) continue;
-          const float3 gv = interact_vjp<kSoft>(w.lst[j], me, a.eps2, lam);
+          const float3 gv = interact_vjp<kSoft>(src_at(w, j), me, a.eps2, lam);
           part.x += gv.x; part.y += gv.y; part.z += gv.z;
         }
         mx -= (double)part.x; my -= (double)part.y; mz -= (double)part.z;
-        // source side: lane j sums +g over the group's targets and spreads
-        // it over the source's bodies in proportion to their mass
+        // source side: lane j sums +g over the group's targets, in pairs of
+        // targets, and spreads it over the source's bodies in proportion to
+        // their mass
         if (lane < k) {
-          const float4 src = w.lst[lane];
+          const float4 src = src_at(w, lane);
           const int2 e = w.ent[lane];
-          float3 gs = make_float3(0.f, 0.f, 0.f);
-          for (int t = 0; t < gr.y; ++t) {
-            if (e.y == 1 && e.x == w.tid[t]) continue;
-            const float4 tl = w.tlam[t];
-            const float3 gv = interact_vjp<kSoft>(src, w.tme[t], a.eps2,
-                                                  make_float3(tl.x, tl.y, tl.z));
+          const float2 s2x = make_float2(src.x, src.x), s2y = make_float2(src.y, src.y);
+          const float2 s2z = make_float2(src.z, src.z);
+          const bool single = e.y == 1;
+          PairAcc g2;
+          g2.x = g2.y = g2.z = make_float2(0.f, 0.f);
+          int t = 0;
+          for (; t + 2 <= gr.y; t += 2) {
+            const int2 ids = *reinterpret_cast<const int2*>(&w.tid[t]);
+            float2 m2 = make_float2(src.w, src.w);
+            if (single && e.x == ids.x) m2.x = 0.f;
+            if (single && e.x == ids.y) m2.y = 0.f;
+            PairTgt tp;
+            tp.x = row2(w.tgt[0], t);
+            tp.y = row2(w.tgt[1], t);
+            tp.z = row2(w.tgt[2], t);
+            interact_vjp2<kSoft>(s2x, s2y, s2z, m2, tp, e2, row2(w.tgt[3], t),
+                                 row2(w.tgt[4], t), row2(w.tgt[5], t), g2);
+          }
+          float3 gs = make_float3(g2.x.x + g2.x.y, g2.y.x + g2.y.y, g2.z.x + g2.z.y);
+          for (; t < gr.y; ++t) {
+            if (single && e.x == w.tid[t]) continue;
+            const float4 tp = make_float4(-w.tgt[0][t], -w.tgt[1][t], -w.tgt[2][t], 0.f);
+            const float3 gv = interact_vjp<kSoft>(src, tp, a.eps2,
+                                                  make_float3(w.tgt[3][t], w.tgt[4][t],
+                                                              w.tgt[5][t]));
             gs.x += gv.x; gs.y += gv.y; gs.z += gv.z;
           }
           const double inv = 1.0 / w.mass[lane];

@@ -81,4 +81,30 @@ __device__ __forceinline__ float3 interact_vjp(const float4 s, const float4 p, f
   return make_float3(f * fmaf(-t, dx, lam.x), f * fmaf(-t, dy, lam.y), f * fmaf(-t, dz, lam.z));
 }
 
+// interact_vjp() on two sources (or two targets) at once in packed FP32,
+// added into acc: acc += m_s (lam r^-3 - 3 d (d . lam) r^-5), pair half by
+// pair half.  p holds the negated target coordinates, sx .. sm the sources'
+// coordinates and masses (a mass of 0 drops its half), lx .. lz the
+// adjoints.
+template <bool kSoft>
+__device__ __forceinline__ void interact_vjp2(const float2 sx, const float2 sy, const float2 sz,
+                                              const float2 sm, const PairTgt& p, const float2 e2,
+                                              const float2 lx, const float2 ly, const float2 lz,
+                                              PairAcc& acc) {
+  const float2 dx = __fadd2_rn(sx, p.x), dy = __fadd2_rn(sy, p.y), dz = __fadd2_rn(sz, p.z);
+  const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, e2)));
+  float2 inv = make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
+  if (!kSoft) {
+    inv.x = (r2.x > 0.f) ? inv.x : 0.f;
+    inv.y = (r2.y > 0.f) ? inv.y : 0.f;
+  }
+  const float2 inv2 = __fmul2_rn(inv, inv);
+  const float2 f = __fmul2_rn(sm, __fmul2_rn(inv2, inv));
+  const float2 dl = __ffma2_rn(dx, lx, __ffma2_rn(dy, ly, __fmul2_rn(dz, lz)));
+  const float2 nt = __fmul2_rn(__fmul2_rn(make_float2(-3.f, -3.f), dl), inv2);
+  acc.x = __ffma2_rn(f, __ffma2_rn(nt, dx, lx), acc.x);
+  acc.y = __ffma2_rn(f, __ffma2_rn(nt, dy, ly), acc.y);
+  acc.z = __ffma2_rn(f, __ffma2_rn(nt, dz, lz), acc.z);
+}
+
 }  // namespace nb
