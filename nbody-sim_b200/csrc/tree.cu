@@ -86,6 +86,16 @@ __device__ void compute_geom(const unsigned long long* enc, TreeGeom& g) {
   g.scale = (rhs > 0.0) ? 512.0 / rhs : 0.0;
 }
 
+// The key kernels give each block one contiguous run of keys (a multiple of
+// the block size, so every warp's keys are 32 consecutive ones): the keys
+// arrive nearly sorted, so a run's high digits take few values, and the
+// block adds far fewer non-zero bins to the global histograms than a
+// grid-strided block, whose keys span the whole key range, would.
+__device__ __forceinline__ long long key_block_span(long long end) {
+  const long long per = (end + gridDim.x - 1) / gridDim.x;
+  return (per + blockDim.x - 1) / blockDim.x * blockDim.x;
+}
+
 // Keys of n positions; hist (optional, 4 x 256 words, cleared) receives the
 // digit counts of the four 8-bit passes of the radix sort that follows.
 template <typename T>
@@ -104,8 +114,9 @@ k_keys(const T* __restrict__ x, const T* __restrict__ y, const T* __restrict__ z
     for (int i = threadIdx.x; i < 4 * kHistBins; i += blockDim.x) (&s_h[0][0])[i] = 0;
   __syncthreads();
   const long long end = hist ? (n + 31) / 32 * 32 : n;  // whole warps count digits (hist_add)
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < end;
-       i += (long long)gridDim.x * blockDim.x) {
+  const long long span = key_block_span(end);
+  const long long stop = min(end, ((long long)blockIdx.x + 1) * span);
+  for (long long i = (long long)blockIdx.x * span + threadIdx.x; i < stop; i += blockDim.x) {
     const bool valid = i < n;
     uint32_t key = 0;
     if (valid) {
@@ -159,8 +170,9 @@ k_keys_multi(const T* __restrict__ x, const T* __restrict__ y, const T* __restri
     __syncthreads();
   }
   const long long end = hist ? (n + 31) / 32 * 32 : n;  // whole warps count digits (hist_add)
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < end;
-       i += (long long)gridDim.x * blockDim.x) {
+  const long long span = key_block_span(end);
+  const long long stop = min(end, ((long long)blockIdx.x + 1) * span);
+  for (long long i = (long long)blockIdx.x * span + threadIdx.x; i < stop; i += blockDim.x) {
     const bool valid = i < n;
     uint64_t key = 0;
     if (valid) {
