@@ -652,7 +652,8 @@ struct EmitArgs {
 template <typename K>
 __device__ void write_node(const EmitArgs<K>& a, int c, int f) {
   const int first = (c >= a.n - 1) ? c - (a.n - 1) : a.lo[c];
-  const TreeGeom* geom = a.geom + key_disk(a.keys[first]);
+  // 30-bit keys carry no disk: the geometry needs no key load then
+  const TreeGeom* geom = a.geom + (sizeof(K) == 4 ? 0 : key_disk(a.keys[first]));
   const float rhs = geom->rhs;
   if (c >= a.n - 1) {  // single-body leaf
     const int j = c - (a.n - 1);
@@ -704,7 +705,7 @@ __global__ void __launch_bounds__(kThreads, 6) k_emit(const EmitArgs<K> a) {
   if (!(h & kNchTop)) return;
   int f;
   if (h & kNchRoot) {
-    f = key_disk(a.keys[(b >= a.n - 1) ? b - (a.n - 1) : a.lo[b]]);
+    f = (sizeof(K) == 4) ? 0 : key_disk(a.keys[(b >= a.n - 1) ? b - (a.n - 1) : a.lo[b]]);
   } else {
     const int P = a.opar[b];
     if (P < 0) return;  // under a node the walk opens as bodies: no record
