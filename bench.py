@@ -60,6 +60,12 @@ def parse():
                          "(nbody_sim_params.group_span)")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-studies", action="store_true",
+                    help="headline line without the force-error, reference-engine, ensemble "
+                         "and adjoint sub-records")
+    ap.add_argument("--adjoint-fd", type=int, default=48,
+                    help="velocity components checked by central differences in the headline "
+                         "line's adjoint record")
     ap.add_argument("--no-flush", action="store_true")
     ap.add_argument("--workload", choices=["disk1m", "ensemble", "precision", "adjoint", "c2run"],
                     default="disk1m",
@@ -112,6 +118,22 @@ def barrier(ws):
 def make_ic(nb, n, seed, dtype=np.float32):
     d = nb.make_disk(n, WORKLOAD["r_min"], WORKLOAD["r_max"], 0.01, 0.005, 1.0, seed)
     st = {k: v.astype(dtype) for k, v in d.items()}
+    st["m"] = np.full(n, WORKLOAD["m"], np.float32)
+    return st
+
+
+def oracle_port():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    return oracle.Port()
+
+
+def make_ic_oracle(n, seed):
+    """The same disk as make_ic, from the oracle's restatement of the recipe
+    (oracle/port.c orc_make_disk, bit-identical), so that the reference arm
+    loads none of the product's libraries."""
+    d = oracle_port().make_disk(n, WORKLOAD["r_min"], WORKLOAD["r_max"], 0.01, 0.005, 1.0, seed)
+    st = {k: v.astype(np.float32) for k, v in d.items()}
     st["m"] = np.full(n, WORKLOAD["m"], np.float32)
     return st
 
@@ -188,18 +210,33 @@ def walk_traffic():
     return None
 
 
+def workload_name(n, theta, precision="f32"):
+    return (f"Keplerian disk N={n} r=[0.3,30] AU theta={theta} eps=5e-4 dt=0.002, "
+            f"{precision.upper()} state, no collisions/drag/perturber")
+
+
+# what one timed CPU step of the reference algorithm does (oracle/port.c)
+CPU_STEP = ("CAS octree build, the reference's 20 parallel summarize passes, DFS sort, walk, "
+            "KDK")
+
+
 def cpu_port_step(st, n, nthreads=0, steps=1):
-    """The CPU restatement of the reference step (oracle/port.c), timed."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
-    port = oracle.Port()
+    """The CPU restatement of the reference step (oracle/port.c), timed, with
+    the reference's fixed 20 summarize passes (BHTree.cu:501-516) rather than
+    the oracle's converged sweep (same values on these trees, the reference's
+    amount of work)."""
+    port = oracle_port()
     w = WORKLOAD
     sp = port.step_params(w["dt"], w["theta"], w["eps"], 1.0, r_coll=0.0, collisions=False)
     s = {k: np.array(st[k][:n], np.float32) for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
-    port.run(s, sp, 0, nthreads=nthreads)  # initial forces (untimed)
-    t0 = time.perf_counter()
-    port.run(s, sp, steps, nthreads=nthreads, initial_forces=False)
-    return time.perf_counter() - t0
+    port.set_summarize_passes(20)
+    try:
+        port.run(s, sp, 0, nthreads=nthreads)  # initial forces (untimed)
+        t0 = time.perf_counter()
+        port.run(s, sp, steps, nthreads=nthreads, initial_forces=False)
+        return time.perf_counter() - t0
+    finally:
+        port.set_summarize_passes(0)
 
 
 def run_reference(args, ws, rank):
@@ -207,10 +244,8 @@ def run_reference(args, ws, rank):
     formulas, oracle/port.c) on all host cores; rank 0 only."""
     if rank != 0:
         return
-    import importlib
-    nb = importlib.import_module("nbody-sim_b200")
     n = args.n
-    st = make_ic(nb, n, 0)
+    st = make_ic_oracle(n, 0)
     cores = os.cpu_count() or 1
     for _ in range(args.warmup):
         cpu_port_step(st, n, 0, 1)
@@ -222,15 +257,85 @@ def run_reference(args, ws, rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": f"Keplerian disk N={n} r=[0.3,30] AU theta={args.theta} "
-                               f"eps=5e-4 dt=0.002, FP32 state", "n": n, "theta": args.theta,
-                   "parallelism": "cpu", "l2": "n/a (host)"},
+        "config": {"workload": workload_name(n, args.theta), "n": n, "theta": args.theta,
+                   "state": "f32", "parallelism": "cpu", "l2": "n/a (host)"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{args.steps} full steps at N={n} (CAS-octree build, "
-                                   "20-pass summarize, DFS sort, walk, KDK), OpenMP"},
+                         "sample": f"{args.steps} full steps at N={n} ({CPU_STEP}), OpenMP "
+                                   "over all host threads; initial conditions from the oracle's "
+                                   "restatement of the disk recipe"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+# Algorithmic HBM bytes per body of each step phase at FP32 state without
+# collisions (the unique bytes a phase must move; its kernels' own layout):
+#   stream  read x, v, a (36) + write x, v (24)
+#   sort    keys: read x (12) + write key, index (8); four 8-bit passes of
+#           key + index read and written (4 x 16)
+#   permute read index (4) + gather x, v, mass, id (32); write x, v, mass, id
+#           (32) + the walk's float4 body (16)
+#   tree    keys (4) + binary topology (16) + body read (16) + node COM and
+#           mass (32)
+PHASE_BYTES_F32 = {"stream": 60, "sort": 84, "permute": 84, "tree": 68}
+
+
+def hbm_peak():
+    """Measured copy bandwidth of this pool's B200s (GB/s), else the
+    earlier measurement used as the fallback."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        for k in ("hbm_gbs", "hbm_GBs", "hbm_copy_gbs"):
+            if k in d:
+                return float(d[k]), "measured (MEASURED_PEAKS.json)"
+    return 6650.0, "fallback (6.65 TB/s)"
+
+
+def phase_hbm(prof, n):
+    peak, src = hbm_peak()
+    out = {"peak_gbs": peak, "peak_source": src}
+    for k, b in PHASE_BYTES_F32.items():
+        ms = prof.get(k, 0.0)
+        if ms > 0:
+            gbs = b * n / (ms * 1e-3) / 1e9
+            out[k] = {"bytes_per_body": b, "ms": ms, "gbs": gbs, "frac": gbs / peak}
+    return out
+
+
+def ref_engine_study(st, n, theta, steps=3):
+    """The reference's own CUDA engine (src/physics/*.cu compiled unchanged for
+    sm_100a, oracle/_ref/libref_engine.so) through the step loop of
+    src/main.cu:101-139 on the same disk: the throughput that the plain
+    path's 3x target is set against.  The CPU restatement first checks that
+    the reference build keeps every body and summarizes the whole tree on
+    this input."""
+    path = os.path.join(ROOT, "oracle", "_ref", "libref_engine.so")
+    if not os.path.exists(path):
+        return {"unavailable": "oracle/_ref/libref_engine.so not built"}
+    port = oracle_port()
+    import oracle
+    t = port.build_tree(st["x"], st["y"], st["z"], st["m"])
+    info = port.tree_info(t)
+    port.free_tree(t)
+    if info.lost_bodies or info.unsummarized or info.height > 20:
+        return {"unavailable": f"reference build unsafe on this input (lost {info.lost_bodies}, "
+                               f"unsummarized {info.unsummarized}, height {info.height})"}
+    w = WORKLOAD
+    eng = oracle.RefEngine(n, path=path)
+    try:
+        eng.set_state(st)
+        eng.build()
+        eng.force(theta, w["eps"], 1.0)
+        eng.steps(0, 1, w["dt"], theta, w["eps"], 1.0, 0.0, 0.0, 0.0)  # warm-up
+        ms = eng.steps(1, steps, w["dt"], theta, w["eps"], 1.0, 0.0, 0.0, 0.0)
+    finally:
+        eng.close()
+    return {"value": n * steps / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / steps,
+            "steps": steps, "tree_height": info.height,
+            "how": "src/main.cu:101-139 launcher sequence (each launcher synchronous), "
+                   "wall time of the loop, after one warm-up step"}
 
 
 def run_ours(args, ws, rank, local):
@@ -329,9 +434,8 @@ def run_ours(args, ws, rank, local):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"Keplerian disk N={n} r=[0.3,30] AU theta={args.theta} "
-                               f"eps=5e-4 dt=0.002, {args.precision.upper()} state, "
-                               "no collisions/drag/perturber", "n": n, "theta": args.theta,
+        "config": {"workload": workload_name(n, args.theta, args.precision), "n": n,
+                   "theta": args.theta,
                    "state": args.precision, "leaf_max": args.leaf_max,
                    "parallelism": f"replicas x{ws}",
                    "l2": "flushed (256 MB write) before every timed step"},
@@ -350,19 +454,50 @@ def run_ours(args, ws, rank, local):
         "e2e": e2e,
         "clocks": ck,
     }
+    line["phase_hbm"] = phase_hbm(line["phase_ms_per_step"], n)
+    if rank == 0 and ws == 1 and not args.no_studies and prec == nb.STATE_F32:
+        dg = importlib.import_module("nbody-sim_b200.diagnostics")
+        targets = np.sort(np.random.default_rng(0).choice(n, min(args.targets, n),
+                                                          replace=False))
+        fe = dg.engine_force_errors(prm, st, targets)
+        line["force_err"] = {"targets": len(targets), "total": fe["total"], "self": fe["self"],
+                             "vs": "FP64 direct sum (nbody_direct_f64) on the same FP32 "
+                                   "positions; the engine's own walk (the timed one)"}
+        ref = ref_engine_study(st, n, args.theta)
+        if "value" in ref:
+            ref["ours_over_reference"] = value / ref["value"]
+        line["ref_engine"] = ref
+        sim.close()
+        ens = ensemble_study(args, ws, rank, local, args.steps)
+        line["ensemble"] = {"value": ens["value"], "ms_per_step": ens["ms_per_step"],
+                            "n_total": ens["config"]["n_total"], "disks": args.disks,
+                            "one_by_one_value": ens["one_by_one"]["value"],
+                            "one_by_one_ms_per_step": ens["one_by_one"]["ms_per_step"],
+                            "ensemble_over_one_by_one": ens["one_by_one"]["speedup"],
+                            "workload": ens["config"]["workload"]}
+        adj = adjoint_study(args, args.adjoint_fd)
+        line["adjoint"] = {"gradient_over_plain_forward": adj["ms"]["gradient_over_plain_forward"],
+                           "ms": adj["ms"], "memory_bytes": adj["memory_bytes"],
+                           "fd_check": adj["fd_check"], "perturber": adj["perturber"],
+                           "workload": adj["config"]["workload"]}
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
         secs = cpu_port_step(st, n, 0, 1)
         line["cpu_baseline"] = {"value": n / secs, "unit": UNIT, "cores": cores, "kind": "port",
                                 "sample": f"1 full step at N={n} of the reference algorithm "
-                                          "(oracle/port.c: CAS octree, summarize, DFS, walk, "
-                                          "KDK), OpenMP"}
+                                          f"(oracle/port.c: {CPU_STEP}), OpenMP"}
     sim.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
 
 
 def run_ensemble(args, ws, rank, local):
+    line = ensemble_study(args, ws, rank, local, args.steps)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def ensemble_study(args, ws, rank, local, steps):
     """64 disks of uneven size (N log-uniform in [2048, 65536]) with their own
     perturbers, collisions and drag, FP64 state: the batched ensemble engine
     against the same disks stepped one by one through nbody_sim.  With several
@@ -390,13 +525,13 @@ def run_ensemble(args, ws, rank, local):
         ens.step(1)
     ens.sync()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
     s0 = ens.stats()
     clocks = Clocks(torch.cuda.current_device()) if rank == 0 else None
     barrier(ws)
     torch.cuda.synchronize()
-    for k in range(args.steps):
+    for k in range(steps):
         if not args.no_flush:
             flush.zero_()
         starts[k].record(stream)
@@ -409,7 +544,7 @@ def run_ensemble(args, ws, rank, local):
     s1 = ens.stats()
     ms = sum(a.elapsed_time(b) for a, b in zip(starts, ends))
     ms_max = allreduce_max(ms, ws)
-    value = n_all * args.steps / (ms_max * 1e-3)
+    value = n_all * steps / (ms_max * 1e-3)
 
     # e2e: nbody_ensemble_step_host, state and accelerations in from pinned
     # host buffers and back out, every step
@@ -457,8 +592,8 @@ def run_ensemble(args, ws, rank, local):
     solo_ms = allreduce_max(solo_ms, ws)
     line = {
         "metric": f"ensemble particle-steps/s ({args.disks} disks)", "value": value, "unit": UNIT,
-        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "n_gpus": ws, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / steps, "higher_is_better": True,
         "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"{args.disks} Keplerian disks, N log-uniform [2048,65536] "
                                f"(total {n_all}), r=[0.5,5] AU, m=1e-8, perturber log-uniform "
@@ -473,7 +608,7 @@ def run_ensemble(args, ws, rank, local):
         "graph_launches": int(s1.graph_launches - s0.graph_launches),
         "one_by_one": {"ms_per_step": solo_ms,
                        "value": n_all / (solo_ms * 1e-3),
-                       "speedup": solo_ms / (ms_max / args.steps),
+                       "speedup": solo_ms / (ms_max / steps),
                        "sample": f"each disk alone through nbody_sim, {args.solo_steps} steps "
                                  "after 2 warm-up, per-step times summed"},
         "e2e": {"value": n_all * e_steps / (e_ms * 1e-3), "unit": UNIT,
@@ -483,8 +618,7 @@ def run_ensemble(args, ws, rank, local):
         "clocks": ck,
     }
     ens.close()
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    return line
 
 
 def run_precision(args, ws, rank, local):
@@ -543,6 +677,14 @@ def run_precision(args, ws, rank, local):
 
 
 def run_adjoint(args, ws, rank, local):
+    if rank != 0:
+        return
+    import torch
+    torch.cuda.set_device(local)
+    print(json.dumps(adjoint_study(args, args.fd_components)), flush=True)
+
+
+def adjoint_study(args, fd_components):
     """Gradient study: N = 65536 disk (r in [0.5, 5] AU, m = 1e-8, eps 1e-3),
     gas drag 1e-3, perturber 3 M_J at 10 AU, 200 steps of dt 0.005, FP64
     state.  Loss: mass-weighted mean e^2 of the bodies ending inside 2 AU.
@@ -553,10 +695,7 @@ def run_adjoint(args, ws, rank, local):
     recording forward and the backward against the plain engine
     (nbody_sim, FP64 state, same physics) over the same steps."""
     import torch
-    if rank != 0:
-        return
     nb = importlib.import_module("nbody-sim_b200")
-    torch.cuda.set_device(local)
     n, steps, pm, pr = 65536, 200, 3.0, 10.0
     prm = nb.sim_params(dt=0.005, theta=0.5, softening=1e-3, star_mass=1.0, r_coll=0.0,
                         restitution=0.0, gas_drag_rate=1e-3, perturber_enabled=1,
@@ -608,7 +747,7 @@ def run_adjoint(args, ws, rank, local):
 
     speed = torch.sqrt((v0 * v0).sum(0))
     rng = np.random.default_rng(0)
-    picks = rng.choice(3 * n, min(args.fd_components, 3 * n), replace=False)
+    picks = rng.choice(3 * n, min(fd_components, 3 * n), replace=False)
     def fd_v(c, k, hrel):
         h = hrel * float(speed[k])
         vp = v0.clone(); vp[c, k] += h
@@ -679,7 +818,7 @@ def run_adjoint(args, ws, rank, local):
         "perturber": par,
     }
     eng.close()
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def run_c2(args, ws, rank, local):

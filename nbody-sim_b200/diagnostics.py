@@ -90,6 +90,43 @@ def force_errors(st, theta: float, eps: float, star_mass: float, targets, leaf_m
     return out
 
 
+def engine_force_errors(params, st, targets):
+    """The engine's own walk (nbody_sim with ``params``: the groups, walk mode
+    and leaf size a timed step uses) against the FP64 direct sum on the same
+    float32 positions, at the target indices: relative error of the total
+    acceleration and of the self-gravity part (a second engine with
+    star_mass 0) as median / p99 / max."""
+    import torch
+    nb = _nb()
+    n = len(st["x"])
+    tg = np.asarray(targets, np.int64)
+    acc = {}
+    for name, sm in (("self", 0.0), ("total", params.star_mass)):
+        p = type(params).from_buffer_copy(params)
+        p.star_mass = sm
+        p.state_precision = nb.STATE_F32
+        sim = nb.Sim(p, n)
+        sim.set_state(*[np.ascontiguousarray(st[k], np.float32)
+                        for k in ("x", "y", "z", "vx", "vy", "vz")], st["m"])
+        g = sim.get_state(accel=True)
+        acc[name] = np.stack([g[k][tg] for k in ("ax", "ay", "az")], 1).astype(np.float64)
+        status = sim.stats().status
+        sim.close()
+        if status:
+            raise RuntimeError(f"engine status {status} in the force-error run")
+    x64 = [torch.from_numpy(np.asarray(st[k], np.float32).astype(np.float64)).cuda()
+           for k in ("x", "y", "z")]
+    m32 = torch.from_numpy(np.ascontiguousarray(st["m"], np.float32)).cuda()
+    t32 = torch.from_numpy(tg.astype(np.int32)).cuda()
+    eps = params.softening
+    dx, dy, dz, _ = nb.direct_f64(*x64, m32, eps, targets=t32)
+    d_self = np.stack([dx.cpu().numpy(), dy.cpu().numpy(), dz.cpu().numpy()], 1)
+    xs = [np.asarray(st[k], np.float32)[tg].astype(np.float64) for k in ("x", "y", "z")]
+    d_total = d_self + np.stack(star_accel(*xs, eps, params.star_mass), 1)
+    return {"self": _summary(_rel_err(acc["self"], d_self)),
+            "total": _summary(_rel_err(acc["total"], d_total))}
+
+
 def conserved(st, m, eps: float, star_mass: float):
     """Softened energy (kinetic, star, pair parts) and L_y of a state.
 

@@ -119,6 +119,8 @@ class Port:
                                      C.c_double, C.c_int, _D, _D, _D, C.c_int]
         L.orc_energy_f64.argtypes = [_D, _D, _D, _D, _D, _D, _D, C.c_int, C.c_double,
                                      C.c_double, _D, _D, C.c_int]
+        L.orc_set_summarize_passes.argtypes = [C.c_int]
+        L.orc_make_disk.argtypes = [C.c_int] + [C.c_double] * 5 + [C.c_uint64] + [_D] * 6
 
     # -- tree -------------------------------------------------------------
     def build_tree(self, x, y, z, m):
@@ -269,6 +271,20 @@ class Port:
         self.lib.orc_perturber_force(*[_ptr(q, _F) for q in a + x], p.x, p.y, p.z, p.mass_msun,
                                      softening, len(x[0]))
         return a
+
+    def set_summarize_passes(self, passes: int):
+        """passes > 0: every later step summarizes the tree with the
+        reference's fixed number of parallel passes (BHTree.cu:501-516)
+        instead of the converged sweep; 0 restores the sweep."""
+        self.lib.orc_set_summarize_passes(int(passes))
+
+    def make_disk(self, n, r_min, r_max, sigma_e=0.01, sigma_i=0.005, star_mass=1.0, seed=0):
+        """The product's synthetic-disk recipe (nbody_make_disk), restated in
+        oracle/port.c: dict of float64 arrays x..vz."""
+        out = {k: np.zeros(n, np.float64) for k in ("x", "y", "z", "vx", "vy", "vz")}
+        self.lib.orc_make_disk(n, r_min, r_max, sigma_e, sigma_i, star_mass, seed,
+                               *[_ptr(out[k], _D) for k in ("x", "y", "z", "vx", "vy", "vz")])
+        return out
 
     # -- FoF -----------------------------------------------------------------
     def fof(self, x, y, z, link_length):

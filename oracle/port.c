@@ -182,6 +182,70 @@ void orc_tree_summarize(orc_tree* t) {
     t->unsummarized = unsum;
 }
 
+/* launchSummarizeKernel, BHTree.cu:501-516: `passes` parallel launches of
+ * bhtree_summarizeKernel (:282-317), each over every internal slot.  A pass
+ * here reads the previous pass's children and writes its own copy (a Jacobi
+ * sweep: the kernel's in-place passes can finish sooner, never later), so
+ * every node of height <= passes ends summarized, as in the reference.  This
+ * is the reference's amount of summarize work, for the timed CPU baseline;
+ * its values equal orc_tree_summarize's whenever the tree's height is at
+ * most `passes`. */
+static int g_summarize_passes = 0;
+
+void orc_set_summarize_passes(int passes) { g_summarize_passes = passes > 0 ? passes : 0; }
+
+void orc_tree_summarize_passes(orc_tree* t, int passes, int nthreads) {
+    const int n = t->n_bodies, root = t->n_total - 1;
+    int last = t->next_node < t->n_total ? t->next_node : t->n_total;
+    if (last > root) last = root;
+    const int slots = last - n + 1; /* [n, last) and the root */
+    float* nm = (float*)malloc((size_t)slots * 4 * sizeof(float));
+    int* nc = (int*)malloc((size_t)slots * sizeof(int));
+    set_threads(nthreads);
+    for (int pass = 0; pass < passes; ++pass) {
+#pragma omp parallel for schedule(static, 1024)
+        for (int j = 0; j < slots; ++j) {
+            const int node = (j == slots - 1) ? root : n + j;
+            float mm = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
+            int cnt = 0, ready = 1;
+            for (int k = 0; k < 8; ++k) {
+                int c = t->child[(long)node * 8 + k];
+                if (c < 0) continue;
+                if (t->count[c] == 0) { ready = 0; break; }
+                float cm = t->mass[c];
+                mm += cm;
+                cx += t->pos_x[c] * cm;
+                cy += t->pos_y[c] * cm;
+                cz += t->pos_z[c] * cm;
+                cnt += t->count[c];
+            }
+            if (ready && mm > 0.f) {
+                nm[4 * j] = cx / mm; nm[4 * j + 1] = cy / mm; nm[4 * j + 2] = cz / mm;
+                nm[4 * j + 3] = mm; nc[j] = cnt;
+            } else {
+                nm[4 * j] = t->pos_x[node]; nm[4 * j + 1] = t->pos_y[node];
+                nm[4 * j + 2] = t->pos_z[node]; nm[4 * j + 3] = t->mass[node];
+                nc[j] = t->count[node];
+            }
+        }
+#pragma omp parallel for schedule(static, 1024)
+        for (int j = 0; j < slots; ++j) {
+            const int node = (j == slots - 1) ? root : n + j;
+            t->pos_x[node] = nm[4 * j]; t->pos_y[node] = nm[4 * j + 1];
+            t->pos_z[node] = nm[4 * j + 2]; t->mass[node] = nm[4 * j + 3];
+            t->count[node] = nc[j];
+        }
+    }
+    int unsum = 0;
+    for (int j = 0; j < slots; ++j) {
+        const int node = (j == slots - 1) ? root : n + j;
+        if (t->count[node] == 0) unsum++;
+    }
+    t->unsummarized = unsum;
+    free(nm);
+    free(nc);
+}
+
 /* bhtree_sortKernel, BHTree.cu:322-352 */
 void orc_tree_sort(orc_tree* t) {
     int stack[2048];
@@ -465,7 +529,8 @@ void orc_compute_forces(orc_tree* t, const float* x, const float* y, const float
                         const float* m, float* ax, float* ay, float* az, int n,
                         const orc_step_params* sp, float sim_time, int nthreads) {
     orc_tree_build(t, x, y, z, m, n);
-    orc_tree_summarize(t);
+    if (g_summarize_passes > 0) orc_tree_summarize_passes(t, g_summarize_passes, nthreads);
+    else orc_tree_summarize(t);
     orc_tree_sort(t);
     orc_reset_acc(ax, ay, az, n);
     orc_force(t, x, y, z, ax, ay, az, sp->theta, sp->softening, sp->star_mass, nthreads);
@@ -627,4 +692,65 @@ void orc_energy_f64(const double* x, const double* y, const double* z, const dou
     }
     *energy = kin + star + pair;
     *ly = l;
+}
+
+/* ---------------------------------------------------------- disk recipe */
+
+/* The synthetic Keplerian disk that the product's nbody_make_disk writes,
+ * restated so that CPU-only callers (the reference arm of the benchmark) can
+ * build the same initial conditions without loading the product library.
+ * Semi-major axis by the inverse CDF of Sigma ~ r^-1.5
+ * (src/disk/DiskInit.cpp:42-44), Rayleigh e (capped at 0.9) and inclination,
+ * uniform node, periapsis and mean anomaly, Kepler's equation by Newton,
+ * perifocal -> +Z-pole frame -> disk plane XZ with +Y up.  Draw k of body i is
+ * splitmix64 (Vigna's published mixer) of splitmix64(seed) ^ (16 i + k). */
+static uint64_t orc_splitmix64(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+static double orc_unit(uint64_t seed_mix, uint64_t i, uint64_t k) {
+    return (double)(orc_splitmix64(seed_mix ^ (i * 16u + k)) >> 11) * (1.0 / 9007199254740992.0);
+}
+
+void orc_make_disk(int n, double r_min, double r_max, double sigma_e, double sigma_i,
+                   double mu, uint64_t seed, double* x, double* y, double* z, double* vx,
+                   double* vy, double* vz) {
+    const double two_pi = 6.283185307179586476925287;
+    const uint64_t sm = orc_splitmix64(seed);
+    const double sa = sqrt(r_min), sb = sqrt(r_max);
+#pragma omp parallel for schedule(static, 4096)
+    for (int i = 0; i < n; ++i) {
+        const double sr = orc_unit(sm, i, 0) * (sb - sa) + sa;
+        const double a = sr * sr;
+        double e = sigma_e * sqrt(-2.0 * log1p(-orc_unit(sm, i, 1)));
+        const double inc = sigma_i * sqrt(-2.0 * log1p(-orc_unit(sm, i, 2)));
+        if (e > 0.9) e = 0.9;
+        const double node = two_pi * orc_unit(sm, i, 3);
+        const double peri = two_pi * orc_unit(sm, i, 4);
+        const double mean = two_pi * orc_unit(sm, i, 5);
+        double ea = (e < 0.8) ? mean : 3.141592653589793;
+        for (int it = 0; it < 60; ++it) {
+            const double step = (ea - e * sin(ea) - mean) / (1.0 - e * cos(ea));
+            ea -= step;
+            if (fabs(step) < 1e-15) break;
+        }
+        const double ce = cos(ea), se = sin(ea), q = sqrt(1.0 - e * e);
+        const double nmot = sqrt(mu / (a * a * a)), den = 1.0 - e * ce;
+        const double px = a * (ce - e), py = a * q * se;
+        const double pvx = -a * nmot * se / den, pvy = a * nmot * q * ce / den;
+        const double cn = cos(node), sn = sin(node), cp = cos(peri), sp = sin(peri);
+        const double ci = cos(inc), si = sin(inc);
+        const double m11 = cn * cp - sn * sp * ci, m12 = -cn * sp - sn * cp * ci;
+        const double m21 = sn * cp + cn * sp * ci, m22 = -sn * sp + cn * cp * ci;
+        const double m31 = sp * si, m32 = cp * si;
+        x[i] = m11 * px + m12 * py;
+        y[i] = -(m31 * px + m32 * py);
+        z[i] = m21 * px + m22 * py;
+        vx[i] = m11 * pvx + m12 * pvy;
+        vy[i] = -(m31 * pvx + m32 * pvy);
+        vz[i] = m21 * pvx + m22 * pvy;
+    }
 }

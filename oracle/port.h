@@ -17,6 +17,8 @@
 #ifndef NBODY_ORACLE_PORT_H
 #define NBODY_ORACLE_PORT_H
 
+#include <stdint.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -115,6 +117,19 @@ void orc_energy_f64(const double* x, const double* y, const double* z, const dou
                     const double* vy, const double* vz, const double* m, int n,
                     double softening, double star_mass, double* energy, double* ly,
                     int nthreads);
+
+/* The fixed-pass summarize of the reference (launchSummarizeKernel,
+ * BHTree.cu:501-516).  orc_set_summarize_passes(20) makes every later
+ * orc_compute_forces / orc_step use it instead of the converged sweep (0
+ * restores the sweep); used to time the reference's own summarize work. */
+void orc_tree_summarize_passes(orc_tree* t, int passes, int nthreads);
+void orc_set_summarize_passes(int passes);
+
+/* The synthetic Keplerian disk recipe of the product's nbody_make_disk,
+ * restated for callers that must not load the product (FP64 SoA out). */
+void orc_make_disk(int n, double r_min, double r_max, double sigma_e, double sigma_i,
+                   double mu, uint64_t seed, double* x, double* y, double* z, double* vx,
+                   double* vy, double* vz);
 
 #ifdef __cplusplus
 }
