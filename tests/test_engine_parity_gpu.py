@@ -1,0 +1,236 @@
+"""The engine (nbody_sim) against the oracle at the stated configurations.
+
+* Full physics of the N = 131,072 disk (collisions with factor 5 and e = 0,
+  gas drag 1e-3 / T0, a 1 M_J perturber on a circular orbit at 5.2 AU,
+  dt 0.005 T0): the engine's fused stream kernel (dv + K2 + drag + K1 +
+  drift) and its walk-epilogue perturber against the restated reference loop
+  (src/main.cu:101-139, Integrator.cu:40-76, Perturber.cu:13-35), in every
+  state precision.  Drag and the perturber change the velocities by about
+  1e-6 over 20 steps, below the force-approximation gap between the two
+  engines, so their effect is also checked on its own: each engine's state
+  with the effect minus its state without it.
+* The small disk exactly as specified (N = 4,096, 100 steps, FoF every 10
+  steps with the collision radius as linking length): each output
+  snapshot's agg_size, labels and aggregate records bit-exact against the
+  reference's own detectAggregates (src/analysis/Aggregate.cpp:26-76), also at
+  a linking length large enough to form groups.
+* One output snapshot of the N = 131,072 full-physics run, FoF bit-exact
+  against detectAggregates (its O(N^2) loop, about 7 s a call).
+* The perturber launcher bit-exact against the reference's own kernel
+  (Perturber.cu:13-51) compiled for sm_100a.
+"""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, disk
+
+pytestmark = pytest.mark.gpu
+
+C2 = dict(n=131072, dt=0.005, theta=0.5, eps=1e-3, m=1e-8, factor=5.0, drag=1e-3,
+          pert_mjup=1.0, pert_r=5.2, pert_phase0=0.0, steps=20)
+STATE = ("x", "y", "z", "vx", "vy", "vz")
+
+
+def _r_coll(nb, factor, m):
+    return factor * nb.particle_physical_radius(m)
+
+
+def engine_run(nb, st, precision, drag, pert_on, steps, r_coll, cfg=C2):
+    prm = nb.sim_params(dt=cfg["dt"], theta=cfg["theta"], softening=cfg["eps"], star_mass=1.0,
+                        r_coll=r_coll, restitution=0.0, gas_drag_rate=drag,
+                        perturber_enabled=int(pert_on), perturber_mass_mjup=cfg["pert_mjup"],
+                        perturber_radius_au=cfg["pert_r"], perturber_phase0=cfg["pert_phase0"],
+                        state_precision=precision, leaf_max=8)
+    n = len(st["x"])
+    sim = nb.Sim(prm, n)
+    sim.set_state(*[st[k] for k in STATE], st["m"])
+    sim.step(steps)
+    sim.sync()
+    out = sim.get_state(double=True, accel=False)
+    assert sim.stats().status == 0
+    sim.close()
+    return out
+
+
+def oracle_run(port, st, drag, pert_on, steps, r_coll, cfg=C2):
+    pert = port.perturber(True, cfg["pert_mjup"], cfg["pert_r"], cfg["pert_phase0"], 1.0) \
+        if pert_on else None
+    sp = port.step_params(cfg["dt"], cfg["theta"], cfg["eps"], 1.0, r_coll=r_coll,
+                          restitution=0.0, gas_drag_rate=drag, collisions=True, pert=pert)
+    ref = {k: np.array(st[k], np.float32) for k in STATE + ("m",)}
+    port.run(ref, sp, steps)
+    return {k: ref[k].astype(np.float64) for k in STATE}
+
+
+@pytest.fixture(scope="module")
+def c2(nb, port):
+    """The C2 disk and the oracle's runs without and with drag / perturber."""
+    n = C2["n"]
+    d = nb.make_disk(n, 0.5, 5.0, 0.01, 0.005, 1.0, 0)
+    st = {k: d[k] for k in STATE}
+    st["m"] = np.full(n, C2["m"], np.float32)
+    st32 = {k: st[k].astype(np.float32) for k in STATE}
+    st32["m"] = st["m"]
+    r_coll = _r_coll(nb, C2["factor"], C2["m"])
+    runs = {(dr, pe): oracle_run(port, st32, C2["drag"] if dr else 0.0, pe, C2["steps"], r_coll)
+            for dr in (False, True) for pe in (False, True)}
+    return st, st32, r_coll, runs
+
+
+@pytest.mark.parametrize("precision", [1, 0, 2], ids=["f64", "f32", "f32x2"])
+def test_c2_physics_tracks_the_reference_loop(nb, cuda, c2, precision):
+    """All of C2's physics for 20 steps against the oracle: the same
+    tolerances as the gravity-only loop test (both engines approximate the
+    forces to ~1e-4 of the star-dominated total)."""
+    st, st32, r_coll, runs = c2
+    src = st if precision != 0 else st32
+    got = engine_run(nb, src, precision, C2["drag"], True, C2["steps"], r_coll)
+    ref = runs[(True, True)]
+    for k in ("x", "y", "z"):
+        d = np.abs(got[k] - ref[k])
+        print(f"{k}: max {d.max():.3e} median {np.median(d):.3e}")
+        assert d.max() < 2e-4 and np.median(d) < 2e-6, (k, d.max(), np.median(d))
+    for k in ("vx", "vy", "vz"):
+        d = np.abs(got[k] - ref[k])
+        print(f"{k}: max {d.max():.3e} median {np.median(d):.3e}")
+        assert d.max() < 2e-3 and np.median(d) < 2e-5, (k, d.max(), np.median(d))
+
+
+@pytest.mark.parametrize("effect", ["drag", "perturber"])
+def test_c2_drag_and_perturber_effects_match_the_reference(nb, cuda, c2, effect):
+    """The velocity change that drag (Integrator.cu:40-76) or the perturber
+    (Perturber.cu:13-35, orbit Perturber.h:39-66) alone makes over 20 C2
+    steps, engine (FP64 state) against oracle (FP32 state, the reference's).
+    The two changes are compared by their least-squares ratio over all
+    131,072 x 3 components and by the residual's RMS; the residual is set by
+    the FP32 rounding of the oracle's velocities (about 3e-8 per step), not by
+    the physics."""
+    st, st32, r_coll, runs = c2
+    dr, pe = (True, False) if effect == "drag" else (False, True)
+    base = engine_run(nb, st, 1, 0.0, False, C2["steps"], r_coll)
+    with_ = engine_run(nb, st, 1, C2["drag"] if dr else 0.0, pe, C2["steps"], r_coll)
+    de = np.concatenate([with_[k] - base[k] for k in ("vx", "vy", "vz")])
+    do = np.concatenate([runs[(dr, pe)][k] - runs[(False, False)][k]
+                         for k in ("vx", "vy", "vz")])
+    slope = float(de @ do) / float(do @ do)
+    resid = float(np.sqrt(np.mean((de - do) ** 2)) / np.sqrt(np.mean(do ** 2)))
+    print(f"{effect}: |dv| rms {np.sqrt(np.mean(do ** 2)):.3e} slope {slope:.6f} "
+          f"residual/rms {resid:.3e}")
+    assert np.sqrt(np.mean(do ** 2)) > 1e-7  # the effect is there
+    assert abs(slope - 1.0) < 2e-2, slope
+    assert resid < 0.3, resid
+
+
+# ----------------------------------------------------------------- C1
+def test_c1_run_fof_snapshots_bit_exact_vs_detect_aggregates(nb, cuda, port, refhost):
+    """C1 as specified: N = 4096, m = 1e-8, r in [0.5, 5] AU, eps 1e-3,
+    theta 0.5, collision factor 1, e = 0, no drag, dt 0.01, 100 steps, FP32
+    state, an output every 10 steps through the GPU pipeline (frame, FoF,
+    agg_size, aggregates) with the collision radius as linking length.  At
+    that radius this sparse disk forms no group, so every snapshot is also
+    checked at a 0.02 AU linking length, where it forms dozens."""
+    n, m = 4096, 1e-8
+    st = disk(nb, n, 0.5, 5.0, seed=0, m=m)
+    r_coll = _r_coll(nb, 1.0, m)
+    prm = nb.sim_params(dt=0.01, theta=0.5, softening=1e-3, star_mass=1.0, r_coll=r_coll,
+                        restitution=0.0, gas_drag_rate=0.0, state_precision=nb.STATE_F32,
+                        leaf_max=8)
+    sim = nb.Sim(prm, n)
+    sim.set_state(*[st[k] for k in STATE], st["m"])
+    groups_seen = 0
+    for out in range(10):
+        sim.step(10)
+        snap = sim.get_state(accel=False)
+        sim.output_begin(r_coll, m, 0.1 * (out + 1), out)
+        fr = sim.output_wait()
+        assert all(np.array_equal(fr[k], snap[k]) for k in ("x", "y", "z"))
+        for ll in (r_coll, 0.02):
+            rl, rsize, rng_, ra = refhost.detect_aggregates(*[snap[k] for k in STATE], ll, m)
+            labels, agg, ng = sim.fof(ll)
+            assert ng == rng_
+            assert np.array_equal(agg, rsize)
+            # labels: the smallest member index of each body's group
+            pl, ps, pg = port.fof(snap["x"], snap["y"], snap["z"], ll)
+            assert np.array_equal(labels, pl) and pg == ng
+            if ll == r_coll:
+                assert np.array_equal(fr["agg_size"], rsize)
+                assert fr["n_aggregates"] == rng_
+            groups_seen += ng if ll != r_coll else 0
+    assert groups_seen > 100
+    assert sim.stats().status == 0
+    got = sim.get_state(double=True, accel=False)
+    sim.close()
+    # the trajectory after the 100 steps against the restated reference loop
+    ref = {k: st[k].copy() for k in STATE + ("m",)}
+    sp = port.step_params(0.01, 0.5, 1e-3, 1.0, r_coll=r_coll, restitution=0.0)
+    port.run(ref, sp, 100)
+    for k in STATE:
+        d = np.abs(got[k] - ref[k])
+        print(f"C1 100 steps {k}: max {d.max():.3e} median {np.median(d):.3e}")
+        assert np.median(d) < 2e-5, (k, np.median(d))
+
+
+def test_c2_snapshot_fof_bit_exact_at_full_size(nb, cuda, refhost):
+    """One output of the C2 run (after 50 steps, FP64 state, all physics):
+    the pipeline's agg_size and records against detectAggregates on the same
+    FP32 frame, at the collision radius and at 2e-3 AU (many groups)."""
+    n, m = C2["n"], C2["m"]
+    d = nb.make_disk(n, 0.5, 5.0, 0.01, 0.005, 1.0, 0)
+    r_coll = _r_coll(nb, C2["factor"], m)
+    prm = nb.sim_params(dt=C2["dt"], theta=0.5, softening=1e-3, star_mass=1.0, r_coll=r_coll,
+                        restitution=0.0, gas_drag_rate=C2["drag"], perturber_enabled=1,
+                        perturber_mass_mjup=1.0, perturber_radius_au=5.2, perturber_phase0=0.0,
+                        state_precision=nb.STATE_F64)
+    sim = nb.Sim(prm, n)
+    sim.set_state(*[d[k] for k in STATE], np.full(n, m, np.float32))
+    sim.step(50)
+    snap = sim.get_state(accel=False)
+    for ll in (r_coll, 2e-3):
+        sim.output_begin(ll, m, 0.25, 1)
+        fr = sim.output_wait()
+        rl, rsize, rng_, ra = refhost.detect_aggregates(*[snap[k] for k in STATE], ll, m)
+        assert fr["n_aggregates"] == rng_
+        assert np.array_equal(fr["agg_size"], rsize)
+        got = fr["aggregates"]
+        assert [a.n_particles for a in got] == list(ra["n"])
+        c = np.array([[a.cx, a.cy, a.cz] for a in got], np.float32).reshape(-1)
+        v = np.array([[a.vx, a.vy, a.vz] for a in got], np.float32).reshape(-1)
+        assert np.array_equal(c, ra["c"]) and np.array_equal(v, ra["v"])
+        if ll != r_coll:
+            assert rng_ > 1000, rng_
+    assert sim.stats().status == 0
+    sim.close()
+
+
+# ----------------------------------------------------- perturber kernel
+def test_perturber_kernel_bit_exact_vs_reference(nb, cuda):
+    """launchPerturberForceKernel (Perturber.cu:39-51) from the reference
+    build against nbody_perturber_force, on a disk with nonzero a, at the
+    perturber positions of three times of the orbit."""
+    import oracle
+    path = os.path.join(ROOT, "oracle", "_ref", "libref_engine.so")
+    if not os.path.exists(path):
+        pytest.skip("oracle/_ref reference engine not built")
+    n = 5000
+    st = disk(nb, n, 0.5, 8.0, seed=11)
+    rng = np.random.default_rng(11)
+    for k in ("ax", "ay", "az"):
+        st[k] = rng.standard_normal(n).astype(np.float32) * 0.1
+    port = oracle.Port()
+    pert = port.perturber(True, 3.0, 6.0, 0.3, 1.0)
+    ref = oracle.RefEngine(n, path=path)
+    from test_gpu_core import to_gpu, host
+    p = to_gpu(nb, cuda, st)
+    ref.set_state(st)
+    for t in (0.0, 1.7, 12.5):
+        q = port.perturber_at(pert, t)
+        ref._chk(ref.lib.ref_eng_perturber_force(ref.h, q.x, q.y, q.z, q.mass_msun, 1e-3))
+        nb.perturber_force(p, q.x, q.y, q.z, q.mass_msun, 1e-3)
+    r = ref.get_state()
+    for k in ("ax", "ay", "az"):
+        np.testing.assert_array_equal(host(p, k), r[k], err_msg=k)
+    ref.close()
