@@ -209,23 +209,32 @@ int nbody_fof(nbody_tree* t, const float* x, const float* y, const float* z, int
  * an nbody_tree, which allocates.
  *
  * All scratch (sort buffers, tree, union-find arrays, a bounded stack-spill
- * area) lives in one statically sized device array inside libnbody_b200.so,
- * NBODY_FOF_NOALLOC_SCRATCH_BYTES bytes (12.6 MiB), which every GPU that
- * loads the library holds until the process exits.  n is limited to
- * NBODY_FOF_NOALLOC_MAX_N bodies; larger n returns NBODY_ERR_ARG with a
- * message naming the limit.  Inputs and outputs are as for nbody_fof
+ * area, and a set-up input) lives in one statically sized device array inside
+ * libnbody_b200.so, NBODY_FOF_NOALLOC_SCRATCH_BYTES bytes (13.2 MiB).  n is
+ * limited to NBODY_FOF_NOALLOC_MAX_N bodies; larger n returns NBODY_ERR_ARG
+ * with a message naming the limit.  Inputs and outputs are as for nbody_fof
  * (device x, y, z, labels, agg_size; host *n_groups), bit-identical results.
  *
- * The first call on each device looks up that device's address of the array
- * (cudaGetSymbolAddress) with the device current; later calls reuse it.  All
- * calls on a device share the one array and each call overwrites it: the
+ * Set-up.  The first call on each device sets that device up, with the
+ * device current: it looks up the device's address of the array
+ * (cudaGetSymbolAddress) and runs the FoF once on a set-up input of
+ * NBODY_FOF_NOALLOC_MAX_N bodies held in the array.  Under CUDA's lazy module
+ * loading (the default) that first use is when the runtime backs the array
+ * with device memory and loads the code of every kernel the call launches, so
+ * the first call DOES take device memory (the array, about 13 MiB, plus
+ * kernel code) and holds it until the process exits; later calls take none.
+ * Make that first call at start-up, before the rest of the GPU's memory is
+ * reserved and before any stream capture; a call with n = 0 (pointers other
+ * than n_groups may then be NULL) does only the set-up.
+ *
+ * All calls on a device share the one array and each call overwrites it: the
  * function runs on the legacy default stream and synchronises before it
  * returns, so calls from one host thread never overlap, but calls that could
  * overlap on the GPU (other host threads, or the default stream in
  * per-thread mode) race on the scratch and must be serialised by the caller.
  * The function calls no cudaMalloc, cudaFree or allocating library routine. */
 #define NBODY_FOF_NOALLOC_MAX_N 32768
-#define NBODY_FOF_NOALLOC_SCRATCH_BYTES 13241856
+#define NBODY_FOF_NOALLOC_SCRATCH_BYTES 13831680
 int nbody_fof_noalloc(const float* x, const float* y, const float* z, int n, float link_length,
                       int* labels, uint16_t* agg_size, int* n_groups);
 
@@ -314,6 +323,11 @@ typedef struct nbody_sim_params {
                                 group's own sources (no second tree walk).
                                 Same pairs; a body's impulses are summed in
                                 another order.                            */
+  int spill_cap;             /* walk / neighbour-search stack entries per
+                                warp kept in HBM when the shared-memory
+                                stack is full; <= 0: default (4096).  A
+                                walk that needs more stops, and the step
+                                reports NBODY_ERR_OVERFLOW (status bit 1). */
 } nbody_sim_params;
 
 /* Parameters of src/main.cu:58-73 from a Config (r_coll = factor * radius). */
@@ -526,6 +540,26 @@ int nbody_ensemble_stats_get(nbody_ensemble* e, nbody_ensemble_stats* out);
  * order; calls are synchronous. */
 typedef struct nbody_adjoint nbody_adjoint;
 int nbody_adjoint_create(const nbody_sim_params* p, int n, int n_steps, nbody_adjoint** out);
+/* How the backward gets at the forward's levels:
+ *  NBODY_ADJOINT_TAPE        (nbody_adjoint_create) every level's FP64 state
+ *                            and tape stay in HBM; the backward recomputes
+ *                            nothing.
+ *  NBODY_ADJOINT_CHECKPOINT  only FP64 states every checkpoint_every levels are
+ *                            kept; the backward rebuilds each level by running
+ *                            the step backwards in time (time-reversed
+ *                            leapfrog, drag inverted in closed form) from the
+ *                            level after it, re-records its tree and tape, and
+ *                            restarts each segment from its exact checkpoint;
+ *                            two levels of state and tape are held.  No replay.
+ *  NBODY_ADJOINT_DIRECT      self-gravity by FP64 direct summation over every
+ *                            pair instead of the tree (O(N^2) per step, every
+ *                            level kept): the reference gradient of the same
+ *                            loss; replay runs the direct-sum dynamics. */
+#define NBODY_ADJOINT_TAPE 0
+#define NBODY_ADJOINT_CHECKPOINT 1
+#define NBODY_ADJOINT_DIRECT 2
+int nbody_adjoint_create_mode(const nbody_sim_params* p, int n, int n_steps, int mode,
+                              int checkpoint_every, nbody_adjoint** out);
 int nbody_adjoint_destroy(nbody_adjoint* a);
 int nbody_adjoint_set_stream(nbody_adjoint* a, void* cuda_stream);
 /* Records n_steps steps from (x0..vz0, mass) with the perturber at
@@ -582,6 +616,13 @@ int nbody_direct_f64(const double* x, const double* y, const double* z, const fl
  * if a tile's look-back wait gave up. */
 int nbody_radix_sort_u32(uint32_t* keys, uint32_t* values, int n, int bits);
 int nbody_radix_sort_u64(uint64_t* keys, uint32_t* values, int n, int bits);
+/* Self-test of the radix sort's one bounded wait (no counterpart in the
+ * reference, whose DFS sort is one serial thread, BHTree.cu:322-352): the
+ * look-back of a tile over predecessor status words that no tile publishes.
+ * The wait must give up after its bound (about a second) instead of hanging;
+ * *status_bits receives the device status bits it raised (32, the bit a real
+ * sort reports as NBODY_ERR_OVERFLOW / NBODY_ERR_CUDA).  Synchronous. */
+int nbody_selftest_sort_wait(int* status_bits);
 
 /* ------------------------------------------------------ initial disks --- */
 

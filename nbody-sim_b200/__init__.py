@@ -122,7 +122,7 @@ class nbody_sim_params(C.Structure):
                 ("perturber_mass_mjup", C.c_float), ("perturber_radius_au", C.c_float),
                 ("perturber_phase0", C.c_float), ("state_precision", C.c_int),
                 ("leaf_max", C.c_int), ("targets_per_lane", C.c_int), ("walk_mode", C.c_int),
-                ("group_span", C.c_int), ("fuse_collisions", C.c_int)]
+                ("group_span", C.c_int), ("fuse_collisions", C.c_int), ("spill_cap", C.c_int)]
 
 
 NBODY_PHASES = 6
@@ -248,6 +248,8 @@ SIGNATURES = [
     ("nbody_ensemble_stats_get", C.c_int, [_VP, C.POINTER(nbody_ensemble_stats)]),
     ("nbody_adjoint_create", C.c_int, [C.POINTER(nbody_sim_params), C.c_int, C.c_int,
                                        C.POINTER(_VP)]),
+    ("nbody_adjoint_create_mode", C.c_int, [C.POINTER(nbody_sim_params), C.c_int, C.c_int,
+                                            C.c_int, C.c_int, C.POINTER(_VP)]),
     ("nbody_adjoint_destroy", C.c_int, [_VP]),
     ("nbody_adjoint_set_stream", C.c_int, [_VP, _VP]),
     ("nbody_adjoint_forward", C.c_int, [_VP] + [_VP] * 7 + [C.c_double, C.c_double] + [_VP] * 6),
@@ -259,6 +261,7 @@ SIGNATURES = [
     ("nbody_direct_f64", C.c_int, [_VP] * 4 + [C.c_int, _VP, C.c_int, C.c_double] + [_VP] * 4),
     ("nbody_radix_sort_u32", C.c_int, [_VP, _VP, C.c_int, C.c_int]),
     ("nbody_radix_sort_u64", C.c_int, [_VP, _VP, C.c_int, C.c_int]),
+    ("nbody_selftest_sort_wait", C.c_int, [_I]),
     ("nbody_make_disk", C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                   C.c_double, C.c_uint64, _D, _D, _D, _D, _D, _D]),
 ]
@@ -496,6 +499,14 @@ def fof_noalloc(x, y, z, link_length: float):
     _check(lib.nbody_fof_noalloc(x.data_ptr(), y.data_ptr(), z.data_ptr(), n, link_length,
                                  labels.data_ptr(), agg.data_ptr(), C.byref(ng)))
     return labels, agg, ng.value
+
+
+def fof_noalloc_setup():
+    """nbody_fof_noalloc with n = 0 on the current device: the device's
+    one-time set-up (the static scratch and the FoF kernels take their device
+    memory now, under lazy module loading), so that later calls take none."""
+    ng = C.c_int()
+    _check(lib.nbody_fof_noalloc(None, None, None, 0, 0.0, None, None, C.byref(ng)))
 
 
 @dataclass
@@ -872,10 +883,18 @@ class Adjoint:
     perturber's (mass in M_J, radius in AU), ``replay`` reruns the frozen-tree
     forward with other inputs."""
 
-    def __init__(self, params: nbody_sim_params, n: int, n_steps: int):
+    MODES = {"tape": 0, "checkpoint": 1, "direct": 2}
+
+    def __init__(self, params: nbody_sim_params, n: int, n_steps: int, mode: str = "tape",
+                 checkpoint_every: int = 50):
+        """mode: "tape" (every level in HBM), "checkpoint" (FP64 checkpoints
+        every ``checkpoint_every`` levels, levels rebuilt by time-reversed
+        leapfrog in the backward) or "direct" (FP64 direct-sum self-gravity:
+        the reference gradient)."""
         h = _VP()
-        _check(lib.nbody_adjoint_create(C.byref(params), n, n_steps, C.byref(h)))
-        self.h, self.n, self.n_steps, self.params = h, n, n_steps, params
+        _check(lib.nbody_adjoint_create_mode(C.byref(params), n, n_steps, self.MODES[mode],
+                                             int(checkpoint_every), C.byref(h)))
+        self.h, self.n, self.n_steps, self.params, self.mode = h, n, n_steps, params, mode
 
     def close(self):
         if getattr(self, "h", None):

@@ -124,3 +124,10 @@ extern "C" int nbody_radix_sort_u32(uint32_t* keys, uint32_t* values, int n, int
 extern "C" int nbody_radix_sort_u64(uint64_t* keys, uint32_t* values, int n, int bits) {
   return radix_sort_api<uint64_t>(keys, values, n, bits, "nbody_radix_sort_u64");
 }
+
+extern "C" int nbody_selftest_sort_wait(int* status_bits) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(status_bits, "nbody_selftest_sort_wait: null argument");
+    *status_bits = nb::sort_wait_selftest();
+  })
+}

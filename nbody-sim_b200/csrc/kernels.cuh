@@ -148,6 +148,9 @@ void launch_moment_prefix(TreeWork& w, int n, const double* xd, const double* yd
 double4* moment_tile_prefix(TreeWork& w, int n);
 
 size_t radix_sort_count_words(int n);
+// Runs the sort's look-back wait against tile-status words that nothing
+// publishes; returns the status bits it raised (kStatusSortWait expected).
+int sort_wait_selftest();
 // Stable LSD sort of (key, value) by the low `bits` bits of the keys; K is
 // uint32_t (single disk, 30-bit Morton keys) or uint64_t (ensemble: disk
 // index above the 30 Morton bits).

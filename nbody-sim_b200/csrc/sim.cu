@@ -529,7 +529,7 @@ struct SimBase {
     tree_alloc(tw, n);
     ax = dalloc<float>(n, "ax"); ay = dalloc<float>(n, "ay"); az = dalloc<float>(n, "az");
     dvx = dalloc<float>(n, "dvx"); dvy = dalloc<float>(n, "dvy"); dvz = dalloc<float>(n, "dvz");
-    spill_cap = 4096;
+    spill_cap = p.spill_cap > 0 ? p.spill_cap : 4096;
     spill = dalloc<int>((size_t)walk_spill_slots(0) * spill_cap, "walk spill");
     work = dalloc<int>(1, "work");
     inter = dalloc<unsigned long long>(1, "inter");
@@ -1348,6 +1348,7 @@ struct EnsembleImpl : EnsembleBase {
     check(cudaMemcpy(d_off, off.data(), sizeof(int) * (D + 1), cudaMemcpyHostToDevice),
           "offsets");
     pert_step = dalloc<int>(1, "perturber row");
+    spill_cap = p.spill_cap > 0 ? p.spill_cap : 4096;
     spill = dalloc<int>((size_t)walk_spill_slots(0) * spill_cap, "walk spill");
     work = dalloc<int>(1, "work");
     inter = dalloc<unsigned long long>(1, "inter");

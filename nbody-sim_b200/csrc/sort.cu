@@ -103,6 +103,55 @@ k_digit_hist(const K* __restrict__ keys, int n, int passes, uint32_t* __restrict
 }
 
 
+// Decoupled look-back of tile t > 0 for digit d: the sum of the counts of
+// tiles 0 .. t-1.  kLookAhead predecessors are loaded per round (tiles below
+// 0 read as an inclusive prefix of 0), so a walk back over aggregates takes
+// that many times fewer dependent L2 round trips; it stops at the first
+// inclusive prefix.  A round whose nearest predecessor has published nothing
+// waits; after kSpinLimit such rounds (about a second) the wait gives up,
+// raises kStatusSortWait and returns the partial sum.  That sum is no larger
+// than the true one, so the caller's scatter stays inside the output.
+__device__ __forceinline__ uint32_t lookback_prefix(const uint32_t* status, int t, int d,
+                                                    int* err) {
+  uint32_t excl = 0;
+  int j = t - 1, spins = 0;
+  while (j >= 0) {
+    uint32_t w[kLookAhead];
+#pragma unroll
+    for (int q = 0; q < kLookAhead; ++q)
+      w[q] = (j - q >= 0) ? __ldcv(status + (size_t)(j - q) * kBins + d) : kFlagP;
+    int used = 0;
+    bool done = false;
+#pragma unroll
+    for (int q = 0; q < kLookAhead; ++q) {
+      if (done || used < q) break;  // stop at the first unpublished word
+      const uint32_t f = w[q] & kFlagMask;
+      if (f == 0u) break;
+      excl += w[q] & kValMask;
+      used = q + 1;
+      if (f == kFlagP) done = true;
+    }
+    if (done) break;
+    if (used == 0) {
+      if (++spins > kSpinLimit) {
+        atomicOr(err, kStatusSortWait);
+        break;
+      }
+      continue;
+    }
+    j -= used;
+  }
+  return excl;
+}
+
+// Self-test of the look-back's bound: the wait of tile t over status words
+// that no tile publishes (the caller passes them zeroed) must give up and
+// raise kStatusSortWait in *err.  One block of kBins threads, one per digit.
+__global__ void __launch_bounds__(kBins)
+k_lookback_probe(const uint32_t* status, int t, int* err, uint32_t* out) {
+  out[threadIdx.x] = lookback_prefix(status, t, threadIdx.x, err);
+}
+
 // One pass: rank a tile, publish, look back, scatter.  ticket and status
 // (ntiles x 256 words) start at zero.
 template <typename K, int kItems>
@@ -185,36 +234,7 @@ k_onesweep(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
     atomicExch(mine, (t == 0 ? kFlagP : kFlagA) | run);
     uint32_t excl = 0;
     if (t > 0) {
-      // kLookAhead predecessors per round, loaded together (tiles below 0
-      // read as an inclusive prefix of 0): a walk back over aggregates takes
-      // that many times fewer dependent L2 round trips.
-      int j = t - 1, spins = 0;
-      while (j >= 0) {
-        uint32_t w[kLookAhead];
-#pragma unroll
-        for (int q = 0; q < kLookAhead; ++q)
-          w[q] = (j - q >= 0) ? __ldcv(status + (size_t)(j - q) * kBins + d) : kFlagP;
-        int used = 0;
-        bool done = false;
-#pragma unroll
-        for (int q = 0; q < kLookAhead; ++q) {
-          if (done || used < q) break;  // stop at the first unpublished word
-          const uint32_t f = w[q] & kFlagMask;
-          if (f == 0u) break;
-          excl += w[q] & kValMask;
-          used = q + 1;
-          if (f == kFlagP) done = true;
-        }
-        if (done) break;
-        if (used == 0) {
-          if (++spins > kSpinLimit) {
-            atomicOr(err, kStatusSortWait);
-            break;
-          }
-          continue;
-        }
-        j -= used;
-      }
+      excl = lookback_prefix(status, t, d, err);
       atomicExch(mine, kFlagP | ((excl + run) & kValMask));
     }
     uint32_t gbase = hincl - hcount;
@@ -434,6 +454,34 @@ void radix_sort_pairs(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt,
           "radix sort copy-back vals");
   }
   check(cudaGetLastError(), "radix_sort_pairs launch");
+}
+
+int sort_wait_selftest() {
+  constexpr int kTiles = 4;
+  uint32_t *status = nullptr, *out = nullptr;
+  int* err = nullptr;
+  auto release = [&]() {
+    cudaFree(status);
+    cudaFree(out);
+    cudaFree(err);
+  };
+  int bits = 0;
+  try {
+    check(cudaMalloc(&status, sizeof(uint32_t) * kTiles * kBins), "probe status");
+    check(cudaMalloc(&out, sizeof(uint32_t) * kBins), "probe out");
+    check(cudaMalloc(&err, sizeof(int)), "probe err");
+    check(cudaMemset(status, 0, sizeof(uint32_t) * kTiles * kBins), "probe status clear");
+    check(cudaMemset(err, 0, sizeof(int)), "probe err clear");
+    k_lookback_probe<<<1, kBins>>>(status, kTiles - 1, err, out);
+    check(cudaGetLastError(), "k_lookback_probe launch");
+    check(cudaDeviceSynchronize(), "k_lookback_probe");
+    check(cudaMemcpy(&bits, err, sizeof(int), cudaMemcpyDeviceToHost), "probe err read");
+  } catch (...) {
+    release();
+    throw;
+  }
+  release();
+  return bits;
 }
 
 template void radix_sort_pairs<uint32_t>(uint32_t*, uint32_t*, uint32_t*, uint32_t*, uint32_t*,
