@@ -45,6 +45,19 @@ def refhost():
 
 
 @pytest.fixture(scope="session")
+def reference_root():
+    """The reference checkout, where oracle/Makefile looks for it
+    (NBODY_REFERENCE_ROOT overrides); tests that read it skip without it."""
+    import subprocess
+    r = subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "print-ref"],
+                       capture_output=True, text=True)
+    path = r.stdout.strip()
+    if not path or not os.path.isdir(os.path.join(path, "src")):
+        pytest.skip("the reference checkout is absent (set NBODY_REFERENCE_ROOT)")
+    return path
+
+
+@pytest.fixture(scope="session")
 def cuda():
     import torch
     if not torch.cuda.is_available():

@@ -90,10 +90,8 @@ def test_config_defaults_match_reference_struct(nb):
     assert c["output_dir"] == "data" and not c["perturber_enabled"]
 
 
-def test_reference_configs_load_identically(nb, refhost):
-    cfgdir = "/root/reference/config"
-    if not os.path.isdir(cfgdir):
-        pytest.skip("reference checkout absent")
+def test_reference_configs_load_identically(nb, refhost, reference_root):
+    cfgdir = os.path.join(reference_root, "config")
     for f in sorted(os.listdir(cfgdir)):
         want = refhost.load_config(os.path.join(cfgdir, f))
         got = nb.load_config(os.path.join(cfgdir, f)).to_dict()
@@ -104,13 +102,11 @@ def test_reference_configs_load_identically(nb, refhost):
                 assert got[k] == want[k], (f, k)
 
 
-def test_reference_config_test_expectation_documented(nb, refhost):
+def test_reference_config_test_expectation_documented(nb, refhost, reference_root):
     """tests/test_config.cpp:5-21 expects output_every_n_steps == 200 and
     total_time == 2000 from config/simulation.json, which holds 50 / 500: the
     reference's own test fails there; both loaders return the file's values."""
-    path = "/root/reference/config/simulation.json"
-    if not os.path.exists(path):
-        pytest.skip("reference checkout absent")
+    path = os.path.join(reference_root, "config", "simulation.json")
     c = nb.load_config(path).to_dict()
     assert c["output_every_n_steps"] == 50 and c["total_time"] == 500.0
     assert c["n_particles"] == 100000 and np.float32(c["theta"]) == np.float32(0.5)
