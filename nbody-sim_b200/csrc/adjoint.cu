@@ -505,18 +505,27 @@ struct ApplyArgs {
 // plus the mass-weighted share of its ancestors' centre-of-mass adjoints),
 // the FP64 star and perturber Jacobians, then -- unless this is level 0 --
 // the drift and first-kick adjoints of the step that produced the level.
-template <bool kStep>
+// kDirect: the force adjoint came from the FP64 direct sum, already whole and
+// in caller order (mu), with no centre-of-mass range adds.
+template <bool kStep, bool kDirect = false>
 __global__ void __launch_bounds__(kThreads) k_adj_apply(const ApplyArgs a) {
   __shared__ double red[4][kThreads / 32];
   double pg[4] = {0.0, 0.0, 0.0, 0.0};
   for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < a.n;
        s += (long long)gridDim.x * blockDim.x) {
-    const uint32_t o = a.perm[s];
-    const double4 P = range_moments(a.rploc, a.rtpre, 0, (int)s + 1);
-    const double m = (double)a.body4[s].w;
-    double gx = a.gx[o] + a.mux[s] + m * P.x;
-    double gy = a.gy[o] + a.muy[s] + m * P.y;
-    double gz = a.gz[o] + a.muz[s] + m * P.z;
+    const uint32_t o = kDirect ? (uint32_t)s : a.perm[s];
+    double gx, gy, gz;
+    if (kDirect) {
+      gx = a.gx[o] + a.mux[s];
+      gy = a.gy[o] + a.muy[s];
+      gz = a.gz[o] + a.muz[s];
+    } else {
+      const double4 P = range_moments(a.rploc, a.rtpre, 0, (int)s + 1);
+      const double m = (double)a.body4[s].w;
+      gx = a.gx[o] + a.mux[s] + m * P.x;
+      gy = a.gy[o] + a.muy[s] + m * P.y;
+      gz = a.gz[o] + a.muz[s] + m * P.z;
+    }
     const double x = a.x[o], y = a.y[o], z = a.z[o];
     const double lx = a.lx[o], ly = a.ly[o], lz = a.lz[o];
     {  // star: a = -M x / r^3, da/dx = -M (I/r^3 - 3 x x^T / r^5)
@@ -566,7 +575,8 @@ __global__ void __launch_bounds__(kThreads) k_adj_apply(const ApplyArgs a) {
   }
 }
 
-struct DragAdjArgs {
+template <typename TA>
+struct DragAdjArgsT {
   // level L (start of the step) and L+1 (end), caller order
   const double* x0;
   const double* y0;
@@ -574,15 +584,15 @@ struct DragAdjArgs {
   const double* v0x;
   const double* v0y;
   const double* v0z;
-  const float* a0x;
-  const float* a0y;
-  const float* a0z;
+  const TA* a0x;
+  const TA* a0y;
+  const TA* a0z;
   const double* x1;
   const double* y1;
   const double* z1;
-  const float* a1x;
-  const float* a1y;
-  const float* a1z;
+  const TA* a1x;
+  const TA* a1y;
+  const TA* a1z;
   const double4* pert_tab;  // levels L and L+1
   int level;
   double eps, star_mass, dth, decay;
@@ -603,7 +613,8 @@ struct DragAdjArgs {
 // Second kick + drag of step L in reverse: v' = v_h + dt/2 A_{L+1} is
 // recomputed as the forward did (its v_phi sign selects the drag branch);
 // drag(x, v') = decay v' + (1 - decay) s sqrt(M) (-z, 0, x) r_xz^{-3/2}.
-__global__ void __launch_bounds__(kThreads) k_adj_drag(const DragAdjArgs a) {
+template <typename TA>
+__global__ void __launch_bounds__(kThreads) k_adj_drag(const DragAdjArgsT<TA> a) {
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n;
        i += (long long)gridDim.x * blockDim.x) {
     double gvx = a.gvx[i], gvy = a.gvy[i], gvz = a.gvz[i];
@@ -644,26 +655,198 @@ __global__ void __launch_bounds__(kThreads) k_adj_drag(const DragAdjArgs a) {
   }
 }
 
+// ------------------------------------------------- time-reversed leapfrog
+struct RevArgs {
+  const double* x;   // level L positions, velocities (caller order)
+  const double* vx;
+  const float* ax;   // level L self-gravity
+  const double4* pert_tab;
+  int level;
+  double* px;        // out: level L-1 positions
+  double* vh;        // out: v_h of step L-1
+  double eps, star_mass, dt, dth, decay;
+  int drag;
+  int n;
+};
+
+// Step L-1 run backwards from level L: the drag is inverted in closed form
+// (drag(x, v') = decay v' + (1 - decay) s sqrt(M) (-z, 0, x) r_xz^{-3/2},
+// s the sign of v_phi, which the drag keeps), then the second kick
+// (v_h = v' - dt/2 acc_L) and the drift (x_{L-1} = x_L - dt v_h).
+__global__ void __launch_bounds__(kThreads) k_dstep_rev(const RevArgs a) {
+  const size_t n1 = a.n, n2 = 2 * (size_t)a.n;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double x = a.x[i], y = a.x[n1 + i], z = a.x[n2 + i];
+    double vx = a.vx[i], vy = a.vx[n1 + i], vz = a.vx[n2 + i];
+    if (a.drag) {
+      const double rxz2 = fma(x, x, __dmul_rn(z, z));
+      if (!(rxz2 < 1e-12)) {
+        const double inv_r = 1.0 / sqrt(rxz2);
+        const double v_phi = __dmul_rn(fma(vx, -z, __dmul_rn(vz, x)), inv_r);
+        const double sgn = (v_phi >= 0.0) ? 1.0 : -1.0;
+        const double c = (1.0 - a.decay) * sgn * sqrt(a.star_mass) * inv_r * sqrt(inv_r);
+        const double inv_d = 1.0 / a.decay;
+        vx = (vx + c * z) * inv_d;
+        vz = (vz - c * x) * inv_d;
+        vy = vy * inv_d;
+      }
+    }
+    double ax, ay, az;
+    total_accel(x, y, z, a.ax[i], a.ax[n1 + i], a.ax[n2 + i], a.eps, a.star_mass,
+                a.pert_tab[a.level], ax, ay, az);
+    vx = fma(-a.dth, ax, vx); vy = fma(-a.dth, ay, vy); vz = fma(-a.dth, az, vz);
+    a.vh[i] = vx; a.vh[n1 + i] = vy; a.vh[n2 + i] = vz;
+    a.px[i] = fma(-a.dt, vx, x); a.px[n1 + i] = fma(-a.dt, vy, y);
+    a.px[n2 + i] = fma(-a.dt, vz, z);
+  }
+}
+
+// The first kick of step L-1 undone once level L-1's self-gravity is known:
+// v_{L-1} = v_h - dt/2 acc_{L-1}.
+__global__ void __launch_bounds__(kThreads) k_kick_rev(const double* __restrict__ x,
+                                                       const double* __restrict__ vh,
+                                                       const float* __restrict__ sg,
+                                                       const double4* __restrict__ pert_tab,
+                                                       int level, double eps, double star_mass,
+                                                       double dth, double* __restrict__ v,
+                                                       int n) {
+  const size_t n1 = n, n2 = 2 * (size_t)n;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    double ax, ay, az;
+    total_accel(x[i], x[n1 + i], x[n2 + i], sg[i], sg[n1 + i], sg[n2 + i], eps, star_mass,
+                pert_tab[level], ax, ay, az);
+    v[i] = fma(-dth, ax, vh[i]);
+    v[n1 + i] = fma(-dth, ay, vh[n1 + i]);
+    v[n2 + i] = fma(-dth, az, vh[n2 + i]);
+  }
+}
+
+// ------------------------------------------------ FP64 direct-sum dynamics
+// The reference gradient's dynamics: self-gravity by FP64 direct summation
+// over every pair (softened, no tree), a_i = sum_j m_j d_ij / r_ij^3 with
+// d_ij = x_j - x_i and r^2 = |d|^2 + eps^2.  Caller order; the source tile
+// is staged in shared memory.
+constexpr int kDirTile = 256;
+
+__global__ void __launch_bounds__(kDirTile) k_direct_acc(const double* __restrict__ x,
+                                                          const float* __restrict__ m, int n,
+                                                          double eps2, double* __restrict__ a) {
+  __shared__ double4 src[kDirTile];
+  const size_t n1 = n, n2 = 2 * (size_t)n;
+  const int i = blockIdx.x * kDirTile + threadIdx.x;
+  const bool valid = i < n;
+  const double px = valid ? x[i] : 0.0, py = valid ? x[n1 + i] : 0.0,
+               pz = valid ? x[n2 + i] : 0.0;
+  double sx = 0.0, sy = 0.0, sz = 0.0;
+  for (int t0 = 0; t0 < n; t0 += kDirTile) {
+    const int j = t0 + threadIdx.x;
+    src[threadIdx.x] = (j < n) ? make_double4(x[j], x[n1 + j], x[n2 + j], (double)m[j])
+                               : make_double4(0.0, 0.0, 0.0, 0.0);
+    __syncthreads();
+    const int k = min(kDirTile, n - t0);
+    for (int q = 0; q < k; ++q) {
+      const double4 s = src[q];
+      const double dx = s.x - px, dy = s.y - py, dz = s.z - pz;
+      const double r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
+      if (t0 + q == i || r2 <= 0.0) continue;
+      const double inv = 1.0 / sqrt(r2);
+      const double f = s.w * inv * inv * inv;
+      sx = fma(f, dx, sx); sy = fma(f, dy, sy); sz = fma(f, dz, sz);
+    }
+    __syncthreads();
+  }
+  if (valid) { a[i] = sx; a[n1 + i] = sy; a[n2 + i] = sz; }
+}
+
+// Vector-Jacobian product of the direct sum: with lam_i the adjoint of a_i
+// and J(d) = (I r^2 - 3 d d^T) / r^5 (symmetric, even in d), the adjoint of
+// x_k is sum_{j != k} J(d_kj) (m_k lam_j - m_j lam_k).  Written to mu
+// (caller order), which the apply kernel adds to the position adjoint.
+__global__ void __launch_bounds__(kDirTile) k_direct_vjp(const double* __restrict__ x,
+                                                          const float* __restrict__ m,
+                                                          const double* __restrict__ lam, int n,
+                                                          double eps2, double* __restrict__ mu) {
+  __shared__ double4 src[kDirTile];
+  __shared__ double3 sl[kDirTile];
+  const size_t n1 = n, n2 = 2 * (size_t)n;
+  const int k = blockIdx.x * kDirTile + threadIdx.x;
+  const bool valid = k < n;
+  const double px = valid ? x[k] : 0.0, py = valid ? x[n1 + k] : 0.0,
+               pz = valid ? x[n2 + k] : 0.0;
+  const double mk = valid ? (double)m[k] : 0.0;
+  const double lkx = valid ? lam[k] : 0.0, lky = valid ? lam[n1 + k] : 0.0,
+               lkz = valid ? lam[n2 + k] : 0.0;
+  double gx = 0.0, gy = 0.0, gz = 0.0;
+  for (int t0 = 0; t0 < n; t0 += kDirTile) {
+    const int j = t0 + threadIdx.x;
+    src[threadIdx.x] = (j < n) ? make_double4(x[j], x[n1 + j], x[n2 + j], (double)m[j])
+                               : make_double4(0.0, 0.0, 0.0, 0.0);
+    sl[threadIdx.x] = (j < n) ? make_double3(lam[j], lam[n1 + j], lam[n2 + j])
+                              : make_double3(0.0, 0.0, 0.0);
+    __syncthreads();
+    const int kk = min(kDirTile, n - t0);
+    for (int q = 0; q < kk; ++q) {
+      const double4 s = src[q];
+      const double3 l = sl[q];
+      const double dx = s.x - px, dy = s.y - py, dz = s.z - pz;
+      const double r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
+      if (t0 + q == k || r2 <= 0.0) continue;
+      const double inv = 1.0 / sqrt(r2);
+      const double inv3 = inv * inv * inv, inv5 = inv3 * inv * inv;
+      const double wx = mk * l.x - s.w * lkx, wy = mk * l.y - s.w * lky,
+                   wz = mk * l.z - s.w * lkz;
+      const double dw = dx * wx + dy * wy + dz * wz;
+      gx += wx * inv3 - 3.0 * dx * dw * inv5;
+      gy += wy * inv3 - 3.0 * dy * dw * inv5;
+      gz += wz * inv3 - 3.0 * dz * dw * inv5;
+    }
+    __syncthreads();
+  }
+  if (valid) { mu[k] = gx; mu[n1 + k] = gy; mu[n2 + k] = gz; }
+}
+
 }  // namespace
 
 // ================================================================== host
+// How the backward gets the forward's levels (nbody_adjoint_create_mode):
+//  kModeTape        every level's state and tape kept in HBM from the forward;
+//  kModeCheckpoint  FP64 states every `every` levels only: the backward
+//                   rebuilds each level by running the step backwards in time
+//                   (time-reversed leapfrog) from the level after it, re-records
+//                   its tree and tape, and restarts every segment from its
+//                   exact checkpoint, so rounding drift never spans more than
+//                   `every` steps; two levels of state and tape are held;
+//  kModeDirect      FP64 direct-sum self-gravity instead of the tree walk (every
+//                   level kept): the reference gradient of the same loss.
+constexpr int kModeTape = NBODY_ADJOINT_TAPE, kModeCheckpoint = NBODY_ADJOINT_CHECKPOINT,
+              kModeDirect = NBODY_ADJOINT_DIRECT;
+
 struct AdjointImpl {
   nbody_sim_params p{};
   int n = 0, steps = 0;
+  int mode = kModeTape;
+  int every = 0;  // checkpoint spacing (kModeCheckpoint)
   cudaStream_t st = 0;
   bool own_stream = false;
   TreeWork tw;
-  // per level L = 0..steps (caller order): positions, velocities, self-gravity
+  // level buffers (caller order): positions, velocities, self-gravity; one
+  // per level, or two (slot L & 1) in checkpoint mode
   std::vector<double*> X, V;
   std::vector<float*> A;
-  // per level tape: sort permutation, groups, group tape; the chunk pool is shared
+  std::vector<double*> AD;  // direct mode: FP64 self-gravity per level
+  std::vector<double*> CK;  // checkpoint mode: x, v (6n) at levels 0, every, 2 every, ...
+  double* vh = nullptr;     // checkpoint mode: v_h of the step being reversed
+  // per level tape: sort permutation, groups, group tape; tape chunks come
+  // from pool 0 (tape mode, every level) or pool L & 1 (checkpoint mode)
   std::vector<uint32_t*> perm;
   std::vector<int2*> groups, gtape;
-  int* ngroups = nullptr;  // per level, device
-  int2* pool = nullptr;
-  int* pool_next = nullptr;
-  int* pool_used = nullptr;
-  int pool_cap = 0;
+  int* ngroups = nullptr;  // per level slot, device
+  int2* pool[2] = {nullptr, nullptr};
+  int* pool_next[2] = {nullptr, nullptr};
+  int* pool_used = nullptr;  // device, one counter per pool
+  int pool_cap = 0;          // chunks per pool
   // scratch
   double *xs = nullptr, *ys = nullptr, *zs = nullptr;
   double *vw = nullptr, *xw = nullptr;      // work velocity (3n) and positions (2 x 3n)
@@ -699,10 +882,15 @@ struct AdjointImpl {
   double* rep_final[2] = {nullptr, nullptr};  // buffer holding a replay's final positions
   cudaStream_t cap_st = nullptr;
 
-  AdjointImpl(const nbody_sim_params& prm, int nn, int nsteps) {
+  int slot(int L) const { return mode == kModeCheckpoint ? (L & 1) : L; }
+  int pidx(int L) const { return mode == kModeCheckpoint ? (L & 1) : 0; }
+
+  AdjointImpl(const nbody_sim_params& prm, int nn, int nsteps, int md, int ck_every) {
     p = prm;
     n = nn;
     steps = nsteps;
+    mode = md;
+    every = ck_every;
     if (p.leaf_max <= 0) p.leaf_max = 8;
     check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "adjoint stream");
     own_stream = true;
@@ -710,15 +898,24 @@ struct AdjointImpl {
     tree_enable_overlap(tw);
     tw.group_max = 32;
     const size_t n3 = 3 * (size_t)n;
-    for (int L = 0; L <= steps; ++L) {
+    const int nslot = (mode == kModeCheckpoint) ? 2 : steps + 1;
+    for (int L = 0; L < nslot; ++L) {
       X.push_back(dalloc<double>(n3, "level positions"));
       V.push_back(dalloc<double>(n3, "level velocities"));
+      if (mode == kModeDirect) {
+        AD.push_back(dalloc<double>(n3, "level self-gravity"));
+        continue;
+      }
       A.push_back(dalloc<float>(n3, "level self-gravity"));
       perm.push_back(dalloc<uint32_t>(n, "level permutation"));
       groups.push_back(dalloc<int2>(n, "level groups"));
       gtape.push_back(dalloc<int2>(n, "level group tape"));
     }
-    ngroups = dalloc<int>(steps + 1, "level group counts");
+    if (mode == kModeCheckpoint) {
+      for (int L = 0; L <= steps; L += every) CK.push_back(dalloc<double>(2 * n3, "checkpoint"));
+      vh = dalloc<double>(n3, "reversed half-step velocity");
+    }
+    ngroups = dalloc<int>(nslot, "level group counts");
     xs = dalloc<double>(n, "sorted x"); ys = dalloc<double>(n, "sorted y");
     zs = dalloc<double>(n, "sorted z");
     vw = dalloc<double>(n3, "work velocity");
@@ -736,7 +933,7 @@ struct AdjointImpl {
     spill = dalloc<int>((size_t)walk_spill_slots(0) * spill_cap, "walk spill");
     work = dalloc<int>(1, "work");
     inter = dalloc<unsigned long long>(1, "interactions");
-    pool_used = dalloc<int>(1, "tape chunks used");
+    pool_used = dalloc<int>(2, "tape chunks used");
     aw64 = dalloc<double>(n3, "FP64 replay self-gravity");
     pert_fwd = dalloc<double4>(steps + 1, "perturber per level");
     pert_rep = dalloc<double4>(steps + 1, "replay perturber per level");
@@ -759,12 +956,14 @@ struct AdjointImpl {
     for (auto* q : X) cudaFree(q);
     for (auto* q : V) cudaFree(q);
     for (auto* q : A) cudaFree(q);
+    for (auto* q : AD) cudaFree(q);
+    for (auto* q : CK) cudaFree(q);
     for (auto* q : perm) cudaFree(q);
     for (auto* q : groups) cudaFree(q);
     for (auto* q : gtape) cudaFree(q);
-    void* ptrs[] = {ngroups, pool, pool_next, pool_used, xs, ys, zs, vw, xw, aw, aw64, gx, gv, lam,
-                    mu, radd, rploc, rtiles, pgrad, mass, spill, work, inter, pert_fwd,
-                    pert_rep};
+    void* ptrs[] = {ngroups, pool[0], pool[1], pool_next[0], pool_next[1], pool_used, xs, ys, zs,
+                    vw, xw, aw, aw64, gx, gv, lam, mu, radd, rploc, rtiles, pgrad, mass, spill,
+                    work, inter, pert_fwd, pert_rep, vh};
     for (void* q : ptrs)
       if (q) cudaFree(q);
     tree_free(tw);
@@ -817,9 +1016,13 @@ struct AdjointImpl {
     launches += 1;
   }
 
-  // Tree + recording walk at level L's positions X[L] -> A[L] and the tape.
+  // Tree + recording walk at level L's positions -> its self-gravity and tape
+  // (level slot L; checkpoint mode starts the slot's tape pool afresh).
   void record_level(int L) {
-    const double* x = X[L];
+    const int sl = slot(L), pi = pidx(L);
+    const double* x = X[sl];
+    if (mode == kModeCheckpoint)
+      check(cudaMemsetAsync(pool_used + pi, 0, sizeof(int), st), "tape reset");
     const size_t n1 = n, n2 = 2 * (size_t)n;
     launch_bbox<double>(tw, x, x + n1, x + n2, n, st);
     uint32_t* hist = radix_sort_prepare(tw.counts, 30, st);  // counted by the key kernel
@@ -830,21 +1033,22 @@ struct AdjointImpl {
                                                    zs, tw.body4);
     tw.prune_max = p.leaf_max;
     launch_tree<uint32_t>(tw, tw.keys, n, 30, 0, 1, tw.geom, nullptr, xs, ys, zs, st);
-    check(cudaMemcpyAsync(perm[L], tw.perm, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st),
-          "tape permutation");
-    k_copy_groups<<<grid1(n), kThreads, 0, st>>>(tw.groups, tw.n_groups, n, groups[L],
-                                                 ngroups + L);
+    check(cudaMemcpyAsync(perm[sl], tw.perm, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice,
+                          st), "tape permutation");
+    k_copy_groups<<<grid1(n), kThreads, 0, st>>>(tw.groups, tw.n_groups, n, groups[sl],
+                                                 ngroups + sl);
     WalkArgs w{};
     w.com = tw.oct.com; w.info = tw.oct.info; w.body = tw.body4; w.n = n;
     w.groups = tw.groups; w.n_groups = tw.n_groups;
     w.theta2 = p.theta * p.theta; w.eps = p.softening; w.star_mass = 0.f;
     w.star_in_walk = 0; w.leaf_max = p.leaf_max; w.pert = nullptr;
-    float* a = A[L];
+    float* a = A[sl];
     w.ax = a; w.ay = a + n1; w.az = a + n2; w.scatter = tw.perm;
     w.spill = spill; w.spill_cap = spill_cap; w.inter = inter; w.counters = nullptr;
     w.work = work; w.status = tw.status; w.targets_per_lane = 1;
-    w.tape = pool; w.tape_next = pool_next; w.tape_used = pool_used; w.tape_cap = pool_cap;
-    w.group_tape = gtape[L];
+    w.tape = pool[pi]; w.tape_next = pool_next[pi]; w.tape_used = pool_used + pi;
+    w.tape_cap = pool_cap;
+    w.group_tape = gtape[sl];
     launch_walk(w, st);
     // bbox, keys, 20 sort, gather, copy groups, karras, mark, 6 scans,
     // moment tiles, tile scan, emit, walk
@@ -904,11 +1108,14 @@ struct AdjointImpl {
     if (chunks <= pool_cap) return;
     check(cudaStreamSynchronize(st), "tape pool sync");
     drop_graphs();  // the captured runs hold the old pool
-    if (pool) cudaFree(pool);
-    if (pool_next) cudaFree(pool_next);
+    const int npools = (mode == kModeCheckpoint) ? 2 : 1;
     pool_cap = chunks;
-    pool = dalloc<int2>((size_t)pool_cap * kTapeChunk, "tape pool");
-    pool_next = dalloc<int>(pool_cap, "tape links");
+    for (int k = 0; k < npools; ++k) {
+      if (pool[k]) cudaFree(pool[k]);
+      if (pool_next[k]) cudaFree(pool_next[k]);
+      pool[k] = dalloc<int2>((size_t)pool_cap * kTapeChunk, "tape pool");
+      pool_next[k] = dalloc<int>(pool_cap, "tape links");
+    }
   }
 
   int read_status() {
@@ -928,22 +1135,26 @@ struct AdjointImpl {
       check(cudaMemcpyAsync(X[0] + (size_t)k * n, x0[k], sizeof(double) * n,
                             cudaMemcpyDeviceToDevice, st),
             "initial positions");
-    // size the tape pool from level 0, then record the whole run (again if
-    // the estimate fell short)
-    if (pool_cap == 0) ensure_pool(std::max(1024, n / 32 * 24));
-    for (int attempt = 0; attempt < 4; ++attempt) {
-      check(cudaMemsetAsync(tw.status, 0, sizeof(int), st), "status reset");
-      check(cudaMemsetAsync(pool_used, 0, sizeof(int), st), "tape reset");
-      record_level(0);
-      int used = 0;
-      check(cudaStreamSynchronize(st), "adjoint sync");
-      check(cudaMemcpy(&used, pool_used, sizeof(int), cudaMemcpyDeviceToHost), "tape used");
-      const long long need = (long long)used * (steps + 1) * 5 / 4 + 1024;
-      if (need > pool_cap) {
-        ensure_pool((int)std::min<long long>(need, 0x7fffffffLL / kTapeChunk));
-        continue;
+    // size the tape pool(s) from level 0, then record the whole run (again
+    // if the estimate fell short)
+    if (mode != kModeDirect) {
+      if (pool_cap == 0) ensure_pool(std::max(1024, n / 32 * 24));
+      for (int attempt = 0; attempt < 4; ++attempt) {
+        check(cudaMemsetAsync(tw.status, 0, sizeof(int), st), "status reset");
+        check(cudaMemsetAsync(pool_used, 0, 2 * sizeof(int), st), "tape reset");
+        record_level(0);
+        int used = 0;
+        check(cudaStreamSynchronize(st), "adjoint sync");
+        check(cudaMemcpy(&used, pool_used, sizeof(int), cudaMemcpyDeviceToHost), "tape used");
+        const long long need = (mode == kModeTape)
+                                   ? (long long)used * (steps + 1) * 5 / 4 + 1024
+                                   : (long long)used * 2 + 1024;
+        if (need > pool_cap) {
+          ensure_pool((int)std::min<long long>(need, 0x7fffffffLL / kTapeChunk));
+          continue;
+        }
+        break;
       }
-      break;
     }
     upload_pert(pert_fwd, pm, pr);
     for (int attempt = 0; attempt < 3; ++attempt) {
@@ -952,23 +1163,14 @@ struct AdjointImpl {
                               cudaMemcpyDeviceToDevice, st),
               "initial velocities");
       check(cudaEventRecord(e0, st), "event");
-      run_graph(g_fwd, [&] {
-        check(cudaMemsetAsync(tw.status, 0, sizeof(int), st), "status reset");
-        check(cudaMemsetAsync(pool_used, 0, sizeof(int), st), "tape reset");
-        record_level(0);
-        for (int L = 0; L <= steps; ++L) {
-          const bool end = L > 0, begin = L < steps;
-          launch_step(end, begin, step_args<float>(X[L], vw, A[L], V[L],
-                                                   begin ? X[L + 1] : nullptr, pert_fwd, L));
-          if (begin) record_level(L + 1);
-        }
-      });
+      run_graph(g_fwd, [&] { forward_levels(); });
       check(cudaEventRecord(e1, st), "event");
       const int s = read_status();
       if (s & kStatusTapeFull) {
-        int used = 0;
-        check(cudaMemcpy(&used, pool_used, sizeof(int), cudaMemcpyDeviceToHost), "tape used");
-        ensure_pool((int)std::min<long long>((long long)used * 3 / 2 + 1024,
+        int used[2] = {0, 0};
+        check(cudaMemcpy(used, pool_used, 2 * sizeof(int), cudaMemcpyDeviceToHost), "tape used");
+        const int u = std::max(used[0], used[1]);
+        ensure_pool((int)std::min<long long>((long long)u * 3 / 2 + 1024,
                                              0x7fffffffLL / kTapeChunk));
         continue;
       }
@@ -981,11 +1183,47 @@ struct AdjointImpl {
     throw ArgError("adjoint forward: tape pool could not be sized", NBODY_ERR_OVERFLOW);
   }
 
+  // The forward's launches (captured as one graph): every level's forces and
+  // the step to the next level.  Tape mode keeps every level; checkpoint mode
+  // writes two level slots and copies (x, v) out every `every` levels; direct
+  // mode sums the self-gravity pair by pair in FP64.
+  void forward_levels() {
+    check(cudaMemsetAsync(tw.status, 0, sizeof(int), st), "status reset");
+    check(cudaMemsetAsync(pool_used, 0, 2 * sizeof(int), st), "tape reset");
+    const size_t n3 = 3 * (size_t)n;
+    if (mode == kModeDirect) {
+      const double eps2 = (double)p.softening * (double)p.softening;
+      for (int L = 0; L <= steps; ++L) {
+        k_direct_acc<<<div_up(n, kDirTile), kDirTile, 0, st>>>(X[L], mass, n, eps2, AD[L]);
+        const bool end = L > 0, begin = L < steps;
+        launch_step(end, begin, step_args<double>(X[L], vw, AD[L], V[L],
+                                                  begin ? X[L + 1] : nullptr, pert_fwd, L));
+        launches += 1;
+      }
+      return;
+    }
+    record_level(0);
+    for (int L = 0; L <= steps; ++L) {
+      const bool end = L > 0, begin = L < steps;
+      const int sl = slot(L);
+      launch_step(end, begin, step_args<float>(X[sl], vw, A[sl], V[sl],
+                                               begin ? X[slot(L + 1)] : nullptr, pert_fwd, L));
+      if (mode == kModeCheckpoint && L % every == 0) {
+        double* c = CK[L / every];
+        check(cudaMemcpyAsync(c, X[sl], sizeof(double) * n3, cudaMemcpyDeviceToDevice, st),
+              "checkpoint x");
+        check(cudaMemcpyAsync(c + n3, V[sl], sizeof(double) * n3, cudaMemcpyDeviceToDevice, st),
+              "checkpoint v");
+      }
+      if (begin) record_level(L + 1);
+    }
+  }
+
   // Level L's bodies in its recorded order and their moment prefix.
   void level_bodies(int L, const double* x) {
     const size_t n1 = n, n2 = 2 * (size_t)n;
-    k_gather_sorted<<<grid1(n), kThreads, 0, st>>>(perm[L], x, x + n1, x + n2, mass, n, xs, ys,
-                                                   zs, tw.body4);
+    k_gather_sorted<<<grid1(n), kThreads, 0, st>>>(perm[slot(L)], x, x + n1, x + n2, mass, n,
+                                                   xs, ys, zs, tw.body4);
     launch_moment_prefix(tw, n, xs, ys, zs, st);
     launches += 3;
   }
@@ -995,12 +1233,13 @@ struct AdjointImpl {
     r.body4 = tw.body4;
     r.ploc = tw.mom_ploc;
     r.tpre = moment_tile_prefix(tw, n);
-    r.perm = perm[L];
-    r.groups = groups[L];
-    r.n_groups = ngroups + L;
-    r.group_tape = gtape[L];
-    r.tape = pool;
-    r.tape_next = pool_next;
+    const int sl = slot(L);
+    r.perm = perm[sl];
+    r.groups = groups[sl];
+    r.n_groups = ngroups + sl;
+    r.group_tape = gtape[sl];
+    r.tape = pool[pidx(L)];
+    r.tape_next = pool_next[pidx(L)];
     r.eps2 = p.softening * p.softening;
     r.work = work;
     r.status = tw.status;
@@ -1032,6 +1271,10 @@ struct AdjointImpl {
   void replay(const double* const* x0, double mass_mj, double radius, double* const* out,
               bool fp64) {
     if (!recorded) throw ArgError("adjoint replay: no recorded forward", NBODY_ERR_STATE);
+    if (mode == kModeCheckpoint)
+      throw ArgError("adjoint replay: a checkpointed engine keeps no tape to replay (use a "
+                     "tape-mode engine)", NBODY_ERR_STATE);
+    if (mode == kModeDirect) fp64 = true;
     const size_t n3 = 3 * (size_t)n;
     upload_pert(pert_rep, mass_mj, radius);
     for (int k = 0; k < 3; ++k) {
@@ -1047,9 +1290,18 @@ struct AdjointImpl {
       double* xa = xw;
       double* xb = xw + n3;
       for (int L = 0; L <= steps; ++L) {
+        const bool end = L > 0, begin = L < steps;
+        if (mode == kModeDirect) {  // the direct-sum dynamics from the new inputs
+          const double eps2 = (double)p.softening * (double)p.softening;
+          k_direct_acc<<<div_up(n, kDirTile), kDirTile, 0, st>>>(xa, mass, n, eps2, aw64);
+          launches += 1;
+          launch_step(end, begin, step_args<double>(xa, vw, aw64, nullptr, begin ? xb : nullptr,
+                                                    pert_rep, L));
+          if (begin) std::swap(xa, xb);
+          continue;
+        }
         level_bodies(L, xa);
         ReplayArgs r = replay_args(L);
-        const bool end = L > 0, begin = L < steps;
         if (fp64) {
           r.dax = aw64; r.day = aw64 + n; r.daz = aw64 + 2 * (size_t)n;
           r.xs = xs; r.ys = ys; r.zs = zs;
@@ -1081,7 +1333,12 @@ struct AdjointImpl {
   // Force adjoint at level L: lam (caller order) -> added to gx; then, for
   // L > 0, the drift and first-kick adjoints of step L-1.
   void force_adjoint(int L, bool step) {
-    level_bodies(L, X[L]);
+    const int sl = slot(L);
+    if (mode == kModeDirect) {
+      force_adjoint_direct(L, step);
+      return;
+    }
+    level_bodies(L, X[sl]);
     check(cudaMemsetAsync(radd, 0, sizeof(double4) * (n + 1), st), "range add reset");
     ReplayArgs r = replay_args(L);
     r.lx = lam; r.ly = lam + n; r.lz = lam + 2 * (size_t)n;
@@ -1092,11 +1349,33 @@ struct AdjointImpl {
     double4* tpre = rtiles + (ntiles + 1);
     k_prefix4_tiles<<<ntiles, kThreads, 0, st>>>(radd, n + 1, rploc, rtiles);
     k_tiles_scan4<<<1, 32, 0, st>>>(rtiles, ntiles, tpre);
-    ApplyArgs a{};
-    a.perm = perm[L]; a.body4 = tw.body4;
-    a.mux = mu; a.muy = mu + n; a.muz = mu + 2 * (size_t)n;
+    ApplyArgs a = apply_args(L);
+    a.perm = perm[sl]; a.body4 = tw.body4;
     a.rploc = rploc; a.rtpre = tpre;
-    a.x = X[L]; a.y = X[L] + n; a.z = X[L] + 2 * (size_t)n;
+    if (step) k_adj_apply<true><<<grid1(n), kThreads, 0, st>>>(a);
+    else k_adj_apply<false><<<grid1(n), kThreads, 0, st>>>(a);
+    check(cudaGetLastError(), "adjoint apply launch");
+    launches += 4;
+  }
+
+  // The direct-sum engine's force adjoint at level L: the pairwise
+  // vector-Jacobian product, then the per-body star, perturber, drift and
+  // kick adjoints.
+  void force_adjoint_direct(int L, bool step) {
+    const double eps2 = (double)p.softening * (double)p.softening;
+    k_direct_vjp<<<div_up(n, kDirTile), kDirTile, 0, st>>>(X[L], mass, lam, n, eps2, mu);
+    ApplyArgs a = apply_args(L);
+    if (step) k_adj_apply<true, true><<<grid1(n), kThreads, 0, st>>>(a);
+    else k_adj_apply<false, true><<<grid1(n), kThreads, 0, st>>>(a);
+    check(cudaGetLastError(), "adjoint apply launch");
+    launches += 2;
+  }
+
+  ApplyArgs apply_args(int L) {
+    const int sl = slot(L);
+    ApplyArgs a{};
+    a.mux = mu; a.muy = mu + n; a.muz = mu + 2 * (size_t)n;
+    a.x = X[sl]; a.y = X[sl] + n; a.z = X[sl] + 2 * (size_t)n;
     a.lx = lam; a.ly = lam + n; a.lz = lam + 2 * (size_t)n;
     a.gx = gx; a.gy = gx + n; a.gz = gx + 2 * (size_t)n;
     a.gvx = gv; a.gvy = gv + n; a.gvz = gv + 2 * (size_t)n;
@@ -1107,10 +1386,7 @@ struct AdjointImpl {
     a.dt = (double)p.dt; a.dth = (double)p.dt * 0.5;
     a.pgrad = pgrad + 4 * (size_t)L;
     a.n = n;
-    if (step) k_adj_apply<true><<<grid1(n), kThreads, 0, st>>>(a);
-    else k_adj_apply<false><<<grid1(n), kThreads, 0, st>>>(a);
-    check(cudaGetLastError(), "adjoint apply launch");
-    launches += 4;
+    return a;
   }
 
   // Adjoint of the final state (device, caller order) -> adjoint of the
@@ -1129,34 +1405,88 @@ struct AdjointImpl {
     finish_backward(g_init, g_par);
   }
 
+  // The drift, second-kick and drag adjoints of step L (levels L and L+1).
+  template <typename TA>
+  void drag_adjoint(int L, const TA* a0, const TA* a1) {
+    const int s0 = slot(L), s1 = slot(L + 1);
+    DragAdjArgsT<TA> d{};
+    d.x0 = X[s0]; d.y0 = X[s0] + n; d.z0 = X[s0] + 2 * (size_t)n;
+    d.v0x = V[s0]; d.v0y = V[s0] + n; d.v0z = V[s0] + 2 * (size_t)n;
+    d.a0x = a0; d.a0y = a0 + n; d.a0z = a0 + 2 * (size_t)n;
+    d.x1 = X[s1]; d.y1 = X[s1] + n; d.z1 = X[s1] + 2 * (size_t)n;
+    d.a1x = a1; d.a1y = a1 + n; d.a1z = a1 + 2 * (size_t)n;
+    d.pert_tab = pert_fwd;
+    d.level = L;
+    d.eps = p.softening; d.star_mass = p.star_mass; d.dth = (double)p.dt * 0.5;
+    d.drag = p.gas_drag_rate > 0.f;
+    d.decay = d.drag ? std::exp(-(double)p.gas_drag_rate * (double)p.dt) : 1.0;
+    d.gx = gx; d.gy = gx + n; d.gz = gx + 2 * (size_t)n;
+    d.gvx = gv; d.gvy = gv + n; d.gvz = gv + 2 * (size_t)n;
+    d.plx = lam; d.ply = lam + n; d.plz = lam + 2 * (size_t)n;
+    d.n = n;
+    k_adj_drag<TA><<<grid1(n), kThreads, 0, st>>>(d);
+    check(cudaGetLastError(), "k_adj_drag launch");
+    launches += 1;
+  }
+
   // Every level of the backward (captured as one graph).
   void backward_levels() {
     const size_t n3 = 3 * (size_t)n;
     check(cudaMemsetAsync(lam, 0, sizeof(double) * n3, st), "pending reset");
     check(cudaMemsetAsync(pgrad, 0, sizeof(double) * 4 * (steps + 1), st), "perturber reset");
     check(cudaMemsetAsync(tw.status, 0, sizeof(int), st), "status reset");
-    const double dth = (double)p.dt * 0.5;
-    const bool drag = p.gas_drag_rate > 0.f;
-    const double decay = drag ? std::exp(-(double)p.gas_drag_rate * (double)p.dt) : 1.0;
+    if (mode == kModeCheckpoint) {
+      backward_levels_reversed();
+      return;
+    }
     for (int L = steps - 1; L >= 0; --L) {
-      DragAdjArgs d{};
-      d.x0 = X[L]; d.y0 = X[L] + n; d.z0 = X[L] + 2 * (size_t)n;
-      d.v0x = V[L]; d.v0y = V[L] + n; d.v0z = V[L] + 2 * (size_t)n;
-      d.a0x = A[L]; d.a0y = A[L] + n; d.a0z = A[L] + 2 * (size_t)n;
-      d.x1 = X[L + 1]; d.y1 = X[L + 1] + n; d.z1 = X[L + 1] + 2 * (size_t)n;
-      d.a1x = A[L + 1]; d.a1y = A[L + 1] + n; d.a1z = A[L + 1] + 2 * (size_t)n;
-      d.pert_tab = pert_fwd;
-      d.level = L;
-      d.eps = p.softening; d.star_mass = p.star_mass; d.dth = dth; d.decay = decay;
-      d.drag = drag;
-      d.gx = gx; d.gy = gx + n; d.gz = gx + 2 * (size_t)n;
-      d.gvx = gv; d.gvy = gv + n; d.gvz = gv + 2 * (size_t)n;
-      d.plx = lam; d.ply = lam + n; d.plz = lam + 2 * (size_t)n;
-      d.n = n;
-      k_adj_drag<<<grid1(n), kThreads, 0, st>>>(d);
-      check(cudaGetLastError(), "k_adj_drag launch");
-      launches += 1;
+      if (mode == kModeDirect) drag_adjoint<double>(L, AD[L], AD[L + 1]);
+      else drag_adjoint<float>(L, A[L], A[L + 1]);
       force_adjoint(L + 1, true);
+    }
+    force_adjoint(0, false);
+  }
+
+  // Checkpoint mode: level `steps` is still in its slot from the forward.
+  // Each earlier level is rebuilt by running step L-1 backwards from level L
+  // (k_dstep_rev), its tree and tape re-recorded (which also gives its
+  // self-gravity, so the first kick is undone too, k_kick_rev); a level that
+  // holds a checkpoint is copied back exactly instead.
+  void backward_levels_reversed() {
+    const size_t n3 = 3 * (size_t)n;
+    const double dth = (double)p.dt * 0.5;
+    for (int L = steps; L >= 1; --L) {
+      const int Lm = L - 1, s = slot(L), sm = slot(Lm);
+      const bool ck = (Lm % every) == 0;
+      if (ck) {
+        const double* c = CK[Lm / every];
+        check(cudaMemcpyAsync(X[sm], c, sizeof(double) * n3, cudaMemcpyDeviceToDevice, st),
+              "checkpoint x");
+        check(cudaMemcpyAsync(V[sm], c + n3, sizeof(double) * n3, cudaMemcpyDeviceToDevice, st),
+              "checkpoint v");
+      } else {
+        RevArgs r{};
+        r.x = X[s]; r.vx = V[s]; r.ax = A[s];
+        r.pert_tab = pert_fwd; r.level = L;
+        r.px = X[sm]; r.vh = vh;
+        r.eps = p.softening; r.star_mass = p.star_mass;
+        r.dt = (double)p.dt; r.dth = dth;
+        r.drag = p.gas_drag_rate > 0.f;
+        r.decay = r.drag ? std::exp(-(double)p.gas_drag_rate * (double)p.dt) : 1.0;
+        r.n = n;
+        k_dstep_rev<<<grid1(n), kThreads, 0, st>>>(r);
+        check(cudaGetLastError(), "k_dstep_rev launch");
+        launches += 1;
+      }
+      record_level(Lm);
+      if (!ck) {
+        k_kick_rev<<<grid1(n), kThreads, 0, st>>>(X[sm], vh, A[sm], pert_fwd, Lm, p.softening,
+                                                   p.star_mass, dth, V[sm], n);
+        check(cudaGetLastError(), "k_kick_rev launch");
+        launches += 1;
+      }
+      drag_adjoint<float>(Lm, A[sm], A[s]);
+      force_adjoint(L, true);
     }
     force_adjoint(0, false);
   }
@@ -1195,12 +1525,18 @@ struct AdjointImpl {
     g_par[1] = gr;
   }
 
+  // Device memory that holds the forward for the backward: the tape (chunk
+  // pools and per-level permutation and groups) and the level states
+  // (checkpoints included).
   size_t tape_bytes() const {
-    return (size_t)pool_cap * (kTapeChunk * sizeof(int2) + sizeof(int)) +
-           (size_t)(steps + 1) * n * (sizeof(uint32_t) + 2 * sizeof(int2));
+    const size_t pools = (mode == kModeCheckpoint) ? 2 : (mode == kModeTape ? 1 : 0);
+    return pools * (size_t)pool_cap * (kTapeChunk * sizeof(int2) + sizeof(int)) +
+           perm.size() * n * (sizeof(uint32_t) + 2 * sizeof(int2));
   }
   size_t state_bytes() const {
-    return (size_t)(steps + 1) * n * (6 * sizeof(double) + 3 * sizeof(float));
+    const size_t lv = X.size() * n * 6 * sizeof(double) + A.size() * n * 3 * sizeof(float) +
+                      AD.size() * n * 3 * sizeof(double);
+    return lv + CK.size() * n * 6 * sizeof(double) + (vh ? n * 3 * sizeof(double) : 0);
   }
 };
 
@@ -1212,7 +1548,8 @@ struct nbody_adjoint {
 
 extern "C" {
 
-int nbody_adjoint_create(const nbody_sim_params* p, int n, int n_steps, nbody_adjoint** out) {
+int nbody_adjoint_create_mode(const nbody_sim_params* p, int n, int n_steps, int mode,
+                              int checkpoint_every, nbody_adjoint** out) {
   NBODY_API_BODY({
     NBODY_REQUIRE(p && out, "nbody_adjoint_create: null argument");
     *out = nullptr;
@@ -1221,8 +1558,19 @@ int nbody_adjoint_create(const nbody_sim_params* p, int n, int n_steps, nbody_ad
     NBODY_REQUIRE(p->dt > 0.f, "nbody_adjoint_create: dt must be positive");
     NBODY_REQUIRE(p->r_coll <= 0.f,
                   "nbody_adjoint_create: collisions are not differentiable (r_coll must be 0)");
-    *out = new nbody_adjoint{new nb::AdjointImpl(*p, n, n_steps)};
+    NBODY_REQUIRE(mode == NBODY_ADJOINT_TAPE || mode == NBODY_ADJOINT_CHECKPOINT ||
+                      mode == NBODY_ADJOINT_DIRECT,
+                  "nbody_adjoint_create: unknown mode");
+    NBODY_REQUIRE(mode != NBODY_ADJOINT_CHECKPOINT || checkpoint_every >= 1,
+                  "nbody_adjoint_create: checkpoint_every must be >= 1");
+    NBODY_REQUIRE(mode != NBODY_ADJOINT_DIRECT || n <= (1 << 20),
+                  "nbody_adjoint_create: the direct-sum engine is O(N^2) per step; n <= 2^20");
+    *out = new nbody_adjoint{new nb::AdjointImpl(*p, n, n_steps, mode, checkpoint_every)};
   })
+}
+
+int nbody_adjoint_create(const nbody_sim_params* p, int n, int n_steps, nbody_adjoint** out) {
+  return nbody_adjoint_create_mode(p, n, n_steps, NBODY_ADJOINT_TAPE, 0, out);
 }
 
 int nbody_adjoint_destroy(nbody_adjoint* a) {

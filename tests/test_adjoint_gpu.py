@@ -123,3 +123,72 @@ def test_adjoint_rejects_collisions(nb, cuda):
     with pytest.raises(nb.NBodyError) as e:
         nb.Adjoint(prm, 100, 5)
     assert e.value.code == nb.NBODY_ERR_ARG
+
+
+def test_checkpointed_engine_gives_the_tape_engine_gradient(nb, cuda):
+    """NBODY_ADJOINT_CHECKPOINT keeps FP64 states every 25 levels only and
+    rebuilds the others in the backward by running each step backwards in
+    time (drag inverted in closed form), re-recording each level's tree and
+    tape.  Its forward is the tape engine's, bit for bit; its gradient
+    equals the tape engine's to the rounding of the reversed steps (their
+    drift is reset at every checkpoint); it holds a fraction of the memory."""
+    n, steps = 3000, 60
+    eng_t, x0, v0, mass, pm, pr = setup(nb, cuda, n=n, steps=steps)
+    eng_c = nb.Adjoint(eng_t.params, n, steps, mode="checkpoint", checkpoint_every=25)
+    xt, vt = eng_t.forward(x0, v0, mass, pm, pr)
+    xc, vc = eng_c.forward(x0, v0, mass, pm, pr)
+    assert cuda.equal(xt, xc) and cuda.equal(vt, vc)
+    _, gxt, gvt, gmt, grt = gradients(nb, cuda, eng_t, x0, v0, mass, pm, pr)
+    _, gxc, gvc, gmc, grc = gradients(nb, cuda, eng_c, x0, v0, mass, pm, pr)
+    scale_v = float(gvt.abs().max())
+    scale_x = float(gxt.abs().max())
+    dv = float((gvc - gvt).abs().max()) / scale_v
+    dx = float((gxc - gxt).abs().max()) / scale_x
+    print(f"checkpoint vs tape: velocity {dv:.3e} position {dx:.3e} of the largest; "
+          f"mass {rel(gmc, gmt):.3e} radius {rel(grc, grt):.3e}")
+    assert dv <= 1e-9 and dx <= 1e-9
+    assert rel(gmc, gmt) <= 1e-9 and rel(grc, grt) <= 1e-9
+    st_t, st_c = eng_t.stats(), eng_c.stats()
+    assert st_c.tape_bytes + st_c.state_bytes < (st_t.tape_bytes + st_t.state_bytes) / 4
+    eng_t.close()
+    eng_c.close()
+
+
+def test_direct_sum_gradient_matches_its_central_differences(nb, cuda):
+    """NBODY_ADJOINT_DIRECT: the same loss with FP64 direct-sum self-gravity.
+    Its dynamics are smooth (no tree), so its replay from perturbed inputs
+    is the finite-difference reference for its own gradient."""
+    n, steps = 1000, 30
+    eng_t, x0, v0, mass, pm, pr = setup(nb, cuda, n=n, steps=steps)
+    eng = nb.Adjoint(eng_t.params, n, steps, mode="direct")
+    eng_t.close()
+    _, gx0, gv0, gm, gr = gradients(nb, cuda, eng, x0, v0, mass, pm, pr)
+    r0 = cuda.sqrt((x0 * x0).sum(0)).cpu().numpy()
+    speed = cuda.sqrt((v0 * v0).sum(0)).cpu().numpy()
+    bodies = np.random.default_rng(1).choice(np.nonzero(r0 < 1.5)[0], 9, replace=False)
+    for k, b in enumerate(bodies):
+        c = k % 3
+        g = fd(nb, cuda, eng, mass, x0, v0, pm, pr, "v", c, int(b), 1e-6 * speed[b])
+        assert rel(float(gv0[c, b]), g) <= 1e-4, (c, b, float(gv0[c, b]), g)
+    fd_m = fd(nb, cuda, eng, mass, x0, v0, pm, pr, "m", dpm=1e-5 * pm)
+    assert rel(gm, fd_m) <= 1e-4, (gm, fd_m)
+    eng.close()
+
+
+def test_tree_gradient_against_the_direct_sum_gradient(nb, cuda):
+    """The frozen-tree adjoint (theta 0.5) against the FP64 direct-sum
+    reference gradient of the same loss: they differ by the walk's force
+    approximation, which is small against the star-dominated dynamics."""
+    n, steps = 3000, 40
+    eng_t, x0, v0, mass, pm, pr = setup(nb, cuda, n=n, steps=steps)
+    eng_d = nb.Adjoint(eng_t.params, n, steps, mode="direct")
+    _, gxt, gvt, gmt, grt = gradients(nb, cuda, eng_t, x0, v0, mass, pm, pr)
+    _, gxd, gvd, gmd, grd = gradients(nb, cuda, eng_d, x0, v0, mass, pm, pr)
+    dv = float((gvt - gvd).norm() / gvd.norm())
+    dx = float((gxt - gxd).norm() / gxd.norm())
+    print(f"tree vs direct-sum gradient: velocity {dv:.3e} position {dx:.3e} (relative "
+          f"L2); mass {rel(gmt, gmd):.3e} radius {rel(grt, grd):.3e}")
+    assert dv <= 1e-3 and dx <= 1e-3
+    assert rel(gmt, gmd) <= 1e-2 and rel(grt, grd) <= 1e-2
+    eng_t.close()
+    eng_d.close()
