@@ -323,6 +323,17 @@ typedef struct nbody_sim_params {
                                 group's own sources (no second tree walk).
                                 Same pairs; a body's impulses are summed in
                                 another order.                            */
+  int span_walk;             /* shared walk: 1 on when the target groups
+                                come from span nodes of more than one group
+                                (group_span > 1, unfused collisions, one
+                                target per lane); 0 (default) or 2 off.  The
+                                groups of one span node
+                                share a first traversal with the node's box,
+                                which decides what every group would decide
+                                alike; each group then starts from the
+                                shared sources and the frontier left.  Same
+                                interactions as a walk from the root, summed
+                                in another order.                          */
   int spill_cap;             /* walk / neighbour-search stack entries per
                                 warp kept in HBM when the shared-memory
                                 stack is full; <= 0: default (4096).  A
@@ -376,6 +387,10 @@ typedef struct nbody_sim_stats {
   int leaf_max;                           /* nbody_sim_autotune, the kept    */
   int walk_mode;                          /* candidate)                      */
   int group_span;
+  int span_walk;                          /* 1: the last walk was shared     */
+  unsigned long long span_shared;         /* shared-walk entries of the last */
+  unsigned long long span_frontier;       /* walk (span-decided sources and  */
+  unsigned long long spans;               /* frontier nodes) and its spans   */
 } nbody_sim_stats;
 int nbody_sim_stats_get(nbody_sim* s, nbody_sim_stats* out);
 /* 1 (default): each step is replayed as one CUDA graph (captured on first

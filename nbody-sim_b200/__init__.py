@@ -122,7 +122,8 @@ class nbody_sim_params(C.Structure):
                 ("perturber_mass_mjup", C.c_float), ("perturber_radius_au", C.c_float),
                 ("perturber_phase0", C.c_float), ("state_precision", C.c_int),
                 ("leaf_max", C.c_int), ("targets_per_lane", C.c_int), ("walk_mode", C.c_int),
-                ("group_span", C.c_int), ("fuse_collisions", C.c_int), ("spill_cap", C.c_int)]
+                ("group_span", C.c_int), ("fuse_collisions", C.c_int), ("span_walk", C.c_int),
+                ("spill_cap", C.c_int)]
 
 
 NBODY_PHASES = 6
@@ -140,7 +141,9 @@ class nbody_sim_stats(C.Structure):
                 ("walk_nodes_visited", C.c_ulonglong), ("walk_stack_spills", C.c_ulonglong),
                 ("walk_groups", C.c_ulonglong), ("launches", C.c_ulonglong),
                 ("graph_launches", C.c_ulonglong), ("targets_per_lane", C.c_int),
-                ("leaf_max", C.c_int), ("walk_mode", C.c_int), ("group_span", C.c_int)]
+                ("leaf_max", C.c_int), ("walk_mode", C.c_int), ("group_span", C.c_int),
+                ("span_walk", C.c_int), ("span_shared", C.c_ulonglong),
+                ("span_frontier", C.c_ulonglong), ("spans", C.c_ulonglong)]
 
 
 class nbody_frame(C.Structure):

@@ -66,6 +66,9 @@ struct TreeWork {
   int2* groups = nullptr;
   uint32_t* group_flag = nullptr;
   int* n_groups = nullptr;
+  // optional (set by the caller): per group, (index of the first group cut
+  // from the same span node, bodies in that node) -- the shared walk's spans
+  int2* group_spans = nullptr;
   int group_max = 32;     // bodies per target group (32 x targets per lane)
   // Octree nodes with <= prune_max bodies get no child records (0: every
   // node down to single bodies).  The walk and the neighbour search open a
@@ -234,9 +237,38 @@ struct WalkArgs {
   float* coll_dv[3];
   const float4* box_lo;   // node boxes (the octree's), for the reach test
   const float4* box_hi;
+  // shared walk (span_lists != nullptr; single disk, targets_per_lane 1, no
+  // tape, no fused collisions): each group starts from its span's shared
+  // sources and frontier (launch_span_walk) instead of the root
+  const int2* group_span;
+  const int4* span_lists;  // at a span's first group: (shared head, shared
+                           // count, frontier head, frontier count); count -1:
+                           // no lists, walk from the root
+  const int* span_pool;    // chunks of 32 entries
+  const int* span_next;    // next chunk (-1 ends)
 };
 int walk_spill_slots(int device);  // warps resident at once (spill area slots)
 void launch_walk(const WalkArgs& a, cudaStream_t s);
+
+// The first, shared traversal of the shared walk: one warp per span node.
+struct SpanArgs {
+  const float4* com;
+  const int4* info;
+  const float4* body;
+  const int2* groups;
+  const int2* group_span;
+  const int* n_groups;
+  float theta2;
+  int leaf_max;
+  int4* span_lists;
+  int* pool;
+  int* next;
+  int* used;               // chunks taken (reset to 0 before the launch)
+  int cap;                 // chunks in the pool
+  int* work;               // span counter (reset to 0 before the launch)
+  unsigned long long* counters;  // optional: shared entries, frontier entries, spans
+};
+void launch_span_walk(const SpanArgs& a, int n, cudaStream_t s);
 
 // ------------------------------------------------------------ collisions
 struct NeighborArgs {

@@ -448,6 +448,31 @@ struct SimBase {
   int* work = nullptr;
   unsigned long long* inter = nullptr;
   unsigned long long* counters = nullptr;  // walk: nodes visited, spills, groups
+  // shared walk: per group its span, per span its lists, the lists' chunk pool
+  int2* group_spans = nullptr;
+  int4* span_lists = nullptr;
+  int* span_pool = nullptr;
+  int* span_next = nullptr;
+  int* span_used = nullptr;
+  int* span_work = nullptr;
+  int span_cap = 0;  // chunks of 32 entries
+  unsigned long long* span_counters = nullptr;  // shared entries, frontier entries, spans
+  bool span_on() const {
+    return p.span_walk == 1 && p.group_span > 1 && p.targets_per_lane == 1 &&
+           !(p.r_coll > 0.f && p.fuse_collisions);
+  }
+  void span_alloc() {
+    if (group_spans) return;
+    group_spans = dalloc<int2>(n, "group spans");
+    span_lists = dalloc<int4>(n, "span lists");
+    span_cap = std::max(1024, n / 8);
+    span_pool = dalloc<int>((size_t)span_cap * 32, "span pool");
+    span_next = dalloc<int>(span_cap, "span chunk links");
+    span_used = dalloc<int>(1, "span chunks used");
+    span_work = dalloc<int>(1, "span counter");
+    span_counters = dalloc<unsigned long long>(3, "span counters");
+    check(cudaMemset(span_counters, 0, 3 * sizeof(unsigned long long)), "span counters");
+  }
   int* parent = nullptr;
   int* labels = nullptr;
   int* sizes = nullptr;
@@ -559,6 +584,9 @@ struct SimBase {
 
   void common_free() {
     drop_graphs();
+    for (void* q : {(void*)group_spans, (void*)span_lists, (void*)span_pool, (void*)span_next,
+                    (void*)span_used, (void*)span_work, (void*)span_counters})
+      if (q) cudaFree(q);
     if (cap_st) cudaStreamDestroy(cap_st);
     if (rb_st) cudaStreamDestroy(rb_st);
     if (ev_pos) cudaEventDestroy(ev_pos);
@@ -752,6 +780,9 @@ struct SimImpl : SimBase {
     cur = 1 - cur;
     mark(NBODY_PHASE_TREE);
     tw.prune_max = p.leaf_max;
+    const bool span = span_on();
+    if (span) span_alloc();
+    tw.group_spans = span ? group_spans : nullptr;
     if (kIsF64<R>)
       launch_tree<uint32_t>(tw, tw.keys, n, 30, 0, 1, tw.geom, nullptr,
                             (const double*)s[cur].v[0], (const double*)s[cur].v[1],
@@ -783,6 +814,15 @@ struct SimImpl : SimBase {
       launches += 1;
     }
     mark(NBODY_PHASE_WALK);
+    if (span) {  // the shared walk's first traversal (one warp per span node), then the walk
+      SpanArgs sa{tw.oct.com, tw.oct.info, tw.body4, tw.groups, group_spans, tw.n_groups,
+                  p.theta * p.theta, p.leaf_max, span_lists, span_pool, span_next, span_used,
+                  span_cap, span_work, span_counters};
+      launch_span_walk(sa, n, st);
+      w.group_span = group_spans; w.span_lists = span_lists;
+      w.span_pool = span_pool; w.span_next = span_next;
+      launches += 2;
+    }
     launch_walk(w, st);
     if (side_coll) check(cudaStreamWaitEvent(st, cs.join, 0), "collision join");
     mark(NBODY_PHASE_COLLIDE);
@@ -1173,6 +1213,15 @@ int nbody_sim_stats_get(nbody_sim* s, nbody_sim_stats* out) {
     out->leaf_max = b->p.leaf_max;
     out->walk_mode = b->p.walk_mode;
     out->group_span = b->p.group_span;
+    out->span_walk = b->span_on() ? 1 : 0;
+    if (b->span_counters) {
+      unsigned long long sc[3];
+      nb::check(cudaMemcpy(sc, b->span_counters, sizeof(sc), cudaMemcpyDeviceToHost),
+                "span counters");
+      out->span_shared = sc[0];
+      out->span_frontier = sc[1];
+      out->spans = sc[2];
+    }
   })
 }
 

@@ -579,6 +579,7 @@ struct ApplyArgs {
   int* group_disk;  // optional: disk of each group
   int* n_nodes;
   int* n_groups;
+  int2* group_span;  // optional: (first group of the span node, its bodies)
 };
 
 template <typename K>
@@ -613,6 +614,7 @@ __global__ void __launch_bounds__(kThreads) k_apply(const ApplyArgs<K> a) {
       const int sz = q + (j < r ? 1 : 0);
       a.groups[goff + j] = make_int2(s, sz);
       if (a.group_disk) a.group_disk[goff + j] = disk;
+      if (a.group_span) a.group_span[goff + j] = make_int2((int)goff, c);
       s += sz;
     }
   }
@@ -915,7 +917,7 @@ void launch_octree(TreeWork& w, const K* keys, int n, int disk_bits, int n_roots
   k_mark<K><<<mtiles, kMarkTile, 0, s>>>(m);
   k_tiles<<<1, 1024, 0, s>>>(tsum, mtiles);
   ApplyArgs<K> ap{n, n_roots, w.bin_lo, w.bin_hi, keys, w.oct_off, tsum, w.groups, group_disk,
-                  w.n_nodes, w.n_groups};
+                  w.n_nodes, w.n_groups, w.group_spans};
   k_apply<K><<<mtiles, kMarkTile, 0, s>>>(ap);
   EmitArgs<K> a{n, disk_bits, n_roots, w.bin_lo, w.bin_hi, w.bin_prefix, keys, w.oct_nch,
                 w.oct_off, opar, w.oct_cidx, w.body4, w.mom_ploc, tpre, geoms, w.oct};

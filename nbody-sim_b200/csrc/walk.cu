@@ -252,6 +252,180 @@ __device__ __forceinline__ void tape_append(const WalkArgs& a, TapeCursor& t, bo
   t.cur = (used + k > 32) ? c2 : c1;
 }
 
+// Squared distance from a box to a point (0 inside) and to the box's
+// farthest corner, in one fixed rounding shared by the walk and the span
+// walk: both are monotone in the box bounds, so a box inside another is
+// never nearer in FP32 either.
+__device__ __forceinline__ float box_d2(float4 c, float x0, float x1, float y0, float y1,
+                                        float z0, float z1) {
+  const float dx = fmaxf(fmaxf(x0 - c.x, c.x - x1), 0.f);
+  const float dy = fmaxf(fmaxf(y0 - c.y, c.y - y1), 0.f);
+  const float dz = fmaxf(fmaxf(z0 - c.z, c.z - z1), 0.f);
+  return dist2(dx, dy, dz);
+}
+
+__device__ __forceinline__ float box_far2(float4 c, float x0, float x1, float y0, float y1,
+                                          float z0, float z1) {
+  const float fx = fmaxf(fabsf(c.x - x0), fabsf(c.x - x1));
+  const float fy = fmaxf(fabsf(c.y - y0), fabsf(c.y - y1));
+  const float fz = fmaxf(fabsf(c.z - z0), fabsf(c.z - z1));
+  return dist2(fx, fy, fz);
+}
+
+// Span-walk list entries: a node index, with kSpanLeafFlag for "the bodies
+// of this leaf" (shared list only).
+constexpr int kSpanLeafFlag = 1 << 30;
+constexpr int kSpanNodeMask = kSpanLeafFlag - 1;
+
+// A chain of 32-entry chunks of ints taken from a pool (the span walk's
+// lists): entries fill each chunk before the next is taken.
+struct Chain {
+  int head = -1, cur = -1, count = 0;
+  bool ok = true;
+};
+
+// Appends k <= 32 entries; lane l with `on` writes entry e at offset o.  A
+// pool that runs dry marks the chain as failed.
+__device__ __forceinline__ void chain_append(const SpanArgs& a, Chain& t, bool on, int o, int k,
+                                             int e, int lane) {
+  if (k <= 0 || !t.ok) return;
+  const int used = t.count & 31;
+  int c1 = t.cur, c2 = -1;
+  if (lane == 0) {
+    if (used == 0) {
+      c1 = atomicAdd(a.used, 1);
+      if (c1 >= a.cap) c1 = -1;
+      if (c1 >= 0) {
+        if (t.cur >= 0) a.next[t.cur] = c1;
+        else t.head = c1;
+      }
+    }
+    if (c1 >= 0 && used + k > 32) {
+      c2 = atomicAdd(a.used, 1);
+      if (c2 >= a.cap) c2 = -1;
+      if (c2 >= 0) a.next[c1] = c2;
+    }
+  }
+  c1 = __shfl_sync(kFull, c1, 0);
+  c2 = __shfl_sync(kFull, c2, 0);
+  t.head = __shfl_sync(kFull, t.head, 0);
+  if (c1 < 0 || (used + k > 32 && c2 < 0)) {
+    t.ok = false;
+    return;
+  }
+  if (on) {
+    const int q = used + o;
+    a.pool[(size_t)((q < 32) ? c1 : c2) * 32 + (q & 31)] = e;
+  }
+  t.count += k;
+  t.cur = (used + k > 32) ? c2 : c1;
+}
+
+// The span walk (the shared walk's first traversal): one warp per span node,
+// the maximal tree node of <= span x 32 bodies that target groups were cut
+// from.  It traverses the tree with the span's bounding box B_S -- the union
+// of its groups' boxes -- and files each node it meets by what every group
+// of the span would do with it:
+//  - a single body, or a node that B_S accepts (half^2 < theta^2 d^2, d from
+//    B_S to the centre of mass): every group box lies inside B_S, so is at
+//    least as far, and accepts it too -> a shared source;
+//  - a node that fails even against B_S's farthest corner (half^2 >= theta^2
+//    far^2): every group box, and every target in it, is nearer, so no box
+//    test and no acceptance vote can accept it and every group opens it ->
+//    its children are traversed here, a leaf's bodies become shared sources;
+//  - anything else -> the span's frontier, decided group by group.
+// box_d2 and box_far2 are monotone in the box bounds in FP32 too, so the
+// shared decisions are exactly the groups' own.  A group's walk evaluates the
+// shared sources and starts from the frontier instead of the root: each
+// target gets the interactions of a walk from the root, in another order.
+// Children that would overflow the stack go to the frontier (deferring a node
+// is always exact); a pool that runs dry leaves the span without lists, and
+// its groups walk from the root.
+__global__ void __launch_bounds__(kWalkWarps * 32) k_span_walk(const SpanArgs a) {
+  __shared__ int s_stk[kWalkWarps][kStk];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  int* stk = s_stk[wib];
+  const int n_groups = *a.n_groups;
+  while (true) {
+    int g = 0;
+    if (lane == 0) g = atomicAdd(a.work, 1);
+    g = __shfl_sync(kFull, g, 0);
+    if (g >= n_groups) break;
+    const int2 sp = __ldg(a.group_span + g);
+    if (sp.x != g) continue;  // not the first group of its span
+    const int lo = __ldg(a.groups + g).x;
+    float x0 = INFINITY, x1 = -INFINITY, y0 = INFINITY, y1 = -INFINITY, z0 = INFINITY,
+          z1 = -INFINITY;
+    for (int i = lane; i < sp.y; i += 32) {
+      const float4 b = __ldg(a.body + lo + i);
+      x0 = fminf(x0, b.x); x1 = fmaxf(x1, b.x);
+      y0 = fminf(y0, b.y); y1 = fmaxf(y1, b.y);
+      z0 = fminf(z0, b.z); z1 = fmaxf(z1, b.z);
+    }
+    x0 = warp_min(x0); x1 = warp_max(x1);
+    y0 = warp_min(y0); y1 = warp_max(y1);
+    z0 = warp_min(z0); z1 = warp_max(z1);
+    Chain sh, fr;
+    int top = 1;
+    if (lane == 0) stk[0] = 0;  // the root
+    __syncwarp();
+    while (top > 0) {
+      const int take = min(top, 32);
+      top -= take;
+      const int node = (lane < take) ? stk[top + lane] : -1;
+      __syncwarp();
+      int cls = 0, first = 0, nch = 0;  // 1 shared node, 2 shared leaf, 3 open, 4 frontier
+      if (node >= 0) {
+        const float4 c = __ldg(a.com + node);
+        const int4 inf = __ldg(a.info + node);
+        const int cnt = inf.z >> 4;
+        nch = inf.z & 15;
+        first = inf.x;
+        const float half = __int_as_float(inf.w);
+        const float h2 = half * half;
+        if (cnt == 1 || h2 < a.theta2 * box_d2(c, x0, x1, y0, y1, z0, z1)) cls = 1;
+        else if (!(h2 < a.theta2 * box_far2(c, x0, x1, y0, y1, z0, z1)))
+          cls = (nch == 0 || cnt <= a.leaf_max) ? 2 : 3;
+        else cls = 4;
+      }
+      unsigned m = __ballot_sync(kFull, cls == 1 || cls == 2);
+      chain_append(a, sh, cls == 1 || cls == 2, __popc(m & lanemask_lt()), __popc(m),
+                   node | (cls == 2 ? kSpanLeafFlag : 0), lane);
+      m = __ballot_sync(kFull, cls == 4);
+      chain_append(a, fr, cls == 4, __popc(m & lanemask_lt()), __popc(m), node, lane);
+      const int pc = (cls == 3) ? nch : 0;
+      const int pincl = warp_incl_scan(pc, lane);
+      const int ptotal = __shfl_sync(kFull, pincl, 31);
+      if (ptotal > 0) {
+        if (top + ptotal <= kStk) {
+          const int base = top + pincl - pc;
+          for (int k = 0; k < pc; ++k) stk[base + k] = first + k;
+          top += ptotal;
+        } else {  // no room: the children are decided group by group
+          for (int k = 0; k < 8; ++k) {
+            const bool on = k < pc;
+            const unsigned mk = __ballot_sync(kFull, on);
+            chain_append(a, fr, on, __popc(mk & lanemask_lt()), __popc(mk), first + k, lane);
+          }
+        }
+      }
+      __syncwarp();
+    }
+    if (lane == 0) {
+      const bool ok = sh.ok && fr.ok;
+      if (ok && sh.cur >= 0) a.next[sh.cur] = -1;
+      if (ok && fr.cur >= 0) a.next[fr.cur] = -1;
+      a.span_lists[g] = ok ? make_int4(sh.head, sh.count, fr.head, fr.count)
+                           : make_int4(-1, -1, -1, -1);
+      if (a.counters) {
+        atomicAdd(a.counters + 0, (unsigned long long)(ok ? sh.count : 0));
+        atomicAdd(a.counters + 1, (unsigned long long)(ok ? fr.count : 0));
+        atomicAdd(a.counters + 2, ok ? 1ull : 0ull);
+      }
+    }
+  }
+}
+
 // kT targets per lane: a group of up to 32 kT bodies per warp.  kRec: also
 // record the group's source list on the tape.  kColl (kT == 1): fused
 // collisions.  A multi-body node whose box comes within r_coll of the group
@@ -261,7 +435,7 @@ __device__ __forceinline__ void tape_append(const WalkArgs& a, TapeCursor& t, bo
 // collision pairs.  The pairs are those of the stand-alone search: the same
 // squared distance and impulse arithmetic (collide_math.cuh); only the order
 // in which a target's impulses are summed differs.
-template <bool kSoft, int kT, bool kRec, int kMode, bool kColl = false>
+template <bool kSoft, int kT, bool kRec, int kMode, bool kColl = false, bool kSpan = false>
 __global__ void __launch_bounds__(kWalkWarps * 32, walk_min_blocks<kMode>())
     k_walk(const WalkArgs a) {
   __shared__ WarpSmem smem[kWalkWarps];
@@ -345,23 +519,53 @@ __global__ void __launch_bounds__(kWalkWarps * 32, walk_min_blocks<kMode>())
     int top = 1, spilled = 0, nlist = 0;
     bool overflow = false;
     TapeCursor tc;
-    if (lane == 0) w.stk[0] = disk;  // root slot of the group's disk
+    // shared walk: the span's shared sources first (decided by the span
+    // walk), then its frontier in place of the root
+    int sh_chunk = -1, sh_left = 0, fr_chunk = -1, fr_left = 0;
+    if (kSpan) {
+      const int4 sl = __ldg(a.span_lists + __ldg(a.group_span + g).x);
+      if (sl.y >= 0) {
+        sh_chunk = sl.x; sh_left = sl.y;
+        fr_chunk = sl.z; fr_left = sl.w;
+        top = 0;
+      }
+    }
+    if (top == 1 && lane == 0) w.stk[0] = disk;  // root slot of the group's disk
     __syncwarp();
 
     while (true) {
-      if (top == 0) {
-        if (spilled == 0) break;
-        const int cnt = min(spilled, kStk / 2);
-        for (int k = lane; k < cnt; k += 32) w.stk[k] = __ldcg(spill + (spilled - cnt) + k);
-        spilled -= cnt;
-        top = cnt;
+      int node = -1, forced = 0;  // forced: 1 source, 2 bodies of a leaf (shared list)
+      if (kSpan && sh_left > 0) {
+        const int k = min(sh_left, 32);
+        const int e = (lane < k) ? __ldg(a.span_pool + (size_t)sh_chunk * 32 + lane) : -1;
+        sh_left -= k;
+        if (sh_left > 0) sh_chunk = __ldg(a.span_next + sh_chunk);
+        node = (e >= 0) ? (e & kSpanNodeMask) : -1;
+        forced = (e >= 0) ? ((e & kSpanLeafFlag) ? 2 : 1) : 0;
+        visited += k;
+      } else {
+        if (top == 0) {
+          if (spilled == 0) {
+            if (!kSpan || fr_left == 0) break;
+            const int k = min(fr_left, 32);
+            if (lane < k) w.stk[lane] = __ldg(a.span_pool + (size_t)fr_chunk * 32 + lane);
+            fr_left -= k;
+            if (fr_left > 0) fr_chunk = __ldg(a.span_next + fr_chunk);
+            top = k;
+          } else {
+            const int cnt = min(spilled, kStk / 2);
+            for (int k = lane; k < cnt; k += 32) w.stk[k] = __ldcg(spill + (spilled - cnt) + k);
+            spilled -= cnt;
+            top = cnt;
+          }
+          __syncwarp();
+        }
+        const int take = min(top, 32);
+        top -= take;
+        visited += take;
+        node = (lane < take) ? w.stk[top + lane] : -1;
         __syncwarp();
       }
-      const int take = min(top, 32);
-      top -= take;
-      visited += take;
-      const int node = (lane < take) ? w.stk[top + lane] : -1;
-      __syncwarp();
 
       int act = 0;  // 1: source, 2: bodies of a leaf, 3: open children
       float4 c = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -376,21 +580,16 @@ __global__ void __launch_bounds__(kWalkWarps * 32, walk_min_blocks<kMode>())
         const int nch = inf.z & 15;
         const float half = __int_as_float(inf.w);
         h2 = half * half;
-        if (cnt == 1) {
+        if (forced == 1 || cnt == 1) {
           act = 1;
+        } else if (forced == 2) {
+          act = 2;
+          first = inf.y;
         } else {
-          const float dx = fmaxf(fmaxf(gx0 - c.x, c.x - gx1), 0.f);
-          const float dy = fmaxf(fmaxf(gy0 - c.y, c.y - gy1), 0.f);
-          const float dz = fmaxf(fmaxf(gz0 - c.z, c.z - gz1), 0.f);
-          d2 = dx * dx + dy * dy + dz * dz;
-          if (walk_vote<kMode>()) {
-            // farthest point of the box: no target is farther than this
-            const float fx = fmaxf(fabsf(c.x - gx0), fabsf(c.x - gx1));
-            const float fy = fmaxf(fabsf(c.y - gy0), fabsf(c.y - gy1));
-            const float fz = fmaxf(fabsf(c.z - gz0), fabsf(c.z - gz1));
-            far2 = fx * fx + fy * fy + fz * fz;
-          }
-          if (half * half < a.theta2 * d2) {
+          d2 = box_d2(c, gx0, gx1, gy0, gy1, gz0, gz1);
+          // farthest point of the box: no target is farther than this
+          if (walk_vote<kMode>()) far2 = box_far2(c, gx0, gx1, gy0, gy1, gz0, gz1);
+          if (h2 < a.theta2 * d2) {
             act = 1;
           } else if (nch == 0 || cnt <= a.leaf_max) {
             act = 2;
@@ -601,12 +800,13 @@ __global__ void __launch_bounds__(kWalkWarps * 32, walk_min_blocks<kMode>())
   }
 }
 
-template <bool kSoft, int kT, bool kRec = false, int kMode = 0, bool kColl = false>
+template <bool kSoft, int kT, bool kRec = false, int kMode = 0, bool kColl = false,
+          bool kSpan = false>
 int walk_blocks_per_sm() {
   static int b = 0;
   if (b == 0) {
-    check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<kSoft, kT, kRec, kMode, kColl>,
-                                                        kWalkWarps * 32, 0),
+    check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+              &b, k_walk<kSoft, kT, kRec, kMode, kColl, kSpan>, kWalkWarps * 32, 0),
           "walk occupancy");
     if (b < 1) b = 1;
   }
@@ -623,19 +823,27 @@ int num_sms() {
   return sms;
 }
 
-template <bool kSoft, int kT, bool kRec = false, int kMode = 0, bool kColl = false>
+template <bool kSoft, int kT, bool kRec = false, int kMode = 0, bool kColl = false,
+          bool kSpan = false>
 void launch_variant(const WalkArgs& a, cudaStream_t s) {
-  int grid = num_sms() * walk_blocks_per_sm<kSoft, kT, kRec, kMode, kColl>();
+  int grid = num_sms() * walk_blocks_per_sm<kSoft, kT, kRec, kMode, kColl, kSpan>();
   grid = std::min(grid, (a.n + kWalkWarps - 1) / kWalkWarps);  // groups <= n
   if (grid < 1) grid = 1;
-  k_walk<kSoft, kT, kRec, kMode, kColl><<<grid, kWalkWarps * 32, 0, s>>>(a);
+  k_walk<kSoft, kT, kRec, kMode, kColl, kSpan><<<grid, kWalkWarps * 32, 0, s>>>(a);
 }
 
-template <bool kSoft, bool kColl>
+template <bool kSoft, bool kColl, bool kSpan = false>
 void launch_mode(const WalkArgs& a, cudaStream_t s) {
-  if (a.walk_mode == 1) launch_variant<kSoft, 1, false, 1, kColl>(a, s);
-  else if (a.walk_mode == 2) launch_variant<kSoft, 1, false, 2, kColl>(a, s);
-  else launch_variant<kSoft, 1, false, 0, kColl>(a, s);
+  if (a.walk_mode == 1) launch_variant<kSoft, 1, false, 1, kColl, kSpan>(a, s);
+  else if (a.walk_mode == 2) launch_variant<kSoft, 1, false, 2, kColl, kSpan>(a, s);
+  else launch_variant<kSoft, 1, false, 0, kColl, kSpan>(a, s);
+}
+
+template <bool kSoft>
+int span_blocks_per_sm() {
+  return std::max(std::max(walk_blocks_per_sm<kSoft, 1, false, 0, false, true>(),
+                           walk_blocks_per_sm<kSoft, 1, false, 1, false, true>()),
+                  walk_blocks_per_sm<kSoft, 1, false, 2, false, true>());
 }
 
 template <bool kSoft>
@@ -656,8 +864,33 @@ int walk_spill_slots(int) {
                                  walk_blocks_per_sm<false, 1, false, 1>()),
                         std::max(walk_blocks_per_sm<true, 1, false, 2>(),
                                  walk_blocks_per_sm<false, 1, false, 2>()))));
-  const int bc = std::max(coll_blocks_per_sm<true>(), coll_blocks_per_sm<false>());
+  const int bc = std::max(std::max(coll_blocks_per_sm<true>(), coll_blocks_per_sm<false>()),
+                          std::max(span_blocks_per_sm<true>(), span_blocks_per_sm<false>()));
   return num_sms() * std::max(b, bc) * kWalkWarps;
+}
+
+// The span walk: its span counter and chunk count zeroed, then one warp per
+// span (grid-strided over the groups).
+__global__ void k_span_reset(int* work, int* used, unsigned long long* counters) {
+  if (threadIdx.x == 0) *work = 0;
+  if (threadIdx.x == 1) *used = 0;
+  if (counters && threadIdx.x >= 2 && threadIdx.x < 5) counters[threadIdx.x - 2] = 0ull;
+}
+
+void launch_span_walk(const SpanArgs& a, int n, cudaStream_t s) {
+  if (n <= 0) return;
+  k_span_reset<<<1, 32, 0, s>>>(a.work, a.used, a.counters);
+  static int blocks = 0;
+  if (blocks == 0) {
+    check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_span_walk, kWalkWarps * 32,
+                                                        0),
+          "span walk occupancy");
+    blocks = std::max(blocks, 1);
+  }
+  int grid = num_sms() * blocks;
+  grid = std::min(grid, (n + kWalkWarps - 1) / kWalkWarps);
+  k_span_walk<<<std::max(grid, 1), kWalkWarps * 32, 0, s>>>(a);
+  check(cudaGetLastError(), "k_span_walk launch");
 }
 
 // The walk's group counter and statistics, zeroed by one launch (three
@@ -685,6 +918,9 @@ void launch_walk(const WalkArgs& a, cudaStream_t s) {
   } else if (a.coll_dv[0]) {  // fused collisions
     if (soft) launch_mode<true, true>(a, s);
     else launch_mode<false, true>(a, s);
+  } else if (a.span_lists) {  // shared walk
+    if (soft) launch_mode<true, false, true>(a, s);
+    else launch_mode<false, false, true>(a, s);
   } else {
     if (soft) launch_mode<true, false>(a, s);
     else launch_mode<false, false>(a, s);

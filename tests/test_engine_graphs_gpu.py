@@ -196,3 +196,34 @@ def test_sim_autotune_keeps_the_state_and_the_fastest_setting(nb, cuda):
     sim.sync()
     assert sim.stats().status == 0 and sim.stats().steps_done == 5
     sim.close()
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+def test_shared_walk_gives_the_same_interactions(nb, cuda, mode):
+    """The shared walk (span_walk): the groups of one span node start from
+    the shared sources and frontier of one traversal with the span's box.
+    Every target must get exactly the interactions of a walk from the root
+    (the interaction count is equal), summed in another order (forces agree
+    to FP32 rounding)."""
+    n = 200_000
+    st = disk(nb, n, 0.3, 30.0, seed=8, m=1e-9)
+    out = {}
+    for sw in (2, 1):
+        prm = nb.sim_params(dt=0.002, theta=0.5, softening=5e-4, star_mass=0.0, r_coll=0.0,
+                            walk_mode=mode, group_span=8, span_walk=sw)
+        sim = nb.Sim(prm, n)
+        sim.set_state(st["x"], st["y"], st["z"], st["vx"], st["vy"], st["vz"], st["m"])
+        g = sim.get_state(accel=True)
+        s = sim.stats()
+        out[sw] = (np.stack([g["ax"], g["ay"], g["az"]], 1).astype(np.float64), s)
+        sim.close()
+    (a0, s0), (a1, s1) = out[2], out[1]
+    assert s0.span_walk == 0 and s1.span_walk == 1 and s1.spans > 0
+    assert s1.status == 0 and s0.status == 0
+    assert s1.interactions == s0.interactions
+    scale = np.sqrt(np.mean((a0 * a0).sum(1)))
+    d = np.linalg.norm(a1 - a0, axis=1) / scale
+    print(f"mode {mode}: spans {s1.spans} shared {s1.span_shared} frontier {s1.span_frontier} "
+          f"visited {s0.walk_nodes_visited} -> {s1.walk_nodes_visited}; "
+          f"diff max {d.max():.2e} median {np.median(d):.2e}")
+    assert d.max() < 1e-5
