@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--group-span", type=int, default=None,
                     help="target groups from maximal nodes of <= span x 32 bodies "
                          "(nbody_sim_params.group_span)")
+    ap.add_argument("--span-walk", type=int, default=None, choices=[0, 1, 2],
+                    help="shared walk (nbody_sim_params.span_walk); default: the engine's")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-studies", action="store_true",
@@ -353,6 +355,8 @@ def run_ours(args, ws, rank, local):
         prm.walk_mode = args.walk_mode
     if args.group_span is not None:
         prm.group_span = args.group_span
+    if args.span_walk is not None:
+        prm.span_walk = args.span_walk
     stream = torch.cuda.current_stream()
     sim = nb.Sim(prm, n)
     sim.set_stream(stream.cuda_stream)

@@ -44,16 +44,44 @@ def _free_port():
         return s.getsockname()[1]
 
 
+# a small ensemble of the C4 recipe for the CPU: 12 disks of 256..2048 bodies
+SMALL = dict(n_disks=12, n_range=(256, 2048))
+
+
+def disk_result(port, spec, steps=2):
+    """One disk of the ensemble advanced on the CPU restatement of the
+    reference step (collisions, drag and its perturber), as the SHA-256 of its
+    final FP32 state: the per-disk record a rank sends back."""
+    import hashlib
+    d = port.make_disk(spec["n"], wl.DISK_R[0], wl.DISK_R[1], 0.01, 0.005, 1.0, spec["seed"])
+    st = {k: v.astype(np.float32) for k, v in d.items()}
+    st["m"] = np.full(spec["n"], wl.PARTICLE_MASS, np.float32)
+    pert = port.perturber(True, spec["perturber_mass_mjup"], spec["perturber_radius_au"],
+                          spec["perturber_phase0"], 1.0)
+    r_coll = 5.0 * 2.416e-5 * (wl.PARTICLE_MASS / 3.003e-7) ** (1.0 / 3.0)
+    sp = port.step_params(0.005, 0.5, wl.SOFTENING, 1.0, r_coll=r_coll, restitution=0.0,
+                          gas_drag_rate=1e-3, collisions=True, pert=pert)
+    port.run(st, sp, steps, nthreads=1)
+    h = hashlib.sha256()
+    for k in ("x", "y", "z", "vx", "vy", "vz"):
+        h.update(np.ascontiguousarray(st[k]).tobytes())
+    return h.hexdigest()
+
+
 def _rank_main(rank, world, port, q):
+    import sys
     import torch.distributed as dist
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(
+        __file__))), "oracle"))
+    import oracle
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
-        specs = wl.c4_disks()
+        specs = wl.c4_disks(**SMALL)
         mine = wl.partition_disks([d["n"] for d in specs], world)[rank]
-        # per-disk result stand-in: the disk's size and seed
-        rows = [(k, specs[k]["n"], specs[k]["seed"]) for k in mine]
+        orc = oracle.Port()
+        rows = [(k, specs[k]["n"], disk_result(orc, specs[k])) for k in mine]
         got = [None] * world
         dist.all_gather_object(got, rows)
         if rank == 0:
@@ -62,19 +90,27 @@ def _rank_main(rank, world, port, q):
         dist.destroy_process_group()
 
 
-def test_two_rank_partition_gathers_every_disk():
+def test_two_rank_partition_gathers_every_disk_result(port):
+    """Two gloo ranks each advance their share of the disks (partition by
+    N log N) and gather the per-disk results: every disk comes back once,
+    from the rank the partition gave it to, with the result a single process
+    computes for it."""
     import multiprocessing as mp
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    port = _free_port()
-    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    pnum = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, pnum, q)) for r in range(2)]
     for p in procs:
         p.start()
-    got = q.get(timeout=120)
+    got = q.get(timeout=300)
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
+    specs = wl.c4_disks(**SMALL)
+    parts = wl.partition_disks([d["n"] for d in specs], 2)
+    assert [sorted(r[0] for r in got[k]) for k in range(2)] == parts
     rows = sorted(r for part in got for r in part)
-    specs = wl.c4_disks()
-    assert [r[0] for r in rows] == list(range(64))
-    assert all(r[1] == specs[r[0]]["n"] for r in rows)
+    assert [r[0] for r in rows] == list(range(len(specs)))
+    for k, n, digest in rows:
+        assert n == specs[k]["n"]
+        assert digest == disk_result(port, specs[k]), k
