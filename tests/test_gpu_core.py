@@ -251,21 +251,29 @@ def test_reference_engine_pins_the_oracle_port(nb, cuda, port):
 
 
 # ----------------------------------------------------------------- engine
+@pytest.mark.parametrize("physics", ["gravity", "drag+perturber"])
 @pytest.mark.parametrize("precision", [0, 1])
-def test_engine_steps_track_the_reference_loop(nb, cuda, port, precision):
-    """C1-like disk (N=4096, theta 0.5, eps 1e-3, dt 0.01) for 20 steps."""
+def test_engine_steps_track_the_reference_loop(nb, cuda, port, precision, physics):
+    """C1-like disk (N=4096, theta 0.5, eps 1e-3, dt 0.01) for 20 steps; the
+    second case adds gas drag 1e-3 (Integrator.cu:40-76) and a 1 M_J
+    perturber at 5.2 AU (Perturber.cu:13-35) on both sides."""
     n = 4096
     st = disk(nb, n, 0.5, 5.0, seed=0, m=1e-8)
     r_coll = nb.particle_physical_radius(1e-8)
+    extra = physics != "gravity"
     prm = nb.sim_params(dt=0.01, theta=0.5, softening=1e-3, star_mass=1.0, r_coll=r_coll,
-                        restitution=0.0, state_precision=precision, leaf_max=8)
+                        restitution=0.0, state_precision=precision, leaf_max=8,
+                        gas_drag_rate=1e-3 if extra else 0.0, perturber_enabled=int(extra),
+                        perturber_mass_mjup=1.0, perturber_radius_au=5.2, perturber_phase0=0.0)
     sim = nb.Sim(prm, n)
     sim.set_state(st["x"], st["y"], st["z"], st["vx"], st["vy"], st["vz"], st["m"])
     sim.step(20)
     sim.sync()
     got = sim.get_state()
     ref = {k: st[k].copy() for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
-    sp = port.step_params(0.01, 0.5, 1e-3, 1.0, r_coll=r_coll, restitution=0.0)
+    pert = port.perturber(True, 1.0, 5.2, 0.0, 1.0) if extra else None
+    sp = port.step_params(0.01, 0.5, 1e-3, 1.0, r_coll=r_coll, restitution=0.0,
+                          gas_drag_rate=1e-3 if extra else 0.0, pert=pert)
     port.run(ref, sp, 20)
     # both engines approximate the same forces to ~1e-4 (total force, star
     # dominated); over 20 steps of dt 0.01 that bounds the drift apart
