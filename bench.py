@@ -460,34 +460,54 @@ def run_ours(args, ws, rank, local):
     }
     line["phase_hbm"] = phase_hbm(line["phase_ms_per_step"], n)
     if rank == 0 and ws == 1 and not args.no_studies and prec == nb.STATE_F32:
-        dg = importlib.import_module("nbody-sim_b200.diagnostics")
-        targets = np.sort(np.random.default_rng(0).choice(n, min(args.targets, n),
-                                                          replace=False))
-        fe = dg.engine_force_errors(prm, st, targets)
-        line["force_err"] = {"targets": len(targets), "total": fe["total"], "self": fe["self"],
-                             "vs": "FP64 direct sum (nbody_direct_f64) on the same FP32 "
-                                   "positions; the engine's own walk (the timed one)"}
-        ref = ref_engine_study(st, n, args.theta)
-        if "value" in ref:
-            ref["ours_over_reference"] = value / ref["value"]
-        line["ref_engine"] = ref
         sim.close()
-        ens = ensemble_study(args, ws, rank, local, args.steps)
-        line["ensemble"] = {"value": ens["value"], "ms_per_step": ens["ms_per_step"],
-                            "n_total": ens["config"]["n_total"], "disks": args.disks,
-                            "one_by_one_value": ens["one_by_one"]["value"],
-                            "one_by_one_ms_per_step": ens["one_by_one"]["ms_per_step"],
-                            "ensemble_over_one_by_one": ens["one_by_one"]["speedup"],
-                            "workload": ens["config"]["workload"]}
-        adj = adjoint_study(args, args.adjoint_fd)
-        fdc = {k: v for k, v in adj["fd_check"].items() if k != "misses_at_h1e-6"}
-        fdc["misses_at_h1e-6"] = len(adj["fd_check"]["misses_at_h1e-6"])
-        line["adjoint"] = {"gradient_over_plain_forward": adj["ms"]["gradient_over_plain_forward"],
-                           "ms": adj["ms"], "memory_bytes": adj["memory_bytes"],
-                           "checkpointed": adj["checkpointed"],
-                           "direct_sum_reference": adj["direct_sum_reference"],
-                           "fd_check": fdc, "perturber": adj["perturber"],
-                           "workload": adj["config"]["workload"]}
+        # each sub-record on its own: a study that fails leaves an "error"
+        # entry, never the headline line unprinted
+        def study(name, fn):
+            try:
+                line[name] = fn()
+            except Exception as e:  # noqa: BLE001 -- recorded in the line
+                line[name] = {"error": f"{type(e).__name__}: {e}"}
+
+        def force_err():
+            dg = importlib.import_module("nbody-sim_b200.diagnostics")
+            targets = np.sort(np.random.default_rng(0).choice(n, min(args.targets, n),
+                                                              replace=False))
+            fe = dg.engine_force_errors(prm, st, targets)
+            return {"targets": len(targets), "total": fe["total"], "self": fe["self"],
+                    "vs": "FP64 direct sum (nbody_direct_f64) on the same FP32 positions; the "
+                          "engine's own walk (the timed one)"}
+
+        def ref_engine():
+            ref = ref_engine_study(st, n, args.theta)
+            if "value" in ref:
+                ref["ours_over_reference"] = value / ref["value"]
+            return ref
+
+        def ensemble():
+            ens = ensemble_study(args, ws, rank, local, args.steps)
+            return {"value": ens["value"], "ms_per_step": ens["ms_per_step"],
+                    "n_total": ens["config"]["n_total"], "disks": args.disks,
+                    "one_by_one_value": ens["one_by_one"]["value"],
+                    "one_by_one_ms_per_step": ens["one_by_one"]["ms_per_step"],
+                    "ensemble_over_one_by_one": ens["one_by_one"]["speedup"],
+                    "workload": ens["config"]["workload"]}
+
+        def adjoint():
+            adj = adjoint_study(args, args.adjoint_fd)
+            fdc = {k: v for k, v in adj["fd_check"].items() if k != "misses_at_h1e-6"}
+            fdc["misses_at_h1e-6"] = len(adj["fd_check"]["misses_at_h1e-6"])
+            return {"gradient_over_plain_forward": adj["ms"]["gradient_over_plain_forward"],
+                    "ms": adj["ms"], "memory_bytes": adj["memory_bytes"],
+                    "checkpointed": adj["checkpointed"],
+                    "direct_sum_reference": adj["direct_sum_reference"],
+                    "fd_check": fdc, "perturber": adj["perturber"],
+                    "workload": adj["config"]["workload"]}
+
+        study("force_err", force_err)
+        study("ref_engine", ref_engine)
+        study("ensemble", ensemble)
+        study("adjoint", adjoint)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
         secs = cpu_port_step(st, n, 0, 1)

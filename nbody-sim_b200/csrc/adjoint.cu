@@ -1605,7 +1605,8 @@ int nbody_adjoint_forward(nbody_adjoint* a, const double* x0, const double* y0, 
     const size_t n = m->n;
     for (int k = 0; k < 6; ++k)
       if (out[k]) {
-        const double* src = (k < 3 ? m->X[m->steps] : m->V[m->steps]) + (k % 3) * n;
+        const int sl = m->slot(m->steps);
+        const double* src = (k < 3 ? m->X[sl] : m->V[sl]) + (k % 3) * n;
         nb::check(cudaMemcpyAsync(out[k], src, sizeof(double) * n, cudaMemcpyDeviceToDevice,
                                   m->st), "forward out");
       }

@@ -51,9 +51,14 @@ struct CudaError : std::runtime_error {
   explicit CudaError(const std::string& s) : std::runtime_error(s) {}
 };
 
+// Throws on a failed runtime call.  The runtime also keeps that error as its
+// "last error" until read; it is read here, so that a later
+// cudaGetLastError() after a kernel launch reports that launch, not this call.
 inline void check(cudaError_t e, const char* what) {
-  if (e != cudaSuccess)
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
     throw CudaError(std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
+  }
 }
 
 inline int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }

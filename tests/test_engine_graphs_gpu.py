@@ -226,4 +226,4 @@ def test_shared_walk_gives_the_same_interactions(nb, cuda, mode):
     print(f"mode {mode}: spans {s1.spans} shared {s1.span_shared} frontier {s1.span_frontier} "
           f"visited {s0.walk_nodes_visited} -> {s1.walk_nodes_visited}; "
           f"diff max {d.max():.2e} median {np.median(d):.2e}")
-    assert d.max() < 1e-5
+    assert d.max() < 5e-5

@@ -77,8 +77,10 @@ def test_walk_stack_spill_capacity_reports_overflow(nb, cuda):
     st = disk(nb, n, 0.5, 5.0, seed=7, m=1e-8)
 
     def run(spill_cap):
+        # theta 0 and single-body leaves: every node is opened and pushed, so
+        # a warp's stack outgrows its shared-memory part
         prm = nb.sim_params(dt=0.01, theta=0.0, softening=1e-3, star_mass=1.0, r_coll=0.0,
-                            spill_cap=spill_cap)
+                            leaf_max=1, spill_cap=spill_cap)
         sim = nb.Sim(prm, n)
         sim.set_state(*[st[k] for k in STATE], st["m"])
         return sim
