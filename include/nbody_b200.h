@@ -360,6 +360,15 @@ int nbody_sim_set_state_f64(nbody_sim* s, const double* x, const double* y, cons
                             const float* mass, int on_device);
 /* Advances nsteps steps (asynchronous). */
 int nbody_sim_step(nbody_sim* s, int nsteps);
+/* Advances nsteps steps and leaves the last one open: its second kick and
+ * drag (src/main.cu:133-138) stay pending, so the next step's first kernel
+ * does them together with that step's first kick and drift, as every step
+ * inside one nbody_sim_step call does.  The engine closes a pending step
+ * itself before any read of the state (get_state, fof, output_begin,
+ * autotune) and nbody_sim_step finishes one; nbody_sim_close does only
+ * that.  For callers that advance one step per call in a loop. */
+int nbody_sim_step_open(nbody_sim* s, int nsteps);
+int nbody_sim_close(nbody_sim* s);
 /* Waits for the engine's stream and reports device status bits as errors. */
 int nbody_sim_sync(nbody_sim* s);
 /* State after the last step, in the caller's order (acceleration pointers may

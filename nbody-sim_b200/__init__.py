@@ -223,6 +223,8 @@ SIGNATURES = [
     ("nbody_sim_set_state", C.c_int, [_VP] + [_VP] * 7 + [C.c_int]),
     ("nbody_sim_set_state_f64", C.c_int, [_VP] + [_VP] * 7 + [C.c_int]),
     ("nbody_sim_step", C.c_int, [_VP, C.c_int]),
+    ("nbody_sim_step_open", C.c_int, [_VP, C.c_int]),
+    ("nbody_sim_close", C.c_int, [_VP]),
     ("nbody_sim_sync", C.c_int, [_VP]),
     ("nbody_sim_get_state", C.c_int, [_VP] + [_VP] * 9 + [C.c_int]),
     ("nbody_sim_get_state_f64", C.c_int, [_VP] + [_VP] * 6 + [C.c_int]),
@@ -686,6 +688,15 @@ class Sim:
 
     def step(self, nsteps: int = 1):
         _check(lib.nbody_sim_step(self.h, nsteps))
+
+    def step_open(self, nsteps: int = 1):
+        """nsteps steps, the last left open (nbody_sim_step_open): a loop of
+        one-step calls then runs every step in its fused form."""
+        _check(lib.nbody_sim_step_open(self.h, nsteps))
+
+    def close_steps(self):
+        """Finishes an open step (nbody_sim_close)."""
+        _check(lib.nbody_sim_close(self.h))
 
     def sync(self):
         _check(lib.nbody_sim_sync(self.h))

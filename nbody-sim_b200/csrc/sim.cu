@@ -534,7 +534,12 @@ struct SimBase {
   virtual void set_state(const void* const* v, bool is_double, const float* mass,
                          bool on_device, bool forces = true) = 0;
   virtual void get_state(void* const* v, bool as_double, float* const* a, bool on_device) = 0;
-  virtual void step(int nsteps) = 0;
+  // nsteps steps; close: end with the last step's second kick and drag.
+  // Left open, the velocities stay at the last step's half step and the next
+  // advance starts with its fused (second kick + drag, first kick) form.
+  virtual void advance(int nsteps, bool close) = 0;
+  void step(int nsteps) { advance(nsteps, true); }
+  bool open = false;  // the last step's second kick and drag are pending
   virtual const uint32_t* ids() = 0;
   // Positions and velocities in caller order as float, on the engine stream.
   virtual void snapshot(float* const* dst) = 0;
@@ -740,6 +745,7 @@ struct SimImpl : SimBase {
     check(cudaGetLastError(), "iota");
     steps_done = 0;
     has_state = true;
+    open = false;
     if (forces) {
       upload_perturber(-1, 1);  // (float)(0) * dt = 0
       launch_bbox<R>(tw, s[0].v[0], s[0].v[1], s[0].v[2], n, st);
@@ -918,28 +924,34 @@ struct SimImpl : SimBase {
     return gx[f][c];
   }
 
-  void step(int nsteps) override {
-    if (nsteps <= 0) return;
-    upload_perturber(steps_done, nsteps);
-    for (int k = 0; k < nsteps; ++k) {
-      if (use_graphs && !profiling) {
-        const int f = (k == 0) ? 1 : 0, c = cur;
-        check(cudaGraphLaunch(graph_for(k == 0), st), "graph launch");
-        launches += g_kernels[f][c];
-        graph_launches += 1;
-        cur = 1 - cur;
-      } else {
-        begin_step_profile();
-        one_step(k == 0);
+  void advance(int nsteps, bool close) override {
+    if (nsteps > 0) {
+      upload_perturber(steps_done, nsteps);
+      for (int k = 0; k < nsteps; ++k) {
+        const bool first = (k == 0) && !open;  // no pending second kick before it
+        if (use_graphs && !profiling) {
+          const int f = first ? 1 : 0, c = cur;
+          check(cudaGraphLaunch(graph_for(first), st), "graph launch");
+          launches += g_kernels[f][c];
+          graph_launches += 1;
+          cur = 1 - cur;
+        } else {
+          begin_step_profile();
+          one_step(first);
+        }
       }
+      steps_done += nsteps;
+      open = true;
     }
-    // the last step's dv + K2 + drag: a record that adds to the stream phase only
-    begin_step_profile(false);
-    stream_kernel(true, false);
-    for (int k = NBODY_PHASE_STREAM + 1; k <= NBODY_PHASES; ++k) mark(k);
-    launches += 1;
-    ev_cur = nullptr;
-    steps_done += nsteps;
+    if (close && open) {
+      // the last step's dv + K2 + drag: a record that adds to the stream phase only
+      begin_step_profile(false);
+      stream_kernel(true, false);
+      for (int k = NBODY_PHASE_STREAM + 1; k <= NBODY_PHASES; ++k) mark(k);
+      launches += 1;
+      ev_cur = nullptr;
+      open = false;
+    }
   }
 
   void get_state(void* const* v, bool as_double, float* const* acc, bool on_device) override {
@@ -1121,6 +1133,22 @@ int nbody_sim_step(nbody_sim* s, int nsteps) {
   })
 }
 
+int nbody_sim_step_open(nbody_sim* s, int nsteps) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(s, "nbody_sim_step_open: null sim");
+    NBODY_REQUIRE(s->impl->has_state, "nbody_sim_step_open: state not set");
+    NBODY_REQUIRE(nsteps >= 0, "nbody_sim_step_open: negative step count");
+    s->impl->advance(nsteps, false);
+  })
+}
+
+int nbody_sim_close(nbody_sim* s) {
+  NBODY_API_BODY({
+    NBODY_REQUIRE(s, "nbody_sim_close: null sim");
+    s->impl->advance(0, true);
+  })
+}
+
 int nbody_sim_sync(nbody_sim* s) {
   NBODY_API_BODY({
     NBODY_REQUIRE(s, "nbody_sim_sync: null sim");
@@ -1139,6 +1167,7 @@ int nbody_sim_get_state(nbody_sim* s, float* x, float* y, float* z, float* vx, f
   NBODY_API_BODY({
     NBODY_REQUIRE(s && x && y && z && vx && vy && vz, "nbody_sim_get_state: null array");
     NBODY_REQUIRE(s->impl->has_state, "nbody_sim_get_state: state not set");
+    s->impl->advance(0, true);  // a pending second kick first
     void* v[6] = {x, y, z, vx, vy, vz};
     float* a[3] = {ax, ay, az};
     s->impl->get_state(v, false, (ax && ay && az) ? a : nullptr, on_device != 0);
@@ -1150,6 +1179,7 @@ int nbody_sim_get_state_f64(nbody_sim* s, double* x, double* y, double* z, doubl
   NBODY_API_BODY({
     NBODY_REQUIRE(s && x && y && z && vx && vy && vz, "nbody_sim_get_state_f64: null array");
     NBODY_REQUIRE(s->impl->has_state, "nbody_sim_get_state_f64: state not set");
+    s->impl->advance(0, true);  // a pending second kick first
     void* v[6] = {x, y, z, vx, vy, vz};
     s->impl->get_state(v, true, nullptr, on_device != 0);
   })
@@ -1160,6 +1190,7 @@ int nbody_sim_fof(nbody_sim* s, float link_length, int* labels, uint16_t* agg_si
   NBODY_API_BODY({
     NBODY_REQUIRE(s && labels && agg_size && n_groups, "nbody_sim_fof: null argument");
     NBODY_REQUIRE(s->impl->has_state, "nbody_sim_fof: state not set");
+    s->impl->advance(0, true);  // a pending second kick first
     s->impl->fof(link_length, labels, agg_size, n_groups, on_device != 0);
   })
 }
@@ -1229,6 +1260,7 @@ int nbody_sim_autotune(nbody_sim* s, const int* candidates, int n_candidates, fl
   NBODY_API_BODY({
     NBODY_REQUIRE(s, "nbody_sim_autotune: null simulation");
     NBODY_REQUIRE(s->impl->has_state, "nbody_sim_autotune: no state set");
+    s->impl->advance(0, true);  // a pending second kick first
     NBODY_REQUIRE(!candidates || n_candidates >= 1, "nbody_sim_autotune: no candidates");
     s->impl->autotune(candidates, n_candidates, ms_out);
   })
@@ -1248,6 +1280,7 @@ int nbody_sim_output_begin(nbody_sim* s, float link_length, float particle_mass,
     NBODY_REQUIRE(s, "nbody_sim_output_begin: null sim");
     nb::SimBase* b = s->impl;
     NBODY_REQUIRE(b->has_state, "nbody_sim_output_begin: state not set");
+    b->advance(0, true);  // a pending second kick first
     NBODY_REQUIRE(link_length >= 0.f, "nbody_sim_output_begin: negative link length");
     if (!b->pipe) b->pipe = new nb::OutputPipe(b->n, b->p.leaf_max);
     const int k = b->pipe->begin_slot();

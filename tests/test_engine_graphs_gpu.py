@@ -227,3 +227,41 @@ def test_shared_walk_gives_the_same_interactions(nb, cuda, mode):
           f"visited {s0.walk_nodes_visited} -> {s1.walk_nodes_visited}; "
           f"diff max {d.max():.2e} median {np.median(d):.2e}")
     assert d.max() < 5e-5
+
+
+@pytest.mark.parametrize("precision", [0, 1], ids=["f32", "f64"])
+def test_open_steps_equal_one_call(nb, cuda, precision):
+    """Steps taken one call at a time and left open (nbody_sim_step_open)
+    run every step in its fused form; with the final second kick done by
+    nbody_sim_close they must equal one nbody_sim_step call of as many
+    steps, bit for bit (drag and perturber on)."""
+    n = 6000
+    st = disk(nb, n, 0.5, 5.0, seed=12, m=1e-8)
+    prm = nb.sim_params(dt=0.005, theta=0.5, softening=1e-3, star_mass=1.0, r_coll=0.0,
+                        gas_drag_rate=1e-3, perturber_enabled=1, perturber_mass_mjup=2.0,
+                        perturber_radius_au=7.0, state_precision=precision)
+    out = []
+    for mode in ("one call", "open"):
+        sim = nb.Sim(prm, n)
+        sim.set_state(st["x"], st["y"], st["z"], st["vx"], st["vy"], st["vz"], st["m"])
+        if mode == "one call":
+            sim.step(7)
+        else:
+            for _ in range(7):
+                sim.step_open(1)
+            sim.close_steps()
+        sim.sync()
+        out.append(sim.get_state(double=True, accel=False))
+        assert sim.stats().steps_done == 7
+        sim.close()
+    for k in out[0]:
+        assert np.array_equal(out[0][k], out[1][k]), k
+    # a read of the state closes a pending step by itself
+    sim = nb.Sim(prm, n)
+    sim.set_state(st["x"], st["y"], st["z"], st["vx"], st["vy"], st["vz"], st["m"])
+    for _ in range(7):
+        sim.step_open(1)
+    g = sim.get_state(double=True, accel=False)
+    sim.close()
+    for k in g:
+        assert np.array_equal(g[k], out[0][k]), k
