@@ -645,12 +645,10 @@ int nbody_radix_sort_u64(uint64_t* keys, uint32_t* values, int n, int bits);
  * bhtree_buildKernel, src/physics/BHTree.cu:175-277).  Device arrays of n - 1
  * internal nodes: children left/right (internal node i, or leaf j encoded as
  * n - 1 + j), key range lo..hi, and the common prefix within the low
- * key_bits.  Equal keys are split by their index.  variant 0 searches the
- * keys; variant 1 (the engine's) searches the common prefixes of adjacent
- * keys and their block minima: the same tree.  Synchronous; allocates its
- * own work space. */
-int nbody_radix_tree_u32(const uint32_t* keys, int n, int key_bits, int variant, int* left,
-                         int* right, int* lo, int* hi, uint8_t* prefix);
+ * key_bits.  Equal keys are split by their index.  Synchronous; allocates
+ * its own work space. */
+int nbody_radix_tree_u32(const uint32_t* keys, int n, int key_bits, int* left, int* right,
+                         int* lo, int* hi, uint8_t* prefix);
 /* Self-test of the radix sort's one bounded wait (no counterpart in the
  * reference, whose DFS sort is one serial thread, BHTree.cu:322-352): the
  * look-back of a tile over predecessor status words that no tile publishes.

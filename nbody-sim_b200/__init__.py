@@ -267,7 +267,7 @@ SIGNATURES = [
     ("nbody_radix_sort_u32", C.c_int, [_VP, _VP, C.c_int, C.c_int]),
     ("nbody_radix_sort_u64", C.c_int, [_VP, _VP, C.c_int, C.c_int]),
     ("nbody_selftest_sort_wait", C.c_int, [_I]),
-    ("nbody_radix_tree_u32", C.c_int, [_VP, C.c_int, C.c_int, C.c_int] + [_VP] * 5),
+    ("nbody_radix_tree_u32", C.c_int, [_VP, C.c_int, C.c_int] + [_VP] * 5),
     ("nbody_make_disk", C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                   C.c_double, C.c_uint64, _D, _D, _D, _D, _D, _D]),
 ]

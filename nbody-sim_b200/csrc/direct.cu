@@ -125,16 +125,15 @@ extern "C" int nbody_radix_sort_u64(uint64_t* keys, uint32_t* values, int n, int
   return radix_sort_api<uint64_t>(keys, values, n, bits, "nbody_radix_sort_u64");
 }
 
-extern "C" int nbody_radix_tree_u32(const uint32_t* keys, int n, int key_bits, int variant,
-                                    int* left, int* right, int* lo, int* hi, uint8_t* prefix) {
+extern "C" int nbody_radix_tree_u32(const uint32_t* keys, int n, int key_bits, int* left,
+                                    int* right, int* lo, int* hi, uint8_t* prefix) {
   NBODY_API_BODY({
     NBODY_REQUIRE(n >= 0, "nbody_radix_tree_u32: negative n");
     NBODY_REQUIRE(key_bits >= 1 && key_bits <= 32, "nbody_radix_tree_u32: bad bit count");
-    NBODY_REQUIRE(variant == 0 || variant == 1, "nbody_radix_tree_u32: variant must be 0 or 1");
     if (n < 2) return NBODY_OK;
     NBODY_REQUIRE(keys && left && right && lo && hi && prefix,
                   "nbody_radix_tree_u32: null array");
-    nb::radix_tree_u32(keys, n, key_bits, variant == 1, left, right, lo, hi, prefix);
+    nb::radix_tree_u32(keys, n, key_bits, left, right, lo, hi, prefix);
   })
 }
 

@@ -48,10 +48,6 @@ struct TreeWork {
   int *bin_left = nullptr, *bin_right = nullptr, *bin_parent = nullptr;
   int *bin_lo = nullptr, *bin_hi = nullptr;
   uint8_t* bin_prefix = nullptr;
-  // optional: common prefix of adjacent sorted keys and its block minima
-  // (lcp_levels), which the Karras pass searches instead of the keys
-  uint8_t* lcp = nullptr;
-  size_t lcp_bytes = 0;
   // FP64 moments: tile-local prefix sums of (m, m x, m y, m z), tile prefixes
   double4* mom_ploc = nullptr;
   double4* mom_tiles = nullptr;
@@ -114,11 +110,9 @@ void launch_gather_body4(TreeWork& w, const float* x, const float* y, const floa
 template <typename K>
 void launch_karras(TreeWork& w, const K* keys, int n, int key_bits, cudaStream_t s);
 // The binary radix tree of n sorted 32-bit keys into caller device arrays of
-// n - 1 internal nodes (synchronous, allocates its own work space);
-// prefix_minima selects the Karras pass that searches the adjacent-key
-// prefixes instead of the keys (the same tree).
-void radix_tree_u32(const uint32_t* keys, int n, int key_bits, bool prefix_minima, int* left,
-                    int* right, int* lo, int* hi, uint8_t* prefix);
+// n - 1 internal nodes (synchronous, allocates its own work space).
+void radix_tree_u32(const uint32_t* keys, int n, int key_bits, int* left, int* right, int* lo,
+                    int* hi, uint8_t* prefix);
 // Octree, FP64 moments and target groups over a Karras tree whose keys carry
 // a disk index in the disk_bits above the 30 Morton bits: one root slot per
 // disk (slots 0..n_roots-1), geoms[d] the root cube of disk d, group_disk

@@ -232,7 +232,10 @@ __device__ __forceinline__ int delta(const K* __restrict__ keys, int n, K ki, in
 // those bits, key_bits for runs of equal keys.  Tried and slower at N = 2^20:
 // staging the block's keys and a halo in shared memory (35 -> 39 us), and a
 // bottom-up agglomerative build (Apetrei 2014; 130 us: the last climbers'
-// chains of atomics and fences run the depth of the tree).
+// chains of atomics and fences run the depth of the tree), and range and
+// split searches over byte arrays of adjacent-key prefixes and their block
+// minima (the tree phase 0.123 -> 0.189 ms: the scans walk ~20 bytes per node
+// one dependent load at a time).
 template <typename K>
 __global__ void __launch_bounds__(kThreads)
 k_karras(const K* __restrict__ keys, int n, int key_bits, int* __restrict__ left,
@@ -261,172 +264,6 @@ k_karras(const K* __restrict__ keys, int n, int key_bits, int* __restrict__ left
   } while (t > 1);
   const int gamma = i + s * d + min(d, 0);
   const int lo = min(i, j), hi = max(i, j);
-  const int lc = (lo == gamma) ? (n - 1) + gamma : gamma;
-  const int rc = (hi == gamma + 1) ? (n - 1) + gamma + 1 : gamma + 1;
-  left[i] = lc;
-  right[i] = rc;
-  parent[lc] = i;
-  parent[rc] = i;
-  lo_out[i] = lo;
-  hi_out[i] = hi;
-  constexpr int kW = 8 * (int)sizeof(K);
-  prefix[i] = (uint8_t)(dnode >= kW ? key_bits : dnode - (kW - key_bits));
-  if (i == 0) parent[0] = -1;
-}
-
-// ----------------------------------------------------------- LCP Karras
-// The same binary radix tree as k_karras, found from the common prefixes of
-// adjacent keys instead of by searching the keys.  lcp[k] = delta(k, k+1);
-// for sorted keys delta(i, j) = min(lcp[i .. j-1]), so
-//   * node i's range ends at the first k >= i (d = +1) with lcp[k] <= dmin,
-//     or starts after the last k < i (d = -1) with lcp[k] <= dmin;
-//   * its split is the first k in its range with lcp[k] == delta(lo, hi).
-// Both are nearest-smaller-value searches, answered over block minima of
-// 32^l entries (levels 1 .. kLcpLevels - 1): a node scans bytes of its own
-// 128-byte lines, where a search of the keys loads 4-byte keys at doubling
-// distances.  Position n - 1 holds 0 and every search stops there.
-constexpr int kLcpLevels = 6;
-
-struct LcpLevels {
-  const uint8_t* lv[kLcpLevels];
-  int len[kLcpLevels];
-};
-
-__host__ __device__ inline int lcp_level_len(int n, int l) {
-  long long len = n;
-  for (int k = 0; k < l; ++k) len = (len + 31) / 32;
-  return (int)len;
-}
-
-size_t lcp_levels_bytes(int n) {
-  size_t b = 0;
-  for (int l = 0; l < kLcpLevels; ++l) b += (size_t)(lcp_level_len(n, l) + 3) / 4 * 4;
-  return b;
-}
-
-LcpLevels lcp_levels(uint8_t* base, int n) {
-  LcpLevels L{};
-  size_t off = 0;
-  for (int l = 0; l < kLcpLevels; ++l) {
-    L.lv[l] = base + off;
-    L.len[l] = lcp_level_len(n, l);
-    off += (size_t)(L.len[l] + 3) / 4 * 4;
-  }
-  return L;
-}
-
-// lcp[k] and the minima of levels 1 and 2 (1024-thread blocks: a warp's 32
-// entries make one level-1 entry, a block's 32 warps one level-2 entry).
-template <typename K>
-__global__ void __launch_bounds__(1024) k_lcp(const K* __restrict__ keys, int n, LcpLevels L) {
-  __shared__ uint32_t s_w[32];
-  const int k = blockIdx.x * 1024 + threadIdx.x;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  uint32_t v = 0;
-  if (k < n - 1) v = (uint32_t)delta(keys, n, __ldg(keys + k), k, k + 1);
-  if (k < L.len[0]) const_cast<uint8_t*>(L.lv[0])[k] = (uint8_t)v;
-  uint32_t m = v;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) m = min(m, __shfl_xor_sync(kFull, m, o));
-  const int k1 = k >> 5;
-  if (lane == 0) {
-    if (k1 < L.len[1]) const_cast<uint8_t*>(L.lv[1])[k1] = (uint8_t)m;
-    s_w[warp] = m;
-  }
-  __syncthreads();
-  if (warp == 0) {
-    uint32_t b = s_w[lane];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) b = min(b, __shfl_xor_sync(kFull, b, o));
-    if (lane == 0 && blockIdx.x < L.len[2]) const_cast<uint8_t*>(L.lv[2])[blockIdx.x] = (uint8_t)b;
-  }
-}
-
-// Levels 3 .. kLcpLevels - 1 from level 2 (one block; level 2 has n / 1024
-// entries).
-__global__ void __launch_bounds__(1024) k_lcp_top(LcpLevels L) {
-  for (int l = 3; l < kLcpLevels; ++l) {
-    const uint8_t* src = L.lv[l - 1];
-    uint8_t* dst = const_cast<uint8_t*>(L.lv[l]);
-    for (int e = threadIdx.x; e < L.len[l]; e += blockDim.x) {
-      uint32_t m = 255;
-      const int q0 = e * 32, q1 = min(q0 + 32, L.len[l - 1]);
-      for (int q = q0; q < q1; ++q) m = min(m, (uint32_t)src[q]);
-      dst[e] = (uint8_t)m;
-    }
-    __syncthreads();
-  }
-}
-
-// Smallest k >= i with lcp[k] <= v, or n - 1 (positions from n - 1 on stop).
-__device__ __forceinline__ int nsv_right(const LcpLevels& L, int i, int v, int n) {
-  if (i >= n - 1) return n - 1;
-  int k = i, l = 0;
-  while (true) {  // ascend: the rest of k's block at level l, else the next block above
-    const int end = min((k | 31) + 1, L.len[l]);
-    int q = k;
-    while (q < end && (int)L.lv[l][q] > v) ++q;
-    if (q < end) {
-      k = q;
-      break;
-    }
-    if (end >= L.len[l] || l + 1 >= kLcpLevels) return n - 1;
-    k = end >> 5;
-    ++l;
-  }
-  while (l > 0) {  // descend to the first entry <= v below
-    --l;
-    int q = k * 32;
-    while ((int)L.lv[l][q] > v) ++q;
-    k = q;
-  }
-  return min(k, n - 1);
-}
-
-// Largest k <= i with lcp[k] <= v, or -1.
-__device__ __forceinline__ int nsv_left(const LcpLevels& L, int i, int v) {
-  if (i < 0) return -1;
-  int k = i, l = 0;
-  while (true) {
-    const int start = k & ~31;
-    int q = k;
-    while (q >= start && (int)L.lv[l][q] > v) --q;
-    if (q >= start) {
-      k = q;
-      break;
-    }
-    if (start == 0 || l + 1 >= kLcpLevels) return -1;
-    k = (start >> 5) - 1;
-    ++l;
-  }
-  while (l > 0) {
-    --l;
-    int q = min(k * 32 + 31, L.len[l] - 1);
-    while ((int)L.lv[l][q] > v) --q;
-    k = q;
-  }
-  return k;
-}
-
-template <typename K>
-__global__ void __launch_bounds__(kThreads)
-k_karras_lcp(const K* __restrict__ keys, int n, int key_bits, LcpLevels L,
-             int* __restrict__ left, int* __restrict__ right, int* __restrict__ parent,
-             int* __restrict__ lo_out, int* __restrict__ hi_out, uint8_t* __restrict__ prefix,
-             int* __restrict__ opar) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n - 1) return;
-  opar[i] = -1;
-  opar[n - 1 + i] = -1;
-  if (i == 0) opar[2 * n - 2] = -1;
-  const int dl = (i > 0) ? (int)L.lv[0][i - 1] : -1;
-  const int dr = (int)L.lv[0][i];
-  const int d = (dr - dl > 0) ? 1 : -1;
-  const int dmin = (d > 0) ? dl : dr;
-  const int j = (d > 0) ? nsv_right(L, i, dmin, n) : nsv_left(L, i - 1, dmin) + 1;
-  const int lo = min(i, j), hi = max(i, j);
-  const int dnode = delta(keys, n, __ldg(keys + lo), lo, hi);
-  const int gamma = nsv_right(L, lo, dnode, n);
   const int lc = (lo == gamma) ? (n - 1) + gamma : gamma;
   const int rc = (hi == gamma + 1) ? (n - 1) + gamma + 1 : gamma + 1;
   left[i] = lc;
@@ -924,8 +761,6 @@ void tree_alloc(TreeWork& w, int cap) {
   w.bin_lo = dalloc<int>(n, "bin_lo");
   w.bin_hi = dalloc<int>(n, "bin_hi");
   w.bin_prefix = dalloc<uint8_t>(n, "bin_prefix");
-  w.lcp_bytes = lcp_levels_bytes(cap);
-  w.lcp = dalloc<uint8_t>(w.lcp_bytes, "lcp levels");
   w.mom_ploc = dalloc<double4>(n + 1, "moment prefix");
   w.mom_tiles = dalloc<double4>(2 * ((n + 1) / kTileM + 2), "moment tiles");
   w.oct_nch = dalloc<uint8_t>(nb, "oct_nch");
@@ -951,7 +786,7 @@ void tree_free(TreeWork& w) {
   void* ptrs[] = {w.keys, w.perm, w.keys_alt, w.perm_alt, w.counts, w.body4, w.bin_left,
                   w.bin_right, w.bin_parent, w.bin_lo, w.bin_hi, w.bin_prefix, w.mom_ploc,
                   w.mom_tiles, w.oct_nch, w.oct_cidx, w.oct_off, w.scan_tmp, w.oct.com, w.oct.info, w.oct.box_lo, w.oct.box_hi, w.bbox_enc,
-                  w.geom, w.n_nodes, w.status, w.groups, w.group_flag, w.n_groups, w.lcp};
+                  w.geom, w.n_nodes, w.status, w.groups, w.group_flag, w.n_groups};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (w.side) cudaStreamDestroy(w.side);
@@ -1046,19 +881,9 @@ template void launch_keys_multi<HiLo>(const HiLo*, const HiLo*, const HiLo*, con
 template <typename K>
 void launch_karras(TreeWork& w, const K* keys, int n, int key_bits, cudaStream_t s) {
   if (n < 2) return;
-  if (w.lcp && w.lcp_bytes >= lcp_levels_bytes(n)) {
-    const LcpLevels L = lcp_levels(w.lcp, n);
-    k_lcp<K><<<div_up(n, 1024), 1024, 0, s>>>(keys, n, L);
-    if (kLcpLevels > 3 && L.len[2] > 1) k_lcp_top<<<1, 1024, 0, s>>>(L);
-    k_karras_lcp<K><<<grid_for(n - 1), kThreads, 0, s>>>(keys, n, key_bits, L, w.bin_left,
-                                                         w.bin_right, w.bin_parent, w.bin_lo,
-                                                         w.bin_hi, w.bin_prefix,
-                                                         (int*)w.group_flag);
-  } else {
-    k_karras<K><<<grid_for(n - 1), kThreads, 0, s>>>(keys, n, key_bits, w.bin_left, w.bin_right,
-                                                     w.bin_parent, w.bin_lo, w.bin_hi,
-                                                     w.bin_prefix, (int*)w.group_flag);
-  }
+  k_karras<K><<<grid_for(n - 1), kThreads, 0, s>>>(keys, n, key_bits, w.bin_left, w.bin_right,
+                                                   w.bin_parent, w.bin_lo, w.bin_hi,
+                                                   w.bin_prefix, (int*)w.group_flag);
   check(cudaGetLastError(), "k_karras launch");
   w.opar_fresh = true;
 }
@@ -1121,15 +946,11 @@ void launch_tree(TreeWork& w, const K* keys, int n, int key_bits, int disk_bits,
 
 template void launch_karras<uint64_t>(TreeWork&, const uint64_t*, int, int, cudaStream_t);
 
-void radix_tree_u32(const uint32_t* keys, int n, int key_bits, bool prefix_minima, int* left,
-                    int* right, int* lo, int* hi, uint8_t* prefix) {
+void radix_tree_u32(const uint32_t* keys, int n, int key_bits, int* left, int* right, int* lo,
+                    int* hi, uint8_t* prefix) {
   TreeWork w;
   tree_alloc(w, n);
   try {
-    if (!prefix_minima) {
-      cudaFree(w.lcp);
-      w.lcp = nullptr;
-    }
     launch_karras<uint32_t>(w, keys, n, key_bits, 0);
     const size_t m = (size_t)std::max(n - 1, 0);
     check(cudaMemcpy(left, w.bin_left, sizeof(int) * m, cudaMemcpyDeviceToDevice), "tree out");

@@ -73,7 +73,7 @@ def test_phase_api_reports_a_non_finite_position(nb, cuda):
 
 
 def test_walk_stack_spill_capacity_reports_overflow(nb, cuda):
-    n = 20000
+    n = 200_000
     st = disk(nb, n, 0.5, 5.0, seed=7, m=1e-8)
 
     def run(spill_cap):
