@@ -422,7 +422,9 @@ int nbody_sim_set_graphs(nbody_sim* s, int on);
 /* Per-phase device time of the steps run while profiling is on: CUDA events
  * at the phase boundaries of every step, on the engine's stream.  Phase k of
  * a step runs from its boundary k to boundary k+1; the stream phase also
- * holds the closing dv + K2 + drag of the call's last step. */
+ * holds the closing dv + K2 + drag of the call's last step.  With graphs on
+ * (the default) each profiled step is captured with the events as nodes of
+ * its graph, so the phases are timed as the step graphs run them. */
 #define NBODY_PHASE_STREAM 0   /* dv + K2 + drag + K1 + drift + bbox          */
 #define NBODY_PHASE_SORT 1     /* Morton keys + radix sort                    */
 #define NBODY_PHASE_PERMUTE 2  /* state gathered into key order               */

@@ -109,6 +109,19 @@ __device__ __forceinline__ unsigned lanemask_lt() {
   return m;
 }
 
+// Programmatic dependent launch (sm_90+).  A kernel launched with the
+// programmatic-serialization attribute may start before the kernel ahead of
+// it in the stream has finished: grid_dependency_wait() returns once that
+// kernel has completed and its writes are visible (at once for a kernel
+// launched without the attribute), and grid_dependents_launch() lets the
+// next such kernel start early.
+__device__ __forceinline__ void grid_dependency_wait() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+__device__ __forceinline__ void grid_dependents_launch() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Spreads the low 10 bits of v so that bit k lands on bit 3k.
 __device__ __forceinline__ uint32_t spread3(uint32_t v) {
   v &= 0x3ffu;

@@ -503,7 +503,10 @@ struct SimBase {
   }
   void mark(int phase) {  // boundary before `phase` (NBODY_PHASES = end)
     if (!ev_cur) return;
-    check(cudaEventRecord((*ev_cur)[phase], st), "cudaEventRecord");
+    // inside a capture: an event-record node of the step's graph
+    check(cudaEventRecordWithFlags((*ev_cur)[phase], st,
+                                   capturing ? cudaEventRecordExternal : cudaEventRecordDefault),
+          "cudaEventRecord");
   }
   void begin_step_profile(bool is_step = true) {
     if (!profiling) { ev_cur = nullptr; return; }
@@ -581,10 +584,15 @@ struct SimBase {
   cudaGraphExec_t gx[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
   unsigned long long g_kernels[2][2] = {{0, 0}, {0, 0}};
   unsigned long long graph_launches = 0;
+  // Profiled steps with graphs on: the same step graphs, captured with an
+  // event-record node at each phase boundary (pev: their events).
+  cudaGraphExec_t pgx[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  std::vector<cudaEvent_t> pev[2][2];
   void drop_graphs() {
-    for (auto& row : gx)
-      for (auto& g : row)
-        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    for (auto* set : {&gx, &pgx})
+      for (auto& row : *set)
+        for (auto& g : row)
+          if (g) { cudaGraphExecDestroy(g); g = nullptr; }
   }
 
   void common_free() {
@@ -602,6 +610,9 @@ struct SimBase {
     }
     for (auto& evs : ev_pending)
       for (cudaEvent_t e : evs) ev_pool.push_back(e);
+    for (auto& row : pev)
+      for (auto& evs : row)
+        for (cudaEvent_t e : evs) ev_pool.push_back(e);
     for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
     tree_free(tw);
     void* ptrs[] = {ax, ay, az, dvx, dvy, dvz, pert_tab, pert_step, spill, work, inter,
@@ -924,6 +935,50 @@ struct SimImpl : SimBase {
     return gx[f][c];
   }
 
+  // A profiled step as the graphs run it: the step graph captured with an
+  // event-record node at each phase boundary (kept like the plain graphs),
+  // replayed, and its events read once it has run, so the phase times hold
+  // the graph's own launch gaps and overlap.
+  void profiled_graph_step(bool first) {
+    const int f = first ? 1 : 0, c = cur;
+    std::vector<cudaEvent_t>& evs = pev[f][c];
+    if (evs.empty())
+      for (int k = 0; k <= NBODY_PHASES; ++k) evs.push_back(take_event());
+    if (!pgx[f][c]) {
+      if (!cap_st) check(cudaStreamCreateWithFlags(&cap_st, cudaStreamNonBlocking), "capture stream");
+      const unsigned long long l0 = launches;
+      cudaStream_t user = st;
+      st = cap_st;
+      cudaGraph_t graph = nullptr;
+      check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+      capturing = true;
+      ev_cur = &evs;
+      one_step(first);
+      ev_cur = nullptr;
+      capturing = false;
+      const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+      st = user;
+      check(ce, "end capture");
+      cur = c;  // captured, not run
+      g_kernels[f][c] = launches - l0;
+      launches = l0;
+      const cudaError_t ie = cudaGraphInstantiate(&pgx[f][c], graph, 0);
+      cudaGraphDestroy(graph);
+      check(ie, "graph instantiate");
+    }
+    check(cudaGraphLaunch(pgx[f][c], st), "graph launch");
+    check(cudaStreamSynchronize(st), "profiled graph step");
+    for (int k = 0; k < NBODY_PHASES; ++k) {
+      float ms = 0.f;
+      check(cudaEventElapsedTime(&ms, evs[k], evs[k + 1]), "cudaEventElapsedTime");
+      phase_ms[k] += ms;
+    }
+    ++profiled_steps;
+    launches += g_kernels[f][c];
+    graph_launches += 1;
+    cur = 1 - cur;
+  }
+
   void advance(int nsteps, bool close) override {
     if (nsteps > 0) {
       upload_perturber(steps_done, nsteps);
@@ -935,6 +990,8 @@ struct SimImpl : SimBase {
           launches += g_kernels[f][c];
           graph_launches += 1;
           cur = 1 - cur;
+        } else if (use_graphs) {
+          profiled_graph_step(first);
         } else {
           begin_step_profile();
           one_step(first);

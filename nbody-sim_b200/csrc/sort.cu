@@ -173,7 +173,13 @@ k_onesweep(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int i = tid; i < kSortWarps * kBins; i += kSortThreads) (&s_cnt[0][0])[i] = 0;
+  // the ticket words were cleared before the sort's first pass
   if (tid == 0) s_tile = atomicAdd(ticket, 1);
+  // Launched as a programmatic dependent of the previous pass, the tile may
+  // start while that pass still runs: everything below reads or clears what
+  // it writes, so wait for it to finish here, then let the next pass launch.
+  grid_dependency_wait();
+  grid_dependents_launch();
   __syncthreads();
   const int t = s_tile;
   // the next pass's status words of this tile (the pass before last used
@@ -367,30 +373,45 @@ int pick_items(int n) {
   return it;
 }
 
+// dependent: launched as a programmatic dependent of the kernel ahead of it
+// on s (the previous pass), so that its launch overlaps that pass's tail.
 template <typename K, int kItems>
 void launch_onesweep(int ntiles, const K* ki, const uint32_t* vi, K* ko, uint32_t* vo, int n,
                      int shift, const uint32_t* base, int* ticket, uint32_t* st, int* err,
-                     uint32_t* clear_next, cudaStream_t s) {
-  k_onesweep<K, kItems><<<ntiles, kSortThreads, 0, s>>>(ki, vi, ko, vo, n, shift, base, ticket,
-                                                        st, err, clear_next);
+                     uint32_t* clear_next, cudaStream_t s, bool dependent) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)ntiles);
+  cfg.blockDim = dim3(kSortThreads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = dependent ? 1 : 0;
+  check(cudaLaunchKernelEx(&cfg, k_onesweep<K, kItems>, ki, vi, ko, vo, n, shift, base, ticket,
+                           st, err, clear_next),
+        "k_onesweep launch");
 }
 
 template <typename K>
 void launch_onesweep_items(int items, int ntiles, const K* ki, const uint32_t* vi, K* ko,
                            uint32_t* vo, int n, int shift, const uint32_t* base, int* ticket,
-                           uint32_t* st, int* err, uint32_t* clear_next, cudaStream_t s) {
+                           uint32_t* st, int* err, uint32_t* clear_next, cudaStream_t s,
+                           bool dependent) {
   if constexpr (sizeof(K) == 4) {
     if (items == 16)
       return launch_onesweep<K, 16>(ntiles, ki, vi, ko, vo, n, shift, base, ticket, st, err,
-                                    clear_next, s);
+                                    clear_next, s, dependent);
   }
   if (items == 8)
     return launch_onesweep<K, 8>(ntiles, ki, vi, ko, vo, n, shift, base, ticket, st, err,
-                                 clear_next, s);
+                                 clear_next, s, dependent);
   if (items == 4)
     return launch_onesweep<K, 4>(ntiles, ki, vi, ko, vo, n, shift, base, ticket, st, err,
-                                 clear_next, s);
-  launch_onesweep<K, 2>(ntiles, ki, vi, ko, vo, n, shift, base, ticket, st, err, clear_next, s);
+                                 clear_next, s, dependent);
+  launch_onesweep<K, 2>(ntiles, ki, vi, ko, vo, n, shift, base, ticket, st, err, clear_next, s,
+                        dependent);
 }
 
 }  // namespace
@@ -440,10 +461,12 @@ void radix_sort_pairs(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt,
   for (int p = 0; p < passes; ++p) {
     uint32_t* cur = (two && (p & 1)) ? st + tile_words : st;
     uint32_t* next = (two && p + 1 < passes) ? ((p & 1) ? st : st + tile_words) : nullptr;
-    if (p == 0 || !two)
+    const bool reset = p == 0 || !two;
+    if (reset)
       check(cudaMemsetAsync(cur, 0, sizeof(uint32_t) * tile_words, s), "radix sort status reset");
+    // a pass right behind the previous one launches as its programmatic dependent
     launch_onesweep_items<K>(items, ntiles, ki, vi, ko, vo, n, 8 * p, hist + (size_t)p * kBins,
-                             tickets + p, cur, err, next, s);
+                             tickets + p, cur, err, next, s, !reset);
     K* t = ki; ki = ko; ko = t;
     uint32_t* u = vi; vi = vo; vo = u;
   }

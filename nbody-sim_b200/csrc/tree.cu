@@ -525,44 +525,49 @@ __global__ void __launch_bounds__(kThreads) k_mark(const MarkArgs<K> a) {
   if (threadIdx.x == 0) a.tile_sum[blockIdx.x] = t;
 }
 
-// Exclusive scan of the tile sums in place (one block; integer sums; each
-// thread loads 8 sums at once).
+__device__ __forceinline__ unsigned long long warp_incl_scan_u64(unsigned long long v, int lane) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned long long q = __shfl_up_sync(kFull, v, o);
+    if (lane >= o) v += q;
+  }
+  return v;
+}
+
+// Exclusive scan of the tile sums in place (one block; integer sums).  Warp
+// w scans 256 consecutive sums of a chunk as 8 rows of 32 with coalesced
+// loads and stores (a thread's own run of 8 consecutive sums made every load
+// touch 16 lines, and the L1 wavefronts took 8 us at 8192 sums).
 __global__ void __launch_bounds__(1024) k_tiles(unsigned long long* __restrict__ v, int m) {
-  constexpr int kPer = 8;
+  constexpr int kRows = 8, kChunk = 1024 * kRows;
   __shared__ unsigned long long s_w[32];
   __shared__ unsigned long long s_carry;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) s_carry = 0;
-  for (int c0 = 0; c0 < m; c0 += 1024 * kPer) {
-    unsigned long long x[kPer], sum = 0;
+  __syncthreads();
+  for (int c0 = 0; c0 < m; c0 += kChunk) {
+    const int base = c0 + warp * (32 * kRows) + lane;
+    unsigned long long x[kRows], ex[kRows], run = 0;
 #pragma unroll
-    for (int k = 0; k < kPer; ++k) {
-      const int i = c0 + tid * kPer + k;
-      x[k] = (i < m) ? v[i] : 0ull;
-      sum += x[k];
-    }
-    unsigned long long inc = sum;
+    for (int k = 0; k < kRows; ++k) x[k] = (base + 32 * k < m) ? v[base + 32 * k] : 0ull;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const unsigned long long q = __shfl_up_sync(kFull, inc, o);
-      if (lane >= o) inc += q;
+    for (int k = 0; k < kRows; ++k) {
+      const unsigned long long inc = warp_incl_scan_u64(x[k], lane);
+      ex[k] = run + inc - x[k];
+      run += __shfl_sync(kFull, inc, 31);
     }
-    if (lane == 31) s_w[warp] = inc;
+    if (lane == 0) s_w[warp] = run;  // the warp's total
     __syncthreads();
-    unsigned long long run = s_carry + inc - sum;
-    for (int w = 0; w < warp; ++w) run += s_w[w];
+    // exclusive prefix of the warps' totals, by every warp for itself
+    const unsigned long long t = s_w[lane];
+    const unsigned long long ti = warp_incl_scan_u64(t, lane);
+    const unsigned long long wpre = s_carry + __shfl_sync(kFull, ti - t, warp);
+    const unsigned long long total = __shfl_sync(kFull, ti, 31);
 #pragma unroll
-    for (int k = 0; k < kPer; ++k) {
-      const int i = c0 + tid * kPer + k;
-      if (i < m) v[i] = run;
-      run += x[k];
-    }
+    for (int k = 0; k < kRows; ++k)
+      if (base + 32 * k < m) v[base + 32 * k] = wpre + ex[k];
     __syncthreads();
-    if (tid == 0) {
-      unsigned long long c = s_carry;
-      for (int w = 0; w < 32; ++w) c += s_w[w];
-      s_carry = c;
-    }
+    if (tid == 0) s_carry += total;
     __syncthreads();
   }
 }
