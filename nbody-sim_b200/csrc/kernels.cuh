@@ -53,7 +53,6 @@ struct TreeWork {
   double4* mom_tiles = nullptr;
   // octree layout
   uint8_t* oct_nch = nullptr;
-  uint8_t* oct_cidx = nullptr;  // a child record's index among its siblings
   uint32_t* oct_off = nullptr;
   uint32_t* scan_tmp = nullptr;
   OctNodes oct;
@@ -64,7 +63,6 @@ struct TreeWork {
   int* status = nullptr;
   // warp target groups: (first body, count), maximal binary nodes <= 32 bodies
   int2* groups = nullptr;
-  uint32_t* group_flag = nullptr;
   int* n_groups = nullptr;
   // optional (set by the caller): per group, (index of the first group cut
   // from the same span node, bodies in that node) -- the shared walk's spans
@@ -85,9 +83,9 @@ struct TreeWork {
   // parallel branches).  Created by tree_enable_overlap; null: one stream.
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-  // The Karras pass also sets the octree-parent words to -1 (host-side flag:
-  // the next octree build over that tree needs no reset of its own).
-  bool opar_fresh = false;
+  // Host-side flag: the moment prefix of the octree build in flight runs on
+  // `side` (joined through ev_join before the records are written).
+  bool moments_on_side = false;
 };
 
 void tree_alloc(TreeWork& w, int cap);
@@ -117,17 +115,21 @@ void radix_tree_u32(const uint32_t* keys, int n, int key_bits, int* left, int* r
 // a disk index in the disk_bits above the 30 Morton bits: one root slot per
 // disk (slots 0..n_roots-1), geoms[d] the root cube of disk d, group_disk
 // (optional) receives each group's disk.
-// moments_ready: the moment prefix is already launched (launch_tree on the
-// side stream, joined through w.ev_join before the records are written).
+// moments_ready: the moment prefix is already launched (on w.side when
+// w.moments_on_side, joined through w.ev_join before the records are
+// written; else earlier on s).
 template <typename K>
 void launch_octree(TreeWork& w, const K* keys, int n, int disk_bits, int n_roots,
                    const TreeGeom* geoms, int* group_disk, const double* xd, const double* yd,
                    const double* zd, cudaStream_t s, bool moments_ready = false);
 // launch_karras + launch_octree, with the moment prefix on w.side when set.
+// tiles_done: the caller has already written the tile-local moment prefix
+// (w.mom_ploc) and the tile sums (w.mom_tiles) on s, as the engine's permute
+// does; only the scan of the tile sums is left.
 template <typename K>
 void launch_tree(TreeWork& w, const K* keys, int n, int key_bits, int disk_bits, int n_roots,
                  const TreeGeom* geoms, int* group_disk, const double* xd, const double* yd,
-                 const double* zd, cudaStream_t s);
+                 const double* zd, cudaStream_t s, bool tiles_done = false);
 // Ensembles: root cube of every disk from its encoded bbox (6 words per
 // disk); bbox accumulators reset for n_disks; composite keys
 // (disk << 30 | Morton) with disk[i] the body's disk.
@@ -153,6 +155,8 @@ void launch_build_moments(TreeWork& w, int n, const double* xd, const double* yd
 void launch_moment_prefix(TreeWork& w, int n, const double* xd, const double* yd,
                           const double* zd, cudaStream_t s);
 double4* moment_tile_prefix(TreeWork& w, int n);
+// Moment tiles over n bodies (blocks of the tile-local scan).
+inline int moment_tiles(int n) { return n / kMomentTile + 1; }
 
 size_t radix_sort_count_words(int n);
 // Runs the sort's look-back wait against tile-status words that nothing

@@ -49,8 +49,8 @@ constexpr size_t kWorkBytes =
     al(sizeof(uint8_t) * kMaxN) +               // bin_prefix
     al(sizeof(double4) * (kMaxN + 1)) +         // moment prefix sums
     al(sizeof(double4) * kMomTiles) +           // moment tile sums / prefixes
-    2 * al(sizeof(uint8_t) * kNb) +             // oct_nch, oct_cidx
-    2 * al(sizeof(uint32_t) * kNb) +            // oct_off, group_flag
+    al(sizeof(uint8_t) * kNb) +                 // oct_nch
+    al(sizeof(uint32_t) * kNb) +                // oct_off
     al(sizeof(uint32_t) * kScanWords) +         // octree tile sums
     4 * al(sizeof(float4) * kNb) +              // octree com, info, box_lo, box_hi
     al(sizeof(unsigned long long) * 6) +        // bbox
@@ -112,9 +112,7 @@ int fof_in_scratch(unsigned char* base, const float* x, const float* y, const fl
   w.mom_ploc = c.take<double4>(kMaxN + 1);
   w.mom_tiles = c.take<double4>(kMomTiles);
   w.oct_nch = c.take<uint8_t>(kNb);
-  w.oct_cidx = c.take<uint8_t>(kNb);
   w.oct_off = c.take<uint32_t>(kNb);
-  w.group_flag = c.take<uint32_t>(kNb);
   w.scan_tmp = c.take<uint32_t>(kScanWords);
   w.oct.com = c.take<float4>(kNb);
   w.oct.info = c.take<int4>(kNb);

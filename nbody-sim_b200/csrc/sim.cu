@@ -22,6 +22,7 @@
 #include "capi_util.h"
 #include "common.cuh"
 #include "kernels.cuh"
+#include "moments.cuh"
 #include "output.h"
 #include "physics.cuh"
 
@@ -71,10 +72,18 @@ struct StepReset {
   unsigned long long* counters = nullptr;
 };
 
+// State gathered into the new key order, plus the float4 bodies, in the
+// moment tiles' layout (kMomentThreads threads with two consecutive bodies
+// each, one block per tile of kMomentTile bodies): the gathered bodies' FP64
+// moments (m, m x, m y, m z) -- from the FP64 positions for a double state,
+// else from the float4 bodies, as k_moment_tiles takes them -- are scanned
+// into the tile-local prefix and the tile sums on the way, so the octree
+// build needs no pass of its own over the bodies.
 template <typename R>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kMomentThreads)
 k_permute(const uint32_t* __restrict__ perm, StateArrays<R> in, StateArrays<R> out, int n,
-          float4* __restrict__ body4, const StepReset r) {
+          float4* __restrict__ body4, const StepReset r, double4* __restrict__ ploc,
+          double4* __restrict__ tile_sum) {
   if (blockIdx.x == 0) {  // counters the step uses next (each has a sole writer)
     for (int i = threadIdx.x; i < r.enc_words; i += blockDim.x)
       r.enc[i] = ((i % 6) < 3) ? ~0ull : 0ull;
@@ -82,24 +91,35 @@ k_permute(const uint32_t* __restrict__ perm, StateArrays<R> in, StateArrays<R> o
     if (threadIdx.x == 1 && r.inter) *r.inter = 0ull;
     if (threadIdx.x >= 2 && threadIdx.x < 5 && r.counters) r.counters[threadIdx.x - 2] = 0ull;
   }
-  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
-       s += (long long)gridDim.x * blockDim.x) {
+  const long long base = (long long)blockIdx.x * kMomentTile + 2ll * threadIdx.x;
+  double4 v[2];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const long long s = base + k;
+    v[k] = make_double4(0, 0, 0, 0);
+    if (s >= n) continue;
     // every gather first, then every store: the arrays carry no restrict, so
     // interleaving them would make each load wait for the store before it
     const uint32_t o = perm[s];
     R q[6];
 #pragma unroll
-    for (int k = 0; k < 6; ++k) q[k] = in.v[k][o];
+    for (int c = 0; c < 6; ++c) q[c] = in.v[c][o];
     const float m = in.m[o];
     const int id = in.id[o];
     const int dk = in.disk ? in.disk[o] : 0;
 #pragma unroll
-    for (int k = 0; k < 6; ++k) out.v[k][s] = q[k];
+    for (int c = 0; c < 6; ++c) out.v[c][s] = q[c];
     out.m[s] = m;
     out.id[s] = id;
     if (in.disk) out.disk[s] = dk;
-    body4[s] = make_float4((float)q[0], (float)q[1], (float)q[2], m);
+    const float4 b = make_float4((float)q[0], (float)q[1], (float)q[2], m);
+    body4[s] = b;
+    if constexpr (kIsF64<R>)
+      v[k] = body_moment((double)m, (double)q[0], (double)q[1], (double)q[2]);
+    else
+      v[k] = body_moment((double)m, (double)b.x, (double)b.y, (double)b.z);
   }
+  moment_tile_scan(v[0], v[1], base, n, ploc, tile_sum);
 }
 
 struct StreamArgs {
@@ -788,8 +808,8 @@ struct SimImpl : SimBase {
     StepReset rs;
     rs.enc = tw.bbox_enc; rs.enc_words = 6;
     rs.work = work; rs.inter = inter; rs.counters = counters;
-    k_permute<R><<<std::max(1, div_up(n, kThreads)), kThreads, 0, st>>>(tw.perm, a, b, n,
-                                                                        tw.body4, rs);
+    k_permute<R><<<moment_tiles(n), kMomentThreads, 0, st>>>(tw.perm, a, b, n, tw.body4, rs,
+                                                             tw.mom_ploc, tw.mom_tiles);
     check(cudaGetLastError(), "k_permute launch");
     check(cudaEventRecordWithFlags(ev_pos, st, capturing ? cudaEventRecordExternal
                                                          : cudaEventRecordDefault),
@@ -803,10 +823,10 @@ struct SimImpl : SimBase {
     if (kIsF64<R>)
       launch_tree<uint32_t>(tw, tw.keys, n, 30, 0, 1, tw.geom, nullptr,
                             (const double*)s[cur].v[0], (const double*)s[cur].v[1],
-                            (const double*)s[cur].v[2], st);
+                            (const double*)s[cur].v[2], st, true);
     else
       launch_tree<uint32_t>(tw, tw.keys, n, 30, 0, 1, tw.geom, nullptr, nullptr, nullptr, nullptr,
-                            st);
+                            st, true);
     WalkArgs w{};
     w.com = tw.oct.com; w.info = tw.oct.info; w.body = tw.body4; w.n = n;
     w.groups = tw.groups; w.n_groups = tw.n_groups;
@@ -844,9 +864,9 @@ struct SimImpl : SimBase {
     if (side_coll) check(cudaStreamWaitEvent(st, cs.join, 0), "collision join");
     mark(NBODY_PHASE_COLLIDE);
     // keys (+ digit histograms), 4 one-sweep passes, permute (+ bbox and
-    // walk counter resets), karras, mark, tile scan, apply, moment tiles,
-    // moment tile scan, emit, walk
-    launches += 14;
+    // walk counter resets, + moment tiles), moment tile scan, karras, mark,
+    // tile scan, apply, emit, walk
+    launches += 13;
   }
 
   // Collisions inside the walk (one warp per group of <= 32 targets).
@@ -1632,8 +1652,8 @@ struct EnsembleImpl : EnsembleBase {
     StepReset rs;
     rs.enc = bbox; rs.enc_words = 6 * D;
     rs.work = work; rs.inter = inter; rs.counters = counters;
-    k_permute<R><<<std::max(1, div_up(n, kThreads)), kThreads, 0, st>>>(tw.perm, a, b, n,
-                                                                        tw.body4, rs);
+    k_permute<R><<<moment_tiles(n), kMomentThreads, 0, st>>>(tw.perm, a, b, n, tw.body4, rs,
+                                                             tw.mom_ploc, tw.mom_tiles);
     check(cudaGetLastError(), "k_permute launch");
     check(cudaEventRecordWithFlags(ev_pos, st, capturing ? cudaEventRecordExternal
                                                          : cudaEventRecordDefault),
@@ -1643,10 +1663,10 @@ struct EnsembleImpl : EnsembleBase {
     if (kIsF64<R>)
       launch_tree<uint64_t>(tw, keys64, n, key_bits, disk_bits, D, geoms, group_disk,
                             (const double*)s[cur].v[0], (const double*)s[cur].v[1],
-                            (const double*)s[cur].v[2], st);
+                            (const double*)s[cur].v[2], st, true);
     else
       launch_tree<uint64_t>(tw, keys64, n, key_bits, disk_bits, D, geoms, group_disk, nullptr,
-                            nullptr, nullptr, st);
+                            nullptr, nullptr, st, true);
     WalkArgs w{};
     w.com = tw.oct.com; w.info = tw.oct.info; w.body = tw.body4; w.n = n;
     w.groups = tw.groups; w.n_groups = tw.n_groups;
@@ -1677,9 +1697,9 @@ struct EnsembleImpl : EnsembleBase {
     launch_walk(w, st);
     if (side_coll) check(cudaStreamWaitEvent(st, cs.join, 0), "collision join");
     // geoms, keys (+ digit histograms), one one-sweep kernel per pass,
-    // permute (+ bbox and walk counter resets), karras, mark, tile scan,
-    // apply, moment tiles, moment tile scan, emit, walk
-    launches += 2 + (key_bits + 7) / 8 + 9;
+    // permute (+ bbox and walk counter resets, + moment tiles), moment tile
+    // scan, karras, mark, tile scan, apply, emit, walk
+    launches += 2 + (key_bits + 7) / 8 + 8;
   }
 
   void collide(cudaStream_t on, int* wk, int* sp) {

@@ -240,13 +240,9 @@ template <typename K>
 __global__ void __launch_bounds__(kThreads)
 k_karras(const K* __restrict__ keys, int n, int key_bits, int* __restrict__ left,
          int* __restrict__ right, int* __restrict__ parent, int* __restrict__ lo_out,
-         int* __restrict__ hi_out, uint8_t* __restrict__ prefix, int* __restrict__ opar) {
+         int* __restrict__ hi_out, uint8_t* __restrict__ prefix) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n - 1) return;
-  // octree parents of the records the build will write: none yet
-  opar[i] = -1;
-  opar[n - 1 + i] = -1;
-  if (i == 0) opar[2 * n - 2] = -1;
   const K ki = __ldg(keys + i);
   const int d = (delta(keys, n, ki, i, i + 1) - delta(keys, n, ki, i, i - 1)) > 0 ? 1 : -1;
   const int dmin = delta(keys, n, ki, i, i - d);
@@ -285,23 +281,8 @@ k_karras(const K* __restrict__ keys, int n, int key_bits, int* __restrict__ left
 // two differences of partial sums no larger than the node's own tiles, so
 // cancellation stays at the level of a tile (~1e-13 relative) rather than of
 // the whole disk.  Fixed tiling: the sums are the same on every run.
-constexpr int kMomThreads = 1024;
+constexpr int kMomThreads = kMomentThreads;
 constexpr int kTileM = kMomentTile;  // 1024 threads x 2 bodies
-constexpr int kPerThr = kTileM / kMomThreads;
-
-__device__ __forceinline__ double4 d4shfl_up(double4 v, int o) {
-  return make_double4(__shfl_up_sync(kFull, v.x, o), __shfl_up_sync(kFull, v.y, o),
-                      __shfl_up_sync(kFull, v.z, o), __shfl_up_sync(kFull, v.w, o));
-}
-
-__device__ __forceinline__ double4 d4warp_incl_scan(double4 v, int lane) {
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const double4 t = d4shfl_up(v, o);
-    if (lane >= o) v = d4add(v, t);
-  }
-  return v;
-}
 
 // Large blocks with two bodies per thread keep the registers low and the
 // loads and stores nearly contiguous (8 bodies per thread needed 93
@@ -310,42 +291,19 @@ __global__ void __launch_bounds__(kMomThreads)
 k_moment_tiles(const float4* __restrict__ body4, const double* __restrict__ xd,
                const double* __restrict__ yd, const double* __restrict__ zd, int n,
                double4* __restrict__ ploc, double4* __restrict__ tile_sum) {
-  __shared__ double4 s_w[kMomThreads / 32];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const long long base = (long long)blockIdx.x * kTileM + (long long)tid * kPerThr;
-  double4 v[kPerThr];
-  double4 sum = make_double4(0, 0, 0, 0);
+  const long long base = (long long)blockIdx.x * kTileM + 2ll * threadIdx.x;
+  double4 v[2];
 #pragma unroll
-  for (int k = 0; k < kPerThr; ++k) {
+  for (int k = 0; k < 2; ++k) {
     const long long i = base + k;
     v[k] = make_double4(0, 0, 0, 0);
     if (i < n) {
       const float4 b = body4[i];
-      const double m = (double)b.w;
-      const double px = xd ? xd[i] : (double)b.x, py = yd ? yd[i] : (double)b.y,
-                   pz = zd ? zd[i] : (double)b.z;
-      v[k] = make_double4(m, m * px, m * py, m * pz);
+      v[k] = body_moment((double)b.w, xd ? xd[i] : (double)b.x, yd ? yd[i] : (double)b.y,
+                         zd ? zd[i] : (double)b.z);
     }
-    sum = d4add(sum, v[k]);
   }
-  const double4 inc = d4warp_incl_scan(sum, lane);
-  if (lane == 31) s_w[warp] = inc;
-  __syncthreads();
-  if (warp == 0) {  // exclusive prefix of the warp sums
-    const double4 x = s_w[lane];
-    const double4 y = d4warp_incl_scan(x, lane);
-    __syncwarp();
-    s_w[lane] = d4sub(y, x);
-  }
-  __syncthreads();
-  double4 run = d4add(s_w[warp], d4sub(inc, sum));
-#pragma unroll
-  for (int k = 0; k < kPerThr; ++k) {
-    const long long i = base + k;
-    if (i <= n) ploc[i] = run;  // index n gets the tile's local prefix at n
-    run = d4add(run, v[k]);
-  }
-  if (tid == kMomThreads - 1) tile_sum[blockIdx.x] = run;
+  moment_tile_scan(v[0], v[1], base, n, ploc, tile_sum);
 }
 
 // Exclusive scan of the tile sums into tpre[0..ntiles] (one block of 1024
@@ -455,14 +413,16 @@ __device__ __forceinline__ void classify(int n, int disk_bits, const int* __rest
 // ------------------------------------------------- octree slots + groups
 // Three passes over the binary nodes, none of which waits on another block:
 //   k_mark   counts each octree node's children (tops with more than `prune`
-//            bodies) and each group node's runs, tells every child its
-//            octree parent and its index among the siblings, and reduces
-//            both counts per tile;
+//            bodies) and each group node's runs, and reduces both counts per
+//            tile;
 //   k_tiles  scans the tile sums (one block);
 //   k_apply  scans the counts within each tile, adds the tile prefix, stores
 //            each node's first child slot and writes the group runs.
-// k_emit then writes every record from the node's own data at its slot:
-// n_roots + off[parent] + index, or the disk index for a disk's root.
+// k_emit then has every octree node with children write its children's
+// records at n_roots + off[node] + index (index: the children in key order),
+// and each disk's root written at the disk index.  Writing a record from its
+// parent needs no per-child parent and index arrays (2 N words written by
+// the slot passes and read back by the record pass).
 // The two counts travel packed in one 64-bit word: children << 31 | runs.
 constexpr int kMarkTile = kThreads;
 constexpr uint8_t kNchTop = 0x80;   // nch[b]: b is an octree node
@@ -480,8 +440,6 @@ struct MarkArgs {
   const uint8_t* prefix;
   uint8_t* nch;                // child count | kNchTop | kNchRoot
   uint32_t* off;               // k_mark: children | runs << 4; k_apply: first child slot - n_roots
-  int* opar;                   // octree parent of each child record (-1 on entry)
-  uint8_t* cidx;               // index of a child record among its siblings
   unsigned long long* tile_sum;
 };
 
@@ -511,10 +469,7 @@ __global__ void __launch_bounds__(kThreads) k_mark(const MarkArgs<K> a) {
     const int c = bin_count(a.lo, a.hi, n, b);
     if (top && b < n - 1 && lb < 10 && c > a.prune)
       nchild = (uint32_t)for_each_oct_child(a.left, a.right, a.prefix, n, a.disk_bits, b, lb,
-                                            [&](int ch, int i) {
-                                              a.opar[ch] = b;
-                                              a.cidx[ch] = (uint8_t)i;
-                                            });
+                                            [](int, int) {});
     const int pc = (p < 0 || lp < 0) ? 0x7fffffff : bin_count(a.lo, a.hi, n, p);
     if (lb >= 0 && c <= a.gspan && pc > a.gspan) runs = (uint32_t)((c + a.gmax - 1) / a.gmax);
     const bool root = top && (p < 0 || lp < 0);
@@ -644,13 +599,11 @@ __device__ __forceinline__ uint32_t compact3(uint32_t v) {
 template <typename K>
 struct EmitArgs {
   int n, disk_bits, n_roots;
-  const int *lo, *hi;
+  const int *left, *right, *lo, *hi;
   const uint8_t* prefix;
   const K* keys;
   const uint8_t* nch;
   const uint32_t* off;
-  const int* opar;
-  const uint8_t* cidx;
   const float4* body4;
   const double4* ploc;
   const double4* tpre;
@@ -704,24 +657,57 @@ __device__ void write_node(const EmitArgs<K>& a, int c, int f) {
   a.oct.box_hi[f] = make_float4(bhi[0], bhi[1], bhi[2], 0.f);
 }
 
-// Every octree node with a record writes it: a disk's root at slot = disk
-// index, a child at n_roots + off[parent] + its sibling index.
+// Slot of the record of disk root c.
 template <typename K>
-__global__ void __launch_bounds__(kThreads, 6) k_emit(const EmitArgs<K> a) {
-  const int nb = 2 * a.n - 1;
+__device__ __forceinline__ int root_slot(const EmitArgs<K>& a, int c) {
+  if (sizeof(K) == 4) return 0;
+  return key_disk(a.keys[(c >= a.n - 1) ? c - (a.n - 1) : a.lo[c]]);
+}
+
+// Records written by their parents.  Thread b (an internal binary node) owes
+// the records of its octree children when it is an octree node with
+// children (slots n_roots + off[b] + i, in key order), of its binary
+// children that are disks' roots (several disks only), and its own when it is
+// node 0 and a root.  An octree node's children are never roots, so each
+// record has one writer.  The warp lists its (node, slot) pairs in shared
+// memory and writes them one per lane.
+constexpr int kEmitPerLane = 9;  // 8 children + node 0's own record
+template <typename K>
+__global__ void __launch_bounds__(kThreads) k_emit(const EmitArgs<K> a) {
+  __shared__ int2 s_rec[kThreads / 32][32 * kEmitPerLane];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int2* rec = s_rec[warp];
+  const int n = a.n;
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= nb) return;
-  const uint8_t h = a.nch[b];
-  if (!(h & kNchTop)) return;
-  int f;
-  if (h & kNchRoot) {
-    f = (sizeof(K) == 4) ? 0 : key_disk(a.keys[(b >= a.n - 1) ? b - (a.n - 1) : a.lo[b]]);
-  } else {
-    const int P = a.opar[b];
-    if (P < 0) return;  // under a node the walk opens as bodies: no record
-    f = a.n_roots + (int)a.off[P] + a.cidx[b];
+  const bool on = b < n - 1;
+  const uint8_t h = on ? a.nch[b] : 0;
+  const int kids = h & kNchCount;
+  const bool self_root = b == 0 && (h & kNchRoot);
+  int lc = -1, rc = -1;
+  if (on && a.n_roots > 1) {  // binary children that are disks' roots
+    const int l = a.left[b], r = a.right[b];
+    if (a.nch[l] & kNchRoot) lc = l;
+    if (a.nch[r] & kNchRoot) rc = r;
   }
-  write_node(a, b, f);
+  const int cnt = kids + (self_root ? 1 : 0) + (lc >= 0 ? 1 : 0) + (rc >= 0 ? 1 : 0);
+  const int incl = warp_incl_scan(cnt, lane);
+  const int total = __shfl_sync(kFull, incl, 31);
+  int o = incl - cnt;
+  if (kids > 0) {
+    const int lb = bin_level(a.prefix, n, b, a.disk_bits);
+    const int first = a.n_roots + (int)a.off[b];
+    for_each_oct_child(a.left, a.right, a.prefix, n, a.disk_bits, b, lb,
+                       [&](int ch, int i) { rec[o + i] = make_int2(ch, first + i); });
+    o += kids;
+  }
+  if (self_root) rec[o++] = make_int2(b, root_slot(a, b));
+  if (lc >= 0) rec[o++] = make_int2(lc, root_slot(a, lc));
+  if (rc >= 0) rec[o++] = make_int2(rc, root_slot(a, rc));
+  __syncwarp();
+  for (int e = lane; e < total; e += 32) {
+    const int2 r = rec[e];
+    write_node(a, r.x, r.y);
+  }
 }
 
 // N == 1: the root is the single body and the only group.
@@ -769,7 +755,6 @@ void tree_alloc(TreeWork& w, int cap) {
   w.mom_ploc = dalloc<double4>(n + 1, "moment prefix");
   w.mom_tiles = dalloc<double4>(2 * ((n + 1) / kTileM + 2), "moment tiles");
   w.oct_nch = dalloc<uint8_t>(nb, "oct_nch");
-  w.oct_cidx = dalloc<uint8_t>(nb, "oct_cidx");
   w.oct_off = dalloc<uint32_t>(nb, "oct_off");
   w.scan_tmp = dalloc<uint32_t>(octree_scan_words((int)nb), "octree tile sums");
   w.oct.com = dalloc<float4>(nb, "oct com");
@@ -780,7 +765,6 @@ void tree_alloc(TreeWork& w, int cap) {
   w.geom = dalloc<TreeGeom>(1, "geom");
   w.n_nodes = dalloc<int>(1, "n_nodes");
   w.groups = dalloc<int2>(n, "groups");
-  w.group_flag = dalloc<uint32_t>(nb, "group flags");
   w.n_groups = dalloc<int>(1, "n_groups");
   w.status = dalloc<int>(1, "status");
   check(cudaMemset(w.status, 0, sizeof(int)), "status init");
@@ -790,8 +774,8 @@ void tree_alloc(TreeWork& w, int cap) {
 void tree_free(TreeWork& w) {
   void* ptrs[] = {w.keys, w.perm, w.keys_alt, w.perm_alt, w.counts, w.body4, w.bin_left,
                   w.bin_right, w.bin_parent, w.bin_lo, w.bin_hi, w.bin_prefix, w.mom_ploc,
-                  w.mom_tiles, w.oct_nch, w.oct_cidx, w.oct_off, w.scan_tmp, w.oct.com, w.oct.info, w.oct.box_lo, w.oct.box_hi, w.bbox_enc,
-                  w.geom, w.n_nodes, w.status, w.groups, w.group_flag, w.n_groups};
+                  w.mom_tiles, w.oct_nch, w.oct_off, w.scan_tmp, w.oct.com, w.oct.info, w.oct.box_lo, w.oct.box_hi, w.bbox_enc,
+                  w.geom, w.n_nodes, w.status, w.groups, w.n_groups};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (w.side) cudaStreamDestroy(w.side);
@@ -888,9 +872,8 @@ void launch_karras(TreeWork& w, const K* keys, int n, int key_bits, cudaStream_t
   if (n < 2) return;
   k_karras<K><<<grid_for(n - 1), kThreads, 0, s>>>(keys, n, key_bits, w.bin_left, w.bin_right,
                                                    w.bin_parent, w.bin_lo, w.bin_hi,
-                                                   w.bin_prefix, (int*)w.group_flag);
+                                                   w.bin_prefix);
   check(cudaGetLastError(), "k_karras launch");
-  w.opar_fresh = true;
 }
 
 template <typename K>
@@ -914,31 +897,36 @@ void launch_octree(TreeWork& w, const K* keys, int n, int disk_bits, int n_roots
     k_moment_tiles<<<ntiles, kMomThreads, 0, s>>>(w.body4, xd, yd, zd, n, w.mom_ploc, tile_sum);
     k_tile_scan<<<1, 1024, 0, s>>>(tile_sum, ntiles, tpre);
   }
-  int* opar = (int*)w.group_flag;
   unsigned long long* tsum = (unsigned long long*)w.scan_tmp;
   const int mtiles = div_up(nb, kMarkTile);
-  if (!w.opar_fresh)  // set by the Karras pass before the first octree build over it
-    check(cudaMemsetAsync(opar, 0xff, sizeof(int) * (size_t)nb, s), "octree parent reset");
-  w.opar_fresh = false;
   MarkArgs<K> m{n, gmax, gspan, w.prune_max, disk_bits, w.bin_left, w.bin_right, w.bin_parent,
-                w.bin_lo, w.bin_hi, w.bin_prefix, w.oct_nch, w.oct_off, opar, w.oct_cidx, tsum};
+                w.bin_lo, w.bin_hi, w.bin_prefix, w.oct_nch, w.oct_off, tsum};
   k_mark<K><<<mtiles, kMarkTile, 0, s>>>(m);
   k_tiles<<<1, 1024, 0, s>>>(tsum, mtiles);
   ApplyArgs<K> ap{n, n_roots, w.bin_lo, w.bin_hi, keys, w.oct_off, tsum, w.groups, group_disk,
                   w.n_nodes, w.n_groups, w.group_spans};
   k_apply<K><<<mtiles, kMarkTile, 0, s>>>(ap);
-  EmitArgs<K> a{n, disk_bits, n_roots, w.bin_lo, w.bin_hi, w.bin_prefix, keys, w.oct_nch,
-                w.oct_off, opar, w.oct_cidx, w.body4, w.mom_ploc, tpre, geoms, w.oct};
-  if (moments_ready) check(cudaStreamWaitEvent(s, w.ev_join, 0), "moment join");
-  k_emit<K><<<grid_for(nb), kThreads, 0, s>>>(a);
+  EmitArgs<K> a{n, disk_bits, n_roots, w.bin_left, w.bin_right, w.bin_lo, w.bin_hi, w.bin_prefix,
+                keys, w.oct_nch, w.oct_off, w.body4, w.mom_ploc, tpre, geoms, w.oct};
+  if (moments_ready && w.moments_on_side) check(cudaStreamWaitEvent(s, w.ev_join, 0), "moment join");
+  k_emit<K><<<grid_for(n - 1), kThreads, 0, s>>>(a);
   check(cudaGetLastError(), "octree launch");
 }
 
 template <typename K>
 void launch_tree(TreeWork& w, const K* keys, int n, int key_bits, int disk_bits, int n_roots,
                  const TreeGeom* geoms, int* group_disk, const double* xd, const double* yd,
-                 const double* zd, cudaStream_t s) {
+                 const double* zd, cudaStream_t s, bool tiles_done) {
+  if (tiles_done && n >= 1) {  // the caller's permute wrote the tile-local prefix and tile sums
+    w.moments_on_side = false;
+    const int ntiles = moment_tiles(n);
+    k_tile_scan<<<1, 1024, 0, s>>>(w.mom_tiles, ntiles, moment_tile_prefix(w, n));
+    launch_karras<K>(w, keys, n, key_bits, s);
+    launch_octree<K>(w, keys, n, disk_bits, n_roots, geoms, group_disk, xd, yd, zd, s, true);
+    return;
+  }
   const bool fork = w.side && n >= 2;
+  w.moments_on_side = fork;
   if (fork) {
     check(cudaEventRecord(w.ev_fork, s), "tree fork");
     check(cudaStreamWaitEvent(w.side, w.ev_fork, 0), "tree fork");
@@ -975,10 +963,10 @@ template void launch_octree<uint64_t>(TreeWork&, const uint64_t*, int, int, int,
                                       const double*, cudaStream_t, bool);
 template void launch_tree<uint32_t>(TreeWork&, const uint32_t*, int, int, int, int,
                                     const TreeGeom*, int*, const double*, const double*,
-                                    const double*, cudaStream_t);
+                                    const double*, cudaStream_t, bool);
 template void launch_tree<uint64_t>(TreeWork&, const uint64_t*, int, int, int, int,
                                     const TreeGeom*, int*, const double*, const double*,
-                                    const double*, cudaStream_t);
+                                    const double*, cudaStream_t, bool);
 
 void launch_moment_prefix(TreeWork& w, int n, const double* xd, const double* yd,
                           const double* zd, cudaStream_t s) {
