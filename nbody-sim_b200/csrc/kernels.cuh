@@ -45,7 +45,8 @@ struct TreeWork {
   // bodies in key order
   float4* body4 = nullptr;
   // binary radix tree (internal nodes 0..n-2, leaves encoded n-1+j)
-  int *bin_left = nullptr, *bin_right = nullptr, *bin_parent = nullptr;
+  int *bin_left = nullptr, *bin_right = nullptr;
+  uint32_t* bin_pinfo = nullptr;  // per node: its parent's body count << 5 | level + 1
   int *bin_lo = nullptr, *bin_hi = nullptr;
   uint8_t* bin_prefix = nullptr;
   // FP64 moments: tile-local prefix sums of (m, m x, m y, m z), tile prefixes

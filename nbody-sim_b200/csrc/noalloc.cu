@@ -45,7 +45,7 @@ constexpr size_t kWorkBytes =
     al(sizeof(uint32_t) * kCountWords) +        // radix-sort counts + scan partials
     al(sizeof(float4) * kMaxN) +                // body4
     4 * al(sizeof(int) * kMaxN) +               // bin_left, bin_right, bin_lo, bin_hi
-    al(sizeof(int) * kNb) +                     // bin_parent
+    al(sizeof(uint32_t) * kNb) +                // bin_pinfo
     al(sizeof(uint8_t) * kMaxN) +               // bin_prefix
     al(sizeof(double4) * (kMaxN + 1)) +         // moment prefix sums
     al(sizeof(double4) * kMomTiles) +           // moment tile sums / prefixes
@@ -107,7 +107,7 @@ int fof_in_scratch(unsigned char* base, const float* x, const float* y, const fl
   w.bin_right = c.take<int>(kMaxN);
   w.bin_lo = c.take<int>(kMaxN);
   w.bin_hi = c.take<int>(kMaxN);
-  w.bin_parent = c.take<int>(kNb);
+  w.bin_pinfo = c.take<uint32_t>(kNb);
   w.bin_prefix = c.take<uint8_t>(kMaxN);
   w.mom_ploc = c.take<double4>(kMaxN + 1);
   w.mom_tiles = c.take<double4>(kMomTiles);

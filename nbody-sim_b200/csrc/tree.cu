@@ -236,10 +236,20 @@ __device__ __forceinline__ int delta(const K* __restrict__ keys, int n, K ki, in
 // split searches over byte arrays of adjacent-key prefixes and their block
 // minima (the tree phase 0.123 -> 0.189 ms: the scans walk ~20 bytes per node
 // one dependent load at a time).
+// Each internal node also tells both of its children what the octree passes
+// need to know about their parent, so that they never chase it: one word of
+// the parent's body count (saturated at 2^27 - 1, far above any group span)
+// << 5 | its octree level + 1 (0: it spans several disks).  Node 0 has no
+// parent and no word.
+constexpr uint32_t kNoParent = 0xffffffffu;
+__device__ __forceinline__ uint32_t pack_pinfo(int count, int level) {
+  return ((uint32_t)min(count, (1 << 27) - 1) << 5) | (uint32_t)(level + 1);
+}
+
 template <typename K>
 __global__ void __launch_bounds__(kThreads)
 k_karras(const K* __restrict__ keys, int n, int key_bits, int* __restrict__ left,
-         int* __restrict__ right, int* __restrict__ parent, int* __restrict__ lo_out,
+         int* __restrict__ right, uint32_t* __restrict__ pinfo, int* __restrict__ lo_out,
          int* __restrict__ hi_out, uint8_t* __restrict__ prefix) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n - 1) return;
@@ -264,13 +274,16 @@ k_karras(const K* __restrict__ keys, int n, int key_bits, int* __restrict__ left
   const int rc = (hi == gamma + 1) ? (n - 1) + gamma + 1 : gamma + 1;
   left[i] = lc;
   right[i] = rc;
-  parent[lc] = i;
-  parent[rc] = i;
   lo_out[i] = lo;
   hi_out[i] = hi;
   constexpr int kW = 8 * (int)sizeof(K);
-  prefix[i] = (uint8_t)(dnode >= kW ? key_bits : dnode - (kW - key_bits));
-  if (i == 0) parent[0] = -1;
+  const int pre = dnode >= kW ? key_bits : dnode - (kW - key_bits);
+  prefix[i] = (uint8_t)pre;
+  // octree level as bin_level gives it (the disk index sits above 30 Morton bits)
+  const int disk_bits = key_bits > 30 ? key_bits - 30 : 0;
+  const uint32_t pi = pack_pinfo(hi - lo + 1, pre < disk_bits ? -1 : (pre - disk_bits) / 3);
+  pinfo[lc] = pi;
+  pinfo[rc] = pi;
 }
 
 // ------------------------------------------------------------- moments
@@ -401,13 +414,16 @@ __device__ __forceinline__ int for_each_oct_child(const int* __restrict__ left,
 // A node is an octree node ("top") when it starts a deeper level than its
 // parent; a disk's root is a top whose parent spans several disks (or node 0
 // of a single disk).  Groups never span disks.
-__device__ __forceinline__ void classify(int n, int disk_bits, const int* __restrict__ parent,
+// lp: the parent's octree level (-1: it spans several disks, or b is node 0,
+// which has no parent); pc: the parent's body count (INT_MAX when lp < 0).
+__device__ __forceinline__ void classify(int n, int disk_bits, const uint32_t* __restrict__ pinfo,
                                          const uint8_t* __restrict__ prefix, int b, int& lb,
-                                         int& lp, bool& top, int& p) {
+                                         int& lp, bool& top, int& pc) {
   lb = bin_level(prefix, n, b, disk_bits);
-  p = (b == 0) ? -1 : parent[b];
-  lp = (p < 0) ? -1 : bin_level(prefix, n, p, disk_bits);
-  top = lb >= 0 && (p < 0 || lb > lp);
+  const uint32_t pi = (b == 0) ? kNoParent : pinfo[b];
+  lp = (pi == kNoParent) ? -1 : (int)(pi & 31u) - 1;
+  top = lb >= 0 && lb > lp;
+  pc = (lp < 0) ? 0x7fffffff : (int)(pi >> 5);
 }
 
 // ------------------------------------------------- octree slots + groups
@@ -436,7 +452,9 @@ __device__ __forceinline__ unsigned long long pack_counts(uint32_t children, uin
 template <typename K>
 struct MarkArgs {
   int n, gmax, gspan, prune, disk_bits;
-  const int *left, *right, *parent, *lo, *hi;
+  const int *left, *right;
+  const uint32_t* pinfo;
+  const int *lo, *hi;
   const uint8_t* prefix;
   uint8_t* nch;                // child count | kNchTop | kNchRoot
   uint32_t* off;               // k_mark: children | runs << 4; k_apply: first child slot - n_roots
@@ -463,16 +481,15 @@ __global__ void __launch_bounds__(kThreads) k_mark(const MarkArgs<K> a) {
   const int b = blockIdx.x * kMarkTile + threadIdx.x;
   uint32_t nchild = 0, runs = 0;
   if (b < nb) {
-    int lb, lp, p;
+    int lb, lp, pc;
     bool top;
-    classify(n, a.disk_bits, a.parent, a.prefix, b, lb, lp, top, p);
+    classify(n, a.disk_bits, a.pinfo, a.prefix, b, lb, lp, top, pc);
     const int c = bin_count(a.lo, a.hi, n, b);
     if (top && b < n - 1 && lb < 10 && c > a.prune)
       nchild = (uint32_t)for_each_oct_child(a.left, a.right, a.prefix, n, a.disk_bits, b, lb,
                                             [](int, int) {});
-    const int pc = (p < 0 || lp < 0) ? 0x7fffffff : bin_count(a.lo, a.hi, n, p);
     if (lb >= 0 && c <= a.gspan && pc > a.gspan) runs = (uint32_t)((c + a.gmax - 1) / a.gmax);
-    const bool root = top && (p < 0 || lp < 0);
+    const bool root = top && lp < 0;
     a.nch[b] = (uint8_t)nchild | (top ? kNchTop : 0) | (root ? kNchRoot : 0);
     a.off[b] = nchild | (runs << 4);
   }
@@ -748,7 +765,7 @@ void tree_alloc(TreeWork& w, int cap) {
   w.body4 = dalloc<float4>(n, "body4");
   w.bin_left = dalloc<int>(n, "bin_left");
   w.bin_right = dalloc<int>(n, "bin_right");
-  w.bin_parent = dalloc<int>(nb, "bin_parent");
+  w.bin_pinfo = dalloc<uint32_t>(nb, "bin_pinfo");
   w.bin_lo = dalloc<int>(n, "bin_lo");
   w.bin_hi = dalloc<int>(n, "bin_hi");
   w.bin_prefix = dalloc<uint8_t>(n, "bin_prefix");
@@ -773,7 +790,7 @@ void tree_alloc(TreeWork& w, int cap) {
 
 void tree_free(TreeWork& w) {
   void* ptrs[] = {w.keys, w.perm, w.keys_alt, w.perm_alt, w.counts, w.body4, w.bin_left,
-                  w.bin_right, w.bin_parent, w.bin_lo, w.bin_hi, w.bin_prefix, w.mom_ploc,
+                  w.bin_right, w.bin_pinfo, w.bin_lo, w.bin_hi, w.bin_prefix, w.mom_ploc,
                   w.mom_tiles, w.oct_nch, w.oct_off, w.scan_tmp, w.oct.com, w.oct.info, w.oct.box_lo, w.oct.box_hi, w.bbox_enc,
                   w.geom, w.n_nodes, w.status, w.groups, w.n_groups};
   for (void* p : ptrs)
@@ -871,7 +888,7 @@ template <typename K>
 void launch_karras(TreeWork& w, const K* keys, int n, int key_bits, cudaStream_t s) {
   if (n < 2) return;
   k_karras<K><<<grid_for(n - 1), kThreads, 0, s>>>(keys, n, key_bits, w.bin_left, w.bin_right,
-                                                   w.bin_parent, w.bin_lo, w.bin_hi,
+                                                   w.bin_pinfo, w.bin_lo, w.bin_hi,
                                                    w.bin_prefix);
   check(cudaGetLastError(), "k_karras launch");
 }
@@ -899,7 +916,7 @@ void launch_octree(TreeWork& w, const K* keys, int n, int disk_bits, int n_roots
   }
   unsigned long long* tsum = (unsigned long long*)w.scan_tmp;
   const int mtiles = div_up(nb, kMarkTile);
-  MarkArgs<K> m{n, gmax, gspan, w.prune_max, disk_bits, w.bin_left, w.bin_right, w.bin_parent,
+  MarkArgs<K> m{n, gmax, gspan, w.prune_max, disk_bits, w.bin_left, w.bin_right, w.bin_pinfo,
                 w.bin_lo, w.bin_hi, w.bin_prefix, w.oct_nch, w.oct_off, tsum};
   k_mark<K><<<mtiles, kMarkTile, 0, s>>>(m);
   k_tiles<<<1, 1024, 0, s>>>(tsum, mtiles);
