@@ -210,7 +210,7 @@ int nbody_fof(nbody_tree* t, const float* x, const float* y, const float* z, int
  *
  * All scratch (sort buffers, tree, union-find arrays, a bounded stack-spill
  * area, and a set-up input) lives in one statically sized device array inside
- * libnbody_b200.so, NBODY_FOF_NOALLOC_SCRATCH_BYTES bytes (12.9 MiB).  n is
+ * libnbody_b200.so, NBODY_FOF_NOALLOC_SCRATCH_BYTES bytes (13.1 MiB).  n is
  * limited to NBODY_FOF_NOALLOC_MAX_N bodies; larger n returns NBODY_ERR_ARG
  * with a message naming the limit.  Inputs and outputs are as for nbody_fof
  * (device x, y, z, labels, agg_size; host *n_groups), bit-identical results.
@@ -234,7 +234,7 @@ int nbody_fof(nbody_tree* t, const float* x, const float* y, const float* z, int
  * per-thread mode) race on the scratch and must be serialised by the caller.
  * The function calls no cudaMalloc, cudaFree or allocating library routine. */
 #define NBODY_FOF_NOALLOC_MAX_N 32768
-#define NBODY_FOF_NOALLOC_SCRATCH_BYTES 13504000
+#define NBODY_FOF_NOALLOC_SCRATCH_BYTES 13766144
 int nbody_fof_noalloc(const float* x, const float* y, const float* z, int n, float link_length,
                       int* labels, uint16_t* agg_size, int* n_groups);
 

@@ -55,6 +55,7 @@ struct TreeWork {
   // octree layout
   uint8_t* oct_nch = nullptr;
   uint32_t* oct_off = nullptr;
+  int* oct_node = nullptr;  // octree slot -> the binary node whose record it holds
   uint32_t* scan_tmp = nullptr;
   OctNodes oct;
   // device words

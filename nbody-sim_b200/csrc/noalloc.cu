@@ -51,6 +51,7 @@ constexpr size_t kWorkBytes =
     al(sizeof(double4) * kMomTiles) +           // moment tile sums / prefixes
     al(sizeof(uint8_t) * kNb) +                 // oct_nch
     al(sizeof(uint32_t) * kNb) +                // oct_off
+    al(sizeof(int) * kNb) +                     // oct_node
     al(sizeof(uint32_t) * kScanWords) +         // octree tile sums
     4 * al(sizeof(float4) * kNb) +              // octree com, info, box_lo, box_hi
     al(sizeof(unsigned long long) * 6) +        // bbox
@@ -113,6 +114,7 @@ int fof_in_scratch(unsigned char* base, const float* x, const float* y, const fl
   w.mom_tiles = c.take<double4>(kMomTiles);
   w.oct_nch = c.take<uint8_t>(kNb);
   w.oct_off = c.take<uint32_t>(kNb);
+  w.oct_node = c.take<int>(kNb);
   w.scan_tmp = c.take<uint32_t>(kScanWords);
   w.oct.com = c.take<float4>(kNb);
   w.oct.info = c.take<int4>(kNb);

@@ -434,11 +434,11 @@ __device__ __forceinline__ void classify(int n, int disk_bits, const uint32_t* _
 //   k_tiles  scans the tile sums (one block);
 //   k_apply  scans the counts within each tile, adds the tile prefix, stores
 //            each node's first child slot and writes the group runs.
-// k_emit then has every octree node with children write its children's
-// records at n_roots + off[node] + index (index: the children in key order),
-// and each disk's root written at the disk index.  Writing a record from its
-// parent needs no per-child parent and index arrays (2 N words written by
-// the slot passes and read back by the record pass).
+// k_apply also lists which binary node each slot holds: an octree node's
+// children at n_roots + off[node] + index (index: the children in key order)
+// and each disk's root at the disk index.  k_emit then writes one record per
+// slot, one thread each.  No per-child parent or sibling-index array is
+// needed (2 N words the slot passes wrote and the record pass read back).
 // The two counts travel packed in one 64-bit word: children << 31 | runs.
 constexpr int kMarkTile = kThreads;
 constexpr uint8_t kNchTop = 0x80;   // nch[b]: b is an octree node
@@ -550,10 +550,13 @@ __device__ __forceinline__ int key_disk(K k) { return (int)(k >> 30); }
 
 template <typename K>
 struct ApplyArgs {
-  int n, n_roots;
-  const int *lo, *hi;
+  int n, n_roots, disk_bits;
+  const int *left, *right, *lo, *hi;
+  const uint8_t* prefix;
+  const uint8_t* nch;
   const K* keys;
   uint32_t* off;
+  int* node_of;  // octree slot -> binary node of its record
   const unsigned long long* tile_pre;
   int2* groups;
   int* group_disk;  // optional: disk of each group
@@ -585,6 +588,16 @@ __global__ void __launch_bounds__(kThreads) k_apply(const ApplyArgs<K> a) {
   const uint32_t first = (uint32_t)(ex >> 31);
   const uint32_t goff = (uint32_t)(ex & 0x7fffffffull);
   a.off[b] = first;
+  if (nchild > 0) {  // which binary node each child slot holds, in key order
+    const int base = a.n_roots + (int)first;
+    for_each_oct_child(a.left, a.right, a.prefix, n, a.disk_bits, b,
+                       bin_level(a.prefix, n, b, a.disk_bits),
+                       [&](int ch, int i) { a.node_of[base + i] = ch; });
+  }
+  if (a.nch[b] & kNchRoot) {  // a disk's root: slot = the disk index
+    const int lo = (b >= n - 1) ? b - (n - 1) : a.lo[b];
+    a.node_of[sizeof(K) == 4 ? 0 : key_disk(a.keys[lo])] = b;
+  }
   if (runs > 0) {  // runs of c / runs or c / runs + 1 consecutive bodies
     const int lo = (b >= n - 1) ? b - (n - 1) : a.lo[b];
     const int c = (b >= n - 1) ? 1 : a.hi[b] - lo + 1;
@@ -616,7 +629,7 @@ __device__ __forceinline__ uint32_t compact3(uint32_t v) {
 template <typename K>
 struct EmitArgs {
   int n, disk_bits, n_roots;
-  const int *left, *right, *lo, *hi;
+  const int *lo, *hi;
   const uint8_t* prefix;
   const K* keys;
   const uint8_t* nch;
@@ -674,57 +687,16 @@ __device__ void write_node(const EmitArgs<K>& a, int c, int f) {
   a.oct.box_hi[f] = make_float4(bhi[0], bhi[1], bhi[2], 0.f);
 }
 
-// Slot of the record of disk root c.
+// One thread per record: slot f holds binary node node_of[f] (written by
+// k_apply); consecutive slots are siblings, so the record stores coalesce.
+// The record count is read on the device (a grid-stride loop over it).
 template <typename K>
-__device__ __forceinline__ int root_slot(const EmitArgs<K>& a, int c) {
-  if (sizeof(K) == 4) return 0;
-  return key_disk(a.keys[(c >= a.n - 1) ? c - (a.n - 1) : a.lo[c]]);
-}
-
-// Records written by their parents.  Thread b (an internal binary node) owes
-// the records of its octree children when it is an octree node with
-// children (slots n_roots + off[b] + i, in key order), of its binary
-// children that are disks' roots (several disks only), and its own when it is
-// node 0 and a root.  An octree node's children are never roots, so each
-// record has one writer.  The warp lists its (node, slot) pairs in shared
-// memory and writes them one per lane.
-constexpr int kEmitPerLane = 9;  // 8 children + node 0's own record
-template <typename K>
-__global__ void __launch_bounds__(kThreads) k_emit(const EmitArgs<K> a) {
-  __shared__ int2 s_rec[kThreads / 32][32 * kEmitPerLane];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int2* rec = s_rec[warp];
-  const int n = a.n;
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool on = b < n - 1;
-  const uint8_t h = on ? a.nch[b] : 0;
-  const int kids = h & kNchCount;
-  const bool self_root = b == 0 && (h & kNchRoot);
-  int lc = -1, rc = -1;
-  if (on && a.n_roots > 1) {  // binary children that are disks' roots
-    const int l = a.left[b], r = a.right[b];
-    if (a.nch[l] & kNchRoot) lc = l;
-    if (a.nch[r] & kNchRoot) rc = r;
-  }
-  const int cnt = kids + (self_root ? 1 : 0) + (lc >= 0 ? 1 : 0) + (rc >= 0 ? 1 : 0);
-  const int incl = warp_incl_scan(cnt, lane);
-  const int total = __shfl_sync(kFull, incl, 31);
-  int o = incl - cnt;
-  if (kids > 0) {
-    const int lb = bin_level(a.prefix, n, b, a.disk_bits);
-    const int first = a.n_roots + (int)a.off[b];
-    for_each_oct_child(a.left, a.right, a.prefix, n, a.disk_bits, b, lb,
-                       [&](int ch, int i) { rec[o + i] = make_int2(ch, first + i); });
-    o += kids;
-  }
-  if (self_root) rec[o++] = make_int2(b, root_slot(a, b));
-  if (lc >= 0) rec[o++] = make_int2(lc, root_slot(a, lc));
-  if (rc >= 0) rec[o++] = make_int2(rc, root_slot(a, rc));
-  __syncwarp();
-  for (int e = lane; e < total; e += 32) {
-    const int2 r = rec[e];
-    write_node(a, r.x, r.y);
-  }
+__global__ void __launch_bounds__(kThreads) k_emit(const EmitArgs<K> a,
+                                                   const int* __restrict__ node_of,
+                                                   const int* __restrict__ n_nodes) {
+  const int total = *n_nodes;
+  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < total; f += gridDim.x * blockDim.x)
+    write_node(a, node_of[f], f);
 }
 
 // N == 1: the root is the single body and the only group.
@@ -773,6 +745,7 @@ void tree_alloc(TreeWork& w, int cap) {
   w.mom_tiles = dalloc<double4>(2 * ((n + 1) / kTileM + 2), "moment tiles");
   w.oct_nch = dalloc<uint8_t>(nb, "oct_nch");
   w.oct_off = dalloc<uint32_t>(nb, "oct_off");
+  w.oct_node = dalloc<int>(nb, "oct_node");
   w.scan_tmp = dalloc<uint32_t>(octree_scan_words((int)nb), "octree tile sums");
   w.oct.com = dalloc<float4>(nb, "oct com");
   w.oct.info = dalloc<int4>(nb, "oct info");
@@ -791,7 +764,7 @@ void tree_alloc(TreeWork& w, int cap) {
 void tree_free(TreeWork& w) {
   void* ptrs[] = {w.keys, w.perm, w.keys_alt, w.perm_alt, w.counts, w.body4, w.bin_left,
                   w.bin_right, w.bin_pinfo, w.bin_lo, w.bin_hi, w.bin_prefix, w.mom_ploc,
-                  w.mom_tiles, w.oct_nch, w.oct_off, w.scan_tmp, w.oct.com, w.oct.info, w.oct.box_lo, w.oct.box_hi, w.bbox_enc,
+                  w.mom_tiles, w.oct_nch, w.oct_off, w.oct_node, w.scan_tmp, w.oct.com, w.oct.info, w.oct.box_lo, w.oct.box_hi, w.bbox_enc,
                   w.geom, w.n_nodes, w.status, w.groups, w.n_groups};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -920,13 +893,17 @@ void launch_octree(TreeWork& w, const K* keys, int n, int disk_bits, int n_roots
                 w.bin_lo, w.bin_hi, w.bin_prefix, w.oct_nch, w.oct_off, tsum};
   k_mark<K><<<mtiles, kMarkTile, 0, s>>>(m);
   k_tiles<<<1, 1024, 0, s>>>(tsum, mtiles);
-  ApplyArgs<K> ap{n, n_roots, w.bin_lo, w.bin_hi, keys, w.oct_off, tsum, w.groups, group_disk,
-                  w.n_nodes, w.n_groups, w.group_spans};
+  ApplyArgs<K> ap{n,         n_roots,  disk_bits, w.bin_left, w.bin_right, w.bin_lo,
+                  w.bin_hi,  w.bin_prefix, w.oct_nch, keys,   w.oct_off,   w.oct_node,
+                  tsum,      w.groups, group_disk, w.n_nodes, w.n_groups,  w.group_spans};
   k_apply<K><<<mtiles, kMarkTile, 0, s>>>(ap);
-  EmitArgs<K> a{n, disk_bits, n_roots, w.bin_left, w.bin_right, w.bin_lo, w.bin_hi, w.bin_prefix,
-                keys, w.oct_nch, w.oct_off, w.body4, w.mom_ploc, tpre, geoms, w.oct};
+  EmitArgs<K> a{n, disk_bits, n_roots, w.bin_lo, w.bin_hi, w.bin_prefix, keys, w.oct_nch,
+                w.oct_off, w.body4, w.mom_ploc, tpre, geoms, w.oct};
   if (moments_ready && w.moments_on_side) check(cudaStreamWaitEvent(s, w.ev_join, 0), "moment join");
-  k_emit<K><<<grid_for(n - 1), kThreads, 0, s>>>(a);
+  // one thread per record for up to n / 2 records (about 0.35 n with leaves of
+  // eight bodies); the loop covers any more
+  k_emit<K><<<std::max(1, div_up(n, 2 * kThreads)), kThreads, 0, s>>>(
+      a, w.oct_node, w.n_nodes);
   check(cudaGetLastError(), "octree launch");
 }
 
