@@ -152,36 +152,34 @@ k_lookback_probe(const uint32_t* status, int t, int* err, uint32_t* out) {
   out[threadIdx.x] = lookback_prefix(status, t, threadIdx.x, err);
 }
 
-// One pass: rank a tile, publish, look back, scatter.  ticket and status
-// (ntiles x 256 words) start at zero.
+// Shared memory of one tile of a one-sweep pass.
 template <typename K, int kItems>
-__global__ void __launch_bounds__(kSortThreads)
-k_onesweep(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
-           K* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int n, int shift,
-           const uint32_t* __restrict__ digit_count, int* __restrict__ ticket,
-           uint32_t* __restrict__ status, int* __restrict__ err,
-           uint32_t* __restrict__ clear_next) {
-  constexpr int kTile = kSortThreads * kItems;
-  __shared__ uint32_t s_cnt[kSortWarps][kBins];
-  __shared__ K s_keys[kTile];
-  __shared__ uint32_t s_vals[kTile];
-  __shared__ uint32_t s_base[kBins];
-  __shared__ uint32_t s_glob[kBins];
-  __shared__ uint32_t s_wsum[kSortWarps];
-  __shared__ uint32_t s_hsum[kSortWarps];
-  __shared__ int s_tile;
+struct SweepSmem {
+  uint32_t cnt[kSortWarps][kBins];
+  K keys[kSortThreads * kItems];
+  uint32_t vals[kSortThreads * kItems];
+  uint32_t base[kBins];
+  uint32_t glob[kBins];
+  uint32_t wsum[kSortWarps];
+  uint32_t hsum[kSortWarps];
+  int tile;
+};
 
+// One tile t of a pass: rank its keys, publish, look back, scatter.  The
+// caller has zeroed sm.cnt and synchronised; status (ntiles x 256 words)
+// starts at zero.  clear_next: the status words of tile t for the pass after
+// next (double buffering), or null.
+template <typename K, int kItems>
+__device__ __forceinline__ void sweep_tile(SweepSmem<K, kItems>& sm, int t,
+                                           const K* __restrict__ keys_in,
+                                           const uint32_t* __restrict__ vals_in,
+                                           K* __restrict__ keys_out,
+                                           uint32_t* __restrict__ vals_out, int n, int shift,
+                                           const uint32_t* __restrict__ digit_count,
+                                           uint32_t* __restrict__ status, int* __restrict__ err,
+                                           uint32_t* __restrict__ clear_next) {
+  constexpr int kTile = kSortThreads * kItems;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int i = tid; i < kSortWarps * kBins; i += kSortThreads) (&s_cnt[0][0])[i] = 0;
-  // the ticket words were cleared before the sort's first pass
-  if (tid == 0) s_tile = atomicAdd(ticket, 1);
-  // Launched as a programmatic dependent of the previous pass, the tile may
-  // start while that pass still runs: everything below reads or clears what
-  // it writes, so wait for it to finish here, then let the next pass launch.
-  grid_dependency_wait();
-  grid_dependents_launch();
-  __syncthreads();
-  const int t = s_tile;
   // the next pass's status words of this tile (the pass before last used
   // them, and it has finished)
   if (clear_next) clear_next[(size_t)t * kBins + tid] = 0u;
@@ -194,7 +192,7 @@ k_onesweep(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
     const uint32_t q = __shfl_up_sync(kFull, hincl, o);
     if (lane >= o) hincl += q;
   }
-  if (lane == 31) s_hsum[warp] = hincl;  // read after the ranking's barrier
+  if (lane == 31) sm.hsum[warp] = hincl;  // read after the ranking's barrier
 
   const long long tile0 = (long long)t * kTile;
   const long long wbase = tile0 + (long long)warp * (kWarp * kItems);
@@ -217,8 +215,8 @@ k_onesweep(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
     const int leader = __ffs(peers) - 1;
     uint32_t old = 0;
     if (valid && lane == leader) {
-      old = s_cnt[warp][d];
-      s_cnt[warp][d] = old + __popc(peers);
+      old = sm.cnt[warp][d];
+      sm.cnt[warp][d] = old + __popc(peers);
     }
     old = __shfl_sync(kFull, old, leader);
     __syncwarp();
@@ -231,8 +229,8 @@ k_onesweep(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
     uint32_t run = 0;
 #pragma unroll
     for (int w = 0; w < kSortWarps; ++w) {
-      const uint32_t c = s_cnt[w][d];
-      s_cnt[w][d] = run;
+      const uint32_t c = sm.cnt[w][d];
+      sm.cnt[w][d] = run;
       run += c;
     }
     // run = this tile's count of digit d: publish it, then look back
@@ -244,8 +242,8 @@ k_onesweep(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
       atomicExch(mine, kFlagP | ((excl + run) & kValMask));
     }
     uint32_t gbase = hincl - hcount;
-    for (int w = 0; w < warp; ++w) gbase += s_hsum[w];
-    s_glob[d] = gbase + excl;
+    for (int w = 0; w < warp; ++w) gbase += sm.hsum[w];
+    sm.glob[d] = gbase + excl;
     // tile-local base of digit d: exclusive prefix over digits
     uint32_t v = run;
 #pragma unroll
@@ -253,11 +251,11 @@ k_onesweep(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
       const uint32_t q = __shfl_up_sync(kFull, v, o);
       if (lane >= o) v += q;
     }
-    if (lane == 31) s_wsum[warp] = v;
+    if (lane == 31) sm.wsum[warp] = v;
     __syncthreads();
     uint32_t add = 0;
-    for (int w = 0; w < warp; ++w) add += s_wsum[w];
-    s_base[d] = v - run + add;
+    for (int w = 0; w < warp; ++w) add += sm.wsum[w];
+    sm.base[d] = v - run + add;
   }
   __syncthreads();
 
@@ -266,21 +264,45 @@ k_onesweep(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
     const long long idx = wbase + r * kWarp + lane;
     if (idx < n) {
       const uint32_t d = (uint32_t)(k_reg[r] >> shift) & 0xffu;
-      const uint32_t lp = s_base[d] + s_cnt[warp][d] + r_reg[r];
-      s_keys[lp] = k_reg[r];
-      s_vals[lp] = v_reg[r];
+      const uint32_t lp = sm.base[d] + sm.cnt[warp][d] + r_reg[r];
+      sm.keys[lp] = k_reg[r];
+      sm.vals[lp] = v_reg[r];
     }
   }
   __syncthreads();
 
   const int tile_n = (int)min((long long)kTile, (long long)n - tile0);
   for (int i = tid; i < tile_n; i += kSortThreads) {
-    const K key = s_keys[i];
+    const K key = sm.keys[i];
     const uint32_t d = (uint32_t)(key >> shift) & 0xffu;
-    const uint32_t g = s_glob[d] + (uint32_t)i - s_base[d];
+    const uint32_t g = sm.glob[d] + (uint32_t)i - sm.base[d];
     keys_out[g] = key;
-    vals_out[g] = s_vals[i];
+    vals_out[g] = sm.vals[i];
   }
+}
+
+// One pass, one tile per block.  ticket and status (ntiles x 256 words)
+// start at zero.
+template <typename K, int kItems>
+__global__ void __launch_bounds__(kSortThreads)
+k_onesweep(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+           K* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int n, int shift,
+           const uint32_t* __restrict__ digit_count, int* __restrict__ ticket,
+           uint32_t* __restrict__ status, int* __restrict__ err,
+           uint32_t* __restrict__ clear_next) {
+  __shared__ SweepSmem<K, kItems> sm;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < kSortWarps * kBins; i += kSortThreads) (&sm.cnt[0][0])[i] = 0;
+  // the ticket words were cleared before the sort's first pass
+  if (tid == 0) sm.tile = atomicAdd(ticket, 1);
+  // Launched as a programmatic dependent of the previous pass, the tile may
+  // start while that pass still runs: everything below reads or clears what
+  // it writes, so wait for it to finish here, then let the next pass launch.
+  grid_dependency_wait();
+  grid_dependents_launch();
+  __syncthreads();
+  sweep_tile<K, kItems>(sm, sm.tile, keys_in, vals_in, keys_out, vals_out, n, shift,
+                        digit_count, status, err, clear_next);
 }
 
 // ---------------------------------------------------------------- scan
@@ -420,8 +442,8 @@ size_t scan_tmp_words(int n);
 
 // Scratch of the sort: per-pass digit counts (passes x 256), per-pass tile
 // tickets (passes), one word for give-up reports when the caller passes no
-// status word, then the tile status words of one pass (ntiles x 256, cleared
-// before every pass).  Sized for the smallest tiles.
+// status word, then the tile status words of one or two passes (ntiles x 256
+// each).  Sized for the smallest tiles.
 size_t radix_sort_count_words(int n) {
   return (size_t)kMaxPasses * kBins + kMaxPasses + 1 + (size_t)kBins * div_up(n, kMinTile);
 }
@@ -451,6 +473,7 @@ void radix_sort_pairs(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt,
     const int hgrid = std::max(1, std::min(div_up(n, kSortThreads * 8), 148 * 4));
     k_digit_hist<K><<<hgrid, kSortThreads, 0, s>>>(keys, n, passes, hist);
   }
+
   K *ki = keys, *ko = keys_alt;
   uint32_t *vi = vals, *vo = vals_alt;
   // Two status buffers when the scratch holds them (it is sized for the
