@@ -276,10 +276,10 @@ def run_reference(args, ws, rank):
 #   sort    keys: read x (12) + write key, index (8); four 8-bit passes of
 #           key + index read and written (4 x 16)
 #   permute read index (4) + gather x, v, mass, id (32); write x, v, mass, id
-#           (32) + the walk's float4 body (16)
-#   tree    keys (4) + binary topology (16) + body read (16) + node COM and
-#           mass (32)
-PHASE_BYTES_F32 = {"stream": 60, "sort": 84, "permute": 84, "tree": 68}
+#           (32) + the walk's float4 body (16) + the FP64 moment prefix (32)
+#   tree    keys (4) + binary topology (16) + moment prefix read (32) + node
+#           COM and mass (32)
+PHASE_BYTES_F32 = {"stream": 60, "sort": 84, "permute": 116, "tree": 84}
 
 
 def hbm_peak():
