@@ -38,9 +38,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 METRIC = "particle-steps/s at N=1M theta=0.5"
 UNIT = "particle-steps/s"
 WORKLOAD = dict(n=1 << 20, r_min=0.3, r_max=30.0, m=1e-9, eps=5e-4, theta=0.5, dt=0.002)
-# interactions of the walk, per accepted source-target pair (survey 8d):
-# 3 sub, 3 FMA as 2 each for r^2+eps^2, rsqrt as 1, 3 mul, 3 FMA as 2 each
-FLOP_PER_INTERACTION = 20
+# FLOP of the walk per accepted source-target interaction, as the kernel
+# computes it: 3 sub (d = s - p), 3 FMA as 2 each (r^2 + eps^2), rsqrt as 1,
+# 3 mul (inv^3 and m inv^3), 3 FMA as 2 each (the three accumulations) = 19
+FLOP_PER_INTERACTION = 19
 
 
 def parse():
