@@ -102,6 +102,29 @@ def test_ensemble_matches_separate_runs(nb, cuda, precision):
         off += spec["n"]
 
 
+TINY = [{"n": 2, "seed": 5}, {"n": 3, "seed": 6}, {"n": 2, "seed": 7},
+        {"n": 700, "seed": 8}, {"n": 3, "seed": 9}]
+
+
+def test_ensemble_with_disks_of_two_or_three_bodies(nb, cuda):
+    """The smallest disks an ensemble takes (two bodies each at least): their
+    roots sit right under binary nodes that span several disks and have only
+    leaves below them; each disk still matches the same disk run on its own."""
+    prm = params(nb, 1)
+    steps = 4
+    e0, e1, stats, _ = ensemble(nb, prm, TINY, steps)
+    assert stats.status == 0
+    off = 0
+    for spec in TINY:
+        s0, s1 = separate(nb, prm, spec, steps)
+        sl = slice(off, off + spec["n"])
+        a0 = {k: v[sl] for k, v in e0.items()}
+        assert np.max(rel_acc_err(s0, a0)) < 1e-5, spec
+        for k in ("x", "y", "z"):
+            assert np.max(np.abs(e1[k][sl] - s1[k])) < 1e-7, (spec, k)
+        off += spec["n"]
+
+
 def test_ensemble_graphs_equal_plain_launches(nb, cuda):
     prm = params(nb, 1)
     _, g, sg, _ = ensemble(nb, prm, SPECS, 5, graphs=True)
