@@ -242,6 +242,62 @@ def cpu_port_step(st, n, nthreads=0, steps=1):
         port.set_summarize_passes(0)
 
 
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_study(nb, st, n, all_core_step_secs):
+    """The reference's CPU path on the host cores beside the GPU: one step of
+    the CPU restatement (oracle/port.c) on one core and on all cores at the
+    C1 and C2 sizes and at N (one core: one step), and the reference's own
+    detectAggregates (Aggregate.cpp, one core, O(N^2)) at C1 and C2 sizes with
+    their collision radii as linking lengths, beside the engine's GPU FoF on
+    the same bodies."""
+    import torch
+    cores = os.cpu_count() or 1
+    out = {"cores": cores, "cpu": cpu_model(), "port_step_s": {}, "detect_aggregates_s": {},
+           "gpu_fof_s": {}}
+    for size in (4096, 131072):
+        out["port_step_s"][str(size)] = {"1": cpu_port_step(st, size, 1, 1),
+                                         "all": cpu_port_step(st, size, 0, 1)}
+    out["port_step_s"][str(n)] = {"1": cpu_port_step(st, n, 1, 1), "all": all_core_step_secs}
+    ref = os.path.join(ROOT, "oracle", "_ref", "libref_host.so")
+    rh = None
+    if os.path.exists(ref):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        rh = oracle.RefHost(ref)
+    # C1: factor 1 at m = 1e-8; C2: factor 5 (the reference's collision radius)
+    r1 = nb.particle_physical_radius(1e-8)
+    for size, link in ((4096, r1), (131072, 5.0 * r1)):
+        xs = [np.ascontiguousarray(st[k][:size], np.float32) for k in ("x", "y", "z")]
+        key = str(size)
+        if rh is not None:
+            t0 = time.perf_counter()
+            rh.detect_aggregates_count(*xs, float(link))
+            out["detect_aggregates_s"][key] = time.perf_counter() - t0
+        tree = nb.Octree(size)
+        dev = [torch.from_numpy(a).cuda() for a in xs]
+        tree.fof(*dev, float(link))  # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        tree.fof(*dev, float(link))
+        torch.cuda.synchronize()
+        out["gpu_fof_s"][key] = time.perf_counter() - t0
+        tree.close()
+    out["sample"] = ("bodies 0..size-1 of the headline disk; one step (or one FoF call) each, "
+                     "after one untimed forces pass; GPU FoF is the stand-alone nbody_fof, host "
+                     "wall time of one call")
+    return out
+
+
 def run_reference(args, ws, rank):
     """The reference's CPU path (its host build of the force and integrator
     formulas, oracle/port.c) on all host cores; rank 0 only."""
@@ -521,6 +577,11 @@ def run_ours(args, ws, rank, local):
         line["cpu_baseline"] = {"value": n / secs, "unit": UNIT, "cores": cores, "kind": "port",
                                 "sample": f"1 full step at N={n} of the reference algorithm "
                                           f"(oracle/port.c: {CPU_STEP}), OpenMP"}
+        if not args.no_studies and prec == nb.STATE_F32:
+            try:
+                line["cpu_study"] = cpu_study(nb, st, n, secs)
+            except Exception as e:  # noqa: BLE001 -- recorded in the line
+                line["cpu_study"] = {"error": f"{type(e).__name__}: {e}"}
     sim.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
