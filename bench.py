@@ -559,7 +559,9 @@ def run_ours(args, ws, rank, local):
         def adjoint():
             adj = adjoint_study(args, args.adjoint_fd)
             fdc = {k: v for k, v in adj["fd_check"].items() if k != "misses_at_h1e-6"}
-            fdc["misses_at_h1e-6"] = len(adj["fd_check"]["misses_at_h1e-6"])
+            # each miss at h = 1e-6 with its error at 1e-5 and 1e-4: how the
+            # quotient's error moves with h says whether round-off limits it
+            fdc["misses_at_h1e-6"] = adj["fd_check"]["misses_at_h1e-6"][:10]
             return {"gradient_over_plain_forward": adj["ms"]["gradient_over_plain_forward"],
                     "ms": adj["ms"], "memory_bytes": adj["memory_bytes"],
                     "checkpointed": adj["checkpointed"],
