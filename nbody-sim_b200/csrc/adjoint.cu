@@ -843,12 +843,28 @@ struct AdjointImpl {
   std::vector<uint32_t*> perm;
   std::vector<int2*> groups, gtape;
   int* ngroups = nullptr;  // per level slot, device
-  int2* pool[2] = {nullptr, nullptr};
-  int* pool_next[2] = {nullptr, nullptr};
+  // Checkpoint mode holds three levels at a time (and a tape pool each): the
+  // backward re-records level L-1 while it differentiates level L, and
+  // level L+1's slot may still be in use then.
+  static constexpr int kCkSlots = 3;
+  int2* pool[kCkSlots] = {nullptr, nullptr, nullptr};
+  int* pool_next[kCkSlots] = {nullptr, nullptr, nullptr};
   int* pool_used = nullptr;  // device, one counter per pool
   int pool_cap = 0;          // chunks per pool
   // scratch
-  double *xs = nullptr, *ys = nullptr, *zs = nullptr;
+  double *xs = nullptr, *ys = nullptr, *zs = nullptr;  // sorted positions of the tree builds
+  // A level's bodies for the replays and the force adjoints (level_bodies):
+  // sorted FP64 positions (lev_x..z), float bodies and their moment prefix
+  // (tv holds body4, mom_ploc and mom_tiles only), apart from the tree
+  // builds' own so that a backward can rebuild one level while it
+  // differentiates another.
+  double *lev_x = nullptr, *lev_y = nullptr, *lev_z = nullptr;
+  TreeWork tv;
+  int* work_b = nullptr;  // the replays' group counter
+  // checkpoint-mode backward: the rebuilds of earlier levels run on rev_st
+  // beside the differentiation on the engine stream, ordered by these events
+  cudaStream_t rev_st = nullptr;
+  std::vector<cudaEvent_t> bwd_events;
   double *vw = nullptr, *xw = nullptr;      // work velocity (3n) and positions (2 x 3n)
   float* aw = nullptr;                       // work self-gravity (3n)
   double* aw64 = nullptr;                    // FP64 replay self-gravity (3n)
@@ -882,8 +898,9 @@ struct AdjointImpl {
   double* rep_final[2] = {nullptr, nullptr};  // buffer holding a replay's final positions
   cudaStream_t cap_st = nullptr;
 
-  int slot(int L) const { return mode == kModeCheckpoint ? (L & 1) : L; }
-  int pidx(int L) const { return mode == kModeCheckpoint ? (L & 1) : 0; }
+  int slot(int L) const { return mode == kModeCheckpoint ? (L % kCkSlots) : L; }
+  int pidx(int L) const { return mode == kModeCheckpoint ? (L % kCkSlots) : 0; }
+  int n_pools() const { return mode == kModeCheckpoint ? kCkSlots : (mode == kModeTape ? 1 : 0); }
 
   AdjointImpl(const nbody_sim_params& prm, int nn, int nsteps, int md, int ck_every) {
     p = prm;
@@ -899,7 +916,7 @@ struct AdjointImpl {
     // slowed the build (N = 2^20: 115 us against 88 us in one stream)
     tw.group_max = 32;
     const size_t n3 = 3 * (size_t)n;
-    const int nslot = (mode == kModeCheckpoint) ? 2 : steps + 1;
+    const int nslot = (mode == kModeCheckpoint) ? kCkSlots : steps + 1;
     for (int L = 0; L < nslot; ++L) {
       X.push_back(dalloc<double>(n3, "level positions"));
       V.push_back(dalloc<double>(n3, "level velocities"));
@@ -918,6 +935,12 @@ struct AdjointImpl {
     }
     ngroups = dalloc<int>(nslot, "level group counts");
     xs = dalloc<double>(n, "sorted x"); ys = dalloc<double>(n, "sorted y");
+    lev_x = dalloc<double>(n, "level sorted x"); lev_y = dalloc<double>(n, "level sorted y");
+    lev_z = dalloc<double>(n, "level sorted z");
+    tv.body4 = dalloc<float4>(n, "level bodies");
+    tv.mom_ploc = dalloc<double4>(n + 1, "level moment prefix");
+    tv.mom_tiles = dalloc<double4>(2 * (moment_tiles(n) + 1), "level moment tiles");
+    work_b = dalloc<int>(1, "replay work");
     zs = dalloc<double>(n, "sorted z");
     vw = dalloc<double>(n3, "work velocity");
     xw = dalloc<double>(2 * n3, "work positions");
@@ -934,7 +957,7 @@ struct AdjointImpl {
     spill = dalloc<int>((size_t)walk_spill_slots(0) * spill_cap, "walk spill");
     work = dalloc<int>(1, "work");
     inter = dalloc<unsigned long long>(1, "interactions");
-    pool_used = dalloc<int>(2, "tape chunks used");
+    pool_used = dalloc<int>(kCkSlots, "tape chunks used");
     aw64 = dalloc<double>(n3, "FP64 replay self-gravity");
     pert_fwd = dalloc<double4>(steps + 1, "perturber per level");
     pert_rep = dalloc<double4>(steps + 1, "replay perturber per level");
@@ -962,12 +985,16 @@ struct AdjointImpl {
     for (auto* q : perm) cudaFree(q);
     for (auto* q : groups) cudaFree(q);
     for (auto* q : gtape) cudaFree(q);
-    void* ptrs[] = {ngroups, pool[0], pool[1], pool_next[0], pool_next[1], pool_used, xs, ys, zs,
-                    vw, xw, aw, aw64, gx, gv, lam, mu, radd, rploc, rtiles, pgrad, mass, spill,
-                    work, inter, pert_fwd, pert_rep, vh};
+    void* ptrs[] = {ngroups, pool[0], pool[1], pool[2], pool_next[0], pool_next[1], pool_next[2],
+                    pool_used, xs, ys, zs, lev_x, lev_y, lev_z, work_b, vw, xw, aw, aw64, gx, gv, lam, mu,
+                    radd, rploc, rtiles, pgrad, mass, spill, work, inter, pert_fwd, pert_rep, vh};
     for (void* q : ptrs)
       if (q) cudaFree(q);
+    for (cudaEvent_t e : bwd_events)
+      cudaEventDestroy(e);
+    if (rev_st) cudaStreamDestroy(rev_st);
     tree_free(tw);
+    tree_free(tv);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     if (own_stream && st) cudaStreamDestroy(st);
@@ -1109,7 +1136,7 @@ struct AdjointImpl {
     if (chunks <= pool_cap) return;
     check(cudaStreamSynchronize(st), "tape pool sync");
     drop_graphs();  // the captured runs hold the old pool
-    const int npools = (mode == kModeCheckpoint) ? 2 : 1;
+    const int npools = n_pools();
     pool_cap = chunks;
     for (int k = 0; k < npools; ++k) {
       if (pool[k]) cudaFree(pool[k]);
@@ -1142,7 +1169,7 @@ struct AdjointImpl {
       if (pool_cap == 0) ensure_pool(std::max(1024, n / 32 * 24));
       for (int attempt = 0; attempt < 4; ++attempt) {
         check(cudaMemsetAsync(tw.status, 0, sizeof(int), st), "status reset");
-        check(cudaMemsetAsync(pool_used, 0, 2 * sizeof(int), st), "tape reset");
+        check(cudaMemsetAsync(pool_used, 0, kCkSlots * sizeof(int), st), "tape reset");
         record_level(0);
         int used = 0;
         check(cudaStreamSynchronize(st), "adjoint sync");
@@ -1168,9 +1195,10 @@ struct AdjointImpl {
       check(cudaEventRecord(e1, st), "event");
       const int s = read_status();
       if (s & kStatusTapeFull) {
-        int used[2] = {0, 0};
-        check(cudaMemcpy(used, pool_used, 2 * sizeof(int), cudaMemcpyDeviceToHost), "tape used");
-        const int u = std::max(used[0], used[1]);
+        int used[kCkSlots] = {0, 0, 0};
+        check(cudaMemcpy(used, pool_used, kCkSlots * sizeof(int), cudaMemcpyDeviceToHost),
+              "tape used");
+        const int u = std::max(used[0], std::max(used[1], used[2]));
         ensure_pool((int)std::min<long long>((long long)u * 3 / 2 + 1024,
                                              0x7fffffffLL / kTapeChunk));
         continue;
@@ -1190,7 +1218,7 @@ struct AdjointImpl {
   // mode sums the self-gravity pair by pair in FP64.
   void forward_levels() {
     check(cudaMemsetAsync(tw.status, 0, sizeof(int), st), "status reset");
-    check(cudaMemsetAsync(pool_used, 0, 2 * sizeof(int), st), "tape reset");
+    check(cudaMemsetAsync(pool_used, 0, kCkSlots * sizeof(int), st), "tape reset");
     const size_t n3 = 3 * (size_t)n;
     if (mode == kModeDirect) {
       const double eps2 = (double)p.softening * (double)p.softening;
@@ -1224,16 +1252,16 @@ struct AdjointImpl {
   void level_bodies(int L, const double* x) {
     const size_t n1 = n, n2 = 2 * (size_t)n;
     k_gather_sorted<<<grid1(n), kThreads, 0, st>>>(perm[slot(L)], x, x + n1, x + n2, mass, n,
-                                                   xs, ys, zs, tw.body4);
-    launch_moment_prefix(tw, n, xs, ys, zs, st);
+                                                   lev_x, lev_y, lev_z, tv.body4);
+    launch_moment_prefix(tv, n, lev_x, lev_y, lev_z, st);
     launches += 3;
   }
 
   ReplayArgs replay_args(int L) {
     ReplayArgs r{};
-    r.body4 = tw.body4;
-    r.ploc = tw.mom_ploc;
-    r.tpre = moment_tile_prefix(tw, n);
+    r.body4 = tv.body4;
+    r.ploc = tv.mom_ploc;
+    r.tpre = moment_tile_prefix(tv, n);
     const int sl = slot(L);
     r.perm = perm[sl];
     r.groups = groups[sl];
@@ -1242,13 +1270,13 @@ struct AdjointImpl {
     r.tape = pool[pidx(L)];
     r.tape_next = pool_next[pidx(L)];
     r.eps2 = p.softening * p.softening;
-    r.work = work;
+    r.work = work_b;
     r.status = tw.status;
     return r;
   }
 
   void launch_replay(const ReplayArgs& r, bool adj, bool fp64 = false) {
-    check(cudaMemsetAsync(work, 0, sizeof(int), st), "replay work reset");
+    check(cudaMemsetAsync(r.work, 0, sizeof(int), st), "replay work reset");
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -1305,7 +1333,7 @@ struct AdjointImpl {
         ReplayArgs r = replay_args(L);
         if (fp64) {
           r.dax = aw64; r.day = aw64 + n; r.daz = aw64 + 2 * (size_t)n;
-          r.xs = xs; r.ys = ys; r.zs = zs;
+          r.xs = lev_x; r.ys = lev_y; r.zs = lev_z;
           launch_replay(r, false, true);
           launch_step(end, begin, step_args<double>(xa, vw, aw64, nullptr, begin ? xb : nullptr,
                                                     pert_rep, L));
@@ -1351,7 +1379,7 @@ struct AdjointImpl {
     k_prefix4_tiles<<<ntiles, kThreads, 0, st>>>(radd, n + 1, rploc, rtiles);
     k_tiles_scan4<<<1, 32, 0, st>>>(rtiles, ntiles, tpre);
     ApplyArgs a = apply_args(L);
-    a.perm = perm[sl]; a.body4 = tw.body4;
+    a.perm = perm[sl]; a.body4 = tv.body4;
     a.rploc = rploc; a.rtpre = tpre;
     if (step) k_adj_apply<true><<<grid1(n), kThreads, 0, st>>>(a);
     else k_adj_apply<false><<<grid1(n), kThreads, 0, st>>>(a);
@@ -1453,12 +1481,35 @@ struct AdjointImpl {
   // (k_dstep_rev), its tree and tape re-recorded (which also gives its
   // self-gravity, so the first kick is undone too, k_kick_rev); a level that
   // holds a checkpoint is copied back exactly instead.
+  // The rebuilds form one chain R(L) (level L-1 from level L) on rev_st, the
+  // differentiation another, D(L) (the drag and second-kick adjoints of step
+  // L-1, then the force adjoint at level L), on the engine stream.  D(L)
+  // waits for R(L); R(L) writes the slot and tape pool of level L-1, which
+  // with three of each is level L+2's, so it waits for D(L+2) and runs beside
+  // D(L+1).  The two chains use disjoint buffers (tw and xs..zs for the
+  // rebuilds; tv, lev_x..z and work_b for the adjoints); the order of every
+  // computation is that of the serial loop, so the gradients are the same.
   void backward_levels_reversed() {
     const size_t n3 = 3 * (size_t)n;
     const double dth = (double)p.dt * 0.5;
+    if (!rev_st) check(cudaStreamCreateWithFlags(&rev_st, cudaStreamNonBlocking), "rebuild stream");
+    if (bwd_events.empty()) {
+      bwd_events.resize(2 * (size_t)(steps + 2) + 1);
+      for (cudaEvent_t& e : bwd_events)
+        check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "backward event");
+    }
+    cudaEvent_t* evR = bwd_events.data();              // R(L) done, L = 1..steps
+    cudaEvent_t* evD = bwd_events.data() + steps + 2;  // D(L) done, L = 1..steps
+    cudaEvent_t fork = bwd_events.back();
+    cudaStream_t dst = st;
+    check(cudaEventRecord(fork, dst), "backward fork");
+    check(cudaStreamWaitEvent(rev_st, fork, 0), "backward fork");
     for (int L = steps; L >= 1; --L) {
       const int Lm = L - 1, s = slot(L), sm = slot(Lm);
       const bool ck = (Lm % every) == 0;
+      // R(L) on the rebuild stream
+      if (L + 2 <= steps) check(cudaStreamWaitEvent(rev_st, evD[L + 2], 0), "slot reuse");
+      st = rev_st;
       if (ck) {
         const double* c = CK[Lm / every];
         check(cudaMemcpyAsync(X[sm], c, sizeof(double) * n3, cudaMemcpyDeviceToDevice, st),
@@ -1486,10 +1537,15 @@ struct AdjointImpl {
         check(cudaGetLastError(), "k_kick_rev launch");
         launches += 1;
       }
+      check(cudaEventRecord(evR[L], st), "rebuild done");
+      // D(L) on the engine stream
+      st = dst;
+      check(cudaStreamWaitEvent(st, evR[L], 0), "rebuild wait");
       drag_adjoint<float>(Lm, A[sm], A[s]);
       force_adjoint(L, true);
+      check(cudaEventRecord(evD[L], st), "adjoint done");
     }
-    force_adjoint(0, false);
+    force_adjoint(0, false);  // R(1), the last rebuild, was waited for by D(1)
   }
 
   void finish_backward(double* const* g_init, double* g_par) {
@@ -1530,7 +1586,7 @@ struct AdjointImpl {
   // pools and per-level permutation and groups) and the level states
   // (checkpoints included).
   size_t tape_bytes() const {
-    const size_t pools = (mode == kModeCheckpoint) ? 2 : (mode == kModeTape ? 1 : 0);
+    const size_t pools = n_pools();
     return pools * (size_t)pool_cap * (kTapeChunk * sizeof(int2) + sizeof(int)) +
            perm.size() * n * (sizeof(uint32_t) + 2 * sizeof(int2));
   }
