@@ -103,6 +103,14 @@ __device__ __forceinline__ int warp_incl_scan(int v, int lane) {
   }
   return v;
 }
+__device__ __forceinline__ unsigned warp_incl_scan(unsigned v, int lane) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned t = __shfl_up_sync(kFull, v, o);
+    if (lane >= o) v += t;
+  }
+  return v;
+}
 __device__ __forceinline__ unsigned lanemask_lt() {
   unsigned m;
   asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));

@@ -682,10 +682,26 @@ __global__ void __launch_bounds__(kWalkWarps * 32, walk_min_blocks<kMode>())
         nlist -= 32;
       }
 
-      // opened nodes -> children on the stack
+      // Opened nodes -> children on the stack, leaves -> their bodies into
+      // the list.  One scan counts both: children (<= 8 a lane, <= 256 a
+      // pop) in the top 9 bits, bodies in the low 23; a leaf of >= 2^18
+      // bodies (that many on one key) takes a scan of its own.
       const int pc = (act == 3) ? cnt : 0;
-      const int pincl = warp_incl_scan(pc, lane);
-      const int ptotal = __shfl_sync(kFull, pincl, 31);
+      const int bc = (act == 2) ? cnt : 0;
+      int pincl, bincl, ptotal, btotal;
+      if (__any_sync(kFull, bc >= (1 << 18))) {
+        pincl = warp_incl_scan(pc, lane);
+        bincl = warp_incl_scan(bc, lane);
+        ptotal = __shfl_sync(kFull, pincl, 31);
+        btotal = __shfl_sync(kFull, bincl, 31);
+      } else {
+        const unsigned incl = warp_incl_scan(((unsigned)pc << 23) | (unsigned)bc, lane);
+        const unsigned tot = __shfl_sync(kFull, incl, 31);
+        pincl = (int)(incl >> 23);
+        bincl = (int)(incl & 0x7fffffu);
+        ptotal = (int)(tot >> 23);
+        btotal = (int)(tot & 0x7fffffu);
+      }
       if (ptotal > 0) {
         if (top + ptotal > kStk) {
           if (spilled + top > a.spill_cap) { overflow = true; break; }
@@ -696,15 +712,14 @@ __global__ void __launch_bounds__(kWalkWarps * 32, walk_min_blocks<kMode>())
           __syncwarp();
         }
         const int base = top + pincl - pc;
-        for (int k = 0; k < pc; ++k) w.stk[base + k] = first + k;
+#pragma unroll
+        for (int k = 0; k < 8; ++k)  // a node has at most 8 children
+          if (k < pc) w.stk[base + k] = first + k;
         top += ptotal;
         __syncwarp();
       }
 
       // leaves to open -> their bodies into the list, 32 at a time
-      const int bc = (act == 2) ? cnt : 0;
-      const int bincl = warp_incl_scan(bc, lane);
-      const int btotal = __shfl_sync(kFull, bincl, 31);
       if (btotal > 0) {
         w.sc[lane] = bincl;
         w.slo[lane] = first;
