@@ -61,6 +61,9 @@ def parse():
                          "(nbody_sim_params.group_span)")
     ap.add_argument("--span-walk", type=int, default=None, choices=[0, 1, 2],
                     help="shared walk (nbody_sim_params.span_walk); default: the engine's")
+    ap.add_argument("--targets-per-lane", type=int, default=None, choices=[1, 2],
+                    help="walk targets per lane, groups of 32 or 64 "
+                         "(nbody_sim_params.targets_per_lane); default: the engine's")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-studies", action="store_true",
@@ -414,6 +417,8 @@ def run_ours(args, ws, rank, local):
         prm.group_span = args.group_span
     if args.span_walk is not None:
         prm.span_walk = args.span_walk
+    if args.targets_per_lane is not None:
+        prm.targets_per_lane = args.targets_per_lane
     stream = torch.cuda.current_stream()
     sim = nb.Sim(prm, n)
     sim.set_stream(stream.cuda_stream)
