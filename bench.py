@@ -53,7 +53,8 @@ def parse():
     ap.add_argument("--n", type=int, default=WORKLOAD["n"])
     ap.add_argument("--theta", type=float, default=WORKLOAD["theta"])
     ap.add_argument("--precision", choices=["f32", "f64"], default="f32")
-    ap.add_argument("--leaf-max", type=int, default=8)
+    ap.add_argument("--leaf-max", type=int, default=0,
+                    help="walk leaf size (nbody_sim_params.leaf_max); 0: the engine's default")
     ap.add_argument("--walk-mode", type=int, default=None, choices=[0, 1, 2],
                     help="force-walk variant (nbody_sim_params.walk_mode); default: the engine's")
     ap.add_argument("--group-span", type=int, default=None,
@@ -508,7 +509,7 @@ def run_ours(args, ws, rank, local):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": workload_name(n, args.theta, args.precision), "n": n,
                    "theta": args.theta,
-                   "state": args.precision, "leaf_max": args.leaf_max,
+                   "state": args.precision, "leaf_max": stats.leaf_max,
                    "parallelism": f"replicas x{ws}",
                    "l2": "flushed (256 MB write) before every timed step"},
         "gpu_launches": int(launches),
@@ -773,7 +774,8 @@ def run_precision(args, ws, rank, local):
         "study": "precision", "n": n, "targets": len(targets), "data": "synthetic",
         "config": {"workload": f"Keplerian disk N={n} r=[0.3,30] AU m=1e-9 eps=5e-4 dt=0.002, "
                                "gravity only", "drift_steps": args.drift_steps,
-                   "drift_theta": 0.5, "leaf_max": args.leaf_max},
+                   "drift_theta": 0.5,
+                   "leaf_max": args.leaf_max or "engine default (12 from 2^19 bodies, else 8)"},
         "force_error_vs_fp64_direct": forces, "drift": drift,
     }
     print(json.dumps(line), flush=True)

@@ -299,7 +299,8 @@ typedef struct nbody_sim_params {
   float perturber_radius_au;
   float perturber_phase0;
   int state_precision;       /* NBODY_STATE_*                              */
-  int leaf_max;              /* <= 0: default (8)                          */
+  int leaf_max;              /* <= 0: default (12 from 2^19 bodies, else 8;
+                                an ensemble: 8)                             */
   int targets_per_lane;      /* walk: 1 (groups <= 32) or 2 (<= 64); 0: 1  */
   int walk_mode;             /* walk kernel variant (1 target per lane):
                                 0 acceptance vote, 96 registers; 1

@@ -636,7 +636,7 @@ def sim_params(cfg: nbody_config | None = None, **kw) -> nbody_sim_params:
     if cfg is not None:
         lib.nbody_sim_params_from_config(C.byref(cfg), C.byref(p))
     else:
-        p.dt, p.theta, p.softening, p.star_mass, p.leaf_max = 0.01, 0.5, 0.01, 1.0, 8
+        p.dt, p.theta, p.softening, p.star_mass, p.leaf_max = 0.01, 0.5, 0.01, 1.0, 0
         p.targets_per_lane = 1
         p.walk_mode = WALK_MODE_DEFAULT
         p.group_span = GROUP_SPAN_DEFAULT

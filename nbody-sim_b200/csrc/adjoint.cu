@@ -908,7 +908,7 @@ struct AdjointImpl {
     steps = nsteps;
     mode = md;
     every = ck_every;
-    if (p.leaf_max <= 0) p.leaf_max = 8;
+    if (p.leaf_max <= 0) p.leaf_max = kLeafMaxSmall;
     check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "adjoint stream");
     own_stream = true;
     tree_alloc(tw, n);

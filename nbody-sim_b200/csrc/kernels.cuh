@@ -195,6 +195,15 @@ constexpr int kDefaultWalkMode = 1;
 // span 1 there.
 constexpr int kDefaultGroupSpan = 8;
 constexpr int kGroupSpanMinBodies = 1 << 19;
+// Default leaf size (bodies a walk takes directly instead of opening the
+// node): 12 from 2^19 bodies on (the step at N = 2^20 takes 0.602 ms against
+// 0.608 ms with 8: fewer nodes to build and visit outweigh 3% more
+// interactions), else 8.
+constexpr int kLeafMaxLarge = 12;
+constexpr int kLeafMaxSmall = 8;
+inline int default_leaf_max(int n) {
+  return n >= kGroupSpanMinBodies ? kLeafMaxLarge : kLeafMaxSmall;
+}
 
 struct WalkArgs {
   const float4* com;

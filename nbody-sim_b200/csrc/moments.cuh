@@ -33,6 +33,7 @@ __device__ __forceinline__ double4 range_moments(const double4* __restrict__ plo
 // holding two consecutive bodies each.
 constexpr int kMomentThreads = 1024;
 static_assert(kMomentTile == 2 * kMomentThreads, "two bodies per thread");
+static_assert(kMomentThreads % 32 == 0 && kMomentThreads <= 1024, "one warp scans the warp sums");
 
 __device__ __forceinline__ double4 d4shfl_up(double4 v, int o) {
   return make_double4(__shfl_up_sync(0xffffffffu, v.x, o), __shfl_up_sync(0xffffffffu, v.y, o),
@@ -66,11 +67,12 @@ __device__ __forceinline__ void moment_tile_scan(double4 v0, double4 v1, long lo
   const double4 inc = d4warp_incl_scan(sum, lane);
   if (lane == 31) s_w[warp] = inc;
   __syncthreads();
-  if (warp == 0) {  // exclusive prefix of the warp sums
-    const double4 x = s_w[lane];
+  if (warp == 0) {  // exclusive prefix of the warp sums (kMomentThreads / 32 <= 32 of them)
+    constexpr int kWarps = kMomentThreads / 32;
+    const double4 x = (lane < kWarps) ? s_w[lane] : make_double4(0, 0, 0, 0);
     const double4 y = d4warp_incl_scan(x, lane);
     __syncwarp();
-    s_w[lane] = d4sub(y, x);
+    if (lane < kWarps) s_w[lane] = d4sub(y, x);
   }
   __syncthreads();
   double4 run = d4add(s_w[warp], d4sub(inc, sum));

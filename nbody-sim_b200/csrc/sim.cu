@@ -700,7 +700,7 @@ struct SimImpl : SimBase {
   SimImpl(const nbody_sim_params& prm, int nn) {
     p = prm;
     n = nn;
-    if (p.leaf_max <= 0) p.leaf_max = 8;
+    if (p.leaf_max <= 0) p.leaf_max = default_leaf_max(n);
     if (p.targets_per_lane != 2) p.targets_per_lane = 1;
     if (p.walk_mode < 0 || p.walk_mode > 2) p.walk_mode = kDefaultWalkMode;
     if (p.group_span <= 0) p.group_span = (n >= kGroupSpanMinBodies) ? kDefaultGroupSpan : 1;
@@ -1147,7 +1147,7 @@ void nbody_sim_params_from_config(const nbody_config* cfg, nbody_sim_params* out
   out->perturber_radius_au = cfg->perturber_radius_AU;
   out->perturber_phase0 = cfg->perturber_phase0;
   out->state_precision = NBODY_STATE_F32;
-  out->leaf_max = 8;
+  out->leaf_max = 0;  // by the body count
   out->targets_per_lane = 1;
   out->walk_mode = nb::kDefaultWalkMode;
   out->group_span = 0;
@@ -1463,7 +1463,7 @@ struct EnsembleImpl : EnsembleBase {
 
   EnsembleImpl(const nbody_sim_params& prm, const nbody_disk_spec* disks, int nd) {
     p = prm;
-    if (p.leaf_max <= 0) p.leaf_max = 8;
+    if (p.leaf_max <= 0) p.leaf_max = kLeafMaxSmall;
     if (p.targets_per_lane != 2) p.targets_per_lane = 1;
     if (p.walk_mode < 0 || p.walk_mode > 2) p.walk_mode = kDefaultWalkMode;
     if (p.group_span <= 0) p.group_span = 1;  // small compact disks: keep every group
