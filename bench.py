@@ -30,6 +30,7 @@ import os
 import statistics
 import subprocess
 import sys
+import threading
 import time
 
 import numpy as np
@@ -146,14 +147,34 @@ def make_ic_oracle(n, seed):
 
 
 class Clocks:
-    """nvidia-smi samples (200 ms) of the GPU during the timed region."""
+    """SM clock and clock-event reasons sampled during the timed region: NVML
+    read every 5 ms from a thread (the region lasts ~0.1-1 s), else
+    nvidia-smi at its 200 ms rate.  Reads only; nothing is set."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clocks-event reason bits
+    REASONS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+               "hw_thermal_slowdown": 0x40}
 
     def __init__(self, index: int):
         self.p = None
+        self.samples = []
+        self.smax = None
+        self.thread = None
+        self.stop_ev = threading.Event()
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            self.h = self._handle(pynvml, index)
+            self.smax = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.thread = None
         try:
             self.p = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
@@ -162,7 +183,39 @@ class Clocks:
         except (OSError, ValueError):
             self.p = None
 
+    @staticmethod
+    def _handle(pynvml, index: int):
+        """The NVML handle of CUDA device `index`, matched by PCI bus id (NVML
+        numbers every GPU of the machine, CUDA only the visible ones)."""
+        try:
+            pr = torch.cuda.get_device_properties(index)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            return pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml.nvmlDeviceGetHandleByIndex(index)
+
+    def _poll(self):
+        nv = self.nvml
+        while not self.stop_ev.is_set():
+            try:
+                sm = float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                rs = int(nv.nvmlDeviceGetCurrentClocksEventReasons(self.h))
+                self.samples.append((sm, rs))
+            except Exception:
+                return
+            self.stop_ev.wait(0.005)
+
     def stop(self):
+        if self.thread is not None:
+            self.stop_ev.set()
+            self.thread.join(timeout=5)
+            if not self.samples:
+                return None
+            reasons = sorted({nm for _, rs in self.samples for nm, bit in self.REASONS.items()
+                              if rs & bit})
+            return {"sm_mhz": statistics.median(sm for sm, _ in self.samples),
+                    "sm_max_mhz": self.smax, "reasons": reasons, "samples": len(self.samples),
+                    "source": "NVML, 5 ms"}
         if self.p is None:
             return None
         time.sleep(0.25)
@@ -189,7 +242,7 @@ class Clocks:
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi, 200 ms"}
 
 
 def fp32_peak(smax_mhz: float | None):
