@@ -88,6 +88,10 @@ struct TreeWork {
   // Host-side flag: the moment prefix of the octree build in flight runs on
   // `side` (joined through ev_join before the records are written).
   bool moments_on_side = false;
+  // the emit pass writes the records' boxes (oct.box_lo / box_hi): the
+  // neighbour search and the fused-collision walk read them, the plain walk
+  // does not
+  bool boxes = true;
 };
 
 void tree_alloc(TreeWork& w, int cap);

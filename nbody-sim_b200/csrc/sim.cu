@@ -817,6 +817,7 @@ struct SimImpl : SimBase {
     cur = 1 - cur;
     mark(NBODY_PHASE_TREE);
     tw.prune_max = p.leaf_max;
+    tw.boxes = p.r_coll > 0.f;  // only the collision searches read the records' boxes
     const bool span = span_on();
     if (span) span_alloc();
     tw.group_spans = span ? group_spans : nullptr;
@@ -1660,6 +1661,7 @@ struct EnsembleImpl : EnsembleBase {
           "position event");
     cur = 1 - cur;
     tw.prune_max = p.leaf_max;
+    tw.boxes = p.r_coll > 0.f;  // only the collision searches read the records' boxes
     if (kIsF64<R>)
       launch_tree<uint64_t>(tw, keys64, n, key_bits, disk_bits, D, geoms, group_disk,
                             (const double*)s[cur].v[0], (const double*)s[cur].v[1],

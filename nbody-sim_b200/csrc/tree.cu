@@ -639,6 +639,7 @@ struct EmitArgs {
   const double4* tpre;
   const TreeGeom* geom;
   OctNodes oct;
+  bool boxes;  // also the records' boxes (the neighbour search reads them)
 };
 
 // Writes the octree record of binary node c into slot f.
@@ -653,8 +654,10 @@ __device__ void write_node(const EmitArgs<K>& a, int c, int f) {
     const float4 p = a.body4[j];
     a.oct.com[f] = p;
     a.oct.info[f] = make_int4(-1, j, (1 << 4), __float_as_int(ldexpf(rhs, -10)));
-    a.oct.box_lo[f] = make_float4(p.x, p.y, p.z, 0.f);
-    a.oct.box_hi[f] = make_float4(p.x, p.y, p.z, 0.f);
+    if (a.boxes) {
+      a.oct.box_lo[f] = make_float4(p.x, p.y, p.z, 0.f);
+      a.oct.box_hi[f] = make_float4(p.x, p.y, p.z, 0.f);
+    }
     return;
   }
   const int L = ((int)a.prefix[c] - a.disk_bits) / 3;
@@ -683,8 +686,10 @@ __device__ void write_node(const EmitArgs<K>& a, int c, int f) {
   a.oct.com[f] = com;
   a.oct.info[f] = make_int4(first_child, lo, ((hi - lo + 1) << 4) | k,
                             __float_as_int(ldexpf(rhs, -L)));
-  a.oct.box_lo[f] = make_float4(blo[0], blo[1], blo[2], 0.f);
-  a.oct.box_hi[f] = make_float4(bhi[0], bhi[1], bhi[2], 0.f);
+  if (a.boxes) {
+    a.oct.box_lo[f] = make_float4(blo[0], blo[1], blo[2], 0.f);
+    a.oct.box_hi[f] = make_float4(bhi[0], bhi[1], bhi[2], 0.f);
+  }
 }
 
 // One thread per record: slot f holds binary node node_of[f] (written by
@@ -898,7 +903,7 @@ void launch_octree(TreeWork& w, const K* keys, int n, int disk_bits, int n_roots
                   tsum,      w.groups, group_disk, w.n_nodes, w.n_groups,  w.group_spans};
   k_apply<K><<<mtiles, kMarkTile, 0, s>>>(ap);
   EmitArgs<K> a{n, disk_bits, n_roots, w.bin_lo, w.bin_hi, w.bin_prefix, keys, w.oct_nch,
-                w.oct_off, w.body4, w.mom_ploc, tpre, geoms, w.oct};
+                w.oct_off, w.body4, w.mom_ploc, tpre, geoms, w.oct, w.boxes};
   if (moments_ready && w.moments_on_side) check(cudaStreamWaitEvent(s, w.ev_join, 0), "moment join");
   // one thread per record for up to n / 2 records (about 0.35 n with leaves of
   // eight bodies); the loop covers any more
