@@ -287,6 +287,28 @@ def test_engine_steps_track_the_reference_loop(nb, cuda, port, precision, physic
     sim.close()
 
 
+@pytest.mark.parametrize("n", [1, 2, 3])
+def test_engine_steps_with_one_to_three_bodies(nb, cuda, port, n):
+    """The smallest systems through the engine (a one-record tree for one
+    body, the sort's values taken from the positions) against the oracle's
+    loop: with at most leaf-size bodies every force is a direct sum."""
+    st = disk(nb, 3, 0.5, 5.0, seed=2, m=1e-6)
+    st = {k: v[:n].copy() for k, v in st.items()}
+    prm = nb.sim_params(dt=0.01, theta=0.5, softening=1e-3, star_mass=1.0, r_coll=0.0,
+                        state_precision=0)
+    sim = nb.Sim(prm, n)
+    sim.set_state(st["x"], st["y"], st["z"], st["vx"], st["vy"], st["vz"], st["m"])
+    sim.step(10)
+    sim.sync()
+    got = sim.get_state()
+    ref = {k: st[k].copy() for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+    port.run(ref, port.step_params(0.01, 0.5, 1e-3, 1.0, r_coll=0.0), 10)
+    for k in ("x", "y", "z", "vx", "vy", "vz"):
+        assert np.allclose(got[k], ref[k], rtol=0, atol=1e-5), (k, got[k], ref[k])
+    assert sim.stats().status == 0
+    sim.close()
+
+
 # ------------------------------------------------------------ radix sort
 @pytest.mark.parametrize("n", [0, 1, 2, 1000, 131072, 200_000, 900_000, 1_400_000])
 def test_radix_sort_u32_is_a_stable_argsort(nb, cuda, n):
