@@ -246,28 +246,14 @@ __device__ __forceinline__ uint32_t pack_pinfo(int count, int level) {
   return ((uint32_t)min(count, (1 << 27) - 1) << 5) | (uint32_t)(level + 1);
 }
 
+// Writes internal node i: range end j, split offset s along direction d, and
+// dnode = delta(i, j).
 template <typename K>
-__global__ void __launch_bounds__(kThreads)
-k_karras(const K* __restrict__ keys, int n, int key_bits, int* __restrict__ left,
-         int* __restrict__ right, uint32_t* __restrict__ pinfo, int* __restrict__ lo_out,
-         int* __restrict__ hi_out, uint8_t* __restrict__ prefix) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n - 1) return;
-  const K ki = __ldg(keys + i);
-  const int d = (delta(keys, n, ki, i, i + 1) - delta(keys, n, ki, i, i - 1)) > 0 ? 1 : -1;
-  const int dmin = delta(keys, n, ki, i, i - d);
-  int lmax = 2;
-  while (delta(keys, n, ki, i, i + lmax * d) > dmin) lmax <<= 1;
-  int l = 0;
-  for (int t = lmax >> 1; t >= 1; t >>= 1)
-    if (delta(keys, n, ki, i, i + (l + t) * d) > dmin) l += t;
-  const int j = i + l * d;
-  const int dnode = delta(keys, n, ki, i, j);
-  int s = 0, t = l;
-  do {
-    t = (t + 1) >> 1;
-    if (delta(keys, n, ki, i, i + (s + t) * d) > dnode) s += t;
-  } while (t > 1);
+__device__ __forceinline__ void karras_write(int i, int j, int d, int s, int dnode, int n,
+                                             int key_bits, int* __restrict__ left,
+                                             int* __restrict__ right, uint32_t* __restrict__ pinfo,
+                                             int* __restrict__ lo_out, int* __restrict__ hi_out,
+                                             uint8_t* __restrict__ prefix) {
   const int gamma = i + s * d + min(d, 0);
   const int lo = min(i, j), hi = max(i, j);
   const int lc = (lo == gamma) ? (n - 1) + gamma : gamma;
@@ -284,6 +270,90 @@ k_karras(const K* __restrict__ keys, int n, int key_bits, int* __restrict__ left
   const uint32_t pi = pack_pinfo(hi - lo + 1, pre < disk_bits ? -1 : (pre - disk_bits) / 3);
   pinfo[lc] = pi;
   pinfo[rc] = pi;
+}
+
+// The whole warp narrows [lo, hi) to the last m with delta(i, i + m d) > thr
+// (true at lo, false at hi; the predicate only turns false once as m grows,
+// Karras 2012 sec. 3): each round every lane tests one of 31 evenly spaced
+// points and a ballot keeps the step after the last true one.
+template <typename K>
+__device__ __forceinline__ long long warp_last_above(const K* __restrict__ keys, int n, K ki,
+                                                     int i, int d, int thr, long long lo,
+                                                     long long hi, int lane) {
+  while (hi - lo > 1) {
+    const long long step = (hi - lo + 31) / 32;
+    const long long m = lo + (long long)(lane + 1) * step;
+    const bool q = m < hi && delta(keys, n, ki, i, i + (int)m * d) > thr;
+    const long long nlo = lo + (long long)__popc(__ballot_sync(kFull, q)) * step;
+    hi = min(hi, nlo + step);
+    lo = nlo;
+  }
+  return lo;
+}
+
+// One thread per internal node (Karras 2012, Fig. 4): direction, range end
+// by an exponential then a binary search, split by a binary search.  A warp
+// runs each search as many steps as its widest node needs, so a node whose
+// range reaches kKarrasCap bodies is handed to the whole warp instead, which
+// searches 32 points a step: the lanes' own searches stop at kKarrasCap.
+constexpr int kKarrasCap = 1024;
+
+template <typename K>
+__global__ void __launch_bounds__(kThreads)
+k_karras(const K* __restrict__ keys, int n, int key_bits, int* __restrict__ left,
+         int* __restrict__ right, uint32_t* __restrict__ pinfo, int* __restrict__ lo_out,
+         int* __restrict__ hi_out, uint8_t* __restrict__ prefix) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const bool act = i < n - 1;  // every lane stays for the warp's ballots
+  K ki = 0;
+  int d = 1, dmin = 0;
+  bool wide = false;
+  if (act) {
+    ki = __ldg(keys + i);
+    d = (delta(keys, n, ki, i, i + 1) - delta(keys, n, ki, i, i - 1)) > 0 ? 1 : -1;
+    dmin = delta(keys, n, ki, i, i - d);
+    int lmax = 2;
+    while (lmax <= kKarrasCap && delta(keys, n, ki, i, i + lmax * d) > dmin) lmax <<= 1;
+    wide = lmax > kKarrasCap;
+    if (!wide) {
+      int l = 0;
+      for (int t = lmax >> 1; t >= 1; t >>= 1)
+        if (delta(keys, n, ki, i, i + (l + t) * d) > dmin) l += t;
+      const int j = i + l * d;
+      const int dnode = delta(keys, n, ki, i, j);
+      int s = 0, t = l;
+      do {
+        t = (t + 1) >> 1;
+        if (delta(keys, n, ki, i, i + (s + t) * d) > dnode) s += t;
+      } while (t > 1);
+      karras_write<K>(i, j, d, s, dnode, n, key_bits, left, right, pinfo, lo_out, hi_out,
+                      prefix);
+    }
+  }
+  // wide nodes, one at a time: delta(i, i + kKarrasCap d) > dmin holds, and
+  // nothing lies beyond n - 1 steps
+  unsigned todo = __ballot_sync(kFull, wide);
+  while (todo) {
+    const int b = __ffs(todo) - 1;
+    todo &= todo - 1;
+    const int bi = __shfl_sync(kFull, i, b), bd = __shfl_sync(kFull, d, b);
+    const int bmin = __shfl_sync(kFull, dmin, b);
+    const K bk = __shfl_sync(kFull, ki, b);
+    // the power of two the range end lies below: lane k tests kKarrasCap << k
+    const long long mk = (long long)kKarrasCap << lane;
+    const bool p = mk < n && delta(keys, n, bk, bi, bi + (int)mk * bd) > bmin;
+    const int top = 31 - __clz(__ballot_sync(kFull, p) | 1u);
+    const long long lo = (long long)kKarrasCap << top;
+    const int l = (int)warp_last_above(keys, n, bk, bi, bd, bmin, lo, min(2 * lo, (long long)n),
+                                       lane);
+    const int j = bi + l * bd;
+    const int dnode = delta(keys, n, bk, bi, j);
+    const int s = (int)warp_last_above(keys, n, bk, bi, bd, dnode, 0ll, (long long)l, lane);
+    if (lane == b)
+      karras_write<K>(bi, j, bd, s, dnode, n, key_bits, left, right, pinfo, lo_out, hi_out,
+                      prefix);
+  }
 }
 
 // ------------------------------------------------------------- moments
