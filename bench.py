@@ -170,6 +170,9 @@ class Clocks:
             self.nvml = pynvml
             self.h = self._handle(pynvml, index)
             self.smax = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+            # both reads the poll makes, once here: a failure falls back to nvidia-smi
+            pynvml.nvmlDeviceGetClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            pynvml.nvmlDeviceGetCurrentClocksEventReasons(self.h)
             self.thread = threading.Thread(target=self._poll, daemon=True)
             self.thread.start()
             return
