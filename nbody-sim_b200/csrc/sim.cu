@@ -142,10 +142,14 @@ struct StreamArgs {
 
 // Fused step boundary.  kEnd: dv + K2 + drag (main.cu:131-139);
 // kBegin: K1 + drift (main.cu:104-107) + bbox of the new positions.
-template <typename R, bool kEnd, bool kBegin, bool kMulti = false>
-__global__ void __launch_bounds__(kThreads) k_stream(StateArrays<R> st, int n, StreamArgs a) {
+template <typename R, bool kEnd, bool kBegin, bool kMulti>
+__device__ __forceinline__ void stream_body(StateArrays<R> st, int n, const StreamArgs& a) {
   using C = typename ComputeOf<R>::type;
-  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  // FP32 state: the bbox in FP32 (a min or max of floats is one of them, so
+  // it equals the FP64 one it is widened to at the end)
+  using B = typename std::conditional<std::is_same<C, float>::value, float, double>::type;
+  B lo[3] = {(B)INFINITY, (B)INFINITY, (B)INFINITY};
+  B hi[3] = {-(B)INFINITY, -(B)INFINITY, -(B)INFINITY};
   for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
        s += (long long)gridDim.x * blockDim.x) {
     C x = (C)st.v[0][s], y = (C)st.v[1][s], z = (C)st.v[2][s];
@@ -210,9 +214,9 @@ __global__ void __launch_bounds__(kThreads) k_stream(StateArrays<R> st, int n, S
           atomicMin(bb + 2, ordered_bits((double)z)); atomicMax(bb + 5, ordered_bits((double)z));
         }
       } else {
-        lo[0] = fmin(lo[0], (double)x); hi[0] = fmax(hi[0], (double)x);
-        lo[1] = fmin(lo[1], (double)y); hi[1] = fmax(hi[1], (double)y);
-        lo[2] = fmin(lo[2], (double)z); hi[2] = fmax(hi[2], (double)z);
+        lo[0] = fmin(lo[0], (B)x); hi[0] = fmax(hi[0], (B)x);
+        lo[1] = fmin(lo[1], (B)y); hi[1] = fmax(hi[1], (B)y);
+        lo[2] = fmin(lo[2], (B)z); hi[2] = fmax(hi[2], (B)z);
       }
       st.v[0][s] = (R)x; st.v[1][s] = (R)y; st.v[2][s] = (R)z;
     }
@@ -223,7 +227,7 @@ __global__ void __launch_bounds__(kThreads) k_stream(StateArrays<R> st, int n, S
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-      double p = warp_min(lo[k]), q = warp_max(hi[k]);
+      const double p = (double)warp_min(lo[k]), q = (double)warp_max(hi[k]);
       if (lane == 0) { sb[k][warp] = p; sb[3 + k][warp] = q; }
     }
     __syncthreads();
@@ -237,6 +241,29 @@ __global__ void __launch_bounds__(kThreads) k_stream(StateArrays<R> st, int n, S
       }
     }
   }
+}
+
+template <typename R, bool kEnd, bool kBegin, bool kMulti = false>
+__global__ void __launch_bounds__(kThreads) k_stream(StateArrays<R> st, int n, StreamArgs a) {
+  stream_body<R, kEnd, kBegin, kMulti>(st, n, a);
+}
+
+// The fused boundary of FP32 steps (second kick, drag, first kick, drift) at
+// four blocks per SM (64 registers), so that more of its loads are in
+// flight; the other forms keep the compiler's choice (bounded like this the
+// FP64 ones would spill).
+template <bool kMulti>
+__global__ void __launch_bounds__(kThreads, 4)
+    k_stream_f32(StateArrays<float> st, int n, StreamArgs a) {
+  stream_body<float, true, true, kMulti>(st, n, a);
+}
+
+template <typename R, bool kEnd, bool kBegin, bool kMulti = false>
+void launch_stream(const StateArrays<R>& st, int n, const StreamArgs& a, int g, cudaStream_t s) {
+  if constexpr (std::is_same<R, float>::value && kEnd && kBegin)
+    k_stream_f32<kMulti><<<g, kThreads, 0, s>>>(st, n, a);
+  else
+    k_stream<R, kEnd, kBegin, kMulti><<<g, kThreads, 0, s>>>(st, n, a);
 }
 
 // Writes the state back in caller order (out[id[s]] = state[s]); with
@@ -909,11 +936,11 @@ struct SimImpl : SimBase {
     a.bbox = tw.bbox_enc;
     const int g = stream_grid(n);
     if (end && begin)
-      k_stream<R, true, true><<<g, kThreads, 0, st>>>(s[cur], n, a);
+      launch_stream<R, true, true>(s[cur], n, a, g, st);
     else if (end)
-      k_stream<R, true, false><<<g, kThreads, 0, st>>>(s[cur], n, a);
+      launch_stream<R, true, false>(s[cur], n, a, g, st);
     else
-      k_stream<R, false, true><<<g, kThreads, 0, st>>>(s[cur], n, a);
+      launch_stream<R, false, true>(s[cur], n, a, g, st);
     check(cudaGetLastError(), "k_stream launch");
   }
 
@@ -1726,9 +1753,9 @@ struct EnsembleImpl : EnsembleBase {
     a.decay = drag ? std::exp(-(double)p.gas_drag_rate * (double)p.dt) : 0.0;
     a.eps = p.softening; a.star_mass = p.star_mass; a.bbox = bbox;
     const int g = stream_grid(n);
-    if (end && begin) k_stream<R, true, true, true><<<g, kThreads, 0, st>>>(s[cur], n, a);
-    else if (end) k_stream<R, true, false, true><<<g, kThreads, 0, st>>>(s[cur], n, a);
-    else k_stream<R, false, true, true><<<g, kThreads, 0, st>>>(s[cur], n, a);
+    if (end && begin) launch_stream<R, true, true, true>(s[cur], n, a, g, st);
+    else if (end) launch_stream<R, true, false, true>(s[cur], n, a, g, st);
+    else launch_stream<R, false, true, true>(s[cur], n, a, g, st);
     check(cudaGetLastError(), "k_stream launch");
     launches += 1;
   }
